@@ -1,0 +1,257 @@
+// ORACLE (test infrastructure only; never linked into the product library).
+//
+// Runs the reference's OWN templates (compiled from the reference's source tree,
+// with oracle/shim ahead of it on the include path in place of Eigen) on the
+// benchmark problems and writes .npy fixtures:
+//   * the mesh and DOF maps the reference builds (host inputs of the hot path),
+//   * the assembled saddle blocks A_y, B, C_signed, f, g
+//     (finite_element::system::assemble_main_system_blocks,
+//      src/finite_element/system/assemble_saddle_problem.hpp:131),
+//   * the parabolic graph-norm Schur approximation Hhat
+//     (src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:22).
+//
+// usage: apf_ref_dump <dim:2> <p:1|2> <uniform_levels> <example> <outdir>
+
+#include <cstdio>
+#include <cstdlib>
+#include <filesystem>
+#include <limits>
+#include <unordered_map>
+#include <unordered_set>
+#include <algorithm>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "linear_algebra/eigen_backend/backend.hpp"
+
+#include "algorithm/example_registry.hpp"
+#include "algorithm/examples/space_time_2d/initial_data_2d_examples.hpp"
+#include "algorithm/examples/space_time_2d/space_time_2d_example.hpp"
+#include "algorithm/support/space_time_1d.hpp"
+#include "algorithm/support/space_time_2d.hpp"
+#include "finite_element/fespace/fe_traits.hpp"
+#include "finite_element/fespace/fespace.hpp"
+#include "finite_element/fespace/policies.hpp"
+#include "finite_element/system/assemble_saddle_problem.hpp"
+#include "finite_element/assembly/main_system/parabolic_graph_norm.hpp"
+#include "finite_element/assembly/constrained_dofs.hpp"
+#include "mesh/mesh_traits.hpp"
+
+#include "npy.hpp"
+
+namespace
+{
+    using Backend = la::eigen::Backend;
+
+    void dump_csc(const std::string& dir, const std::string& name, const la::eigen::SparseMatrix& A)
+    {
+        apf_oracle::write_npy(dir + "/" + name + "_outer.npy", A.outer());
+        apf_oracle::write_npy(dir + "/" + name + "_inner.npy", A.inner());
+        apf_oracle::write_npy(dir + "/" + name + "_values.npy", A.values());
+        const std::vector<int> shape{A.rows(), A.cols()};
+        apf_oracle::write_npy(dir + "/" + name + "_shape.npy", shape);
+    }
+
+    void dump_vec(const std::string& dir, const std::string& name, const la::eigen::Vector& v)
+    {
+        apf_oracle::write_npy(dir + "/" + name + ".npy", v.storage());
+    }
+
+    // Flattened CellRestriction for a list of cells:
+    // offsets[c*ndof + i] .. offsets[c*ndof+i+1] index (true_dof, weight) pairs.
+    template<class Space>
+    void dump_restrictions(const std::string& dir, const std::string& name, const Space& space, const std::vector<int>& cells)
+    {
+        std::vector<int> offsets{0};
+        std::vector<int> dofs;
+        std::vector<double> weights;
+        for (const int c : cells)
+        {
+            const auto r = finite_element::assembly::build_cell_restriction(space, c);
+            for (int i = 0; i < r.size(); ++i)
+            {
+                for (const auto& e : r[i])
+                {
+                    dofs.push_back(e.true_dof);
+                    weights.push_back(e.weight);
+                }
+                offsets.push_back(static_cast<int>(dofs.size()));
+            }
+        }
+        apf_oracle::write_npy(dir + "/" + name + "_offsets.npy", offsets);
+        apf_oracle::write_npy(dir + "/" + name + "_dofs.npy", dofs);
+        apf_oracle::write_npy(dir + "/" + name + "_weights.npy", weights);
+    }
+
+    // Per cell: x0 y0 x1 y1 x2 y2 t0 t1 (vertex order of the reference cell).
+    template<class Space>
+    void dump_geometry_2d(const std::string& dir, const std::string& name, const Space& space, const std::vector<int>& cells)
+    {
+        const auto& mesh = space.mesh_ref();
+        std::vector<double> g;
+        g.reserve(cells.size() * 8u);
+        for (const int c : cells)
+        {
+            const auto& cell = mesh.cell(c);
+            for (int k = 0; k < 3; ++k)
+            {
+                const auto& v = mesh.spatial_vertices()[cell.spatial_vertex_ids[k]];
+                g.push_back(v[0]);
+                g.push_back(v[1]);
+            }
+            g.push_back(mesh.temporal_vertices()[cell.temporal_vertex_ids[0]][0]);
+            g.push_back(mesh.temporal_vertices()[cell.temporal_vertex_ids[1]][0]);
+        }
+        apf_oracle::write_npy(dir + "/" + name + ".npy", g.data(), {cells.size(), 8u});
+    }
+
+
+    // Mirror of the reference driver's uniform isotropic X refinement
+    // (algorithm/adaptive_driver.hpp:1482-1830, refine_space_uniform_isotropically_):
+    // spatial waves over all active descendants of the marked parents until every
+    // descendant's x- and y-extent is strictly smaller than its parent's, then one
+    // temporal split of every descendant.  One call = one `uniform_standard`
+    // outer iteration of the paper runs.
+    template<class Space>
+    void uniform_isotropic_refine(Space& space)
+    {
+        auto& mesh = space.unsafe_mesh_ref();
+        struct Ext { double sx, sy, t; };
+        auto extents = [&](int c) {
+            const auto& cell = mesh.cell(c);
+            const auto& sv = mesh.spatial_vertices();
+            const auto& tv = mesh.temporal_vertices();
+            double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300, mnt = 1e300, mxt = -1e300;
+            for (const int v : cell.spatial_vertex_ids) {
+                mnx = std::min(mnx, sv[v][0]); mxx = std::max(mxx, sv[v][0]);
+                mny = std::min(mny, sv[v][1]); mxy = std::max(mxy, sv[v][1]);
+            }
+            for (const int v : cell.temporal_vertex_ids) { mnt = std::min(mnt, tv[v][0]); mxt = std::max(mxt, tv[v][0]); }
+            return Ext{mxx - mnx, mxy - mny, mxt - mnt};
+        };
+        auto smaller = [](double child, double parent) {
+            const double tol = 64.0 * std::numeric_limits<double>::epsilon() * std::max(1.0, parent);
+            return child < parent - tol;
+        };
+        std::unordered_map<int, Ext> parents;
+        for (const int c : space.active_cells()) parents.emplace(c, extents(c));
+        auto ancestor = [&](int c) {
+            while (c >= 0) { if (parents.count(c)) return c; c = mesh.cell(c).parent_id; }
+            return -1;
+        };
+        auto refine_all = [&](const std::vector<int>& ids, mesh::RefinementType type) {
+            std::unordered_set<int> add_ids, remove_ids;
+            std::vector<int> changed;
+            for (const int c : ids) {
+                if (!space.is_active_cell(c)) continue;
+                mesh.refine_storage_leaf_without_closure(c, type);
+                remove_ids.insert(c);
+                changed.push_back(c);
+                for (const int ch : mesh.cell(c).children) { add_ids.insert(ch); changed.push_back(ch); }
+            }
+            space.unsafe_update_active_cells(add_ids, remove_ids);
+            std::sort(changed.begin(), changed.end());
+            changed.erase(std::unique(changed.begin(), changed.end()), changed.end());
+            space.rebuild_incremental_after_refinement(changed);
+        };
+        for (int wave = 0; wave < 32; ++wave) {
+            bool all_smaller = true;
+            for (const int c : space.active_cells()) {
+                const auto e = extents(c);
+                const auto& pe = parents.at(ancestor(c));
+                if (!(smaller(e.sx, pe.sx) && smaller(e.sy, pe.sy))) { all_smaller = false; break; }
+            }
+            const std::vector<int> targets(space.active_cells().begin(), space.active_cells().end());
+            if (all_smaller) { refine_all(targets, mesh::RefinementType::temporal); return; }
+            refine_all(targets, mesh::RefinementType::spatial);
+        }
+        throw std::runtime_error("uniform_isotropic_refine: no spatial shrink after 32 waves");
+    }
+
+    template<int P>
+    int run_2d(int levels, const std::string& example_name, const std::string& dir)
+    {
+        constexpr int QSpace = 4 * P + 1;
+        constexpr int QTime = 2 * P + 1;
+        using GT = mesh::MeshTraits<2>;
+        using FET = finite_element::FiniteElementTraits<GT, P, P>;
+        using XSpace = finite_element::FESpace<GT, FET, finite_element::SpaceTimePolicy>;
+        using YSpace = finite_element::FESpace<GT, FET, finite_element::SpaceOnlyPolicy>;
+
+        auto example = adaptive_algorithm::examples::make_2d_example(example_name);
+        auto mesh = adaptive_algorithm::examples::make_initial_mesh_from_example(example);
+        XSpace x_space(mesh);
+        YSpace y_space(mesh);
+        adaptive_algorithm::examples::initialize_spaces_from_example(x_space, y_space, example);
+        for (int k = 0; k < levels; ++k)
+            uniform_isotropic_refine(x_space);
+        y_space.initialize(x_space.active_cells());
+
+        const auto& y_cells = y_space.active_cells();
+        const auto& x_cells = x_space.active_cells();
+        std::cerr << "2d p=" << P << " levels=" << levels << " x_cells=" << x_cells.size()
+                  << " y_cells=" << y_cells.size()
+                  << " n_x=" << x_space.dof_handler_ref().n_true_dofs()
+                  << " n_y=" << y_space.dof_handler_ref().n_true_dofs() << "\n";
+
+        std::filesystem::create_directories(dir);
+        dump_geometry_2d(dir, "y_geometry", y_space, y_cells);
+        dump_geometry_2d(dir, "x_geometry", x_space, x_cells);
+        dump_restrictions(dir, "y_restriction", y_space, y_cells);
+        dump_restrictions(dir, "x_restriction", x_space, x_cells);
+        {
+            finite_element::assembly::detail::ActiveAncestorCache<XSpace> cache(x_space);
+            std::vector<int> x_pos(static_cast<std::size_t>(mesh.n_cells()), -1);
+            for (std::size_t k = 0; k < x_cells.size(); ++k)
+                x_pos[static_cast<std::size_t>(x_cells[k])] = static_cast<int>(k);
+            std::vector<int> anc;
+            for (const int c : y_cells)
+                anc.push_back(x_pos[static_cast<std::size_t>(cache.find(c))]);
+            apf_oracle::write_npy(dir + "/y_to_x_cell.npy", anc);
+            apf_oracle::write_npy(dir + "/y_cell_ids.npy", y_cells);
+            apf_oracle::write_npy(dir + "/x_cell_ids.npy", x_cells);
+        }
+
+        const auto blocks = finite_element::system::assemble_main_system_blocks<QSpace, QTime, Backend>(
+            y_space, x_space, example.problem, 1e-15, -1.0);
+        dump_csc(dir, "A_y", blocks.A_y());
+        dump_csc(dir, "B", blocks.lower_left_B());
+        dump_csc(dir, "C_signed", blocks.C_signed());
+        dump_vec(dir, "f", blocks.f());
+        dump_vec(dir, "g", blocks.g());
+
+        const auto gn = finite_element::assembly::assemble_parabolic_graph_norm_approximation<QSpace, QTime, Backend>(
+            y_space, x_space, example.problem.M, blocks.A_y(), blocks.C_signed(), 1e-15, 1e-14);
+        dump_csc(dir, "Hhat", gn.approximation.hhat);
+        return 0;
+    }
+}
+
+int main(int argc, char** argv)
+{
+    if (argc != 6)
+    {
+        std::fprintf(stderr, "usage: %s <dim:2> <p:1|2> <uniform_levels> <example> <outdir>\n", argv[0]);
+        return 2;
+    }
+    const int dim = std::atoi(argv[1]);
+    const int p = std::atoi(argv[2]);
+    const int levels = std::atoi(argv[3]);
+    const std::string example = argv[4];
+    const std::string dir = argv[5];
+    try
+    {
+        if (dim == 2 && p == 1)
+            return run_2d<1>(levels, example, dir);
+        if (dim == 2 && p == 2)
+            return run_2d<2>(levels, example, dir);
+    }
+    catch (const std::exception& e)
+    {
+        std::fprintf(stderr, "apf_ref_dump: %s\n", e.what());
+        return 1;
+    }
+    std::fprintf(stderr, "unsupported case\n");
+    return 2;
+}
