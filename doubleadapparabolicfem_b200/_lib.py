@@ -1,0 +1,105 @@
+"""ctypes binding of libapf_b200.so (the C ABI declared in include/apf_b200.h).
+
+The shared library is built in-tree by ``doubleadapparabolicfem_b200.build``.
+Loading fails loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libapf_b200.so")
+
+APF_OK = 0
+APF_ERR_INVALID = -1
+APF_ERR_CUDA = -2
+APF_ERR_CAPACITY = -3
+APF_ERR_NUMERIC = -4
+APF_ERR_NOT_CONVERGED = -5
+APF_ERR_NO_DEVICE = -6
+APF_ERR_INTERNAL = -7
+
+APF_U0_SIN_SIN = 0
+APF_U0_ONE = 1
+APF_U0_ZERO = 2
+
+BLOCKS = {"A_y": 0, "B": 1, "BT": 2, "C_signed": 3, "K": 4, "Hhat": 5, "B_dt": 6, "A_x": 7}
+APF_VEC_F = 0
+APF_VEC_G = 1
+
+
+class ApfError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"apf error {code}: {message}")
+        self.code = code
+
+
+class ProblemDesc(C.Structure):
+    _fields_ = [
+        ("p", C.c_int),
+        ("n_y_cells", C.c_int),
+        ("n_x_cells", C.c_int),
+        ("n_lambda", C.c_int),
+        ("n_u", C.c_int),
+        ("y_geometry", C.c_void_p),
+        ("x_geometry", C.c_void_p),
+        ("y_to_x", C.c_void_p),
+        ("y_restr_offsets", C.c_void_p),
+        ("y_restr_dofs", C.c_void_p),
+        ("y_restr_weights", C.c_void_p),
+        ("y_restr_nnz", C.c_int32),
+        ("x_restr_offsets", C.c_void_p),
+        ("x_restr_dofs", C.c_void_p),
+        ("x_restr_weights", C.c_void_p),
+        ("x_restr_nnz", C.c_int32),
+        ("m_cells", C.c_void_p),
+        ("ell_cells", C.c_void_p),
+        ("u0_kind", C.c_int),
+        ("zero_tol", C.c_double),
+        ("g_scale", C.c_double),
+    ]
+
+
+_lib = None
+
+# exported symbols and their signatures (argtypes, restype)
+SIGNATURES = {
+    "apf_ctx_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
+    "apf_ctx_destroy": ([C.c_void_p], None),
+    "apf_ctx_last_error": ([C.c_void_p], C.c_char_p),
+    "apf_ctx_synchronize": ([C.c_void_p], C.c_int),
+    "apf_ctx_kernel_launches": ([C.c_void_p], C.c_int64),
+    "apf_assemble_main_system": ([C.c_void_p, C.POINTER(ProblemDesc), C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "apf_assemble_graph_norm": ([C.c_void_p, C.c_void_p, C.c_double], C.c_int),
+    "apf_system_block_info": ([C.c_void_p, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                               C.POINTER(C.c_int64)], C.c_int),
+    "apf_system_block_copy": ([C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "apf_system_block_device_ptrs": ([C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                      C.POINTER(C.c_void_p)], C.c_int),
+    "apf_system_vector_copy": ([C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int], C.c_int),
+    "apf_system_destroy": ([C.c_void_p], None),
+}
+
+
+def load():
+    """Load libapf_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m doubleadapparabolicfem_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def check(ctx, rc: int):
+    if rc != APF_OK:
+        lib = load()
+        msg = lib.apf_ctx_last_error(ctx).decode() if ctx else ""
+        raise ApfError(rc, msg)

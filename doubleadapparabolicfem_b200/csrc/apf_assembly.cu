@@ -1,0 +1,1108 @@
+// Main-system assembly on the device: A_y, B, B^T, C_signed, f, g, K, and the
+// parabolic graph-norm block Hhat = -C_signed + B_dt diag(A_y)^-1 B_dt^T + A_x.
+//
+// Design (B200): assembly is "pull" (row gather), not triplet scatter.
+//   1. incidence lists: true DOF -> (cell, local index, restriction entry), built
+//      with a count / scan / fill pass;
+//   2. one warp per matrix row gathers every candidate (column, value) of that row
+//      from its incident cells -- local entries recomputed in closed form from the
+//      cell geometry (affine prisms, cell-constant M) and filtered with
+//      |a_ij| > zero_tol exactly like scatter.hpp:66-115 -- sorts the candidates
+//      in shared memory (bitonic, key = column | deterministic sequence number)
+//      and sums duplicates in a fixed order.  A count pass sizes the rows, a
+//      scan gives row_ptr, a fill pass writes columns and values once.
+// The result is the reference's compressed pattern bit for bit (setFromTriplets
+// keeps summed explicit zeros, so does this) and deterministic values with no
+// floating-point atomics.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+
+#include "apf_device.cuh"
+#include "apf_internal.hpp"
+#include "apf_system.hpp"
+
+namespace apf
+{
+    __constant__ RefTables c_tab[2];
+
+    std::atomic<long long> g_kernel_launches{0};
+
+    namespace
+    {
+        // ------------------------------------------------------------------
+        // incidence lists
+        // ------------------------------------------------------------------
+        // An "assembly cell" a (index into cell_list or the identity) takes its
+        // row restriction from source cell src(a) = src_map ? src_map[cell] : cell.
+        struct IncidenceSpec
+        {
+            int n_asm;                 // number of assembly cells
+            const int* cell_list;      // optional: assembly cell -> cell index
+            const int* src_map;        // optional: cell -> restriction source cell
+            const int* offsets;        // restriction offsets [n_src*ndof+1]
+            const int* dofs;
+            int ndof;
+        };
+
+        __device__ __forceinline__ int asm_cell(const IncidenceSpec& s, int a)
+        {
+            return s.cell_list ? s.cell_list[a] : a;
+        }
+        __device__ __forceinline__ int src_cell(const IncidenceSpec& s, int c)
+        {
+            return s.src_map ? s.src_map[c] : c;
+        }
+
+        __global__ void incidence_count(IncidenceSpec s, int* __restrict__ count)
+        {
+            const long long total = static_cast<long long>(s.n_asm) * s.ndof;
+            for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+                 k += (long long)gridDim.x * blockDim.x)
+            {
+                const int a = static_cast<int>(k / s.ndof), i = static_cast<int>(k % s.ndof);
+                const int c = asm_cell(s, a);
+                const int r = src_cell(s, c) * s.ndof + i;
+                for (int e = s.offsets[r]; e < s.offsets[r + 1]; ++e)
+                    atomicAdd(&count[s.dofs[e]], 1);
+            }
+        }
+
+        __global__ void incidence_fill(IncidenceSpec s, const int* __restrict__ ptr, int* __restrict__ cursor,
+                                       int2* __restrict__ inc)
+        {
+            const long long total = static_cast<long long>(s.n_asm) * s.ndof;
+            for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+                 k += (long long)gridDim.x * blockDim.x)
+            {
+                const int a = static_cast<int>(k / s.ndof), i = static_cast<int>(k % s.ndof);
+                const int c = asm_cell(s, a);
+                const int r = src_cell(s, c) * s.ndof + i;
+                for (int e = s.offsets[r]; e < s.offsets[r + 1]; ++e)
+                {
+                    const int d = s.dofs[e];
+                    const int pos = ptr[d] + atomicAdd(&cursor[d], 1);
+                    inc[pos] = make_int2(c * s.ndof + i, e);
+                }
+            }
+        }
+
+        __global__ void max_row_length(const int* __restrict__ ptr, int n, int* __restrict__ out)
+        {
+            int m = 0;
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                m = max(m, ptr[i + 1] - ptr[i]);
+            for (int o = 16; o > 0; o >>= 1)
+                m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0)
+                atomicMax(out, m);
+        }
+
+        // ------------------------------------------------------------------
+        // local block evaluators
+        // ------------------------------------------------------------------
+        struct AsmData
+        {
+            int p;
+            const double* y_geo;
+            const double* x_geo;
+            const int* y_to_x;
+            const double* m_y; // per Y cell or null
+            const double* m_x; // per X cell or null
+            const int* y_off;
+            const int* y_dofs;
+            const double* y_w;
+            const int* x_off;
+            const int* x_dofs;
+            const double* x_w;
+            double zero_tol;
+        };
+
+        // local entry L_c(i, j) of block `kind` on assembly cell c
+        __device__ double local_entry(const AsmData& d, int kind, int c, int i, int j)
+        {
+            const RefTables& t = c_tab[d.p - 1];
+            if (kind == K_AY || kind == K_AX)
+            {
+                const double* geo = kind == K_AY ? d.y_geo : d.x_geo;
+                const double* m = kind == K_AY ? d.m_y : d.m_x;
+                const CellGeo g = load_geo(geo, c);
+                double q00, q01, q11;
+                q_form(g, m, c, q00, q01, q11);
+                const int s = i / t.nt, a = i % t.nt, r = j / t.nt, b = j % t.nt;
+                return g.det * g.ht * t.Mt[a][b] * ks(t, q00, q01, q11, s, r);
+            }
+            if (kind == K_C)
+            {
+                const CellGeo g = load_geo(d.x_geo, c);
+                const int s = i / t.nt, a = i % t.nt, r = j / t.nt, b = j % t.nt;
+                return -(g.det * t.Mx[s][r] * t.S0[a] * t.S0[b]);
+            }
+            // mixed blocks: row index of B is the X-local index
+            int ix = i, jy = j;
+            if (kind == K_BT || kind == K_BDTT)
+            {
+                ix = j;
+                jy = i;
+            }
+            const bool dt_only = kind == K_BDT || kind == K_BDTT;
+            const int cx = d.y_to_x[c];
+            const CellGeo gy = load_geo(d.y_geo, c);
+            double q00, q01, q11;
+            q_form(gy, d.m_y, c, q00, q01, q11);
+            if (same_geometry(d.y_geo, c, d.x_geo, cx))
+                return b_same(t, gy, q00, q01, q11, ix, jy, dt_only);
+            const CellGeo gx = load_geo(d.x_geo, cx);
+            double v = 0.0;
+            for (int k = 0; k < t.ndof; ++k)
+                v += transfer(t, gy, gx, ix, k) * b_same(t, gy, q00, q01, q11, k, jy, dt_only);
+            return v;
+        }
+
+        // column restriction of local column j on assembly cell c
+        __device__ __forceinline__ void col_restriction(const AsmData& d, int kind, int c, int j, int ndof,
+                                                        const int*& dofs, const double*& w, int& b, int& e)
+        {
+            if (kind == K_AY || kind == K_B || kind == K_BDT)
+            {
+                const int r = c * ndof + j;
+                b = d.y_off[r];
+                e = d.y_off[r + 1];
+                dofs = d.y_dofs;
+                w = d.y_w;
+                return;
+            }
+            const int cx = (kind == K_BT || kind == K_BDTT) ? d.y_to_x[c] : c;
+            const int r = cx * ndof + j;
+            b = d.x_off[r];
+            e = d.x_off[r + 1];
+            dofs = d.x_dofs;
+            w = d.x_w;
+        }
+
+        __device__ __forceinline__ const double* row_weights(const AsmData& d, int kind)
+        {
+            return (kind == K_AY || kind == K_BT || kind == K_BDTT) ? d.y_w : d.x_w;
+        }
+
+        // ------------------------------------------------------------------
+        // warp-level candidate sort / reduce
+        // ------------------------------------------------------------------
+        // key = col (high 32) | seq (17 bits) | slot (15 bits)
+        constexpr int kSlotBits = 15;
+        constexpr int kSeqBits = 17;
+
+        __device__ __forceinline__ unsigned long long make_key(int col, int seq, int slot)
+        {
+            return (static_cast<unsigned long long>(static_cast<unsigned>(col)) << 32) |
+                   (static_cast<unsigned long long>(seq & ((1 << kSeqBits) - 1)) << kSlotBits) |
+                   static_cast<unsigned long long>(slot);
+        }
+
+        // In-place ascending bitonic sort of n (power of two) keys by one warp.
+        __device__ void warp_bitonic_sort(unsigned long long* keys, int n)
+        {
+            const int lane = threadIdx.x & 31;
+            for (int k = 2; k <= n; k <<= 1)
+            {
+                for (int j = k >> 1; j > 0; j >>= 1)
+                {
+                    for (int i = lane; i < n; i += 32)
+                    {
+                        const int ixj = i ^ j;
+                        if (ixj > i)
+                        {
+                            const unsigned long long a = keys[i], b = keys[ixj];
+                            const bool up = (i & k) == 0;
+                            if ((a > b) == up)
+                            {
+                                keys[i] = b;
+                                keys[ixj] = a;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+
+        struct Term
+        {
+            int kind;
+            const int* inc_ptr;
+            const int2* inc;
+            int col_offset;
+        };
+
+        struct GatherArgs
+        {
+            AsmData d;
+            int n_rows;
+            int ndof;
+            int n_terms;
+            Term term[2];
+            int* row_count;      // count pass output
+            const int* row_ptr;  // fill pass input
+            int* col_out;
+            double* val_out;
+            int* status;         // nonzero on overflow
+        };
+
+        // One warp per row.  CAP candidates per warp in shared memory.
+        template<int CAP, bool FILL>
+        __global__ void __launch_bounds__(128) gather_rows(GatherArgs A)
+        {
+            constexpr int kIncCap = 256;
+            extern __shared__ unsigned char smem_raw[];
+            const int warps = blockDim.x >> 5;
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
+            double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
+                           (size_t)w * CAP;
+            int* incs = reinterpret_cast<int*>(reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) +
+                                                                         (size_t)warps * CAP) +
+                                               (size_t)warps * CAP) +
+                        (size_t)w * (2 * kIncCap + 1);
+            int* counter = incs + 2 * kIncCap;
+            const int ndof = A.ndof;
+
+            for (int row = blockIdx.x * warps + w; row < A.n_rows; row += gridDim.x * warps)
+            {
+                if (lane == 0)
+                    *counter = 0;
+                __syncwarp();
+                int seq_base = 0;
+                bool overflow = false;
+                for (int tt = 0; tt < A.n_terms; ++tt)
+                {
+                    const Term T = A.term[tt];
+                    const int ib = T.inc_ptr[row], ie = T.inc_ptr[row + 1];
+                    const int n_inc = ie - ib;
+                    if (n_inc > kIncCap)
+                    {
+                        overflow = true;
+                        break;
+                    }
+                    // stage the incidence list and sort it by (cell*ndof+i) -> deterministic order
+                    for (int k = lane; k < n_inc; k += 32)
+                    {
+                        const int2 v = T.inc[ib + k];
+                        incs[k] = v.x;
+                        incs[kIncCap + k] = v.y;
+                    }
+                    __syncwarp();
+                    int my_ci[8], my_e[8], my_rank[8];
+                    int nm = 0;
+                    for (int k = lane; k < n_inc; k += 32, ++nm)
+                    {
+                        const int ci = incs[k];
+                        int rank = 0;
+                        for (int q = 0; q < n_inc; ++q)
+                            rank += incs[q] < ci;
+                        my_ci[nm] = ci;
+                        my_e[nm] = incs[kIncCap + k];
+                        my_rank[nm] = rank;
+                    }
+                    __syncwarp();
+                    for (int q = 0; q < nm; ++q)
+                    {
+                        incs[my_rank[q]] = my_ci[q];
+                        incs[kIncCap + my_rank[q]] = my_e[q];
+                    }
+                    __syncwarp();
+                    const double* rw = row_weights(A.d, T.kind);
+                    const int items = n_inc * ndof;
+                    for (int it = lane; it < items + ((32 - items % 32) % 32); it += 32)
+                    {
+                        const bool active = it < items;
+                        int nloc = 0;
+                        int cols_l[4];
+                        double vals_l[4];
+                        int seqs_l[4];
+                        int more = 0;
+                        if (active)
+                        {
+                            const int t_idx = it / ndof, j = it % ndof;
+                            const int ci = incs[t_idx];
+                            const int c = ci / ndof, i = ci % ndof;
+                            const double wi = rw[incs[kIncCap + t_idx]];
+                            const double v = local_entry(A.d, T.kind, c, i, j);
+                            if (fabs(v) > A.d.zero_tol)
+                            {
+                                const int* cd;
+                                const double* cw;
+                                int b, e;
+                                col_restriction(A.d, T.kind, c, j, ndof, cd, cw, b, e);
+                                for (int q = b; q < e; ++q)
+                                {
+                                    if (nloc < 4)
+                                    {
+                                        cols_l[nloc] = cd[q] + T.col_offset;
+                                        vals_l[nloc] = wi * cw[q] * v;
+                                        seqs_l[nloc] = seq_base + it * 4 + (q - b);
+                                        ++nloc;
+                                    }
+                                    else
+                                        more = 1;
+                                }
+                            }
+                        }
+                        if (__any_sync(0xffffffffu, more))
+                            overflow = true;
+                        // warp-aggregated append
+                        int incl = nloc;
+                        for (int o = 1; o < 32; o <<= 1)
+                        {
+                            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                            if (lane >= o) incl += y;
+                        }
+                        const int base = *counter;
+                        const int total = __shfl_sync(0xffffffffu, incl, 31);
+                        const int start = base + incl - nloc;
+                        for (int q = 0; q < nloc; ++q)
+                        {
+                            const int slot = start + q;
+                            if (slot < CAP)
+                            {
+                                keys[slot] = make_key(cols_l[q], seqs_l[q], slot);
+                                vals[slot] = vals_l[q];
+                            }
+                        }
+                        __syncwarp();
+                        if (lane == 0)
+                            *counter = base + total;
+                        __syncwarp();
+                    }
+                    seq_base += items * 4;
+                }
+                const int n = *counter;
+                if (n > CAP || overflow || seq_base >= (1 << kSeqBits))
+                {
+                    if (lane == 0)
+                        atomicExch(A.status, APF_ERR_CAPACITY);
+                    if (!FILL && lane == 0)
+                        A.row_count[row] = 0;
+                    __syncwarp();
+                    continue;
+                }
+                int np = 1;
+                while (np < n) np <<= 1;
+                for (int k = n + lane; k < np; k += 32)
+                    keys[k] = ~0ull;
+                __syncwarp();
+                warp_bitonic_sort(keys, np);
+                // heads of equal-column runs
+                int out_base = FILL ? A.row_ptr[row] : 0;
+                int uniq = 0;
+                for (int k0 = 0; k0 < n; k0 += 32)
+                {
+                    const int k = k0 + lane;
+                    bool head = false;
+                    unsigned col = 0;
+                    if (k < n)
+                    {
+                        col = static_cast<unsigned>(keys[k] >> 32);
+                        head = (k == 0) || (static_cast<unsigned>(keys[k - 1] >> 32) != col);
+                    }
+                    const unsigned hm = __ballot_sync(0xffffffffu, head);
+                    if (FILL && head)
+                    {
+                        double s = 0.0;
+                        for (int q = k; q < n && static_cast<unsigned>(keys[q] >> 32) == col; ++q)
+                            s += vals[keys[q] & ((1u << kSlotBits) - 1)];
+                        const int pos = out_base + uniq + __popc(hm & ((1u << lane) - 1));
+                        A.col_out[pos] = static_cast<int>(col);
+                        A.val_out[pos] = s;
+                    }
+                    uniq += __popc(hm);
+                }
+                if (!FILL && lane == 0)
+                    A.row_count[row] = uniq;
+                __syncwarp();
+            }
+        }
+
+        // ------------------------------------------------------------------
+        // vectors f, g (one thread per row; deterministic order after sorting)
+        // ------------------------------------------------------------------
+        struct VecArgs
+        {
+            AsmData d;
+            int n_rows;
+            int ndof;
+            const int* inc_ptr;
+            const int2* inc;
+            int which;            // 0 = f (Y cells, ell), 1 = g (bottom X cells, u0)
+            const double* ell;    // per Y cell
+            int u0_kind;
+            double g_scale;
+            double* out;
+            int* status;
+        };
+
+        __device__ double u0_value(int kind, double x, double y)
+        {
+            if (kind == APF_U0_SIN_SIN)
+                return sinpi(x) * sinpi(y);
+            if (kind == APF_U0_ONE)
+                return 1.0;
+            return 0.0;
+        }
+
+        __device__ double local_vector(const VecArgs& A, int c, int i)
+        {
+            const RefTables& t = c_tab[A.d.p - 1];
+            const int s = i / t.nt, a = i % t.nt;
+            if (A.which == 0)
+            {
+                if (!A.ell)
+                    return 0.0;
+                const CellGeo g = load_geo(A.d.y_geo, c);
+                return A.ell[c] * g.det * g.ht * t.ix[s] * t.it[a];
+            }
+            const CellGeo g = load_geo(A.d.x_geo, c);
+            double acc = 0.0;
+            for (int q = 0; q < t.nbq; ++q)
+            {
+                const double xi = t.bq_pts[q][0], eta = t.bq_pts[q][1];
+                const double x = g.x0 + g.J00 * xi + g.J01 * eta;
+                const double y = g.y0 + g.J10 * xi + g.J11 * eta;
+                acc += A.g_scale * u0_value(A.u0_kind, x, y) * (t.bq_T[q][s] * t.S0[a]) * (g.det * t.bq_w[q]);
+            }
+            return acc;
+        }
+
+        __global__ void gather_vector(VecArgs A)
+        {
+            constexpr int kMaxInc = 64;
+            for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.n_rows; row += gridDim.x * blockDim.x)
+            {
+                const int b = A.inc_ptr[row], e = A.inc_ptr[row + 1];
+                if (e - b > kMaxInc)
+                {
+                    atomicExch(A.status, APF_ERR_CAPACITY);
+                    continue;
+                }
+                // visit incidences in ascending (cell*ndof+i) order
+                int last = -1;
+                double s = 0.0;
+                for (int step = 0; step < e - b; ++step)
+                {
+                    int best = 0x7fffffff, best_e = -1;
+                    for (int q = b; q < e; ++q)
+                    {
+                        const int ci = A.inc[q].x;
+                        if (ci > last && ci < best)
+                        {
+                            best = ci;
+                            best_e = A.inc[q].y;
+                        }
+                    }
+                    last = best;
+                    const int c = best / A.ndof, i = best % A.ndof;
+                    const double v = local_vector(A, c, i);
+                    if (fabs(v) > A.d.zero_tol)
+                    {
+                        const double* w = A.which == 0 ? A.d.y_w : A.d.x_w;
+                        s += w[best_e] * v;
+                    }
+                }
+                A.out[row] = s;
+            }
+        }
+
+        // ------------------------------------------------------------------
+        // CSR algebra: K = [A B^T; B C] and Hhat
+        // ------------------------------------------------------------------
+        __global__ void k_row_counts(int n_lambda, int n_u, const int* __restrict__ a_ptr, const int* __restrict__ bt_ptr,
+                                     const int* __restrict__ b_ptr, const int* __restrict__ c_ptr, int* __restrict__ cnt)
+        {
+            const int n = n_lambda + n_u;
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+            {
+                if (r < n_lambda)
+                    cnt[r] = (a_ptr[r + 1] - a_ptr[r]) + (bt_ptr[r + 1] - bt_ptr[r]);
+                else
+                {
+                    const int q = r - n_lambda;
+                    cnt[r] = (b_ptr[q + 1] - b_ptr[q]) + (c_ptr[q + 1] - c_ptr[q]);
+                }
+            }
+        }
+
+        // one warp per row: copy two CSR row segments (second shifted by n_lambda)
+        __global__ void k_row_fill(int n_lambda, int n_u, const int* __restrict__ k_ptr,
+                                   const int* a_ptr, const int* a_col, const double* a_val,
+                                   const int* bt_ptr, const int* bt_col, const double* bt_val,
+                                   const int* b_ptr, const int* b_col, const double* b_val,
+                                   const int* c_ptr, const int* c_col, const double* c_val,
+                                   int* __restrict__ k_col, double* __restrict__ k_val)
+        {
+            const int n = n_lambda + n_u;
+            const int lane = threadIdx.x & 31;
+            const int warps_total = (gridDim.x * blockDim.x) >> 5;
+            for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps_total)
+            {
+                const int* p1; const int* c1; const double* v1;
+                const int* p2; const int* c2; const double* v2;
+                int q = r;
+                if (r < n_lambda) { p1 = a_ptr; c1 = a_col; v1 = a_val; p2 = bt_ptr; c2 = bt_col; v2 = bt_val; }
+                else { q = r - n_lambda; p1 = b_ptr; c1 = b_col; v1 = b_val; p2 = c_ptr; c2 = c_col; v2 = c_val; }
+                int o = k_ptr[r];
+                const int b1 = p1[q], e1 = p1[q + 1];
+                for (int k = b1 + lane; k < e1; k += 32)
+                {
+                    k_col[o + k - b1] = c1[k];
+                    k_val[o + k - b1] = v1[k];
+                }
+                o += e1 - b1;
+                const int b2 = p2[q], e2 = p2[q + 1];
+                for (int k = b2 + lane; k < e2; k += 32)
+                {
+                    k_col[o + k - b2] = c2[k] + n_lambda;
+                    k_val[o + k - b2] = v2[k];
+                }
+            }
+        }
+
+        __global__ void csr_diagonal(int n, const int* __restrict__ ptr, const int* __restrict__ col,
+                                     const double* __restrict__ val, double diag_tol, double* __restrict__ inv_diag,
+                                     int* __restrict__ status)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+            {
+                double d = 0.0;
+                for (int k = ptr[r]; k < ptr[r + 1]; ++k)
+                    if (col[k] == r)
+                        d += val[k];
+                if (!(d > diag_tol))
+                {
+                    atomicExch(status, APF_ERR_NUMERIC);
+                    inv_diag[r] = 0.0;
+                }
+                else
+                    inv_diag[r] = 1.0 / d;
+            }
+        }
+
+        struct HhatArgs
+        {
+            int n_u;
+            const int *c_ptr, *c_col; const double* c_val;        // C_signed
+            const int *ax_ptr, *ax_col; const double* ax_val;     // A_x
+            const int *bd_ptr, *bd_col; const double* bd_val;     // B_dt (rows u)
+            const int *bt_ptr, *bt_col; const double* bt_val;     // B_dt^T (rows lambda)
+            const double* inv_diag;                                // 1/A_y(c,c)
+            int* row_count;
+            const int* row_ptr;
+            int* col_out;
+            double* val_out;
+            int* status;
+        };
+
+        // Candidates: (col, value, is_ax).  Reference semantics
+        // (schur_approximations.hpp:107-200, sparse_matrix_ops.hpp:286-316 with zero_tol 0):
+        //   hpar = setFromTriplets(-C[nz], (1/A_cc * B_ic) * B_jc for B_ic, B_jc != 0)
+        //   Hhat = setFromTriplets(hpar[nz], A_x[nz])
+        template<int CAP, bool FILL>
+        __global__ void __launch_bounds__(128) hhat_rows(HhatArgs A)
+        {
+            extern __shared__ unsigned char smem_raw[];
+            const int warps = blockDim.x >> 5;
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
+            double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
+                           (size_t)w * CAP;
+            for (int row = blockIdx.x * warps + w; row < A.n_u; row += gridDim.x * warps)
+            {
+                int n = 0;
+                bool overflow = false;
+                // -C row (seq region 0)
+                {
+                    const int b = A.c_ptr[row], e = A.c_ptr[row + 1];
+                    for (int k0 = b; k0 < e; k0 += 32)
+                    {
+                        const int k = k0 + lane;
+                        const bool ok = k < e && A.c_val[k] != 0.0;
+                        const unsigned m = __ballot_sync(0xffffffffu, ok);
+                        const int slot = n + __popc(m & ((1u << lane) - 1));
+                        if (ok && slot < CAP)
+                        {
+                            keys[slot] = make_key(A.c_col[k], k - b, slot);
+                            vals[slot] = -A.c_val[k];
+                        }
+                        n += __popc(m);
+                    }
+                }
+                // Schur part: for each nonzero B_dt(row, c): (inv_c * B(row,c)) * B(j, c)
+                int seq = 4096;
+                {
+                    const int b = A.bd_ptr[row], e = A.bd_ptr[row + 1];
+                    for (int k = b; k < e; ++k)
+                    {
+                        const double vi = A.bd_val[k];
+                        const int c = A.bd_col[k];
+                        const int tb = A.bt_ptr[c], te = A.bt_ptr[c + 1];
+                        if (vi != 0.0)
+                        {
+                            const double sv = A.inv_diag[c] * vi;
+                            for (int q0 = tb; q0 < te; q0 += 32)
+                            {
+                                const int q = q0 + lane;
+                                double contrib = 0.0;
+                                bool ok = false;
+                                if (q < te)
+                                {
+                                    const double vj = A.bt_val[q];
+                                    contrib = sv * vj;
+                                    ok = vj != 0.0 && fabs(contrib) > 0.0;
+                                }
+                                const unsigned m = __ballot_sync(0xffffffffu, ok);
+                                const int slot = n + __popc(m & ((1u << lane) - 1));
+                                if (ok && slot < CAP)
+                                {
+                                    keys[slot] = make_key(A.bt_col[q], seq + (q - tb), slot);
+                                    vals[slot] = contrib;
+                                }
+                                n += __popc(m);
+                            }
+                        }
+                        seq += te - tb;
+                    }
+                }
+                const int n_h = n;
+                // A_x row: flagged by seq region >= (1 << 16)
+                {
+                    const int b = A.ax_ptr[row], e = A.ax_ptr[row + 1];
+                    for (int k0 = b; k0 < e; k0 += 32)
+                    {
+                        const int k = k0 + lane;
+                        const bool ok = k < e && A.ax_val[k] != 0.0;
+                        const unsigned m = __ballot_sync(0xffffffffu, ok);
+                        const int slot = n + __popc(m & ((1u << lane) - 1));
+                        if (ok && slot < CAP)
+                        {
+                            keys[slot] = make_key(A.ax_col[k], (1 << 16) + (k - b), slot);
+                            vals[slot] = A.ax_val[k];
+                        }
+                        n += __popc(m);
+                    }
+                }
+                (void)n_h;
+                if (n > CAP || seq >= (1 << 16) || overflow)
+                {
+                    if (lane == 0)
+                        atomicExch(A.status, APF_ERR_CAPACITY);
+                    if (!FILL && lane == 0)
+                        A.row_count[row] = 0;
+                    __syncwarp();
+                    continue;
+                }
+                int np = 1;
+                while (np < n) np <<= 1;
+                for (int k = n + lane; k < np; k += 32)
+                    keys[k] = ~0ull;
+                __syncwarp();
+                warp_bitonic_sort(keys, np);
+                const int out_base = FILL ? A.row_ptr[row] : 0;
+                int uniq = 0;
+                for (int k0 = 0; k0 < n; k0 += 32)
+                {
+                    const int k = k0 + lane;
+                    bool head = false, keep = false;
+                    unsigned col = 0;
+                    double hs = 0.0, as = 0.0;
+                    if (k < n)
+                    {
+                        col = static_cast<unsigned>(keys[k] >> 32);
+                        head = (k == 0) || (static_cast<unsigned>(keys[k - 1] >> 32) != col);
+                        if (head)
+                        {
+                            for (int q = k; q < n && static_cast<unsigned>(keys[q] >> 32) == col; ++q)
+                            {
+                                const unsigned long long kk = keys[q];
+                                const int sq = static_cast<int>((kk >> kSlotBits) & ((1u << kSeqBits) - 1));
+                                const double v = vals[kk & ((1u << kSlotBits) - 1)];
+                                if (sq >= (1 << 16)) as += v; else hs += v;
+                            }
+                            keep = (hs != 0.0) || (as != 0.0);
+                        }
+                    }
+                    const unsigned km = __ballot_sync(0xffffffffu, keep);
+                    if (FILL && keep)
+                    {
+                        const int pos = out_base + uniq + __popc(km & ((1u << lane) - 1));
+                        A.col_out[pos] = static_cast<int>(col);
+                        A.val_out[pos] = (hs != 0.0 ? hs : 0.0) + (as != 0.0 ? as : 0.0);
+                    }
+                    uniq += __popc(km);
+                }
+                if (!FILL && lane == 0)
+                    A.row_count[row] = uniq;
+                __syncwarp();
+            }
+        }
+
+        int grid_for(long long work, int block, int max_blocks = 148 * 32)
+        {
+            long long g = (work + block - 1) / block;
+            if (g < 1) g = 1;
+            if (g > max_blocks) g = max_blocks;
+            return static_cast<int>(g);
+        }
+    } // namespace
+
+    // ----------------------------------------------------------------------
+    // host orchestration
+    // ----------------------------------------------------------------------
+    void upload_tables_once(int device)
+    {
+        static bool done[64] = {};
+        if (device >= 0 && device < 64 && done[device])
+            return;
+        RefTables t[2] = {make_ref_tables(1), make_ref_tables(2)};
+        APF_CUDA(cudaMemcpyToSymbol(c_tab, t, sizeof(t)));
+        if (device >= 0 && device < 64)
+            done[device] = true;
+    }
+
+    Incidence build_incidence(cudaStream_t s, int n_dofs, int n_asm, const int* cell_list, const int* src_map,
+                              const int* offsets, const int* dofs, int ndof)
+    {
+        Incidence inc;
+        inc.ptr.allocate(static_cast<std::size_t>(n_dofs) + 1, s);
+        DeviceBuffer<int> count(static_cast<std::size_t>(n_dofs) + 1, s);
+        count.zero();
+        IncidenceSpec spec{n_asm, cell_list, src_map, offsets, dofs, ndof};
+        const long long work = static_cast<long long>(n_asm) * ndof;
+        if (work > 0)
+        {
+            incidence_count<<<grid_for(work, 256), 256, 0, s>>>(spec, count.get());
+            g_kernel_launches += 1;
+        }
+        APF_CUDA(cudaGetLastError());
+        const long long total = exclusive_scan(count.get(), inc.ptr.get(), n_dofs, s);
+        g_kernel_launches += 3;
+        inc.entries.allocate(static_cast<std::size_t>(std::max<long long>(total, 1)), s);
+        count.zero();
+        if (work > 0)
+        {
+            incidence_fill<<<grid_for(work, 256), 256, 0, s>>>(spec, inc.ptr.get(), count.get(), inc.entries.get());
+            g_kernel_launches += 1;
+        }
+        APF_CUDA(cudaGetLastError());
+        DeviceBuffer<int> mx(1, s);
+        mx.zero();
+        if (n_dofs > 0)
+        {
+            max_row_length<<<grid_for(n_dofs, 256, 1024), 256, 0, s>>>(inc.ptr.get(), n_dofs, mx.get());
+            g_kernel_launches += 1;
+        }
+        APF_CUDA(cudaMemcpyAsync(&inc.max_len, mx.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        return inc;
+    }
+
+    namespace
+    {
+        AsmData make_asm_data(const SystemInputs& in, double zero_tol)
+        {
+            AsmData d{};
+            d.p = in.p;
+            d.y_geo = in.y_geo.get();
+            d.x_geo = in.x_geo.get();
+            d.y_to_x = in.y_to_x.get();
+            d.m_y = in.m_y.size() ? in.m_y.get() : nullptr;
+            d.m_x = in.m_x.size() ? in.m_x.get() : nullptr;
+            d.y_off = in.y_off.get();
+            d.y_dofs = in.y_dofs.get();
+            d.y_w = in.y_w.get();
+            d.x_off = in.x_off.get();
+            d.x_dofs = in.x_dofs.get();
+            d.x_w = in.x_w.get();
+            d.zero_tol = zero_tol;
+            return d;
+        }
+
+        template<int CAP>
+        void run_gather(cudaStream_t s, GatherArgs& a, int* status)
+        {
+            // shared memory per warp: CAP keys + CAP values + staged incidences
+            const int warps = CAP <= 2048 ? 4 : 1;
+            const int threads = warps * 32;
+            const size_t smem = (size_t)warps * CAP * 16 + (size_t)warps * (2 * 256 + 1) * sizeof(int);
+            if (smem > 48 * 1024)
+            {
+                APF_CUDA(cudaFuncSetAttribute(gather_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                APF_CUDA(cudaFuncSetAttribute(gather_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            }
+            const int blocks = grid_for(a.n_rows, warps, 148 * 16);
+            (void)status;
+            if (a.row_ptr == nullptr)
+                gather_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
+            else
+                gather_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
+            g_kernel_launches += 1;
+            APF_CUDA(cudaGetLastError());
+        }
+
+        void dispatch_gather(cudaStream_t s, GatherArgs& a, int cap)
+        {
+            if (cap <= 512) run_gather<512>(s, a, a.status);
+            else if (cap <= 2048) run_gather<2048>(s, a, a.status);
+            else if (cap <= 8192) run_gather<8192>(s, a, a.status);
+            else throw Error(APF_ERR_CAPACITY, "row candidate count exceeds 8192");
+        }
+
+        int check_status(DeviceBuffer<int>& st, cudaStream_t s)
+        {
+            int h = 0;
+            APF_CUDA(cudaMemcpyAsync(&h, st.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+            sync(s);
+            return h;
+        }
+    }
+
+    // Build one CSR block from up to two gather terms.
+    void gather_csr(cudaStream_t s, const SystemInputs& in, double zero_tol, int n_rows, int n_cols, int n_terms,
+                    const int* kinds, const Incidence* const* incs, const int* col_offsets, int kmax, DeviceCsr& out)
+    {
+        GatherArgs a{};
+        a.d = make_asm_data(in, zero_tol);
+        a.n_rows = n_rows;
+        a.ndof = in.ndof;
+        a.n_terms = n_terms;
+        int cap = 0;
+        for (int t = 0; t < n_terms; ++t)
+        {
+            a.term[t] = Term{kinds[t], incs[t]->ptr.get(), incs[t]->entries.get(), col_offsets[t]};
+            require(incs[t]->max_len <= 256, APF_ERR_CAPACITY, "a DOF has more than 256 cell incidences");
+            cap += incs[t]->max_len * in.ndof * kmax;
+        }
+        require(kmax <= 4, APF_ERR_CAPACITY, "restriction rows with more than 4 entries are not supported");
+        DeviceBuffer<int> status(1, s);
+        status.zero();
+        a.status = status.get();
+        DeviceBuffer<int> counts(static_cast<std::size_t>(n_rows) + 1, s);
+        a.row_count = counts.get();
+        a.row_ptr = nullptr;
+        if (n_rows > 0)
+            dispatch_gather(s, a, cap);
+        out.rows = n_rows;
+        out.cols = n_cols;
+        out.row_ptr.allocate(static_cast<std::size_t>(n_rows) + 1, s);
+        const long long nnz = exclusive_scan(counts.get(), out.row_ptr.get(), n_rows, s);
+        g_kernel_launches += 3;
+        if (check_status(status, s) != 0)
+            throw Error(APF_ERR_CAPACITY, "assembly: per-row candidate buffer overflow");
+        out.col_idx.allocate(static_cast<std::size_t>(nnz), s);
+        out.values.allocate(static_cast<std::size_t>(nnz), s);
+        a.row_ptr = out.row_ptr.get();
+        a.col_out = out.col_idx.get();
+        a.val_out = out.values.get();
+        if (n_rows > 0)
+            dispatch_gather(s, a, cap);
+        if (check_status(status, s) != 0)
+            throw Error(APF_ERR_CAPACITY, "assembly: per-row candidate buffer overflow");
+    }
+
+    void gather_vector_host(cudaStream_t s, const SystemInputs& in, double zero_tol, int which, const Incidence& inc,
+                            int n_rows, const double* ell, int u0_kind, double g_scale, DeviceBuffer<double>& out)
+    {
+        VecArgs a{};
+        a.d = make_asm_data(in, zero_tol);
+        a.n_rows = n_rows;
+        a.ndof = in.ndof;
+        a.inc_ptr = inc.ptr.get();
+        a.inc = inc.entries.get();
+        a.which = which;
+        a.ell = ell;
+        a.u0_kind = u0_kind;
+        a.g_scale = g_scale;
+        out.allocate(static_cast<std::size_t>(n_rows), s);
+        a.out = out.get();
+        DeviceBuffer<int> status(1, s);
+        status.zero();
+        a.status = status.get();
+        if (n_rows > 0)
+        {
+            gather_vector<<<grid_for(n_rows, 128), 128, 0, s>>>(a);
+            g_kernel_launches += 1;
+            APF_CUDA(cudaGetLastError());
+        }
+        if (check_status(status, s) != 0)
+            throw Error(APF_ERR_CAPACITY, "assembly: more than 64 incidences for a vector row");
+    }
+
+    void build_k(cudaStream_t s, int n_lambda, int n_u, const DeviceCsr& a, const DeviceCsr& bt, const DeviceCsr& b,
+                 const DeviceCsr& c, DeviceCsr& k)
+    {
+        const int n = n_lambda + n_u;
+        DeviceBuffer<int> cnt(static_cast<std::size_t>(n) + 1, s);
+        k_row_counts<<<grid_for(n, 256), 256, 0, s>>>(n_lambda, n_u, a.row_ptr.get(), bt.row_ptr.get(), b.row_ptr.get(),
+                                                      c.row_ptr.get(), cnt.get());
+        g_kernel_launches += 1;
+        APF_CUDA(cudaGetLastError());
+        k.rows = k.cols = n;
+        k.row_ptr.allocate(static_cast<std::size_t>(n) + 1, s);
+        const long long nnz = exclusive_scan(cnt.get(), k.row_ptr.get(), n, s);
+        g_kernel_launches += 3;
+        k.col_idx.allocate(static_cast<std::size_t>(nnz), s);
+        k.values.allocate(static_cast<std::size_t>(nnz), s);
+        k_row_fill<<<grid_for((long long)n * 32, 256), 256, 0, s>>>(
+            n_lambda, n_u, k.row_ptr.get(), a.row_ptr.get(), a.col_idx.get(), a.values.get(), bt.row_ptr.get(),
+            bt.col_idx.get(), bt.values.get(), b.row_ptr.get(), b.col_idx.get(), b.values.get(), c.row_ptr.get(),
+            c.col_idx.get(), c.values.get(), k.col_idx.get(), k.values.get());
+        g_kernel_launches += 1;
+        APF_CUDA(cudaGetLastError());
+    }
+
+    void build_hhat(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& C, const DeviceCsr& A_x, const DeviceCsr& B_dt,
+                    const DeviceCsr& B_dtT, double diag_tol, DeviceCsr& H, DeviceBuffer<double>& inv_diag)
+    {
+        const int n_u = C.rows;
+        DeviceBuffer<int> status(1, s);
+        status.zero();
+        inv_diag.allocate(static_cast<std::size_t>(A_y.rows), s);
+        csr_diagonal<<<grid_for(A_y.rows, 256), 256, 0, s>>>(A_y.rows, A_y.row_ptr.get(), A_y.col_idx.get(),
+                                                             A_y.values.get(), diag_tol, inv_diag.get(), status.get());
+        g_kernel_launches += 1;
+        APF_CUDA(cudaGetLastError());
+        if (check_status(status, s) != 0)
+            throw Error(APF_ERR_NUMERIC, "diagonal_schur_approximation: A_y diagonal must be positive.");
+        HhatArgs a{};
+        a.n_u = n_u;
+        a.c_ptr = C.row_ptr.get(); a.c_col = C.col_idx.get(); a.c_val = C.values.get();
+        a.ax_ptr = A_x.row_ptr.get(); a.ax_col = A_x.col_idx.get(); a.ax_val = A_x.values.get();
+        a.bd_ptr = B_dt.row_ptr.get(); a.bd_col = B_dt.col_idx.get(); a.bd_val = B_dt.values.get();
+        a.bt_ptr = B_dtT.row_ptr.get(); a.bt_col = B_dtT.col_idx.get(); a.bt_val = B_dtT.values.get();
+        a.inv_diag = inv_diag.get();
+        a.status = status.get();
+        DeviceBuffer<int> counts(static_cast<std::size_t>(n_u) + 1, s);
+        a.row_count = counts.get();
+        constexpr int CAP = 4096;
+        const int warps = 2, threads = warps * 32;
+        const size_t smem = (size_t)warps * CAP * 16;
+        APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int blocks = grid_for(n_u, warps, 148 * 8);
+        if (n_u > 0)
+        {
+            hhat_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
+            g_kernel_launches += 1;
+            APF_CUDA(cudaGetLastError());
+        }
+        H.rows = H.cols = n_u;
+        H.row_ptr.allocate(static_cast<std::size_t>(n_u) + 1, s);
+        const long long nnz = exclusive_scan(counts.get(), H.row_ptr.get(), n_u, s);
+        g_kernel_launches += 3;
+        if (check_status(status, s) != 0)
+            throw Error(APF_ERR_CAPACITY, "graph norm: per-row candidate buffer overflow");
+        H.col_idx.allocate(static_cast<std::size_t>(nnz), s);
+        H.values.allocate(static_cast<std::size_t>(nnz), s);
+        a.row_ptr = H.row_ptr.get();
+        a.col_out = H.col_idx.get();
+        a.val_out = H.values.get();
+        if (n_u > 0)
+        {
+            hhat_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
+            g_kernel_launches += 1;
+            APF_CUDA(cudaGetLastError());
+        }
+        if (check_status(status, s) != 0)
+            throw Error(APF_ERR_CAPACITY, "graph norm: per-row candidate buffer overflow");
+    }
+
+    // M per X cell, taken from the Y cells it contains (M is cell-constant).
+    namespace
+    {
+        __global__ void scatter_m_to_x(int ny, const int* __restrict__ y_to_x, const double* __restrict__ m_y,
+                                       double* __restrict__ m_x)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ny; c += gridDim.x * blockDim.x)
+            {
+                const int x = y_to_x[c];
+                m_x[3ll * x + 0] = m_y[3ll * c + 0];
+                m_x[3ll * x + 1] = m_y[3ll * c + 1];
+                m_x[3ll * x + 2] = m_y[3ll * c + 2];
+            }
+        }
+
+        __global__ void mark_bottom(int nx, const double* __restrict__ x_geo, int* __restrict__ flag)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nx; c += gridDim.x * blockDim.x)
+                flag[c] = x_geo[8ll * c + 6] == 0.0 ? 1 : 0;
+        }
+
+        __global__ void compact_flags(int n, const int* __restrict__ flag, const int* __restrict__ pos,
+                                      int* __restrict__ list)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+                if (flag[c])
+                    list[pos[c]] = c;
+        }
+
+        __global__ void max_restr_row(int n, const int* __restrict__ off, int* __restrict__ out)
+        {
+            int m = 0;
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                m = max(m, off[i + 1] - off[i]);
+            for (int o = 16; o > 0; o >>= 1)
+                m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0)
+                atomicMax(out, m);
+        }
+    }
+
+    void prepare_inputs(cudaStream_t s, SystemInputs& in)
+    {
+        // M on X cells
+        if (in.m_y.size())
+        {
+            in.m_x.allocate(static_cast<std::size_t>(in.n_x_cells) * 3, s);
+            std::vector<double> ident;
+            // default identity for X cells not covered (should not happen for a valid Y/X pair)
+            ident.resize(static_cast<std::size_t>(in.n_x_cells) * 3);
+            for (int c = 0; c < in.n_x_cells; ++c)
+            {
+                ident[3 * c] = 1.0; ident[3 * c + 1] = 0.0; ident[3 * c + 2] = 1.0;
+            }
+            APF_CUDA(cudaMemcpyAsync(in.m_x.get(), ident.data(), ident.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+            scatter_m_to_x<<<grid_for(in.n_y_cells, 256), 256, 0, s>>>(in.n_y_cells, in.y_to_x.get(), in.m_y.get(), in.m_x.get());
+            g_kernel_launches += 1;
+            APF_CUDA(cudaGetLastError());
+            sync(s);
+        }
+        // bottom X cells (temporal boundary at t = 0)
+        DeviceBuffer<int> flag(static_cast<std::size_t>(in.n_x_cells) + 1, s);
+        DeviceBuffer<int> pos(static_cast<std::size_t>(in.n_x_cells) + 1, s);
+        if (in.n_x_cells > 0)
+        {
+            mark_bottom<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, in.x_geo.get(), flag.get());
+            g_kernel_launches += 1;
+        }
+        const long long nb = exclusive_scan(flag.get(), pos.get(), in.n_x_cells, s);
+        g_kernel_launches += 3;
+        in.n_bottom = static_cast<int>(nb);
+        in.bottom_list.allocate(static_cast<std::size_t>(std::max<long long>(nb, 1)), s);
+        if (in.n_x_cells > 0)
+        {
+            compact_flags<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, flag.get(), pos.get(), in.bottom_list.get());
+            g_kernel_launches += 1;
+        }
+        // max entries per restriction row
+        DeviceBuffer<int> mx(1, s);
+        mx.zero();
+        const int ny_rows = in.n_y_cells * in.ndof, nx_rows = in.n_x_cells * in.ndof;
+        if (ny_rows > 0)
+            max_restr_row<<<grid_for(ny_rows, 256, 1024), 256, 0, s>>>(ny_rows, in.y_off.get(), mx.get());
+        if (nx_rows > 0)
+            max_restr_row<<<grid_for(nx_rows, 256, 1024), 256, 0, s>>>(nx_rows, in.x_off.get(), mx.get());
+        g_kernel_launches += 2;
+        APF_CUDA(cudaGetLastError());
+        APF_CUDA(cudaMemcpyAsync(&in.kmax, mx.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        if (in.kmax < 1)
+            in.kmax = 1;
+    }
+}

@@ -1,0 +1,330 @@
+// extern "C" entry points of libapf_b200 (declared in include/apf_b200.h) and the
+// host-side drivers that sequence the device kernels.
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "apf_internal.hpp"
+#include "apf_system.hpp"
+
+struct apf_ctx
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+};
+
+struct apf_system
+{
+    apf_ctx* ctx = nullptr;
+    apf::System sys;
+};
+
+namespace
+{
+    template<class F>
+    int guarded(apf_ctx* ctx, F&& f)
+    {
+        try
+        {
+            if (ctx)
+            {
+                int cur = -1;
+                cudaGetDevice(&cur);
+                if (cur != ctx->device)
+                    APF_CUDA(cudaSetDevice(ctx->device));
+            }
+            f();
+            if (ctx)
+                ctx->last_error.clear();
+            return APF_OK;
+        }
+        catch (const apf::Error& e)
+        {
+            if (ctx)
+                ctx->last_error = e.what();
+            return e.code;
+        }
+        catch (const std::exception& e)
+        {
+            if (ctx)
+                ctx->last_error = e.what();
+            return APF_ERR_INTERNAL;
+        }
+    }
+
+    template<class T>
+    void stage(apf::DeviceBuffer<T>& dst, const T* src, std::size_t n, bool on_device, cudaStream_t s)
+    {
+        dst.allocate(n, s);
+        if (n == 0)
+            return;
+        apf::require(src != nullptr, APF_ERR_INVALID, "null input array");
+        APF_CUDA(cudaMemcpyAsync(dst.get(), src, n * sizeof(T),
+                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    }
+}
+
+namespace apf
+{
+    void assemble_main(System& S)
+    {
+        cudaStream_t s = S.stream;
+        SystemInputs& in = S.in;
+        prepare_inputs(s, in);
+        const int nd = in.ndof;
+        S.inc_y = build_incidence(s, in.n_lambda, in.n_y_cells, nullptr, nullptr, in.y_off.get(), in.y_dofs.get(), nd);
+        S.inc_xy = build_incidence(s, in.n_u, in.n_y_cells, nullptr, in.y_to_x.get(), in.x_off.get(), in.x_dofs.get(), nd);
+        S.inc_xb = build_incidence(s, in.n_u, in.n_bottom, in.bottom_list.get(), nullptr, in.x_off.get(), in.x_dofs.get(), nd);
+        {
+            const int kinds[1] = {K_AY};
+            const Incidence* incs[1] = {&S.inc_y};
+            const int offs[1] = {0};
+            gather_csr(s, in, in.zero_tol, in.n_lambda, in.n_lambda, 1, kinds, incs, offs, in.kmax, S.blocks[APF_BLOCK_A_Y]);
+        }
+        {
+            const int kinds[1] = {K_BT};
+            const Incidence* incs[1] = {&S.inc_y};
+            const int offs[1] = {0};
+            gather_csr(s, in, in.zero_tol, in.n_lambda, in.n_u, 1, kinds, incs, offs, in.kmax, S.blocks[APF_BLOCK_BT]);
+        }
+        {
+            const int kinds[1] = {K_B};
+            const Incidence* incs[1] = {&S.inc_xy};
+            const int offs[1] = {0};
+            gather_csr(s, in, in.zero_tol, in.n_u, in.n_lambda, 1, kinds, incs, offs, in.kmax, S.blocks[APF_BLOCK_B]);
+        }
+        {
+            const int kinds[1] = {K_C};
+            const Incidence* incs[1] = {&S.inc_xb};
+            const int offs[1] = {0};
+            gather_csr(s, in, in.zero_tol, in.n_u, in.n_u, 1, kinds, incs, offs, in.kmax, S.blocks[APF_BLOCK_C]);
+        }
+        S.have[APF_BLOCK_A_Y] = S.have[APF_BLOCK_BT] = S.have[APF_BLOCK_B] = S.have[APF_BLOCK_C] = true;
+        gather_vector_host(s, in, in.zero_tol, 0, S.inc_y, in.n_lambda, in.ell.size() ? in.ell.get() : nullptr,
+                           in.u0_kind, in.g_scale, S.f);
+        gather_vector_host(s, in, in.zero_tol, 1, S.inc_xb, in.n_u, nullptr, in.u0_kind, in.g_scale, S.g);
+        build_k(s, in.n_lambda, in.n_u, S.blocks[APF_BLOCK_A_Y], S.blocks[APF_BLOCK_BT], S.blocks[APF_BLOCK_B],
+                S.blocks[APF_BLOCK_C], S.blocks[APF_BLOCK_K]);
+        S.have[APF_BLOCK_K] = true;
+        sync(s);
+    }
+
+    void assemble_graph_norm(System& S, double diag_tol)
+    {
+        require(S.have[APF_BLOCK_A_Y] && S.have[APF_BLOCK_C], APF_ERR_INVALID,
+                "assemble_graph_norm: assemble the main system first");
+        cudaStream_t s = S.stream;
+        SystemInputs& in = S.in;
+        const int nd = in.ndof;
+        // The graph-norm blocks are assembled with the same local filter as the main
+        // system (parabolic_graph_norm.hpp:22-65 passes zero_tol through).
+        S.inc_x = build_incidence(s, in.n_u, in.n_x_cells, nullptr, nullptr, in.x_off.get(), in.x_dofs.get(), nd);
+        {
+            const int kinds[1] = {K_AX};
+            const Incidence* incs[1] = {&S.inc_x};
+            const int offs[1] = {0};
+            gather_csr(s, in, in.zero_tol, in.n_u, in.n_u, 1, kinds, incs, offs, in.kmax, S.blocks[APF_BLOCK_AX]);
+        }
+        {
+            const int kinds[1] = {K_BDT};
+            const Incidence* incs[1] = {&S.inc_xy};
+            const int offs[1] = {0};
+            gather_csr(s, in, in.zero_tol, in.n_u, in.n_lambda, 1, kinds, incs, offs, in.kmax, S.blocks[APF_BLOCK_BDT]);
+        }
+        DeviceCsr bdtT;
+        {
+            const int kinds[1] = {K_BDTT};
+            const Incidence* incs[1] = {&S.inc_y};
+            const int offs[1] = {0};
+            gather_csr(s, in, in.zero_tol, in.n_lambda, in.n_u, 1, kinds, incs, offs, in.kmax, bdtT);
+        }
+        S.have[APF_BLOCK_AX] = S.have[APF_BLOCK_BDT] = true;
+        build_hhat(s, S.blocks[APF_BLOCK_A_Y], S.blocks[APF_BLOCK_C], S.blocks[APF_BLOCK_AX], S.blocks[APF_BLOCK_BDT],
+                   bdtT, diag_tol, S.blocks[APF_BLOCK_HHAT], S.inv_diag_ay);
+        S.have[APF_BLOCK_HHAT] = true;
+        sync(s);
+    }
+}
+
+extern "C" {
+
+int apf_ctx_create(int device, void* stream, apf_ctx** out)
+{
+    if (!out)
+        return APF_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+        return APF_ERR_NO_DEVICE;
+    if (device < 0 || device >= n)
+        return APF_ERR_INVALID;
+    auto ctx = std::make_unique<apf_ctx>();
+    ctx->device = device;
+    const int rc = guarded(ctx.get(), [&] {
+        APF_CUDA(cudaSetDevice(device));
+        if (stream)
+            ctx->stream = static_cast<cudaStream_t>(stream);
+        else
+        {
+            APF_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+            ctx->own_stream = true;
+        }
+        apf::upload_tables_once(device);
+    });
+    if (rc != APF_OK)
+        return rc;
+    *out = ctx.release();
+    return APF_OK;
+}
+
+void apf_ctx_destroy(apf_ctx* ctx)
+{
+    if (!ctx)
+        return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream && ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* apf_ctx_last_error(const apf_ctx* ctx)
+{
+    return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+int apf_ctx_synchronize(apf_ctx* ctx)
+{
+    return guarded(ctx, [&] { APF_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+int64_t apf_ctx_kernel_launches(const apf_ctx*)
+{
+    return apf::g_kernel_launches.load();
+}
+
+int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs_on_device, apf_system** out)
+{
+    if (!ctx || !d || !out)
+        return APF_ERR_INVALID;
+    *out = nullptr;
+    auto h = std::make_unique<apf_system>();
+    h->ctx = ctx;
+    const int rc = guarded(ctx, [&] {
+        apf::require(d->p == 1 || d->p == 2, APF_ERR_INVALID, "p must be 1 or 2");
+        apf::require(d->n_y_cells >= 0 && d->n_x_cells >= 0 && d->n_lambda >= 0 && d->n_u >= 0, APF_ERR_INVALID,
+                     "negative sizes");
+        apf::require(d->u0_kind >= 0 && d->u0_kind <= 2, APF_ERR_INVALID, "unknown u0_kind");
+        auto& S = h->sys;
+        S.stream = ctx->stream;
+        auto& in = S.in;
+        in.p = d->p;
+        in.ndof = (d->p + 1) * (d->p + 2) / 2 * (d->p + 1);
+        in.n_y_cells = d->n_y_cells;
+        in.n_x_cells = d->n_x_cells;
+        in.n_lambda = d->n_lambda;
+        in.n_u = d->n_u;
+        in.u0_kind = d->u0_kind;
+        in.zero_tol = d->zero_tol;
+        in.g_scale = d->g_scale;
+        const bool dev = inputs_on_device != 0;
+        cudaStream_t s = ctx->stream;
+        const std::size_t ny = static_cast<std::size_t>(d->n_y_cells), nx = static_cast<std::size_t>(d->n_x_cells);
+        stage(in.y_geo, d->y_geometry, ny * 8, dev, s);
+        stage(in.x_geo, d->x_geometry, nx * 8, dev, s);
+        stage(in.y_to_x, d->y_to_x, ny, dev, s);
+        stage(in.y_off, d->y_restr_offsets, ny * in.ndof + 1, dev, s);
+        stage(in.y_dofs, d->y_restr_dofs, static_cast<std::size_t>(d->y_restr_nnz), dev, s);
+        stage(in.y_w, d->y_restr_weights, static_cast<std::size_t>(d->y_restr_nnz), dev, s);
+        stage(in.x_off, d->x_restr_offsets, nx * in.ndof + 1, dev, s);
+        stage(in.x_dofs, d->x_restr_dofs, static_cast<std::size_t>(d->x_restr_nnz), dev, s);
+        stage(in.x_w, d->x_restr_weights, static_cast<std::size_t>(d->x_restr_nnz), dev, s);
+        if (d->m_cells)
+            stage(in.m_y, d->m_cells, ny * 3, dev, s);
+        if (d->ell_cells)
+            stage(in.ell, d->ell_cells, ny, dev, s);
+        apf::assemble_main(S);
+    });
+    if (rc != APF_OK)
+        return rc;
+    *out = h.release();
+    return APF_OK;
+}
+
+int apf_assemble_graph_norm(apf_ctx* ctx, apf_system* sys, double diagonal_tolerance)
+{
+    if (!ctx || !sys)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] { apf::assemble_graph_norm(sys->sys, diagonal_tolerance); });
+}
+
+int apf_system_block_info(const apf_system* sys, int block, int32_t* rows, int32_t* cols, int64_t* nnz)
+{
+    if (!sys || block < 0 || block >= APF_N_BLOCKS || !sys->sys.have[block])
+        return APF_ERR_INVALID;
+    const auto& b = sys->sys.blocks[block];
+    if (rows) *rows = b.rows;
+    if (cols) *cols = b.cols;
+    if (nnz) *nnz = b.nnz();
+    return APF_OK;
+}
+
+int apf_system_block_copy(apf_ctx* ctx, const apf_system* sys, int block, int32_t* row_ptr, int32_t* col_idx,
+                          double* values, int to_device)
+{
+    if (!ctx || !sys || block < 0 || block >= APF_N_BLOCKS || !sys->sys.have[block])
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        const auto& b = sys->sys.blocks[block];
+        const cudaMemcpyKind k = to_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (row_ptr)
+            APF_CUDA(cudaMemcpyAsync(row_ptr, b.row_ptr.get(), (b.rows + 1) * sizeof(int), k, ctx->stream));
+        if (col_idx && b.nnz())
+            APF_CUDA(cudaMemcpyAsync(col_idx, b.col_idx.get(), b.nnz() * sizeof(int), k, ctx->stream));
+        if (values && b.nnz())
+            APF_CUDA(cudaMemcpyAsync(values, b.values.get(), b.nnz() * sizeof(double), k, ctx->stream));
+        APF_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int apf_system_block_device_ptrs(const apf_system* sys, int block, const int32_t** row_ptr, const int32_t** col_idx,
+                                 const double** values)
+{
+    if (!sys || block < 0 || block >= APF_N_BLOCKS || !sys->sys.have[block])
+        return APF_ERR_INVALID;
+    const auto& b = sys->sys.blocks[block];
+    if (row_ptr) *row_ptr = b.row_ptr.get();
+    if (col_idx) *col_idx = b.col_idx.get();
+    if (values) *values = b.values.get();
+    return APF_OK;
+}
+
+int apf_system_vector_copy(apf_ctx* ctx, const apf_system* sys, int which, double* out, int to_device)
+{
+    if (!ctx || !sys || !out || (which != APF_VEC_F && which != APF_VEC_G))
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        const auto& v = which == APF_VEC_F ? sys->sys.f : sys->sys.g;
+        if (v.size())
+            APF_CUDA(cudaMemcpyAsync(out, v.get(), v.size() * sizeof(double),
+                                     to_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+        APF_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+void apf_system_destroy(apf_system* sys)
+{
+    if (!sys)
+        return;
+    if (sys->ctx)
+    {
+        cudaSetDevice(sys->ctx->device);
+        cudaStreamSynchronize(sys->ctx->stream);
+    }
+    delete sys;
+}
+
+} // extern "C"

@@ -1,0 +1,116 @@
+// Internal definitions shared by the CUDA translation units of libapf_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/apf_b200.h"
+
+namespace apf
+{
+    // Error raised inside the library; the C-ABI layer converts it to a status code
+    // plus a message retrievable with apf_last_error().
+    struct Error : std::runtime_error
+    {
+        int code;
+        Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+    };
+
+#define APF_CUDA(call)                                                                      \
+    do                                                                                      \
+    {                                                                                       \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            throw ::apf::Error(APF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+    inline void require(bool ok, int code, const std::string& msg)
+    {
+        if (!ok)
+            throw Error(code, msg);
+    }
+
+    // Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on the owning stream).
+    template<class T>
+    class DeviceBuffer
+    {
+    public:
+        DeviceBuffer() = default;
+        DeviceBuffer(std::size_t n, cudaStream_t s) { allocate(n, s); }
+        DeviceBuffer(const DeviceBuffer&) = delete;
+        DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+        DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_) { o.p_ = nullptr; o.n_ = 0; }
+        DeviceBuffer& operator=(DeviceBuffer&& o) noexcept
+        {
+            if (this != &o)
+            {
+                release();
+                p_ = o.p_; n_ = o.n_; s_ = o.s_;
+                o.p_ = nullptr; o.n_ = 0;
+            }
+            return *this;
+        }
+        ~DeviceBuffer() { release(); }
+
+        void allocate(std::size_t n, cudaStream_t s)
+        {
+            release();
+            s_ = s;
+            n_ = n;
+            if (n > 0)
+                APF_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p_), n * sizeof(T), s));
+        }
+        void release() noexcept
+        {
+            if (p_)
+                cudaFreeAsync(p_, s_);
+            p_ = nullptr;
+            n_ = 0;
+        }
+        void zero()
+        {
+            if (n_)
+                APF_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s_));
+        }
+        void upload(const T* host, std::size_t n)
+        {
+            if (n != n_)
+                allocate(n, s_);
+            if (n)
+                APF_CUDA(cudaMemcpyAsync(p_, host, n * sizeof(T), cudaMemcpyHostToDevice, s_));
+        }
+        T* get() const noexcept { return p_; }
+        std::size_t size() const noexcept { return n_; }
+        cudaStream_t stream() const noexcept { return s_; }
+
+    private:
+        T* p_ = nullptr;
+        std::size_t n_ = 0;
+        cudaStream_t s_ = nullptr;
+    };
+
+    // Row-compressed sparse matrix resident on the device (int32 indices, f64 values).
+    struct DeviceCsr
+    {
+        int rows = 0;
+        int cols = 0;
+        DeviceBuffer<int> row_ptr;
+        DeviceBuffer<int> col_idx;
+        DeviceBuffer<double> values;
+        std::int64_t nnz() const noexcept { return static_cast<std::int64_t>(col_idx.size()); }
+    };
+
+    // Exclusive scan of n int32 counts into out[0..n] (out[n] = total); returns the total.
+    long long exclusive_scan(const int* counts, int* out, int n, cudaStream_t s);
+
+    // Block until the stream is idle and surface any asynchronous error.
+    inline void sync(cudaStream_t s)
+    {
+        APF_CUDA(cudaStreamSynchronize(s));
+    }
+}

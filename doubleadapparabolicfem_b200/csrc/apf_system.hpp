@@ -1,0 +1,76 @@
+// Device-resident problem inputs and assembled system (internal).
+#pragma once
+
+#include <atomic>
+#include <memory>
+
+#include "apf_internal.hpp"
+
+namespace apf
+{
+    extern std::atomic<long long> g_kernel_launches;
+
+    // local-block kinds of the row gather
+    enum Kind : int
+    {
+        K_AY = 0,   // rows Y, cols Y, cells Y
+        K_BT = 1,   // rows Y, cols X (ancestor), cells Y: B(j, i)
+        K_B = 2,    // rows X (ancestor), cols Y, cells Y
+        K_C = 3,    // rows X, cols X, cells bottom X
+        K_AX = 4,   // rows X, cols X, cells X
+        K_BDT = 5,  // as K_B, time-derivative part only
+        K_BDTT = 6, // as K_BT, time-derivative part only
+    };
+
+    // true DOF -> list of (cell*ndof + local, restriction entry)
+    struct Incidence
+    {
+        DeviceBuffer<int> ptr;
+        DeviceBuffer<int2> entries;
+        int max_len = 0;
+    };
+
+    struct SystemInputs
+    {
+        int p = 1, ndof = 6;
+        int n_y_cells = 0, n_x_cells = 0, n_lambda = 0, n_u = 0;
+        DeviceBuffer<double> y_geo, x_geo;
+        DeviceBuffer<int> y_to_x;
+        DeviceBuffer<int> y_off, y_dofs, x_off, x_dofs;
+        DeviceBuffer<double> y_w, x_w;
+        DeviceBuffer<double> m_y, m_x, ell;
+        DeviceBuffer<int> bottom_list;
+        int n_bottom = 0;
+        int kmax = 1;
+        int u0_kind = 0;
+        double zero_tol = 1e-15, g_scale = -1.0;
+    };
+
+    struct System
+    {
+        cudaStream_t stream = nullptr;
+        SystemInputs in;
+        Incidence inc_y, inc_xy, inc_xb, inc_x;
+        DeviceCsr blocks[APF_N_BLOCKS];
+        bool have[APF_N_BLOCKS] = {};
+        DeviceBuffer<double> f, g;
+        DeviceBuffer<double> inv_diag_ay;
+    };
+
+    void upload_tables_once(int device);
+    void prepare_inputs(cudaStream_t s, SystemInputs& in);
+    Incidence build_incidence(cudaStream_t s, int n_dofs, int n_asm, const int* cell_list, const int* src_map,
+                              const int* offsets, const int* dofs, int ndof);
+    void gather_csr(cudaStream_t s, const SystemInputs& in, double zero_tol, int n_rows, int n_cols, int n_terms,
+                    const int* kinds, const Incidence* const* incs, const int* col_offsets, int kmax, DeviceCsr& out);
+    void gather_vector_host(cudaStream_t s, const SystemInputs& in, double zero_tol, int which, const Incidence& inc,
+                            int n_rows, const double* ell, int u0_kind, double g_scale, DeviceBuffer<double>& out);
+    void build_k(cudaStream_t s, int n_lambda, int n_u, const DeviceCsr& a, const DeviceCsr& bt, const DeviceCsr& b,
+                 const DeviceCsr& c, DeviceCsr& k);
+    void build_hhat(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& C, const DeviceCsr& A_x, const DeviceCsr& B_dt,
+                    const DeviceCsr& B_dtT, double diag_tol, DeviceCsr& H, DeviceBuffer<double>& inv_diag);
+
+    // assembly drivers (apf_capi.cu)
+    void assemble_main(System& sys);
+    void assemble_graph_norm(System& sys, double diag_tol);
+}

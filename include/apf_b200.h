@@ -1,0 +1,135 @@
+/*
+ * apf_b200.h — C ABI of libapf_b200, the B200 (sm_100a) implementation of the
+ * data-parallel core of one adaptive cycle of the space-time parabolic FEM of
+ * Rsmeets99/DoubleAdapParabolicFEM.
+ *
+ * Plain C: pointers, sizes and int32 status codes (APF_OK == 0; negative on error,
+ * message via apf_ctx_last_error).  No call aborts and no device code traps.
+ * One context per host thread; a context is not thread-safe.
+ *
+ * Each entry point names the reference interface it replaces (paths relative to
+ * the reference project root).
+ */
+#ifndef APF_B200_H
+#define APF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+#define APF_OK 0
+#define APF_ERR_INVALID (-1)       /* bad argument / inconsistent sizes */
+#define APF_ERR_CUDA (-2)          /* CUDA runtime error */
+#define APF_ERR_CAPACITY (-3)      /* a per-row candidate buffer overflowed */
+#define APF_ERR_NUMERIC (-4)       /* non-positive diagonal, breakdown, non-finite value */
+#define APF_ERR_NOT_CONVERGED (-5) /* iterative solve missed its tolerance */
+#define APF_ERR_NO_DEVICE (-6)     /* no CUDA device */
+#define APF_ERR_INTERNAL (-7)
+
+/* ---- initial data u0 of the examples (algorithm/examples/space_time_2d/initial_data_2d_examples.hpp) */
+#define APF_U0_SIN_SIN 0 /* smooth_initial: sin(pi x) sin(pi y) */
+#define APF_U0_ONE 1     /* non_matching_initial: 1 */
+#define APF_U0_ZERO 2
+
+/* ---- blocks of an assembled system ---------------------------------------- */
+#define APF_BLOCK_A_Y 0  /* A_y   (n_lambda x n_lambda) */
+#define APF_BLOCK_B 1    /* B     (n_u x n_lambda), lower-left orientation */
+#define APF_BLOCK_BT 2   /* B^T   (n_lambda x n_u) == CSC arrays of B */
+#define APF_BLOCK_C 3    /* C_signed (n_u x n_u) */
+#define APF_BLOCK_K 4    /* K = [A_y B^T; B C_signed] ((n_lambda+n_u)^2) */
+#define APF_BLOCK_HHAT 5 /* parabolic graph-norm Schur approximation (n_u x n_u) */
+#define APF_BLOCK_BDT 6  /* time-derivative part of B (n_u x n_lambda) */
+#define APF_BLOCK_AX 7   /* X-space spatial stiffness (n_u x n_u) */
+#define APF_N_BLOCKS 8
+
+#define APF_VEC_F 0 /* lambda right-hand side (n_lambda) */
+#define APF_VEC_G 1 /* u right-hand side (n_u) */
+
+typedef struct apf_ctx apf_ctx;
+typedef struct apf_system apf_system;
+
+/* Space-time mesh, DOF maps and coefficients: the host-side inputs of
+ * finite_element::system::assemble_main_system_blocks
+ * (src/finite_element/system/assemble_saddle_problem.hpp:131-364) for 2+1D tensor
+ * P_p x P_p Lagrange prisms, p in {1,2}.
+ *
+ * Cells are affine prisms; geometry row = x0 y0 x1 y1 x2 y2 t0 t1 (the reference
+ * cell's vertex order, src/finite_element/geometry/cell_geometry.hpp:188-242).
+ * Restrictions are the flattened CellRestriction of
+ * src/finite_element/assembly/constrained_dofs.hpp:37-226: local row (cell c,
+ * local i) owns entries [offsets[c*ndof+i], offsets[c*ndof+i+1]) of (dofs,
+ * weights); ndof = (p+1)(p+2)/2 * (p+1); local index = i_space*(p+1) + i_time
+ * (src/finite_element/basis/functions/triangular_prism_lagrange.hpp:27-30).
+ * The diffusion tensor and the load are constant per Y cell. */
+typedef struct apf_problem_desc
+{
+    int p;
+    int n_y_cells;
+    int n_x_cells;
+    int n_lambda; /* true DOFs of the test space Y (broken in time) */
+    int n_u;      /* true DOFs of the trial space X (continuous in time) */
+    const double* y_geometry;   /* [n_y_cells*8] */
+    const double* x_geometry;   /* [n_x_cells*8] */
+    const int32_t* y_to_x;      /* [n_y_cells] active X ancestor of each Y cell */
+    const int32_t* y_restr_offsets; /* [n_y_cells*ndof+1] */
+    const int32_t* y_restr_dofs;    /* [y_restr_nnz] */
+    const double* y_restr_weights;  /* [y_restr_nnz] */
+    int32_t y_restr_nnz;
+    const int32_t* x_restr_offsets; /* [n_x_cells*ndof+1] */
+    const int32_t* x_restr_dofs;
+    const double* x_restr_weights;
+    int32_t x_restr_nnz;
+    const double* m_cells;   /* [n_y_cells*3] (m00, m01, m11) or NULL = identity */
+    const double* ell_cells; /* [n_y_cells] constant load per Y cell or NULL = zero */
+    int u0_kind;             /* APF_U0_* */
+    double zero_tol;         /* per-local-entry filter, reference default 1e-15 */
+    double g_scale;          /* reference default -1 */
+} apf_problem_desc;
+
+/* ---- context ----------------------------------------------------------------- */
+/* stream: a cudaStream_t (NULL = the context creates its own non-blocking stream). */
+int apf_ctx_create(int device, void* stream, apf_ctx** out);
+void apf_ctx_destroy(apf_ctx* ctx);
+const char* apf_ctx_last_error(const apf_ctx* ctx);
+int apf_ctx_synchronize(apf_ctx* ctx);
+/* Number of kernels this context has launched since creation. */
+int64_t apf_ctx_kernel_launches(const apf_ctx* ctx);
+
+/* ---- assembly ------------------------------------------------------------------ */
+/* Replaces finite_element::system::assemble_main_system_blocks<QS,QT,Backend>
+ * (src/finite_element/system/assemble_saddle_problem.hpp:131) and
+ * la::saddle::make_saddle_point_blocks + compose_saddle_point_matrix
+ * (src/linear_algebra/system/saddle_point_system.hpp:105-141,
+ *  src/linear_algebra/assembly/compose_block_system.hpp:116).
+ * Builds A_y, B, B^T, C_signed, K, f and g on the device.  Pattern = union over
+ * cells of the restricted local entries with |a_ij| > zero_tol, duplicates summed
+ * (explicit zeros kept), exactly as scatter.hpp:66-115 + setFromTriplets.
+ * inputs_on_device: 1 if every pointer in desc is a device pointer, 0 if host. */
+int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* desc, int inputs_on_device,
+                             apf_system** out);
+
+/* Replaces finite_element::assembly::assemble_parabolic_graph_norm_approximation
+ * (src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:22-65) with
+ * la::preconditioners::parabolic_graph_norm_approximation
+ * (src/linear_algebra/preconditioners/schur_approximations.hpp:237-287):
+ * Hhat = -C_signed + B_dt diag(A_y)^-1 B_dt^T + A_x.  Also keeps B_dt and A_x. */
+int apf_assemble_graph_norm(apf_ctx* ctx, apf_system* sys, double diagonal_tolerance);
+
+/* Block sizes; nnz counts stored entries (explicit zeros included). */
+int apf_system_block_info(const apf_system* sys, int block, int32_t* rows, int32_t* cols, int64_t* nnz);
+/* Copy a block in CSR form.  to_device: 1 = destination pointers are device memory. */
+int apf_system_block_copy(apf_ctx* ctx, const apf_system* sys, int block, int32_t* row_ptr,
+                          int32_t* col_idx, double* values, int to_device);
+/* Device pointers of a block's CSR arrays (owned by sys; valid until sys is destroyed). */
+int apf_system_block_device_ptrs(const apf_system* sys, int block, const int32_t** row_ptr,
+                                 const int32_t** col_idx, const double** values);
+int apf_system_vector_copy(apf_ctx* ctx, const apf_system* sys, int which, double* out, int to_device);
+void apf_system_destroy(apf_system* sys);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

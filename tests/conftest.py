@@ -1,0 +1,82 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+REPO = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+GOLDEN = os.path.join(REPO, "tests", "golden")
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libapf_b200.so")
+    config.addinivalue_line("markers", "slow: larger cases")
+
+
+GOLDEN_CASES = ["p1_l1_smooth", "p1_l2_smooth", "p2_l1_smooth", "p1_l1_nonmatching"]
+
+
+def load_golden(name):
+    """Golden fixture -> (oracle MainProblem, dict of reference outputs as scipy CSC / arrays)."""
+    import apf_oracle as O
+    import scipy.sparse as sp
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    p = int(z["meta_p"][0])
+    ndof = (p + 1) * (p + 2) // 2 * (p + 1)
+
+    def restr(prefix):
+        return O.Restriction(z[f"{prefix}_offsets"], z[f"{prefix}_dofs"], z[f"{prefix}_weights"], ndof)
+
+    def csc(nm):
+        sh = tuple(int(v) for v in z[f"{nm}_shape"])
+        return sp.csc_matrix((z[f"{nm}_values"], z[f"{nm}_inner"], z[f"{nm}_outer"]), shape=sh)
+
+    out = {nm: csc(nm) for nm in ("A_y", "B", "C_signed", "Hhat")}
+    out["f"] = z["f"]
+    out["g"] = z["g"]
+    prob = O.MainProblem(p=p, y_geom=z["y_geometry"], x_geom=z["x_geometry"], y_to_x=z["y_to_x_cell"],
+                         y_restr=restr("y_restriction"), x_restr=restr("x_restriction"),
+                         n_lambda=out["A_y"].shape[0], n_u=out["C_signed"].shape[0])
+    example = str(z["meta_example"][0])
+    return prob, out, example
+
+
+def to_product_problem(prob, example):
+    """Oracle MainProblem -> product SpaceTimeProblem (same arrays)."""
+    from doubleadapparabolicfem_b200.mesh import Restriction, SpaceTimeProblem
+    u0 = 0 if example == "smooth_initial" else 1
+    return SpaceTimeProblem(
+        p=prob.p, y_geometry=prob.y_geom, x_geometry=prob.x_geom, y_to_x=prob.y_to_x.astype(np.int32),
+        y_restriction=Restriction(prob.y_restr.offsets.astype(np.int32), prob.y_restr.dofs.astype(np.int32),
+                                  prob.y_restr.weights, prob.y_restr.ndof),
+        x_restriction=Restriction(prob.x_restr.offsets.astype(np.int32), prob.x_restr.dofs.astype(np.int32),
+                                  prob.x_restr.weights, prob.x_restr.ndof),
+        n_lambda=prob.n_lambda, n_u=prob.n_u, u0_kind=u0)
+
+
+def assert_same_sparse(ref, mine, rtol, what=""):
+    """Bit-exact pattern, values within rtol relative to max |ref|."""
+    r = ref.tocsr()
+    r.sort_indices()
+    m = mine.tocsr()
+    m.sort_indices()
+    assert r.shape == m.shape, f"{what}: shape {r.shape} vs {m.shape}"
+    assert np.array_equal(r.indptr, m.indptr), f"{what}: row pointers differ"
+    assert np.array_equal(r.indices, m.indices), f"{what}: column indices differ"
+    scale = max(np.abs(r.data).max(initial=0.0), 1e-300)
+    err = np.abs(r.data - m.data).max(initial=0.0) / scale
+    assert err <= rtol, f"{what}: max relative error {err:.3e} > {rtol:.1e}"
+    return err
+
+
+@pytest.fixture(scope="session")
+def gpu_ctx():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from doubleadapparabolicfem_b200 import build
+    build.build()
+    from doubleadapparabolicfem_b200.assembly import Context
+    return Context(0)

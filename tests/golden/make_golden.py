@@ -1,0 +1,73 @@
+"""Regenerate the golden fixtures in this directory from the reference itself.
+
+Runs oracle/_ref/apf_ref_dump (the reference's own assembly templates compiled by
+oracle/Makefile against oracle/shim) on small uniform meshes and packs each case
+into one .npz.  Also extracts the uniform-refinement rows (exact DOF counts and
+6-significant-digit estimator values) of the reference's published paper data
+(algorithm_data_plot/{1d,2d}/*.csv) into paper_uniform_rows.json.
+
+usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+"""
+from __future__ import annotations
+
+import csv
+import glob
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.abspath(os.path.join(HERE, "..", ".."))
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "apf_ref_dump")
+
+CASES = [
+    # (name, dim, p, outer level, example)
+    ("p1_l1_smooth", 2, 1, 1, "smooth_initial"),
+    ("p1_l2_smooth", 2, 1, 2, "smooth_initial"),
+    ("p2_l1_smooth", 2, 2, 1, "smooth_initial"),
+    ("p1_l1_nonmatching", 2, 1, 1, "non_matching_initial"),
+]
+
+
+def dump_case(dim, p, level, example, outdir):
+    subprocess.run([REF_BIN, str(dim), str(p), str(level), example, outdir], check=True)
+    arrays = {}
+    for f in sorted(glob.glob(os.path.join(outdir, "*.npy"))):
+        arrays[os.path.basename(f)[:-4]] = np.load(f)
+    return arrays
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), f"REF={ref_root}"], check=True)
+    for name, dim, p, level, example in CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            arrays = dump_case(dim, p, level, example, tmp)
+        arrays["meta_p"] = np.array([p])
+        arrays["meta_level"] = np.array([level])
+        arrays["meta_example"] = np.array([example])
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays)
+        print("wrote", name)
+    rows = []
+    for dim in ("1d", "2d"):
+        for path in sorted(glob.glob(os.path.join(ref_root, "algorithm_data_plot", dim, "*.csv"))):
+            with open(path) as fh:
+                for r in csv.DictReader(fh):
+                    if r.get("record_type") != "outer" or r.get("mode_short") != "uniform":
+                        continue
+                    rows.append({k: r.get(k) for k in (
+                        "dimension", "example", "p", "outer_iteration", "x_true_dofs_before",
+                        "y_true_dofs_after", "eta_squared", "y_flux_squared", "y_reconstruction_squared",
+                        "divergence_residual_squared", "y_estimator_squared", "iteration_seconds", "source_group",
+                        "job_id")})
+    with open(os.path.join(HERE, "paper_uniform_rows.json"), "w") as fh:
+        json.dump(rows, fh, indent=0)
+    print("wrote paper_uniform_rows.json", len(rows))
+
+
+if __name__ == "__main__":
+    main()

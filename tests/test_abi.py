@@ -1,0 +1,51 @@
+"""CPU tests of the C-ABI boundary: the library builds for sm_100a, loads without a
+GPU, and exports every function include/apf_b200.h declares."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import REPO
+
+HEADER = os.path.join(REPO, "include", "apf_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(apf_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from doubleadapparabolicfem_b200 import build
+    path = build.build()
+    return ctypes.CDLL(path)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "apf_assemble_main_system" in names
+    assert len(names) >= 10
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    from doubleadapparabolicfem_b200 import _lib
+    assert set(declared_functions()) <= set(_lib.SIGNATURES)
+
+
+def test_context_creation_without_gpu_reports_error():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from doubleadapparabolicfem_b200 import _lib
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    rc = lib.apf_ctx_create(0, None, ctypes.byref(h))
+    assert rc == _lib.APF_ERR_NO_DEVICE

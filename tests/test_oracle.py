@@ -1,0 +1,119 @@
+"""CPU tests: the oracle restatement against the reference's own outputs, and the
+host-side mesh generator against the reference's meshes and published DOF counts."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, GOLDEN_CASES, assert_same_sparse, load_golden
+
+import apf_oracle as O
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_main_blocks_match_reference(name):
+    prob, ref, example = load_golden(name)
+    u0 = O.sin_initial if example == "smooth_initial" else O.one_initial
+    out = O.assemble_main_blocks(prob, u0=u0)
+    for nm in ("A_y", "B", "C_signed"):
+        assert_same_sparse(ref[nm], out[nm], 1e-12, nm)
+    assert np.abs(out["f"] - ref["f"]).max() <= 1e-12 * max(1.0, np.abs(ref["f"]).max())
+    assert np.abs(out["g"] - ref["g"]).max() <= 1e-12 * np.abs(ref["g"]).max()
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_graph_norm_matches_reference(name):
+    prob, ref, example = load_golden(name)
+    gn = O.assemble_graph_norm(prob, ref["A_y"], ref["C_signed"])
+    assert_same_sparse(ref["Hhat"], gn["Hhat"], 1e-12, "Hhat")
+
+
+def _paper_rows():
+    with open(os.path.join(GOLDEN, "paper_uniform_rows.json")) as fh:
+        return json.load(fh)
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_uniform_mesh_dof_counts_match_paper_data(p):
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    rows = [r for r in _paper_rows() if r["dimension"] == "2d" and r["p"] == f"p{p}"
+            and r["example"] == "smooth_initial"]
+    assert rows
+    checked = 0
+    for r in rows:
+        level = int(r["outer_iteration"])
+        if level < 1 or level > (5 if p == 1 else 4):
+            continue
+        prob = uniform_problem(level, p)
+        assert prob.n_u == int(r["x_true_dofs_before"]), r
+        assert prob.n_lambda == int(r["y_true_dofs_after"]), r
+        checked += 1
+    assert checked >= 3
+
+
+def _cell_key(geom):
+    tri = geom[:, :6].reshape(-1, 3, 2)
+    order = np.lexsort((tri[:, :, 1], tri[:, :, 0]))
+    tri_sorted = np.take_along_axis(tri, order[:, :, None], axis=1).reshape(-1, 6)
+    return np.round(np.concatenate([tri_sorted, geom[:, 6:]], 1) * 2 ** 20).astype(np.int64)
+
+
+@pytest.mark.parametrize("name", ["p1_l1_smooth", "p1_l2_smooth", "p2_l1_smooth"])
+def test_uniform_mesh_geometry_equals_reference(name):
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    prob, ref, _ = load_golden(name)
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    mine = uniform_problem(int(z["meta_level"][0]), prob.p)
+    a = _cell_key(prob.y_geom)
+    b = _cell_key(mine.y_geometry)
+    sa = a[np.lexsort(a.T[::-1])]
+    sb = b[np.lexsort(b.T[::-1])]
+    assert np.array_equal(sa, sb)
+    assert mine.n_lambda == prob.n_lambda and mine.n_u == prob.n_u
+
+
+def dof_permutation(prob_ref, prob_mine, space):
+    """perm[i_ref] = i_mine by matching DOF coordinates."""
+    from doubleadapparabolicfem_b200.mesh import dof_coordinates, SpaceTimeProblem, Restriction
+    ref_as_product = SpaceTimeProblem(
+        p=prob_ref.p, y_geometry=prob_ref.y_geom, x_geometry=prob_ref.x_geom, y_to_x=prob_ref.y_to_x,
+        y_restriction=Restriction(prob_ref.y_restr.offsets, prob_ref.y_restr.dofs, prob_ref.y_restr.weights,
+                                  prob_ref.y_restr.ndof),
+        x_restriction=Restriction(prob_ref.x_restr.offsets, prob_ref.x_restr.dofs, prob_ref.x_restr.weights,
+                                  prob_ref.x_restr.ndof),
+        n_lambda=prob_ref.n_lambda, n_u=prob_ref.n_u)
+    cr = np.round(dof_coordinates(ref_as_product, space) * 2 ** 20).astype(np.int64)
+    cm = np.round(dof_coordinates(prob_mine, space) * 2 ** 20).astype(np.int64)
+    kr = np.lexsort(cr.T[::-1])
+    km = np.lexsort(cm.T[::-1])
+    assert np.array_equal(cr[kr], cm[km])
+    perm = np.empty(len(kr), dtype=np.int64)
+    perm[kr] = km
+    return perm
+
+
+@pytest.mark.parametrize("name", ["p1_l2_smooth", "p2_l1_smooth"])
+def test_generated_mesh_assembles_to_reference_blocks(name):
+    """Our own uniform mesh + numbering, assembled by the oracle, equals the reference's
+    blocks after the coordinate permutation (pattern bit-exact, values 1e-12)."""
+    import scipy.sparse as sp
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    prob, ref, example = load_golden(name)
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    mine = uniform_problem(int(z["meta_level"][0]), prob.p)
+    py = dof_permutation(prob, mine, "y")
+    px = dof_permutation(prob, mine, "x")
+    mp = O.MainProblem(p=mine.p, y_geom=mine.y_geometry, x_geom=mine.x_geometry, y_to_x=mine.y_to_x,
+                       y_restr=O.Restriction(mine.y_restriction.offsets, mine.y_restriction.dofs,
+                                             mine.y_restriction.weights, mine.ndof),
+                       x_restr=O.Restriction(mine.x_restriction.offsets, mine.x_restriction.dofs,
+                                             mine.x_restriction.weights, mine.ndof),
+                       n_lambda=mine.n_lambda, n_u=mine.n_u)
+    out = O.assemble_main_blocks(mp)
+    Py = sp.csr_matrix((np.ones(len(py)), (np.arange(len(py)), py)), shape=(len(py), len(py)))
+    Px = sp.csr_matrix((np.ones(len(px)), (np.arange(len(px)), px)), shape=(len(px), len(px)))
+    assert_same_sparse(ref["A_y"], Py @ out["A_y"] @ Py.T, 1e-12, "A_y")
+    assert_same_sparse(ref["B"], Px @ out["B"] @ Py.T, 1e-12, "B")
+    assert_same_sparse(ref["C_signed"], Px @ out["C_signed"] @ Px.T, 1e-12, "C")
+    assert np.abs(Px @ out["g"] - ref["g"]).max() <= 1e-12 * np.abs(ref["g"]).max()
