@@ -27,6 +27,7 @@ namespace apf
     __constant__ RefTables c_tab[2];
 
     std::atomic<long long> g_kernel_launches{0};
+    thread_local Profiler* t_profiler = nullptr;
 
     namespace
     {
@@ -777,26 +778,31 @@ namespace apf
         const long long work = static_cast<long long>(n_asm) * ndof;
         if (work > 0)
         {
-            incidence_count<<<grid_for(work, 256), 256, 0, s>>>(spec, count.get());
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("incidence_count", s);
+                incidence_count<<<grid_for(work, 256), 256, 0, s>>>(spec, count.get());
+            }
         }
         APF_CUDA(cudaGetLastError());
         const long long total = exclusive_scan(count.get(), inc.ptr.get(), n_dofs, s);
-        g_kernel_launches += 3;
         inc.entries.allocate(static_cast<std::size_t>(std::max<long long>(total, 1)), s);
         count.zero();
         if (work > 0)
         {
-            incidence_fill<<<grid_for(work, 256), 256, 0, s>>>(spec, inc.ptr.get(), count.get(), inc.entries.get());
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("incidence_fill", s);
+                incidence_fill<<<grid_for(work, 256), 256, 0, s>>>(spec, inc.ptr.get(), count.get(), inc.entries.get());
+            }
         }
         APF_CUDA(cudaGetLastError());
         DeviceBuffer<int> mx(1, s);
         mx.zero();
         if (n_dofs > 0)
         {
-            max_row_length<<<grid_for(n_dofs, 256, 1024), 256, 0, s>>>(inc.ptr.get(), n_dofs, mx.get());
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("max_row_length", s);
+                max_row_length<<<grid_for(n_dofs, 256, 1024), 256, 0, s>>>(inc.ptr.get(), n_dofs, mx.get());
+            }
         }
         APF_CUDA(cudaMemcpyAsync(&inc.max_len, mx.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         sync(s);
@@ -839,10 +845,15 @@ namespace apf
             const int blocks = grid_for(a.n_rows, warps, 148 * 16);
             (void)status;
             if (a.row_ptr == nullptr)
-                gather_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
+                {
+                    APF_KERNEL("gather_rows_count", s);
+                    gather_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
+                }
             else
-                gather_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
-            g_kernel_launches += 1;
+                {
+                    APF_KERNEL("gather_rows_fill", s);
+                    gather_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
+                }
             APF_CUDA(cudaGetLastError());
         }
 
@@ -892,7 +903,6 @@ namespace apf
         out.cols = n_cols;
         out.row_ptr.allocate(static_cast<std::size_t>(n_rows) + 1, s);
         const long long nnz = exclusive_scan(counts.get(), out.row_ptr.get(), n_rows, s);
-        g_kernel_launches += 3;
         if (check_status(status, s) != 0)
             throw Error(APF_ERR_CAPACITY, "assembly: per-row candidate buffer overflow");
         out.col_idx.allocate(static_cast<std::size_t>(nnz), s);
@@ -926,8 +936,10 @@ namespace apf
         a.status = status.get();
         if (n_rows > 0)
         {
-            gather_vector<<<grid_for(n_rows, 128), 128, 0, s>>>(a);
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("gather_vector", s);
+                gather_vector<<<grid_for(n_rows, 128), 128, 0, s>>>(a);
+            }
             APF_CUDA(cudaGetLastError());
         }
         if (check_status(status, s) != 0)
@@ -939,21 +951,24 @@ namespace apf
     {
         const int n = n_lambda + n_u;
         DeviceBuffer<int> cnt(static_cast<std::size_t>(n) + 1, s);
-        k_row_counts<<<grid_for(n, 256), 256, 0, s>>>(n_lambda, n_u, a.row_ptr.get(), bt.row_ptr.get(), b.row_ptr.get(),
-                                                      c.row_ptr.get(), cnt.get());
-        g_kernel_launches += 1;
+        {
+            APF_KERNEL("k_row_counts", s);
+            k_row_counts<<<grid_for(n, 256), 256, 0, s>>>(n_lambda, n_u, a.row_ptr.get(), bt.row_ptr.get(), b.row_ptr.get(),
+                                                          c.row_ptr.get(), cnt.get());
+        }
         APF_CUDA(cudaGetLastError());
         k.rows = k.cols = n;
         k.row_ptr.allocate(static_cast<std::size_t>(n) + 1, s);
         const long long nnz = exclusive_scan(cnt.get(), k.row_ptr.get(), n, s);
-        g_kernel_launches += 3;
         k.col_idx.allocate(static_cast<std::size_t>(nnz), s);
         k.values.allocate(static_cast<std::size_t>(nnz), s);
-        k_row_fill<<<grid_for((long long)n * 32, 256), 256, 0, s>>>(
-            n_lambda, n_u, k.row_ptr.get(), a.row_ptr.get(), a.col_idx.get(), a.values.get(), bt.row_ptr.get(),
-            bt.col_idx.get(), bt.values.get(), b.row_ptr.get(), b.col_idx.get(), b.values.get(), c.row_ptr.get(),
-            c.col_idx.get(), c.values.get(), k.col_idx.get(), k.values.get());
-        g_kernel_launches += 1;
+        {
+            APF_KERNEL("k_row_fill", s);
+            k_row_fill<<<grid_for((long long)n * 32, 256), 256, 0, s>>>(
+                n_lambda, n_u, k.row_ptr.get(), a.row_ptr.get(), a.col_idx.get(), a.values.get(), bt.row_ptr.get(),
+                bt.col_idx.get(), bt.values.get(), b.row_ptr.get(), b.col_idx.get(), b.values.get(), c.row_ptr.get(),
+                c.col_idx.get(), c.values.get(), k.col_idx.get(), k.values.get());
+        }
         APF_CUDA(cudaGetLastError());
     }
 
@@ -964,9 +979,11 @@ namespace apf
         DeviceBuffer<int> status(1, s);
         status.zero();
         inv_diag.allocate(static_cast<std::size_t>(A_y.rows), s);
-        csr_diagonal<<<grid_for(A_y.rows, 256), 256, 0, s>>>(A_y.rows, A_y.row_ptr.get(), A_y.col_idx.get(),
-                                                             A_y.values.get(), diag_tol, inv_diag.get(), status.get());
-        g_kernel_launches += 1;
+        {
+            APF_KERNEL("csr_diagonal", s);
+            csr_diagonal<<<grid_for(A_y.rows, 256), 256, 0, s>>>(A_y.rows, A_y.row_ptr.get(), A_y.col_idx.get(),
+                                                                 A_y.values.get(), diag_tol, inv_diag.get(), status.get());
+        }
         APF_CUDA(cudaGetLastError());
         if (check_status(status, s) != 0)
             throw Error(APF_ERR_NUMERIC, "diagonal_schur_approximation: A_y diagonal must be positive.");
@@ -988,14 +1005,15 @@ namespace apf
         const int blocks = grid_for(n_u, warps, 148 * 8);
         if (n_u > 0)
         {
-            hhat_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("hhat_rows_count", s);
+                hhat_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
+            }
             APF_CUDA(cudaGetLastError());
         }
         H.rows = H.cols = n_u;
         H.row_ptr.allocate(static_cast<std::size_t>(n_u) + 1, s);
         const long long nnz = exclusive_scan(counts.get(), H.row_ptr.get(), n_u, s);
-        g_kernel_launches += 3;
         if (check_status(status, s) != 0)
             throw Error(APF_ERR_CAPACITY, "graph norm: per-row candidate buffer overflow");
         H.col_idx.allocate(static_cast<std::size_t>(nnz), s);
@@ -1005,8 +1023,10 @@ namespace apf
         a.val_out = H.values.get();
         if (n_u > 0)
         {
-            hhat_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("hhat_rows_fill", s);
+                hhat_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
+            }
             APF_CUDA(cudaGetLastError());
         }
         if (check_status(status, s) != 0)
@@ -1068,8 +1088,10 @@ namespace apf
                 ident[3 * c] = 1.0; ident[3 * c + 1] = 0.0; ident[3 * c + 2] = 1.0;
             }
             APF_CUDA(cudaMemcpyAsync(in.m_x.get(), ident.data(), ident.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-            scatter_m_to_x<<<grid_for(in.n_y_cells, 256), 256, 0, s>>>(in.n_y_cells, in.y_to_x.get(), in.m_y.get(), in.m_x.get());
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("scatter_m_to_x", s);
+                scatter_m_to_x<<<grid_for(in.n_y_cells, 256), 256, 0, s>>>(in.n_y_cells, in.y_to_x.get(), in.m_y.get(), in.m_x.get());
+            }
             APF_CUDA(cudaGetLastError());
             sync(s);
         }
@@ -1078,27 +1100,35 @@ namespace apf
         DeviceBuffer<int> pos(static_cast<std::size_t>(in.n_x_cells) + 1, s);
         if (in.n_x_cells > 0)
         {
-            mark_bottom<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, in.x_geo.get(), flag.get());
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("mark_bottom", s);
+                mark_bottom<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, in.x_geo.get(), flag.get());
+            }
         }
         const long long nb = exclusive_scan(flag.get(), pos.get(), in.n_x_cells, s);
-        g_kernel_launches += 3;
         in.n_bottom = static_cast<int>(nb);
         in.bottom_list.allocate(static_cast<std::size_t>(std::max<long long>(nb, 1)), s);
         if (in.n_x_cells > 0)
         {
-            compact_flags<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, flag.get(), pos.get(), in.bottom_list.get());
-            g_kernel_launches += 1;
+            {
+                APF_KERNEL("compact_flags", s);
+                compact_flags<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, flag.get(), pos.get(), in.bottom_list.get());
+            }
         }
         // max entries per restriction row
         DeviceBuffer<int> mx(1, s);
         mx.zero();
         const int ny_rows = in.n_y_cells * in.ndof, nx_rows = in.n_x_cells * in.ndof;
         if (ny_rows > 0)
-            max_restr_row<<<grid_for(ny_rows, 256, 1024), 256, 0, s>>>(ny_rows, in.y_off.get(), mx.get());
+            {
+                APF_KERNEL("max_restr_row", s);
+                max_restr_row<<<grid_for(ny_rows, 256, 1024), 256, 0, s>>>(ny_rows, in.y_off.get(), mx.get());
+            }
         if (nx_rows > 0)
-            max_restr_row<<<grid_for(nx_rows, 256, 1024), 256, 0, s>>>(nx_rows, in.x_off.get(), mx.get());
-        g_kernel_launches += 2;
+            {
+                APF_KERNEL("max_restr_row", s);
+                max_restr_row<<<grid_for(nx_rows, 256, 1024), 256, 0, s>>>(nx_rows, in.x_off.get(), mx.get());
+            }
         APF_CUDA(cudaGetLastError());
         APF_CUDA(cudaMemcpyAsync(&in.kmax, mx.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         sync(s);

@@ -13,6 +13,8 @@ struct apf_ctx
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::string last_error;
+    apf::Profiler profiler;
+    std::string report;
 };
 
 struct apf_system
@@ -26,6 +28,11 @@ namespace
     template<class F>
     int guarded(apf_ctx* ctx, F&& f)
     {
+        struct ProfilerScope
+        {
+            explicit ProfilerScope(apf_ctx* c) { apf::t_profiler = c ? &c->profiler : nullptr; }
+            ~ProfilerScope() { apf::t_profiler = nullptr; }
+        } scope(ctx);
         try
         {
             if (ctx)
@@ -204,6 +211,36 @@ int apf_ctx_synchronize(apf_ctx* ctx)
 int64_t apf_ctx_kernel_launches(const apf_ctx*)
 {
     return apf::g_kernel_launches.load();
+}
+
+int apf_ctx_set_timing(apf_ctx* ctx, int enable)
+{
+    if (!ctx)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        ctx->profiler.flush();
+        ctx->profiler.enabled = enable != 0;
+        ctx->profiler.totals.clear();
+    });
+}
+
+const char* apf_ctx_timing_report(apf_ctx* ctx)
+{
+    if (!ctx)
+        return "{}";
+    ctx->profiler.flush();
+    std::string r = "{";
+    bool first = true;
+    for (const auto& [name, v] : ctx->profiler.totals)
+    {
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "%s\"%s\": [%lld, %.6f]", first ? "" : ", ", name.c_str(), v.first, v.second);
+        r += buf;
+        first = false;
+    }
+    r += "}";
+    ctx->report = r;
+    return ctx->report.c_str();
 }
 
 int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs_on_device, apf_system** out)

@@ -3,10 +3,13 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/apf_b200.h"
@@ -104,6 +107,76 @@ namespace apf
         DeviceBuffer<double> values;
         std::int64_t nnz() const noexcept { return static_cast<std::int64_t>(col_idx.size()); }
     };
+
+    extern std::atomic<long long> g_kernel_launches;
+
+    // Optional per-kernel CUDA-event timing (enabled per context with apf_ctx_set_timing).
+    struct Profiler
+    {
+        bool enabled = false;
+        struct Rec
+        {
+            const char* name;
+            cudaEvent_t a, b;
+        };
+        std::vector<Rec> pending;
+        std::map<std::string, std::pair<long long, double>> totals; // name -> (launches, ms)
+
+        void flush()
+        {
+            for (auto& r : pending)
+            {
+                float ms = 0.f;
+                cudaEventSynchronize(r.b);
+                cudaEventElapsedTime(&ms, r.a, r.b);
+                auto& t = totals[r.name];
+                t.first += 1;
+                t.second += ms;
+                cudaEventDestroy(r.a);
+                cudaEventDestroy(r.b);
+            }
+            pending.clear();
+        }
+    };
+
+    // Profiler of the context whose call is running on this thread (set by the C-ABI layer).
+    extern thread_local Profiler* t_profiler;
+
+    // Counts a kernel launch and, when timing is on, brackets it with CUDA events
+    // recorded on the launching stream.
+    class KernelTimer
+    {
+    public:
+        KernelTimer(const char* name, cudaStream_t s) : s_(s)
+        {
+            g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+            if (t_profiler && t_profiler->enabled)
+            {
+                rec_.name = name;
+                cudaEventCreate(&rec_.a);
+                cudaEventCreate(&rec_.b);
+                cudaEventRecord(rec_.a, s);
+                on_ = true;
+            }
+        }
+        ~KernelTimer()
+        {
+            if (on_)
+            {
+                cudaEventRecord(rec_.b, s_);
+                t_profiler->pending.push_back(rec_);
+            }
+        }
+
+    private:
+        cudaStream_t s_;
+        Profiler::Rec rec_{};
+        bool on_ = false;
+    };
+
+#define APF_KT_CAT2(a, b) a##b
+#define APF_KT_CAT(a, b) APF_KT_CAT2(a, b)
+#define APF_KERNEL(name, stream) ::apf::KernelTimer APF_KT_CAT(apf_kt_, __LINE__)(name, stream)
 
     // Exclusive scan of n int32 counts into out[0..n] (out[n] = total); returns the total.
     long long exclusive_scan(const int* counts, int* out, int n, cudaStream_t s);

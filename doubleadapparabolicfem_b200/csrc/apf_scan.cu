@@ -100,9 +100,18 @@ namespace apf
             APF_CUDA(cudaMemsetAsync(out, 0, sizeof(int), s));
             return 0;
         }
-        scan_block_sums<<<nb, kScanBlock, 0, s>>>(counts, n, sums.get());
-        scan_sums_serial<<<1, kScanBlock, 0, s>>>(sums.get(), nb, total);
-        scan_apply<<<nb, kScanBlock, 0, s>>>(counts, n, sums.get(), total, out);
+        {
+            APF_KERNEL("scan_block_sums", s);
+            scan_block_sums<<<nb, kScanBlock, 0, s>>>(counts, n, sums.get());
+        }
+        {
+            APF_KERNEL("scan_sums_serial", s);
+            scan_sums_serial<<<1, kScanBlock, 0, s>>>(sums.get(), nb, total);
+        }
+        {
+            APF_KERNEL("scan_apply", s);
+            scan_apply<<<nb, kScanBlock, 0, s>>>(counts, n, sums.get(), total, out);
+        }
         APF_CUDA(cudaGetLastError());
         long long h_total = 0;
         APF_CUDA(cudaMemcpyAsync(&h_total, total, sizeof(long long), cudaMemcpyDeviceToHost, s));

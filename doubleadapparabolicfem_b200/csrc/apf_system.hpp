@@ -8,8 +8,6 @@
 
 namespace apf
 {
-    extern std::atomic<long long> g_kernel_launches;
-
     // local-block kinds of the row gather
     enum Kind : int
     {

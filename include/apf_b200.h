@@ -95,8 +95,14 @@ int apf_ctx_create(int device, void* stream, apf_ctx** out);
 void apf_ctx_destroy(apf_ctx* ctx);
 const char* apf_ctx_last_error(const apf_ctx* ctx);
 int apf_ctx_synchronize(apf_ctx* ctx);
-/* Number of kernels this context has launched since creation. */
+/* Number of kernels the library has launched in this process. */
 int64_t apf_ctx_kernel_launches(const apf_ctx* ctx);
+/* Per-kernel CUDA-event timing on the context's stream (the GPU counterpart of the
+ * reference's TimingRecorder, src/finite_element/detail/timing.hpp).  Enabling
+ * resets the totals. */
+int apf_ctx_set_timing(apf_ctx* ctx, int enable);
+/* JSON object {"kernel": [launches, total_ms], ...}; valid until the next call. */
+const char* apf_ctx_timing_report(apf_ctx* ctx);
 
 /* ---- assembly ------------------------------------------------------------------ */
 /* Replaces finite_element::system::assemble_main_system_blocks<QS,QT,Backend>

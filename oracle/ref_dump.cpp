@@ -11,6 +11,7 @@
 //     (src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:22).
 //
 // usage: apf_ref_dump <dim:2> <p:1|2> <uniform_levels> <example> <outdir>
+//        apf_ref_dump bench <p:1|2> <uniform_levels> <example> <reps>
 
 #include <cstdio>
 #include <cstdlib>
@@ -19,6 +20,8 @@
 #include <unordered_map>
 #include <unordered_set>
 #include <algorithm>
+#include <chrono>
+#include <omp.h>
 #include <iostream>
 #include <string>
 #include <vector>
@@ -169,6 +172,46 @@ namespace
         throw std::runtime_error("uniform_isotropic_refine: no spatial shrink after 32 waves");
     }
 
+    // Times the reference's own CPU assembly path (main blocks + graph-norm block)
+    // on the uniform mesh of outer level `levels`; prints one JSON line.
+    template<int P>
+    int bench_2d(int levels, const std::string& example_name, int reps)
+    {
+        constexpr int QSpace = 4 * P + 1;
+        constexpr int QTime = 2 * P + 1;
+        using GT = mesh::MeshTraits<2>;
+        using FET = finite_element::FiniteElementTraits<GT, P, P>;
+        using XSpace = finite_element::FESpace<GT, FET, finite_element::SpaceTimePolicy>;
+        using YSpace = finite_element::FESpace<GT, FET, finite_element::SpaceOnlyPolicy>;
+        auto example = adaptive_algorithm::examples::make_2d_example(example_name);
+        auto mesh = adaptive_algorithm::examples::make_initial_mesh_from_example(example);
+        XSpace x_space(mesh);
+        YSpace y_space(mesh);
+        adaptive_algorithm::examples::initialize_spaces_from_example(x_space, y_space, example);
+        for (int k = 0; k < levels; ++k)
+            uniform_isotropic_refine(x_space);
+        y_space.initialize(x_space.active_cells());
+        const int n_cells = static_cast<int>(y_space.active_cells().size());
+        const int n_dofs = x_space.dof_handler_ref().n_true_dofs() + y_space.dof_handler_ref().n_true_dofs();
+        double best = 1e300, total = 0.0;
+        for (int r = 0; r < reps; ++r)
+        {
+            const auto t0 = std::chrono::steady_clock::now();
+            const auto blocks = finite_element::system::assemble_main_system_blocks<QSpace, QTime, Backend>(
+                y_space, x_space, example.problem, 1e-15, -1.0);
+            const auto gn = finite_element::assembly::assemble_parabolic_graph_norm_approximation<QSpace, QTime, Backend>(
+                y_space, x_space, example.problem.M, blocks.A_y(), blocks.C_signed(), 1e-15, 1e-14);
+            const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            best = std::min(best, dt);
+            total += dt;
+            if (gn.approximation.hhat.rows() < 0) return 3;
+        }
+        std::printf("{\"stage\": \"assembly+graph_norm\", \"p\": %d, \"level\": %d, \"n_cells\": %d, \"n_dofs\": %d, "
+                    "\"reps\": %d, \"mean_s\": %.6f, \"best_s\": %.6f, \"threads\": %d}\n",
+                    P, levels, n_cells, n_dofs, reps, total / reps, best, omp_get_max_threads());
+        return 0;
+    }
+
     template<int P>
     int run_2d(int levels, const std::string& example_name, const std::string& dir)
     {
@@ -230,6 +273,23 @@ namespace
 
 int main(int argc, char** argv)
 {
+    if (argc == 6 && std::string(argv[1]) == "bench")
+    {
+        const int p = std::atoi(argv[2]);
+        const int levels = std::atoi(argv[3]);
+        const int reps = std::atoi(argv[5]);
+        try
+        {
+            if (p == 1) return bench_2d<1>(levels, argv[4], reps);
+            if (p == 2) return bench_2d<2>(levels, argv[4], reps);
+        }
+        catch (const std::exception& e)
+        {
+            std::fprintf(stderr, "apf_ref_dump: %s\n", e.what());
+            return 1;
+        }
+        return 2;
+    }
     if (argc != 6)
     {
         std::fprintf(stderr, "usage: %s <dim:2> <p:1|2> <uniform_levels> <example> <outdir>\n", argv[0]);
