@@ -61,6 +61,39 @@ class ProblemDesc(C.Structure):
     ]
 
 
+class SolverOptions(C.Structure):
+    _fields_ = [
+        ("tolerance", C.c_double),
+        ("max_iterations", C.c_int),
+        ("use_true_residual_batching", C.c_int),
+        ("true_residual_check_interval", C.c_int),
+        ("preconditioner", C.c_int),
+        ("amg_smooth_steps", C.c_int),
+        ("amg_strength", C.c_double),
+        ("amg_coarse_size", C.c_int),
+    ]
+
+
+class SolverDiagnostics(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("residual_check_batches", C.c_int),
+        ("converged", C.c_int),
+        ("backend_converged", C.c_int),
+        ("backend_reported_error", C.c_double),
+        ("final_true_residual", C.c_double),
+        ("setup_seconds", C.c_double),
+        ("solve_seconds", C.c_double),
+        ("amg_levels_lambda", C.c_int),
+        ("amg_levels_u", C.c_int),
+        ("amg_nnz_lambda", C.c_int64),
+        ("amg_nnz_u", C.c_int64),
+    ]
+
+
+APF_PRECOND_AMG_BLOCK = 0
+APF_PRECOND_LEARNED = 1
+
 _lib = None
 
 # exported symbols and their signatures (argtypes, restype)
@@ -81,6 +114,11 @@ SIGNATURES = {
                                       C.POINTER(C.c_void_p)], C.c_int),
     "apf_system_vector_copy": ([C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int], C.c_int),
     "apf_system_destroy": ([C.c_void_p], None),
+    "apf_solver_options_default": ([C.POINTER(SolverOptions)], None),
+    "apf_setup_preconditioner": ([C.c_void_p, C.c_void_p, C.POINTER(SolverOptions)], C.c_int),
+    "apf_solve_minres": ([C.c_void_p, C.c_void_p, C.POINTER(SolverOptions), C.c_void_p, C.c_void_p, C.c_int,
+                          C.POINTER(SolverDiagnostics)], C.c_int),
+    "apf_system_solution_device_ptr": ([C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
 }
 
 

@@ -1,0 +1,48 @@
+// Smoothed-aggregation algebraic multigrid on the device, used as an SPD block
+// preconditioner (one symmetric V-cycle = a fixed SPD linear operator, so MINRES
+// remains a short-recurrence method).
+#pragma once
+
+#include <vector>
+
+#include "apf_sparse.cuh"
+
+namespace apf
+{
+    struct AmgOptions
+    {
+        double strength = 0.08;   // strong: |a_ij| >= strength * sqrt(a_ii a_jj)
+        int smooth_steps = 1;     // damped-Jacobi sweeps before and after the coarse correction
+        int coarse_size = 1024;   // dense solve at or below this size
+        int max_levels = 20;
+    };
+
+    struct AmgLevel
+    {
+        DeviceCsr A_own;              // level operator (coarse levels own theirs)
+        const DeviceCsr* A = nullptr; // finest level references the caller's matrix
+        DeviceCsr P;                  // prolongation (n x n_coarse)
+        DeviceCsr R;                  // restriction = P^T
+        DeviceBuffer<double> dinv;    // 1 / diag(A)
+        double omega = 0.0;           // Jacobi damping 4 / (3 rho(D^-1 A))
+        DeviceBuffer<double> x, b, r, t;
+    };
+
+    class Amg
+    {
+    public:
+        void setup(cudaStream_t s, const DeviceCsr& A, const AmgOptions& opt, Workspace& w);
+        // x = V-cycle(b); x and b are device vectors of the finest size.
+        void apply(cudaStream_t s, const double* b, double* x);
+        int levels() const { return static_cast<int>(levels_.size()); }
+        long long operator_nnz() const;
+        std::vector<int> level_rows() const;
+
+    private:
+        void vcycle(cudaStream_t s, int l, const double* b, double* x);
+        std::vector<AmgLevel> levels_;
+        DeviceBuffer<double> coarse_inv_; // dense inverse of the coarsest operator, row-major
+        int n_coarse_ = 0;
+        AmgOptions opt_{};
+    };
+}

@@ -17,8 +17,10 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <type_traits>
 
 #include "apf_device.cuh"
+#include "apf_warpsort.cuh"
 #include "apf_internal.hpp"
 #include "apf_system.hpp"
 
@@ -189,44 +191,6 @@ namespace apf
         // ------------------------------------------------------------------
         // warp-level candidate sort / reduce
         // ------------------------------------------------------------------
-        // key = col (high 32) | seq (17 bits) | slot (15 bits)
-        constexpr int kSlotBits = 15;
-        constexpr int kSeqBits = 17;
-
-        __device__ __forceinline__ unsigned long long make_key(int col, int seq, int slot)
-        {
-            return (static_cast<unsigned long long>(static_cast<unsigned>(col)) << 32) |
-                   (static_cast<unsigned long long>(seq & ((1 << kSeqBits) - 1)) << kSlotBits) |
-                   static_cast<unsigned long long>(slot);
-        }
-
-        // In-place ascending bitonic sort of n (power of two) keys by one warp.
-        __device__ void warp_bitonic_sort(unsigned long long* keys, int n)
-        {
-            const int lane = threadIdx.x & 31;
-            for (int k = 2; k <= n; k <<= 1)
-            {
-                for (int j = k >> 1; j > 0; j >>= 1)
-                {
-                    for (int i = lane; i < n; i += 32)
-                    {
-                        const int ixj = i ^ j;
-                        if (ixj > i)
-                        {
-                            const unsigned long long a = keys[i], b = keys[ixj];
-                            const bool up = (i & k) == 0;
-                            if ((a > b) == up)
-                            {
-                                keys[i] = b;
-                                keys[ixj] = a;
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
-            }
-        }
-
         struct Term
         {
             int kind;
@@ -600,6 +564,26 @@ namespace apf
             double* val_out;
             int* status;
         };
+
+        // max over rows of |C row| + sum_{c in B_dt row} |B_dt^T row c| + |A_x row|
+        __global__ void hhat_row_bound(HhatArgs A, int* __restrict__ out)
+        {
+            int m = 0;
+            for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.n_u; row += gridDim.x * blockDim.x)
+            {
+                int n = (A.c_ptr[row + 1] - A.c_ptr[row]) + (A.ax_ptr[row + 1] - A.ax_ptr[row]);
+                for (int k = A.bd_ptr[row]; k < A.bd_ptr[row + 1]; ++k)
+                {
+                    const int c = A.bd_col[k];
+                    n += A.bt_ptr[c + 1] - A.bt_ptr[c];
+                }
+                m = max(m, n);
+            }
+            for (int o = 16; o > 0; o >>= 1)
+                m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0)
+                atomicMax(out, m);
+        }
 
         // Candidates: (col, value, is_ax).  Reference semantics
         // (schur_approximations.hpp:107-200, sparse_matrix_ops.hpp:286-316 with zero_tol 0):
@@ -997,20 +981,47 @@ namespace apf
         a.status = status.get();
         DeviceBuffer<int> counts(static_cast<std::size_t>(n_u) + 1, s);
         a.row_count = counts.get();
-        constexpr int CAP = 4096;
-        const int warps = 2, threads = warps * 32;
-        const size_t smem = (size_t)warps * CAP * 16;
-        APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const int blocks = grid_for(n_u, warps, 148 * 8);
+        // upper bound of the candidates of any row -> candidate buffer size
+        DeviceBuffer<int> bound(1, s);
+        bound.zero();
         if (n_u > 0)
         {
+            APF_KERNEL("hhat_row_bound", s);
+            hhat_row_bound<<<grid_for(n_u, 256, 148 * 8), 256, 0, s>>>(a, bound.get());
+        }
+        int cap = 0;
+        APF_CUDA(cudaMemcpyAsync(&cap, bound.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        auto run = [&](auto cap_tag, bool fill) {
+            constexpr int CAP = decltype(cap_tag)::value;
+            const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 16)));
+            const int threads = warps * 32;
+            const size_t smem = (size_t)warps * CAP * 16;
+            const int blocks = grid_for(n_u, warps, 148 * 32);
+            if (fill)
             {
+                APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                APF_KERNEL("hhat_rows_fill", s);
+                hhat_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
+            }
+            else
+            {
+                APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 APF_KERNEL("hhat_rows_count", s);
                 hhat_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
             }
             APF_CUDA(cudaGetLastError());
-        }
+        };
+        auto dispatch = [&](bool fill) {
+            if (n_u == 0) return;
+            if (cap <= 256) run(std::integral_constant<int, 256>{}, fill);
+            else if (cap <= 512) run(std::integral_constant<int, 512>{}, fill);
+            else if (cap <= 1024) run(std::integral_constant<int, 1024>{}, fill);
+            else if (cap <= 2048) run(std::integral_constant<int, 2048>{}, fill);
+            else if (cap <= 4096) run(std::integral_constant<int, 4096>{}, fill);
+            else throw Error(APF_ERR_CAPACITY, "graph norm: a row has more than 4096 candidates");
+        };
+        dispatch(false);
         H.rows = H.cols = n_u;
         H.row_ptr.allocate(static_cast<std::size_t>(n_u) + 1, s);
         const long long nnz = exclusive_scan(counts.get(), H.row_ptr.get(), n_u, s);
@@ -1021,14 +1032,7 @@ namespace apf
         a.row_ptr = H.row_ptr.get();
         a.col_out = H.col_idx.get();
         a.val_out = H.values.get();
-        if (n_u > 0)
-        {
-            {
-                APF_KERNEL("hhat_rows_fill", s);
-                hhat_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
-            }
-            APF_CUDA(cudaGetLastError());
-        }
+        dispatch(true);
         if (check_status(status, s) != 0)
             throw Error(APF_ERR_CAPACITY, "graph norm: per-row candidate buffer overflow");
     }

@@ -1,5 +1,8 @@
 // extern "C" entry points of libapf_b200 (declared in include/apf_b200.h) and the
 // host-side drivers that sequence the device kernels.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -350,6 +353,126 @@ int apf_system_vector_copy(apf_ctx* ctx, const apf_system* sys, int which, doubl
                                      to_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
         APF_CUDA(cudaStreamSynchronize(ctx->stream));
     });
+}
+
+void apf_solver_options_default(apf_solver_options* opt)
+{
+    if (!opt)
+        return;
+    opt->tolerance = 1e-8;
+    opt->max_iterations = 20000;
+    opt->use_true_residual_batching = 1;
+    opt->true_residual_check_interval = 100;
+    opt->preconditioner = APF_PRECOND_AMG_BLOCK;
+    opt->amg_smooth_steps = 1;
+    opt->amg_strength = 0.08;
+    opt->amg_coarse_size = 256;
+}
+
+namespace
+{
+    apf::AmgOptions amg_options(const apf_solver_options* o)
+    {
+        apf::AmgOptions a;
+        a.smooth_steps = std::max(1, o->amg_smooth_steps);
+        a.strength = o->amg_strength;
+        a.coarse_size = std::max(16, o->amg_coarse_size);
+        return a;
+    }
+
+    void setup_precond(apf_ctx* ctx, apf_system* h, const apf_solver_options* opt)
+    {
+        auto& S = h->sys;
+        apf::require(S.have[APF_BLOCK_HHAT], APF_ERR_INVALID,
+                     "ParabolicGraphNorm requires graph-norm block context from assembly (call apf_assemble_graph_norm)");
+        const auto t0 = std::chrono::steady_clock::now();
+        S.precond = std::make_unique<apf::BlockPreconditioner>();
+        S.precond_opts = amg_options(opt);
+        S.precond->setup(ctx->stream, S.blocks[APF_BLOCK_A_Y], S.blocks[APF_BLOCK_HHAT], S.precond_opts, S.ws);
+        apf::sync(ctx->stream);
+        S.precond_setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+}
+
+int apf_setup_preconditioner(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt)
+{
+    if (!ctx || !sys || !opt)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] { setup_precond(ctx, sys, opt); });
+}
+
+int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* initial_guess,
+                     double* solution, int pointers_on_device, apf_solver_diagnostics* diag)
+{
+    if (!ctx || !sys || !opt)
+        return APF_ERR_INVALID;
+    apf::MinresSummary summary;
+    double solve_seconds = 0.0;
+    int rc = guarded(ctx, [&] {
+        auto& S = sys->sys;
+        cudaStream_t s = ctx->stream;
+        apf::require(opt->tolerance >= 0.0, APF_ERR_INVALID, "negative tolerance");
+        if (!S.precond)
+            setup_precond(ctx, sys, opt);
+        const int nl = S.in.n_lambda, nu = S.in.n_u, n = nl + nu;
+        S.rhs.allocate(n, s);
+        apf::copy(s, nl, S.f.get(), S.rhs.get());
+        apf::copy(s, nu, S.g.get(), S.rhs.get() + nl);
+        S.solution.allocate(n, s);
+        if (initial_guess)
+            APF_CUDA(cudaMemcpyAsync(S.solution.get(), initial_guess, n * sizeof(double),
+                                     pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        else
+            apf::fill(s, n, 0.0, S.solution.get());
+        apf::MinresOptions mo;
+        mo.tolerance = opt->tolerance;
+        mo.max_iterations = opt->max_iterations;
+        mo.batch = opt->use_true_residual_batching ? opt->true_residual_check_interval : opt->max_iterations;
+        const auto t0 = std::chrono::steady_clock::now();
+        summary = apf::minres_solve(s, S.blocks[APF_BLOCK_K], *S.precond, S.rhs.get(), S.solution.get(), mo, S.ws);
+        solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (solution)
+            APF_CUDA(cudaMemcpyAsync(solution, S.solution.get(), n * sizeof(double),
+                                     pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+        apf::sync(s);
+    });
+    if (diag)
+    {
+        *diag = apf_solver_diagnostics{};
+        diag->iterations = summary.iterations;
+        diag->residual_check_batches = summary.batches;
+        diag->converged = summary.converged ? 1 : 0;
+        diag->backend_converged = summary.backend_converged ? 1 : 0;
+        diag->backend_reported_error = summary.backend_error;
+        diag->final_true_residual = summary.true_residual;
+        diag->setup_seconds = sys->sys.precond_setup_seconds;
+        diag->solve_seconds = solve_seconds;
+        if (sys->sys.precond)
+        {
+            diag->amg_levels_lambda = sys->sys.precond->amg_a.levels();
+            diag->amg_levels_u = sys->sys.precond->amg_h.levels();
+            diag->amg_nnz_lambda = sys->sys.precond->amg_a.operator_nnz();
+            diag->amg_nnz_u = sys->sys.precond->amg_h.operator_nnz();
+        }
+    }
+    if (rc == APF_OK && !summary.converged)
+    {
+        char buf[256];
+        std::snprintf(buf, sizeof(buf),
+                      "MINRES(ParabolicGraphNorm) solve failed. iterations=%d, error=%.12e, true_relative_residual=%.12e",
+                      summary.iterations, summary.backend_error, summary.true_residual);
+        ctx->last_error = buf;
+        rc = APF_ERR_NOT_CONVERGED;
+    }
+    return rc;
+}
+
+int apf_system_solution_device_ptr(const apf_system* sys, const double** solution)
+{
+    if (!sys || !solution || !sys->sys.solution.size())
+        return APF_ERR_INVALID;
+    *solution = sys->sys.solution.get();
+    return APF_OK;
 }
 
 void apf_system_destroy(apf_system* sys)

@@ -1,0 +1,351 @@
+// Block-preconditioned MINRES on the device.
+//
+// Restates the reference's solve path (src/linear_algebra/eigen_backend/preconditioners/
+// parabolic_graph_norm_minres.hpp:232-369 with iterative_residual_acceptance.hpp:118-216):
+//   * preconditioned MINRES (Paige & Saunders 1975, Lanczos form) on K = [A_y B^T; B C];
+//   * block preconditioner P = blkdiag(A_y, Hhat): the reference factors both blocks with a
+//     sparse Cholesky; here each block is applied as one symmetric smoothed-aggregation
+//     AMG V-cycle (a fixed SPD operator), or the learned preconditioner built on it;
+//   * backend stopping test ||r_0|| phibar_k / beta_1 < tol ||b||;
+//   * batches of `true_residual_check_interval` iterations; after each batch the FP64
+//     true residual ||K x - b|| / ||b|| accepts; if the backend had converged but the
+//     true residual did not, the backend tolerance is multiplied by 0.1 (floor
+//     max(eps, tol sqrt(eps))); the batch restarts from the current iterate.
+// All Lanczos scalars live in device memory; the host only reads the status every
+// `kCheckEvery` iterations, so iterations run back to back on the stream.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <limits>
+
+#include "apf_minres.cuh"
+
+namespace apf
+{
+    namespace
+    {
+        struct MinresDev
+        {
+            double beta, oldb, alfa, dbar, epsln, phibar, cs, sn, gamma, delta, phi, oldeps;
+            double beta1, r0n, bn, tol, err, bb;
+            int done, bad, its, pad;
+        };
+
+        constexpr int kThreads = 256;
+        constexpr int kCheckEvery = 8;
+
+        int nb(long long n)
+        {
+            return static_cast<int>(std::max<long long>(1, std::min<long long>((n + kThreads - 1) / kThreads, kRedBlocks)));
+        }
+
+        __device__ __forceinline__ double block_sum(double v)
+        {
+            __shared__ double ws[kThreads / 32];
+            for (int o = 16; o > 0; o >>= 1)
+                v += __shfl_down_sync(0xffffffffu, v, o);
+            if ((threadIdx.x & 31) == 0)
+                ws[threadIdx.x >> 5] = v;
+            __syncthreads();
+            double t = 0.0;
+            if (threadIdx.x == 0)
+                for (int w = 0; w < kThreads / 32; ++w)
+                    t += ws[w];
+            return t;
+        }
+
+        __global__ void k_vscale(int n, const double* __restrict__ z, double* __restrict__ v, const MinresDev* S)
+        {
+            if (S->done)
+                return;
+            const double s = 1.0 / S->beta;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                v[i] = s * z[i];
+        }
+
+        // y -= (beta/oldb) r1 (not on the first iteration); partial sums of v.y
+        __global__ void k_t1(int n, double* __restrict__ y, const double* __restrict__ r1, const double* __restrict__ v,
+                             const MinresDev* S, int first, double* __restrict__ partials)
+        {
+            const double c = (first || S->done) ? 0.0 : S->beta / S->oldb;
+            double acc = 0.0;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+            {
+                const double yi = y[i] - c * r1[i];
+                y[i] = yi;
+                acc += v[i] * yi;
+            }
+            const double t = block_sum(acc);
+            if (threadIdx.x == 0)
+                partials[blockIdx.x] = t;
+        }
+
+        __global__ void k_alfa(int nparts, const double* __restrict__ partials, MinresDev* S)
+        {
+            __shared__ double ws[32];
+            double s = 0.0;
+            for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+                s += partials[i];
+            for (int o = 16; o > 0; o >>= 1)
+                s += __shfl_down_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0)
+                ws[threadIdx.x >> 5] = s;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                double t = 0.0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+                    t += ws[w];
+                if (!S->done)
+                    S->alfa = t;
+            }
+        }
+
+        __global__ void k_t2(int n, double* __restrict__ y, const double* __restrict__ r2, const MinresDev* S)
+        {
+            if (S->done)
+                return;
+            const double c = S->alfa / S->beta;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                y[i] -= c * r2[i];
+        }
+
+        __global__ void k_dot_partials(int n, const double* __restrict__ a, const double* __restrict__ b,
+                                       double* __restrict__ partials)
+        {
+            double acc = 0.0;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                acc += a[i] * b[i];
+            const double t = block_sum(acc);
+            if (threadIdx.x == 0)
+                partials[blockIdx.x] = t;
+        }
+
+        // Lanczos / Givens recurrences after beta_{k+1}^2 = r2.z is known
+        __global__ void k_scalars(int nparts, const double* __restrict__ partials, MinresDev* S)
+        {
+            __shared__ double ws[32];
+            double s = 0.0;
+            for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+                s += partials[i];
+            for (int o = 16; o > 0; o >>= 1)
+                s += __shfl_down_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0)
+                ws[threadIdx.x >> 5] = s;
+            __syncthreads();
+            if (threadIdx.x != 0 || S->done)
+                return;
+            double bb = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+                bb += ws[w];
+            S->bb = bb;
+            if (!(bb >= 0.0) || !isfinite(bb))
+            {
+                S->bad = 1;
+                S->done = 1;
+                return;
+            }
+            S->oldb = S->beta;
+            const double beta = sqrt(bb);
+            S->beta = beta;
+            S->oldeps = S->epsln;
+            const double delta = S->cs * S->dbar + S->sn * S->alfa;
+            const double gbar = S->sn * S->dbar - S->cs * S->alfa;
+            S->delta = delta;
+            S->epsln = S->sn * beta;
+            S->dbar = -S->cs * beta;
+            const double gamma = fmax(hypot(gbar, beta), 1e-300);
+            S->gamma = gamma;
+            S->cs = gbar / gamma;
+            S->sn = beta / gamma;
+            S->phi = S->cs * S->phibar;
+            S->phibar = S->sn * S->phibar;
+            S->its += 1;
+            S->err = S->r0n * (S->phibar / S->beta1) / S->bn;
+        }
+
+        // w_new = (v - oldeps w1 - delta w2)/gamma; x += phi w_new; (w1, w2) <- (w2, w_new)
+        __global__ void k_w(int n, const double* __restrict__ v, double* __restrict__ w1, double* __restrict__ w2,
+                            double* __restrict__ x, MinresDev* S)
+        {
+            if (S->done)
+                return;
+            const double oe = S->oldeps, de = S->delta, ig = 1.0 / S->gamma, ph = S->phi;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+            {
+                const double wn = (v[i] - oe * w1[i] - de * w2[i]) * ig;
+                w1[i] = w2[i];
+                w2[i] = wn;
+                x[i] += ph * wn;
+            }
+        }
+
+        // set done once the backend test passes (runs after k_w so the last update lands)
+        __global__ void k_check(MinresDev* S, int max_its)
+        {
+            if (S->done)
+                return;
+            if (S->err < S->tol || S->beta == 0.0 || S->its >= max_its)
+                S->done = 1;
+        }
+    }
+
+    void BlockPreconditioner::setup(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& Hhat, const AmgOptions& opt,
+                                    Workspace& w)
+    {
+        n_lambda = A_y.rows;
+        n_u = Hhat.rows;
+        amg_a.setup(s, A_y, opt, w);
+        amg_h.setup(s, Hhat, opt, w);
+    }
+
+    void BlockPreconditioner::apply(cudaStream_t s, const double* r, double* z)
+    {
+        amg_a.apply(s, r, z);
+        amg_h.apply(s, r + n_lambda, z + n_lambda);
+    }
+
+    MinresSummary minres_solve(cudaStream_t s, const DeviceCsr& K, Preconditioner& P, const double* b, double* x,
+                               const MinresOptions& opt, Workspace& w)
+    {
+        const int n = K.rows;
+        w.ensure(s);
+        MinresSummary sum;
+        DeviceBuffer<double> r1(n, s), r2(n, s), y(n, s), z(n, s), v(n, s), w1(n, s), w2(n, s), res(n, s);
+        DeviceBuffer<MinresDev> S(1, s);
+        DeviceBuffer<double> parts(kRedBlocks, s);
+        const double bn = std::sqrt(dot_host(s, w, n, b, b));
+        if (bn == 0.0)
+        {
+            fill(s, n, 0.0, x);
+            sum.converged = true;
+            sum.true_residual = 0.0;
+            return sum;
+        }
+        auto true_residual = [&]() {
+            residual(s, K, x, b, res.get());
+            return std::sqrt(dot_host(s, w, n, res.get(), res.get())) / bn;
+        };
+        const int limit = std::max(1, opt.max_iterations);
+        const int batch = std::min(limit, std::max(1, opt.batch));
+        const double target = std::max(0.0, opt.tolerance);
+        const double min_backend = std::max(std::numeric_limits<double>::epsilon(),
+                                            target * std::sqrt(std::numeric_limits<double>::epsilon()));
+        double backend_tol = target;
+        while (sum.iterations < limit)
+        {
+            const int this_batch = std::min(batch, limit - sum.iterations);
+            // --- one backend MINRES run from the current x ---
+            residual(s, K, x, b, r1.get());
+            P.apply(s, r1.get(), z.get());
+            const double r0n = std::sqrt(dot_host(s, w, n, r1.get(), r1.get()));
+            const double bb1 = dot_host(s, w, n, r1.get(), z.get());
+            if (!(bb1 >= 0.0))
+                throw Error(APF_ERR_NUMERIC, "MINRES: preconditioner is not positive definite");
+            const double beta1 = std::sqrt(bb1);
+            int its = 0;
+            bool backend_conv = false;
+            double backend_err = r0n / bn;
+            if (beta1 == 0.0 || r0n <= backend_tol * bn)
+            {
+                backend_conv = true;
+            }
+            else
+            {
+                MinresDev h{};
+                h.beta = beta1;
+                h.oldb = 0.0;
+                h.phibar = beta1;
+                h.cs = -1.0;
+                h.sn = 0.0;
+                h.beta1 = beta1;
+                h.r0n = r0n;
+                h.bn = bn;
+                h.tol = backend_tol;
+                h.err = backend_err;
+                APF_CUDA(cudaMemcpyAsync(S.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s));
+                copy(s, n, r1.get(), r2.get());
+                fill(s, n, 0.0, w1.get());
+                fill(s, n, 0.0, w2.get());
+                double* pr1 = r1.get();
+                double* pr2 = r2.get();
+                double* py = y.get();
+                int issued = 0;
+                MinresDev hs{};
+                while (issued < this_batch)
+                {
+                    const int chunk = std::min(kCheckEvery, this_batch - issued);
+                    for (int c = 0; c < chunk; ++c)
+                    {
+                        const int first = issued == 0;
+                        {
+                            APF_KERNEL("minres_vscale", s);
+                            k_vscale<<<nb(n), kThreads, 0, s>>>(n, z.get(), v.get(), S.get());
+                        }
+                        spmv(s, K, v.get(), py);
+                        {
+                            APF_KERNEL("minres_t1", s);
+                            k_t1<<<kRedBlocks, kThreads, 0, s>>>(n, py, pr1, v.get(), S.get(), first, parts.get());
+                        }
+                        {
+                            APF_KERNEL("minres_alfa", s);
+                            k_alfa<<<1, 256, 0, s>>>(kRedBlocks, parts.get(), S.get());
+                        }
+                        {
+                            APF_KERNEL("minres_t2", s);
+                            k_t2<<<nb(n), kThreads, 0, s>>>(n, py, pr2, S.get());
+                        }
+                        // rotate: r1 <- r2, r2 <- y
+                        double* t = pr1;
+                        pr1 = pr2;
+                        pr2 = py;
+                        py = t;
+                        P.apply(s, pr2, z.get());
+                        {
+                            APF_KERNEL("minres_dot", s);
+                            k_dot_partials<<<kRedBlocks, kThreads, 0, s>>>(n, pr2, z.get(), parts.get());
+                        }
+                        {
+                            APF_KERNEL("minres_scalars", s);
+                            k_scalars<<<1, 256, 0, s>>>(kRedBlocks, parts.get(), S.get());
+                        }
+                        {
+                            APF_KERNEL("minres_w", s);
+                            k_w<<<nb(n), kThreads, 0, s>>>(n, v.get(), w1.get(), w2.get(), x, S.get());
+                        }
+                        {
+                            APF_KERNEL("minres_check", s);
+                            k_check<<<1, 1, 0, s>>>(S.get(), this_batch);
+                        }
+                        ++issued;
+                    }
+                    APF_CUDA(cudaMemcpyAsync(&hs, S.get(), sizeof(hs), cudaMemcpyDeviceToHost, s));
+                    sync(s);
+                    if (hs.bad)
+                        throw Error(APF_ERR_NUMERIC, "MINRES: preconditioner is not positive definite");
+                    if (hs.done)
+                        break;
+                }
+                its = hs.its;
+                backend_err = hs.err;
+                backend_conv = hs.err < backend_tol || hs.beta == 0.0;
+            }
+            ++sum.batches;
+            sum.iterations += its;
+            sum.backend_error = backend_err;
+            sum.backend_converged = backend_conv;
+            const double rel = true_residual();
+            sum.true_residual = rel;
+            if (std::isfinite(rel) && rel <= target)
+            {
+                sum.converged = true;
+                return sum;
+            }
+            if (!std::isfinite(rel) || !std::isfinite(backend_err) || its <= 0)
+                return sum;
+            if (backend_conv)
+                backend_tol = std::max(min_backend, backend_tol * 0.1);
+        }
+        return sum;
+    }
+}

@@ -1,0 +1,45 @@
+// Block-preconditioned MINRES on the device (see apf_minres.cu).
+#pragma once
+
+#include "apf_amg.cuh"
+
+namespace apf
+{
+    // z = P^{-1} r for a fixed SPD operator P (full saddle size n_lambda + n_u).
+    class Preconditioner
+    {
+    public:
+        virtual ~Preconditioner() = default;
+        virtual void apply(cudaStream_t s, const double* r, double* z) = 0;
+    };
+
+    // blkdiag(A_y, Hhat)^{-1} approximated by one AMG V-cycle per block.
+    class BlockPreconditioner : public Preconditioner
+    {
+    public:
+        void setup(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& Hhat, const AmgOptions& opt, Workspace& w);
+        void apply(cudaStream_t s, const double* r, double* z) override;
+        int n_lambda = 0, n_u = 0;
+        Amg amg_a, amg_h;
+    };
+
+    struct MinresOptions
+    {
+        double tolerance = 1e-8;
+        int max_iterations = 20000;
+        int batch = 100; // true_residual_check_interval (0 or negative: no batching)
+    };
+
+    struct MinresSummary
+    {
+        int iterations = 0;
+        int batches = 0;
+        double backend_error = 0.0;
+        bool backend_converged = false;
+        double true_residual = 0.0;
+        bool converged = false;
+    };
+
+    MinresSummary minres_solve(cudaStream_t s, const DeviceCsr& K, Preconditioner& P, const double* b, double* x,
+                               const MinresOptions& opt, Workspace& w);
+}

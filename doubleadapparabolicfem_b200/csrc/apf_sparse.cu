@@ -1,0 +1,491 @@
+// Sparse/vector building blocks (see apf_sparse.cuh).
+#include <algorithm>
+#include <type_traits>
+
+#include "apf_sparse.cuh"
+#include "apf_warpsort.cuh"
+
+namespace apf
+{
+    namespace
+    {
+        int blocks_for(long long work, int threads, int cap = 148 * 32)
+        {
+            long long g = (work + threads - 1) / threads;
+            return static_cast<int>(std::max<long long>(1, std::min<long long>(g, cap)));
+        }
+
+        // G lanes per row; the row loop is warp-uniform so the shuffles see all 32 lanes.
+        // MODE 0: y = alpha A x + beta y;  1: y = b - A x;  2: y = x + alpha dinv (b - A x)
+        template<int G, int MODE>
+        __global__ void __launch_bounds__(256) spmv_kernel(int rows, const int* __restrict__ rp, const int* __restrict__ ci,
+                                                           const double* __restrict__ va, const double* __restrict__ x,
+                                                           const double* __restrict__ b, double* __restrict__ y,
+                                                           double alpha, double beta, const double* __restrict__ dinv)
+        {
+            constexpr int RPW = 32 / G; // rows per warp and step
+            const int lane = threadIdx.x & (G - 1);
+            const int sub = (threadIdx.x & 31) / G;
+            const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+            const long long nwarps = (gridDim.x * (long long)blockDim.x) >> 5;
+            for (long long base = warp * RPW; base < rows; base += nwarps * RPW)
+            {
+                const long long r = base + sub;
+                double sum = 0.0;
+                if (r < rows)
+                {
+                    const int s0 = rp[r], e = rp[r + 1];
+                    for (int k = s0 + lane; k < e; k += G)
+                        sum += va[k] * __ldg(x + ci[k]);
+                }
+#pragma unroll
+                for (int o = G / 2; o > 0; o >>= 1)
+                    sum += __shfl_down_sync(0xffffffffu, sum, o, G);
+                if (lane == 0 && r < rows)
+                {
+                    if (MODE == 1)
+                        y[r] = b[r] - sum;
+                    else if (MODE == 2)
+                        y[r] = x[r] + alpha * dinv[r] * (b[r] - sum);
+                    else
+                        y[r] = beta == 0.0 ? alpha * sum : alpha * sum + beta * y[r];
+                }
+            }
+        }
+
+        __global__ void dot_partials(int n, const double* __restrict__ a, const double* __restrict__ b,
+                                     double* __restrict__ partials)
+        {
+            __shared__ double ws[kRedThreads / 32];
+            double s = 0.0;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                s += a[i] * b[i];
+            for (int o = 16; o > 0; o >>= 1)
+                s += __shfl_down_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0)
+                ws[threadIdx.x >> 5] = s;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                double t = 0.0;
+                for (int w = 0; w < kRedThreads / 32; ++w)
+                    t += ws[w];
+                partials[blockIdx.x] = t;
+            }
+        }
+
+        __global__ void sum_partials(int n, const double* __restrict__ partials, double* __restrict__ out)
+        {
+            __shared__ double ws[32];
+            double s = 0.0;
+            for (int i = threadIdx.x; i < n; i += blockDim.x)
+                s += partials[i];
+            for (int o = 16; o > 0; o >>= 1)
+                s += __shfl_down_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0)
+                ws[threadIdx.x >> 5] = s;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                double t = 0.0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+                    t += ws[w];
+                *out = t;
+            }
+        }
+
+        __global__ void axpby_kernel(int n, double a, const double* __restrict__ x, double b, double* __restrict__ y)
+        {
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                y[i] = a * x[i] + (b == 0.0 ? 0.0 : b * y[i]);
+        }
+
+        __global__ void fill_kernel(int n, double v, double* __restrict__ y)
+        {
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                y[i] = v;
+        }
+
+        __global__ void inv_diag_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                        const double* __restrict__ va, double* __restrict__ inv)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+            {
+                double d = 0.0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                    if (ci[k] == r)
+                        d += va[k];
+                inv[r] = d != 0.0 ? 1.0 / d : 0.0;
+            }
+        }
+
+        // ---- sparse product C = A B ---------------------------------------------
+        __global__ void spgemm_bound(int rows, const int* __restrict__ ap, const int* __restrict__ ac,
+                                     const int* __restrict__ bp, int* __restrict__ out)
+        {
+            int m = 0;
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+            {
+                int n = 0;
+                for (int k = ap[r]; k < ap[r + 1]; ++k)
+                    n += bp[ac[k] + 1] - bp[ac[k]];
+                m = max(m, n);
+            }
+            for (int o = 16; o > 0; o >>= 1)
+                m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0)
+                atomicMax(out, m);
+        }
+
+        struct GemmArgs
+        {
+            int rows;
+            const int *ap, *ac;
+            const double* av;
+            const int *bp, *bc;
+            const double* bv;
+            int* count;
+            const int* cp;
+            int* cc;
+            double* cv;
+        };
+
+        template<int CAP, bool FILL>
+        __global__ void __launch_bounds__(256) spgemm_rows(GemmArgs A)
+        {
+            extern __shared__ unsigned char smem_raw[];
+            const int warps = blockDim.x >> 5;
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
+            double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
+                           (size_t)w * CAP;
+            for (int row = blockIdx.x * warps + w; row < A.rows; row += gridDim.x * warps)
+            {
+                int n = 0, seq = 0;
+                for (int k = A.ap[row]; k < A.ap[row + 1]; ++k)
+                {
+                    const int j = A.ac[k];
+                    const double a = A.av[k];
+                    const int b = A.bp[j], e = A.bp[j + 1];
+                    for (int q = b + lane; q < e; q += 32)
+                    {
+                        const int slot = n + (q - b);
+                        keys[slot] = make_key(A.bc[q], seq + (q - b), slot);
+                        vals[slot] = a * A.bv[q];
+                    }
+                    n += e - b;
+                    seq += e - b;
+                }
+                __syncwarp();
+                const int np = next_pow2(n);
+                for (int k = n + lane; k < np; k += 32)
+                    keys[k] = ~0ull;
+                __syncwarp();
+                warp_bitonic_sort(keys, np);
+                const int base = FILL ? A.cp[row] : 0;
+                int uniq = 0;
+                for (int k0 = 0; k0 < n; k0 += 32)
+                {
+                    const int k = k0 + lane;
+                    bool head = false;
+                    unsigned col = 0;
+                    if (k < n)
+                    {
+                        col = static_cast<unsigned>(keys[k] >> 32);
+                        head = k == 0 || static_cast<unsigned>(keys[k - 1] >> 32) != col;
+                    }
+                    const unsigned hm = __ballot_sync(0xffffffffu, head);
+                    if (FILL && head)
+                    {
+                        double s = 0.0;
+                        for (int q = k; q < n && static_cast<unsigned>(keys[q] >> 32) == col; ++q)
+                            s += vals[keys[q] & ((1u << kSlotBits) - 1)];
+                        const int pos = base + uniq + __popc(hm & ((1u << lane) - 1));
+                        A.cc[pos] = static_cast<int>(col);
+                        A.cv[pos] = s;
+                    }
+                    uniq += __popc(hm);
+                }
+                if (!FILL && lane == 0)
+                    A.count[row] = uniq;
+                __syncwarp();
+            }
+        }
+
+        // ---- transpose -----------------------------------------------------------
+        __global__ void col_count(int nnz, const int* __restrict__ ci, int* __restrict__ cnt)
+        {
+            for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz; k += (long long)gridDim.x * blockDim.x)
+                atomicAdd(&cnt[ci[k]], 1);
+        }
+
+        __global__ void transpose_fill(int rows, const int* __restrict__ rp, const int* __restrict__ ci,
+                                       const double* __restrict__ va, const int* __restrict__ tp, int* __restrict__ cursor,
+                                       int* __restrict__ tc, double* __restrict__ tv)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                {
+                    const int c = ci[k];
+                    const int pos = tp[c] + atomicAdd(&cursor[c], 1);
+                    tc[pos] = r;
+                    tv[pos] = va[k];
+                }
+        }
+
+        // sort every row segment by column (one warp per row; rows up to CAP long)
+        template<int CAP>
+        __global__ void __launch_bounds__(256) sort_rows(int rows, const int* __restrict__ rp, int* __restrict__ ci,
+                                                         double* __restrict__ va)
+        {
+            extern __shared__ unsigned char smem_raw[];
+            const int warps = blockDim.x >> 5;
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
+            double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
+                           (size_t)w * CAP;
+            for (int row = blockIdx.x * warps + w; row < rows; row += gridDim.x * warps)
+            {
+                const int b = rp[row], n = rp[row + 1] - b;
+                for (int k = lane; k < n; k += 32)
+                {
+                    keys[k] = (static_cast<unsigned long long>(static_cast<unsigned>(ci[b + k])) << 32) | (unsigned)k;
+                    vals[k] = va[b + k];
+                }
+                const int np = next_pow2(n);
+                for (int k = n + lane; k < np; k += 32)
+                    keys[k] = ~0ull;
+                __syncwarp();
+                warp_bitonic_sort(keys, np);
+                for (int k = lane; k < n; k += 32)
+                {
+                    ci[b + k] = static_cast<int>(keys[k] >> 32);
+                    va[b + k] = vals[keys[k] & 0xffffffffu];
+                }
+                __syncwarp();
+            }
+        }
+
+        __global__ void max_len_kernel(int n, const int* __restrict__ p, int* __restrict__ out)
+        {
+            int m = 0;
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                m = max(m, p[i + 1] - p[i]);
+            for (int o = 16; o > 0; o >>= 1)
+                m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0)
+                atomicMax(out, m);
+        }
+
+        int read_int(cudaStream_t s, const int* d)
+        {
+            int h = 0;
+            APF_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+            sync(s);
+            return h;
+        }
+
+        template<class F>
+        void with_cap(int n, F&& f)
+        {
+            if (n <= 64) f(std::integral_constant<int, 64>{});
+            else if (n <= 256) f(std::integral_constant<int, 256>{});
+            else if (n <= 1024) f(std::integral_constant<int, 1024>{});
+            else if (n <= 4096) f(std::integral_constant<int, 4096>{});
+            else if (n <= 8192) f(std::integral_constant<int, 8192>{});
+            else throw Error(APF_ERR_CAPACITY, "sparse product: a row has more than 8192 candidate entries");
+        }
+
+        template<int CAP>
+        int warps_for_cap()
+        {
+            return std::max(1, std::min(8, (96 * 1024) / (CAP * 16)));
+        }
+    }
+
+    namespace
+    {
+        template<int MODE>
+        void spmv_dispatch(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, double* y, double alpha,
+                           double beta, const double* dinv = nullptr)
+        {
+            if (A.rows == 0)
+                return;
+            const double avg = static_cast<double>(A.nnz()) / A.rows;
+            const int threads = 256;
+            APF_KERNEL(MODE == 1 ? "residual" : (MODE == 2 ? "jacobi_sweep" : "spmv"), s);
+            auto go = [&](auto g) {
+                constexpr int G = decltype(g)::value;
+                spmv_kernel<G, MODE><<<blocks_for((long long)A.rows * G, threads, 148 * 64), threads, 0, s>>>(
+                    A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(), x, b, y, alpha, beta, dinv);
+            };
+            if (avg <= 6) go(std::integral_constant<int, 4>{});
+            else if (avg <= 14) go(std::integral_constant<int, 8>{});
+            else if (avg <= 40) go(std::integral_constant<int, 16>{});
+            else go(std::integral_constant<int, 32>{});
+            APF_CUDA(cudaGetLastError());
+        }
+    }
+
+    void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha, double beta)
+    {
+        spmv_dispatch<0>(s, A, x, nullptr, y, alpha, beta);
+    }
+
+    void jacobi_sweep(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, const double* dinv,
+                      double omega, double* y)
+    {
+        spmv_dispatch<2>(s, A, x, b, y, omega, 0.0, dinv);
+    }
+
+    void residual(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, double* r)
+    {
+        spmv_dispatch<1>(s, A, x, b, r, 1.0, 0.0);
+    }
+
+    void dot_device(cudaStream_t s, Workspace& w, int n, const double* a, const double* b, double* out)
+    {
+        w.ensure(s);
+        {
+            APF_KERNEL("dot_partials", s);
+            dot_partials<<<kRedBlocks, kRedThreads, 0, s>>>(n, a, b, w.partials.get());
+        }
+        {
+            APF_KERNEL("sum_partials", s);
+            sum_partials<<<1, 256, 0, s>>>(kRedBlocks, w.partials.get(), out);
+        }
+        APF_CUDA(cudaGetLastError());
+    }
+
+    double dot_host(cudaStream_t s, Workspace& w, int n, const double* a, const double* b)
+    {
+        w.ensure(s);
+        dot_device(s, w, n, a, b, w.scalars.get());
+        double h = 0.0;
+        APF_CUDA(cudaMemcpyAsync(&h, w.scalars.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        return h;
+    }
+
+    void axpby(cudaStream_t s, int n, double a, const double* x, double b, double* y)
+    {
+        APF_KERNEL("axpby", s);
+        axpby_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, a, x, b, y);
+    }
+
+    void copy(cudaStream_t s, int n, const double* x, double* y)
+    {
+        if (n)
+            APF_CUDA(cudaMemcpyAsync(y, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    }
+
+    void fill(cudaStream_t s, int n, double v, double* y)
+    {
+        APF_KERNEL("fill", s);
+        fill_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, v, y);
+    }
+
+    void inverse_diagonal(cudaStream_t s, const DeviceCsr& A, DeviceBuffer<double>& inv)
+    {
+        inv.allocate(static_cast<std::size_t>(A.rows), s);
+        APF_KERNEL("inv_diag", s);
+        inv_diag_kernel<<<blocks_for(A.rows, 256), 256, 0, s>>>(A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(),
+                                                                 inv.get());
+    }
+
+    void spgemm(cudaStream_t s, const DeviceCsr& A, const DeviceCsr& B, DeviceCsr& C)
+    {
+        require(A.cols == B.rows, APF_ERR_INVALID, "spgemm: inner dimensions differ");
+        C.rows = A.rows;
+        C.cols = B.cols;
+        C.row_ptr.allocate(static_cast<std::size_t>(A.rows) + 1, s);
+        if (A.rows == 0)
+        {
+            APF_CUDA(cudaMemsetAsync(C.row_ptr.get(), 0, sizeof(int), s));
+            return;
+        }
+        DeviceBuffer<int> bound(1, s);
+        bound.zero();
+        {
+            APF_KERNEL("spgemm_bound", s);
+            spgemm_bound<<<blocks_for(A.rows, 256, 148 * 8), 256, 0, s>>>(A.rows, A.row_ptr.get(), A.col_idx.get(),
+                                                                           B.row_ptr.get(), bound.get());
+        }
+        const int cap = read_int(s, bound.get());
+        DeviceBuffer<int> count(static_cast<std::size_t>(A.rows) + 1, s);
+        GemmArgs g{A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(), B.row_ptr.get(), B.col_idx.get(),
+                   B.values.get(), count.get(), nullptr, nullptr, nullptr};
+        auto launch = [&](auto tag, bool fill_pass) {
+            constexpr int CAP = decltype(tag)::value;
+            const int warps = warps_for_cap<CAP>();
+            const size_t smem = (size_t)warps * CAP * 16;
+            const int blocks = blocks_for(A.rows, warps, 148 * 32);
+            if (fill_pass)
+            {
+                APF_CUDA(cudaFuncSetAttribute(spgemm_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                APF_KERNEL("spgemm_fill", s);
+                spgemm_rows<CAP, true><<<blocks, warps * 32, smem, s>>>(g);
+            }
+            else
+            {
+                APF_CUDA(cudaFuncSetAttribute(spgemm_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                APF_KERNEL("spgemm_count", s);
+                spgemm_rows<CAP, false><<<blocks, warps * 32, smem, s>>>(g);
+            }
+            APF_CUDA(cudaGetLastError());
+        };
+        with_cap(std::max(cap, 1), [&](auto tag) { launch(tag, false); });
+        const long long nnz = exclusive_scan(count.get(), C.row_ptr.get(), A.rows, s);
+        C.col_idx.allocate(static_cast<std::size_t>(nnz), s);
+        C.values.allocate(static_cast<std::size_t>(nnz), s);
+        g.cp = C.row_ptr.get();
+        g.cc = C.col_idx.get();
+        g.cv = C.values.get();
+        with_cap(std::max(cap, 1), [&](auto tag) { launch(tag, true); });
+    }
+
+    void transpose(cudaStream_t s, const DeviceCsr& A, DeviceCsr& T)
+    {
+        T.rows = A.cols;
+        T.cols = A.rows;
+        DeviceBuffer<int> cnt(static_cast<std::size_t>(A.cols) + 1, s);
+        cnt.zero();
+        if (A.nnz())
+        {
+            APF_KERNEL("col_count", s);
+            col_count<<<blocks_for(A.nnz(), 256), 256, 0, s>>>(static_cast<int>(A.nnz()), A.col_idx.get(), cnt.get());
+        }
+        T.row_ptr.allocate(static_cast<std::size_t>(A.cols) + 1, s);
+        const long long nnz = exclusive_scan(cnt.get(), T.row_ptr.get(), A.cols, s);
+        T.col_idx.allocate(static_cast<std::size_t>(nnz), s);
+        T.values.allocate(static_cast<std::size_t>(nnz), s);
+        cnt.zero();
+        if (A.rows)
+        {
+            APF_KERNEL("transpose_fill", s);
+            transpose_fill<<<blocks_for(A.rows, 256), 256, 0, s>>>(A.rows, A.row_ptr.get(), A.col_idx.get(),
+                                                                    A.values.get(), T.row_ptr.get(), cnt.get(),
+                                                                    T.col_idx.get(), T.values.get());
+        }
+        DeviceBuffer<int> mx(1, s);
+        mx.zero();
+        if (T.rows)
+        {
+            APF_KERNEL("max_len", s);
+            max_len_kernel<<<blocks_for(T.rows, 256, 1024), 256, 0, s>>>(T.rows, T.row_ptr.get(), mx.get());
+        }
+        const int longest = read_int(s, mx.get());
+        if (T.rows == 0 || longest <= 1)
+            return;
+        with_cap(longest, [&](auto tag) {
+            constexpr int CAP = decltype(tag)::value;
+            const int warps = warps_for_cap<CAP>();
+            const size_t smem = (size_t)warps * CAP * 16;
+            APF_CUDA(cudaFuncSetAttribute(sort_rows<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            APF_KERNEL("sort_rows", s);
+            sort_rows<CAP><<<blocks_for(T.rows, warps, 148 * 32), warps * 32, smem, s>>>(T.rows, T.row_ptr.get(),
+                                                                                          T.col_idx.get(), T.values.get());
+            APF_CUDA(cudaGetLastError());
+        });
+    }
+}

@@ -1,0 +1,46 @@
+// Sparse/vector building blocks on the device (CSR f64/int32): SpMV, sparse products
+// by per-row gather + warp sort, transposes, deterministic reductions.
+#pragma once
+
+#include "apf_internal.hpp"
+
+namespace apf
+{
+    // Deterministic reductions: fixed grid, per-block partials, fixed-order final sum.
+    constexpr int kRedBlocks = 592; // 4 x 148 SMs
+    constexpr int kRedThreads = 256;
+
+    struct Workspace
+    {
+        DeviceBuffer<double> partials; // kRedBlocks * 4
+        DeviceBuffer<double> scalars;  // scratch device scalars
+        void ensure(cudaStream_t s)
+        {
+            if (!partials.size())
+                partials.allocate(kRedBlocks * 4, s);
+            if (!scalars.size())
+                scalars.allocate(64, s);
+        }
+    };
+
+    // y = alpha * A x + beta * y   (beta == 0 ignores y's old contents)
+    void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0);
+    // y = x + omega * dinv * (b - A x)   (one damped-Jacobi sweep; y must not alias x)
+    void jacobi_sweep(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, const double* dinv,
+                      double omega, double* y);
+    // r = b - A x
+    void residual(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, double* r);
+    // out = dot(a, b) written to a device scalar (deterministic)
+    void dot_device(cudaStream_t s, Workspace& w, int n, const double* a, const double* b, double* out);
+    double dot_host(cudaStream_t s, Workspace& w, int n, const double* a, const double* b);
+    // C = A * B (pattern = all candidate products, duplicates summed in a fixed order)
+    void spgemm(cudaStream_t s, const DeviceCsr& A, const DeviceCsr& B, DeviceCsr& C);
+    // T = A^T (rows sorted)
+    void transpose(cudaStream_t s, const DeviceCsr& A, DeviceCsr& T);
+    // inverse diagonal of a square CSR
+    void inverse_diagonal(cudaStream_t s, const DeviceCsr& A, DeviceBuffer<double>& inv);
+    // vector helpers
+    void axpby(cudaStream_t s, int n, double a, const double* x, double b, double* y); // y = a x + b y
+    void copy(cudaStream_t s, int n, const double* x, double* y);
+    void fill(cudaStream_t s, int n, double v, double* y);
+}

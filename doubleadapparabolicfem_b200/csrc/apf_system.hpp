@@ -5,6 +5,7 @@
 #include <memory>
 
 #include "apf_internal.hpp"
+#include "apf_minres.cuh"
 
 namespace apf
 {
@@ -53,6 +54,12 @@ namespace apf
         bool have[APF_N_BLOCKS] = {};
         DeviceBuffer<double> f, g;
         DeviceBuffer<double> inv_diag_ay;
+        // solve state
+        Workspace ws;
+        std::unique_ptr<BlockPreconditioner> precond;
+        AmgOptions precond_opts{};
+        DeviceBuffer<double> rhs, solution;
+        double precond_setup_seconds = 0.0;
     };
 
     void upload_tables_once(int device);

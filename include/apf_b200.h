@@ -135,6 +135,60 @@ int apf_system_block_device_ptrs(const apf_system* sys, int block, const int32_t
 int apf_system_vector_copy(apf_ctx* ctx, const apf_system* sys, int which, double* out, int to_device);
 void apf_system_destroy(apf_system* sys);
 
+/* ---- block-preconditioned MINRES ------------------------------------------------ */
+#define APF_PRECOND_AMG_BLOCK 0 /* blkdiag(A_y, Hhat), one SA-AMG V-cycle per block */
+#define APF_PRECOND_LEARNED 1   /* learned preconditioner (falls back to APF_PRECOND_AMG_BLOCK) */
+
+/* Mirrors the fields of la::concepts::SolverOptions the MINRES path reads
+ * (src/linear_algebra/concepts/solver.hpp:212-255). */
+typedef struct apf_solver_options
+{
+    double tolerance;                 /* true relative residual target (reference yml: 1e-8) */
+    int max_iterations;               /* reference default 20000 in the runner */
+    int use_true_residual_batching;   /* reference default 1 */
+    int true_residual_check_interval; /* reference default 100 */
+    int preconditioner;               /* APF_PRECOND_* */
+    int amg_smooth_steps;             /* damped-Jacobi sweeps per side of the V-cycle (>= 1) */
+    double amg_strength;              /* strength-of-connection threshold (e.g. 0.08) */
+    int amg_coarse_size;              /* dense coarsest solve at or below this size */
+} apf_solver_options;
+
+/* Mirrors SolverDiagnostics.iterative_stats (src/linear_algebra/concepts/solver.hpp:186-197). */
+typedef struct apf_solver_diagnostics
+{
+    int iterations;
+    int residual_check_batches;
+    int converged;                /* accepted by the FP64 true residual */
+    int backend_converged;
+    double backend_reported_error;
+    double final_true_residual;   /* ||K x - b||_2 / ||b||_2 */
+    double setup_seconds;         /* preconditioner setup */
+    double solve_seconds;
+    int amg_levels_lambda, amg_levels_u;
+    int64_t amg_nnz_lambda, amg_nnz_u;
+} apf_solver_diagnostics;
+
+void apf_solver_options_default(apf_solver_options* opt);
+
+/* Preconditioner setup for the assembled system (requires apf_assemble_graph_norm).
+ * Replaces ParabolicGraphNormBlockPreconditioner::compute_from_graph_norm
+ * (src/linear_algebra/eigen_backend/preconditioners/parabolic_graph_norm_minres.hpp:55-111). */
+int apf_setup_preconditioner(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt);
+
+/* Solve K [lambda; u] = [f; g] by block-preconditioned MINRES with true-residual batches.
+ * Replaces SaddlePreconditionedSolveDispatcher<Backend>::solve ->
+ * solve_minres_with_parabolic_graph_norm
+ * (src/linear_algebra/eigen_backend/preconditioners/solve_saddle_system.hpp:32-121,
+ *  parabolic_graph_norm_minres.hpp:232-369).  Sets up the preconditioner if needed.
+ * initial_guess: NULL (zero start) or n_lambda+n_u values; solution: n_lambda+n_u values
+ * (may be NULL: the solution stays on the device).  Returns APF_ERR_NOT_CONVERGED with
+ * diag filled when the true residual misses the tolerance (the reference throws
+ * PreconditionedSolveFailure, parabolic_graph_norm_minres.hpp:357-366). */
+int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* initial_guess,
+                     double* solution, int pointers_on_device, apf_solver_diagnostics* diag);
+/* Device pointer of the last solution (n_lambda + n_u values, owned by sys). */
+int apf_system_solution_device_ptr(const apf_system* sys, const double** solution);
+
 #ifdef __cplusplus
 }
 #endif
