@@ -18,6 +18,7 @@ Errors raise ``ApfError`` with the library's message (the reference throws
 from __future__ import annotations
 
 import ctypes as C
+import sys
 
 import numpy as np
 
@@ -52,6 +53,9 @@ class Context:
             self.handle = None
 
     def __del__(self):
+        # at interpreter shutdown the process exit releases the device resources
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:
@@ -194,6 +198,8 @@ class MainSystemBlocks:
             self.handle = None
 
     def __del__(self):
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:

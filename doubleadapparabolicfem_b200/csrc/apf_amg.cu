@@ -1,14 +1,19 @@
 // Smoothed-aggregation AMG (see apf_amg.cuh).
 //
-// Setup per level: strength graph |a_ij| >= theta sqrt(a_ii a_jj); aggregates from a
-// distance-1 maximal independent set (hash priorities, deterministic); tentative
-// prolongator T (one 1 per row); P = (I - omega D_F^-1 A_F) T with the filtered
+// Setup per level: strength graph |a_ij| >= theta sqrt(a_ii a_jj) between unknowns of the
+// same component (the time-local index of a Y DOF: the broken-in-time test space makes
+// (1,-1) across the two time sides of a node a lower-energy mode than the constant, so the
+// sides are aggregated separately and each keeps its own constant near-nullspace vector);
+// aggregates from a distance-1 maximal independent set (hash priorities, deterministic);
+// tentative prolongator T (one 1 per row); P = (I - omega D_F^-1 A_F) T with the filtered
 // operator A_F (weak entries lumped onto the diagonal); A_c = P^T A P.  The coarsest
-// operator is inverted densely on the host once per setup.  The V-cycle uses the same
-// number of damped-Jacobi sweeps before and after the coarse correction, so it is
-// symmetric and positive definite.
+// operator is inverted densely on the host once per setup (or, when coarsening stalls
+// above the dense size, smoothed with a fixed number of Jacobi sweeps).  The V-cycle uses
+// the same damped-Jacobi sweeps before and after the coarse correction, so it is a
+// symmetric positive definite linear operator.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "apf_amg.cuh"
@@ -36,55 +41,60 @@ namespace apf
             return hi > hj || (hi == hj && i > j);
         }
 
-        __device__ __forceinline__ double diag_of(const int* rp, const int* ci, const double* va, int r)
+        struct Strength
         {
-            double d = 0.0;
-            for (int k = rp[r]; k < rp[r + 1]; ++k)
-                if (ci[k] == r)
-                    d += va[k];
-            return d;
-        }
+            const double* diag;
+            double theta;
+            const int* comp; // optional component of each unknown
+            __device__ __forceinline__ bool operator()(int i, int j, double v) const
+            {
+                return j != i && (comp == nullptr || comp[i] == comp[j]) &&
+                       fabs(v) >= theta * sqrt(fabs(diag[i] * diag[j]));
+            }
+        };
 
         __global__ void diag_kernel(int n, const int* rp, const int* ci, const double* va, double* d)
         {
             for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
-                d[r] = diag_of(rp, ci, va, r);
+            {
+                double s = 0.0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                    if (ci[k] == r)
+                        s += va[k];
+                d[r] = s;
+            }
         }
 
         enum : int { UNDECIDED = 0, ROOT = 1, OUT = 2 };
 
-        __global__ void mis_init(int n, const int* rp, const int* ci, const double* va, const double* diag, double theta,
-                                 int* state)
+        __global__ void mis_init(int n, const int* rp, const int* ci, const double* va, Strength st, int* state)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             {
                 bool any = false;
                 for (int k = rp[i]; k < rp[i + 1] && !any; ++k)
-                {
-                    const int j = ci[k];
-                    any = j != i && fabs(va[k]) >= theta * sqrt(fabs(diag[i] * diag[j]));
-                }
+                    any = st(i, ci[k], va[k]);
                 state[i] = any ? UNDECIDED : ROOT;
             }
         }
 
-        __global__ void mis_select(int n, const int* rp, const int* ci, const double* va, const double* diag, double theta,
-                                   const int* sin, int* sout, int* undecided)
+        __global__ void mis_select(int n, const int* rp, const int* ci, const double* va, Strength st, const int* sin,
+                                   int* sout, int* undecided)
         {
             int cnt = 0;
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             {
-                const int st = sin[i];
-                if (st != UNDECIDED)
+                const int s0 = sin[i];
+                if (s0 != UNDECIDED)
                 {
-                    sout[i] = st;
+                    sout[i] = s0;
                     continue;
                 }
                 bool is_max = true, has_root = false;
                 for (int k = rp[i]; k < rp[i + 1]; ++k)
                 {
                     const int j = ci[k];
-                    if (j == i || fabs(va[k]) < theta * sqrt(fabs(diag[i] * diag[j])))
+                    if (!st(i, j, va[k]))
                         continue;
                     const int sj = sin[j];
                     if (sj == ROOT)
@@ -109,14 +119,16 @@ namespace apf
         }
 
         // each non-root joins its strongest root neighbour (ties: smallest index)
-        __global__ void assign_aggregates(int n, const int* rp, const int* ci, const double* va, const double* diag,
-                                          double theta, const int* state, const int* root_pos, int* agg, int* status)
+        __global__ void assign_aggregates(int n, const int* rp, const int* ci, const double* va, Strength st,
+                                          const int* state, const int* root_pos, int* agg, int* comp_coarse, int* status)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             {
                 if (state[i] == ROOT)
                 {
                     agg[i] = root_pos[i];
+                    if (comp_coarse)
+                        comp_coarse[root_pos[i]] = st.comp ? st.comp[i] : 0;
                     continue;
                 }
                 int best = -1;
@@ -124,7 +136,7 @@ namespace apf
                 for (int k = rp[i]; k < rp[i + 1]; ++k)
                 {
                     const int j = ci[k];
-                    if (j == i || state[j] != ROOT || fabs(va[k]) < theta * sqrt(fabs(diag[i] * diag[j])))
+                    if (state[j] != ROOT || !st(i, j, va[k]))
                         continue;
                     const double v = fabs(va[k]);
                     if (v > bv || (v == bv && j < best))
@@ -155,36 +167,31 @@ namespace apf
             }
         }
 
-        // M = I - omega D_F^-1 A_F restricted to the strong pattern (+ diagonal)
-        __global__ void filtered_count(int n, const int* rp, const int* ci, const double* va, const double* diag,
-                                       double theta, int* cnt)
+        // M = I - omega D_F^-1 A_F on the strong pattern (+ diagonal)
+        __global__ void filtered_count(int n, const int* rp, const int* ci, const double* va, Strength st, int* cnt)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             {
                 int c = 1;
                 for (int k = rp[i]; k < rp[i + 1]; ++k)
-                {
-                    const int j = ci[k];
-                    if (j != i && fabs(va[k]) >= theta * sqrt(fabs(diag[i] * diag[j])))
-                        ++c;
-                }
+                    c += st(i, ci[k], va[k]);
                 cnt[i] = c;
             }
         }
 
-        __global__ void filtered_fill(int n, const int* rp, const int* ci, const double* va, const double* diag,
-                                      double theta, double omega, const int* mp, int* mc, double* mv)
+        __global__ void filtered_fill(int n, const int* rp, const int* ci, const double* va, Strength st, double omega,
+                                      const int* mp, int* mc, double* mv)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             {
                 double dF = 0.0;
                 for (int k = rp[i]; k < rp[i + 1]; ++k)
-                {
-                    const int j = ci[k];
-                    const bool strong = j != i && fabs(va[k]) >= theta * sqrt(fabs(diag[i] * diag[j]));
-                    if (!strong)
+                    if (!st(i, ci[k], va[k]))
                         dF += va[k]; // diagonal and lumped weak entries
-                }
+                // lumping positive weak couplings can shrink the diagonal; keep it well away from 0
+                const double dii = st.diag[i];
+                if (!(dF >= 0.25 * dii))
+                    dF = dii;
                 const double s = dF != 0.0 ? omega / dF : 0.0;
                 int o = mp[i];
                 bool diag_done = false;
@@ -194,11 +201,11 @@ namespace apf
                     if (!diag_done && j >= i)
                     {
                         mc[o] = i;
-                        mv[o] = 1.0 - s * dF;
+                        mv[o] = 1.0 - omega;
                         ++o;
                         diag_done = true;
                     }
-                    if (j != i && fabs(va[k]) >= theta * sqrt(fabs(diag[i] * diag[j])))
+                    if (st(i, j, va[k]))
                     {
                         mc[o] = j;
                         mv[o] = -s * va[k];
@@ -208,21 +215,9 @@ namespace apf
                 if (!diag_done)
                 {
                     mc[o] = i;
-                    mv[o] = 1.0 - s * dF;
+                    mv[o] = 1.0 - omega;
                 }
             }
-        }
-
-        __global__ void scale_kernel(int n, const double* a, const double* d, double* y)
-        {
-            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-                y[i] = a[i] * d[i];
-        }
-
-        __global__ void init_random(int n, double* x)
-        {
-            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-                x[i] = 0.5 + (hash_u32(static_cast<unsigned>(i) * 2654435761u) & 0xffff) / 65536.0;
         }
 
         __global__ void jacobi_first(int n, const double* b, const double* dinv, double omega, double* x)
@@ -249,6 +244,29 @@ namespace apf
             }
         }
 
+        // Gershgorin bound of rho(D^-1 A): max_i sum_j |a_ij| / a_ii (an upper bound, so the
+        // damped-Jacobi factor 4 / (3 rho) keeps every sweep contractive and the V-cycle SPD)
+        __global__ void gershgorin_kernel(int n, const int* rp, const int* ci, const double* va, unsigned long long* out)
+        {
+            double m = 0.0;
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+            {
+                double d = 0.0, s = 0.0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                {
+                    s += fabs(va[k]);
+                    if (ci[k] == r)
+                        d += va[k];
+                }
+                if (d > 0.0)
+                    m = fmax(m, s / d);
+            }
+            for (int o = 16; o > 0; o >>= 1)
+                m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0)
+                atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m))); // non-negative doubles order like their bits
+        }
+
         int read_int(cudaStream_t s, const int* d)
         {
             int h = 0;
@@ -257,35 +275,26 @@ namespace apf
             return h;
         }
 
-        // rho(D^-1 A) by power iteration
-        double spectral_radius(cudaStream_t s, const DeviceCsr& A, const double* dinv, Workspace& w)
+        double spectral_radius(cudaStream_t s, const DeviceCsr& A)
         {
-            const int n = A.rows;
-            DeviceBuffer<double> x(n, s), y(n, s);
+            DeviceBuffer<unsigned long long> out(1, s);
+            out.zero();
             {
-                APF_KERNEL("amg_init_random", s);
-                init_random<<<nblocks(n, 256), 256, 0, s>>>(n, x.get());
+                APF_KERNEL("amg_gershgorin", s);
+                gershgorin_kernel<<<nblocks(A.rows, 256, 1024), 256, 0, s>>>(A.rows, A.row_ptr.get(), A.col_idx.get(),
+                                                                              A.values.get(), out.get());
             }
-            double lam = 1.0;
-            for (int it = 0; it < 12; ++it)
-            {
-                spmv(s, A, x.get(), y.get());
-                {
-                    APF_KERNEL("amg_scale", s);
-                    scale_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, y.get(), dinv, y.get());
-                }
-                const double yy = dot_host(s, w, n, y.get(), y.get());
-                const double xx = dot_host(s, w, n, x.get(), x.get());
-                lam = std::sqrt(yy / std::max(xx, 1e-300));
-                axpby(s, n, 1.0 / std::sqrt(std::max(yy, 1e-300)), y.get(), 0.0, x.get());
-            }
-            return lam;
+            unsigned long long h = 0;
+            APF_CUDA(cudaMemcpyAsync(&h, out.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+            sync(s);
+            double r;
+            std::memcpy(&r, &h, sizeof(r));
+            return r > 0.0 ? r : 1.0;
         }
 
-        // dense SPD inverse via Cholesky (host, coarsest level only)
+        // dense SPD inverse via Cholesky (host, coarsest level only); a: row-major, overwritten
         void dense_spd_inverse(std::vector<double>& a, int n)
         {
-            // a: row-major n x n, overwritten by its inverse
             std::vector<double> L(a);
             for (int j = 0; j < n; ++j)
             {
@@ -306,7 +315,6 @@ namespace apf
                     L[(size_t)i * n + j] = v / d;
                 }
             }
-            // inverse column by column: solve L L^T x = e_c
             std::vector<double> col(n);
             for (int c = 0; c < n; ++c)
             {
@@ -332,15 +340,21 @@ namespace apf
         }
     }
 
-    void Amg::setup(cudaStream_t s, const DeviceCsr& A, const AmgOptions& opt, Workspace& w)
+    void Amg::setup(cudaStream_t s, const DeviceCsr& A, const AmgOptions& opt, Workspace& w, const int* component)
     {
         opt_ = opt;
         levels_.clear();
         levels_.reserve(static_cast<std::size_t>(opt.max_levels));
         levels_.emplace_back();
         levels_[0].A = &A;
+        if (component)
+        {
+            levels_[0].comp.allocate(static_cast<std::size_t>(A.rows), s);
+            APF_CUDA(cudaMemcpyAsync(levels_[0].comp.get(), component, A.rows * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        }
         w.ensure(s);
-        bool force_dense = false;
+        bool force_dense = false, force_jacobi = false;
+        jacobi_coarse_ = false;
         for (int l = 0;; ++l)
         {
             AmgLevel& L = levels_[static_cast<std::size_t>(l)];
@@ -350,9 +364,20 @@ namespace apf
             L.b.allocate(n, s);
             L.r.allocate(n, s);
             L.t.allocate(n, s);
-            if (force_dense || n <= opt.coarse_size || l + 1 >= opt.max_levels)
+            if (!force_dense && n > opt.coarse_size && l + 1 >= opt.max_levels)
+                force_jacobi = true;
+            if (force_jacobi)
             {
-                // dense inverse of the coarsest operator
+                // coarsest level too large for a dense solve: a fixed number of damped-Jacobi
+                // sweeps from zero (a symmetric positive definite polynomial in D^-1 A)
+                inverse_diagonal(s, Al, L.dinv);
+                L.omega = 4.0 / (3.0 * spectral_radius(s, Al));
+                jacobi_coarse_ = true;
+                n_coarse_ = n;
+                break;
+            }
+            if (force_dense || n <= opt.coarse_size)
+            {
                 std::vector<int> rp(n + 1), ci(Al.nnz());
                 std::vector<double> va(Al.nnz());
                 APF_CUDA(cudaMemcpyAsync(rp.data(), Al.row_ptr.get(), (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -362,7 +387,6 @@ namespace apf
                     APF_CUDA(cudaMemcpyAsync(va.data(), Al.values.get(), Al.nnz() * sizeof(double), cudaMemcpyDeviceToHost, s));
                 }
                 sync(s);
-                require(n <= 6000, APF_ERR_CAPACITY, "AMG: coarsest level too large for the dense solve");
                 std::vector<double> dense((size_t)n * n, 0.0);
                 for (int r = 0; r < n; ++r)
                     for (int k = rp[r]; k < rp[r + 1]; ++k)
@@ -381,29 +405,28 @@ namespace apf
                 APF_KERNEL("amg_diag", s);
                 diag_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), diag.get());
             }
-            const double rho = 1.05 * spectral_radius(s, Al, L.dinv.get(), w);
-            L.omega = 4.0 / (3.0 * rho);
+            L.omega = 4.0 / (3.0 * spectral_radius(s, Al));
+            const Strength st{diag.get(), opt.strength, L.comp.size() ? L.comp.get() : nullptr};
             // aggregation
             DeviceBuffer<int> st0(n, s), st1(n, s), cnt(1, s);
             {
                 APF_KERNEL("amg_mis_init", s);
-                mis_init<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), diag.get(),
-                                                         opt.strength, st0.get());
+                mis_init<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), st, st0.get());
             }
             int* cur = st0.get();
             int* nxt = st1.get();
-            for (int it = 0; it < 200; ++it)
+            for (int it = 0;; ++it)
             {
+                require(it < 200, APF_ERR_INTERNAL, "AMG: independent-set selection did not finish");
                 cnt.zero();
                 {
                     APF_KERNEL("amg_mis_select", s);
-                    mis_select<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(),
-                                                               diag.get(), opt.strength, cur, nxt, cnt.get());
+                    mis_select<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), st,
+                                                               cur, nxt, cnt.get());
                 }
                 std::swap(cur, nxt);
                 if (read_int(s, cnt.get()) == 0)
                     break;
-                require(it < 199, APF_ERR_INTERNAL, "AMG: independent-set selection did not finish");
             }
             DeviceBuffer<int> flag(n + 1, s), pos(n + 1, s), agg(n, s), status(1, s);
             status.zero();
@@ -412,20 +435,26 @@ namespace apf
                 root_flags<<<nblocks(n, 256), 256, 0, s>>>(n, cur, flag.get());
             }
             const int nc = static_cast<int>(exclusive_scan(flag.get(), pos.get(), n, s));
+            if (nc == 0 || nc > (4 * static_cast<long long>(n)) / 5)
             {
-                APF_KERNEL("amg_assign", s);
-                assign_aggregates<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(),
-                                                                  diag.get(), opt.strength, cur, pos.get(), agg.get(),
-                                                                  status.get());
-            }
-            require(read_int(s, status.get()) == 0, APF_ERR_INTERNAL, "AMG: a node has no aggregate");
-            if (nc >= n || nc == 0)
-            {
-                // no coarsening possible: redo this level as the dense coarsest level
-                force_dense = true;
+                // coarsening stalls: this level becomes the coarsest one
+                if (n <= kMaxDense)
+                    force_dense = true;
+                else
+                    force_jacobi = true;
                 --l;
                 continue;
             }
+            DeviceBuffer<int> comp_c;
+            if (st.comp)
+                comp_c.allocate(nc, s);
+            {
+                APF_KERNEL("amg_assign", s);
+                assign_aggregates<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), st,
+                                                                  cur, pos.get(), agg.get(),
+                                                                  st.comp ? comp_c.get() : nullptr, status.get());
+            }
+            require(read_int(s, status.get()) == 0, APF_ERR_INTERNAL, "AMG: a node has no aggregate");
             // tentative prolongator
             DeviceCsr T;
             T.rows = n;
@@ -443,8 +472,8 @@ namespace apf
             DeviceBuffer<int> mcnt(n + 1, s);
             {
                 APF_KERNEL("amg_filtered_count", s);
-                filtered_count<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(),
-                                                               diag.get(), opt.strength, mcnt.get());
+                filtered_count<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), st,
+                                                               mcnt.get());
             }
             M.row_ptr.allocate(n + 1, s);
             const long long mnnz = exclusive_scan(mcnt.get(), M.row_ptr.get(), n, s);
@@ -452,19 +481,38 @@ namespace apf
             M.values.allocate(mnnz, s);
             {
                 APF_KERNEL("amg_filtered_fill", s);
-                filtered_fill<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(),
-                                                              diag.get(), opt.strength, L.omega, M.row_ptr.get(),
-                                                              M.col_idx.get(), M.values.get());
+                filtered_fill<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), st,
+                                                              L.omega, M.row_ptr.get(), M.col_idx.get(), M.values.get());
             }
-            spgemm(s, M, T, L.P);
-            transpose(s, L.P, L.R);
-            DeviceCsr AP;
-            spgemm(s, Al, L.P, AP);
+            DeviceCsr Ac;
+            try
+            {
+                spgemm(s, M, T, L.P);
+                transpose(s, L.P, L.R);
+                DeviceCsr AP;
+                spgemm(s, Al, L.P, AP);
+                spgemm(s, L.R, AP, Ac);
+            }
+            catch (const Error& e)
+            {
+                if (e.code != APF_ERR_CAPACITY)
+                    throw;
+                // the Galerkin product got too dense: stop coarsening at this level
+                L.P = DeviceCsr{};
+                L.R = DeviceCsr{};
+                if (n <= kMaxDense)
+                    force_dense = true;
+                else
+                    force_jacobi = true;
+                --l;
+                continue;
+            }
             levels_.emplace_back();
             AmgLevel& C = levels_.back();
-            AmgLevel& Lr = levels_[levels_.size() - 2];
-            spgemm(s, Lr.R, AP, C.A_own);
+            C.A_own = std::move(Ac);
             C.A = &C.A_own;
+            if (comp_c.size())
+                C.comp = std::move(comp_c);
             sync(s);
         }
     }
@@ -490,22 +538,25 @@ namespace apf
         AmgLevel& L = levels_[static_cast<std::size_t>(l)];
         const DeviceCsr& A = *L.A;
         const int n = A.rows;
-        if (l == static_cast<int>(levels_.size()) - 1)
+        const bool coarsest = l == static_cast<int>(levels_.size()) - 1;
+        if (coarsest && !jacobi_coarse_)
         {
             APF_KERNEL("amg_coarse_solve", s);
             dense_matvec<<<nblocks((long long)n * 32, 256, 1024), 256, 0, s>>>(n, coarse_inv_.get(), b, x);
             return;
         }
-        // pre-smoothing from x = 0
+        const int pre = coarsest ? kCoarseSweeps : opt_.smooth_steps;
         {
             APF_KERNEL("amg_jacobi_first", s);
             jacobi_first<<<nblocks(n, 256), 256, 0, s>>>(n, b, L.dinv.get(), L.omega, x);
         }
-        for (int k = 1; k < opt_.smooth_steps; ++k)
+        for (int k = 1; k < pre; ++k)
         {
             jacobi_sweep(s, A, x, b, L.dinv.get(), L.omega, L.t.get());
             copy(s, n, L.t.get(), x);
         }
+        if (coarsest)
+            return;
         residual(s, A, x, b, L.r.get());
         AmgLevel& C = levels_[static_cast<std::size_t>(l) + 1];
         spmv(s, L.R, L.r.get(), C.b.get());

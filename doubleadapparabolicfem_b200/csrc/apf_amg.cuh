@@ -25,13 +25,17 @@ namespace apf
         DeviceCsr R;                  // restriction = P^T
         DeviceBuffer<double> dinv;    // 1 / diag(A)
         double omega = 0.0;           // Jacobi damping 4 / (3 rho(D^-1 A))
+        DeviceBuffer<int> comp;       // component of each unknown (empty: one component)
         DeviceBuffer<double> x, b, r, t;
     };
 
     class Amg
     {
     public:
-        void setup(cudaStream_t s, const DeviceCsr& A, const AmgOptions& opt, Workspace& w);
+        // component (optional, device, A.rows values): unknowns of different components are
+        // never aggregated together.
+        void setup(cudaStream_t s, const DeviceCsr& A, const AmgOptions& opt, Workspace& w,
+                   const int* component = nullptr);
         // x = V-cycle(b); x and b are device vectors of the finest size.
         void apply(cudaStream_t s, const double* b, double* x);
         int levels() const { return static_cast<int>(levels_.size()); }
@@ -43,6 +47,9 @@ namespace apf
         std::vector<AmgLevel> levels_;
         DeviceBuffer<double> coarse_inv_; // dense inverse of the coarsest operator, row-major
         int n_coarse_ = 0;
+        bool jacobi_coarse_ = false;      // coarsest level smoothed only (too large for a dense solve)
+        static constexpr int kCoarseSweeps = 8;
+        static constexpr int kMaxDense = 1500; // largest coarsest level inverted densely (host O(n^3))
         AmgOptions opt_{};
     };
 }

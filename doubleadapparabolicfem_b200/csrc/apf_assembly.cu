@@ -590,7 +590,7 @@ namespace apf
         //   hpar = setFromTriplets(-C[nz], (1/A_cc * B_ic) * B_jc for B_ic, B_jc != 0)
         //   Hhat = setFromTriplets(hpar[nz], A_x[nz])
         template<int CAP, bool FILL>
-        __global__ void __launch_bounds__(128) hhat_rows(HhatArgs A)
+        __global__ void __launch_bounds__(256) hhat_rows(HhatArgs A)
         {
             extern __shared__ unsigned char smem_raw[];
             const int warps = blockDim.x >> 5;
@@ -1076,6 +1076,41 @@ namespace apf
             if ((threadIdx.x & 31) == 0)
                 atomicMax(out, m);
         }
+    }
+
+    namespace
+    {
+        // time coordinate of every true DOF named by a restriction row, quantized to 2^-20
+        // (dyadic mesh times are exact): DOFs on one time level share a component
+        __global__ void dof_time_component(int rows, int ndof, int p, const double* __restrict__ geo,
+                                           const int* __restrict__ off, const int* __restrict__ dofs,
+                                           int* __restrict__ comp)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+            {
+                const int c = r / ndof, a = (r % ndof) % (p + 1);
+                const double t0 = geo[8ll * c + 6], t1 = geo[8ll * c + 7];
+                const int level = static_cast<int>(llround((t0 + (t1 - t0) * a / p) * 1048576.0));
+                for (int e = off[r]; e < off[r + 1]; ++e)
+                    comp[dofs[e]] = level;
+            }
+        }
+    }
+
+    void dof_time_components(cudaStream_t s, const SystemInputs& in, bool y_space, DeviceBuffer<int>& comp)
+    {
+        const int n = y_space ? in.n_lambda : in.n_u;
+        comp.allocate(static_cast<std::size_t>(n), s);
+        comp.zero();
+        const int rows = (y_space ? in.n_y_cells : in.n_x_cells) * in.ndof;
+        if (rows > 0)
+        {
+            APF_KERNEL("dof_time_component", s);
+            dof_time_component<<<grid_for(rows, 256), 256, 0, s>>>(
+                rows, in.ndof, in.p, y_space ? in.y_geo.get() : in.x_geo.get(), y_space ? in.y_off.get() : in.x_off.get(),
+                y_space ? in.y_dofs.get() : in.x_dofs.get(), comp.get());
+        }
+        APF_CUDA(cudaGetLastError());
     }
 
     void prepare_inputs(cudaStream_t s, SystemInputs& in)

@@ -386,10 +386,16 @@ namespace
         apf::require(S.have[APF_BLOCK_HHAT], APF_ERR_INVALID,
                      "ParabolicGraphNorm requires graph-norm block context from assembly (call apf_assemble_graph_norm)");
         const auto t0 = std::chrono::steady_clock::now();
-        S.precond = std::make_unique<apf::BlockPreconditioner>();
+        S.precond.reset();
+        auto p = std::make_unique<apf::BlockPreconditioner>();
         S.precond_opts = amg_options(opt);
-        S.precond->setup(ctx->stream, S.blocks[APF_BLOCK_A_Y], S.blocks[APF_BLOCK_HHAT], S.precond_opts, S.ws);
+        apf::DeviceBuffer<int> y_comp, x_comp;
+        apf::dof_time_components(ctx->stream, S.in, true, y_comp);
+        apf::dof_time_components(ctx->stream, S.in, false, x_comp);
+        p->setup(ctx->stream, S.blocks[APF_BLOCK_A_Y], S.blocks[APF_BLOCK_HHAT], S.precond_opts, S.ws, y_comp.get(),
+                 x_comp.get());
         apf::sync(ctx->stream);
+        S.precond = std::move(p); // only a fully set-up preconditioner is kept
         S.precond_setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
 }
@@ -465,6 +471,32 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
         rc = APF_ERR_NOT_CONVERGED;
     }
     return rc;
+}
+
+int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const double* r, double* z,
+                             int pointers_on_device)
+{
+    if (!ctx || !sys || !r || !z || block < 0 || block > 2)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        auto& S = sys->sys;
+        apf::require(S.precond != nullptr, APF_ERR_INVALID, "preconditioner has not been set up");
+        cudaStream_t s = ctx->stream;
+        const int nl = S.in.n_lambda, nu = S.in.n_u;
+        const int n = block == 0 ? nl : (block == 1 ? nu : nl + nu);
+        apf::DeviceBuffer<double> dr(n, s), dz(n, s);
+        APF_CUDA(cudaMemcpyAsync(dr.get(), r, n * sizeof(double),
+                                 pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        if (block == 0)
+            S.precond->amg_a.apply(s, dr.get(), dz.get());
+        else if (block == 1)
+            S.precond->amg_h.apply(s, dr.get(), dz.get());
+        else
+            S.precond->apply(s, dr.get(), dz.get());
+        APF_CUDA(cudaMemcpyAsync(z, dz.get(), n * sizeof(double),
+                                 pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+        apf::sync(s);
+    });
 }
 
 int apf_system_solution_device_ptr(const apf_system* sys, const double** solution)

@@ -190,13 +190,108 @@ namespace apf
         }
     }
 
+    namespace
+    {
+        // Hhat_F: drop |h_ij| < tau sqrt(h_ii h_jj) (j != i) and add |h_ij| to h_ii.  Each
+        // dropped pair adds [[|a|,-a],[-a,|a|]] >= 0, so Hhat_F >= Hhat > 0 stays SPD.
+        __global__ void drop_count(int n, const int* rp, const int* ci, const double* va, double tau, int* cnt)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+            {
+                double d = 0.0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                    if (ci[k] == r)
+                        d += va[k];
+                int c = 0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                {
+                    const int j = ci[k];
+                    if (j == r)
+                    {
+                        ++c;
+                        continue;
+                    }
+                    double dj = 0.0;
+                    for (int q = rp[j]; q < rp[j + 1]; ++q)
+                        if (ci[q] == j)
+                            dj += va[q];
+                    c += fabs(va[k]) >= tau * sqrt(fabs(d * dj));
+                }
+                cnt[r] = c;
+            }
+        }
+
+        __global__ void drop_fill(int n, const int* rp, const int* ci, const double* va, double tau, const int* fp,
+                                  int* fc, double* fv)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+            {
+                double d = 0.0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                    if (ci[k] == r)
+                        d += va[k];
+                double lump = 0.0;
+                int o = fp[r], diag_pos = -1;
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                {
+                    const int j = ci[k];
+                    if (j == r)
+                    {
+                        diag_pos = o;
+                        fc[o] = j;
+                        fv[o] = 0.0;
+                        ++o;
+                        continue;
+                    }
+                    double dj = 0.0;
+                    for (int q = rp[j]; q < rp[j + 1]; ++q)
+                        if (ci[q] == j)
+                            dj += va[q];
+                    if (fabs(va[k]) >= tau * sqrt(fabs(d * dj)))
+                    {
+                        fc[o] = j;
+                        fv[o] = va[k];
+                        ++o;
+                    }
+                    else
+                        lump += fabs(va[k]);
+                }
+                if (diag_pos >= 0)
+                    fv[diag_pos] = d + lump;
+            }
+        }
+    }
+
     void BlockPreconditioner::setup(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& Hhat, const AmgOptions& opt,
-                                    Workspace& w)
+                                    Workspace& w, const int* y_component, const int* x_component)
     {
         n_lambda = A_y.rows;
         n_u = Hhat.rows;
-        amg_a.setup(s, A_y, opt, w);
-        amg_h.setup(s, Hhat, opt, w);
+        amg_a.setup(s, A_y, opt, w, y_component);
+        // Hhat carries many couplings far below its diagonal scale (products of the
+        // time-derivative columns that nearly cancel); the hierarchy is built on the
+        // SPD filtered operator Hhat_F >= Hhat
+        const int n = Hhat.rows;
+        DeviceBuffer<int> cnt(static_cast<std::size_t>(n) + 1, s);
+        const int blocks = static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 32)));
+        if (n > 0)
+        {
+            APF_KERNEL("hhat_drop_count", s);
+            drop_count<<<blocks, 256, 0, s>>>(n, Hhat.row_ptr.get(), Hhat.col_idx.get(), Hhat.values.get(), kHhatDrop,
+                                             cnt.get());
+        }
+        hhat_f.rows = hhat_f.cols = n;
+        hhat_f.row_ptr.allocate(static_cast<std::size_t>(n) + 1, s);
+        const long long nnz = exclusive_scan(cnt.get(), hhat_f.row_ptr.get(), n, s);
+        hhat_f.col_idx.allocate(static_cast<std::size_t>(nnz), s);
+        hhat_f.values.allocate(static_cast<std::size_t>(nnz), s);
+        if (n > 0)
+        {
+            APF_KERNEL("hhat_drop_fill", s);
+            drop_fill<<<blocks, 256, 0, s>>>(n, Hhat.row_ptr.get(), Hhat.col_idx.get(), Hhat.values.get(), kHhatDrop,
+                                            hhat_f.row_ptr.get(), hhat_f.col_idx.get(), hhat_f.values.get());
+        }
+        amg_h.setup(s, hhat_f, opt, w, x_component);
     }
 
     void BlockPreconditioner::apply(cudaStream_t s, const double* r, double* z)
@@ -282,7 +377,7 @@ namespace apf
                             APF_KERNEL("minres_vscale", s);
                             k_vscale<<<nb(n), kThreads, 0, s>>>(n, z.get(), v.get(), S.get());
                         }
-                        spmv(s, K, v.get(), py);
+                        spmv(s, K, v.get(), py, 1.0, 0.0, "minres_spmv_K");
                         {
                             APF_KERNEL("minres_t1", s);
                             k_t1<<<kRedBlocks, kThreads, 0, s>>>(n, py, pr1, v.get(), S.get(), first, parts.get());

@@ -17,10 +17,14 @@ namespace apf
     class BlockPreconditioner : public Preconditioner
     {
     public:
-        void setup(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& Hhat, const AmgOptions& opt, Workspace& w);
+        // y_component / x_component: time level of every Y / X DOF (device) or null
+        void setup(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& Hhat, const AmgOptions& opt, Workspace& w,
+                   const int* y_component = nullptr, const int* x_component = nullptr);
         void apply(cudaStream_t s, const double* r, double* z) override;
         int n_lambda = 0, n_u = 0;
         Amg amg_a, amg_h;
+        DeviceCsr hhat_f; // filtered SPD operator the Hhat hierarchy is built on
+        static constexpr double kHhatDrop = 0.01;
     };
 
     struct MinresOptions

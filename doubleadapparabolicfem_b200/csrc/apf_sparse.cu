@@ -307,13 +307,13 @@ namespace apf
     {
         template<int MODE>
         void spmv_dispatch(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, double* y, double alpha,
-                           double beta, const double* dinv = nullptr)
+                           double beta, const double* dinv = nullptr, const char* name = nullptr)
         {
             if (A.rows == 0)
                 return;
             const double avg = static_cast<double>(A.nnz()) / A.rows;
             const int threads = 256;
-            APF_KERNEL(MODE == 1 ? "residual" : (MODE == 2 ? "jacobi_sweep" : "spmv"), s);
+            APF_KERNEL(name ? name : (MODE == 1 ? "residual" : (MODE == 2 ? "jacobi_sweep" : "spmv")), s);
             auto go = [&](auto g) {
                 constexpr int G = decltype(g)::value;
                 spmv_kernel<G, MODE><<<blocks_for((long long)A.rows * G, threads, 148 * 64), threads, 0, s>>>(
@@ -327,9 +327,9 @@ namespace apf
         }
     }
 
-    void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha, double beta)
+    void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha, double beta, const char* name)
     {
-        spmv_dispatch<0>(s, A, x, nullptr, y, alpha, beta);
+        spmv_dispatch<0>(s, A, x, nullptr, y, alpha, beta, nullptr, name);
     }
 
     void jacobi_sweep(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, const double* dinv,

@@ -24,7 +24,8 @@ namespace apf
     };
 
     // y = alpha * A x + beta * y   (beta == 0 ignores y's old contents)
-    void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0);
+    void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0,
+              const char* name = nullptr);
     // y = x + omega * dinv * (b - A x)   (one damped-Jacobi sweep; y must not alias x)
     void jacobi_sweep(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, const double* dinv,
                       double omega, double* y);

@@ -63,6 +63,9 @@ namespace apf
     };
 
     void upload_tables_once(int device);
+    // quantized time coordinate of every Y (y_space) or X DOF: the AMG coarsens each time
+    // level separately (its low-energy modes are arbitrary in time, smooth in space)
+    void dof_time_components(cudaStream_t s, const SystemInputs& in, bool y_space, DeviceBuffer<int>& comp);
     void prepare_inputs(cudaStream_t s, SystemInputs& in);
     Incidence build_incidence(cudaStream_t s, int n_dofs, int n_asm, const int* cell_list, const int* src_map,
                               const int* offsets, const int* dofs, int ndof);

@@ -87,3 +87,11 @@ def split_solution(blocks: MainSystemBlocks, x: np.ndarray):
     """[lambda; u] -> (lambda, u) (solve_main_system.hpp: update_from_true_solution)."""
     nl = blocks.n_lambda()
     return x[:nl], x[nl:]
+
+
+def preconditioner_apply(blocks: MainSystemBlocks, r: np.ndarray, block: int = 2) -> np.ndarray:
+    """z = P^{-1} r with the set-up preconditioner (block 0: A_y part, 1: Hhat part, 2: full)."""
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    z = np.empty_like(r)
+    blocks.ctx.check(blocks.ctx.lib.apf_preconditioner_apply(blocks.ctx.handle, blocks.handle, block, _ptr(r), _ptr(z), 0))
+    return z

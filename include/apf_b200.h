@@ -186,6 +186,11 @@ int apf_setup_preconditioner(apf_ctx* ctx, apf_system* sys, const apf_solver_opt
  * PreconditionedSolveFailure, parabolic_graph_norm_minres.hpp:357-366). */
 int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* initial_guess,
                      double* solution, int pointers_on_device, apf_solver_diagnostics* diag);
+/* z = P^{-1} r with the set-up preconditioner: block 0 = A_y part (n_lambda values),
+ * 1 = Hhat part (n_u values), 2 = the full block operator (n_lambda + n_u).  For tests
+ * and diagnostics (symmetry, PCG quality) of the preconditioner. */
+int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const double* r, double* z,
+                             int pointers_on_device);
 /* Device pointer of the last solution (n_lambda + n_u values, owned by sys). */
 int apf_system_solution_device_ptr(const apf_system* sys, const double** solution);
 
