@@ -144,3 +144,21 @@ def check(ctx, rc: int):
         lib = load()
         msg = lib.apf_ctx_last_error(ctx).decode() if ctx else ""
         raise ApfError(rc, msg)
+
+
+class EstimatorResult(C.Structure):
+    _fields_ = [
+        ("flux_squared", C.c_double),
+        ("divergence_squared", C.c_double),
+        ("reconstruction_squared", C.c_double),
+        ("eta_squared", C.c_double),
+        ("n_slabs", C.c_int),
+        ("n_patches", C.c_int),
+        ("max_patch_cells", C.c_int),
+        ("reconstruction_iterations", C.c_int),
+        ("reconstruction_residual", C.c_double),
+    ]
+
+
+SIGNATURES["apf_estimate"] = ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.POINTER(EstimatorResult)], C.c_int)

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "apf_internal.hpp"
+#include "apf_estimator.cuh"
 #include "apf_system.hpp"
 
 struct apf_ctx
@@ -496,6 +497,37 @@ int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const dou
         APF_CUDA(cudaMemcpyAsync(z, dz.get(), n * sizeof(double),
                                  pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
         apf::sync(s);
+    });
+}
+
+int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int pointers_on_device,
+                 double* flux_squared, double* divergence_squared, double* reconstruction_squared, double* eta_squared,
+                 apf_estimator_result* result)
+{
+    if (!ctx || !sys || !y_vertex_ids)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        auto& S = sys->sys;
+        const std::size_t n = 3ull * static_cast<std::size_t>(S.in.n_y_cells);
+        std::vector<int> vids(n);
+        if (n)
+            APF_CUDA(cudaMemcpyAsync(vids.data(), y_vertex_ids, n * sizeof(int),
+                                     pointers_on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, ctx->stream));
+        apf::sync(ctx->stream);
+        const apf::EstimatorTotals t = apf::estimate_p1(ctx->stream, S, vids, flux_squared, divergence_squared,
+                                                        reconstruction_squared, eta_squared, pointers_on_device != 0);
+        if (result)
+        {
+            result->flux_squared = t.flux;
+            result->divergence_squared = t.div;
+            result->reconstruction_squared = t.recon;
+            result->eta_squared = t.eta;
+            result->n_slabs = t.n_slabs;
+            result->n_patches = t.n_patches;
+            result->max_patch_cells = t.max_patch_cells;
+            result->reconstruction_iterations = t.recon_iterations;
+            result->reconstruction_residual = t.recon_residual;
+        }
     });
 }
 

@@ -1,0 +1,993 @@
+// Equilibrated-flux estimator of one inner iteration (p = 1) on the device.
+//
+// The reference computes, per time slab n and spatial vertex a, the mixed RT_1 x P_1
+// problem on the vertex patch omega_a (time_slab_equilibrated_flux_reconstruction.hpp,
+// dense_local_error_blocks_2d.hpp, vec_f_2d.hpp:27-80, vec_g_2d.hpp:30-95):
+//   (M^-1 sigma, tau) + (div tau, r)      = -(psi_a grad theta~, tau)
+//   (div sigma, q)          + (mu, E q)   =  (psi_a (l - d_t u) - grad psi_a . M grad theta~, q)
+//   E r = 0   (one mean-zero row per time DOF, interior patches only)
+// with theta~ = lambda~ + u, flux RT_1(omega_a) x P_1(slab) with zero normal flux on the
+// patch boundary except on the physical boundary of boundary patches, and broken P_1 x P_1
+// scalars; then sigma = sum_a sigma_a and per slab cell K
+//   flux^2_K = ||M^-1/2 (sigma + M grad theta~)||^2_K,  div^2_K = ||l - d_t u - div sigma||^2_K.
+//
+// B200 design: the space-time patch operator is Mt (x) [A_x B_x^T 0; B_x 0 e^T; 0 e 0] for
+// cell-constant M on a slab, so after multiplying the right-hand side by Mt^-1 the problem
+// splits into one spatial system per time DOF sharing one matrix: a thread block assembles
+// that matrix (size ~ 7 x patch valence) in shared memory, factors it once (LU with
+// partial pivoting) and solves both time components.  Each patch writes its flux restricted
+// to each of its cells into the cell's slot of that patch's vertex (3 slots per triangle),
+// so the per-cell indicator kernel sums the slots in a fixed order: no atomics.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <unordered_map>
+#include <vector>
+
+#include "apf_estimator.cuh"
+
+namespace apf
+{
+    namespace
+    {
+        // reference RT_1 basis (8 functions) over the vector monomials
+        // (1,0) (x,0) (y,0) (0,1) (0,x) (0,y) (x^2,xy) (xy,y^2); DOFs: edge k (opposite vertex
+        // k, from v_{k+1} to v_{k+2}) moments with q = 1 and q = 2s-1 against the outward
+        // normal, then the two interior moments int sigma_x, int sigma_y.
+        struct EstTables
+        {
+            double rt[8][8];
+            int nq;
+            double qp[16][2];
+            double qw[16];
+            double tg[2];
+            double tw[2];
+        };
+        __constant__ EstTables c_est;
+
+        void mono(double x, double y, double v[8][2])
+        {
+            const double m[8][2] = {{1, 0}, {x, 0}, {y, 0}, {0, 1}, {0, x}, {0, y}, {x * x, x * y}, {x * y, y * y}};
+            std::memcpy(v, m, sizeof(m));
+        }
+
+        void solve_dense_host(std::vector<double> a, int n, std::vector<double>& inv)
+        {
+            // Gauss-Jordan with partial pivoting: inv = a^-1 (row-major)
+            inv.assign(static_cast<std::size_t>(n) * n, 0.0);
+            for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+            for (int k = 0; k < n; ++k)
+            {
+                int p = k;
+                for (int i = k + 1; i < n; ++i)
+                    if (std::fabs(a[(size_t)i * n + k]) > std::fabs(a[(size_t)p * n + k])) p = i;
+                for (int j = 0; j < n; ++j)
+                {
+                    std::swap(a[(size_t)k * n + j], a[(size_t)p * n + j]);
+                    std::swap(inv[(size_t)k * n + j], inv[(size_t)p * n + j]);
+                }
+                const double d = a[(size_t)k * n + k];
+                for (int j = 0; j < n; ++j)
+                {
+                    a[(size_t)k * n + j] /= d;
+                    inv[(size_t)k * n + j] /= d;
+                }
+                for (int i = 0; i < n; ++i)
+                {
+                    if (i == k) continue;
+                    const double f = a[(size_t)i * n + k];
+                    if (f == 0.0) continue;
+                    for (int j = 0; j < n; ++j)
+                    {
+                        a[(size_t)i * n + j] -= f * a[(size_t)k * n + j];
+                        inv[(size_t)i * n + j] -= f * inv[(size_t)k * n + j];
+                    }
+                }
+            }
+        }
+
+        EstTables make_est_tables()
+        {
+            EstTables t{};
+            // Gauss-Legendre on [0,1], 4 points -> Duffy rule of degree 5 (16 points)
+            const double g4x[4] = {0.06943184420297371, 0.33000947820757187, 0.6699905217924281, 0.9305681557970263};
+            const double g4w[4] = {0.17392742256872692, 0.3260725774312731, 0.3260725774312731, 0.17392742256872692};
+            t.nq = 16;
+            int k = 0;
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j)
+                {
+                    t.qp[k][0] = g4x[i];
+                    t.qp[k][1] = (1.0 - g4x[i]) * g4x[j];
+                    t.qw[k] = g4w[i] * g4w[j] * (1.0 - g4x[i]);
+                    ++k;
+                }
+            t.tg[0] = 0.5 - 0.5 / std::sqrt(3.0);
+            t.tg[1] = 0.5 + 0.5 / std::sqrt(3.0);
+            t.tw[0] = t.tw[1] = 0.5;
+            // DOF matrix D[dof][monomial]
+            const double v[3][2] = {{0, 0}, {1, 0}, {0, 1}};
+            std::vector<double> D(64, 0.0);
+            for (int e = 0; e < 3; ++e)
+            {
+                const double* P = v[(e + 1) % 3];
+                const double* Q = v[(e + 2) % 3];
+                const double dx = Q[0] - P[0], dy = Q[1] - P[1];
+                const double nrm[2] = {dy, -dx}; // outward (reference triangle is counter-clockwise) x edge length
+                for (int g = 0; g < 4; ++g)
+                {
+                    const double s = g4x[g];
+                    double m[8][2];
+                    mono(P[0] + s * dx, P[1] + s * dy, m);
+                    for (int mm = 0; mm < 8; ++mm)
+                    {
+                        const double fn = m[mm][0] * nrm[0] + m[mm][1] * nrm[1];
+                        D[(2 * e + 0) * 8 + mm] += g4w[g] * fn;
+                        D[(2 * e + 1) * 8 + mm] += g4w[g] * fn * (2.0 * s - 1.0);
+                    }
+                }
+            }
+            for (int q = 0; q < 16; ++q)
+            {
+                double m[8][2];
+                mono(t.qp[q][0], t.qp[q][1], m);
+                for (int mm = 0; mm < 8; ++mm)
+                {
+                    D[6 * 8 + mm] += t.qw[q] * m[mm][0];
+                    D[7 * 8 + mm] += t.qw[q] * m[mm][1];
+                }
+            }
+            // basis coefficients C with D C^T = I  ->  C^T = D^-1
+            std::vector<double> Dinv;
+            solve_dense_host(D, 8, Dinv);
+            for (int j = 0; j < 8; ++j)
+                for (int mm = 0; mm < 8; ++mm)
+                    t.rt[j][mm] = Dinv[(size_t)mm * 8 + j];
+            return t;
+        }
+
+        __device__ __forceinline__ void rt_ref(int j, double x, double y, double& vx, double& vy, double& dv)
+        {
+            const double* c = c_est.rt[j];
+            vx = c[0] + c[1] * x + c[2] * y + c[6] * x * x + c[7] * x * y;
+            vy = c[3] + c[4] * x + c[5] * y + c[6] * x * y + c[7] * y * y;
+            dv = c[1] + c[5] + 3.0 * c[6] * x + 3.0 * c[7] * y;
+        }
+
+        struct Cell
+        {
+            double x0, y0, J00, J01, J10, J11, det, t0, ht;
+            double g[3][2]; // gradients of the barycentric functions
+            double m00, m01, m11, mi00, mi01, mi11;
+            double ell;
+        };
+
+        __device__ Cell load_cell(const double* geo, const double* m, const double* ell, int c)
+        {
+            Cell k;
+            const double* g = geo + 8ll * c;
+            k.x0 = g[0]; k.y0 = g[1];
+            k.J00 = g[2] - g[0]; k.J10 = g[3] - g[1];
+            k.J01 = g[4] - g[0]; k.J11 = g[5] - g[1];
+            k.det = k.J00 * k.J11 - k.J01 * k.J10;
+            k.t0 = g[6]; k.ht = g[7] - g[6];
+            const double id = 1.0 / k.det;
+            // grad lambda_1 = first row of J^-1, grad lambda_2 = second row
+            k.g[1][0] = k.J11 * id;  k.g[1][1] = -k.J01 * id;
+            k.g[2][0] = -k.J10 * id; k.g[2][1] = k.J00 * id;
+            k.g[0][0] = -k.g[1][0] - k.g[2][0];
+            k.g[0][1] = -k.g[1][1] - k.g[2][1];
+            k.m00 = 1.0; k.m01 = 0.0; k.m11 = 1.0;
+            if (m)
+            {
+                k.m00 = m[3ll * c]; k.m01 = m[3ll * c + 1]; k.m11 = m[3ll * c + 2];
+            }
+            const double md = k.m00 * k.m11 - k.m01 * k.m01;
+            k.mi00 = k.m11 / md; k.mi01 = -k.m01 / md; k.mi11 = k.m00 / md;
+            k.ell = ell ? ell[c] : 0.0;
+            return k;
+        }
+
+        // physical basis value / divergence at reference point; edge functions carry sign(detJ)
+        __device__ __forceinline__ void rt_phys(const Cell& k, int j, double x, double y, double& vx, double& vy, double& dv)
+        {
+            double rx, ry, rd;
+            rt_ref(j, x, y, rx, ry, rd);
+            const double s = (j < 6 && k.det < 0.0) ? -1.0 : 1.0;
+            const double f = s / k.det;
+            vx = f * (k.J00 * rx + k.J01 * ry);
+            vy = f * (k.J10 * rx + k.J11 * ry);
+            dv = f * rd;
+        }
+
+        struct PatchArgs
+        {
+            int n_patches;
+            const int* patch_slab;
+            const int* patch_topo;
+            const int* topo_ptr;       // patch cells of each topology patch
+            const int* topo_cell;      // local cell index in the slab cell list
+            const int* topo_center;    // local vertex index of the patch vertex in that cell
+            const int* topo_edge;      // per patch cell x 3: free patch edge id (-1: constrained) | sign_p bit 30
+            const int* topo_nfree;
+            const int* topo_boundary;
+            const int* slab_ptr;
+            const int* slab_cells;
+            const double* geo;
+            const double* m;
+            const double* ell;
+            const double* theta;       // [cell][6] nodal lambda~ + u
+            const double* u;           // [cell][6] nodal u
+            double* sigma;             // [cell][3 slots][2 time][8]
+            int nmax;
+            int* status;
+        };
+
+        // one thread block per patch
+        template<int NMAX>
+        __global__ void __launch_bounds__(128) patch_solve(PatchArgs A)
+        {
+            extern __shared__ double sm[];
+            double* K = sm;                         // NMAX x (NMAX + 2) augmented, row-major
+            const int LD = NMAX + 2;
+            __shared__ int s_piv;
+            __shared__ double s_pv[128];
+            __shared__ int s_pi[128];
+            const int tid = threadIdx.x;
+            for (int p = blockIdx.x; p < A.n_patches; p += gridDim.x)
+            {
+                const int slab = A.patch_slab[p], tp = A.patch_topo[p];
+                const int cb = A.topo_ptr[tp], ce = A.topo_ptr[tp + 1], nc = ce - cb;
+                const int nfree = A.topo_nfree[tp];
+                const bool interior = A.topo_boundary[tp] == 0;
+                const int nf = 2 * nfree + 2 * nc, ns = 3 * nc;
+                const int n = nf + ns + (interior ? 1 : 0);
+                if (n > NMAX)
+                {
+                    if (tid == 0)
+                        atomicExch(A.status, APF_ERR_CAPACITY);
+                    continue;
+                }
+                for (int i = tid; i < NMAX * LD; i += blockDim.x)
+                    K[i] = 0.0;
+                __syncthreads();
+                for (int ic = 0; ic < nc; ++ic)
+                {
+                    const int c = A.slab_cells[A.slab_ptr[slab] + A.topo_cell[cb + ic]];
+                    const int a = A.topo_center[cb + ic];
+                    const Cell k = load_cell(A.geo, A.m, A.ell, c);
+                    // local dof -> (patch dof, coefficient)
+                    int pd[8];
+                    double cf[8];
+                    const double sdet = k.det < 0.0 ? -1.0 : 1.0;
+                    for (int e = 0; e < 3; ++e)
+                    {
+                        const int code = A.topo_edge[3 * (cb + ic) + e];
+                        const int pe = code & 0xffff;
+                        const double sp = (code >> 30) & 1 ? -1.0 : 1.0;
+                        const bool free_edge = pe != 0xffff;
+                        const double sn = sdet * sp;
+                        pd[2 * e] = free_edge ? 2 * pe : -1;
+                        pd[2 * e + 1] = free_edge ? 2 * pe + 1 : -1;
+                        cf[2 * e] = sn;
+                        cf[2 * e + 1] = sn * sp;
+                    }
+                    pd[6] = 2 * nfree + 2 * ic;
+                    pd[7] = 2 * nfree + 2 * ic + 1;
+                    cf[6] = cf[7] = 1.0;
+                    const int sbase = nf + 3 * ic;
+                    // theta~ in time: W_s[k] = sum_b c_{s,b} ht Mtr[b][k]
+                    const double* th = A.theta + 6ll * c;
+                    const double* uu = A.u + 6ll * c;
+                    double gth[2][2]; // grad theta~ weighted against time basis k
+                    for (int kk = 0; kk < 2; ++kk)
+                    {
+                        gth[kk][0] = gth[kk][1] = 0.0;
+                        for (int s = 0; s < 3; ++s)
+                        {
+                            const double W = k.ht * ((kk == 0 ? 1.0 / 3.0 : 1.0 / 6.0) * th[2 * s] +
+                                                     (kk == 0 ? 1.0 / 6.0 : 1.0 / 3.0) * th[2 * s + 1]);
+                            gth[kk][0] += k.g[s][0] * W;
+                            gth[kk][1] += k.g[s][1] * W;
+                        }
+                    }
+                    double du[3];
+                    for (int s = 0; s < 3; ++s)
+                        du[s] = (uu[2 * s + 1] - uu[2 * s]) / k.ht;
+                    const double adet = fabs(k.det);
+                    // entries: A_loc (64) + B_loc (24) + F_loc (16) + G_loc (6) + E (3)
+                    for (int t = tid; t < 113; t += blockDim.x)
+                    {
+                        if (t < 64)
+                        {
+                            const int j = t / 8, l = t % 8;
+                            if (pd[j] < 0 || pd[l] < 0)
+                                continue;
+                            double acc = 0.0;
+                            for (int q = 0; q < c_est.nq; ++q)
+                            {
+                                double ax, ay, ad, bx, by, bd;
+                                rt_phys(k, j, c_est.qp[q][0], c_est.qp[q][1], ax, ay, ad);
+                                rt_phys(k, l, c_est.qp[q][0], c_est.qp[q][1], bx, by, bd);
+                                acc += c_est.qw[q] * (ax * (k.mi00 * bx + k.mi01 * by) + ay * (k.mi01 * bx + k.mi11 * by));
+                            }
+                            K[pd[j] * LD + pd[l]] += cf[j] * cf[l] * acc * adet;
+                        }
+                        else if (t < 88)
+                        {
+                            const int r = (t - 64) / 8, l = (t - 64) % 8;
+                            if (pd[l] < 0)
+                                continue;
+                            double acc = 0.0;
+                            for (int q = 0; q < c_est.nq; ++q)
+                            {
+                                double bx, by, bd;
+                                rt_phys(k, l, c_est.qp[q][0], c_est.qp[q][1], bx, by, bd);
+                                const double x = c_est.qp[q][0], y = c_est.qp[q][1];
+                                const double lam = r == 0 ? 1.0 - x - y : (r == 1 ? x : y);
+                                acc += c_est.qw[q] * bd * lam;
+                            }
+                            const double v = cf[l] * acc * adet;
+                            K[(sbase + r) * LD + pd[l]] += v;
+                            K[pd[l] * LD + sbase + r] += v;
+                        }
+                        else if (t < 104)
+                        {
+                            const int j = (t - 88) / 2, kk = (t - 88) % 2;
+                            if (pd[j] < 0)
+                                continue;
+                            double acc = 0.0;
+                            for (int q = 0; q < c_est.nq; ++q)
+                            {
+                                double ax, ay, ad;
+                                rt_phys(k, j, c_est.qp[q][0], c_est.qp[q][1], ax, ay, ad);
+                                const double x = c_est.qp[q][0], y = c_est.qp[q][1];
+                                const double psi = a == 0 ? 1.0 - x - y : (a == 1 ? x : y);
+                                acc += c_est.qw[q] * psi * (gth[kk][0] * ax + gth[kk][1] * ay);
+                            }
+                            K[pd[j] * LD + NMAX + kk] += -cf[j] * acc * adet;
+                        }
+                        else if (t < 110)
+                        {
+                            const int r = (t - 104) / 2, kk = (t - 104) % 2;
+                            double acc = 0.0, lam_int = 0.0;
+                            for (int q = 0; q < c_est.nq; ++q)
+                            {
+                                const double x = c_est.qp[q][0], y = c_est.qp[q][1];
+                                const double l3[3] = {1.0 - x - y, x, y};
+                                const double dtu = l3[0] * du[0] + l3[1] * du[1] + l3[2] * du[2];
+                                acc += c_est.qw[q] * l3[a] * (k.ell - dtu) * l3[r];
+                                lam_int += c_est.qw[q] * l3[r];
+                            }
+                            // grad psi_a . M grad theta~_k
+                            const double mg0 = k.m00 * gth[kk][0] + k.m01 * gth[kk][1];
+                            const double mg1 = k.m01 * gth[kk][0] + k.m11 * gth[kk][1];
+                            const double gpm = k.g[a][0] * mg0 + k.g[a][1] * mg1;
+                            K[(sbase + r) * LD + NMAX + kk] += (0.5 * k.ht * acc - gpm * lam_int) * adet;
+                        }
+                        else if (interior && t < 113)
+                        {
+                            const int r = t - 110;
+                            // mean-zero row: int_K lambda_r = |K| / 3
+                            const double v = adet / 6.0;
+                            K[(n - 1) * LD + sbase + r] += v;
+                            K[(sbase + r) * LD + n - 1] += v;
+                        }
+                    }
+                    __syncthreads();
+                }
+                // right-hand sides times Mt^-1 (Mt = ht [[1/3,1/6],[1/6,1/3]], inverse (1/ht) [[4,-2],[-2,4]])
+                {
+                    const int c0 = A.slab_cells[A.slab_ptr[slab] + A.topo_cell[cb]];
+                    const double ht = A.geo[8ll * c0 + 7] - A.geo[8ll * c0 + 6];
+                    for (int i = tid; i < n; i += blockDim.x)
+                    {
+                        const double b0 = K[i * LD + NMAX], b1 = K[i * LD + NMAX + 1];
+                        K[i * LD + NMAX] = (4.0 * b0 - 2.0 * b1) / ht;
+                        K[i * LD + NMAX + 1] = (-2.0 * b0 + 4.0 * b1) / ht;
+                    }
+                }
+                __syncthreads();
+                // LU with partial pivoting on the augmented n x (n+2) system
+                bool singular = false;
+                for (int col = 0; col < n; ++col)
+                {
+                    double best = -1.0;
+                    int bi = col;
+                    for (int i = col + tid; i < n; i += blockDim.x)
+                    {
+                        const double v = fabs(K[i * LD + col]);
+                        if (v > best) { best = v; bi = i; }
+                    }
+                    s_pv[tid] = best;
+                    s_pi[tid] = bi;
+                    __syncthreads();
+                    if (tid == 0)
+                    {
+                        double bv = -1.0;
+                        int b = col;
+                        for (int t = 0; t < (int)blockDim.x; ++t)
+                            if (s_pv[t] > bv || (s_pv[t] == bv && s_pi[t] < b)) { bv = s_pv[t]; b = s_pi[t]; }
+                        s_piv = b;
+                    }
+                    __syncthreads();
+                    const int pr = s_piv;
+                    if (pr != col)
+                    {
+                        for (int j = tid; j < n; j += blockDim.x)
+                        {
+                            const double t0 = K[col * LD + j];
+                            K[col * LD + j] = K[pr * LD + j];
+                            K[pr * LD + j] = t0;
+                        }
+                        if (tid < 2)
+                        {
+                            const double t0 = K[col * LD + NMAX + tid];
+                            K[col * LD + NMAX + tid] = K[pr * LD + NMAX + tid];
+                            K[pr * LD + NMAX + tid] = t0;
+                        }
+                    }
+                    __syncthreads();
+                    const double d = K[col * LD + col];
+                    if (!(d != 0.0) || !isfinite(d))
+                    {
+                        singular = true;
+                        break;
+                    }
+                    const int rem = n - col - 1;
+                    for (int i = tid; i < rem; i += blockDim.x)
+                        K[(col + 1 + i) * LD + col] /= d;
+                    __syncthreads();
+                    const int w = rem + 2;
+                    for (int t = tid; t < rem * w; t += blockDim.x)
+                    {
+                        const int i = col + 1 + t / w, jj = t % w;
+                        const int j = jj < rem ? col + 1 + jj : NMAX + (jj - rem);
+                        K[i * LD + j] -= K[i * LD + col] * K[col * LD + j];
+                    }
+                    __syncthreads();
+                }
+                if (singular)
+                {
+                    if (tid == 0)
+                        atomicExch(A.status, APF_ERR_NUMERIC);
+                    __syncthreads();
+                    continue;
+                }
+                // back substitution (two right-hand sides, one warp each)
+                if (tid < 64)
+                {
+                    const int kk = tid >> 5, lane = tid & 31;
+                    for (int i = n - 1; i >= 0; --i)
+                    {
+                        double s = 0.0;
+                        for (int j = i + 1 + lane; j < n; j += 32)
+                            s += K[i * LD + j] * K[j * LD + NMAX + kk];
+                        for (int o = 16; o > 0; o >>= 1)
+                            s += __shfl_down_sync(0xffffffffu, s, o);
+                        if (lane == 0)
+                            K[i * LD + NMAX + kk] = (K[i * LD + NMAX + kk] - s) / K[i * LD + i];
+                        __syncwarp();
+                    }
+                }
+                __syncthreads();
+                // flux of this patch restricted to each of its cells -> slot of the patch vertex
+                for (int t = tid; t < nc * 16; t += blockDim.x)
+                {
+                    const int ic = t / 16, kk = (t % 16) / 8, j = t % 8;
+                    const int c = A.slab_cells[A.slab_ptr[slab] + A.topo_cell[cb + ic]];
+                    const int a = A.topo_center[cb + ic];
+                    double val = 0.0;
+                    if (j < 6)
+                    {
+                        const int e = j / 2, m = j % 2;
+                        const int code = A.topo_edge[3 * (cb + ic) + e];
+                        const int pe = code & 0xffff;
+                        if (pe != 0xffff)
+                        {
+                            const double sp = (code >> 30) & 1 ? -1.0 : 1.0;
+                            const double det = (A.geo[8ll * c + 2] - A.geo[8ll * c]) * (A.geo[8ll * c + 5] - A.geo[8ll * c + 1]) -
+                                               (A.geo[8ll * c + 4] - A.geo[8ll * c]) * (A.geo[8ll * c + 3] - A.geo[8ll * c + 1]);
+                            const double sn = (det < 0.0 ? -1.0 : 1.0) * sp;
+                            const double cfj = m == 0 ? sn : sn * sp;
+                            val = cfj * K[(2 * pe + m) * LD + NMAX + kk];
+                        }
+                    }
+                    else
+                        val = K[(2 * nfree + 2 * ic + (j - 6)) * LD + NMAX + kk];
+                    A.sigma[((3ll * c + a) * 2 + kk) * 8 + j] = val;
+                }
+                __syncthreads();
+            }
+        }
+
+        struct IndicatorArgs
+        {
+            int n_cells;
+            const double* geo;
+            const double* m;
+            const double* ell;
+            const double* theta;
+            const double* u;
+            const double* lam_delta; // [cell][6]
+            const double* lam_tilde; // [cell][6]
+            const double* sigma;
+            double* flux;
+            double* div;
+            double* recon;
+            double* eta;
+        };
+
+        __global__ void cell_indicators(IndicatorArgs A)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n_cells; c += gridDim.x * blockDim.x)
+            {
+                const Cell k = load_cell(A.geo, A.m, A.ell, c);
+                double S[2][8];
+                for (int kk = 0; kk < 2; ++kk)
+                    for (int j = 0; j < 8; ++j)
+                    {
+                        double s = 0.0;
+                        for (int slot = 0; slot < 3; ++slot)
+                            s += A.sigma[((3ll * c + slot) * 2 + kk) * 8 + j];
+                        S[kk][j] = s;
+                    }
+                const double* th = A.theta + 6ll * c;
+                const double* uu = A.u + 6ll * c;
+                double du[3];
+                for (int s = 0; s < 3; ++s)
+                    du[s] = (uu[2 * s + 1] - uu[2 * s]) / k.ht;
+                const double adet = fabs(k.det);
+                double flux = 0.0, div = 0.0;
+                for (int gt = 0; gt < 2; ++gt)
+                {
+                    const double tau = c_est.tg[gt], wt = c_est.tw[gt] * k.ht;
+                    const double tb[2] = {1.0 - tau, tau};
+                    double gth0 = 0.0, gth1 = 0.0;
+                    for (int s = 0; s < 3; ++s)
+                    {
+                        const double v = th[2 * s] * tb[0] + th[2 * s + 1] * tb[1];
+                        gth0 += k.g[s][0] * v;
+                        gth1 += k.g[s][1] * v;
+                    }
+                    const double mg0 = k.m00 * gth0 + k.m01 * gth1, mg1 = k.m01 * gth0 + k.m11 * gth1;
+                    for (int q = 0; q < c_est.nq; ++q)
+                    {
+                        const double x = c_est.qp[q][0], y = c_est.qp[q][1];
+                        double sx = 0.0, sy = 0.0, sd = 0.0;
+                        for (int j = 0; j < 8; ++j)
+                        {
+                            double vx, vy, dv;
+                            rt_phys(k, j, x, y, vx, vy, dv);
+                            const double cj = S[0][j] * tb[0] + S[1][j] * tb[1];
+                            sx += cj * vx;
+                            sy += cj * vy;
+                            sd += cj * dv;
+                        }
+                        const double ex = sx + mg0, ey = sy + mg1;
+                        const double w = c_est.qw[q] * adet * wt;
+                        flux += w * (ex * (k.mi00 * ex + k.mi01 * ey) + ey * (k.mi01 * ex + k.mi11 * ey));
+                        const double l3[3] = {1.0 - x - y, x, y};
+                        const double dtu = l3[0] * du[0] + l3[1] * du[1] + l3[2] * du[2];
+                        const double r = k.ell - dtu - sd;
+                        div += w * r * r;
+                    }
+                }
+                // ||lambda_delta - lambda~||^2 in the local A_y energy: det ht Mt[a][b] Ks[s][r]
+                double e[6];
+                for (int i = 0; i < 6; ++i)
+                    e[i] = A.lam_delta[6ll * c + i] - A.lam_tilde[6ll * c + i];
+                double rec = 0.0;
+                for (int i = 0; i < 6; ++i)
+                    for (int j = 0; j < 6; ++j)
+                    {
+                        const int s = i / 2, a = i % 2, r = j / 2, b = j % 2;
+                        const double mt = (a == b ? 1.0 / 3.0 : 1.0 / 6.0);
+                        const double ks = k.g[s][0] * (k.m00 * k.g[r][0] + k.m01 * k.g[r][1]) +
+                                          k.g[s][1] * (k.m01 * k.g[r][0] + k.m11 * k.g[r][1]);
+                        rec += e[i] * (0.5 * adet * k.ht * mt * ks) * e[j];
+                    }
+                if (A.flux) A.flux[c] = flux;
+                if (A.div) A.div[c] = div;
+                if (A.recon) A.recon[c] = rec;
+                if (A.eta) A.eta[c] = flux + rec;
+            }
+        }
+
+        // nodal values of a true-DOF vector on every cell (restriction rows with weights)
+        __global__ void gather_nodal(int n_cells, int ndof, const int* off, const int* dofs, const double* w,
+                                     const double* vec, const double* vec2, double* out)
+        {
+            const long long total = (long long)n_cells * ndof;
+            for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < total; r += (long long)gridDim.x * blockDim.x)
+            {
+                double s = 0.0;
+                for (int e = off[r]; e < off[r + 1]; ++e)
+                    s += w[e] * (vec[dofs[e]] + (vec2 ? vec2[dofs[e]] : 0.0));
+                out[r] = s;
+            }
+        }
+
+        __global__ void sum_partials_kernel(int n, const double* a, double* partials)
+        {
+            __shared__ double ws[8];
+            double s = 0.0;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                s += a[i];
+            for (int o = 16; o > 0; o >>= 1)
+                s += __shfl_down_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0)
+                ws[threadIdx.x >> 5] = s;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                double t = 0.0;
+                for (int w = 0; w < 8; ++w)
+                    t += ws[w];
+                partials[blockIdx.x] = t;
+            }
+        }
+
+        int nb(long long n, int threads = 256, int cap = 148 * 32)
+        {
+            return static_cast<int>(std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, cap)));
+        }
+
+        double device_sum(cudaStream_t s, int n, const double* a)
+        {
+            DeviceBuffer<double> parts(kRedBlocks, s);
+            {
+                APF_KERNEL("est_sum_partials", s);
+                sum_partials_kernel<<<kRedBlocks, 256, 0, s>>>(n, a, parts.get());
+            }
+            std::vector<double> h(kRedBlocks);
+            APF_CUDA(cudaMemcpyAsync(h.data(), parts.get(), kRedBlocks * sizeof(double), cudaMemcpyDeviceToHost, s));
+            sync(s);
+            double t = 0.0;
+            for (double v : h)
+                t += v;
+            return t;
+        }
+    }
+
+    // ---------------------------------------------------------------------------
+    // host-side patch topology (integer work; built once per distinct slab mesh)
+    // ---------------------------------------------------------------------------
+    void build_patches(const std::vector<double>& geo, const std::vector<int>& vids, int n_cells, PatchSet& ps)
+    {
+        // slabs by the (exact, dyadic) start time of their cells
+        std::vector<std::int64_t> key(n_cells);
+        for (int c = 0; c < n_cells; ++c)
+            key[c] = std::llround(geo[8ll * c + 6] * 1099511627776.0);
+        std::vector<int> order(n_cells);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+        ps.slab_ptr.assign(1, 0);
+        ps.slab_cells.clear();
+        ps.slab_cells.reserve(n_cells);
+        for (int i = 0; i < n_cells; ++i)
+        {
+            if (i > 0 && key[order[i]] != key[order[i - 1]])
+                ps.slab_ptr.push_back(i);
+            ps.slab_cells.push_back(order[i]);
+        }
+        ps.slab_ptr.push_back(n_cells);
+        const int n_slabs = static_cast<int>(ps.slab_ptr.size()) - 1;
+        for (int s = 0; s < n_slabs; ++s)
+        {
+            const double t1 = geo[8ll * ps.slab_cells[ps.slab_ptr[s]] + 7];
+            for (int i = ps.slab_ptr[s]; i < ps.slab_ptr[s + 1]; ++i)
+                require(geo[8ll * ps.slab_cells[i] + 7] == t1, APF_ERR_INVALID,
+                        "estimator: the cells of a time slab must share their time interval");
+        }
+        // group slabs with identical spatial meshes (same vertex-id sequence)
+        std::vector<int> group_of(n_slabs, -1);
+        std::vector<int> group_rep;
+        std::unordered_map<std::uint64_t, std::vector<int>> by_hash;
+        for (int s = 0; s < n_slabs; ++s)
+        {
+            std::uint64_t h = 1469598103934665603ull;
+            for (int i = ps.slab_ptr[s]; i < ps.slab_ptr[s + 1]; ++i)
+                for (int k = 0; k < 3; ++k)
+                    h = (h ^ static_cast<std::uint64_t>(vids[3ll * ps.slab_cells[i] + k])) * 1099511628211ull;
+            auto& cand = by_hash[h];
+            for (int g : cand)
+            {
+                const int r = group_rep[g];
+                const int len = ps.slab_ptr[s + 1] - ps.slab_ptr[s];
+                if (len != ps.slab_ptr[r + 1] - ps.slab_ptr[r])
+                    continue;
+                bool same = true;
+                for (int i = 0; i < len && same; ++i)
+                    for (int k = 0; k < 3 && same; ++k)
+                        same = vids[3ll * ps.slab_cells[ps.slab_ptr[s] + i] + k] ==
+                               vids[3ll * ps.slab_cells[ps.slab_ptr[r] + i] + k];
+                if (same)
+                {
+                    group_of[s] = g;
+                    break;
+                }
+            }
+            if (group_of[s] < 0)
+            {
+                group_of[s] = static_cast<int>(group_rep.size());
+                cand.push_back(group_of[s]);
+                group_rep.push_back(s);
+            }
+        }
+        // topology patches of every group
+        ps.topo_ptr.assign(1, 0);
+        ps.topo_cell.clear();
+        ps.topo_center.clear();
+        ps.topo_edge.clear();
+        ps.topo_nfree.clear();
+        ps.topo_boundary.clear();
+        std::vector<int> group_first(group_rep.size()), group_count(group_rep.size());
+        ps.max_cells = 0;
+        ps.max_n = 0;
+        for (std::size_t g = 0; g < group_rep.size(); ++g)
+        {
+            const int s = group_rep[g];
+            const int b = ps.slab_ptr[s], len = ps.slab_ptr[s + 1] - b;
+            auto vid = [&](int local, int k) { return vids[3ll * ps.slab_cells[b + local] + k]; };
+            // edge multiplicity in the slab mesh
+            std::unordered_map<std::uint64_t, int> edge_count;
+            edge_count.reserve(static_cast<std::size_t>(len) * 3);
+            auto ekey = [](int p, int q) {
+                const std::uint32_t lo = static_cast<std::uint32_t>(std::min(p, q)), hi = static_cast<std::uint32_t>(std::max(p, q));
+                return (static_cast<std::uint64_t>(lo) << 32) | hi;
+            };
+            for (int i = 0; i < len; ++i)
+                for (int k = 0; k < 3; ++k)
+                    ++edge_count[ekey(vid(i, (k + 1) % 3), vid(i, (k + 2) % 3))];
+            // vertex -> incident (local cell, local vertex), vertices in first-appearance order
+            std::unordered_map<int, int> vindex;
+            std::vector<std::vector<std::pair<int, int>>> inc;
+            std::vector<char> vbound;
+            for (int i = 0; i < len; ++i)
+                for (int k = 0; k < 3; ++k)
+                {
+                    auto it = vindex.find(vid(i, k));
+                    int vi;
+                    if (it == vindex.end())
+                    {
+                        vi = static_cast<int>(inc.size());
+                        vindex.emplace(vid(i, k), vi);
+                        inc.emplace_back();
+                        vbound.push_back(0);
+                    }
+                    else
+                        vi = it->second;
+                    inc[vi].emplace_back(i, k);
+                }
+            for (int i = 0; i < len; ++i)
+                for (int k = 0; k < 3; ++k)
+                    if (edge_count[ekey(vid(i, (k + 1) % 3), vid(i, (k + 2) % 3))] == 1)
+                    {
+                        vbound[vindex[vid(i, (k + 1) % 3)]] = 1;
+                        vbound[vindex[vid(i, (k + 2) % 3)]] = 1;
+                    }
+            group_first[g] = static_cast<int>(ps.topo_nfree.size());
+            group_count[g] = static_cast<int>(inc.size());
+            for (std::size_t v = 0; v < inc.size(); ++v)
+            {
+                const bool boundary = vbound[v] != 0;
+                std::unordered_map<std::uint64_t, int> free_id;
+                int nfree = 0;
+                for (const auto& [i, a] : inc[v])
+                {
+                    ps.topo_cell.push_back(i);
+                    ps.topo_center.push_back(a);
+                    const int va = vid(i, a);
+                    for (int k = 0; k < 3; ++k)
+                    {
+                        const int P = vid(i, (k + 1) % 3), Q = vid(i, (k + 2) % 3);
+                        const std::uint64_t ek = ekey(P, Q);
+                        const int cnt = edge_count[ek];
+                        const bool touches = P == va || Q == va;
+                        const bool is_free = (touches && cnt == 2) || (boundary && cnt == 1);
+                        int code = 0xffff;
+                        if (is_free)
+                        {
+                            auto it = free_id.find(ek);
+                            if (it == free_id.end())
+                                it = free_id.emplace(ek, nfree++).first;
+                            code = it->second;
+                        }
+                        if (P > Q)
+                            code |= 1 << 30; // local parameterisation runs from the higher to the lower id
+                        ps.topo_edge.push_back(code);
+                    }
+                }
+                ps.max_cells = std::max<int>(ps.max_cells, static_cast<int>(inc[v].size()));
+                ps.max_n = std::max<int>(ps.max_n, 2 * nfree + 5 * static_cast<int>(inc[v].size()) + (boundary ? 0 : 1));
+                ps.topo_ptr.push_back(static_cast<int>(ps.topo_cell.size()));
+                ps.topo_nfree.push_back(nfree);
+                ps.topo_boundary.push_back(boundary ? 1 : 0);
+            }
+        }
+        ps.patch_slab.clear();
+        ps.patch_topo.clear();
+        for (int s = 0; s < n_slabs; ++s)
+        {
+            const int g = group_of[s];
+            for (int v = 0; v < group_count[g]; ++v)
+            {
+                ps.patch_slab.push_back(s);
+                ps.patch_topo.push_back(group_first[g] + v);
+            }
+        }
+        ps.n_slabs = n_slabs;
+    }
+
+    void upload_est_tables_once()
+    {
+        static bool done = false;
+        if (done)
+            return;
+        const EstTables t = make_est_tables();
+        APF_CUDA(cudaMemcpyToSymbol(c_est, &t, sizeof(t)));
+        done = true;
+    }
+
+    EstimatorTotals estimate_p1(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
+                                double* recon, double* eta, bool out_on_device)
+    {
+        SystemInputs& in = S.in;
+        require(in.p == 1, APF_ERR_INVALID, "estimator: only p = 1 is implemented");
+        require(S.solution.size() == static_cast<std::size_t>(in.n_lambda + in.n_u), APF_ERR_INVALID,
+                "estimator: solve the main system first");
+        require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
+        require(in.n_x_cells == in.n_y_cells, APF_ERR_INVALID, "estimator: Y cells must coincide with X cells");
+        upload_est_tables_once();
+        EstimatorTotals tot{};
+        const int ny = in.n_y_cells, nl = in.n_lambda, nu = in.n_u;
+        // ---- lambda~ : A_y lambda~ = f - B^T u (PCG with the A_y AMG, start lambda_delta)
+        DeviceBuffer<double> rhs(nl, s), lt(nl, s), r(nl, s), z(nl, s), pv(nl, s), q(nl, s);
+        copy(s, nl, S.f.get(), rhs.get());
+        spmv(s, S.blocks[APF_BLOCK_BT], S.solution.get() + nl, rhs.get(), -1.0, 1.0);
+        copy(s, nl, S.solution.get(), lt.get());
+        const DeviceCsr& Ay = S.blocks[APF_BLOCK_A_Y];
+        residual(s, Ay, lt.get(), rhs.get(), r.get());
+        const double bn = std::sqrt(dot_host(s, S.ws, nl, rhs.get(), rhs.get()));
+        double rn = std::sqrt(dot_host(s, S.ws, nl, r.get(), r.get()));
+        int its = 0;
+        if (bn > 0.0 && rn > 1e-14 * bn)
+        {
+            S.precond->amg_a.apply(s, r.get(), z.get());
+            copy(s, nl, z.get(), pv.get());
+            double rz = dot_host(s, S.ws, nl, r.get(), z.get());
+            for (its = 1; its <= 400; ++its)
+            {
+                spmv(s, Ay, pv.get(), q.get());
+                const double alpha = rz / dot_host(s, S.ws, nl, pv.get(), q.get());
+                axpby(s, nl, alpha, pv.get(), 1.0, lt.get());
+                axpby(s, nl, -alpha, q.get(), 1.0, r.get());
+                rn = std::sqrt(dot_host(s, S.ws, nl, r.get(), r.get()));
+                if (!(rn > 1e-14 * bn))
+                    break;
+                S.precond->amg_a.apply(s, r.get(), z.get());
+                const double rz2 = dot_host(s, S.ws, nl, r.get(), z.get());
+                axpby(s, nl, 1.0, z.get(), rz2 / rz, pv.get());
+                rz = rz2;
+            }
+        }
+        tot.recon_iterations = its;
+        tot.recon_residual = bn > 0.0 ? rn / bn : 0.0;
+        // ---- nodal data per cell
+        const int nd = in.ndof;
+        DeviceBuffer<double> theta(6ll * ny, s), ucell(6ll * ny, s), ldel(6ll * ny, s), ltil(6ll * ny, s);
+        const double* u = S.solution.get() + nl;
+        {
+            APF_KERNEL("est_gather_nodal", s);
+            gather_nodal<<<nb((long long)ny * nd), 256, 0, s>>>(ny, nd, in.y_off.get(), in.y_dofs.get(), in.y_w.get(),
+                                                                lt.get(), nullptr, ltil.get());
+        }
+        {
+            APF_KERNEL("est_gather_nodal", s);
+            gather_nodal<<<nb((long long)ny * nd), 256, 0, s>>>(ny, nd, in.y_off.get(), in.y_dofs.get(), in.y_w.get(),
+                                                                S.solution.get(), nullptr, ldel.get());
+        }
+        {
+            APF_KERNEL("est_gather_nodal", s);
+            gather_nodal<<<nb((long long)ny * nd), 256, 0, s>>>(ny, nd, in.x_off.get(), in.x_dofs.get(), in.x_w.get(), u,
+                                                                nullptr, ucell.get());
+        }
+        axpby(s, 6 * ny, 1.0, ltil.get(), 0.0, theta.get());
+        axpby(s, 6 * ny, 1.0, ucell.get(), 1.0, theta.get());
+        // ---- patches (host topology)
+        std::vector<double> geo(8ll * ny);
+        APF_CUDA(cudaMemcpyAsync(geo.data(), in.y_geo.get(), geo.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        PatchSet ps;
+        build_patches(geo, vids_host, ny, ps);
+        tot.n_slabs = ps.n_slabs;
+        tot.n_patches = static_cast<int>(ps.patch_slab.size());
+        tot.max_patch_cells = ps.max_cells;
+        auto up = [&](DeviceBuffer<int>& d, const std::vector<int>& h) { d.upload(h.data(), h.size()); };
+        DeviceBuffer<int> d_pslab(0, s), d_ptopo(0, s), d_tptr(0, s), d_tcell(0, s), d_tcen(0, s), d_tedge(0, s),
+            d_tnf(0, s), d_tbd(0, s), d_sptr(0, s), d_scell(0, s), status(1, s);
+        up(d_pslab, ps.patch_slab);
+        up(d_ptopo, ps.patch_topo);
+        up(d_tptr, ps.topo_ptr);
+        up(d_tcell, ps.topo_cell);
+        up(d_tcen, ps.topo_center);
+        up(d_tedge, ps.topo_edge);
+        up(d_tnf, ps.topo_nfree);
+        up(d_tbd, ps.topo_boundary);
+        up(d_sptr, ps.slab_ptr);
+        up(d_scell, ps.slab_cells);
+        status.zero();
+        DeviceBuffer<double> sigma(48ll * ny, s);
+        sigma.zero();
+        PatchArgs pa{};
+        pa.n_patches = tot.n_patches;
+        pa.patch_slab = d_pslab.get();
+        pa.patch_topo = d_ptopo.get();
+        pa.topo_ptr = d_tptr.get();
+        pa.topo_cell = d_tcell.get();
+        pa.topo_center = d_tcen.get();
+        pa.topo_edge = d_tedge.get();
+        pa.topo_nfree = d_tnf.get();
+        pa.topo_boundary = d_tbd.get();
+        pa.slab_ptr = d_sptr.get();
+        pa.slab_cells = d_scell.get();
+        pa.geo = in.y_geo.get();
+        pa.m = in.m_y.size() ? in.m_y.get() : nullptr;
+        pa.ell = in.ell.size() ? in.ell.get() : nullptr;
+        pa.theta = theta.get();
+        pa.u = ucell.get();
+        pa.sigma = sigma.get();
+        pa.status = status.get();
+        const int nmax_needed = ps.max_n;
+        auto launch = [&](auto tag) {
+            constexpr int NMAX = decltype(tag)::value;
+            const size_t smem = sizeof(double) * NMAX * (NMAX + 2);
+            APF_CUDA(cudaFuncSetAttribute(patch_solve<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            pa.nmax = NMAX;
+            APF_KERNEL("est_patch_solve", s);
+            patch_solve<NMAX><<<std::max(1, std::min(tot.n_patches, 148 * 16)), 128, smem, s>>>(pa);
+        };
+        if (tot.n_patches > 0)
+        {
+            if (nmax_needed <= 64)
+                launch(std::integral_constant<int, 64>{});
+            else if (nmax_needed <= 96)
+                launch(std::integral_constant<int, 96>{});
+            else if (nmax_needed <= 144)
+                launch(std::integral_constant<int, 144>{});
+            else
+                throw Error(APF_ERR_CAPACITY, "estimator: patch too large (more than 16 cells around a vertex)");
+            APF_CUDA(cudaGetLastError());
+        }
+        int hstat = 0;
+        APF_CUDA(cudaMemcpyAsync(&hstat, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        if (hstat == APF_ERR_NUMERIC)
+            throw Error(APF_ERR_NUMERIC, "estimator: singular patch system");
+        if (hstat != 0)
+            throw Error(APF_ERR_CAPACITY, "estimator: patch system larger than the kernel's buffer");
+        // ---- indicators
+        DeviceBuffer<double> f2(ny, s), d2(ny, s), r2(ny, s), e2(ny, s);
+        IndicatorArgs ia{ny, in.y_geo.get(), pa.m, pa.ell, theta.get(), ucell.get(), ldel.get(), ltil.get(), sigma.get(),
+                         f2.get(), d2.get(), r2.get(), e2.get()};
+        {
+            APF_KERNEL("est_cell_indicators", s);
+            cell_indicators<<<nb(ny, 128), 128, 0, s>>>(ia);
+        }
+        APF_CUDA(cudaGetLastError());
+        tot.flux = device_sum(s, ny, f2.get());
+        tot.div = device_sum(s, ny, d2.get());
+        tot.recon = device_sum(s, ny, r2.get());
+        tot.eta = device_sum(s, ny, e2.get());
+        const cudaMemcpyKind kind = out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (flux) APF_CUDA(cudaMemcpyAsync(flux, f2.get(), ny * sizeof(double), kind, s));
+        if (div) APF_CUDA(cudaMemcpyAsync(div, d2.get(), ny * sizeof(double), kind, s));
+        if (recon) APF_CUDA(cudaMemcpyAsync(recon, r2.get(), ny * sizeof(double), kind, s));
+        if (eta) APF_CUDA(cudaMemcpyAsync(eta, e2.get(), ny * sizeof(double), kind, s));
+        sync(s);
+        return tot;
+    }
+}

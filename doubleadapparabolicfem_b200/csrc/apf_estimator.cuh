@@ -1,0 +1,40 @@
+// Equilibrated-flux estimator (see apf_estimator.cu).
+#pragma once
+
+#include <vector>
+
+#include "apf_system.hpp"
+
+namespace apf
+{
+    // Vertex patches of every time slab; patches of slabs with identical spatial meshes
+    // share one topology entry.
+    struct PatchSet
+    {
+        int n_slabs = 0;
+        int max_cells = 0;
+        int max_n = 0;                  // largest patch system (flux + scalar + constraint)
+        std::vector<int> slab_ptr;      // slab -> range in slab_cells
+        std::vector<int> slab_cells;    // Y cell ids grouped by slab
+        std::vector<int> topo_ptr;      // topology patch -> range of patch cells
+        std::vector<int> topo_cell;     // local cell index in the slab's cell list
+        std::vector<int> topo_center;   // local vertex index of the patch vertex
+        std::vector<int> topo_edge;     // 3 per patch cell: free edge id | sign bit 30
+        std::vector<int> topo_nfree;
+        std::vector<int> topo_boundary;
+        std::vector<int> patch_slab;    // patch -> slab
+        std::vector<int> patch_topo;    // patch -> topology patch
+    };
+
+    struct EstimatorTotals
+    {
+        double flux = 0.0, div = 0.0, recon = 0.0, eta = 0.0;
+        int n_slabs = 0, n_patches = 0, max_patch_cells = 0, recon_iterations = 0;
+        double recon_residual = 0.0;
+    };
+
+    void build_patches(const std::vector<double>& geo, const std::vector<int>& vids, int n_cells, PatchSet& ps);
+
+    EstimatorTotals estimate_p1(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
+                                double* recon, double* eta, bool out_on_device);
+}

@@ -1,0 +1,43 @@
+"""Host-side mirror of the reference's estimator entry points (p = 1).
+
+``estimate(blocks)`` runs, on the solution of the last
+``solver.solve_saddle_system_with_preconditioner`` call, what one inner iteration of
+``finite_element::time_slabs::compute_adaptive_test_space_iteration``
+(src/finite_element/time_slabs/time_slab_adaptive_loop.hpp:727) computes after the
+main solve:
+
+* the slab reconstruction lambda~ (``TimeSlabReconstruction::solve_all_slabs``,
+  time_slab_reconstruction.hpp:584);
+* the vertex-patch equilibrated fluxes (``solve_all_patches``,
+  time_slab_equilibrated_flux_reconstruction.hpp:2515);
+* the per-source-cell maps ``by_source_cell_flux`` / ``by_source_cell_residual``
+  (time_slab_equilibrated_flux_indicators.hpp:203), the reconstruction term
+  (time_slab_error_norms.hpp:946) and eta^2 = flux^2 + reconstruction^2
+  (time_slab_estimator_combination.hpp).
+
+Per-cell results are numpy arrays over the Y cells in input order.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .assembly import MainSystemBlocks, _ptr
+
+
+def estimate(blocks: MainSystemBlocks, y_vertex_ids: np.ndarray | None = None):
+    vids = y_vertex_ids if y_vertex_ids is not None else blocks.problem.y_vertex_ids
+    if vids is None:
+        raise ValueError("the estimator needs the spatial vertex ids of the Y cells")
+    vids = np.ascontiguousarray(vids, dtype=np.int32)
+    n = blocks.problem.n_y_cells
+    out = {k: np.empty(n) for k in ("flux", "divergence", "reconstruction", "eta")}
+    res = _lib.EstimatorResult()
+    ctx = blocks.ctx
+    ctx.check(ctx.lib.apf_estimate(ctx.handle, blocks.handle, _ptr(vids), 0, _ptr(out["flux"]),
+                                   _ptr(out["divergence"]), _ptr(out["reconstruction"]), _ptr(out["eta"]),
+                                   C.byref(res)))
+    totals = {name: getattr(res, name) for name, _ in res._fields_}
+    return out, totals

@@ -52,6 +52,7 @@ class SpaceTimeProblem:
     m_cells: np.ndarray | None = None     # [n_y_cells, 3] or None (identity)
     ell_cells: np.ndarray | None = None   # [n_y_cells] or None (zero load)
     u0_kind: int = 0                      # 0 sin(pi x) sin(pi y), 1 one, 2 zero
+    y_vertex_ids: np.ndarray | None = None  # [n_y_cells, 3] spatial vertex ids (estimator patches)
     meta: dict = field(default_factory=dict)
 
     @property
@@ -142,10 +143,13 @@ def uniform_problem(level: int, p: int = 1, u0_kind: int = 0, m_cells=None) -> S
         return Restriction(offsets, dofs, np.ones(dofs.size), ndof)
 
     ncell = geo.shape[0]
+    # spatial vertex ids (grid index of the P1 vertices), the same in every slab
+    vids = (tris[..., 1] * (n + 1) + tris[..., 0]).astype(np.int32)
     return SpaceTimeProblem(
         p=p, y_geometry=geo, x_geometry=geo.copy(), y_to_x=np.arange(ncell, dtype=np.int32),
         y_restriction=restriction(y_ids), x_restriction=restriction(x_ids),
         n_lambda=int(n_lambda), n_u=int(n_u), m_cells=m_cells, u0_kind=u0_kind,
+        y_vertex_ids=np.tile(vids, (nt, 1)),
         meta=dict(level=level, n=n, nt=nt, n_spatial_interior=n_sp))
 
 

@@ -191,6 +191,44 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
  * and diagnostics (symmetry, PCG quality) of the preconditioner. */
 int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const double* r, double* z,
                              int pointers_on_device);
+/* ---- equilibrated-flux estimator ------------------------------------------------ */
+/* Totals of the last estimate (the reference's CellwiseEquilibratedFluxError /
+ * CellwiseTimeSlabEstimatorError totals, time_slab_cellwise_errors.hpp:325-450). */
+typedef struct apf_estimator_result
+{
+    double flux_squared;           /* sum_K ||M^-1/2 (sigma + M grad theta~)||^2_K */
+    double divergence_squared;     /* sum_K ||l - d_t u - div sigma||^2_K */
+    double reconstruction_squared; /* sum_K ||lambda_delta - lambda~||^2_{Y,K} */
+    double eta_squared;            /* flux + reconstruction */
+    int n_slabs;
+    int n_patches;
+    int max_patch_cells;
+    int reconstruction_iterations;
+    double reconstruction_residual; /* relative residual of the slab reconstruction solve */
+} apf_estimator_result;
+
+/* The estimator of one inner iteration for p = 1, on the solution of the last
+ * apf_solve_minres call:
+ *   lambda~ : slab Riesz reconstruction, A_y lambda~ = f - B^T u (Y is broken in time, so
+ *             this is every slab's reconstruction system at once), replacing
+ *             TimeSlabReconstruction::solve_all_slabs (src/finite_element/time_slabs/
+ *             time_slab_reconstruction.hpp:584);
+ *   sigma_a : one mixed RT_1 x P_1 local problem per (time slab, spatial vertex) patch,
+ *             replacing TimeSlabEquilibratedFluxReconstruction2plus1d::solve_all_patches
+ *             (time_slab_equilibrated_flux_reconstruction.hpp:2515) with the bordered
+ *             dense system of dense_local_error_blocks_2d.hpp:812-905;
+ *   indicators per Y cell: compute_equilibrated_flux_error_squared_by_source_cell_2plus1d
+ *             (time_slab_equilibrated_flux_indicators.hpp:203), the reconstruction term of
+ *             compute_Y_error_squared_by_source_cell (time_slab_error_norms.hpp:946) and
+ *             their sum (time_slab_estimator_combination.hpp).
+ * y_vertex_ids: [n_y_cells*3] spatial vertex ids of every Y cell (the reference mesh's
+ * cell.spatial_vertex_ids); host or device per pointers_on_device.  Y cells must
+ * coincide with their X ancestors.  Output arrays ([n_y_cells] each, host or device per
+ * pointers_on_device) may be NULL. */
+int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int pointers_on_device,
+                 double* flux_squared, double* divergence_squared, double* reconstruction_squared,
+                 double* eta_squared, apf_estimator_result* result);
+
 /* Device pointer of the last solution (n_lambda + n_u values, owned by sys). */
 int apf_system_solution_device_ptr(const apf_system* sys, const double** solution);
 

@@ -39,6 +39,7 @@
 #include "finite_element/system/assemble_saddle_problem.hpp"
 #include "finite_element/assembly/main_system/parabolic_graph_norm.hpp"
 #include "finite_element/assembly/constrained_dofs.hpp"
+#include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
 #include "mesh/mesh_traits.hpp"
 
 #include "npy.hpp"
@@ -240,6 +241,13 @@ namespace
 
         std::filesystem::create_directories(dir);
         dump_geometry_2d(dir, "y_geometry", y_space, y_cells);
+        {
+            std::vector<int> vids;
+            for (const int c : y_cells)
+                for (int k = 0; k < 3; ++k)
+                    vids.push_back(mesh.cell(c).spatial_vertex_ids[k]);
+            apf_oracle::write_npy(dir + "/y_vertex_ids.npy", vids.data(), {y_cells.size(), 3u});
+        }
         dump_geometry_2d(dir, "x_geometry", x_space, x_cells);
         dump_restrictions(dir, "y_restriction", y_space, y_cells);
         dump_restrictions(dir, "x_restriction", x_space, x_cells);
@@ -267,6 +275,36 @@ namespace
         const auto gn = finite_element::assembly::assemble_parabolic_graph_norm_approximation<QSpace, QTime, Backend>(
             y_space, x_space, example.problem.M, blocks.A_y(), blocks.C_signed(), 1e-15, 1e-14);
         dump_csc(dir, "Hhat", gn.approximation.hhat);
+
+        if (std::getenv("APF_REF_ESTIMATE") != nullptr)
+        {
+            // the reference's whole inner iteration (time_slab_adaptive_loop.hpp:727):
+            // main solve (direct), slab reconstruction, vertex-patch flux solves, indicators
+            typename Backend::Solver solver;
+            la::concepts::SolverOptions opts;
+            finite_element::time_slabs::AdaptiveTestSpaceIterationParameters<Backend, XSpace, YSpace> params;
+            const auto state = finite_element::time_slabs::compute_adaptive_test_space_iteration<QSpace, QTime, Backend>(
+                y_space, x_space, example.problem, solver, opts, params);
+            dump_vec(dir, "lambda_delta", state.lambda_delta.true_coefficients());
+            dump_vec(dir, "u_delta", state.u_delta.true_coefficients());
+            auto dump_map = [&](const std::string& name, const auto& m) {
+                std::vector<int> ids;
+                std::vector<double> vals;
+                for (const int c : y_cells)
+                {
+                    const auto it = m.find(c);
+                    vals.push_back(it == m.end() ? std::numeric_limits<double>::quiet_NaN() : it->second);
+                }
+                apf_oracle::write_npy(dir + "/" + name + ".npy", vals);
+            };
+            dump_map("est_flux", state.flux_diagnostics.by_source_cell_flux);
+            dump_map("est_div", state.flux_diagnostics.by_source_cell_residual);
+            dump_map("est_recon", state.reconstruction_y_squared.by_source_cell);
+            dump_map("est_eta", state.estimator.estimator_squared.by_source_cell);
+            std::fprintf(stderr, "estimate: flux=%.6e div=%.6e recon=%.6e eta=%.6e\n",
+                         state.flux_diagnostics.total_flux(), state.flux_diagnostics.total_residual(),
+                         state.reconstruction_y_squared.total(), state.estimator.total());
+        }
         return 0;
     }
 }

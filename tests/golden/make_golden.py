@@ -1,8 +1,10 @@
 """Regenerate the golden fixtures in this directory from the reference itself.
 
-Runs oracle/_ref/apf_ref_dump (the reference's own assembly templates compiled by
+Runs oracle/_ref/apf_ref_dump (the reference's own templates compiled by
 oracle/Makefile against oracle/shim) on small uniform meshes and packs each case
-into one .npz.  Also extracts the uniform-refinement rows (exact DOF counts and
+into one .npz: mesh and DOF maps, assembled blocks, and the reference's whole inner
+iteration (direct main solve, slab reconstruction, vertex-patch flux solves,
+per-cell indicators).  Also extracts the uniform-refinement rows (exact DOF counts and
 6-significant-digit estimator values) of the reference's published paper data
 (algorithm_data_plot/{1d,2d}/*.csv) into paper_uniform_rows.json.
 
@@ -30,11 +32,13 @@ CASES = [
     ("p1_l2_smooth", 2, 1, 2, "smooth_initial"),
     ("p2_l1_smooth", 2, 2, 1, "smooth_initial"),
     ("p1_l1_nonmatching", 2, 1, 1, "non_matching_initial"),
+    ("p1_l3_smooth", 2, 1, 3, "smooth_initial"),
 ]
 
 
 def dump_case(dim, p, level, example, outdir):
-    subprocess.run([REF_BIN, str(dim), str(p), str(level), example, outdir], check=True)
+    env = dict(os.environ, APF_REF_ESTIMATE="1")
+    subprocess.run([REF_BIN, str(dim), str(p), str(level), example, outdir], check=True, env=env)
     arrays = {}
     for f in sorted(glob.glob(os.path.join(outdir, "*.npy"))):
         arrays[os.path.basename(f)[:-4]] = np.load(f)
