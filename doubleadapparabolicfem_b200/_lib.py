@@ -162,3 +162,6 @@ class EstimatorResult(C.Structure):
 
 SIGNATURES["apf_estimate"] = ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                C.c_void_p, C.POINTER(EstimatorResult)], C.c_int)
+
+SIGNATURES["apf_true_residual_noalloc"] = ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int)

@@ -531,6 +531,18 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
     });
 }
 
+int apf_true_residual_noalloc(apf_ctx* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_idx,
+                              const double* values, const double* x, const double* b, double* absolute_residual,
+                              double* relative_residual)
+{
+    if (!ctx)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        apf::true_residual_noalloc(ctx->device, ctx->stream, rows, row_ptr, col_idx, values, x, b, absolute_residual,
+                                   relative_residual);
+    });
+}
+
 int apf_system_solution_device_ptr(const apf_system* sys, const double** solution)
 {
     if (!sys || !solution || !sys->sys.solution.size())

@@ -78,6 +78,11 @@ namespace apf
     void build_hhat(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& C, const DeviceCsr& A_x, const DeviceCsr& B_dt,
                     const DeviceCsr& B_dtT, double diag_tol, DeviceCsr& H, DeviceBuffer<double>& inv_diag);
 
+    // ||b - K x||_2 and ||b - K x||_2 / ||b||_2 with no device allocation (apf_noalloc.cu)
+    void true_residual_noalloc(int device, cudaStream_t s, int rows, const int* row_ptr, const int* col_idx,
+                               const double* values, const double* x, const double* b, double* absolute,
+                               double* relative);
+
     // assembly drivers (apf_capi.cu)
     void assemble_main(System& sys);
     void assemble_graph_norm(System& sys, double diag_tol);

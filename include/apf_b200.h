@@ -229,6 +229,21 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
                  double* flux_squared, double* divergence_squared, double* reconstruction_squared,
                  double* eta_squared, apf_estimator_result* result);
 
+/* ---- allocation-free residual check ---------------------------------------------- */
+/* No counterpart in the reference: an addition for callers that cannot allocate device
+ * memory where they need the check -- e.g. a solver loop whose device memory is all owned
+ * by its own pool, or a job running the GPU so full that a late cudaMalloc could fail.
+ * Computes ||b - K x||_2 and ||b - K x||_2 / ||b||_2 (||b|| = 0: the absolute value) for a
+ * CSR matrix K (rows x rows, int32 indices, f64 values) and vectors x, b, all device
+ * pointers, on the context's stream.  Allocates no device memory: its scratch is one
+ * fixed 64 KiB device array shared by all calls on a device, so at most 16,777,216 rows
+ * (larger K: APF_ERR_CAPACITY).  The first call on a device looks the array's address up
+ * (make it before any stream capture); calls whose GPU work overlaps race on the shared
+ * array.  Results are written to the host doubles given (either may be NULL). */
+int apf_true_residual_noalloc(apf_ctx* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_idx,
+                              const double* values, const double* x, const double* b, double* absolute_residual,
+                              double* relative_residual);
+
 /* Device pointer of the last solution (n_lambda + n_u values, owned by sys). */
 int apf_system_solution_device_ptr(const apf_system* sys, const double** solution);
 
