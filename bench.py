@@ -1,4 +1,4 @@
-"""Benchmark: one adaptive-cycle hot path of the 2+1D space-time heat problem on B200.
+"""Benchmark: one inner iteration of the adaptive cycle of the 2+1D space-time heat problem on B200.
 
 Workload (default): 2+1D heat equation on (0,1)^2 x (0,1), u0 = sin(pi x) sin(pi y),
 f = 0, M = I, uniform space-time prism mesh of outer level 6 (2,097,152 prisms,
@@ -7,16 +7,21 @@ Synthetic input: the mesh and DOF maps are generated on the host
 (doubleadapparabolicfem_b200.mesh.uniform_problem), with the reference's cell
 geometry and DOF counts.
 
-A step = the hot path over one mesh: main-system assembly (A_y, B, B^T, C_signed,
-K, f, g) and the parabolic graph-norm preconditioner block Hhat, from inputs already
-in HBM.  ``e2e`` = the same through the C ABI from pinned host buffers (H2D of the
-mesh inputs and D2H of the right-hand sides inside the timed region).
+A step = the hot path of one inner iteration over one mesh, as
+compute_adaptive_test_space_iteration runs it: main-system assembly (A_y, B, B^T,
+C_signed, K, f, g), the parabolic graph-norm block Hhat, the block preconditioner's
+set-up, MINRES to FP64 true relative residual 1e-8, and the equilibrated-flux estimator
+(slab reconstruction, vertex-patch flux solves, per-cell indicators), from inputs
+already in HBM.  ``e2e`` = the same through the C ABI from pinned host buffers (H2D of
+the mesh inputs and D2H of the solution and the per-cell indicators inside the timed
+region).
 
 Multi-GPU: the path runs one problem per GPU (replicas; no collective in the data
 path).  ``value`` = total DOFs processed by all ranks / max-over-ranks time.
 
-``--impl reference`` times the reference's own CPU implementation of the path
-(oracle/_ref/apf_ref_dump: the reference templates compiled here) on the host cores.
+``--impl reference`` times the reference's own CPU implementation of the same inner
+iteration (oracle/_ref/apf_ref_dump: the reference templates compiled here) on the
+host cores, on a bounded sample of the workload.
 """
 from __future__ import annotations
 
@@ -27,7 +32,6 @@ import statistics
 import subprocess
 import sys
 import threading
-import time
 
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
@@ -39,12 +43,13 @@ UNIT = "DOFs/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=6)
     ap.add_argument("--p", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-estimator", action="store_true")
     ap.add_argument("--tol", type=float, default=1e-8)
     return ap.parse_args()
 
@@ -110,12 +115,20 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def sample_level_for(level: int) -> int:
+    """Outer level of the bounded CPU sample: level 3 (4,096 prisms, 5,625 DOFs, a few
+    seconds per inner iteration on 8 cores) for the large meshes; the reference's direct
+    solves grow superlinearly, so a larger sample would not finish in minutes."""
+    return max(1, min(3, level - 3))
+
+
 def cpu_reference_sample(level: int, p: int, reps: int, threads: int | None = None):
-    """Time the reference's own CPU path (oracle/_ref) on a bounded sample."""
+    """Time the reference's own CPU inner iteration (oracle/_ref) on a bounded sample."""
     exe = os.path.join(REPO, "oracle", "_ref", "apf_ref_dump")
     if not os.path.exists(exe):
         return None
     env = dict(os.environ)
+    env["APF_REF_CYCLE"] = "1"
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
     out = subprocess.run([exe, "bench", str(p), str(level), "smooth_initial", str(reps)], capture_output=True, text=True,
@@ -130,9 +143,7 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    # bounded sample of the workload: the same mesh family one outer level coarser
-    # (1/8 of the cells), which keeps each step to a few seconds of CPU time
-    sample_level = max(1, args.level - 1)
+    sample_level = sample_level_for(args.level)
     exe = os.path.join(REPO, "oracle", "_ref", "apf_ref_dump")
     if not os.path.exists(exe):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/apf_ref_dump was not built (needs the reference sources)"}))
@@ -143,6 +154,9 @@ def run_reference(args, world, rank):
     info = None
     for _ in range(args.steps):
         info = cpu_reference_sample(sample_level, args.p, 1, threads)
+        if info is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/apf_ref_dump bench failed"}))
+            return
         times.append(info["mean_s"])
     t = sum(times)
     value = args.steps * info["n_dofs"] / t
@@ -150,47 +164,37 @@ def run_reference(args, world, rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"2+1D heat, uniform outer level {args.level} P{args.p} mesh (sampled at level {sample_level})",
-                   "stages": ["assembly", "graph_norm"]},
+        "config": {"workload": f"2+1D heat, u0=sin(pi x)sin(pi y), uniform outer level {args.level} P{args.p} mesh "
+                               f"(sampled at outer level {sample_level})",
+                   "stages": ["assembly", "graph_norm", "main_solve", "slab_reconstruction", "patch_fluxes",
+                              "indicators"],
+                   "solver": "the reference's main solve through the oracle shim's direct solver",
+                   "flux_squared": info.get("flux_squared")},
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"outer level {sample_level} ({info['n_cells']} prisms, {info['n_dofs']} DOFs) per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["threads"], "kind": "reference",
+                         "sample": f"one inner iteration of the reference at outer level {sample_level} "
+                                   f"({info['n_cells']} prisms, {info['n_dofs']} DOFs) per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
-def fill_kernel_bytes(problem, blocks_info):
-    """Algorithmic bytes of the gather_rows_fill launches of one step: each launch reads
-    its incidence list and the geometry / restriction rows of the incident cells once
-    and writes its CSR block once."""
-    ndof = problem.ndof
-    ny, nx = problem.n_y_cells, problem.n_x_cells
-    geo = 64
-    restr = ndof * (4 + 4 + 8)          # offsets + dofs + weights per cell
-    total = 0
-    for name, (rows, cols, nnz, cells) in blocks_info.items():
-        total += nnz * 12 + (rows + 1) * 4          # CSR written
-        total += (rows + 1) * 4 + cells * ndof * 8  # incidence lists read
-        total += cells * (geo + restr)              # cell data read
-    return total
-
-
 def run_ours(args, world, rank, local):
+    import ctypes as C
+
     import numpy as np
     import torch
     from doubleadapparabolicfem_b200 import build as b
     from doubleadapparabolicfem_b200 import _lib
     from doubleadapparabolicfem_b200.assembly import Context, MainSystemBlocks, make_desc, _Keep
     from doubleadapparabolicfem_b200.mesh import uniform_problem, SpaceTimeProblem, Restriction
-    import ctypes as C
 
     b.build()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
-        import torch.distributed as dist
         import datetime
+        import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     stream = torch.cuda.Stream(device=dev)
     ctx = Context(local, stream=stream.cuda_stream)
@@ -198,6 +202,8 @@ def run_ours(args, world, rank, local):
 
     host = uniform_problem(args.level, args.p)
     n_dofs = host.n_lambda + host.n_u
+    ny = host.n_y_cells
+    run_estimator = not args.no_estimator and args.p == 1
 
     def to_dev(a, dtype):
         return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(dev)
@@ -213,30 +219,48 @@ def run_ours(args, world, rank, local):
                                       conv(host.y_restriction.weights, np.float64), host.ndof),
             x_restriction=Restriction(conv(host.x_restriction.offsets, np.int32), conv(host.x_restriction.dofs, np.int32),
                                       conv(host.x_restriction.weights, np.float64), host.ndof),
-            n_lambda=host.n_lambda, n_u=host.n_u, u0_kind=host.u0_kind)
+            n_lambda=host.n_lambda, n_u=host.n_u, u0_kind=host.u0_kind,
+            y_vertex_ids=conv(host.y_vertex_ids, np.int32))
 
     dprob = clone_problem(to_dev)
     hprob = clone_problem(to_pinned)
-    h2d_bytes = sum(int(t.numel() * t.element_size()) for t in (
-        hprob.y_geometry, hprob.x_geometry, hprob.y_to_x, hprob.y_restriction.offsets, hprob.y_restriction.dofs,
-        hprob.y_restriction.weights, hprob.x_restriction.offsets, hprob.x_restriction.dofs, hprob.x_restriction.weights))
-    x_out = torch.empty(n_dofs, dtype=torch.float64).pin_memory()
-    d2h_bytes = n_dofs * 8
+    h2d_tensors = [hprob.y_geometry, hprob.x_geometry, hprob.y_to_x, hprob.y_restriction.offsets,
+                   hprob.y_restriction.dofs, hprob.y_restriction.weights, hprob.x_restriction.offsets,
+                   hprob.x_restriction.dofs, hprob.x_restriction.weights]
+    if run_estimator:
+        h2d_tensors.append(hprob.y_vertex_ids)
+    h2d_bytes = sum(int(t.numel() * t.element_size()) for t in h2d_tensors)
+    x_host = torch.empty(n_dofs, dtype=torch.float64).pin_memory()
+    eta_host = torch.empty(ny, dtype=torch.float64).pin_memory()
+    eta_dev = torch.empty(ny, dtype=torch.float64, device=dev)
+    d2h_bytes = n_dofs * 8 + (ny * 8 if run_estimator else 0)
     sopt = _lib.SolverOptions()
     lib.apf_solver_options_default(C.byref(sopt))
     sopt.tolerance = args.tol
     solve_diags = []
+    est_results = []
 
-    def step(prob, on_device, read_back):
+    def step(prob, on_device):
         keep = _Keep()
         desc = make_desc(prob, 1e-15, -1.0, keep)
         h = C.c_void_p()
         ctx.check(lib.apf_assemble_main_system(ctx.handle, C.byref(desc), 1 if on_device else 0, C.byref(h)))
-        ctx.check(lib.apf_assemble_graph_norm(ctx.handle, h, 1e-14))
-        d = _lib.SolverDiagnostics()
-        out = C.c_void_p(x_out.data_ptr()) if read_back else None
-        ctx.check(lib.apf_solve_minres(ctx.handle, h, C.byref(sopt), None, out, 0, C.byref(d)))
-        solve_diags.append({k: getattr(d, k) for k, _ in d._fields_})
+        try:
+            ctx.check(lib.apf_assemble_graph_norm(ctx.handle, h, 1e-14))
+            d = _lib.SolverDiagnostics()
+            out = None if on_device else C.c_void_p(x_host.data_ptr())
+            ctx.check(lib.apf_solve_minres(ctx.handle, h, C.byref(sopt), None, out, 0, C.byref(d)))
+            solve_diags.append({k: getattr(d, k) for k, _ in d._fields_})
+            if run_estimator:
+                res = _lib.EstimatorResult()
+                eta = eta_dev if on_device else eta_host
+                ctx.check(lib.apf_estimate(ctx.handle, h, C.c_void_p(prob.y_vertex_ids.data_ptr()),
+                                           1 if on_device else 0, None, None, None, C.c_void_p(eta.data_ptr()),
+                                           C.byref(res)))
+                est_results.append({k: getattr(res, k) for k, _ in res._fields_})
+        except Exception:
+            lib.apf_system_destroy(h)
+            raise
         return h
 
     def barrier():
@@ -254,7 +278,7 @@ def run_ours(args, world, rank, local):
 
     # warm-up
     for _ in range(args.warmup):
-        lib.apf_system_destroy(step(dprob, True, False))
+        lib.apf_system_destroy(step(dprob, True))
     ctx.synchronize()
 
     # timed device-resident steps, with per-kernel CUDA-event timing on the library's stream
@@ -267,7 +291,7 @@ def run_ours(args, world, rank, local):
     with ClockSampler(local) as clocks:
         ev0.record(stream)
         for _ in range(args.steps):
-            lib.apf_system_destroy(step(dprob, True, False))
+            lib.apf_system_destroy(step(dprob, True))
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     barrier()
@@ -275,6 +299,8 @@ def run_ours(args, world, rank, local):
     report = json.loads(lib.apf_ctx_timing_report(ctx.handle).decode())
     ctx.check(lib.apf_ctx_set_timing(ctx.handle, 0))
     elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    timed_diags = solve_diags[-args.steps:]
+    timed_est = est_results[-args.steps:]
 
     # e2e through the C ABI from pinned host buffers
     barrier()
@@ -283,49 +309,40 @@ def run_ours(args, world, rank, local):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        lib.apf_system_destroy(step(hprob, False, True))
+        lib.apf_system_destroy(step(hprob, False))
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
     e2e_elapsed = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e_diags = solve_diags[-args.steps:]
 
-    # roofline of the dominant kernel (algorithmic bytes per launch / event-timed duration)
-    dominant = max(report.items(), key=lambda kv: kv[1][1])
-    h = step(dprob, True, False)
+    # block sizes for the roofline's algorithmic bytes
+    h = step(dprob, True)
     m = MainSystemBlocks(ctx, h, host)
-    info = {}
-    cells = {"A_y": host.n_y_cells, "BT": host.n_y_cells, "B": host.n_y_cells, "C_signed": host.n_x_cells // (2 ** args.level),
-             "A_x": host.n_x_cells, "B_dt": host.n_y_cells}
-    for name in ("A_y", "BT", "B", "C_signed", "A_x", "B_dt"):
-        r, c, nnz = m.block_info(name)
-        info[name] = (r, c, nnz, cells[name])
-    info["B_dtT"] = (host.n_lambda, host.n_u, info["B_dt"][2], host.n_y_cells)
     nnz_k = m.block_info("K")[2]
     nnz_h = m.block_info("Hhat")[2]
     m.close()
     peak, peak_kind = measured_peaks()
-    fill_bytes = fill_kernel_bytes(host, info)
-    fill_launches, fill_ms = report.get("gather_rows_fill", [1, float("nan")])
-    fill_achieved = (fill_bytes / 7.0) / (fill_ms / 1e3 / fill_launches) / 1e9
-    # K SpMV inside MINRES: CSR values + column indices + row pointers once, x read once, y written once
+    # K SpMV inside MINRES: CSR values + column indices + row pointers once, x read once,
+    # y written once
     spmv_bytes = 12.0 * nnz_k + 4.0 * (n_dofs + 1) + 16.0 * n_dofs
     spmv_launches, spmv_ms = report.get("minres_spmv_K", [1, float("nan")])
     spmv_achieved = spmv_bytes / (spmv_ms / 1e3 / spmv_launches) / 1e9
-    its = [d["iterations"] for d in solve_diags[-args.steps:]]
-    res = [d["final_true_residual"] for d in solve_diags[-args.steps:]]
-    rank0 = rank == 0
-    if not rank0:
+    dominant = max(report.items(), key=lambda kv: kv[1][1])
+    if rank != 0:
         return
     cpu = None
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sample_level = max(1, args.level - 2)
-        info_cpu = cpu_reference_sample(sample_level, args.p, 2, threads)
+        sample_level = sample_level_for(args.level)
+        info_cpu = cpu_reference_sample(sample_level, args.p, 3, threads)
         if info_cpu:
             cpu = {"value": info_cpu["n_dofs"] / info_cpu["mean_s"], "unit": UNIT, "cores": info_cpu["threads"],
                    "kind": "reference",
-                   "sample": f"reference CPU assembly + graph norm on outer level {sample_level} "
-                             f"({info_cpu['n_cells']} prisms, {info_cpu['n_dofs']} DOFs), mean of 2 reps"}
+                   "sample": f"one inner iteration of the reference (assembly, graph norm, direct main solve, "
+                             f"estimator) at outer level {sample_level} ({info_cpu['n_cells']} prisms, "
+                             f"{info_cpu['n_dofs']} DOFs), mean of 3"}
+    total_ms = sum(v[1] for v in report.values())
     line = {
         "metric": METRIC,
         "value": args.steps * n_dofs * world / elapsed,
@@ -340,23 +357,29 @@ def run_ours(args, world, rank, local):
         "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": f"2+1D heat, u0=sin(pi x)sin(pi y), uniform outer level {args.level} P{args.p} "
-                               f"({host.n_y_cells} prisms, {n_dofs} DOFs)",
-                   "stages": ["assembly", "graph_norm", "amg_setup", "minres"],
+                               f"({ny} prisms, {n_dofs} DOFs)",
+                   "stages": ["assembly", "graph_norm", "amg_setup", "minres"] +
+                             (["slab_reconstruction", "patch_fluxes", "indicators"] if run_estimator else []),
                    "tolerance": args.tol,
-                   "preconditioner": "blkdiag(A_y, Hhat) by SA-AMG V-cycles",
-                   "minres_iterations": its, "final_true_residual_max": max(res),
+                   "preconditioner": "plain: blkdiag(A_y, Hhat) by SA-AMG V-cycles",
+                   "minres_iterations": [d["iterations"] for d in timed_diags],
+                   "final_true_residual_max": max(d["final_true_residual"] for d in timed_diags),
+                   "e2e_final_true_residual_max": max(d["final_true_residual"] for d in e2e_diags),
+                   "flux_squared": timed_est[-1]["flux_squared"] if timed_est else None,
+                   "n_patches": timed_est[-1]["n_patches"] if timed_est else None,
                    "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (mesh inputs %.0f MB, outputs K %d nnz, Hhat %d nnz)" % (h2d_bytes / 1e6, nnz_k, nnz_h)},
+                   "l2": "inputs larger than L2 (mesh inputs %.0f MB; K %d nnz, Hhat %d nnz)" % (h2d_bytes / 1e6, nnz_k,
+                                                                                               nnz_h)},
         "e2e": {"value": args.steps * n_dofs * world / e2e_elapsed, "unit": UNIT,
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
         "gpu_launches": launches,
         "roofline": {"kernel": "minres_spmv_K", "bound": "hbm", "achieved": spmv_achieved, "peak": peak, "unit": "GB/s",
                      "frac": spmv_achieved / peak, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": spmv_bytes, "traffic": None,
-                     "dominant_kernel": dominant[0],
-                     "assembly_gather_rows_fill": {"achieved": fill_achieved, "frac": fill_achieved / peak,
-                                                   "algorithmic_bytes_per_launch": fill_bytes / 7.0}},
-        "kernel_times_ms": {k: round(v[1] / args.steps, 4) for k, v in sorted(report.items(), key=lambda kv: -kv[1][1])},
+                     "algorithmic_bytes_per_launch": spmv_bytes, "launches_per_step": spmv_launches / args.steps,
+                     "traffic": None, "dominant_kernel": dominant[0],
+                     "dominant_share": dominant[1][1] / total_ms if total_ms else None},
+        "kernel_times_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in
+                                     sorted(report.items(), key=lambda kv: -kv[1][1])[:25]},
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
     }
