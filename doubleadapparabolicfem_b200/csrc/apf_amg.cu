@@ -292,50 +292,45 @@ namespace apf
             return r > 0.0 ? r : 1.0;
         }
 
-        // dense SPD inverse via Cholesky (host, coarsest level only); a: row-major, overwritten
-        void dense_spd_inverse(std::vector<double>& a, int n)
+        // coarsest operator scattered into a zeroed dense row-major n x n array (one thread per row)
+        __global__ void csr_to_dense(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                     const double* __restrict__ va, double* __restrict__ D)
         {
-            std::vector<double> L(a);
-            for (int j = 0; j < n; ++j)
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                    D[(long long)r * n + ci[k]] += va[k];
+        }
+
+        // One Gauss-Jordan exchange step on pivot k (B from A, out of place): after the steps
+        // k = 0..n-1 the array holds A^-1.  An SPD matrix needs no pivoting (every pivot is a
+        // diagonal entry of a Schur complement, hence positive); a pivot that is not positive
+        // and finite sets *status and the step leaves B = A.
+        __global__ void gauss_jordan_step(int n, int k, const double* __restrict__ A, double* __restrict__ B,
+                                          int* __restrict__ status)
+        {
+            const double p = A[(long long)k * n + k];
+            const bool ok = p > 0.0 && isfinite(p);
+            if (!ok && blockIdx.x == 0 && threadIdx.x == 0)
+                *status = 1;
+            const double ip = ok ? 1.0 / p : 0.0;
+            const long long total = (long long)n * n;
+            for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+                 t += (long long)gridDim.x * blockDim.x)
             {
-                double d = L[(size_t)j * n + j];
-                for (int k = 0; k < j; ++k)
-                    d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
-                if (!(d > 0.0))
-                    throw Error(APF_ERR_NUMERIC, "AMG coarsest operator is not positive definite");
-                d = std::sqrt(d);
-                L[(size_t)j * n + j] = d;
-                for (int i = j + 1; i < n; ++i)
-                {
-                    double v = L[(size_t)i * n + j];
-                    const double* li = &L[(size_t)i * n];
-                    const double* lj = &L[(size_t)j * n];
-                    for (int k = 0; k < j; ++k)
-                        v -= li[k] * lj[k];
-                    L[(size_t)i * n + j] = v / d;
-                }
-            }
-            std::vector<double> col(n);
-            for (int c = 0; c < n; ++c)
-            {
-                std::fill(col.begin(), col.end(), 0.0);
-                col[c] = 1.0;
-                for (int i = 0; i < n; ++i)
-                {
-                    double v = col[i];
-                    for (int k = 0; k < i; ++k)
-                        v -= L[(size_t)i * n + k] * col[k];
-                    col[i] = v / L[(size_t)i * n + i];
-                }
-                for (int i = n - 1; i >= 0; --i)
-                {
-                    double v = col[i];
-                    for (int k = i + 1; k < n; ++k)
-                        v -= L[(size_t)k * n + i] * col[k];
-                    col[i] = v / L[(size_t)i * n + i];
-                }
-                for (int i = 0; i < n; ++i)
-                    a[(size_t)i * n + c] = col[i];
+                const int i = static_cast<int>(t / n), j = static_cast<int>(t % n);
+                const double a = A[t];
+                double v;
+                if (!ok)
+                    v = a;
+                else if (i == k && j == k)
+                    v = ip;
+                else if (i == k)
+                    v = -a * ip;
+                else if (j == k)
+                    v = a * ip;
+                else
+                    v = a - A[(long long)i * n + k] * A[(long long)k * n + j] * ip;
+                B[t] = v;
             }
         }
     }
@@ -378,24 +373,36 @@ namespace apf
             }
             if (force_dense || n <= opt.coarse_size)
             {
-                std::vector<int> rp(n + 1), ci(Al.nnz());
-                std::vector<double> va(Al.nnz());
-                APF_CUDA(cudaMemcpyAsync(rp.data(), Al.row_ptr.get(), (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
-                if (Al.nnz())
+                // dense inverse on the device: scatter, then n Gauss-Jordan exchange steps
+                const std::size_t nn = static_cast<std::size_t>(n) * n;
+                coarse_inv_.allocate(nn, s);
+                coarse_inv_.zero();
+                DeviceBuffer<double> other(nn, s);
+                DeviceBuffer<int> status(1, s);
+                status.zero();
                 {
-                    APF_CUDA(cudaMemcpyAsync(ci.data(), Al.col_idx.get(), Al.nnz() * sizeof(int), cudaMemcpyDeviceToHost, s));
-                    APF_CUDA(cudaMemcpyAsync(va.data(), Al.values.get(), Al.nnz() * sizeof(double), cudaMemcpyDeviceToHost, s));
+                    APF_KERNEL("amg_coarse_dense", s);
+                    csr_to_dense<<<nblocks(n, 128), 128, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(),
+                                                                 coarse_inv_.get());
                 }
+                double* cur = coarse_inv_.get();
+                double* nxt = other.get();
+                const int gj_blocks = nblocks(static_cast<long long>(nn), 256, 148 * 8);
+                for (int k = 0; k < n; ++k)
+                {
+                    {
+                        APF_KERNEL("amg_coarse_gauss_jordan", s);
+                        gauss_jordan_step<<<gj_blocks, 256, 0, s>>>(n, k, cur, nxt, status.get());
+                    }
+                    std::swap(cur, nxt);
+                }
+                if (cur != coarse_inv_.get())
+                    APF_CUDA(cudaMemcpyAsync(coarse_inv_.get(), cur, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                APF_CUDA(cudaGetLastError());
+                int bad = 0;
+                APF_CUDA(cudaMemcpyAsync(&bad, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
                 sync(s);
-                std::vector<double> dense((size_t)n * n, 0.0);
-                for (int r = 0; r < n; ++r)
-                    for (int k = rp[r]; k < rp[r + 1]; ++k)
-                        dense[(size_t)r * n + ci[k]] += va[k];
-                dense_spd_inverse(dense, n);
-                coarse_inv_.allocate(dense.size(), s);
-                APF_CUDA(cudaMemcpyAsync(coarse_inv_.get(), dense.data(), dense.size() * sizeof(double),
-                                         cudaMemcpyHostToDevice, s));
-                sync(s);
+                require(bad == 0, APF_ERR_NUMERIC, "AMG coarsest operator is not positive definite");
                 n_coarse_ = n;
                 break;
             }

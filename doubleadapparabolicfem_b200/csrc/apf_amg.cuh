@@ -49,7 +49,7 @@ namespace apf
         int n_coarse_ = 0;
         bool jacobi_coarse_ = false;      // coarsest level smoothed only (too large for a dense solve)
         static constexpr int kCoarseSweeps = 8;
-        static constexpr int kMaxDense = 1500; // largest coarsest level inverted densely (host O(n^3))
+        static constexpr int kMaxDense = 1500; // largest coarsest level inverted densely (device Gauss-Jordan, n launches)
         AmgOptions opt_{};
     };
 }

@@ -255,6 +255,7 @@ int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs
     auto h = std::make_unique<apf_system>();
     h->ctx = ctx;
     const int rc = guarded(ctx, [&] {
+        APF_HOST_RANGE("call_assemble_main_system");
         apf::require(d->p == 1 || d->p == 2, APF_ERR_INVALID, "p must be 1 or 2");
         apf::require(d->n_y_cells >= 0 && d->n_x_cells >= 0 && d->n_lambda >= 0 && d->n_u >= 0, APF_ERR_INVALID,
                      "negative sizes");
@@ -299,7 +300,10 @@ int apf_assemble_graph_norm(apf_ctx* ctx, apf_system* sys, double diagonal_toler
 {
     if (!ctx || !sys)
         return APF_ERR_INVALID;
-    return guarded(ctx, [&] { apf::assemble_graph_norm(sys->sys, diagonal_tolerance); });
+    return guarded(ctx, [&] {
+        APF_HOST_RANGE("call_assemble_graph_norm");
+        apf::assemble_graph_norm(sys->sys, diagonal_tolerance);
+    });
 }
 
 int apf_system_block_info(const apf_system* sys, int block, int32_t* rows, int32_t* cols, int64_t* nnz)
@@ -386,6 +390,7 @@ namespace
         auto& S = h->sys;
         apf::require(S.have[APF_BLOCK_HHAT], APF_ERR_INVALID,
                      "ParabolicGraphNorm requires graph-norm block context from assembly (call apf_assemble_graph_norm)");
+        APF_HOST_RANGE("setup_preconditioner");
         const auto t0 = std::chrono::steady_clock::now();
         S.precond.reset();
         auto p = std::make_unique<apf::BlockPreconditioner>();
@@ -416,6 +421,7 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
     apf::MinresSummary summary;
     double solve_seconds = 0.0;
     int rc = guarded(ctx, [&] {
+        APF_HOST_RANGE("call_solve_minres");
         auto& S = sys->sys;
         cudaStream_t s = ctx->stream;
         apf::require(opt->tolerance >= 0.0, APF_ERR_INVALID, "negative tolerance");
@@ -507,6 +513,7 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
     if (!ctx || !sys || !y_vertex_ids)
         return APF_ERR_INVALID;
     return guarded(ctx, [&] {
+        APF_HOST_RANGE("call_estimate");
         auto& S = sys->sys;
         const std::size_t n = 3ull * static_cast<std::size_t>(S.in.n_y_cells);
         std::vector<int> vids(n);

@@ -13,9 +13,11 @@
 //
 // B200 design: the space-time patch operator is Mt (x) [A_x B_x^T 0; B_x 0 e^T; 0 e 0] for
 // cell-constant M on a slab, so after multiplying the right-hand side by Mt^-1 the problem
-// splits into one spatial system per time DOF sharing one matrix: a thread block assembles
-// that matrix (size ~ 7 x patch valence) in shared memory, factors it once (LU with
-// partial pivoting) and solves both time components.  Each patch writes its flux restricted
+// splits into one spatial system per time DOF sharing one matrix: one warp assembles that
+// matrix (size ~ 7 x patch valence) in its slice of shared memory from reference-cell
+// integral tables, factors it once (LU with partial pivoting) and solves both time
+// components; patches are sorted into size buckets so each launch sizes shared memory to
+// its largest patch.  Each patch writes its flux restricted
 // to each of its cells into the cell's slot of that patch's vertex (3 slots per triangle),
 // so the per-cell indicator kernel sums the slots in a fixed order: no atomics.
 #include <algorithm>
@@ -225,282 +227,314 @@ namespace apf
             int* status;
         };
 
-        // one thread block per patch
-        template<int NMAX>
-        __global__ void __launch_bounds__(128) patch_solve(PatchArgs A)
+        // Reference-cell integrals of the RT_1 basis against itself, its divergence and the
+        // barycentric functions (exact with the 16-point rule: polynomial degree <= 4).
+        struct PatchTables
         {
-            extern __shared__ double sm[];
-            double* K = sm;                         // NMAX x (NMAX + 2) augmented, row-major
-            const int LD = NMAX + 2;
-            __shared__ int s_piv;
-            __shared__ double s_pv[128];
-            __shared__ int s_pi[128];
-            const int tid = threadIdx.x;
-            for (int p = blockIdx.x; p < A.n_patches; p += gridDim.x)
+            double r00[8][8], r01[8][8], r11[8][8]; // int phi_j^a phi_l^b
+            double rd[8][3];                       // int div phi_l lambda_r
+            double rl[3][8][2];                    // int lambda_a phi_j^c
+            double mm[3][3];                       // int lambda_a lambda_r
+            double mmm[3][3][3];                   // int lambda_a lambda_s lambda_r
+        };
+        constexpr int kPatchTableDoubles = sizeof(PatchTables) / sizeof(double);
+
+        PatchTables make_patch_tables(const EstTables& t)
+        {
+            PatchTables p{};
+            for (int q = 0; q < t.nq; ++q)
             {
+                const double x = t.qp[q][0], y = t.qp[q][1], w = t.qw[q];
+                double v[8][2], d[8];
+                for (int j = 0; j < 8; ++j)
+                {
+                    const double* c = t.rt[j];
+                    v[j][0] = c[0] + c[1] * x + c[2] * y + c[6] * x * x + c[7] * x * y;
+                    v[j][1] = c[3] + c[4] * x + c[5] * y + c[6] * x * y + c[7] * y * y;
+                    d[j] = c[1] + c[5] + 3.0 * c[6] * x + 3.0 * c[7] * y;
+                }
+                const double l3[3] = {1.0 - x - y, x, y};
+                for (int j = 0; j < 8; ++j)
+                    for (int l = 0; l < 8; ++l)
+                    {
+                        p.r00[j][l] += w * v[j][0] * v[l][0];
+                        p.r01[j][l] += w * v[j][0] * v[l][1];
+                        p.r11[j][l] += w * v[j][1] * v[l][1];
+                    }
+                for (int l = 0; l < 8; ++l)
+                    for (int r = 0; r < 3; ++r)
+                        p.rd[l][r] += w * d[l] * l3[r];
+                for (int a = 0; a < 3; ++a)
+                    for (int j = 0; j < 8; ++j)
+                        for (int c = 0; c < 2; ++c)
+                            p.rl[a][j][c] += w * l3[a] * v[j][c];
+                for (int a = 0; a < 3; ++a)
+                    for (int r = 0; r < 3; ++r)
+                    {
+                        p.mm[a][r] += w * l3[a] * l3[r];
+                        for (int s2 = 0; s2 < 3; ++s2)
+                            p.mmm[a][s2][r] += w * l3[a] * l3[s2] * l3[r];
+                    }
+            }
+            return p;
+        }
+
+        // One warp per patch; the patch system (n rows, two right-hand-side columns at n and
+        // n + 1) lives in this warp's slice of shared memory with an odd row stride, so
+        // column walks (pivot search, back substitution) are free of bank conflicts.
+        //   assembly : lanes over the 113 local entries of each patch cell, from the
+        //              reference-cell tables (Piola map, cell-constant M);
+        //   LU       : partial pivoting by a warp arg-max, right-looking update with lanes
+        //              over columns, applied to both right-hand sides at once;
+        //   solve    : column-oriented back substitution, lanes over rows.
+        // Patches arrive sorted into size buckets; NMAX is the bucket's bound.
+        template<int NMAX>
+        __global__ void __launch_bounds__(32) patch_solve(PatchArgs A, const PatchTables* __restrict__ tables,
+                                                          const int* __restrict__ order, int count)
+        {
+            constexpr int LD = NMAX + 3; // odd: NMAX is even
+            extern __shared__ double sm[];
+            PatchTables& T = *reinterpret_cast<PatchTables*>(sm);
+            double* K = sm + kPatchTableDoubles + (kPatchTableDoubles & 1);
+            const int lane = threadIdx.x;
+            for (int i = lane; i < kPatchTableDoubles; i += 32)
+                sm[i] = reinterpret_cast<const double*>(tables)[i];
+            __syncwarp();
+            for (int idx = blockIdx.x; idx < count; idx += gridDim.x)
+            {
+                const int p = order[idx];
                 const int slab = A.patch_slab[p], tp = A.patch_topo[p];
                 const int cb = A.topo_ptr[tp], ce = A.topo_ptr[tp + 1], nc = ce - cb;
                 const int nfree = A.topo_nfree[tp];
                 const bool interior = A.topo_boundary[tp] == 0;
-                const int nf = 2 * nfree + 2 * nc, ns = 3 * nc;
-                const int n = nf + ns + (interior ? 1 : 0);
+                const int nf = 2 * nfree + 2 * nc;
+                const int n = nf + 3 * nc + (interior ? 1 : 0);
                 if (n > NMAX)
                 {
-                    if (tid == 0)
+                    if (lane == 0)
                         atomicExch(A.status, APF_ERR_CAPACITY);
                     continue;
                 }
-                for (int i = tid; i < NMAX * LD; i += blockDim.x)
+                const int sb = A.slab_ptr[slab];
+                for (int i = lane; i < n * LD; i += 32)
                     K[i] = 0.0;
-                __syncthreads();
+                __syncwarp();
+                double ht = 0.0;
                 for (int ic = 0; ic < nc; ++ic)
                 {
-                    const int c = A.slab_cells[A.slab_ptr[slab] + A.topo_cell[cb + ic]];
+                    const int c = A.slab_cells[sb + A.topo_cell[cb + ic]];
                     const int a = A.topo_center[cb + ic];
                     const Cell k = load_cell(A.geo, A.m, A.ell, c);
-                    // local dof -> (patch dof, coefficient)
+                    ht = k.ht;
+                    const double adet = fabs(k.det);
+                    // local dof -> patch dof and the coefficient of the physical basis:
+                    // phi_j = e_j J phi^_j, e_j = orientation x Piola sign / det
                     int pd[8];
-                    double cf[8];
-                    const double sdet = k.det < 0.0 ? -1.0 : 1.0;
-                    for (int e = 0; e < 3; ++e)
+                    double e[8];
+                    for (int ed = 0; ed < 3; ++ed)
                     {
-                        const int code = A.topo_edge[3 * (cb + ic) + e];
+                        const int code = A.topo_edge[3 * (cb + ic) + ed];
                         const int pe = code & 0xffff;
                         const double sp = (code >> 30) & 1 ? -1.0 : 1.0;
                         const bool free_edge = pe != 0xffff;
-                        const double sn = sdet * sp;
-                        pd[2 * e] = free_edge ? 2 * pe : -1;
-                        pd[2 * e + 1] = free_edge ? 2 * pe + 1 : -1;
-                        cf[2 * e] = sn;
-                        cf[2 * e + 1] = sn * sp;
+                        pd[2 * ed] = free_edge ? 2 * pe : -1;
+                        pd[2 * ed + 1] = free_edge ? 2 * pe + 1 : -1;
+                        e[2 * ed] = sp / k.det;     // (sdet sp) (sdet / det)
+                        e[2 * ed + 1] = 1.0 / k.det; // (sdet sp sp) (sdet / det)
                     }
                     pd[6] = 2 * nfree + 2 * ic;
                     pd[7] = 2 * nfree + 2 * ic + 1;
-                    cf[6] = cf[7] = 1.0;
+                    e[6] = e[7] = 1.0 / k.det;
                     const int sbase = nf + 3 * ic;
-                    // theta~ in time: W_s[k] = sum_b c_{s,b} ht Mtr[b][k]
+                    // S = J^T M^-1 J
+                    const double q00 = k.mi00 * k.J00 + k.mi01 * k.J10, q10 = k.mi01 * k.J00 + k.mi11 * k.J10;
+                    const double q01 = k.mi00 * k.J01 + k.mi01 * k.J11, q11 = k.mi01 * k.J01 + k.mi11 * k.J11;
+                    const double S00 = k.J00 * q00 + k.J10 * q10;
+                    const double S01 = k.J00 * q01 + k.J10 * q11;
+                    const double S11 = k.J01 * q01 + k.J11 * q11;
+                    // time-weighted gradients of theta~: gth[kk] = grad theta~ tested with time basis kk
                     const double* th = A.theta + 6ll * c;
                     const double* uu = A.u + 6ll * c;
-                    double gth[2][2]; // grad theta~ weighted against time basis k
+                    double gth[2][2];
                     for (int kk = 0; kk < 2; ++kk)
                     {
                         gth[kk][0] = gth[kk][1] = 0.0;
-                        for (int s = 0; s < 3; ++s)
+                        for (int s2 = 0; s2 < 3; ++s2)
                         {
-                            const double W = k.ht * ((kk == 0 ? 1.0 / 3.0 : 1.0 / 6.0) * th[2 * s] +
-                                                     (kk == 0 ? 1.0 / 6.0 : 1.0 / 3.0) * th[2 * s + 1]);
-                            gth[kk][0] += k.g[s][0] * W;
-                            gth[kk][1] += k.g[s][1] * W;
+                            const double W = k.ht * ((kk == 0 ? 1.0 / 3.0 : 1.0 / 6.0) * th[2 * s2] +
+                                                     (kk == 0 ? 1.0 / 6.0 : 1.0 / 3.0) * th[2 * s2 + 1]);
+                            gth[kk][0] += k.g[s2][0] * W;
+                            gth[kk][1] += k.g[s2][1] * W;
                         }
                     }
                     double du[3];
-                    for (int s = 0; s < 3; ++s)
-                        du[s] = (uu[2 * s + 1] - uu[2 * s]) / k.ht;
-                    const double adet = fabs(k.det);
-                    // entries: A_loc (64) + B_loc (24) + F_loc (16) + G_loc (6) + E (3)
-                    for (int t = tid; t < 113; t += blockDim.x)
+                    for (int s2 = 0; s2 < 3; ++s2)
+                        du[s2] = (uu[2 * s2 + 1] - uu[2 * s2]) / k.ht;
+                    for (int t = lane; t < 113; t += 32)
                     {
                         if (t < 64)
                         {
-                            const int j = t / 8, l = t % 8;
+                            const int j = t >> 3, l = t & 7;
                             if (pd[j] < 0 || pd[l] < 0)
                                 continue;
-                            double acc = 0.0;
-                            for (int q = 0; q < c_est.nq; ++q)
-                            {
-                                double ax, ay, ad, bx, by, bd;
-                                rt_phys(k, j, c_est.qp[q][0], c_est.qp[q][1], ax, ay, ad);
-                                rt_phys(k, l, c_est.qp[q][0], c_est.qp[q][1], bx, by, bd);
-                                acc += c_est.qw[q] * (ax * (k.mi00 * bx + k.mi01 * by) + ay * (k.mi01 * bx + k.mi11 * by));
-                            }
-                            K[pd[j] * LD + pd[l]] += cf[j] * cf[l] * acc * adet;
+                            const double r = S00 * T.r00[j][l] + S01 * (T.r01[j][l] + T.r01[l][j]) + S11 * T.r11[j][l];
+                            K[pd[j] * LD + pd[l]] += e[j] * e[l] * adet * r;
                         }
                         else if (t < 88)
                         {
-                            const int r = (t - 64) / 8, l = (t - 64) % 8;
+                            const int r = (t - 64) >> 3, l = (t - 64) & 7;
                             if (pd[l] < 0)
                                 continue;
-                            double acc = 0.0;
-                            for (int q = 0; q < c_est.nq; ++q)
-                            {
-                                double bx, by, bd;
-                                rt_phys(k, l, c_est.qp[q][0], c_est.qp[q][1], bx, by, bd);
-                                const double x = c_est.qp[q][0], y = c_est.qp[q][1];
-                                const double lam = r == 0 ? 1.0 - x - y : (r == 1 ? x : y);
-                                acc += c_est.qw[q] * bd * lam;
-                            }
-                            const double v = cf[l] * acc * adet;
+                            const double v = e[l] * adet * T.rd[l][r];
                             K[(sbase + r) * LD + pd[l]] += v;
                             K[pd[l] * LD + sbase + r] += v;
                         }
                         else if (t < 104)
                         {
-                            const int j = (t - 88) / 2, kk = (t - 88) % 2;
+                            const int j = (t - 88) >> 1, kk = (t - 88) & 1;
                             if (pd[j] < 0)
                                 continue;
-                            double acc = 0.0;
-                            for (int q = 0; q < c_est.nq; ++q)
-                            {
-                                double ax, ay, ad;
-                                rt_phys(k, j, c_est.qp[q][0], c_est.qp[q][1], ax, ay, ad);
-                                const double x = c_est.qp[q][0], y = c_est.qp[q][1];
-                                const double psi = a == 0 ? 1.0 - x - y : (a == 1 ? x : y);
-                                acc += c_est.qw[q] * psi * (gth[kk][0] * ax + gth[kk][1] * ay);
-                            }
-                            K[pd[j] * LD + NMAX + kk] += -cf[j] * acc * adet;
+                            const double gJ0 = gth[kk][0] * k.J00 + gth[kk][1] * k.J10;
+                            const double gJ1 = gth[kk][0] * k.J01 + gth[kk][1] * k.J11;
+                            K[pd[j] * LD + n + kk] += -e[j] * adet * (gJ0 * T.rl[a][j][0] + gJ1 * T.rl[a][j][1]);
                         }
                         else if (t < 110)
                         {
-                            const int r = (t - 104) / 2, kk = (t - 104) % 2;
-                            double acc = 0.0, lam_int = 0.0;
-                            for (int q = 0; q < c_est.nq; ++q)
-                            {
-                                const double x = c_est.qp[q][0], y = c_est.qp[q][1];
-                                const double l3[3] = {1.0 - x - y, x, y};
-                                const double dtu = l3[0] * du[0] + l3[1] * du[1] + l3[2] * du[2];
-                                acc += c_est.qw[q] * l3[a] * (k.ell - dtu) * l3[r];
-                                lam_int += c_est.qw[q] * l3[r];
-                            }
-                            // grad psi_a . M grad theta~_k
+                            const int r = (t - 104) >> 1, kk = (t - 104) & 1;
+                            double acc = k.ell * T.mm[a][r];
+                            for (int s2 = 0; s2 < 3; ++s2)
+                                acc -= du[s2] * T.mmm[a][s2][r];
                             const double mg0 = k.m00 * gth[kk][0] + k.m01 * gth[kk][1];
                             const double mg1 = k.m01 * gth[kk][0] + k.m11 * gth[kk][1];
                             const double gpm = k.g[a][0] * mg0 + k.g[a][1] * mg1;
-                            K[(sbase + r) * LD + NMAX + kk] += (0.5 * k.ht * acc - gpm * lam_int) * adet;
+                            K[(sbase + r) * LD + n + kk] += (0.5 * k.ht * acc - gpm / 6.0) * adet;
                         }
-                        else if (interior && t < 113)
+                        else if (interior)
                         {
+                            // mean-zero row: int_K lambda_r = |K| / 6 on the reference scale
                             const int r = t - 110;
-                            // mean-zero row: int_K lambda_r = |K| / 3
                             const double v = adet / 6.0;
                             K[(n - 1) * LD + sbase + r] += v;
                             K[(sbase + r) * LD + n - 1] += v;
                         }
                     }
-                    __syncthreads();
+                    __syncwarp();
                 }
                 // right-hand sides times Mt^-1 (Mt = ht [[1/3,1/6],[1/6,1/3]], inverse (1/ht) [[4,-2],[-2,4]])
+                for (int i = lane; i < n; i += 32)
                 {
-                    const int c0 = A.slab_cells[A.slab_ptr[slab] + A.topo_cell[cb]];
-                    const double ht = A.geo[8ll * c0 + 7] - A.geo[8ll * c0 + 6];
-                    for (int i = tid; i < n; i += blockDim.x)
-                    {
-                        const double b0 = K[i * LD + NMAX], b1 = K[i * LD + NMAX + 1];
-                        K[i * LD + NMAX] = (4.0 * b0 - 2.0 * b1) / ht;
-                        K[i * LD + NMAX + 1] = (-2.0 * b0 + 4.0 * b1) / ht;
-                    }
+                    const double b0 = K[i * LD + n], b1 = K[i * LD + n + 1];
+                    K[i * LD + n] = (4.0 * b0 - 2.0 * b1) / ht;
+                    K[i * LD + n + 1] = (-2.0 * b0 + 4.0 * b1) / ht;
                 }
-                __syncthreads();
-                // LU with partial pivoting on the augmented n x (n+2) system
+                __syncwarp();
+                // LU with partial pivoting on the augmented n x (n + 2) system
                 bool singular = false;
                 for (int col = 0; col < n; ++col)
                 {
                     double best = -1.0;
-                    int bi = col;
-                    for (int i = col + tid; i < n; i += blockDim.x)
+                    int bi = n;
+                    for (int i = col + lane; i < n; i += 32)
                     {
                         const double v = fabs(K[i * LD + col]);
-                        if (v > best) { best = v; bi = i; }
-                    }
-                    s_pv[tid] = best;
-                    s_pi[tid] = bi;
-                    __syncthreads();
-                    if (tid == 0)
-                    {
-                        double bv = -1.0;
-                        int b = col;
-                        for (int t = 0; t < (int)blockDim.x; ++t)
-                            if (s_pv[t] > bv || (s_pv[t] == bv && s_pi[t] < b)) { bv = s_pv[t]; b = s_pi[t]; }
-                        s_piv = b;
-                    }
-                    __syncthreads();
-                    const int pr = s_piv;
-                    if (pr != col)
-                    {
-                        for (int j = tid; j < n; j += blockDim.x)
+                        if (v > best)
                         {
-                            const double t0 = K[col * LD + j];
-                            K[col * LD + j] = K[pr * LD + j];
-                            K[pr * LD + j] = t0;
-                        }
-                        if (tid < 2)
-                        {
-                            const double t0 = K[col * LD + NMAX + tid];
-                            K[col * LD + NMAX + tid] = K[pr * LD + NMAX + tid];
-                            K[pr * LD + NMAX + tid] = t0;
+                            best = v;
+                            bi = i;
                         }
                     }
-                    __syncthreads();
-                    const double d = K[col * LD + col];
-                    if (!(d != 0.0) || !isfinite(d))
+                    for (int o = 16; o > 0; o >>= 1)
+                    {
+                        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+                        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                        if (ov > best || (ov == best && oi < bi))
+                        {
+                            best = ov;
+                            bi = oi;
+                        }
+                    }
+                    if (bi >= n || !(best > 0.0) || !isfinite(best))
                     {
                         singular = true;
                         break;
                     }
-                    const int rem = n - col - 1;
-                    for (int i = tid; i < rem; i += blockDim.x)
-                        K[(col + 1 + i) * LD + col] /= d;
-                    __syncthreads();
-                    const int w = rem + 2;
-                    for (int t = tid; t < rem * w; t += blockDim.x)
+                    if (bi != col)
+                        for (int j = col + lane; j < n + 2; j += 32)
+                        {
+                            const double t0 = K[col * LD + j];
+                            K[col * LD + j] = K[bi * LD + j];
+                            K[bi * LD + j] = t0;
+                        }
+                    __syncwarp();
+                    const double inv = 1.0 / K[col * LD + col];
+                    for (int j = col + 1 + lane; j < n + 2; j += 32)
                     {
-                        const int i = col + 1 + t / w, jj = t % w;
-                        const int j = jj < rem ? col + 1 + jj : NMAX + (jj - rem);
-                        K[i * LD + j] -= K[i * LD + col] * K[col * LD + j];
+                        const double u = K[col * LD + j] * inv;
+                        for (int i = col + 1; i < n; ++i)
+                            K[i * LD + j] -= K[i * LD + col] * u;
                     }
-                    __syncthreads();
+                    __syncwarp();
                 }
                 if (singular)
                 {
-                    if (tid == 0)
+                    if (lane == 0)
                         atomicExch(A.status, APF_ERR_NUMERIC);
-                    __syncthreads();
+                    __syncwarp();
                     continue;
                 }
-                // back substitution (two right-hand sides, one warp each)
-                if (tid < 64)
+                // back substitution, both right-hand sides, lanes over the rows above
+                for (int i = n - 1; i >= 0; --i)
                 {
-                    const int kk = tid >> 5, lane = tid & 31;
-                    for (int i = n - 1; i >= 0; --i)
+                    const double d = K[i * LD + i];
+                    const double x0 = K[i * LD + n] / d, x1 = K[i * LD + n + 1] / d;
+                    for (int r = lane; r < i; r += 32)
                     {
-                        double s = 0.0;
-                        for (int j = i + 1 + lane; j < n; j += 32)
-                            s += K[i * LD + j] * K[j * LD + NMAX + kk];
-                        for (int o = 16; o > 0; o >>= 1)
-                            s += __shfl_down_sync(0xffffffffu, s, o);
-                        if (lane == 0)
-                            K[i * LD + NMAX + kk] = (K[i * LD + NMAX + kk] - s) / K[i * LD + i];
-                        __syncwarp();
+                        const double kri = K[r * LD + i];
+                        K[r * LD + n] -= kri * x0;
+                        K[r * LD + n + 1] -= kri * x1;
+                    }
+                    __syncwarp();
+                    if (lane == 0)
+                    {
+                        K[i * LD + n] = x0;
+                        K[i * LD + n + 1] = x1;
                     }
                 }
-                __syncthreads();
+                __syncwarp();
                 // flux of this patch restricted to each of its cells -> slot of the patch vertex
-                for (int t = tid; t < nc * 16; t += blockDim.x)
+                for (int t = lane; t < nc * 16; t += 32)
                 {
-                    const int ic = t / 16, kk = (t % 16) / 8, j = t % 8;
-                    const int c = A.slab_cells[A.slab_ptr[slab] + A.topo_cell[cb + ic]];
+                    const int ic = t >> 4, kk = (t >> 3) & 1, j = t & 7;
+                    const int c = A.slab_cells[sb + A.topo_cell[cb + ic]];
                     const int a = A.topo_center[cb + ic];
                     double val = 0.0;
                     if (j < 6)
                     {
-                        const int e = j / 2, m = j % 2;
-                        const int code = A.topo_edge[3 * (cb + ic) + e];
+                        const int ed = j >> 1, m = j & 1;
+                        const int code = A.topo_edge[3 * (cb + ic) + ed];
                         const int pe = code & 0xffff;
                         if (pe != 0xffff)
                         {
                             const double sp = (code >> 30) & 1 ? -1.0 : 1.0;
-                            const double det = (A.geo[8ll * c + 2] - A.geo[8ll * c]) * (A.geo[8ll * c + 5] - A.geo[8ll * c + 1]) -
-                                               (A.geo[8ll * c + 4] - A.geo[8ll * c]) * (A.geo[8ll * c + 3] - A.geo[8ll * c + 1]);
+                            const double* g = A.geo + 8ll * c;
+                            const double det = (g[2] - g[0]) * (g[5] - g[1]) - (g[4] - g[0]) * (g[3] - g[1]);
                             const double sn = (det < 0.0 ? -1.0 : 1.0) * sp;
                             const double cfj = m == 0 ? sn : sn * sp;
-                            val = cfj * K[(2 * pe + m) * LD + NMAX + kk];
+                            val = cfj * K[(2 * pe + m) * LD + n + kk];
                         }
                     }
                     else
-                        val = K[(2 * nfree + 2 * ic + (j - 6)) * LD + NMAX + kk];
+                        val = K[(2 * nfree + 2 * ic + (j - 6)) * LD + n + kk];
                     A.sigma[((3ll * c + a) * 2 + kk) * 8 + j] = val;
                 }
-                __syncthreads();
+                __syncwarp();
             }
+        }
+
+        template<int NMAX>
+        constexpr std::size_t patch_smem_bytes()
+        {
+            return sizeof(double) * (kPatchTableDoubles + (kPatchTableDoubles & 1) + NMAX * (NMAX + 3));
         }
 
         struct IndicatorArgs
@@ -856,6 +890,7 @@ namespace apf
         int its = 0;
         if (bn > 0.0 && rn > 1e-14 * bn)
         {
+            APF_HOST_RANGE("est_reconstruction_pcg");
             S.precond->amg_a.apply(s, r.get(), z.get());
             copy(s, nl, z.get(), pv.get());
             double rz = dot_host(s, S.ws, nl, r.get(), z.get());
@@ -902,7 +937,10 @@ namespace apf
         APF_CUDA(cudaMemcpyAsync(geo.data(), in.y_geo.get(), geo.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         sync(s);
         PatchSet ps;
-        build_patches(geo, vids_host, ny, ps);
+        {
+            APF_HOST_RANGE("est_build_patches");
+            build_patches(geo, vids_host, ny, ps);
+        }
         tot.n_slabs = ps.n_slabs;
         tot.n_patches = static_cast<int>(ps.patch_slab.size());
         tot.max_patch_cells = ps.max_cells;
@@ -941,25 +979,56 @@ namespace apf
         pa.u = ucell.get();
         pa.sigma = sigma.get();
         pa.status = status.get();
-        const int nmax_needed = ps.max_n;
-        auto launch = [&](auto tag) {
+        // patches sorted into size buckets (one warp each; shared memory sized per bucket)
+        constexpr int kBuckets = 5;
+        static constexpr int kBucketMax[kBuckets] = {32, 48, 64, 96, 144};
+        std::vector<int> bucket_count(kBuckets + 1, 0), order(tot.n_patches);
+        {
+            std::vector<signed char> bucket_of(tot.n_patches);
+            for (int p = 0; p < tot.n_patches; ++p)
+            {
+                const int tp = ps.patch_topo[p];
+                const int nc = ps.topo_ptr[tp + 1] - ps.topo_ptr[tp];
+                const int n = 2 * ps.topo_nfree[tp] + 5 * nc + (ps.topo_boundary[tp] ? 0 : 1);
+                int b = 0;
+                while (b < kBuckets && n > kBucketMax[b])
+                    ++b;
+                require(b < kBuckets, APF_ERR_CAPACITY, "estimator: patch too large (more than 144 unknowns)");
+                bucket_of[p] = static_cast<signed char>(b);
+                ++bucket_count[b + 1];
+            }
+            for (int b = 0; b < kBuckets; ++b)
+                bucket_count[b + 1] += bucket_count[b];
+            std::vector<int> fill(bucket_count.begin(), bucket_count.end() - 1);
+            for (int p = 0; p < tot.n_patches; ++p)
+                order[fill[bucket_of[p]]++] = p;
+        }
+        DeviceBuffer<int> d_order(0, s);
+        up(d_order, order);
+        const PatchTables ptab = make_patch_tables(make_est_tables());
+        DeviceBuffer<double> d_ptab(kPatchTableDoubles, s);
+        d_ptab.upload(reinterpret_cast<const double*>(&ptab), kPatchTableDoubles);
+        const PatchTables* tables = reinterpret_cast<const PatchTables*>(d_ptab.get());
+        auto launch = [&](auto tag, int b) {
             constexpr int NMAX = decltype(tag)::value;
-            const size_t smem = sizeof(double) * NMAX * (NMAX + 2);
+            const int count = bucket_count[b + 1] - bucket_count[b];
+            if (count == 0)
+                return;
+            constexpr std::size_t smem = patch_smem_bytes<NMAX>();
             APF_CUDA(cudaFuncSetAttribute(patch_solve<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             pa.nmax = NMAX;
+            const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
+            const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32)));
             APF_KERNEL("est_patch_solve", s);
-            patch_solve<NMAX><<<std::max(1, std::min(tot.n_patches, 148 * 16)), 128, smem, s>>>(pa);
+            patch_solve<NMAX><<<grid, 32, smem, s>>>(pa, tables, d_order.get() + bucket_count[b], count);
         };
         if (tot.n_patches > 0)
         {
-            if (nmax_needed <= 64)
-                launch(std::integral_constant<int, 64>{});
-            else if (nmax_needed <= 96)
-                launch(std::integral_constant<int, 96>{});
-            else if (nmax_needed <= 144)
-                launch(std::integral_constant<int, 144>{});
-            else
-                throw Error(APF_ERR_CAPACITY, "estimator: patch too large (more than 16 cells around a vertex)");
+            launch(std::integral_constant<int, 32>{}, 0);
+            launch(std::integral_constant<int, 48>{}, 1);
+            launch(std::integral_constant<int, 64>{}, 2);
+            launch(std::integral_constant<int, 96>{}, 3);
+            launch(std::integral_constant<int, 144>{}, 4);
             APF_CUDA(cudaGetLastError());
         }
         int hstat = 0;

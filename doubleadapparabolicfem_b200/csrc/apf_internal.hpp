@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <map>
@@ -174,9 +175,41 @@ namespace apf
         bool on_ = false;
     };
 
+    // Host wall time of a stretch of host-side work (patch topology, set-up loops), recorded
+    // as "host:<name>" beside the kernel times when timing is on.
+    class HostRange
+    {
+    public:
+        explicit HostRange(const char* name) : name_(name)
+        {
+            if (t_profiler && t_profiler->enabled)
+            {
+                on_ = true;
+                t0_ = std::chrono::steady_clock::now();
+            }
+        }
+        ~HostRange()
+        {
+            if (on_)
+            {
+                const double ms =
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
+                auto& t = t_profiler->totals[std::string("host:") + name_];
+                t.first += 1;
+                t.second += ms;
+            }
+        }
+
+    private:
+        const char* name_;
+        bool on_ = false;
+        std::chrono::steady_clock::time_point t0_;
+    };
+
 #define APF_KT_CAT2(a, b) a##b
 #define APF_KT_CAT(a, b) APF_KT_CAT2(a, b)
 #define APF_KERNEL(name, stream) ::apf::KernelTimer APF_KT_CAT(apf_kt_, __LINE__)(name, stream)
+#define APF_HOST_RANGE(name) ::apf::HostRange APF_KT_CAT(apf_hr_, __LINE__)(name)
 
     // Exclusive scan of n int32 counts into out[0..n] (out[n] = total); returns the total.
     long long exclusive_scan(const int* counts, int* out, int n, cudaStream_t s);
