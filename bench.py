@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-estimator", action="store_true")
     ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--precond", default="learned", choices=["learned", "plain"],
+                    help="learned: the shipped model (plain block preconditioner as fallback), timed beside plain")
     return ap.parse_args()
 
 
@@ -237,6 +239,12 @@ def run_ours(args, world, rank, local):
     sopt = _lib.SolverOptions()
     lib.apf_solver_options_default(C.byref(sopt))
     sopt.tolerance = args.tol
+    from doubleadapparabolicfem_b200 import learned as LM
+    learned_model = None
+    if args.precond == "learned" and os.path.exists(LM.DEFAULT_WEIGHTS):
+        learned_model = LM.LearnedModel.load()
+        LM.use_model(ctx, learned_model)
+        sopt.preconditioner = _lib.APF_PRECOND_LEARNED
     solve_diags = []
     est_results = []
 
@@ -298,6 +306,29 @@ def run_ours(args, world, rank, local):
     elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     timed_diags = solve_diags[-args.steps:]
     timed_est = est_results[-args.steps:]
+
+    # the plain block preconditioner on the same steps, for the learned-vs-plain comparison
+    plain = None
+    if sopt.preconditioner == _lib.APF_PRECOND_LEARNED:
+        sopt.preconditioner = _lib.APF_PRECOND_AMG_BLOCK
+        lib.apf_system_destroy(step(dprob, True))
+        barrier()
+        torch.cuda.synchronize(dev)
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            lib.apf_system_destroy(step(dprob, True))
+        p1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        plain_elapsed = max_over_ranks(p0.elapsed_time(p1) / 1e3)
+        pd = solve_diags[-args.steps:]
+        plain = {"value": args.steps * n_dofs * world / plain_elapsed, "ms_per_step": 1e3 * plain_elapsed / args.steps,
+                 "minres_iterations": [d["iterations"] for d in pd],
+                 "final_true_residual_max": max(d["final_true_residual"] for d in pd),
+                 "minres_solve_s_mean": sum(d["solve_seconds"] for d in pd) / len(pd)}
+        sopt.preconditioner = _lib.APF_PRECOND_LEARNED
 
     # e2e through the C ABI from pinned host buffers
     barrier()
@@ -365,7 +396,12 @@ def run_ours(args, world, rank, local):
                    "stages": ["assembly", "graph_norm", "amg_setup", "minres"] +
                              (["slab_reconstruction", "patch_fluxes", "indicators"] if run_estimator else []),
                    "tolerance": args.tol,
-                   "preconditioner": "plain: blkdiag(A_y, Hhat) by SA-AMG V-cycles",
+                   "preconditioner": ("learned smoother weights in the blkdiag(A_y, Hhat) SA-AMG V-cycles "
+                                      "(plain fallback)" if plain else
+                                      "plain: blkdiag(A_y, Hhat) by SA-AMG V-cycles"),
+                   "learned_fallbacks": sum(d["learned_fallback"] for d in timed_diags),
+                   "minres_solve_s_mean": sum(d["solve_seconds"] for d in timed_diags) / len(timed_diags),
+                   "plain_preconditioner": plain,
                    "minres_iterations": [d["iterations"] for d in timed_diags],
                    "final_true_residual_max": max(d["final_true_residual"] for d in timed_diags),
                    "e2e_final_true_residual_max": max(d["final_true_residual"] for d in e2e_diags),

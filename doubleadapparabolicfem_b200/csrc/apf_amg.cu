@@ -522,6 +522,20 @@ namespace apf
                 C.comp = std::move(comp_c);
             sync(s);
         }
+        // sliced-ELLPACK copies for the V-cycle SpMVs (level 0's operator belongs to the
+        // caller, which builds its own)
+        for (std::size_t l = 0; l < levels_.size(); ++l)
+        {
+            AmgLevel& L = levels_[l];
+            if (l > 0 && !(l + 1 == levels_.size() && !jacobi_coarse_))
+                build_sell(s, L.A_own);
+            if (L.P.rows)
+            {
+                build_sell(s, L.P);
+                build_sell(s, L.R);
+            }
+        }
+        sync(s);
     }
 
     long long Amg::operator_nnz() const
@@ -553,26 +567,54 @@ namespace apf
             return;
         }
         const int pre = coarsest ? kCoarseSweeps : opt_.smooth_steps;
+        const int post = coarsest ? 0 : opt_.smooth_steps;
+        // smoother weights: omega D^-1 (plain) or the level's per-row weights
+        const bool own = L.w.size() != 0;
+        const double* wv = own ? L.w.get() : L.dinv.get();
+        const double om = own ? 1.0 : L.omega;
+        // the iterate alternates between x and the level's scratch t; starting in the right
+        // one makes the last of the pre + post smoothing writes land in x (no copies)
+        double* cur = (pre + post) % 2 == 1 ? x : L.t.get();
+        double* other = cur == x ? L.t.get() : x;
         {
             APF_KERNEL("amg_jacobi_first", s);
-            jacobi_first<<<nblocks(n, 256), 256, 0, s>>>(n, b, L.dinv.get(), L.omega, x);
+            jacobi_first<<<nblocks(n, 256), 256, 0, s>>>(n, b, wv, om, cur);
         }
         for (int k = 1; k < pre; ++k)
         {
-            jacobi_sweep(s, A, x, b, L.dinv.get(), L.omega, L.t.get());
-            copy(s, n, L.t.get(), x);
+            jacobi_sweep(s, A, cur, b, wv, om, other);
+            std::swap(cur, other);
         }
         if (coarsest)
             return;
-        residual(s, A, x, b, L.r.get());
+        residual(s, A, cur, b, L.r.get());
         AmgLevel& C = levels_[static_cast<std::size_t>(l) + 1];
         spmv(s, L.R, L.r.get(), C.b.get());
         vcycle(s, l + 1, C.b.get(), C.x.get());
-        spmv(s, L.P, C.x.get(), x, 1.0, 1.0);
-        for (int k = 0; k < opt_.smooth_steps; ++k)
+        spmv(s, L.P, C.x.get(), cur, L.alpha, 1.0);
+        for (int k = 0; k < post; ++k)
         {
-            jacobi_sweep(s, A, x, b, L.dinv.get(), L.omega, L.t.get());
-            copy(s, n, L.t.get(), x);
+            jacobi_sweep(s, A, cur, b, wv, om, other);
+            std::swap(cur, other);
+        }
+    }
+
+    void Amg::set_smoother(int l, DeviceBuffer<double>&& w, double alpha)
+    {
+        require(l >= 0 && l < levels(), APF_ERR_INVALID, "AMG: no such level");
+        AmgLevel& L = levels_[static_cast<std::size_t>(l)];
+        require(w.size() == 0 || w.size() == static_cast<std::size_t>(L.A->rows), APF_ERR_INVALID,
+                "AMG: smoother weights of the wrong size");
+        L.w = std::move(w);
+        L.alpha = alpha;
+    }
+
+    void Amg::reset_smoothers()
+    {
+        for (auto& L : levels_)
+        {
+            L.w.release();
+            L.alpha = 1.0;
         }
     }
 

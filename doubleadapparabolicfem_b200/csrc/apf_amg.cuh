@@ -12,7 +12,7 @@ namespace apf
     struct AmgOptions
     {
         double strength = 0.08;   // strong: |a_ij| >= strength * sqrt(a_ii a_jj)
-        int smooth_steps = 1;     // damped-Jacobi sweeps before and after the coarse correction
+        int smooth_steps = 2;     // damped-Jacobi sweeps before and after the coarse correction
         int coarse_size = 1024;   // dense solve at or below this size
         int max_levels = 20;
     };
@@ -27,6 +27,8 @@ namespace apf
         double omega = 0.0;           // Jacobi damping 4 / (3 rho(D^-1 A))
         DeviceBuffer<int> comp;       // component of each unknown (empty: one component)
         DeviceBuffer<double> x, b, r, t;
+        DeviceBuffer<double> w;       // per-row smoother weights replacing omega D^-1 (empty: plain)
+        double alpha = 1.0;           // coarse-correction scale
     };
 
     class Amg
@@ -41,6 +43,21 @@ namespace apf
         int levels() const { return static_cast<int>(levels_.size()); }
         long long operator_nnz() const;
         std::vector<int> level_rows() const;
+        // level access for the learned smoother weights and their training
+        AmgLevel& level(int l) { return levels_[static_cast<std::size_t>(l)]; }
+        const AmgLevel& level(int l) const { return levels_[static_cast<std::size_t>(l)]; }
+        bool dense_coarse() const { return !jacobi_coarse_; }
+        int smooth_steps() const { return opt_.smooth_steps; }
+        const double* coarse_inverse() const { return coarse_inv_.get(); }
+        static constexpr int coarse_sweeps() { return kCoarseSweeps; }
+        // Replace level l's Jacobi weights omega D^-1 by the per-row weights w (device, moved
+        // in) and scale its coarse correction by alpha; both keep the V-cycle symmetric.
+        void set_smoother(int l, DeviceBuffer<double>&& w, double alpha);
+        // back to omega D^-1 and alpha = 1 on every level
+        void reset_smoothers();
+        // x = the coarsest level's solve of b (dense inverse or fixed Jacobi sweeps; a
+        // symmetric linear map)
+        void coarse_apply(cudaStream_t s, const double* b, double* x) { vcycle(s, levels() - 1, b, x); }
 
     private:
         void vcycle(cudaStream_t s, int l, const double* b, double* x);

@@ -5,10 +5,12 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <new>
 #include <string>
 
 #include "apf_internal.hpp"
 #include "apf_estimator.cuh"
+#include "apf_learned.cuh"
 #include "apf_system.hpp"
 
 struct apf_ctx
@@ -19,6 +21,13 @@ struct apf_ctx
     std::string last_error;
     apf::Profiler profiler;
     std::string report;
+    std::unique_ptr<apf::LearnedModel> learned; // model of APF_PRECOND_LEARNED set-ups
+    unsigned long long learned_version = 0;
+};
+
+struct apf_learned_model
+{
+    apf::LearnedModel model;
 };
 
 struct apf_system
@@ -369,7 +378,7 @@ void apf_solver_options_default(apf_solver_options* opt)
     opt->use_true_residual_batching = 1;
     opt->true_residual_check_interval = 100;
     opt->preconditioner = APF_PRECOND_AMG_BLOCK;
-    opt->amg_smooth_steps = 1;
+    opt->amg_smooth_steps = 2;
     opt->amg_strength = 0.08;
     opt->amg_coarse_size = 256;
 }
@@ -385,6 +394,30 @@ namespace
         return a;
     }
 
+    // smoother weights of the set-up hierarchy: plain omega D^-1, or the learned model's
+    void install_smoothers(apf_ctx* ctx, apf::System& S, int kind)
+    {
+        apf::require(kind == APF_PRECOND_AMG_BLOCK || kind == APF_PRECOND_LEARNED, APF_ERR_INVALID,
+                     "unknown preconditioner");
+        if (kind == APF_PRECOND_LEARNED)
+        {
+            apf::require(ctx->learned != nullptr, APF_ERR_INVALID,
+                         "APF_PRECOND_LEARNED needs a model (apf_ctx_set_learned_model)");
+            if (S.precond_kind == APF_PRECOND_LEARNED && S.precond_model_version == ctx->learned_version)
+                return;
+            APF_HOST_RANGE("learned_install");
+            apf::apply_learned_smoothers(ctx->stream, *ctx->learned, S.precond->amg_a, 0);
+            apf::apply_learned_smoothers(ctx->stream, *ctx->learned, S.precond->amg_h, 1);
+            S.precond_model_version = ctx->learned_version;
+        }
+        else if (S.precond_kind != APF_PRECOND_AMG_BLOCK)
+        {
+            S.precond->amg_a.reset_smoothers();
+            S.precond->amg_h.reset_smoothers();
+        }
+        S.precond_kind = kind;
+    }
+
     void setup_precond(apf_ctx* ctx, apf_system* h, const apf_solver_options* opt)
     {
         auto& S = h->sys;
@@ -395,6 +428,8 @@ namespace
         S.precond.reset();
         auto p = std::make_unique<apf::BlockPreconditioner>();
         S.precond_opts = amg_options(opt);
+        if (!S.blocks[APF_BLOCK_A_Y].sell)
+            apf::build_sell(ctx->stream, S.blocks[APF_BLOCK_A_Y]);
         apf::DeviceBuffer<int> y_comp, x_comp;
         apf::dof_time_components(ctx->stream, S.in, true, y_comp);
         apf::dof_time_components(ctx->stream, S.in, false, x_comp);
@@ -402,6 +437,8 @@ namespace
                  x_comp.get());
         apf::sync(ctx->stream);
         S.precond = std::move(p); // only a fully set-up preconditioner is kept
+        S.precond_kind = APF_PRECOND_AMG_BLOCK;
+        install_smoothers(ctx, S, opt->preconditioner);
         S.precond_setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
 }
@@ -420,6 +457,7 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
         return APF_ERR_INVALID;
     apf::MinresSummary summary;
     double solve_seconds = 0.0;
+    int used = -1, fallback = 0;
     int rc = guarded(ctx, [&] {
         APF_HOST_RANGE("call_solve_minres");
         auto& S = sys->sys;
@@ -427,6 +465,8 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
         apf::require(opt->tolerance >= 0.0, APF_ERR_INVALID, "negative tolerance");
         if (!S.precond)
             setup_precond(ctx, sys, opt);
+        else
+            install_smoothers(ctx, S, opt->preconditioner);
         const int nl = S.in.n_lambda, nu = S.in.n_u, n = nl + nu;
         S.rhs.allocate(n, s);
         apf::copy(s, nl, S.f.get(), S.rhs.get());
@@ -437,12 +477,27 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
                                      pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
         else
             apf::fill(s, n, 0.0, S.solution.get());
+        if (!S.blocks[APF_BLOCK_K].sell)
+            apf::build_sell(s, S.blocks[APF_BLOCK_K]);
         apf::MinresOptions mo;
         mo.tolerance = opt->tolerance;
         mo.max_iterations = opt->max_iterations;
         mo.batch = opt->use_true_residual_batching ? opt->true_residual_check_interval : opt->max_iterations;
         const auto t0 = std::chrono::steady_clock::now();
         summary = apf::minres_solve(s, S.blocks[APF_BLOCK_K], *S.precond, S.rhs.get(), S.solution.get(), mo, S.ws);
+        used = S.precond_kind;
+        if (!summary.converged && S.precond_kind == APF_PRECOND_LEARNED)
+        {
+            // the plain block preconditioner is the fallback: a fresh run from the learned
+            // run's iterate
+            install_smoothers(ctx, S, APF_PRECOND_AMG_BLOCK);
+            const apf::MinresSummary first = summary;
+            summary = apf::minres_solve(s, S.blocks[APF_BLOCK_K], *S.precond, S.rhs.get(), S.solution.get(), mo, S.ws);
+            summary.iterations += first.iterations;
+            summary.batches += first.batches;
+            used = APF_PRECOND_AMG_BLOCK;
+            fallback = 1;
+        }
         solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (solution)
             APF_CUDA(cudaMemcpyAsync(solution, S.solution.get(), n * sizeof(double),
@@ -460,6 +515,8 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
         diag->final_true_residual = summary.true_residual;
         diag->setup_seconds = sys->sys.precond_setup_seconds;
         diag->solve_seconds = solve_seconds;
+        diag->preconditioner_used = used;
+        diag->learned_fallback = fallback;
         if (sys->sys.precond)
         {
             diag->amg_levels_lambda = sys->sys.precond->amg_a.levels();
@@ -571,3 +628,209 @@ void apf_system_destroy(apf_system* sys)
 }
 
 } // extern "C"
+
+// ---- learned preconditioner ----------------------------------------------------------
+
+int apf_learned_model_create(apf_learned_model** out)
+{
+    if (!out)
+        return APF_ERR_INVALID;
+    *out = new (std::nothrow) apf_learned_model();
+    return *out ? APF_OK : APF_ERR_INTERNAL;
+}
+
+int apf_learned_model_destroy(apf_learned_model* model)
+{
+    delete model;
+    return APF_OK;
+}
+
+int apf_learned_model_set_params(apf_learned_model* model, const float* params, int n)
+{
+    if (!model || !params || n != apf::learned::kParams)
+        return APF_ERR_INVALID;
+    std::memcpy(model->model.params.data(), params, sizeof(float) * n);
+    return APF_OK;
+}
+
+int apf_learned_model_get_params(const apf_learned_model* model, float* params, int n)
+{
+    if (!model || !params || n != apf::learned::kParams)
+        return APF_ERR_INVALID;
+    std::memcpy(params, model->model.params.data(), sizeof(float) * n);
+    return APF_OK;
+}
+
+int apf_ctx_set_learned_model(apf_ctx* ctx, const apf_learned_model* model)
+{
+    if (!ctx)
+        return APF_ERR_INVALID;
+    if (model)
+        ctx->learned = std::make_unique<apf::LearnedModel>(model->model);
+    else
+        ctx->learned.reset();
+    ++ctx->learned_version;
+    return APF_OK;
+}
+
+int apf_learned_loss_and_grad(apf_ctx* ctx, apf_system* sys, const apf_learned_model* model, int samples, int steps,
+                              uint64_t seed, const double* start_vectors, int pointers_on_device, double* loss,
+                              float* grad)
+{
+    if (!ctx || !sys || !model)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        auto& S = sys->sys;
+        apf::require(S.precond != nullptr, APF_ERR_INVALID, "learned loss: set up the preconditioner first");
+        cudaStream_t s = ctx->stream;
+        const long long n = static_cast<long long>(S.in.n_lambda) + S.in.n_u;
+        apf::DeviceBuffer<double> starts;
+        const double* sv = nullptr;
+        if (start_vectors)
+        {
+            if (pointers_on_device)
+                sv = start_vectors;
+            else
+            {
+                starts.allocate(static_cast<std::size_t>(n) * std::max(1, samples), s);
+                starts.upload(start_vectors, static_cast<std::size_t>(n) * std::max(1, samples));
+                sv = starts.get();
+            }
+        }
+        const double L = apf::learned_loss_and_grad(s, model->model, *S.precond, S.blocks[APF_BLOCK_A_Y],
+                                                     S.blocks[APF_BLOCK_HHAT], samples, steps, seed, sv, grad, S.ws);
+        apf::sync(s);
+        S.precond_kind = -2; // FP32-model weights installed: the next solve re-installs
+        if (loss)
+            *loss = L;
+    });
+}
+
+int apf_learned_forward(apf_ctx* ctx, const apf_learned_model* model, int n, const float* features, float* y,
+                        int precision, int pointers_on_device)
+{
+    if (!ctx || !model || n < 0 || (n > 0 && (!features || !y)) || (precision != 0 && precision != 1))
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        cudaStream_t s = ctx->stream;
+        apf::DeviceBuffer<float> dp(apf::learned::kParams, s);
+        dp.upload(model->model.params.data(), apf::learned::kParams);
+        apf::DeviceBuffer<float> f, out;
+        const float* fp = features;
+        float* yp = y;
+        if (!pointers_on_device)
+        {
+            f.allocate(static_cast<std::size_t>(n) * apf::learned::kFeatures, s);
+            f.upload(features, static_cast<std::size_t>(n) * apf::learned::kFeatures);
+            out.allocate(n, s);
+            fp = f.get();
+            yp = out.get();
+        }
+        apf::learned_forward(s, dp.get(), n, fp, yp, precision);
+        if (!pointers_on_device && n > 0)
+            APF_CUDA(cudaMemcpyAsync(y, out.get(), n * sizeof(float), cudaMemcpyDeviceToHost, s));
+        apf::sync(s);
+    });
+}
+
+namespace
+{
+    apf::Amg& amg_of(apf_system* sys, int block)
+    {
+        auto& S = sys->sys;
+        apf::require(S.precond != nullptr, APF_ERR_INVALID, "no preconditioner set up");
+        apf::require(block == 0 || block == 1, APF_ERR_INVALID, "block must be 0 (A_y) or 1 (Hhat)");
+        return block == 0 ? S.precond->amg_a : S.precond->amg_h;
+    }
+
+    apf::AmgLevel& level_of(apf_system* sys, int block, int level)
+    {
+        apf::Amg& amg = amg_of(sys, block);
+        apf::require(level >= 0 && level < amg.levels(), APF_ERR_INVALID, "no such AMG level");
+        return amg.level(level);
+    }
+}
+
+int apf_amg_info(apf_ctx* ctx, apf_system* sys, int block, int* levels, int* dense_coarse, int* coarse_sweeps,
+                 int* smooth_steps)
+{
+    if (!ctx || !sys)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        apf::Amg& amg = amg_of(sys, block);
+        if (levels) *levels = amg.levels();
+        if (dense_coarse) *dense_coarse = amg.dense_coarse() ? 1 : 0;
+        if (coarse_sweeps) *coarse_sweeps = apf::Amg::coarse_sweeps();
+        if (smooth_steps) *smooth_steps = sys->sys.precond_opts.smooth_steps;
+    });
+}
+
+int apf_amg_level_info(apf_ctx* ctx, apf_system* sys, int block, int level, int* rows, int64_t* nnz_a,
+                       int64_t* nnz_p, double* omega, double* alpha)
+{
+    if (!ctx || !sys)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        apf::AmgLevel& L = level_of(sys, block, level);
+        if (rows) *rows = L.A->rows;
+        if (nnz_a) *nnz_a = L.A->nnz();
+        if (nnz_p) *nnz_p = L.P.nnz();
+        if (omega) *omega = L.omega;
+        if (alpha) *alpha = L.alpha;
+    });
+}
+
+int apf_amg_level_copy(apf_ctx* ctx, apf_system* sys, int block, int level, int which, int32_t* row_ptr,
+                       int32_t* col_idx, double* values)
+{
+    if (!ctx || !sys || (which != 0 && which != 1))
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        apf::AmgLevel& L = level_of(sys, block, level);
+        const apf::DeviceCsr& M = which == 0 ? *L.A : L.P;
+        cudaStream_t s = ctx->stream;
+        if (row_ptr && M.row_ptr.size())
+            APF_CUDA(cudaMemcpyAsync(row_ptr, M.row_ptr.get(), M.row_ptr.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (col_idx && M.nnz())
+            APF_CUDA(cudaMemcpyAsync(col_idx, M.col_idx.get(), M.nnz() * sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (values && M.nnz())
+            APF_CUDA(cudaMemcpyAsync(values, M.values.get(), M.nnz() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        apf::sync(s);
+    });
+}
+
+int apf_amg_level_weights(apf_ctx* ctx, apf_system* sys, int block, int level, double* weights)
+{
+    if (!ctx || !sys || !weights)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        apf::AmgLevel& L = level_of(sys, block, level);
+        cudaStream_t s = ctx->stream;
+        const int n = L.A->rows;
+        if (L.w.size())
+            APF_CUDA(cudaMemcpyAsync(weights, L.w.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        else
+        {
+            apf::DeviceBuffer<double> t(n, s);
+            apf::axpby(s, n, L.omega, L.dinv.get(), 0.0, t.get());
+            APF_CUDA(cudaMemcpyAsync(weights, t.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        apf::sync(s);
+    });
+}
+
+int apf_amg_level_features(apf_ctx* ctx, apf_system* sys, int block, int level, float* features)
+{
+    if (!ctx || !sys || !features)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        apf::AmgLevel& L = level_of(sys, block, level);
+        cudaStream_t s = ctx->stream;
+        const int n = L.A->rows;
+        apf::DeviceBuffer<float> f(static_cast<std::size_t>(n) * apf::learned::kFeatures, s);
+        apf::learned_features(s, *L.A, L.dinv.get(), level, block, f.get());
+        if (n)
+            APF_CUDA(cudaMemcpyAsync(features, f.get(), f.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+        apf::sync(s);
+    });
+}

@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -98,7 +99,20 @@ namespace apf
         cudaStream_t s_ = nullptr;
     };
 
+    // Sliced-ELLPACK copy of a CSR matrix for the SpMV: slices of 32 consecutive rows, each
+    // slice stored column-major at its own width (one thread per row, coalesced loads),
+    // padding entries have value 0 and column 0.
+    struct DeviceSell
+    {
+        int slices = 0;
+        DeviceBuffer<int> slice_ptr; // slices + 1 element offsets
+        DeviceBuffer<int> col;
+        DeviceBuffer<double> val;
+    };
+
     // Row-compressed sparse matrix resident on the device (int32 indices, f64 values).
+    // `sell`, when built (build_sell), is used by the SpMV kernels instead of the CSR arrays;
+    // it must be rebuilt if the values change.
     struct DeviceCsr
     {
         int rows = 0;
@@ -106,6 +120,7 @@ namespace apf
         DeviceBuffer<int> row_ptr;
         DeviceBuffer<int> col_idx;
         DeviceBuffer<double> values;
+        std::unique_ptr<DeviceSell> sell;
         std::int64_t nnz() const noexcept { return static_cast<std::int64_t>(col_idx.size()); }
     };
 

@@ -291,6 +291,7 @@ namespace apf
             drop_fill<<<blocks, 256, 0, s>>>(n, Hhat.row_ptr.get(), Hhat.col_idx.get(), Hhat.values.get(), kHhatDrop,
                                             hhat_f.row_ptr.get(), hhat_f.col_idx.get(), hhat_f.values.get());
         }
+        build_sell(s, hhat_f);
         amg_h.setup(s, hhat_f, opt, w, x_component);
     }
 

@@ -53,6 +53,86 @@ namespace apf
             }
         }
 
+        // SELL-32 SpMV: one thread per row, one warp per slice (same MODEs as spmv_kernel)
+        template<int MODE>
+        __global__ void __launch_bounds__(256) sell_kernel(int rows, int slices, const int* __restrict__ sp,
+                                                           const int* __restrict__ col, const double* __restrict__ val,
+                                                           const double* __restrict__ x, const double* __restrict__ b,
+                                                           double* __restrict__ y, double alpha, double beta,
+                                                           const double* __restrict__ dinv)
+        {
+            const int lane = threadIdx.x & 31;
+            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            const int nwarps = (gridDim.x * blockDim.x) >> 5;
+            for (int sl = warp; sl < slices; sl += nwarps)
+            {
+                const int base = sp[sl];
+                const int width = (sp[sl + 1] - base) >> 5;
+                const double* v = val + base + lane;
+                const int* c = col + base + lane;
+                double s0 = 0.0, s1 = 0.0;
+                int j = 0;
+                for (; j + 1 < width; j += 2)
+                {
+                    s0 += v[32 * j] * __ldg(x + c[32 * j]);
+                    s1 += v[32 * j + 32] * __ldg(x + c[32 * j + 32]);
+                }
+                if (j < width)
+                    s0 += v[32 * j] * __ldg(x + c[32 * j]);
+                const double sum = s0 + s1;
+                const int r = sl * 32 + lane;
+                if (r < rows)
+                {
+                    if (MODE == 1)
+                        y[r] = b[r] - sum;
+                    else if (MODE == 2)
+                        y[r] = x[r] + alpha * dinv[r] * (b[r] - sum);
+                    else
+                        y[r] = beta == 0.0 ? alpha * sum : alpha * sum + beta * y[r];
+                }
+            }
+        }
+
+        // slice widths x 32 (element counts per slice)
+        __global__ void sell_count(int rows, int slices, const int* __restrict__ rp, int* __restrict__ cnt)
+        {
+            const int lane = threadIdx.x & 31;
+            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            const int nwarps = (gridDim.x * blockDim.x) >> 5;
+            for (int sl = warp; sl < slices; sl += nwarps)
+            {
+                const int r = sl * 32 + lane;
+                int len = r < rows ? rp[r + 1] - rp[r] : 0;
+                for (int o = 16; o > 0; o >>= 1)
+                    len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
+                if (lane == 0)
+                    cnt[sl] = 32 * len;
+            }
+        }
+
+        __global__ void sell_fill(int rows, int slices, const int* __restrict__ rp, const int* __restrict__ ci,
+                                  const double* __restrict__ va, const int* __restrict__ sp, int* __restrict__ col,
+                                  double* __restrict__ val)
+        {
+            const int lane = threadIdx.x & 31;
+            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            const int nwarps = (gridDim.x * blockDim.x) >> 5;
+            for (int sl = warp; sl < slices; sl += nwarps)
+            {
+                const int base = sp[sl];
+                const int width = (sp[sl + 1] - base) >> 5;
+                const int r = sl * 32 + lane;
+                const int b = r < rows ? rp[r] : 0;
+                const int len = r < rows ? rp[r + 1] - b : 0;
+                for (int j = 0; j < width; ++j)
+                {
+                    const int o = base + 32 * j + lane;
+                    col[o] = j < len ? ci[b + j] : 0;
+                    val[o] = j < len ? va[b + j] : 0.0;
+                }
+            }
+        }
+
         __global__ void dot_partials(int n, const double* __restrict__ a, const double* __restrict__ b,
                                      double* __restrict__ partials)
         {
@@ -314,6 +394,14 @@ namespace apf
             const double avg = static_cast<double>(A.nnz()) / A.rows;
             const int threads = 256;
             APF_KERNEL(name ? name : (MODE == 1 ? "residual" : (MODE == 2 ? "jacobi_sweep" : "spmv")), s);
+            if (A.sell)
+            {
+                const DeviceSell& S = *A.sell;
+                sell_kernel<MODE><<<blocks_for((long long)S.slices * 32, threads, 148 * 64), threads, 0, s>>>(
+                    A.rows, S.slices, S.slice_ptr.get(), S.col.get(), S.val.get(), x, b, y, alpha, beta, dinv);
+                APF_CUDA(cudaGetLastError());
+                return;
+            }
             auto go = [&](auto g) {
                 constexpr int G = decltype(g)::value;
                 spmv_kernel<G, MODE><<<blocks_for((long long)A.rows * G, threads, 148 * 64), threads, 0, s>>>(
@@ -325,6 +413,36 @@ namespace apf
             else go(std::integral_constant<int, 32>{});
             APF_CUDA(cudaGetLastError());
         }
+    }
+
+    bool build_sell(cudaStream_t s, DeviceCsr& A, double max_padding)
+    {
+        A.sell.reset();
+        if (A.rows == 0 || A.nnz() == 0)
+            return false;
+        const int slices = (A.rows + 31) / 32;
+        DeviceBuffer<int> cnt(slices, s);
+        const int grid = blocks_for((long long)slices * 32, 256, 148 * 32);
+        {
+            APF_KERNEL("sell_count", s);
+            sell_count<<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), cnt.get());
+        }
+        auto S = std::make_unique<DeviceSell>();
+        S->slices = slices;
+        S->slice_ptr.allocate(static_cast<std::size_t>(slices) + 1, s);
+        const long long total = exclusive_scan(cnt.get(), S->slice_ptr.get(), slices, s);
+        if (total > static_cast<long long>(max_padding * static_cast<double>(A.nnz())) || total >= (1ll << 31))
+            return false;
+        S->col.allocate(static_cast<std::size_t>(total), s);
+        S->val.allocate(static_cast<std::size_t>(total), s);
+        {
+            APF_KERNEL("sell_fill", s);
+            sell_fill<<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), A.col_idx.get(), A.values.get(),
+                                          S->slice_ptr.get(), S->col.get(), S->val.get());
+        }
+        APF_CUDA(cudaGetLastError());
+        A.sell = std::move(S);
+        return true;
     }
 
     void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha, double beta, const char* name)

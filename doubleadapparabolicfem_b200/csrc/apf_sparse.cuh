@@ -23,6 +23,9 @@ namespace apf
         }
     };
 
+    // Build A.sell (sliced ELLPACK) unless its padding would exceed max_padding x nnz;
+    // returns whether it was built.
+    bool build_sell(cudaStream_t s, DeviceCsr& A, double max_padding = 1.35);
     // y = alpha * A x + beta * y   (beta == 0 ignores y's old contents)
     void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0,
               const char* name = nullptr);

@@ -60,6 +60,8 @@ namespace apf
         AmgOptions precond_opts{};
         DeviceBuffer<double> rhs, solution;
         double precond_setup_seconds = 0.0;
+        int precond_kind = -1;                    // APF_PRECOND_* installed in precond's V-cycles
+        unsigned long long precond_model_version = 0; // learned model the weights came from
     };
 
     void upload_tables_once(int device);

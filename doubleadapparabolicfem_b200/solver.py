@@ -28,7 +28,7 @@ class SolverOptions:
     use_true_residual_batching: bool = True
     true_residual_check_interval: int = 100
     preconditioner: str = "amg_block"        # "amg_block" | "learned"
-    amg_smooth_steps: int = 1
+    amg_smooth_steps: int = 2
     amg_strength: float = 0.08
     amg_coarse_size: int = 256
 

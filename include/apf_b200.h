@@ -166,6 +166,8 @@ typedef struct apf_solver_diagnostics
     double solve_seconds;
     int amg_levels_lambda, amg_levels_u;
     int64_t amg_nnz_lambda, amg_nnz_u;
+    int preconditioner_used;      /* APF_PRECOND_*: LEARNED, or AMG_BLOCK after a fallback */
+    int learned_fallback;         /* 1: the learned run missed the tolerance, plain run from its iterate */
 } apf_solver_diagnostics;
 
 void apf_solver_options_default(apf_solver_options* opt);
@@ -246,6 +248,55 @@ int apf_true_residual_noalloc(apf_ctx* ctx, int32_t rows, const int32_t* row_ptr
 
 /* Device pointer of the last solution (n_lambda + n_u values, owned by sys). */
 int apf_system_solution_device_ptr(const apf_system* sys, const double** solution);
+
+/* ---- learned preconditioner (no counterpart in the reference) -------------------- */
+/* The reference's MINRES preconditioner is blkdiag(A_y, Hhat)^-1 by sparse Cholesky
+ * (parabolic_graph_norm_minres.hpp:46-181); here each block is one SA-AMG V-cycle.  The
+ * learned variant keeps that structure and replaces the damped-Jacobi weights omega/a_ii of
+ * every non-coarsest level by w_i = omega/a_ii exp(0.5 tanh(MLP(f_i))), f_i = 8 scale-free
+ * features of matrix row i, and scales each level's coarse correction by
+ * alpha_l = 2 sigmoid(theta_l).  The MLP (8 -> 32 -> 32 -> 1, tanh) runs in BF16 with FP32
+ * accumulation on the tensor cores at preconditioner set-up; the V-cycles stay symmetric
+ * and a Gershgorin bound keeps every smoother convergent, so the preconditioner is SPD.
+ * Parameters: APF_LEARNED_NUM_PARAMS floats (layout in apf_learned.cuh); all zero gives
+ * the plain weights and alpha = 1. */
+#define APF_LEARNED_NUM_PARAMS 1409
+typedef struct apf_learned_model apf_learned_model;
+int apf_learned_model_create(apf_learned_model** out);
+int apf_learned_model_destroy(apf_learned_model* model);
+int apf_learned_model_set_params(apf_learned_model* model, const float* params, int n);
+int apf_learned_model_get_params(const apf_learned_model* model, float* params, int n);
+/* Model used by set-ups with preconditioner = APF_PRECOND_LEARNED (NULL clears; the context
+ * keeps a copy of the parameters). */
+int apf_ctx_set_learned_model(apf_ctx* ctx, const apf_learned_model* model);
+/* Training objective on an assembled system whose preconditioner is set up: the
+ * energy-norm contraction of `steps` stationary V-cycle iterations of both blocks,
+ *   L = sum_block mean_sample (1/steps) log(||E^steps e||_T^2 / ||e||_T^2),  E = I - V T,
+ * T = A_y and Hhat, e = start vectors ([samples][n_lambda + n_u], NULL: seeded normal
+ * vectors), and dL/dparams (APF_LEARNED_NUM_PARAMS floats, host, may be NULL) by reverse
+ * mode through the V-cycles and the MLP (FP32 forward / backward kernels). */
+int apf_learned_loss_and_grad(apf_ctx* ctx, apf_system* sys, const apf_learned_model* model, int samples, int steps,
+                              uint64_t seed, const double* start_vectors, int pointers_on_device, double* loss,
+                              float* grad);
+/* y = MLP(features) for n rows of 8 features: precision 0 = FP32 CUDA cores (training
+ * pass), 1 = BF16 tensor cores with FP32 accumulation (inference). */
+int apf_learned_forward(apf_ctx* ctx, const apf_learned_model* model, int n, const float* features, float* y,
+                        int precision, int pointers_on_device);
+
+/* ---- AMG hierarchy inspection (tests and the oracle's V-cycle restatement) ---------- */
+/* block 0 = A_y, 1 = Hhat (its hierarchy is built on the filtered Hhat_F). */
+int apf_amg_info(apf_ctx* ctx, apf_system* sys, int block, int* levels, int* dense_coarse, int* coarse_sweeps,
+                 int* smooth_steps);
+/* rows, nnz of A_l and (l < levels-1) P_l, the Jacobi omega_l and the coarse scale alpha_l */
+int apf_amg_level_info(apf_ctx* ctx, apf_system* sys, int block, int level, int* rows, int64_t* nnz_a,
+                       int64_t* nnz_p, double* omega, double* alpha);
+/* CSR arrays (host) of A_l (which = 0) or P_l (which = 1) */
+int apf_amg_level_copy(apf_ctx* ctx, apf_system* sys, int block, int level, int which, int32_t* row_ptr,
+                       int32_t* col_idx, double* values);
+/* smoother weights of level l (host, rows values): omega_l / a_ii, or the learned weights */
+int apf_amg_level_weights(apf_ctx* ctx, apf_system* sys, int block, int level, double* weights);
+/* row features of level l (host, rows x 8 floats) as the learned model sees them */
+int apf_amg_level_features(apf_ctx* ctx, apf_system* sys, int block, int level, float* features);
 
 #ifdef __cplusplus
 }

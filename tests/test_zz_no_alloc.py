@@ -52,9 +52,12 @@ def test_noalloc_residual_matches_minres_report(gpu_ctx):
         results.append((absolute, relative))
     free_after_second = torch.cuda.mem_get_info(gpu_ctx.device)[0]
 
+    # The solver evaluates the same FP64 residual with its own SpMV (another summation
+    # order): b - K x carries rounding of order eps * ||b||, so near convergence the two
+    # relative residuals agree to an absolute 1e-14, not to a fraction of their size.
     reported = diag["final_true_residual"]
     for absolute, relative in results:
-        assert abs(relative - reported) <= 1e-12 * reported, (relative, reported)
+        assert abs(relative - reported) <= 1e-12 * reported + 1e-14, (relative, reported)
         assert abs(absolute - relative * float(torch.linalg.norm(b))) <= 1e-12 * absolute
     assert results[0] == results[1]
     assert free_after_second == free_before_second
