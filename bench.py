@@ -295,12 +295,16 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize(dev)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    step_events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with ClockSampler(local) as clocks:
         ev0.record(stream)
-        for _ in range(args.steps):
+        for k in range(args.steps):
             lib.apf_system_destroy(step(dprob, True))
+            step_events[k].record(stream)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
+    step_ms = [round(ev0.elapsed_time(step_events[0]), 2)] + [
+        round(step_events[k - 1].elapsed_time(step_events[k]), 2) for k in range(1, args.steps)]
     barrier()
     launches = ctx.kernel_launches() - launches0
     elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
@@ -403,6 +407,7 @@ def run_ours(args, world, rank, local):
                    "minres_solve_s_mean": sum(d["solve_seconds"] for d in timed_diags) / len(timed_diags),
                    "plain_preconditioner": plain,
                    "minres_iterations": [d["iterations"] for d in timed_diags],
+                   "step_ms": step_ms,
                    "final_true_residual_max": max(d["final_true_residual"] for d in timed_diags),
                    "e2e_final_true_residual_max": max(d["final_true_residual"] for d in e2e_diags),
                    "flux_squared": timed_est[-1]["flux_squared"] if timed_est else None,

@@ -168,7 +168,7 @@ SIGNATURES["apf_estimate"] = ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_
 SIGNATURES["apf_true_residual_noalloc"] = ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int)
 
-APF_LEARNED_NUM_PARAMS = 1409
+APF_LEARNED_NUM_PARAMS = 1442
 _P = C.c_void_p
 SIGNATURES.update({
     "apf_learned_model_create": ([C.POINTER(_P)], C.c_int),
@@ -176,14 +176,14 @@ SIGNATURES.update({
     "apf_learned_model_set_params": ([_P, _P, C.c_int], C.c_int),
     "apf_learned_model_get_params": ([_P, _P, C.c_int], C.c_int),
     "apf_ctx_set_learned_model": ([_P, _P], C.c_int),
-    "apf_learned_loss_and_grad": ([_P, _P, _P, C.c_int, C.c_int, C.c_uint64, _P, C.c_int, C.POINTER(C.c_double), _P],
-                                  C.c_int),
+    "apf_learned_loss_and_grad": ([_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_uint64, _P, C.c_int,
+                                   C.POINTER(C.c_double), _P], C.c_int),
     "apf_learned_forward": ([_P, _P, C.c_int, _P, _P, C.c_int, C.c_int], C.c_int),
     "apf_amg_info": ([_P, _P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                       C.POINTER(C.c_int)], C.c_int),
     "apf_amg_level_info": ([_P, _P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                             C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "apf_amg_level_copy": ([_P, _P, C.c_int, C.c_int, C.c_int, _P, _P, _P], C.c_int),
-    "apf_amg_level_weights": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
+    "apf_amg_level_weights": ([_P, _P, C.c_int, C.c_int, C.c_int, _P], C.c_int),
     "apf_amg_level_features": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
 })

@@ -568,21 +568,27 @@ namespace apf
         }
         const int pre = coarsest ? kCoarseSweeps : opt_.smooth_steps;
         const int post = coarsest ? 0 : opt_.smooth_steps;
-        // smoother weights: omega D^-1 (plain) or the level's per-row weights
+        // smoother weights: omega D^-1 (plain) or the level's per-row weights, one vector
+        // for the first pre-smoothing sweep and one for the later sweeps; post-smoothing
+        // applies the pre-smoothing weights in reverse order
         const bool own = L.w.size() != 0;
-        const double* wv = own ? L.w.get() : L.dinv.get();
         const double om = own ? 1.0 : L.omega;
+        auto weights = [&](int sweep) -> const double* {
+            if (!own)
+                return L.dinv.get();
+            return sweep == 0 || L.w2.size() == 0 ? L.w.get() : L.w2.get();
+        };
         // the iterate alternates between x and the level's scratch t; starting in the right
         // one makes the last of the pre + post smoothing writes land in x (no copies)
         double* cur = (pre + post) % 2 == 1 ? x : L.t.get();
         double* other = cur == x ? L.t.get() : x;
         {
             APF_KERNEL("amg_jacobi_first", s);
-            jacobi_first<<<nblocks(n, 256), 256, 0, s>>>(n, b, wv, om, cur);
+            jacobi_first<<<nblocks(n, 256), 256, 0, s>>>(n, b, weights(0), om, cur);
         }
         for (int k = 1; k < pre; ++k)
         {
-            jacobi_sweep(s, A, cur, b, wv, om, other);
+            jacobi_sweep(s, A, cur, b, weights(k), om, other);
             std::swap(cur, other);
         }
         if (coarsest)
@@ -594,18 +600,21 @@ namespace apf
         spmv(s, L.P, C.x.get(), cur, L.alpha, 1.0);
         for (int k = 0; k < post; ++k)
         {
-            jacobi_sweep(s, A, cur, b, wv, om, other);
+            jacobi_sweep(s, A, cur, b, weights(post - 1 - k), om, other);
             std::swap(cur, other);
         }
     }
 
-    void Amg::set_smoother(int l, DeviceBuffer<double>&& w, double alpha)
+    void Amg::set_smoother(int l, DeviceBuffer<double>&& w, DeviceBuffer<double>&& w2, double alpha)
     {
         require(l >= 0 && l < levels(), APF_ERR_INVALID, "AMG: no such level");
         AmgLevel& L = levels_[static_cast<std::size_t>(l)];
-        require(w.size() == 0 || w.size() == static_cast<std::size_t>(L.A->rows), APF_ERR_INVALID,
-                "AMG: smoother weights of the wrong size");
+        const auto rows = static_cast<std::size_t>(L.A->rows);
+        require((w.size() == 0 || w.size() == rows) && (w2.size() == 0 || w2.size() == rows) &&
+                    !(w.size() == 0 && w2.size() != 0),
+                APF_ERR_INVALID, "AMG: smoother weights of the wrong size");
         L.w = std::move(w);
+        L.w2 = std::move(w2);
         L.alpha = alpha;
     }
 
@@ -614,6 +623,7 @@ namespace apf
         for (auto& L : levels_)
         {
             L.w.release();
+            L.w2.release();
             L.alpha = 1.0;
         }
     }

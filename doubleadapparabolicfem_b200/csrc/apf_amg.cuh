@@ -27,7 +27,8 @@ namespace apf
         double omega = 0.0;           // Jacobi damping 4 / (3 rho(D^-1 A))
         DeviceBuffer<int> comp;       // component of each unknown (empty: one component)
         DeviceBuffer<double> x, b, r, t;
-        DeviceBuffer<double> w;       // per-row smoother weights replacing omega D^-1 (empty: plain)
+        DeviceBuffer<double> w;       // per-row weights of the first pre-smoothing sweep (empty: omega D^-1)
+        DeviceBuffer<double> w2;      // weights of the later pre-smoothing sweeps (empty: w)
         double alpha = 1.0;           // coarse-correction scale
     };
 
@@ -50,9 +51,11 @@ namespace apf
         int smooth_steps() const { return opt_.smooth_steps; }
         const double* coarse_inverse() const { return coarse_inv_.get(); }
         static constexpr int coarse_sweeps() { return kCoarseSweeps; }
-        // Replace level l's Jacobi weights omega D^-1 by the per-row weights w (device, moved
-        // in) and scale its coarse correction by alpha; both keep the V-cycle symmetric.
-        void set_smoother(int l, DeviceBuffer<double>&& w, double alpha);
+        // Replace level l's Jacobi weights omega D^-1 by per-row weights (device, moved in):
+        // w for the first pre-smoothing sweep, w2 for the later ones (post-smoothing runs the
+        // same weights in reverse order), and scale its coarse correction by alpha; the
+        // V-cycle stays symmetric.
+        void set_smoother(int l, DeviceBuffer<double>&& w, DeviceBuffer<double>&& w2, double alpha);
         // back to omega D^-1 and alpha = 1 on every level
         void reset_smoothers();
         // x = the coarsest level's solve of b (dense inverse or fixed Jacobi sweeps; a

@@ -674,8 +674,8 @@ int apf_ctx_set_learned_model(apf_ctx* ctx, const apf_learned_model* model)
 }
 
 int apf_learned_loss_and_grad(apf_ctx* ctx, apf_system* sys, const apf_learned_model* model, int samples, int steps,
-                              uint64_t seed, const double* start_vectors, int pointers_on_device, double* loss,
-                              float* grad)
+                              int burn_in, uint64_t seed, const double* start_vectors, int pointers_on_device,
+                              double* loss, float* grad)
 {
     if (!ctx || !sys || !model)
         return APF_ERR_INVALID;
@@ -698,7 +698,8 @@ int apf_learned_loss_and_grad(apf_ctx* ctx, apf_system* sys, const apf_learned_m
             }
         }
         const double L = apf::learned_loss_and_grad(s, model->model, *S.precond, S.blocks[APF_BLOCK_A_Y],
-                                                     S.blocks[APF_BLOCK_HHAT], samples, steps, seed, sv, grad, S.ws);
+                                                     S.blocks[APF_BLOCK_HHAT], samples, steps, burn_in, seed, sv, grad,
+                                                     S.ws);
         apf::sync(s);
         S.precond_kind = -2; // FP32-model weights installed: the next solve re-installs
         if (loss)
@@ -722,13 +723,14 @@ int apf_learned_forward(apf_ctx* ctx, const apf_learned_model* model, int n, con
         {
             f.allocate(static_cast<std::size_t>(n) * apf::learned::kFeatures, s);
             f.upload(features, static_cast<std::size_t>(n) * apf::learned::kFeatures);
-            out.allocate(n, s);
+            out.allocate(static_cast<std::size_t>(n) * apf::learned::kOutputs, s);
             fp = f.get();
             yp = out.get();
         }
         apf::learned_forward(s, dp.get(), n, fp, yp, precision);
         if (!pointers_on_device && n > 0)
-            APF_CUDA(cudaMemcpyAsync(y, out.get(), n * sizeof(float), cudaMemcpyDeviceToHost, s));
+            APF_CUDA(cudaMemcpyAsync(y, out.get(), static_cast<std::size_t>(n) * apf::learned::kOutputs * sizeof(float),
+                                     cudaMemcpyDeviceToHost, s));
         apf::sync(s);
     });
 }
@@ -799,16 +801,17 @@ int apf_amg_level_copy(apf_ctx* ctx, apf_system* sys, int block, int level, int 
     });
 }
 
-int apf_amg_level_weights(apf_ctx* ctx, apf_system* sys, int block, int level, double* weights)
+int apf_amg_level_weights(apf_ctx* ctx, apf_system* sys, int block, int level, int o, double* weights)
 {
-    if (!ctx || !sys || !weights)
+    if (!ctx || !sys || !weights || (o != 0 && o != 1))
         return APF_ERR_INVALID;
     return guarded(ctx, [&] {
         apf::AmgLevel& L = level_of(sys, block, level);
         cudaStream_t s = ctx->stream;
         const int n = L.A->rows;
-        if (L.w.size())
-            APF_CUDA(cudaMemcpyAsync(weights, L.w.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        const apf::DeviceBuffer<double>& W = (o == 1 && L.w2.size()) ? L.w2 : L.w;
+        if (W.size())
+            APF_CUDA(cudaMemcpyAsync(weights, W.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
         else
         {
             apf::DeviceBuffer<double> t(n, s);

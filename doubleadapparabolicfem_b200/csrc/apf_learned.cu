@@ -74,7 +74,8 @@ namespace apf
         }
 
         // FP32 forward pass, one thread per row; also used by the training pass
-        __device__ __forceinline__ float mlp_fp32(const float* __restrict__ P, const float* f, float* h1, float* h2)
+        __device__ __forceinline__ void mlp_fp32(const float* __restrict__ P, const float* f, float* h1, float* h2,
+                                                 float* y)
         {
             for (int j = 0; j < kHidden; ++j)
             {
@@ -90,10 +91,13 @@ namespace apf
                     a = fmaf(P[kW2 + j * kHidden + k], h1[k], a);
                 h2[j] = tanhf(a);
             }
-            float y = P[kB3];
-            for (int k = 0; k < kHidden; ++k)
-                y = fmaf(P[kW3 + k], h2[k], y);
-            return y;
+            for (int o = 0; o < kOutputs; ++o)
+            {
+                float a = P[kB3 + o];
+                for (int k = 0; k < kHidden; ++k)
+                    a = fmaf(P[kW3 + o * kHidden + k], h2[k], a);
+                y[o] = a;
+            }
         }
 
         __global__ void forward_fp32_kernel(int n, const float* __restrict__ params, const float* __restrict__ feat,
@@ -105,10 +109,12 @@ namespace apf
             __syncthreads();
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             {
-                float f[kFeatures], h1[kHidden], h2[kHidden];
+                float f[kFeatures], h1[kHidden], h2[kHidden], out[kOutputs];
                 for (int k = 0; k < kFeatures; ++k)
                     f[k] = feat[static_cast<long long>(i) * kFeatures + k];
-                y[i] = mlp_fp32(P, f, h1, h2);
+                mlp_fp32(P, f, h1, h2, out);
+                for (int o = 0; o < kOutputs; ++o)
+                    y[static_cast<long long>(i) * kOutputs + o] = out[o];
             }
         }
 
@@ -131,7 +137,7 @@ namespace apf
         // BF16 forward pass on the tensor cores: one warp per tile of 16 rows.
         // Layer 1: [16 x 16 (8 features, zero padded)] x [16 x 32]; layer 2: [16 x 32] x [32 x 32];
         // the FP32 accumulator fragments of one layer are repacked in registers as the next
-        // layer's BF16 operand fragments; the last layer (32 -> 1) is a quad shuffle reduction.
+        // layer's BF16 operand fragments; the last layer (32 -> 2) is a quad shuffle reduction.
         __global__ void __launch_bounds__(128) forward_bf16_kernel(int n, const float* __restrict__ params,
                                                                    const float* __restrict__ feat, float* __restrict__ y)
         {
@@ -140,7 +146,7 @@ namespace apf
             // B fragments of W1^T (k = feature, n = hidden unit) and W2^T, biases and w3 in the
             // accumulator layout (columns 2t, 2t+1 of each 8-wide tile)
             unsigned b1f[4][2], b2f[2][4][2];
-            float bias1[4][2], bias2[4][2], w3[4][2];
+            float bias1[4][2], bias2[4][2], w3[kOutputs][4][2];
             for (int nt = 0; nt < 4; ++nt)
             {
                 const int col = nt * 8 + g;
@@ -157,10 +163,13 @@ namespace apf
                 {
                     bias1[nt][c] = params[kB1 + nt * 8 + 2 * t + c];
                     bias2[nt][c] = params[kB2 + nt * 8 + 2 * t + c];
-                    w3[nt][c] = params[kW3 + nt * 8 + 2 * t + c];
+                    for (int o = 0; o < kOutputs; ++o)
+                        w3[o][nt][c] = params[kW3 + o * kHidden + nt * 8 + 2 * t + c];
                 }
             }
-            const float b3 = params[kB3];
+            float b3[kOutputs];
+            for (int o = 0; o < kOutputs; ++o)
+                b3[o] = params[kB3 + o];
             const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
             const int nw = (gridDim.x * blockDim.x) >> 5;
             const int tiles = (n + 15) / 16;
@@ -197,35 +206,49 @@ namespace apf
                     a2[ks][2] = pack_bf16(tanhf(h1[n1][0]), tanhf(h1[n1][1]));
                     a2[ks][3] = pack_bf16(tanhf(h1[n1][2]), tanhf(h1[n1][3]));
                 }
-                float acc0 = 0.f, acc1 = 0.f;
+                float acc0[kOutputs], acc1[kOutputs];
+                for (int o = 0; o < kOutputs; ++o)
+                    acc0[o] = acc1[o] = 0.f;
                 for (int nt = 0; nt < 4; ++nt)
                 {
                     float h2[4] = {bias2[nt][0], bias2[nt][1], bias2[nt][0], bias2[nt][1]};
                     mma_bf16(h2, a2[0], b2f[0][nt][0], b2f[0][nt][1]);
                     mma_bf16(h2, a2[1], b2f[1][nt][0], b2f[1][nt][1]);
-                    acc0 = fmaf(w3[nt][0], tanhf(h2[0]), fmaf(w3[nt][1], tanhf(h2[1]), acc0));
-                    acc1 = fmaf(w3[nt][0], tanhf(h2[2]), fmaf(w3[nt][1], tanhf(h2[3]), acc1));
+                    const float t0 = tanhf(h2[0]), t1 = tanhf(h2[1]), t2 = tanhf(h2[2]), t3 = tanhf(h2[3]);
+                    for (int o = 0; o < kOutputs; ++o)
+                    {
+                        acc0[o] = fmaf(w3[o][nt][0], t0, fmaf(w3[o][nt][1], t1, acc0[o]));
+                        acc1[o] = fmaf(w3[o][nt][0], t2, fmaf(w3[o][nt][1], t3, acc1[o]));
+                    }
                 }
-                acc0 += __shfl_xor_sync(0xffffffffu, acc0, 1);
-                acc0 += __shfl_xor_sync(0xffffffffu, acc0, 2);
-                acc1 += __shfl_xor_sync(0xffffffffu, acc1, 1);
-                acc1 += __shfl_xor_sync(0xffffffffu, acc1, 2);
+                for (int o = 0; o < kOutputs; ++o)
+                {
+                    acc0[o] += __shfl_xor_sync(0xffffffffu, acc0[o], 1);
+                    acc0[o] += __shfl_xor_sync(0xffffffffu, acc0[o], 2);
+                    acc1[o] += __shfl_xor_sync(0xffffffffu, acc1[o], 1);
+                    acc1[o] += __shfl_xor_sync(0xffffffffu, acc1[o], 2);
+                }
                 if (t == 0)
                 {
-                    if (r0 < n)
-                        y[r0] = acc0 + b3;
-                    if (r1 < n)
-                        y[r1] = acc1 + b3;
+                    for (int o = 0; o < kOutputs; ++o)
+                    {
+                        if (r0 < n)
+                            y[static_cast<long long>(r0) * kOutputs + o] = acc0[o] + b3[o];
+                        if (r1 < n)
+                            y[static_cast<long long>(r1) * kOutputs + o] = acc1[o] + b3[o];
+                    }
                 }
             }
         }
 
-        // w_i = omega * dinv_i * exp(range * tanh(y_i))
-        __global__ void weights_kernel(int n, const float* __restrict__ y, const double* __restrict__ dinv, double omega,
-                                       double* __restrict__ w)
+        // w_i = omega * dinv_i * exp(range * tanh(y_i^(o)))
+        __global__ void weights_kernel(int n, const float* __restrict__ y, int o, const double* __restrict__ dinv,
+                                       double omega, double* __restrict__ w)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-                w[i] = omega * dinv[i] * exp(static_cast<double>(kWeightRange) * tanh(static_cast<double>(y[i])));
+                w[i] = omega * dinv[i] *
+                       exp(static_cast<double>(kWeightRange) *
+                           tanh(static_cast<double>(y[static_cast<long long>(i) * kOutputs + o])));
         }
 
         // symmetric Gershgorin row sums of W^1/2 A W^1/2, maximum via integer atomics on the
@@ -249,10 +272,39 @@ namespace apf
                 atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(best)));
         }
 
-        __global__ void scale_kernel(int n, double a, double* __restrict__ x)
+        // w *= bound / g when the Gershgorin bound g (device, double bits) exceeds bound
+        __global__ void bound_kernel(int n, const unsigned long long* __restrict__ gbits, double bound,
+                                     double* __restrict__ w)
         {
+            const double g = __longlong_as_double(static_cast<long long>(*gbits));
+            if (!(g > bound))
+                return;
+            const double a = bound / g;
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-                x[i] *= a;
+                w[i] *= a;
+        }
+
+        // weights of sweep class o on one level from model outputs y, bounded on the device
+        void bounded_weights(cudaStream_t s, const AmgLevel& L, const float* y, int o, DeviceBuffer<double>& w)
+        {
+            const DeviceCsr& A = *L.A;
+            const int n = A.rows;
+            w.allocate(n, s);
+            {
+                APF_KERNEL("learned_weights", s);
+                weights_kernel<<<nblk(n, 256), 256, 0, s>>>(n, y, o, L.dinv.get(), L.omega, w.get());
+            }
+            DeviceBuffer<unsigned long long> gmax(1, s);
+            gmax.zero();
+            {
+                APF_KERNEL("learned_gershgorin", s);
+                gershgorin_sym_kernel<<<nblk(n, 256, 1024), 256, 0, s>>>(n, A.row_ptr.get(), A.col_idx.get(),
+                                                                         A.values.get(), w.get(), gmax.get());
+            }
+            {
+                APF_KERNEL("learned_bound", s);
+                bound_kernel<<<nblk(n, 256), 256, 0, s>>>(n, gmax.get(), kSmootherBound, w.get());
+            }
         }
 
         double alpha_of(const LearnedModel& m, int block, int level)
@@ -288,42 +340,6 @@ namespace apf
         }
     }
 
-    namespace
-    {
-        // smoother weights of one level from the model (BF16 inference), made safe
-        void level_weights(cudaStream_t s, const float* dparams, const AmgLevel& L, int level, int block,
-                           DeviceBuffer<double>& w, int precision)
-        {
-            const DeviceCsr& A = *L.A;
-            const int n = A.rows;
-            DeviceBuffer<float> feat(static_cast<std::size_t>(n) * kFeatures, s), y(n, s);
-            learned_features(s, A, L.dinv.get(), level, block, feat.get());
-            learned_forward(s, dparams, n, feat.get(), y.get(), precision);
-            w.allocate(n, s);
-            {
-                APF_KERNEL("learned_weights", s);
-                weights_kernel<<<nblk(n, 256), 256, 0, s>>>(n, y.get(), L.dinv.get(), L.omega, w.get());
-            }
-            DeviceBuffer<unsigned long long> gmax(1, s);
-            gmax.zero();
-            {
-                APF_KERNEL("learned_gershgorin", s);
-                gershgorin_sym_kernel<<<nblk(n, 256, 1024), 256, 0, s>>>(n, A.row_ptr.get(), A.col_idx.get(),
-                                                                         A.values.get(), w.get(), gmax.get());
-            }
-            unsigned long long bits = 0;
-            APF_CUDA(cudaMemcpyAsync(&bits, gmax.get(), sizeof(bits), cudaMemcpyDeviceToHost, s));
-            sync(s);
-            double g;
-            std::memcpy(&g, &bits, sizeof(g));
-            if (g > kSmootherBound)
-            {
-                APF_KERNEL("learned_scale", s);
-                scale_kernel<<<nblk(n, 256), 256, 0, s>>>(n, kSmootherBound / g, w.get());
-            }
-        }
-    }
-
     void apply_learned_smoothers(cudaStream_t s, const LearnedModel& model, Amg& amg, int block)
     {
         DeviceBuffer<float> dparams(kParams, s);
@@ -331,9 +347,15 @@ namespace apf
         const int nl = amg.levels();
         for (int l = 0; l + 1 < nl; ++l)
         {
-            DeviceBuffer<double> w;
-            level_weights(s, dparams.get(), amg.level(l), l, block, w, 1);
-            amg.set_smoother(l, std::move(w), alpha_of(model, block, l));
+            const AmgLevel& L = amg.level(l);
+            const int n = L.A->rows;
+            DeviceBuffer<float> feat(static_cast<std::size_t>(n) * kFeatures, s), y(static_cast<std::size_t>(n) * kOutputs, s);
+            learned_features(s, *L.A, L.dinv.get(), l, block, feat.get());
+            learned_forward(s, dparams.get(), n, feat.get(), y.get(), 1);
+            DeviceBuffer<double> w, w2;
+            bounded_weights(s, L, y.get(), 0, w);
+            bounded_weights(s, L, y.get(), 1, w2);
+            amg.set_smoother(l, std::move(w), std::move(w2), alpha_of(model, block, l));
         }
     }
 }
@@ -360,14 +382,15 @@ namespace apf
                 y[i] += a[i] * b[i];
         }
 
-        // ybar_i = wbar_i * dw_i / dy_i = wbar_i * w_i * range * (1 - tanh^2 y_i)
-        __global__ void ybar_kernel(int n, const double* __restrict__ wbar, const double* __restrict__ w,
+        // ybar_i^(o) = wbar_i * dw_i / dy_i^(o) = wbar_i * w_i * range * (1 - tanh^2 y_i^(o))
+        __global__ void ybar_kernel(int n, int o, const double* __restrict__ wbar, const double* __restrict__ w,
                                     const float* __restrict__ y, float* __restrict__ ybar)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             {
-                const double th = tanh(static_cast<double>(y[i]));
-                ybar[i] = static_cast<float>(wbar[i] * w[i] * kWeightRange * (1.0 - th * th));
+                const long long k = static_cast<long long>(i) * kOutputs + o;
+                const double th = tanh(static_cast<double>(y[k]));
+                ybar[k] = static_cast<float>(wbar[i] * w[i] * kWeightRange * (1.0 - th * th));
             }
         }
 
@@ -410,7 +433,7 @@ namespace apf
             __shared__ float sd1[kTile][kHidden + 1];
             __shared__ float sh2[kTile][kHidden + 1];
             __shared__ float sd2[kTile][kHidden + 1];
-            __shared__ float syb[kTile];
+            __shared__ float syb[kTile][kOutputs];
             const int tid = threadIdx.x;
             for (int i = tid; i < kParams; i += blockDim.x)
                 P[i] = params[i];
@@ -423,21 +446,29 @@ namespace apf
                 if (tid < kTile)
                 {
                     const int r = tile * kTile + tid;
-                    float f[kFeatures], h1[kHidden], h2[kHidden];
-                    float yb = 0.f;
+                    float f[kFeatures], h1[kHidden], h2[kHidden], y[kOutputs];
+                    float yb[kOutputs];
+                    for (int o = 0; o < kOutputs; ++o)
+                        yb[o] = 0.f;
                     if (r < n)
                     {
                         for (int k = 0; k < kFeatures; ++k)
                             f[k] = feat[static_cast<long long>(r) * kFeatures + k];
-                        yb = ybar[r];
+                        for (int o = 0; o < kOutputs; ++o)
+                            yb[o] = ybar[static_cast<long long>(r) * kOutputs + o];
                     }
                     else
                         for (int k = 0; k < kFeatures; ++k)
                             f[k] = 0.f;
-                    mlp_fp32(P, f, h1, h2);
+                    mlp_fp32(P, f, h1, h2, y);
                     float d2[kHidden];
                     for (int j = 0; j < kHidden; ++j)
-                        d2[j] = yb * P[kW3 + j] * (1.f - h2[j] * h2[j]);
+                    {
+                        float a = 0.f;
+                        for (int o = 0; o < kOutputs; ++o)
+                            a = fmaf(yb[o], P[kW3 + o * kHidden + j], a);
+                        d2[j] = a * (1.f - h2[j] * h2[j]);
+                    }
                     for (int k = 0; k < kHidden; ++k)
                     {
                         float a = 0.f;
@@ -450,7 +481,8 @@ namespace apf
                     }
                     for (int k = 0; k < kFeatures; ++k)
                         sf[tid][k] = f[k];
-                    syb[tid] = yb;
+                    for (int o = 0; o < kOutputs; ++o)
+                        syb[tid][o] = yb[o];
                 }
                 __syncthreads();
                 // W2[j][k]: entries tid, tid + 256, tid + 512, tid + 768
@@ -471,22 +503,28 @@ namespace apf
                 }
                 if (tid < kHidden)
                 {
-                    float a1 = 0.f, a2 = 0.f, a3 = 0.f;
+                    float a1 = 0.f, a2 = 0.f;
                     for (int r = 0; r < kTile; ++r)
                     {
                         a1 += sd1[r][tid];
                         a2 += sd2[r][tid];
-                        a3 = fmaf(syb[r], sh2[r][tid], a3);
                     }
                     gB1 += a1;
                     gB2 += a2;
-                    gW3 += a3;
                 }
-                if (tid == 0)
+                if (tid < kOutputs * kHidden) // W3[o][j]
+                {
+                    const int o = tid / kHidden, j = tid % kHidden;
+                    float a = 0.f;
+                    for (int r = 0; r < kTile; ++r)
+                        a = fmaf(syb[r][o], sh2[r][j], a);
+                    gW3 += a;
+                }
+                if (tid < kOutputs)
                 {
                     float a = 0.f;
                     for (int r = 0; r < kTile; ++r)
-                        a += syb[r];
+                        a += syb[r][tid];
                     gB3 += a;
                 }
                 __syncthreads();
@@ -499,10 +537,11 @@ namespace apf
             {
                 out[kB1 + tid] = gB1;
                 out[kB2 + tid] = gB2;
-                out[kW3 + tid] = gW3;
             }
-            if (tid == 0)
-                out[kB3] = gB3;
+            if (tid < kOutputs * kHidden)
+                out[kW3 + tid] = gW3;
+            if (tid < kOutputs)
+                out[kB3 + tid] = gB3;
         }
 
         static_assert(kHidden * kHidden == 4 * kBackThreads, "W2 gradient ownership");
@@ -558,8 +597,11 @@ namespace apf
                             T.post_r[a].emplace_back(n, s);
                         }
                     }
-                    wbar_[l].allocate(n, s);
-                    wbar_[l].zero();
+                    for (int o = 0; o < kOutputs; ++o)
+                    {
+                        wbar_[l].emplace_back(n, s);
+                        wbar_[l].back().zero();
+                    }
                 }
                 // per level: 6 work vectors, then the level's input [6] and output [7] as seen
                 // from the finer level
@@ -573,11 +615,15 @@ namespace apf
 
             void forward(int app, const double* b, double* x) { fwd(0, app, b, x); }
             void reverse(int app, const double* xbar, double* bbar) { rev(0, app, xbar, bbar); }
-            DeviceBuffer<double>& wbar(int l) { return wbar_[l]; }
+            DeviceBuffer<double>& wbar(int l, int o) { return wbar_[l][o]; }
             double abar(int l) const { return abar_[l]; }
 
         private:
             int g(int n) const { return nblk(n, 256); }
+            // sweep class of pre-smoothing sweep k and its weights (post-smoothing sweep k in
+            // time order is pre-smoothing sweep sweeps - 1 - k)
+            static int cls(int k) { return k == 0 ? 0 : 1; }
+            static const double* W(const AmgLevel& L, int o) { return o == 0 ? L.w.get() : L.w2.get(); }
 
             void mul(int n, const double* a, const double* b, double* y)
             {
@@ -606,12 +652,12 @@ namespace apf
                 double* xc = scratch_[l + 1][7].get();
                 auto& T = tape_[l];
                 copy(s_, n, b, T.b[app].get());
-                mul(n, L.w.get(), b, x);                       // first pre-smoothing sweep from 0
+                mul(n, W(L, 0), b, x);                         // first pre-smoothing sweep from 0
                 for (int k = 1; k < sweeps_; ++k)
                 {
                     double* r = T.pre_r[app][k].get();
                     residual(s_, A, x, b, r);
-                    fma(n, L.w.get(), r, x);
+                    fma(n, W(L, cls(k)), r, x);
                 }
                 residual(s_, A, x, b, r1);
                 spmv(s_, L.R, r1, bc);
@@ -622,7 +668,7 @@ namespace apf
                 {
                     double* r = T.post_r[app][k].get();
                     residual(s_, A, x, b, r);
-                    fma(n, L.w.get(), r, x);
+                    fma(n, W(L, cls(sweeps_ - 1 - k)), r, x);
                 }
             }
 
@@ -648,15 +694,15 @@ namespace apf
                 fill(s_, n, 0.0, bb);
                 // one sweep x+ = x + W r, r = b - A x, read backwards:
                 //   wbar += xb (.) r;  rb = W xb;  bb += rb;  xb = xb - A rb
-                auto sweep_back = [&](const double* r) {
-                    fma(n, xb, r, wbar_[l].get());
-                    mul(n, L.w.get(), xb, rb);
+                auto sweep_back = [&](const double* r, int o) {
+                    fma(n, xb, r, wbar_[l][o].get());
+                    mul(n, W(L, o), xb, rb);
                     axpby(s_, n, 1.0, rb, 1.0, bb);
                     residual(s_, A, rb, xb, tmp);
                     std::swap(xb, tmp);
                 };
                 for (int k = sweeps_ - 1; k >= 0; --k)
-                    sweep_back(T.post_r[app][k].get());
+                    sweep_back(T.post_r[app][k].get(), cls(sweeps_ - 1 - k));
                 // coarse correction x+ = x + alpha P V(R (b - A x))
                 abar_[l] += dot_host(s_, ws_, n, xb, T.pxc[app].get());
                 spmv(s_, L.R, xb, xcb, L.alpha, 0.0);
@@ -666,10 +712,10 @@ namespace apf
                 residual(s_, A, rb, xb, tmp);
                 std::swap(xb, tmp);
                 for (int k = sweeps_ - 1; k >= 1; --k)
-                    sweep_back(T.pre_r[app][k].get());
+                    sweep_back(T.pre_r[app][k].get(), cls(k));
                 // first sweep x = W b
-                fma(n, L.w.get(), xb, bb);
-                fma(n, xb, T.b[app].get(), wbar_[l].get());
+                fma(n, W(L, 0), xb, bb);
+                fma(n, xb, T.b[app].get(), wbar_[l][0].get());
             }
 
             cudaStream_t s_;
@@ -678,7 +724,7 @@ namespace apf
             int sweeps_;
             std::vector<LevelTape> tape_;
             std::vector<std::vector<DeviceBuffer<double>>> scratch_;
-            std::vector<DeviceBuffer<double>> wbar_;
+            std::vector<std::vector<DeviceBuffer<double>>> wbar_;
             std::vector<double> abar_;
         };
 
@@ -690,9 +736,11 @@ namespace apf
 
     double learned_loss_and_grad(cudaStream_t s, const LearnedModel& model, BlockPreconditioner& P,
                                  const DeviceCsr& target_a, const DeviceCsr& target_h, int samples, int steps,
-                                 unsigned long long seed, const double* start_vectors, float* grad, Workspace& ws)
+                                 int burn_in, unsigned long long seed, const double* start_vectors, float* grad,
+                                 Workspace& ws)
     {
-        require(samples >= 1 && steps >= 1, APF_ERR_INVALID, "learned loss: samples and steps must be positive");
+        require(samples >= 1 && steps >= 1 && burn_in >= 0, APF_ERR_INVALID,
+                "learned loss: samples and steps must be positive, burn_in non-negative");
         ws.ensure(s);
         DeviceBuffer<float> dparams(kParams, s);
         dparams.upload(model.params.data(), kParams);
@@ -705,40 +753,21 @@ namespace apf
             const DeviceCsr& T = block == 0 ? target_a : target_h;
             const int n = T.rows;
             const int nl = amg.levels();
-            // model outputs on every non-coarsest level (FP32 forward), weights installed
+            // model outputs on every non-coarsest level (FP32 forward), weights installed; the
+            // Gershgorin rescale is a constant factor (no gradient through the bound)
             std::vector<LevelModelState> st(std::max(0, nl - 1));
             for (int l = 0; l + 1 < nl; ++l)
             {
                 AmgLevel& L = amg.level(l);
                 const int nr = L.A->rows;
                 st[l].feat.allocate(static_cast<std::size_t>(nr) * kFeatures, s);
-                st[l].y.allocate(nr, s);
+                st[l].y.allocate(static_cast<std::size_t>(nr) * kOutputs, s);
                 learned_features(s, *L.A, L.dinv.get(), l, block, st[l].feat.get());
                 learned_forward(s, dparams.get(), nr, st[l].feat.get(), st[l].y.get(), 0);
-                DeviceBuffer<double> w(nr, s);
-                {
-                    APF_KERNEL("learned_weights", s);
-                    weights_kernel<<<nblk(nr, 256), 256, 0, s>>>(nr, st[l].y.get(), L.dinv.get(), L.omega, w.get());
-                }
-                DeviceBuffer<unsigned long long> gmax(1, s);
-                gmax.zero();
-                {
-                    APF_KERNEL("learned_gershgorin", s);
-                    gershgorin_sym_kernel<<<nblk(nr, 256, 1024), 256, 0, s>>>(nr, L.A->row_ptr.get(), L.A->col_idx.get(),
-                                                                              L.A->values.get(), w.get(), gmax.get());
-                }
-                unsigned long long bits = 0;
-                APF_CUDA(cudaMemcpyAsync(&bits, gmax.get(), sizeof(bits), cudaMemcpyDeviceToHost, s));
-                sync(s);
-                double gm;
-                std::memcpy(&gm, &bits, sizeof(gm));
-                if (gm > kSmootherBound)
-                {
-                    // constant rescale (no gradient through the bound)
-                    APF_KERNEL("learned_scale", s);
-                    scale_kernel<<<nblk(nr, 256), 256, 0, s>>>(nr, kSmootherBound / gm, w.get());
-                }
-                amg.set_smoother(l, std::move(w), alpha_of(model, block, l));
+                DeviceBuffer<double> w, w2;
+                bounded_weights(s, L, st[l].y.get(), 0, w);
+                bounded_weights(s, L, st[l].y.get(), 1, w2);
+                amg.set_smoother(l, std::move(w), std::move(w2), alpha_of(model, block, l));
             }
             TapedVcycle V(s, amg, steps, amg.smooth_steps(), ws);
             DeviceBuffer<double> e(n, s), a(n, s), v(n, s), te(n, s), ebar(n, s), abarv(n, s);
@@ -753,9 +782,21 @@ namespace apf
                     APF_KERNEL("learned_train_normal", s);
                     normal_kernel<<<nblk(n, 256), 256, 0, s>>>(n, seed * 2654435761ull + 2ull * smp + block, e.get());
                 }
+                // burn-in (no gradient): e <- E^burn_in e, rescaled to unit energy
+                for (int j = 0; j < burn_in; ++j)
+                {
+                    spmv(s, T, e.get(), a.get());
+                    amg.apply(s, a.get(), v.get());
+                    axpby(s, n, -1.0, v.get(), 1.0, e.get());
+                }
                 spmv(s, T, e.get(), te.get());
-                const double q0 = dot_host(s, ws, n, e.get(), te.get());
-                require(q0 > 0.0, APF_ERR_NUMERIC, "learned loss: start vector with zero energy");
+                double q0 = dot_host(s, ws, n, e.get(), te.get());
+                require(q0 > 0.0 && std::isfinite(q0), APF_ERR_NUMERIC, "learned loss: start vector with no energy");
+                if (burn_in > 0)
+                {
+                    axpby(s, n, 0.0, e.get(), 1.0 / std::sqrt(q0), e.get());
+                    q0 = 1.0;
+                }
                 for (int j = 0; j < steps; ++j)
                 {
                     spmv(s, T, e.get(), a.get());
@@ -790,12 +831,15 @@ namespace apf
                 const double ab = V.abar(l) / samples;
                 g[kAlpha + block * kMaxLevels + std::min(l, kMaxLevels - 1)] += static_cast<float>(ab * al * (1.0 - al / 2.0));
                 const int nr = amg.level(l).A->rows;
-                DeviceBuffer<float> yb(nr, s);
-                axpby(s, nr, 0.0, V.wbar(l).get(), 1.0 / samples, V.wbar(l).get());
+                DeviceBuffer<float> yb(static_cast<std::size_t>(nr) * kOutputs, s);
+                for (int o = 0; o < kOutputs; ++o)
                 {
+                    DeviceBuffer<double>& wb = V.wbar(l, o);
+                    axpby(s, nr, 0.0, wb.get(), 1.0 / samples, wb.get());
                     APF_KERNEL("learned_train_ybar", s);
-                    ybar_kernel<<<nblk(nr, 256), 256, 0, s>>>(nr, V.wbar(l).get(), amg.level(l).w.get(), st[l].y.get(),
-                                                              yb.get());
+                    ybar_kernel<<<nblk(nr, 256), 256, 0, s>>>(nr, o, wb.get(),
+                                                              o == 0 ? amg.level(l).w.get() : amg.level(l).w2.get(),
+                                                              st[l].y.get(), yb.get());
                 }
                 const int blocks = std::max(1, std::min(148 * 2, (nr + kTile - 1) / kTile));
                 DeviceBuffer<float> partial(static_cast<std::size_t>(blocks) * kParams, s), sum(kParams, s);

@@ -5,17 +5,19 @@ The reference preconditions MINRES with blkdiag(A_y, Hhat)^-1 by sparse Cholesky
 this package applies one smoothed-aggregation V-cycle per block.  The learned variant
 keeps the V-cycles and lets a small network choose their smoothing:
 
-* per matrix row i of every non-coarsest AMG level, an MLP (8 -> 32 -> 32 -> 1, tanh) maps
-  8 scale-free row features to y_i, and the damped-Jacobi weight becomes
-  w_i = omega_l / a_ii * exp(0.5 tanh(y_i));
+* per matrix row i of every non-coarsest AMG level, an MLP (8 -> 32 -> 32 -> 2, tanh) maps
+  8 scale-free row features to y_i, and the damped-Jacobi weights become
+  w_i^(o) = omega_l / a_ii * exp(0.5 tanh(y_i^(o))), o = 0 for the first pre-smoothing
+  sweep and 1 for the later ones (post-smoothing runs them in reverse order);
 * per block and level, alpha_l = 2 sigmoid(theta_l) scales the coarse correction.
 
 Inference runs once per preconditioner set-up, in BF16 with FP32 accumulation on the
 tensor cores.  Training minimises the energy-norm contraction of a few stationary V-cycle
-iterations on systems the method itself assembles (seeded meshes with random
-piecewise-constant diffusivity), with the loss gradient computed on the GPU by reverse mode
-through the V-cycles and the MLP (hand-written FP32 forward / backward kernels); the
-optimiser step (Adam) runs on the host over the 1,409 parameters.  The plain block
+iterations (after a burn-in that leaves the slowly contracting modes) on systems the method
+itself assembles (seeded meshes with random piecewise-constant diffusivity), with the loss
+gradient computed on the GPU by reverse mode through the V-cycles and the MLP (hand-written
+FP32 forward / backward kernels); the optimiser step (Adam) runs on the host over the
+1,442 parameters.  The plain block
 preconditioner is the fallback (``apf_solve_minres`` reruns plain from the learned run's
 iterate when the learned run misses the tolerance) and the judge (the FP64 true residual).
 """
@@ -34,14 +36,15 @@ from .mesh import SpaceTimeProblem, uniform_problem
 N_PARAMS = _lib.APF_LEARNED_NUM_PARAMS
 N_FEATURES = 8
 HIDDEN = 32
+OUTPUTS = 2
 MAX_LEVELS = 16
 # flat parameter layout (apf_learned.cuh)
 W1, B1 = 0, HIDDEN * N_FEATURES
 W2 = B1 + HIDDEN
 B2 = W2 + HIDDEN * HIDDEN
 W3 = B2 + HIDDEN
-B3 = W3 + HIDDEN
-ALPHA = B3 + 1
+B3 = W3 + OUTPUTS * HIDDEN
+ALPHA = B3 + OUTPUTS
 
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "learned_precond.npz")
 
@@ -75,7 +78,7 @@ class LearnedModel:
         p = np.zeros(N_PARAMS, np.float32)
         p[W1:B1] = rng.normal(0, scale, HIDDEN * N_FEATURES)
         p[W2:B2] = rng.normal(0, scale / np.sqrt(HIDDEN / N_FEATURES), HIDDEN * HIDDEN)
-        p[W3:B3] = rng.normal(0, 1e-3, HIDDEN)
+        p[W3:B3] = rng.normal(0, 1e-3, OUTPUTS * HIDDEN)
         return LearnedModel(p)
 
     def save(self, path: str, **meta):
@@ -105,20 +108,21 @@ def use_model(ctx: Context, model: LearnedModel | None):
 
 
 def loss_and_grad(blocks: MainSystemBlocks, model: LearnedModel, samples: int = 4, steps: int = 3, seed: int = 0,
-                  start_vectors: np.ndarray | None = None, with_grad: bool = True):
+                  start_vectors: np.ndarray | None = None, with_grad: bool = True, burn_in: int = 0):
     """Training objective and its gradient on an assembled system with a set-up preconditioner."""
     ctx = blocks.ctx
     loss = C.c_double()
     grad = np.zeros(N_PARAMS, np.float32) if with_grad else None
     sv = None if start_vectors is None else np.ascontiguousarray(start_vectors, dtype=np.float64)
-    ctx.check(ctx.lib.apf_learned_loss_and_grad(ctx.handle, blocks.handle, model.handle, samples, steps, seed,
-                                                _ptr(sv), 0, C.byref(loss), _ptr(grad)))
+    ctx.check(ctx.lib.apf_learned_loss_and_grad(ctx.handle, blocks.handle, model.handle, samples, steps, burn_in,
+                                                seed, _ptr(sv), 0, C.byref(loss), _ptr(grad)))
     return loss.value, grad
 
 
 def forward(ctx: Context, model: LearnedModel, features: np.ndarray, precision: int = 1) -> np.ndarray:
+    """MLP outputs [rows, 2] (precision 0: FP32 CUDA cores, 1: BF16 tensor cores)."""
     f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, N_FEATURES)
-    y = np.empty(f.shape[0], np.float32)
+    y = np.empty((f.shape[0], OUTPUTS), np.float32)
     ctx.check(ctx.lib.apf_learned_forward(ctx.handle, model.handle, f.shape[0], _ptr(f), _ptr(y), precision, 0))
     return y
 
@@ -129,7 +133,7 @@ class AmgLevelData:
     P: object | None     # scipy CSR (None on the coarsest level)
     omega: float
     alpha: float
-    weights: np.ndarray  # smoother weights in use
+    weights: np.ndarray  # smoother weights in use [2, rows] (first sweep, later sweeps)
     features: np.ndarray # [rows, 8]
 
 
@@ -157,8 +161,9 @@ def amg_hierarchy(blocks: MainSystemBlocks, block: int):
             return sp.csr_matrix((va, ci, rp), shape=(n, ncols))
 
         A = fetch(0, nnz_a.value, n)
-        w = np.empty(n)
-        ctx.check(lib.apf_amg_level_weights(ctx.handle, blocks.handle, block, l, _ptr(w)))
+        w = np.empty((2, n))
+        for o in range(2):
+            ctx.check(lib.apf_amg_level_weights(ctx.handle, blocks.handle, block, l, o, _ptr(w[o])))
         f = np.empty((n, N_FEATURES), np.float32)
         ctx.check(lib.apf_amg_level_features(ctx.handle, blocks.handle, block, l, _ptr(f)))
         out.append(AmgLevelData(A=A, P=None, omega=omega.value, alpha=alpha.value, weights=w, features=f))
@@ -218,7 +223,7 @@ class Adam:
 
 
 def train(ctx: Context, systems, model: LearnedModel, epochs: int = 10, lr: float = 3e-3, samples: int = 4,
-          steps: int = 3, seed: int = 0, log=None, train_alpha: bool = False):
+          steps: int = 3, seed: int = 0, log=None, train_alpha: bool = False, burn_in: int = 0):
     """Adam on the mean loss over ``systems`` (assembled MainSystemBlocks with set-up
     preconditioners).  Returns the per-epoch mean losses.
 
@@ -231,7 +236,8 @@ def train(ctx: Context, systems, model: LearnedModel, epochs: int = 10, lr: floa
     for ep in range(epochs):
         losses = []
         for k, blocks in enumerate(systems):
-            loss, grad = loss_and_grad(blocks, model, samples=samples, steps=steps, seed=seed + 1000 * ep + k)
+            loss, grad = loss_and_grad(blocks, model, samples=samples, steps=steps, seed=seed + 1000 * ep + k,
+                                       burn_in=burn_in)
             if not train_alpha:
                 grad[ALPHA:] = 0.0
             losses.append(loss)
@@ -243,8 +249,9 @@ def train(ctx: Context, systems, model: LearnedModel, epochs: int = 10, lr: floa
     return history
 
 
-def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, levels=(3, 4), epochs: int = 20,
-                        lr: float = 1e-2, seed: int = 0, device: int = 0, log=print):
+def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, levels=(3, 4), epochs: int = 40,
+                        lr: float = 1e-2, seed: int = 0, device: int = 0, log=print, steps: int = 4,
+                        burn_in: int = 8):
     """Train the shipped model on method-generated systems: uniform meshes of the given outer
     levels with seeded random piecewise-constant diffusivity (log-uniform in [0.01, 100] on
     4x4 or 8x8 blocks), plus the constant-diffusivity mesh of each level."""
@@ -264,8 +271,10 @@ def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, leve
         setup_preconditioner(b, SolverOptions())
         blocks.append(b)
     model = LearnedModel.initial(seed)
-    hist = train(ctx, blocks, model, epochs=epochs, lr=lr, samples=2, steps=3, seed=seed, log=log)
-    model.save(out_path, history=np.asarray(hist), levels=np.asarray(levels), n_train=n_train, epochs=epochs)
+    hist = train(ctx, blocks, model, epochs=epochs, lr=lr, samples=2, steps=steps, seed=seed, log=log,
+                 burn_in=burn_in)
+    model.save(out_path, history=np.asarray(hist), levels=np.asarray(levels), n_train=n_train, epochs=epochs,
+               steps=steps, burn_in=burn_in)
     return model, hist
 
 
@@ -275,8 +284,11 @@ if __name__ == "__main__":
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--n-train", type=int, default=24)
     ap.add_argument("--levels", default="3,4")
-    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--lr", type=float, default=1e-2)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--burn-in", type=int, default=8)
     a = ap.parse_args()
-    train_default_model(a.out, a.n_train, tuple(int(x) for x in a.levels.split(",")), a.epochs, a.lr, a.seed)
+    train_default_model(a.out, a.n_train, tuple(int(x) for x in a.levels.split(",")), a.epochs, a.lr, a.seed,
+                        steps=a.steps, burn_in=a.burn_in)

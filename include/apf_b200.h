@@ -253,14 +253,15 @@ int apf_system_solution_device_ptr(const apf_system* sys, const double** solutio
 /* The reference's MINRES preconditioner is blkdiag(A_y, Hhat)^-1 by sparse Cholesky
  * (parabolic_graph_norm_minres.hpp:46-181); here each block is one SA-AMG V-cycle.  The
  * learned variant keeps that structure and replaces the damped-Jacobi weights omega/a_ii of
- * every non-coarsest level by w_i = omega/a_ii exp(0.5 tanh(MLP(f_i))), f_i = 8 scale-free
- * features of matrix row i, and scales each level's coarse correction by
- * alpha_l = 2 sigmoid(theta_l).  The MLP (8 -> 32 -> 32 -> 1, tanh) runs in BF16 with FP32
- * accumulation on the tensor cores at preconditioner set-up; the V-cycles stay symmetric
- * and a Gershgorin bound keeps every smoother convergent, so the preconditioner is SPD.
- * Parameters: APF_LEARNED_NUM_PARAMS floats (layout in apf_learned.cuh); all zero gives
- * the plain weights and alpha = 1. */
-#define APF_LEARNED_NUM_PARAMS 1409
+ * every non-coarsest level by w_i^(o) = omega/a_ii exp(0.5 tanh(y_i^(o))), y_i = MLP(f_i),
+ * f_i = 8 scale-free features of matrix row i, o = 0 for the first pre-smoothing sweep and
+ * 1 for the later ones (post-smoothing runs them in reverse order), and scales each
+ * level's coarse correction by alpha_l = 2 sigmoid(theta_l).  The MLP (8 -> 32 -> 32 -> 2,
+ * tanh) runs in BF16 with FP32 accumulation on the tensor cores at preconditioner set-up;
+ * the V-cycles stay symmetric and a Gershgorin bound keeps every sweep convergent, so the
+ * preconditioner is SPD.  Parameters: APF_LEARNED_NUM_PARAMS floats (layout in
+ * apf_learned.cuh); all zero gives the plain weights and alpha = 1. */
+#define APF_LEARNED_NUM_PARAMS 1442
 typedef struct apf_learned_model apf_learned_model;
 int apf_learned_model_create(apf_learned_model** out);
 int apf_learned_model_destroy(apf_learned_model* model);
@@ -272,14 +273,16 @@ int apf_ctx_set_learned_model(apf_ctx* ctx, const apf_learned_model* model);
 /* Training objective on an assembled system whose preconditioner is set up: the
  * energy-norm contraction of `steps` stationary V-cycle iterations of both blocks,
  *   L = sum_block mean_sample (1/steps) log(||E^steps e||_T^2 / ||e||_T^2),  E = I - V T,
- * T = A_y and Hhat, e = start vectors ([samples][n_lambda + n_u], NULL: seeded normal
- * vectors), and dL/dparams (APF_LEARNED_NUM_PARAMS floats, host, may be NULL) by reverse
- * mode through the V-cycles and the MLP (FP32 forward / backward kernels). */
+ * T = A_y and Hhat, e = E^burn_in e0 (no gradient through the burn-in), e0 = start vectors
+ * ([samples][n_lambda + n_u], NULL: seeded normal vectors), and dL/dparams
+ * (APF_LEARNED_NUM_PARAMS floats, host, may be NULL) by reverse mode through the V-cycles
+ * and the MLP (FP32 forward / backward kernels). */
 int apf_learned_loss_and_grad(apf_ctx* ctx, apf_system* sys, const apf_learned_model* model, int samples, int steps,
-                              uint64_t seed, const double* start_vectors, int pointers_on_device, double* loss,
-                              float* grad);
-/* y = MLP(features) for n rows of 8 features: precision 0 = FP32 CUDA cores (training
- * pass), 1 = BF16 tensor cores with FP32 accumulation (inference). */
+                              int burn_in, uint64_t seed, const double* start_vectors, int pointers_on_device,
+                              double* loss, float* grad);
+/* y = MLP(features) for n rows of 8 features, 2 outputs per row (y[2 i + o]): precision
+ * 0 = FP32 CUDA cores (training pass), 1 = BF16 tensor cores with FP32 accumulation
+ * (inference). */
 int apf_learned_forward(apf_ctx* ctx, const apf_learned_model* model, int n, const float* features, float* y,
                         int precision, int pointers_on_device);
 
@@ -293,8 +296,9 @@ int apf_amg_level_info(apf_ctx* ctx, apf_system* sys, int block, int level, int*
 /* CSR arrays (host) of A_l (which = 0) or P_l (which = 1) */
 int apf_amg_level_copy(apf_ctx* ctx, apf_system* sys, int block, int level, int which, int32_t* row_ptr,
                        int32_t* col_idx, double* values);
-/* smoother weights of level l (host, rows values): omega_l / a_ii, or the learned weights */
-int apf_amg_level_weights(apf_ctx* ctx, apf_system* sys, int block, int level, double* weights);
+/* smoother weights of level l (host, rows values) for sweep class o (0: first sweep,
+ * 1: later sweeps): omega_l / a_ii, or the learned weights */
+int apf_amg_level_weights(apf_ctx* ctx, apf_system* sys, int block, int level, int o, double* weights);
 /* row features of level l (host, rows x 8 floats) as the learned model sees them */
 int apf_amg_level_features(apf_ctx* ctx, apf_system* sys, int block, int level, float* features);
 

@@ -5,11 +5,12 @@ is the package's own, read from its exported hierarchy).
 
 Objects:
 * ``features(A, level, block)``: the 8 scale-free row features;
-* ``mlp(params, F)``: 8 -> 32 -> 32 -> 1 with tanh, FP64;
-* ``weights(...)``: w_i = omega / a_ii * exp(0.5 tanh(y_i)), rescaled so that the symmetric
-  Gershgorin bound of W^1/2 A W^1/2 stays <= 1.9;
-* ``vcycle(...)``: ``smooth_steps`` damped-Jacobi sweeps with w before and after the coarse
-  correction (scaled by alpha), coarsest level solved densely (or by the plain Jacobi
+* ``mlp(params, F)``: 8 -> 32 -> 32 -> 2 with tanh, FP64;
+* ``weights(...)``: w_i^(o) = omega / a_ii * exp(0.5 tanh(y_i^(o))), each rescaled so that the
+  symmetric Gershgorin bound of W^1/2 A W^1/2 stays <= 1.9;
+* ``vcycle(...)``: ``smooth_steps`` damped-Jacobi sweeps before the coarse correction (the
+  first with w^(0), the later ones with w^(1)), the same sweeps in reverse order after it,
+  coarse correction scaled by alpha, coarsest level solved densely (or by the plain Jacobi
   sweeps);
 * ``loss(...)``: sum over the two blocks of mean_e (1/k) log(||E^k e||_T^2 / ||e||_T^2),
   E = I - V T;
@@ -19,13 +20,13 @@ from __future__ import annotations
 
 import numpy as np
 
-N_FEATURES, HIDDEN, MAX_LEVELS = 8, 32, 16
+N_FEATURES, HIDDEN, OUTPUTS, MAX_LEVELS = 8, 32, 2, 16
 W1, B1 = 0, HIDDEN * N_FEATURES
 W2 = B1 + HIDDEN
 B2 = W2 + HIDDEN * HIDDEN
 W3 = B2 + HIDDEN
-B3 = W3 + HIDDEN
-ALPHA = B3 + 1
+B3 = W3 + OUTPUTS * HIDDEN
+ALPHA = B3 + OUTPUTS
 N_PARAMS = ALPHA + 2 * MAX_LEVELS
 WEIGHT_RANGE = 0.5
 SMOOTHER_BOUND = 1.9
@@ -58,7 +59,7 @@ def mlp(params: np.ndarray, F: np.ndarray) -> np.ndarray:
     p = np.asarray(params, dtype=np.float64)
     h1 = np.tanh(F @ p[W1:B1].reshape(HIDDEN, N_FEATURES).T + p[B1:W2])
     h2 = np.tanh(h1 @ p[W2:B2].reshape(HIDDEN, HIDDEN).T + p[B2:W3])
-    return h2 @ p[W3:B3] + p[B3]
+    return h2 @ p[W3:B3].reshape(OUTPUTS, HIDDEN).T + p[B3:ALPHA]
 
 
 def alpha(params, block: int, level: int) -> float:
@@ -66,15 +67,20 @@ def alpha(params, block: int, level: int) -> float:
     return 2.0 / (1.0 + np.exp(-th))
 
 
-def weights(params, A, F, omega: float) -> np.ndarray:
+def weights(params, A, F, omega: float):
+    """[w^(0), w^(1)] of one level."""
     A = A.tocsr()
-    w = omega / A.diagonal() * np.exp(WEIGHT_RANGE * np.tanh(mlp(params, F)))
-    sw = np.sqrt(w)
+    y = mlp(params, F)
     absA = abs(A)
-    g = (sw * (absA @ sw)).max()
-    if g > SMOOTHER_BOUND:
-        w = w * (SMOOTHER_BOUND / g)
-    return w
+    out = []
+    for o in range(OUTPUTS):
+        w = omega / A.diagonal() * np.exp(WEIGHT_RANGE * np.tanh(y[:, o]))
+        sw = np.sqrt(w)
+        g = (sw * (absA @ sw)).max()
+        if g > SMOOTHER_BOUND:
+            w = w * (SMOOTHER_BOUND / g)
+        out.append(w)
+    return out
 
 
 class Hierarchy:
@@ -111,13 +117,15 @@ class Hierarchy:
         if l == len(self.A) - 1:
             return self.coarse(b)
         A, P, w = self.A[l], self.P[l], self.w[l]
-        x = w * b
-        for _ in range(self.smooth_steps - 1):
-            x = x + w * (b - A @ x)
+        s = self.smooth_steps
+        cls = [0] + [1] * (s - 1)
+        x = w[0] * b
+        for k in range(1, s):
+            x = x + w[cls[k]] * (b - A @ x)
         xc = self.vcycle(P.T @ (b - A @ x), l + 1)
         x = x + self.alpha[l] * (P @ xc)
-        for _ in range(self.smooth_steps):
-            x = x + w * (b - A @ x)
+        for k in range(s):
+            x = x + w[cls[s - 1 - k]] * (b - A @ x)
         return x
 
 

@@ -39,16 +39,17 @@ def test_zero_parameters_give_plain_smoother():
     H, A = _toy()
     H.set_params(np.zeros(O.N_PARAMS))
     for l in range(len(H.A) - 1):
-        assert np.allclose(H.w[l], H.omega[l] / H.A[l].diagonal(), rtol=1e-15)
+        for o in range(O.OUTPUTS):
+            assert np.allclose(H.w[l][o], H.omega[l] / H.A[l].diagonal(), rtol=1e-15)
         assert H.alpha[l] == 1.0
 
 
 def test_gershgorin_rescale_bounds_the_smoother():
     H, A = _toy()
     p = np.zeros(O.N_PARAMS)
-    p[O.B3] = 20.0  # weights exp(0.5) times the plain ones
+    p[O.B3:O.ALPHA] = 20.0  # weights exp(0.5) times the plain ones
     H.set_params(p)
-    w = H.w[0]
+    w = H.w[0][0]
     M = sp.diags(np.sqrt(w)) @ A @ sp.diags(np.sqrt(w))
     assert np.linalg.eigvalsh(M.toarray()).max() < 2.0
 
