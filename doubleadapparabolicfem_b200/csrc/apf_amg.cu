@@ -522,17 +522,19 @@ namespace apf
                 C.comp = std::move(comp_c);
             sync(s);
         }
-        // sliced-ELLPACK copies for the V-cycle SpMVs (level 0's operator belongs to the
-        // caller, which builds its own)
+        // f32 sliced-ELLPACK copies of the V-cycle operators: the V-cycle reads its matrices
+        // 5 to 10 times per application, and f32 values (symmetric rounding, f64 products and
+        // accumulation) cut those reads by a third while keeping the preconditioner a fixed
+        // symmetric operator
         for (std::size_t l = 0; l < levels_.size(); ++l)
         {
             AmgLevel& L = levels_[l];
-            if (l > 0 && !(l + 1 == levels_.size() && !jacobi_coarse_))
-                build_sell(s, L.A_own);
+            if (!(l + 1 == levels_.size() && !jacobi_coarse_))
+                L.A32 = make_sell32(s, *L.A);
             if (L.P.rows)
             {
-                build_sell(s, L.P);
-                build_sell(s, L.R);
+                L.P32 = make_sell32(s, L.P);
+                L.R32 = make_sell32(s, L.R);
             }
         }
         sync(s);
@@ -586,21 +588,22 @@ namespace apf
             APF_KERNEL("amg_jacobi_first", s);
             jacobi_first<<<nblocks(n, 256), 256, 0, s>>>(n, b, weights(0), om, cur);
         }
+        const DeviceSell& A32 = *L.A32;
         for (int k = 1; k < pre; ++k)
         {
-            jacobi_sweep(s, A, cur, b, weights(k), om, other);
+            jacobi_sweep(s, A32, cur, b, weights(k), om, other);
             std::swap(cur, other);
         }
         if (coarsest)
             return;
-        residual(s, A, cur, b, L.r.get());
+        residual(s, A32, cur, b, L.r.get());
         AmgLevel& C = levels_[static_cast<std::size_t>(l) + 1];
-        spmv(s, L.R, L.r.get(), C.b.get());
+        spmv(s, *L.R32, L.r.get(), C.b.get());
         vcycle(s, l + 1, C.b.get(), C.x.get());
-        spmv(s, L.P, C.x.get(), cur, L.alpha, 1.0);
+        spmv(s, *L.P32, C.x.get(), cur, L.alpha, 1.0);
         for (int k = 0; k < post; ++k)
         {
-            jacobi_sweep(s, A, cur, b, weights(post - 1 - k), om, other);
+            jacobi_sweep(s, A32, cur, b, weights(post - 1 - k), om, other);
             std::swap(cur, other);
         }
     }

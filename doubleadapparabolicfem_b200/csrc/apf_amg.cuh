@@ -30,6 +30,8 @@ namespace apf
         DeviceBuffer<double> w;       // per-row weights of the first pre-smoothing sweep (empty: omega D^-1)
         DeviceBuffer<double> w2;      // weights of the later pre-smoothing sweeps (empty: w)
         double alpha = 1.0;           // coarse-correction scale
+        // f32-valued sliced-ELLPACK copies of A, P, R for the V-cycle's SpMVs
+        std::unique_ptr<DeviceSell> A32, P32, R32;
     };
 
     class Amg

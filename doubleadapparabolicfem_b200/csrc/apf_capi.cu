@@ -192,6 +192,15 @@ int apf_ctx_create(int device, void* stream, apf_ctx** out)
             ctx->own_stream = true;
         }
         apf::upload_tables_once(device);
+        // The library's buffers come from this process's default stream-ordered pool.  Its
+        // default release threshold (0) hands freed memory back to the driver at every
+        // synchronisation, so each inner iteration would map its GBs of assembly, AMG and
+        // estimator buffers afresh; keeping freed memory in the pool makes the next
+        // iteration's allocations cheap.  (Process-local; released at exit.)
+        cudaMemPool_t pool;
+        APF_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        std::uint64_t keep = UINT64_MAX;
+        APF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     });
     if (rc != APF_OK)
         return rc;

@@ -104,11 +104,20 @@ namespace apf
     // padding entries have value 0 and column 0.
     struct DeviceSell
     {
+        int rows = 0;
         int slices = 0;
         DeviceBuffer<int> slice_ptr; // slices + 1 element offsets
         DeviceBuffer<int> col;
-        DeviceBuffer<double> val;
+        DeviceBuffer<double> val;    // f64 values, or empty when val32 holds them
+        DeviceBuffer<float> val32;   // f32 values (preconditioner copies; products accumulate in f64)
+        // CSR layout instead of slices (operators with few or long rows): row pointers and
+        // column indices of the source matrix, which must outlive this copy
+        const int* csr_rp = nullptr;
+        const int* csr_ci = nullptr;
+        double avg_row = 0.0;
     };
+    constexpr int kSellMinRows = 148 * 32 * 8; // below: too few slices to fill the GPU
+    constexpr double kSellMaxRow = 40.0;       // above: one thread per row serialises
 
     // Row-compressed sparse matrix resident on the device (int32 indices, f64 values).
     // `sell`, when built (build_sell), is used by the SpMV kernels instead of the CSR arrays;

@@ -17,9 +17,9 @@ namespace apf
 
         // G lanes per row; the row loop is warp-uniform so the shuffles see all 32 lanes.
         // MODE 0: y = alpha A x + beta y;  1: y = b - A x;  2: y = x + alpha dinv (b - A x)
-        template<int G, int MODE>
+        template<int G, int MODE, class V = double>
         __global__ void __launch_bounds__(256) spmv_kernel(int rows, const int* __restrict__ rp, const int* __restrict__ ci,
-                                                           const double* __restrict__ va, const double* __restrict__ x,
+                                                           const V* __restrict__ va, const double* __restrict__ x,
                                                            const double* __restrict__ b, double* __restrict__ y,
                                                            double alpha, double beta, const double* __restrict__ dinv)
         {
@@ -36,7 +36,7 @@ namespace apf
                 {
                     const int s0 = rp[r], e = rp[r + 1];
                     for (int k = s0 + lane; k < e; k += G)
-                        sum += va[k] * __ldg(x + ci[k]);
+                        sum += static_cast<double>(va[k]) * __ldg(x + ci[k]);
                 }
 #pragma unroll
                 for (int o = G / 2; o > 0; o >>= 1)
@@ -54,9 +54,9 @@ namespace apf
         }
 
         // SELL-32 SpMV: one thread per row, one warp per slice (same MODEs as spmv_kernel)
-        template<int MODE>
+        template<int MODE, class V>
         __global__ void __launch_bounds__(256) sell_kernel(int rows, int slices, const int* __restrict__ sp,
-                                                           const int* __restrict__ col, const double* __restrict__ val,
+                                                           const int* __restrict__ col, const V* __restrict__ val,
                                                            const double* __restrict__ x, const double* __restrict__ b,
                                                            double* __restrict__ y, double alpha, double beta,
                                                            const double* __restrict__ dinv)
@@ -68,17 +68,17 @@ namespace apf
             {
                 const int base = sp[sl];
                 const int width = (sp[sl + 1] - base) >> 5;
-                const double* v = val + base + lane;
+                const V* v = val + base + lane;
                 const int* c = col + base + lane;
                 double s0 = 0.0, s1 = 0.0;
                 int j = 0;
                 for (; j + 1 < width; j += 2)
                 {
-                    s0 += v[32 * j] * __ldg(x + c[32 * j]);
-                    s1 += v[32 * j + 32] * __ldg(x + c[32 * j + 32]);
+                    s0 += static_cast<double>(v[32 * j]) * __ldg(x + c[32 * j]);
+                    s1 += static_cast<double>(v[32 * j + 32]) * __ldg(x + c[32 * j + 32]);
                 }
                 if (j < width)
-                    s0 += v[32 * j] * __ldg(x + c[32 * j]);
+                    s0 += static_cast<double>(v[32 * j]) * __ldg(x + c[32 * j]);
                 const double sum = s0 + s1;
                 const int r = sl * 32 + lane;
                 if (r < rows)
@@ -91,6 +91,12 @@ namespace apf
                         y[r] = beta == 0.0 ? alpha * sum : alpha * sum + beta * y[r];
                 }
             }
+        }
+
+        __global__ void to_f32_kernel(long long n, const double* __restrict__ a, float* __restrict__ b)
+        {
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                b[i] = static_cast<float>(a[i]);
         }
 
         // slice widths x 32 (element counts per slice)
@@ -110,9 +116,10 @@ namespace apf
             }
         }
 
+        template<class V>
         __global__ void sell_fill(int rows, int slices, const int* __restrict__ rp, const int* __restrict__ ci,
                                   const double* __restrict__ va, const int* __restrict__ sp, int* __restrict__ col,
-                                  double* __restrict__ val)
+                                  V* __restrict__ val)
         {
             const int lane = threadIdx.x & 31;
             const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -128,7 +135,7 @@ namespace apf
                 {
                     const int o = base + 32 * j + lane;
                     col[o] = j < len ? ci[b + j] : 0;
-                    val[o] = j < len ? va[b + j] : 0.0;
+                    val[o] = static_cast<V>(j < len ? va[b + j] : 0.0);
                 }
             }
         }
@@ -385,6 +392,41 @@ namespace apf
 
     namespace
     {
+        // G lanes per row from the mean row length
+        template<class F>
+        void with_lanes(double avg, F&& go)
+        {
+            if (avg <= 6) go(std::integral_constant<int, 4>{});
+            else if (avg <= 14) go(std::integral_constant<int, 8>{});
+            else if (avg <= 40) go(std::integral_constant<int, 16>{});
+            else go(std::integral_constant<int, 32>{});
+        }
+
+        template<int MODE>
+        void sell_launch(cudaStream_t s, const DeviceSell& S, const double* x, const double* b, double* y, double alpha,
+                         double beta, const double* dinv)
+        {
+            if (S.csr_rp)
+            {
+                // CSR layout with f32 values (short or wide-row operators)
+                with_lanes(S.avg_row, [&](auto g) {
+                    constexpr int G = decltype(g)::value;
+                    spmv_kernel<G, MODE, float><<<blocks_for((long long)S.rows * G, 256, 148 * 64), 256, 0, s>>>(
+                        S.rows, S.csr_rp, S.csr_ci, S.val32.get(), x, b, y, alpha, beta, dinv);
+                });
+                APF_CUDA(cudaGetLastError());
+                return;
+            }
+            const int grid = blocks_for((long long)S.slices * 32, 256, 148 * 64);
+            if (S.val32.size())
+                sell_kernel<MODE, float><<<grid, 256, 0, s>>>(S.rows, S.slices, S.slice_ptr.get(), S.col.get(),
+                                                              S.val32.get(), x, b, y, alpha, beta, dinv);
+            else
+                sell_kernel<MODE, double><<<grid, 256, 0, s>>>(S.rows, S.slices, S.slice_ptr.get(), S.col.get(),
+                                                               S.val.get(), x, b, y, alpha, beta, dinv);
+            APF_CUDA(cudaGetLastError());
+        }
+
         template<int MODE>
         void spmv_dispatch(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, double* y, double alpha,
                            double beta, const double* dinv = nullptr, const char* name = nullptr)
@@ -396,10 +438,7 @@ namespace apf
             APF_KERNEL(name ? name : (MODE == 1 ? "residual" : (MODE == 2 ? "jacobi_sweep" : "spmv")), s);
             if (A.sell)
             {
-                const DeviceSell& S = *A.sell;
-                sell_kernel<MODE><<<blocks_for((long long)S.slices * 32, threads, 148 * 64), threads, 0, s>>>(
-                    A.rows, S.slices, S.slice_ptr.get(), S.col.get(), S.val.get(), x, b, y, alpha, beta, dinv);
-                APF_CUDA(cudaGetLastError());
+                sell_launch<MODE>(s, *A.sell, x, b, y, alpha, beta, dinv);
                 return;
             }
             auto go = [&](auto g) {
@@ -428,6 +467,7 @@ namespace apf
             sell_count<<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), cnt.get());
         }
         auto S = std::make_unique<DeviceSell>();
+        S->rows = A.rows;
         S->slices = slices;
         S->slice_ptr.allocate(static_cast<std::size_t>(slices) + 1, s);
         const long long total = exclusive_scan(cnt.get(), S->slice_ptr.get(), slices, s);
@@ -437,12 +477,81 @@ namespace apf
         S->val.allocate(static_cast<std::size_t>(total), s);
         {
             APF_KERNEL("sell_fill", s);
-            sell_fill<<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), A.col_idx.get(), A.values.get(),
-                                          S->slice_ptr.get(), S->col.get(), S->val.get());
+            sell_fill<double><<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), A.col_idx.get(), A.values.get(),
+                                                  S->slice_ptr.get(), S->col.get(), S->val.get());
         }
         APF_CUDA(cudaGetLastError());
         A.sell = std::move(S);
         return true;
+    }
+
+    std::unique_ptr<DeviceSell> make_sell32(cudaStream_t s, const DeviceCsr& A)
+    {
+        auto S = std::make_unique<DeviceSell>();
+        S->rows = A.rows;
+        S->avg_row = A.rows ? static_cast<double>(A.nnz()) / A.rows : 0.0;
+        if (A.rows < kSellMinRows || S->avg_row > kSellMaxRow)
+        {
+            // few rows or long rows: one thread per row would leave the GPU idle or
+            // serialise long loops; keep the CSR arrays and lanes per row, f32 values
+            S->csr_rp = A.row_ptr.get();
+            S->csr_ci = A.col_idx.get();
+            S->val32.allocate(static_cast<std::size_t>(A.nnz()), s);
+            if (A.nnz())
+            {
+                APF_KERNEL("sell_fill", s);
+                to_f32_kernel<<<blocks_for(A.nnz(), 256, 148 * 32), 256, 0, s>>>(A.nnz(), A.values.get(), S->val32.get());
+            }
+            APF_CUDA(cudaGetLastError());
+            return S;
+        }
+        S->slices = (A.rows + 31) / 32;
+        S->slice_ptr.allocate(static_cast<std::size_t>(S->slices) + 1, s);
+        if (A.rows == 0)
+            return S;
+        DeviceBuffer<int> cnt(S->slices, s);
+        const int grid = blocks_for((long long)S->slices * 32, 256, 148 * 32);
+        {
+            APF_KERNEL("sell_count", s);
+            sell_count<<<grid, 256, 0, s>>>(A.rows, S->slices, A.row_ptr.get(), cnt.get());
+        }
+        const long long total = exclusive_scan(cnt.get(), S->slice_ptr.get(), S->slices, s);
+        S->col.allocate(static_cast<std::size_t>(total), s);
+        S->val32.allocate(static_cast<std::size_t>(total), s);
+        if (total)
+        {
+            APF_KERNEL("sell_fill", s);
+            sell_fill<float><<<grid, 256, 0, s>>>(A.rows, S->slices, A.row_ptr.get(), A.col_idx.get(), A.values.get(),
+                                                 S->slice_ptr.get(), S->col.get(), S->val32.get());
+        }
+        APF_CUDA(cudaGetLastError());
+        return S;
+    }
+
+    void spmv(cudaStream_t s, const DeviceSell& A, const double* x, double* y, double alpha, double beta,
+              const char* name)
+    {
+        if (A.rows == 0)
+            return;
+        APF_KERNEL(name ? name : "spmv", s);
+        sell_launch<0>(s, A, x, nullptr, y, alpha, beta, nullptr);
+    }
+
+    void jacobi_sweep(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, const double* dinv,
+                      double omega, double* y)
+    {
+        if (A.rows == 0)
+            return;
+        APF_KERNEL("jacobi_sweep", s);
+        sell_launch<2>(s, A, x, b, y, omega, 0.0, dinv);
+    }
+
+    void residual(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, double* r)
+    {
+        if (A.rows == 0)
+            return;
+        APF_KERNEL("residual", s);
+        sell_launch<1>(s, A, x, b, r, 1.0, 0.0, nullptr);
     }
 
     void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha, double beta, const char* name)

@@ -26,6 +26,15 @@ namespace apf
     // Build A.sell (sliced ELLPACK) unless its padding would exceed max_padding x nnz;
     // returns whether it was built.
     bool build_sell(cudaStream_t s, DeviceCsr& A, double max_padding = 1.35);
+    // A sliced-ELLPACK copy of A with f32 values (always built): for the V-cycle operators,
+    // whose rounding to f32 keeps them symmetric and fixed.
+    std::unique_ptr<DeviceSell> make_sell32(cudaStream_t s, const DeviceCsr& A);
+    // the SpMV family on such a copy (same semantics as the DeviceCsr versions below)
+    void spmv(cudaStream_t s, const DeviceSell& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0,
+              const char* name = nullptr);
+    void jacobi_sweep(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, const double* dinv,
+                      double omega, double* y);
+    void residual(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, double* r);
     // y = alpha * A x + beta * y   (beta == 0 ignores y's old contents)
     void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0,
               const char* name = nullptr);
