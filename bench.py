@@ -11,10 +11,10 @@ A step = the hot path of one inner iteration over one mesh, as
 compute_adaptive_test_space_iteration runs it: main-system assembly (A_y, B, B^T,
 C_signed, K, f, g), the parabolic graph-norm block Hhat, the block preconditioner's
 set-up, MINRES to FP64 true relative residual 1e-8, and the equilibrated-flux estimator
-(slab reconstruction, vertex-patch flux solves, per-cell indicators), from inputs
-already in HBM.  ``e2e`` = the same through the C ABI from pinned host buffers (H2D of
-the mesh inputs and D2H of the solution and the per-cell indicators inside the timed
-region).
+(slab reconstruction, vertex-patch flux solves, per-cell indicators) and the driver's
+X-marking indicators, from inputs already in HBM.  ``e2e`` = the same through the C ABI
+from pinned host buffers (H2D of the mesh inputs and D2H of the solution and the
+per-cell Y and X indicators inside the timed region).
 
 Multi-GPU: the path runs one problem per GPU (replicas; no collective in the data
 path).  ``value`` = total DOFs processed by all ranks / max-over-ranks time.
@@ -235,7 +235,10 @@ def run_ours(args, world, rank, local):
     x_host = torch.empty(n_dofs, dtype=torch.float64).pin_memory()
     eta_host = torch.empty(ny, dtype=torch.float64).pin_memory()
     eta_dev = torch.empty(ny, dtype=torch.float64, device=dev)
-    d2h_bytes = n_dofs * 8 + (ny * 8 if run_estimator else 0)
+    nx = host.n_x_cells
+    etax_host = torch.empty(nx, dtype=torch.float64).pin_memory()
+    etax_dev = torch.empty(nx, dtype=torch.float64, device=dev)
+    d2h_bytes = n_dofs * 8 + ((ny + nx) * 8 if run_estimator else 0)
     sopt = _lib.SolverOptions()
     lib.apf_solver_options_default(C.byref(sopt))
     sopt.tolerance = args.tol
@@ -265,7 +268,13 @@ def run_ours(args, world, rank, local):
                 ctx.check(lib.apf_estimate(ctx.handle, h, C.c_void_p(prob.y_vertex_ids.data_ptr()),
                                            1 if on_device else 0, None, None, None, C.c_void_p(eta.data_ptr()),
                                            C.byref(res)))
-                est_results.append({k: getattr(res, k) for k, _ in res._fields_})
+                xt = _lib.XIndicatorTotals()
+                etax = etax_dev if on_device else etax_host
+                ctx.check(lib.apf_x_indicators(ctx.handle, h, 1 if on_device else 0, None, None, None,
+                                               C.c_void_p(etax.data_ptr()), C.byref(xt)))
+                r = {k: getattr(res, k) for k, _ in res._fields_}
+                r.update({"x_" + k: getattr(xt, k) for k, _ in xt._fields_})
+                est_results.append(r)
         except Exception:
             lib.apf_system_destroy(h)
             raise
@@ -398,7 +407,8 @@ def run_ours(args, world, rank, local):
         "config": {"workload": f"2+1D heat, u0=sin(pi x)sin(pi y), uniform outer level {args.level} P{args.p} "
                                f"({ny} prisms, {n_dofs} DOFs)",
                    "stages": ["assembly", "graph_norm", "amg_setup", "minres"] +
-                             (["slab_reconstruction", "patch_fluxes", "indicators"] if run_estimator else []),
+                             (["slab_reconstruction", "patch_fluxes", "indicators", "x_indicators"]
+                              if run_estimator else []),
                    "tolerance": args.tol,
                    "preconditioner": ("learned smoother weights in the blkdiag(A_y, Hhat) SA-AMG V-cycles "
                                       "(plain fallback)" if plain else
@@ -411,6 +421,7 @@ def run_ours(args, world, rank, local):
                    "final_true_residual_max": max(d["final_true_residual"] for d in timed_diags),
                    "e2e_final_true_residual_max": max(d["final_true_residual"] for d in e2e_diags),
                    "flux_squared": timed_est[-1]["flux_squared"] if timed_est else None,
+                   "x_eta_squared": timed_est[-1]["x_eta_squared"] if timed_est else None,
                    "n_patches": timed_est[-1]["n_patches"] if timed_est else None,
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (mesh inputs %.0f MB; K %d nnz, Hhat %d nnz)" % (h2d_bytes / 1e6, nnz_k,

@@ -187,3 +187,11 @@ SIGNATURES.update({
     "apf_amg_level_weights": ([_P, _P, C.c_int, C.c_int, C.c_int, _P], C.c_int),
     "apf_amg_level_features": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
 })
+
+
+class XIndicatorTotals(C.Structure):
+    _fields_ = [("lambda_y_squared", C.c_double), ("initial_trace_squared", C.c_double), ("eta_squared", C.c_double)]
+
+
+SIGNATURES["apf_x_indicators"] = ([_P, _P, C.c_int, _P, _P, _P, _P, C.POINTER(XIndicatorTotals)], C.c_int)
+SIGNATURES["apf_y_estimator_threshold_squared"] = ([C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)], C.c_int)

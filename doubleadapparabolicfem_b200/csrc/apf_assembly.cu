@@ -414,6 +414,15 @@ namespace apf
             return 0.0;
         }
 
+        struct XIndArgs
+        {
+            int p, n_y, n_x, n_bottom, u0_kind;
+            const double *y_geo, *x_geo, *m_y;
+            const int *y_off, *y_dofs, *x_off, *x_dofs, *bottom;
+            const double *y_w, *x_w, *lambda, *u;
+            double *lam_y, *trace_x;
+        };
+
         __device__ double local_vector(const VecArgs& A, int c, int i)
         {
             const RefTables& t = c_tab[A.d.p - 1];
@@ -1173,5 +1182,187 @@ namespace apf
         sync(s);
         if (in.kmax < 1)
             in.kmax = 1;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// X-marking indicators of the adaptive driver (algorithm/detail/indicator_utilities.hpp:
+// compute_x_marking_indicator_components :443-473, compute_spatial_energy_squared_by_active_cell
+// :115-171, aggregate_to_x_active_cells :405-433, compute_initial_trace_mismatch_squared_by_x_cell
+// :336-400)
+// ---------------------------------------------------------------------------------------
+namespace apf
+{
+    namespace
+    {
+        // nodal values of a true-DOF vector on local DOF i of cell c (restriction row)
+        __device__ __forceinline__ double local_value(const int* off, const int* dofs, const double* w, const double* v,
+                                                      long long row)
+        {
+            double s = 0.0;
+            for (int e = off[row]; e < off[row + 1]; ++e)
+                s += w[e] * v[dofs[e]];
+            return s;
+        }
+
+        // lambda_y^2_K = int_K grad_x lambda . M grad_x lambda: the local A_y energy of lambda_delta
+        __global__ void lambda_energy_kernel(XIndArgs A)
+        {
+            const RefTables& t = c_tab[A.p - 1];
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n_y; c += gridDim.x * blockDim.x)
+            {
+                double lam[kMaxNs * kMaxNt];
+                for (int i = 0; i < t.ndof; ++i)
+                    lam[i] = local_value(A.y_off, A.y_dofs, A.y_w, A.lambda, static_cast<long long>(c) * t.ndof + i);
+                const CellGeo g = load_geo(A.y_geo, c);
+                double q00, q01, q11;
+                q_form(g, A.m_y, c, q00, q01, q11);
+                double e = 0.0;
+                for (int i = 0; i < t.ndof; ++i)
+                {
+                    const int s = i / t.nt, a = i % t.nt;
+                    double row = 0.0;
+                    for (int j = 0; j < t.ndof; ++j)
+                    {
+                        const int r = j / t.nt, b = j % t.nt;
+                        row += t.Mt[a][b] * ks(t, q00, q01, q11, s, r) * lam[j];
+                    }
+                    e += lam[i] * row;
+                }
+                A.lam_y[c] = g.det * g.ht * e;
+            }
+        }
+
+        // ||u0 - u_delta(., 0)||^2 on the bottom face of every X cell at t = 0 (bottom Duffy rule)
+        __global__ void initial_trace_kernel(XIndArgs A)
+        {
+            const RefTables& t = c_tab[A.p - 1];
+            for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < A.n_bottom; k += gridDim.x * blockDim.x)
+            {
+                const int c = A.bottom[k];
+                double u[kMaxNs * kMaxNt];
+                for (int i = 0; i < t.ndof; ++i)
+                    u[i] = local_value(A.x_off, A.x_dofs, A.x_w, A.u, static_cast<long long>(c) * t.ndof + i);
+                const CellGeo g = load_geo(A.x_geo, c);
+                double acc = 0.0;
+                for (int q = 0; q < t.nbq; ++q)
+                {
+                    const double xi = t.bq_pts[q][0], eta = t.bq_pts[q][1];
+                    const double x = g.x0 + g.J00 * xi + g.J01 * eta;
+                    const double y = g.y0 + g.J10 * xi + g.J11 * eta;
+                    double uh = 0.0;
+                    for (int s = 0; s < t.ns; ++s)
+                        for (int a = 0; a < t.nt; ++a)
+                            uh += u[s * t.nt + a] * t.bq_T[q][s] * t.S0[a];
+                    const double d = u0_value(A.u0_kind, x, y) - uh;
+                    acc += d * d * g.det * t.bq_w[q];
+                }
+                A.trace_x[c] = acc;
+            }
+        }
+
+        __global__ void child_count_kernel(int n_y, const int* __restrict__ y_to_x, int* __restrict__ cnt)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_y; c += gridDim.x * blockDim.x)
+                atomicAdd(cnt + y_to_x[c], 1);
+        }
+
+        __global__ void child_fill_kernel(int n_y, const int* __restrict__ y_to_x, const int* __restrict__ ptr,
+                                          int* __restrict__ cursor, int* __restrict__ child)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_y; c += gridDim.x * blockDim.x)
+            {
+                const int x = y_to_x[c];
+                child[ptr[x] + atomicAdd(cursor + x, 1)] = c;
+            }
+        }
+
+        // per X cell: sum of its Y children's lambda energies in ascending Y order (children
+        // sorted in place: the fill order of the atomics is not deterministic), plus the trace
+        __global__ void aggregate_kernel(int n_x, const int* __restrict__ ptr, int* __restrict__ child,
+                                         const double* __restrict__ lam_y, const double* __restrict__ trace_x,
+                                         double* __restrict__ lam_x, double* __restrict__ eta_x)
+        {
+            for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n_x; x += gridDim.x * blockDim.x)
+            {
+                const int b = ptr[x], e = ptr[x + 1];
+                for (int i = b + 1; i < e; ++i)
+                {
+                    const int v = child[i];
+                    int j = i - 1;
+                    while (j >= b && child[j] > v)
+                    {
+                        child[j + 1] = child[j];
+                        --j;
+                    }
+                    child[j + 1] = v;
+                }
+                double s = 0.0;
+                for (int i = b; i < e; ++i)
+                    s += lam_y[child[i]];
+                lam_x[x] = s;
+                eta_x[x] = s + trace_x[x];
+            }
+        }
+    }
+
+    void x_indicators(cudaStream_t s, const SystemInputs& in, const double* lambda, const double* u, double* lam_y,
+                      double* lam_x, double* trace_x, double* eta_x)
+    {
+        XIndArgs a{};
+        a.p = in.p;
+        a.n_y = in.n_y_cells;
+        a.n_x = in.n_x_cells;
+        a.n_bottom = in.n_bottom;
+        a.y_geo = in.y_geo.get();
+        a.x_geo = in.x_geo.get();
+        a.m_y = in.m_y.size() ? in.m_y.get() : nullptr;
+        a.y_off = in.y_off.get();
+        a.y_dofs = in.y_dofs.get();
+        a.y_w = in.y_w.get();
+        a.x_off = in.x_off.get();
+        a.x_dofs = in.x_dofs.get();
+        a.x_w = in.x_w.get();
+        a.bottom = in.bottom_list.get();
+        a.u0_kind = in.u0_kind;
+        a.lambda = lambda;
+        a.u = u;
+        a.lam_y = lam_y;
+        a.trace_x = trace_x;
+        if (in.n_x_cells > 0)
+            APF_CUDA(cudaMemsetAsync(trace_x, 0, sizeof(double) * in.n_x_cells, s));
+        if (in.n_y_cells > 0)
+        {
+            APF_KERNEL("xind_lambda_energy", s);
+            lambda_energy_kernel<<<grid_for(in.n_y_cells, 128), 128, 0, s>>>(a);
+        }
+        if (in.n_bottom > 0)
+        {
+            APF_KERNEL("xind_initial_trace", s);
+            initial_trace_kernel<<<grid_for(in.n_bottom, 128), 128, 0, s>>>(a);
+        }
+        DeviceBuffer<int> cnt(static_cast<std::size_t>(in.n_x_cells) + 1, s), ptr(static_cast<std::size_t>(in.n_x_cells) + 1, s),
+            cursor(static_cast<std::size_t>(in.n_x_cells) + 1, s), child(static_cast<std::size_t>(std::max(in.n_y_cells, 1)), s);
+        cnt.zero();
+        cursor.zero();
+        if (in.n_y_cells > 0)
+        {
+            APF_KERNEL("xind_child_count", s);
+            child_count_kernel<<<grid_for(in.n_y_cells, 256), 256, 0, s>>>(in.n_y_cells, in.y_to_x.get(), cnt.get());
+        }
+        exclusive_scan(cnt.get(), ptr.get(), in.n_x_cells, s);
+        if (in.n_y_cells > 0)
+        {
+            APF_KERNEL("xind_child_fill", s);
+            child_fill_kernel<<<grid_for(in.n_y_cells, 256), 256, 0, s>>>(in.n_y_cells, in.y_to_x.get(), ptr.get(),
+                                                                         cursor.get(), child.get());
+        }
+        if (in.n_x_cells > 0)
+        {
+            APF_KERNEL("xind_aggregate", s);
+            aggregate_kernel<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, ptr.get(), child.get(), lam_y,
+                                                                        trace_x, lam_x, eta_x);
+        }
+        APF_CUDA(cudaGetLastError());
     }
 }

@@ -604,6 +604,47 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
     });
 }
 
+int apf_x_indicators(apf_ctx* ctx, apf_system* sys, int pointers_on_device, double* lambda_by_y, double* lambda_by_x,
+                     double* trace_by_x, double* eta_by_x, apf_x_indicator_totals* totals)
+{
+    if (!ctx || !sys)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        auto& S = sys->sys;
+        const auto& in = S.in;
+        apf::require(S.solution.size() == static_cast<std::size_t>(in.n_lambda) + in.n_u, APF_ERR_INVALID,
+                     "X indicators: solve the main system first");
+        cudaStream_t s = ctx->stream;
+        const int ny = in.n_y_cells, nx = in.n_x_cells;
+        apf::DeviceBuffer<double> ly(ny, s), lx(nx, s), tx(nx, s), ex(nx, s);
+        apf::x_indicators(s, in, S.solution.get(), S.solution.get() + in.n_lambda, ly.get(), lx.get(), tx.get(),
+                          ex.get());
+        const cudaMemcpyKind kind = pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (lambda_by_y && ny) APF_CUDA(cudaMemcpyAsync(lambda_by_y, ly.get(), ny * sizeof(double), kind, s));
+        if (lambda_by_x && nx) APF_CUDA(cudaMemcpyAsync(lambda_by_x, lx.get(), nx * sizeof(double), kind, s));
+        if (trace_by_x && nx) APF_CUDA(cudaMemcpyAsync(trace_by_x, tx.get(), nx * sizeof(double), kind, s));
+        if (eta_by_x && nx) APF_CUDA(cudaMemcpyAsync(eta_by_x, ex.get(), nx * sizeof(double), kind, s));
+        if (totals)
+        {
+            S.ws.ensure(s);
+            totals->lambda_y_squared = apf::dot_host(s, S.ws, nx, lx.get(), nullptr);
+            totals->initial_trace_squared = apf::dot_host(s, S.ws, nx, tx.get(), nullptr);
+            totals->eta_squared = totals->lambda_y_squared + totals->initial_trace_squared;
+        }
+        apf::sync(s);
+    });
+}
+
+int apf_y_estimator_threshold_squared(double rho, double lambda_y_squared, double initial_trace_squared,
+                                      double* threshold_squared)
+{
+    if (!threshold_squared || !(rho > 0.0))
+        return APF_ERR_INVALID;
+    const double shifted = rho + 0.5;
+    *threshold_squared = rho * rho * (lambda_y_squared + (1.0 + 1.0 / (shifted * shifted)) * initial_trace_squared);
+    return APF_OK;
+}
+
 int apf_true_residual_noalloc(apf_ctx* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_idx,
                               const double* values, const double* x, const double* b, double* absolute_residual,
                               double* relative_residual)

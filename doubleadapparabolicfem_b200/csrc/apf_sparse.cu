@@ -146,7 +146,7 @@ namespace apf
             __shared__ double ws[kRedThreads / 32];
             double s = 0.0;
             for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-                s += a[i] * b[i];
+                s += b ? a[i] * b[i] : a[i];
             for (int o = 16; o > 0; o >>= 1)
                 s += __shfl_down_sync(0xffffffffu, s, o);
             if ((threadIdx.x & 31) == 0)

@@ -43,7 +43,7 @@ namespace apf
                       double omega, double* y);
     // r = b - A x
     void residual(cudaStream_t s, const DeviceCsr& A, const double* x, const double* b, double* r);
-    // out = dot(a, b) written to a device scalar (deterministic)
+    // out = dot(a, b) written to a device scalar (deterministic); b = null: the sum of a
     void dot_device(cudaStream_t s, Workspace& w, int n, const double* a, const double* b, double* out);
     double dot_host(cudaStream_t s, Workspace& w, int n, const double* a, const double* b);
     // C = A * B (pattern = all candidate products, duplicates summed in a fixed order)

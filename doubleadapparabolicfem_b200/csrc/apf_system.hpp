@@ -69,6 +69,11 @@ namespace apf
     // level separately (its low-energy modes are arbitrary in time, smooth in space)
     void dof_time_components(cudaStream_t s, const SystemInputs& in, bool y_space, DeviceBuffer<int>& comp);
     void prepare_inputs(cudaStream_t s, SystemInputs& in);
+    // X-marking indicators from lambda_delta (Y true DOFs) and u_delta (X true DOFs), all
+    // device arrays: per Y cell lambda energy, per X cell its aggregate, the initial-trace
+    // mismatch (0 off the t = 0 layer) and their sum
+    void x_indicators(cudaStream_t s, const SystemInputs& in, const double* lambda, const double* u, double* lam_y,
+                      double* lam_x, double* trace_x, double* eta_x);
     Incidence build_incidence(cudaStream_t s, int n_dofs, int n_asm, const int* cell_list, const int* src_map,
                               const int* offsets, const int* dofs, int ndof);
     void gather_csr(cudaStream_t s, const SystemInputs& in, double zero_tol, int n_rows, int n_cols, int n_terms,

@@ -41,3 +41,33 @@ def estimate(blocks: MainSystemBlocks, y_vertex_ids: np.ndarray | None = None):
                                    C.byref(res)))
     totals = {name: getattr(res, name) for name, _ in res._fields_}
     return out, totals
+
+
+def x_marking_indicator_components(blocks: MainSystemBlocks):
+    """The adaptive driver's X-marking indicators on the last solve, mirroring
+    ``adaptive_algorithm::detail::compute_x_marking_indicator_components``
+    (algorithm/detail/indicator_utilities.hpp:443-473).  Returns per-cell arrays
+    ``lambda_y_squared_by_y_cell`` (Y cells), ``lambda_y_squared_by_x_cell``,
+    ``initial_trace_squared_by_x_cell`` (0 off the t = 0 layer), ``eta_squared_by_x_cell``
+    (X cells, input order) and the totals."""
+    ny, nx = blocks.problem.n_y_cells, blocks.problem.n_x_cells
+    out = {"lambda_y_squared_by_y_cell": np.empty(ny), "lambda_y_squared_by_x_cell": np.empty(nx),
+           "initial_trace_squared_by_x_cell": np.empty(nx), "eta_squared_by_x_cell": np.empty(nx)}
+    tot = _lib.XIndicatorTotals()
+    ctx = blocks.ctx
+    ctx.check(ctx.lib.apf_x_indicators(ctx.handle, blocks.handle, 0, _ptr(out["lambda_y_squared_by_y_cell"]),
+                                       _ptr(out["lambda_y_squared_by_x_cell"]),
+                                       _ptr(out["initial_trace_squared_by_x_cell"]),
+                                       _ptr(out["eta_squared_by_x_cell"]), C.byref(tot)))
+    return out, {name: getattr(tot, name) for name, _ in tot._fields_}
+
+
+def y_estimator_threshold_squared(rho: float, lambda_y_squared: float, initial_trace_squared: float) -> float:
+    """rho^2 (lambda^2 + (1 + 1/(rho + 1/2)^2) trace^2)
+    (algorithm/detail/indicator_utilities.hpp:475-491); raises for rho <= 0."""
+    lib = _lib.load()
+    out = C.c_double()
+    rc = lib.apf_y_estimator_threshold_squared(rho, lambda_y_squared, initial_trace_squared, C.byref(out))
+    if rc != _lib.APF_OK:
+        raise _lib.ApfError(rc, "compute_y_estimator_threshold_squared: rho must be positive.")
+    return out.value

@@ -231,6 +231,32 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
                  double* flux_squared, double* divergence_squared, double* reconstruction_squared,
                  double* eta_squared, apf_estimator_result* result);
 
+/* ---- X-marking indicators -------------------------------------------------------- */
+/* Totals of XMarkingIndicatorComponents (algorithm/adaptive_result.hpp:294-320). */
+typedef struct apf_x_indicator_totals
+{
+    double lambda_y_squared;      /* sum_K int_K grad_x lambda . M grad_x lambda */
+    double initial_trace_squared; /* sum_K ||u0 - u(., 0)||^2 over the t = 0 faces */
+    double eta_squared;           /* their sum */
+} apf_x_indicator_totals;
+
+/* The adaptive driver's X-marking indicators on the solution of the last apf_solve_minres
+ * call, replacing compute_x_marking_indicator_components
+ * (algorithm/detail/indicator_utilities.hpp:443-473):
+ *   lambda_by_y[K] = int_K grad_x lambda_delta . M grad_x lambda_delta  (per Y cell, :115-171),
+ *   lambda_by_x    = lambda_by_y summed onto each Y cell's X ancestor (:405-433),
+ *   trace_by_x[K]  = ||u0 - u_delta(., 0)||^2 on the t = 0 face of X cell K, 0 elsewhere
+ *                    (:336-400, the bottom Duffy rule of the main assembly),
+ *   eta_by_x       = lambda_by_x + trace_by_x.
+ * Arrays (any may be NULL): n_y_cells / n_x_cells values, host or device. */
+int apf_x_indicators(apf_ctx* ctx, apf_system* sys, int pointers_on_device, double* lambda_by_y, double* lambda_by_x,
+                     double* trace_by_x, double* eta_by_x, apf_x_indicator_totals* totals);
+/* rho^2 (lambda^2 + (1 + 1/(rho + 1/2)^2) trace^2), replacing
+ * compute_y_estimator_threshold_squared (indicator_utilities.hpp:475-491); rho <= 0 gives
+ * APF_ERR_INVALID (the reference throws). */
+int apf_y_estimator_threshold_squared(double rho, double lambda_y_squared, double initial_trace_squared,
+                                      double* threshold_squared);
+
 /* ---- allocation-free residual check ---------------------------------------------- */
 /* No counterpart in the reference: an addition for callers that cannot allocate device
  * memory where they need the check -- e.g. a solver loop whose device memory is all owned

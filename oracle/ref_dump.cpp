@@ -40,6 +40,7 @@
 #include "finite_element/assembly/main_system/parabolic_graph_norm.hpp"
 #include "finite_element/assembly/constrained_dofs.hpp"
 #include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
+#include "algorithm/detail/indicator_utilities.hpp"
 #include "mesh/mesh_traits.hpp"
 
 #include "npy.hpp"
@@ -321,6 +322,23 @@ namespace
                 }
                 apf_oracle::write_npy(dir + "/" + name + ".npy", vals);
             };
+            // the driver's X-marking indicators (adaptive_driver.hpp:355-367)
+            const auto xi = adaptive_algorithm::detail::compute_x_marking_indicator_components<QSpace, QTime>(
+                x_space, state.lambda_delta, state.u_delta, example.problem.u0, example.problem.M);
+            auto dump_over = [&](const std::string& name, const std::vector<int>& cells, const auto& m) {
+                std::vector<double> vals;
+                for (const int c : cells)
+                {
+                    const auto it = m.find(c);
+                    vals.push_back(it == m.end() ? std::numeric_limits<double>::quiet_NaN() : it->second);
+                }
+                apf_oracle::write_npy(dir + "/" + name + ".npy", vals);
+            };
+            const std::vector<int> xcv(x_cells.begin(), x_cells.end());
+            dump_map("xind_lambda_by_y", xi.lambda_y_squared_by_y_cell.by_source_cell);
+            dump_over("xind_lambda_by_x", xcv, xi.lambda_y_squared_by_x_cell.by_source_cell);
+            dump_over("xind_trace_by_x", xcv, xi.initial_trace_squared_by_x_cell.by_source_cell);
+            dump_over("xind_eta_by_x", xcv, xi.eta_squared_by_x_cell.by_source_cell);
             dump_map("est_flux", state.flux_diagnostics.by_source_cell_flux);
             dump_map("est_div", state.flux_diagnostics.by_source_cell_residual);
             dump_map("est_recon", state.reconstruction_y_squared.by_source_cell);

@@ -4,7 +4,7 @@ Runs oracle/_ref/apf_ref_dump (the reference's own templates compiled by
 oracle/Makefile against oracle/shim) on small uniform meshes and packs each case
 into one .npz: mesh and DOF maps, assembled blocks, and the reference's whole inner
 iteration (direct main solve, slab reconstruction, vertex-patch flux solves,
-per-cell indicators).  Also extracts the uniform-refinement rows (exact DOF counts and
+per-cell indicators) and the driver's X-marking indicators.  Also extracts the uniform-refinement rows (exact DOF counts and
 6-significant-digit estimator values) of the reference's published paper data
 (algorithm_data_plot/{1d,2d}/*.csv) into paper_uniform_rows.json.
 
@@ -67,7 +67,7 @@ def main():
                         "dimension", "example", "p", "outer_iteration", "x_true_dofs_before",
                         "y_true_dofs_after", "eta_squared", "y_flux_squared", "y_reconstruction_squared",
                         "divergence_residual_squared", "y_estimator_squared", "iteration_seconds", "source_group",
-                        "job_id")})
+                        "job_id", "lambda_y_squared", "configured_rho", "y_estimator_threshold_squared")})
     with open(os.path.join(HERE, "paper_uniform_rows.json"), "w") as fh:
         json.dump(rows, fh, indent=0)
     print("wrote paper_uniform_rows.json", len(rows))

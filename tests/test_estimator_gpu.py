@@ -56,3 +56,46 @@ def test_estimator_matches_published_paper_values(gpu_ctx):
         _, (_, totals) = _solve_and_estimate(gpu_ctx, uniform_problem(level, 1), tol=1e-10)
         got = totals["flux_squared"]
         assert abs(got - by_level[level]) <= 1e-5 * by_level[level], (level, got, by_level[level])
+
+
+@pytest.mark.parametrize("name", P1_CASES + ["p2_l1_smooth"])
+def test_x_indicators_match_reference(gpu_ctx, name):
+    """The driver's X-marking indicators (per Y cell lambda energy, per X cell aggregate,
+    initial-trace mismatch, eta) against the reference's own, 1e-9 of the largest cell."""
+    from doubleadapparabolicfem_b200.assembly import assemble_main_system_blocks
+    from doubleadapparabolicfem_b200.estimator import x_marking_indicator_components
+    from doubleadapparabolicfem_b200.solver import SolverOptions, solve_saddle_system_with_preconditioner
+    prob, ref, example = load_golden(name)
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    blocks = assemble_main_system_blocks(to_product_problem(prob, example), ctx=gpu_ctx)
+    blocks.assemble_parabolic_graph_norm_approximation()
+    solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=1e-13, amg_coarse_size=64), copy_out=False)
+    cells, totals = x_marking_indicator_components(blocks)
+    pairs = [("lambda_y_squared_by_y_cell", "xind_lambda_by_y"), ("lambda_y_squared_by_x_cell", "xind_lambda_by_x"),
+             ("initial_trace_squared_by_x_cell", "xind_trace_by_x"), ("eta_squared_by_x_cell", "xind_eta_by_x")]
+    for mine, theirs in pairs:
+        r = np.nan_to_num(z[theirs], nan=0.0)
+        scale = max(np.abs(r).max(), 1e-300)
+        assert np.abs(cells[mine] - r).max() <= 1e-9 * scale, mine
+    assert abs(totals["eta_squared"] - np.nansum(z["xind_eta_by_x"])) <= 1e-10 * np.nansum(z["xind_eta_by_x"])
+
+
+def test_x_indicators_match_published_paper_values(gpu_ctx):
+    """Uniform outer levels 1-5 of the smooth_initial P1 runs: lambda_y_squared and
+    eta_squared to the CSV's 6 digits."""
+    from doubleadapparabolicfem_b200.assembly import assemble_main_system_blocks
+    from doubleadapparabolicfem_b200.estimator import x_marking_indicator_components
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    from doubleadapparabolicfem_b200.solver import SolverOptions, solve_saddle_system_with_preconditioner
+    with open(os.path.join(GOLDEN, "paper_uniform_rows.json")) as fh:
+        rows = {int(r["outer_iteration"]): r for r in json.load(fh) if r["dimension"] == "2d" and r["p"] == "p1"
+                and r["example"] == "smooth_initial"}
+    for level in (1, 2, 3, 4, 5):
+        blocks = assemble_main_system_blocks(uniform_problem(level, 1), ctx=gpu_ctx)
+        blocks.assemble_parabolic_graph_norm_approximation()
+        solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=1e-10), copy_out=False)
+        _, totals = x_marking_indicator_components(blocks)
+        lam, eta = float(rows[level]["lambda_y_squared"]), float(rows[level]["eta_squared"])
+        assert abs(totals["lambda_y_squared"] - lam) <= 1e-5 * lam, (level, totals, lam)
+        assert abs(totals["eta_squared"] - eta) <= 1e-5 * eta, (level, totals, eta)
+        blocks.close()

@@ -117,3 +117,42 @@ def test_generated_mesh_assembles_to_reference_blocks(name):
     assert_same_sparse(ref["B"], Px @ out["B"] @ Py.T, 1e-12, "B")
     assert_same_sparse(ref["C_signed"], Px @ out["C_signed"] @ Px.T, 1e-12, "C")
     assert np.abs(Px @ out["g"] - ref["g"]).max() <= 1e-12 * np.abs(ref["g"]).max()
+
+
+def _paper_row(level, p="p1", example="smooth_initial"):
+    rows = [r for r in _paper_rows() if r["dimension"] == "2d" and r["p"] == p and r["example"] == example
+            and int(r["outer_iteration"]) == level]
+    return rows[0]
+
+
+@pytest.mark.parametrize("name", ["p1_l1_smooth", "p1_l2_smooth", "p1_l3_smooth"])
+def test_reference_x_indicators_match_paper(name):
+    """The reference's own X-marking indicators (written by the oracle driver) reproduce
+    the published lambda_y_squared and eta_squared of the uniform runs (6 digits)."""
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    row = _paper_row(int(z["meta_level"][0]))
+    lam = float(row["lambda_y_squared"])
+    eta = float(row["eta_squared"])
+    assert abs(z["xind_lambda_by_x"].sum() - lam) <= 1e-5 * lam
+    assert abs(np.nansum(z["xind_eta_by_x"]) - eta) <= 1e-5 * eta
+    assert abs(z["xind_lambda_by_y"].sum() - z["xind_lambda_by_x"].sum()) <= 1e-12 * lam
+
+
+def test_y_estimator_threshold_matches_paper():
+    """apf_y_estimator_threshold_squared (a host function of the library, no GPU needed)
+    against the published thresholds, from the published lambda^2 and eta^2."""
+    from doubleadapparabolicfem_b200 import build
+    build.build()
+    from doubleadapparabolicfem_b200.estimator import y_estimator_threshold_squared
+    checked = 0
+    for r in _paper_rows():
+        if r["dimension"] != "2d" or not r.get("y_estimator_threshold_squared") or not r.get("configured_rho"):
+            continue
+        lam, eta = float(r["lambda_y_squared"]), float(r["eta_squared"])
+        got = y_estimator_threshold_squared(float(r["configured_rho"]), lam, eta - lam)
+        want = float(r["y_estimator_threshold_squared"])
+        assert abs(got - want) <= 2e-5 * want + 1e-12, r
+        checked += 1
+    assert checked >= 10
+    with pytest.raises(Exception):
+        y_estimator_threshold_squared(0.0, 1.0, 1.0)
