@@ -205,7 +205,7 @@ def run_ours(args, world, rank, local):
     host = uniform_problem(args.level, args.p)
     n_dofs = host.n_lambda + host.n_u
     ny = host.n_y_cells
-    run_estimator = not args.no_estimator and args.p == 1
+    run_estimator = not args.no_estimator
 
     def to_dev(a, dtype):
         return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(dev)

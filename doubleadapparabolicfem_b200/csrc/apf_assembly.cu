@@ -1306,6 +1306,26 @@ namespace apf
         }
     }
 
+    void y_cell_energy(cudaStream_t s, const SystemInputs& in, const double* v, double* out)
+    {
+        XIndArgs a{};
+        a.p = in.p;
+        a.n_y = in.n_y_cells;
+        a.y_geo = in.y_geo.get();
+        a.m_y = in.m_y.size() ? in.m_y.get() : nullptr;
+        a.y_off = in.y_off.get();
+        a.y_dofs = in.y_dofs.get();
+        a.y_w = in.y_w.get();
+        a.lambda = v;
+        a.lam_y = out;
+        if (in.n_y_cells > 0)
+        {
+            APF_KERNEL("y_cell_energy", s);
+            lambda_energy_kernel<<<grid_for(in.n_y_cells, 128), 128, 0, s>>>(a);
+        }
+        APF_CUDA(cudaGetLastError());
+    }
+
     void x_indicators(cudaStream_t s, const SystemInputs& in, const double* lambda, const double* u, double* lam_y,
                       double* lam_x, double* trace_x, double* eta_x)
     {

@@ -587,7 +587,7 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
             APF_CUDA(cudaMemcpyAsync(vids.data(), y_vertex_ids, n * sizeof(int),
                                      pointers_on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, ctx->stream));
         apf::sync(ctx->stream);
-        const apf::EstimatorTotals t = apf::estimate_p1(ctx->stream, S, vids, flux_squared, divergence_squared,
+        const apf::EstimatorTotals t = apf::estimate(ctx->stream, S, vids, flux_squared, divergence_squared,
                                                         reconstruction_squared, eta_squared, pointers_on_device != 0);
         if (result)
         {

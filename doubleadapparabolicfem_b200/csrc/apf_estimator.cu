@@ -686,6 +686,565 @@ namespace apf
         }
     }
 
+    // ---------------------------------------------------------------------------------------
+    // p = 2: RT_2 x P_2 patches, broken P_2 x P_2 scalars, P_2 time basis (nodes 0, 1/2, 1)
+    // ---------------------------------------------------------------------------------------
+    namespace
+    {
+        // the 15 vector monomials spanning RT_2 on the reference triangle:
+        // (P_2)^2 = {1, x, y, x^2, xy, y^2} e_1, same e_2, and x (x^2, xy, y^2)
+        __host__ __device__ inline void mono15(double x, double y, double vx[15], double vy[15], double dv[15])
+        {
+            const double xx = x * x, xy = x * y, yy = y * y;
+            const double ax[15] = {1, x, y, xx, xy, yy, 0, 0, 0, 0, 0, 0, xx * x, xx * y, xy * y};
+            const double ay[15] = {0, 0, 0, 0, 0, 0, 1, x, y, xx, xy, yy, xx * y, xy * y, yy * y};
+            const double ad[15] = {0, 1, 0, 2 * x, y, 0, 0, 0, 1, 0, x, 2 * y, 4 * xx, 4 * xy, 4 * yy};
+            for (int m = 0; m < 15; ++m)
+            {
+                vx[m] = ax[m];
+                vy[m] = ay[m];
+                dv[m] = ad[m];
+            }
+        }
+
+        // P_2 Lagrange basis on the reference triangle, node order v0, m01, v1, m02, m12, v2
+        __host__ __device__ inline void p2_basis(double x, double y, double T[6], double Tx[6], double Ty[6])
+        {
+            const double l0 = 1.0 - x - y, l1 = x, l2 = y;
+            T[0] = l0 * (2 * l0 - 1);  Tx[0] = -(4 * l0 - 1); Ty[0] = -(4 * l0 - 1);
+            T[1] = 4 * l0 * l1;        Tx[1] = 4 * (l0 - l1); Ty[1] = -4 * l1;
+            T[2] = l1 * (2 * l1 - 1);  Tx[2] = 4 * l1 - 1;    Ty[2] = 0;
+            T[3] = 4 * l0 * l2;        Tx[3] = -4 * l2;       Ty[3] = 4 * (l0 - l2);
+            T[4] = 4 * l1 * l2;        Tx[4] = 4 * l2;        Ty[4] = 4 * l1;
+            T[5] = l2 * (2 * l2 - 1);  Tx[5] = 0;             Ty[5] = 4 * l2 - 1;
+        }
+
+        // P_2 time basis on [0, 1] with nodes 0, 1/2, 1 and its derivative
+        __host__ __device__ inline void p2_time(double t, double S[3], double dS[3])
+        {
+            S[0] = (2 * t - 1) * (t - 1); dS[0] = 4 * t - 3;
+            S[1] = 4 * t * (1 - t);       dS[1] = 4 - 8 * t;
+            S[2] = t * (2 * t - 1);       dS[2] = 4 * t - 1;
+        }
+
+        // Reference-cell integrals for the p = 2 patch problems (16-point Duffy rule: exact up
+        // to total degree 6, the highest here) and the time tables.
+        struct Rt2Tables
+        {
+            double c[15][15];                     // phi_j = sum_m c[j][m] mono_m
+            double r00[15][15], r01[15][15], r11[15][15]; // int phi_j^a phi_l^b
+            double rd[15][6];                     // int div phi_l q_r
+            double w[3][6][15];                   // int lambda_a grad T_s . phi_j
+            double mq[3][6];                      // int lambda_a q_r
+            double mqq[3][6][6];                  // int lambda_a T_s q_r
+            double v[6][6][2];                    // int q_r d_c T_s
+            double eq[6];                         // int q_r
+            double mt[3][3], mtinv[3][3];         // int S_a S_b on [0, 1] and its inverse
+            double dt[3][3];                      // int S_b' S_k  (index [b][k])
+            double it[3];                         // int S_k
+            double tg[3], tw[3];                  // 3-point Gauss on [0, 1]
+        };
+        constexpr int kRt2Doubles = sizeof(Rt2Tables) / sizeof(double);
+
+        Rt2Tables make_rt2_tables(const EstTables& t)
+        {
+            Rt2Tables o{};
+            const double g4x[4] = {0.06943184420297371, 0.33000947820757187, 0.6699905217924281, 0.9305681557970263};
+            const double g4w[4] = {0.17392742256872692, 0.3260725774312731, 0.3260725774312731, 0.17392742256872692};
+            // DOF functionals: 3 moments per edge (q = 1, 2s - 1, 6s^2 - 6s + 1 against the
+            // outward normal times the edge length, edge k from v_{k+1} to v_{k+2}), then
+            // int sigma . q for q = e_1, e_2, x e_1, x e_2, y e_1, y e_2
+            std::vector<double> D(225, 0.0);
+            const double vt[3][2] = {{0, 0}, {1, 0}, {0, 1}};
+            for (int e = 0; e < 3; ++e)
+            {
+                const double* P = vt[(e + 1) % 3];
+                const double* Q = vt[(e + 2) % 3];
+                const double dx = Q[0] - P[0], dy = Q[1] - P[1];
+                for (int g = 0; g < 4; ++g)
+                {
+                    const double sg = g4x[g];
+                    double vx[15], vy[15], dv[15];
+                    mono15(P[0] + sg * dx, P[1] + sg * dy, vx, vy, dv);
+                    const double q[3] = {1.0, 2 * sg - 1, 6 * sg * sg - 6 * sg + 1};
+                    for (int m = 0; m < 15; ++m)
+                    {
+                        const double fn = vx[m] * dy - vy[m] * dx;
+                        for (int k = 0; k < 3; ++k)
+                            D[(3 * e + k) * 15 + m] += g4w[g] * fn * q[k];
+                    }
+                }
+            }
+            for (int q = 0; q < t.nq; ++q)
+            {
+                const double x = t.qp[q][0], y = t.qp[q][1], w = t.qw[q];
+                double vx[15], vy[15], dv[15];
+                mono15(x, y, vx, vy, dv);
+                for (int m = 0; m < 15; ++m)
+                {
+                    D[9 * 15 + m] += w * vx[m];
+                    D[10 * 15 + m] += w * vy[m];
+                    D[11 * 15 + m] += w * x * vx[m];
+                    D[12 * 15 + m] += w * x * vy[m];
+                    D[13 * 15 + m] += w * y * vx[m];
+                    D[14 * 15 + m] += w * y * vy[m];
+                }
+            }
+            std::vector<double> Dinv;
+            solve_dense_host(D, 15, Dinv);
+            for (int j = 0; j < 15; ++j)
+                for (int m = 0; m < 15; ++m)
+                    o.c[j][m] = Dinv[(size_t)m * 15 + j];
+            for (int q = 0; q < t.nq; ++q)
+            {
+                const double x = t.qp[q][0], y = t.qp[q][1], w = t.qw[q];
+                double vx[15], vy[15], dv[15];
+                mono15(x, y, vx, vy, dv);
+                double px[15], py[15], pd[15];
+                for (int j = 0; j < 15; ++j)
+                {
+                    px[j] = py[j] = pd[j] = 0.0;
+                    for (int m = 0; m < 15; ++m)
+                    {
+                        px[j] += o.c[j][m] * vx[m];
+                        py[j] += o.c[j][m] * vy[m];
+                        pd[j] += o.c[j][m] * dv[m];
+                    }
+                }
+                double T[6], Tx[6], Ty[6];
+                p2_basis(x, y, T, Tx, Ty);
+                const double l3[3] = {1 - x - y, x, y};
+                for (int j = 0; j < 15; ++j)
+                    for (int l = 0; l < 15; ++l)
+                    {
+                        o.r00[j][l] += w * px[j] * px[l];
+                        o.r01[j][l] += w * px[j] * py[l];
+                        o.r11[j][l] += w * py[j] * py[l];
+                    }
+                for (int l = 0; l < 15; ++l)
+                    for (int r = 0; r < 6; ++r)
+                        o.rd[l][r] += w * pd[l] * T[r];
+                for (int a = 0; a < 3; ++a)
+                    for (int s2 = 0; s2 < 6; ++s2)
+                    {
+                        for (int j = 0; j < 15; ++j)
+                            o.w[a][s2][j] += w * l3[a] * (Tx[s2] * px[j] + Ty[s2] * py[j]);
+                        o.mq[a][s2] += w * l3[a] * T[s2];
+                        for (int r = 0; r < 6; ++r)
+                            o.mqq[a][s2][r] += w * l3[a] * T[s2] * T[r];
+                    }
+                for (int r = 0; r < 6; ++r)
+                {
+                    for (int s2 = 0; s2 < 6; ++s2)
+                    {
+                        o.v[r][s2][0] += w * T[r] * Tx[s2];
+                        o.v[r][s2][1] += w * T[r] * Ty[s2];
+                    }
+                    o.eq[r] += w * T[r];
+                }
+            }
+            // time: 3-point Gauss on [0, 1]
+            const double h = 0.5 * std::sqrt(0.6);
+            o.tg[0] = 0.5 - h; o.tg[1] = 0.5; o.tg[2] = 0.5 + h;
+            o.tw[0] = 5.0 / 18.0; o.tw[1] = 8.0 / 18.0; o.tw[2] = 5.0 / 18.0;
+            for (int g = 0; g < 3; ++g)
+            {
+                double S[3], dS[3];
+                p2_time(o.tg[g], S, dS);
+                for (int a = 0; a < 3; ++a)
+                {
+                    o.it[a] += o.tw[g] * S[a];
+                    for (int b = 0; b < 3; ++b)
+                    {
+                        o.mt[a][b] += o.tw[g] * S[a] * S[b];
+                        o.dt[a][b] += o.tw[g] * dS[a] * S[b];
+                    }
+                }
+            }
+            std::vector<double> M(9), Minv;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    M[a * 3 + b] = o.mt[a][b];
+            solve_dense_host(M, 3, Minv);
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    o.mtinv[a][b] = Minv[a * 3 + b];
+            return o;
+        }
+
+        // one warp per p = 2 patch (same structure as patch_solve): 3 edge moments per free
+        // edge, 6 interior RT_2 moments and 6 scalars per patch cell, the mean-zero row, and
+        // three right-hand-side columns (one per time DOF)
+        template<int NMAX>
+        __global__ void __launch_bounds__(32) patch_solve2(PatchArgs A, const Rt2Tables* __restrict__ tables,
+                                                           const int* __restrict__ order, int count)
+        {
+            constexpr int LD = NMAX + 3; // odd: NMAX is even; columns n, n+1, n+2 hold the rhs
+            extern __shared__ double sm[];
+            Rt2Tables& T = *reinterpret_cast<Rt2Tables*>(sm);
+            double* K = sm + kRt2Doubles + (kRt2Doubles & 1);
+            const int lane = threadIdx.x;
+            for (int i = lane; i < kRt2Doubles; i += 32)
+                sm[i] = reinterpret_cast<const double*>(tables)[i];
+            __syncwarp();
+            for (int idx = blockIdx.x; idx < count; idx += gridDim.x)
+            {
+                const int p = order[idx];
+                const int slab = A.patch_slab[p], tp = A.patch_topo[p];
+                const int cb = A.topo_ptr[tp], ce = A.topo_ptr[tp + 1], nc = ce - cb;
+                const int nfree = A.topo_nfree[tp];
+                const bool interior = A.topo_boundary[tp] == 0;
+                const int nf = 3 * nfree + 6 * nc;
+                const int n = nf + 6 * nc + (interior ? 1 : 0);
+                if (n > NMAX)
+                {
+                    if (lane == 0)
+                        atomicExch(A.status, APF_ERR_CAPACITY);
+                    continue;
+                }
+                const int sb = A.slab_ptr[slab];
+                for (int i = lane; i < n * LD; i += 32)
+                    K[i] = 0.0;
+                __syncwarp();
+                double ht = 0.0;
+                for (int ic = 0; ic < nc; ++ic)
+                {
+                    const int c = A.slab_cells[sb + A.topo_cell[cb + ic]];
+                    const int a = A.topo_center[cb + ic];
+                    const Cell k = load_cell(A.geo, A.m, A.ell, c);
+                    ht = k.ht;
+                    const double adet = fabs(k.det);
+                    int pd[15];
+                    double e[15];
+                    for (int ed = 0; ed < 3; ++ed)
+                    {
+                        const int code = A.topo_edge[3 * (cb + ic) + ed];
+                        const int pe = code & 0xffff;
+                        const double sp = (code >> 30) & 1 ? -1.0 : 1.0;
+                        const bool free_edge = pe != 0xffff;
+                        for (int m = 0; m < 3; ++m)
+                        {
+                            pd[3 * ed + m] = free_edge ? 3 * pe + m : -1;
+                            // orientation sp^(m+1) times the Piola factor sign(det) / det
+                            e[3 * ed + m] = (m == 1 ? 1.0 : sp) / k.det;
+                        }
+                    }
+                    for (int m = 0; m < 6; ++m)
+                    {
+                        pd[9 + m] = 3 * nfree + 6 * ic + m;
+                        e[9 + m] = 1.0 / k.det;
+                    }
+                    const int sbase = nf + 6 * ic;
+                    const double q00 = k.mi00 * k.J00 + k.mi01 * k.J10, q10 = k.mi01 * k.J00 + k.mi11 * k.J10;
+                    const double q01 = k.mi00 * k.J01 + k.mi01 * k.J11, q11 = k.mi01 * k.J01 + k.mi11 * k.J11;
+                    const double S00 = k.J00 * q00 + k.J10 * q10;
+                    const double S01 = k.J00 * q01 + k.J10 * q11;
+                    const double S11 = k.J01 * q01 + k.J11 * q11;
+                    // time-tested nodal data: th[s][kk] = ht sum_b Mt[kk][b] theta_{s,b},
+                    // du[s][kk] = sum_b u_{s,b} int S_b' S_kk
+                    const double* thc = A.theta + 18ll * c;
+                    const double* uuc = A.u + 18ll * c;
+                    double th[6][3], du[6][3];
+                    for (int s2 = 0; s2 < 6; ++s2)
+                        for (int kk = 0; kk < 3; ++kk)
+                        {
+                            double a1 = 0.0, a2 = 0.0;
+                            for (int b = 0; b < 3; ++b)
+                            {
+                                a1 += T.mt[kk][b] * thc[3 * s2 + b];
+                                a2 += uuc[3 * s2 + b] * T.dt[b][kk];
+                            }
+                            th[s2][kk] = k.ht * a1;
+                            du[s2][kk] = a2;
+                        }
+                    // grad psi_a^T M G  (G = J^-T): row vector acting on reference gradients
+                    const double mg0 = k.m00 * k.g[a][0] + k.m01 * k.g[a][1];
+                    const double mg1 = k.m01 * k.g[a][0] + k.m11 * k.g[a][1];
+                    // G = J^-T: (G v)_0 = (J11 v0 - J10 v1) / det, (G v)_1 = (-J01 v0 + J00 v1) / det
+                    const double id = 1.0 / k.det;
+                    const double h0 = (mg0 * k.J11 - mg1 * k.J01) * id; // (M grad psi)^T G e_0
+                    const double h1 = (-mg0 * k.J10 + mg1 * k.J00) * id; // (M grad psi)^T G e_1
+                    for (int t = lane; t < 384; t += 32)
+                    {
+                        if (t < 225)
+                        {
+                            const int j = t / 15, l = t % 15;
+                            if (pd[j] < 0 || pd[l] < 0)
+                                continue;
+                            const double r = S00 * T.r00[j][l] + S01 * (T.r01[j][l] + T.r01[l][j]) + S11 * T.r11[j][l];
+                            K[pd[j] * LD + pd[l]] += e[j] * e[l] * adet * r;
+                        }
+                        else if (t < 315)
+                        {
+                            const int r = (t - 225) / 15, l = (t - 225) % 15;
+                            if (pd[l] < 0)
+                                continue;
+                            const double v = e[l] * adet * T.rd[l][r];
+                            K[(sbase + r) * LD + pd[l]] += v;
+                            K[pd[l] * LD + sbase + r] += v;
+                        }
+                        else if (t < 360)
+                        {
+                            const int j = (t - 315) / 3, kk = (t - 315) % 3;
+                            if (pd[j] < 0)
+                                continue;
+                            double acc = 0.0;
+                            for (int s2 = 0; s2 < 6; ++s2)
+                                acc += th[s2][kk] * T.w[a][s2][j];
+                            K[pd[j] * LD + n + kk] += -e[j] * adet * acc;
+                        }
+                        else if (t < 378)
+                        {
+                            const int r = (t - 360) / 3, kk = (t - 360) % 3;
+                            double acc = k.ell * k.ht * T.it[kk] * T.mq[a][r];
+                            double gx = 0.0, gy = 0.0;
+                            for (int s2 = 0; s2 < 6; ++s2)
+                            {
+                                acc -= du[s2][kk] * T.mqq[a][s2][r];
+                                gx += th[s2][kk] * T.v[r][s2][0];
+                                gy += th[s2][kk] * T.v[r][s2][1];
+                            }
+                            K[(sbase + r) * LD + n + kk] += (acc - (h0 * gx + h1 * gy)) * adet;
+                        }
+                        else if (interior)
+                        {
+                            const int r = t - 378;
+                            const double v = adet * T.eq[r];
+                            K[(n - 1) * LD + sbase + r] += v;
+                            K[(sbase + r) * LD + n - 1] += v;
+                        }
+                    }
+                    __syncwarp();
+                }
+                // right-hand sides times Mt^-1 = (1 / ht) mtinv
+                for (int i = lane; i < n; i += 32)
+                {
+                    const double b0 = K[i * LD + n], b1 = K[i * LD + n + 1], b2 = K[i * LD + n + 2];
+                    for (int kk = 0; kk < 3; ++kk)
+                        K[i * LD + n + kk] = (T.mtinv[kk][0] * b0 + T.mtinv[kk][1] * b1 + T.mtinv[kk][2] * b2) / ht;
+                }
+                __syncwarp();
+                bool singular = false;
+                for (int col = 0; col < n; ++col)
+                {
+                    double best = -1.0;
+                    int bi = n;
+                    for (int i = col + lane; i < n; i += 32)
+                    {
+                        const double v = fabs(K[i * LD + col]);
+                        if (v > best)
+                        {
+                            best = v;
+                            bi = i;
+                        }
+                    }
+                    for (int o = 16; o > 0; o >>= 1)
+                    {
+                        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+                        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                        if (ov > best || (ov == best && oi < bi))
+                        {
+                            best = ov;
+                            bi = oi;
+                        }
+                    }
+                    if (bi >= n || !(best > 0.0) || !isfinite(best))
+                    {
+                        singular = true;
+                        break;
+                    }
+                    if (bi != col)
+                        for (int j = col + lane; j < n + 3; j += 32)
+                        {
+                            const double t0 = K[col * LD + j];
+                            K[col * LD + j] = K[bi * LD + j];
+                            K[bi * LD + j] = t0;
+                        }
+                    __syncwarp();
+                    const double inv = 1.0 / K[col * LD + col];
+                    for (int j = col + 1 + lane; j < n + 3; j += 32)
+                    {
+                        const double u = K[col * LD + j] * inv;
+                        for (int i = col + 1; i < n; ++i)
+                            K[i * LD + j] -= K[i * LD + col] * u;
+                    }
+                    __syncwarp();
+                }
+                if (singular)
+                {
+                    if (lane == 0)
+                        atomicExch(A.status, APF_ERR_NUMERIC);
+                    __syncwarp();
+                    continue;
+                }
+                for (int i = n - 1; i >= 0; --i)
+                {
+                    const double d = K[i * LD + i];
+                    const double x0 = K[i * LD + n] / d, x1 = K[i * LD + n + 1] / d, x2 = K[i * LD + n + 2] / d;
+                    for (int r = lane; r < i; r += 32)
+                    {
+                        const double kri = K[r * LD + i];
+                        K[r * LD + n] -= kri * x0;
+                        K[r * LD + n + 1] -= kri * x1;
+                        K[r * LD + n + 2] -= kri * x2;
+                    }
+                    __syncwarp();
+                    if (lane == 0)
+                    {
+                        K[i * LD + n] = x0;
+                        K[i * LD + n + 1] = x1;
+                        K[i * LD + n + 2] = x2;
+                    }
+                }
+                __syncwarp();
+                // flux of this patch on each of its cells -> slot of the patch vertex:
+                // sigma slots [cell][3 vertices][3 time][15], coefficients of the cell's own
+                // RT_2 basis with the orientation of its edges
+                for (int t = lane; t < nc * 45; t += 32)
+                {
+                    const int ic = t / 45, kk = (t / 15) % 3, j = t % 15;
+                    const int c = A.slab_cells[sb + A.topo_cell[cb + ic]];
+                    const int a = A.topo_center[cb + ic];
+                    double val = 0.0;
+                    if (j < 9)
+                    {
+                        const int ed = j / 3, m = j % 3;
+                        const int code = A.topo_edge[3 * (cb + ic) + ed];
+                        const int pe = code & 0xffff;
+                        if (pe != 0xffff)
+                        {
+                            const double sp = (code >> 30) & 1 ? -1.0 : 1.0;
+                            const double* g = A.geo + 8ll * c;
+                            const double det = (g[2] - g[0]) * (g[5] - g[1]) - (g[4] - g[0]) * (g[3] - g[1]);
+                            const double cf = (det < 0.0 ? -1.0 : 1.0) * (m == 1 ? 1.0 : sp);
+                            val = cf * K[(3 * pe + m) * LD + n + kk];
+                        }
+                    }
+                    else
+                        val = K[(3 * nfree + 6 * ic + (j - 9)) * LD + n + kk];
+                    A.sigma[((3ll * c + a) * 3 + kk) * 15 + j] = val;
+                }
+                __syncwarp();
+            }
+        }
+
+        template<int NMAX>
+        constexpr std::size_t patch2_smem_bytes()
+        {
+            return sizeof(double) * (kRt2Doubles + (kRt2Doubles & 1) + NMAX * (NMAX + 3));
+        }
+
+        // per slab cell (p = 2): flux^2 and div^2 with the 16-point Duffy rule x 3-point Gauss
+        __global__ void cell_indicators2(IndicatorArgs A, const Rt2Tables* __restrict__ tables)
+        {
+            __shared__ double C[15][15];
+            __shared__ double tg[3], tw[3];
+            for (int i = threadIdx.x; i < 225; i += blockDim.x)
+                C[i / 15][i % 15] = tables->c[i / 15][i % 15];
+            if (threadIdx.x < 3)
+            {
+                tg[threadIdx.x] = tables->tg[threadIdx.x];
+                tw[threadIdx.x] = tables->tw[threadIdx.x];
+            }
+            __syncthreads();
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n_cells; c += gridDim.x * blockDim.x)
+            {
+                const Cell k = load_cell(A.geo, A.m, A.ell, c);
+                const double sdet = k.det < 0.0 ? -1.0 : 1.0;
+                const double adet = fabs(k.det);
+                const double* th = A.theta + 18ll * c;
+                const double* uu = A.u + 18ll * c;
+                double Ssum[3][15];
+                for (int kk = 0; kk < 3; ++kk)
+                    for (int j = 0; j < 15; ++j)
+                    {
+                        double sj = 0.0;
+                        for (int slot = 0; slot < 3; ++slot)
+                            sj += A.sigma[((3ll * c + slot) * 3 + kk) * 15 + j];
+                        Ssum[kk][j] = sj;
+                    }
+                double flux = 0.0, div = 0.0;
+                for (int q = 0; q < c_est.nq; ++q)
+                {
+                    const double x = c_est.qp[q][0], y = c_est.qp[q][1];
+                    double mvx[15], mvy[15], mdv[15];
+                    mono15(x, y, mvx, mvy, mdv);
+                    double T[6], Tx[6], Ty[6];
+                    p2_basis(x, y, T, Tx, Ty);
+                    // reference-basis values at this point (before the Piola map)
+                    double bx[15], by[15], bd[15];
+                    for (int j = 0; j < 15; ++j)
+                    {
+                        double vx = 0.0, vy = 0.0, dv = 0.0;
+                        for (int m = 0; m < 15; ++m)
+                        {
+                            vx += C[j][m] * mvx[m];
+                            vy += C[j][m] * mvy[m];
+                            dv += C[j][m] * mdv[m];
+                        }
+                        const double f = (j < 9 ? sdet : 1.0) / k.det;
+                        bx[j] = f * (k.J00 * vx + k.J01 * vy);
+                        by[j] = f * (k.J10 * vx + k.J11 * vy);
+                        bd[j] = f * dv;
+                    }
+                    for (int g = 0; g < 3; ++g)
+                    {
+                        double S[3], dS[3];
+                        p2_time(tg[g], S, dS);
+                        double sx = 0.0, sy = 0.0, sd = 0.0;
+                        for (int kk = 0; kk < 3; ++kk)
+                        {
+                            double cx = 0.0, cy = 0.0, cd = 0.0;
+                            for (int j = 0; j < 15; ++j)
+                            {
+                                cx += Ssum[kk][j] * bx[j];
+                                cy += Ssum[kk][j] * by[j];
+                                cd += Ssum[kk][j] * bd[j];
+                            }
+                            sx += S[kk] * cx;
+                            sy += S[kk] * cy;
+                            sd += S[kk] * cd;
+                        }
+                        // grad theta~ and d_t u at (x, t)
+                        double gr0 = 0.0, gr1 = 0.0, dtu = 0.0;
+                        for (int s2 = 0; s2 < 6; ++s2)
+                        {
+                            double v = 0.0, w = 0.0;
+                            for (int b = 0; b < 3; ++b)
+                            {
+                                v += th[3 * s2 + b] * S[b];
+                                w += uu[3 * s2 + b] * dS[b];
+                            }
+                            gr0 += v * Tx[s2];
+                            gr1 += v * Ty[s2];
+                            dtu += w * T[s2];
+                        }
+                        dtu /= k.ht;
+                        // physical gradient G g_ref, G = J^-T
+                        const double id = 1.0 / k.det;
+                        const double p0 = (k.J11 * gr0 - k.J10 * gr1) * id;
+                        const double p1 = (-k.J01 * gr0 + k.J00 * gr1) * id;
+                        const double mg0 = k.m00 * p0 + k.m01 * p1, mg1 = k.m01 * p0 + k.m11 * p1;
+                        const double ex = sx + mg0, ey = sy + mg1;
+                        const double w = c_est.qw[q] * adet * tw[g] * k.ht;
+                        flux += w * (ex * (k.mi00 * ex + k.mi01 * ey) + ey * (k.mi01 * ex + k.mi11 * ey));
+                        const double r = k.ell - dtu - sd;
+                        div += w * r * r;
+                    }
+                }
+                if (A.flux) A.flux[c] = flux;
+                if (A.div) A.div[c] = div;
+            }
+        }
+
+        __global__ void add_kernel(int n, const double* __restrict__ a, const double* __restrict__ b,
+                                   double* __restrict__ y)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                y[i] = a[i] + b[i];
+        }
+    }
+
     // ---------------------------------------------------------------------------
     // host-side patch topology (integer work; built once per distinct slab mesh)
     // ---------------------------------------------------------------------------
@@ -866,11 +1425,11 @@ namespace apf
         done = true;
     }
 
-    EstimatorTotals estimate_p1(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
+    EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
                                 double* recon, double* eta, bool out_on_device)
     {
         SystemInputs& in = S.in;
-        require(in.p == 1, APF_ERR_INVALID, "estimator: only p = 1 is implemented");
+        require(in.p == 1 || in.p == 2, APF_ERR_INVALID, "estimator: p must be 1 or 2");
         require(S.solution.size() == static_cast<std::size_t>(in.n_lambda + in.n_u), APF_ERR_INVALID,
                 "estimator: solve the main system first");
         require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
@@ -913,7 +1472,8 @@ namespace apf
         tot.recon_residual = bn > 0.0 ? rn / bn : 0.0;
         // ---- nodal data per cell
         const int nd = in.ndof;
-        DeviceBuffer<double> theta(6ll * ny, s), ucell(6ll * ny, s), ldel(6ll * ny, s), ltil(6ll * ny, s);
+        DeviceBuffer<double> theta((long long)nd * ny, s), ucell((long long)nd * ny, s), ldel((long long)nd * ny, s),
+            ltil((long long)nd * ny, s);
         const double* u = S.solution.get() + nl;
         {
             APF_KERNEL("est_gather_nodal", s);
@@ -930,8 +1490,8 @@ namespace apf
             gather_nodal<<<nb((long long)ny * nd), 256, 0, s>>>(ny, nd, in.x_off.get(), in.x_dofs.get(), in.x_w.get(), u,
                                                                 nullptr, ucell.get());
         }
-        axpby(s, 6 * ny, 1.0, ltil.get(), 0.0, theta.get());
-        axpby(s, 6 * ny, 1.0, ucell.get(), 1.0, theta.get());
+        axpby(s, nd * ny, 1.0, ltil.get(), 0.0, theta.get());
+        axpby(s, nd * ny, 1.0, ucell.get(), 1.0, theta.get());
         // ---- patches (host topology)
         std::vector<double> geo(8ll * ny);
         APF_CUDA(cudaMemcpyAsync(geo.data(), in.y_geo.get(), geo.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -958,7 +1518,8 @@ namespace apf
         up(d_sptr, ps.slab_ptr);
         up(d_scell, ps.slab_cells);
         status.zero();
-        DeviceBuffer<double> sigma(48ll * ny, s);
+        const bool p2 = in.p == 2;
+        DeviceBuffer<double> sigma((p2 ? 135ll : 48ll) * ny, s);
         sigma.zero();
         PatchArgs pa{};
         pa.n_patches = tot.n_patches;
@@ -989,7 +1550,8 @@ namespace apf
             {
                 const int tp = ps.patch_topo[p];
                 const int nc = ps.topo_ptr[tp + 1] - ps.topo_ptr[tp];
-                const int n = 2 * ps.topo_nfree[tp] + 5 * nc + (ps.topo_boundary[tp] ? 0 : 1);
+                const int n = (p2 ? 3 * ps.topo_nfree[tp] + 12 * nc : 2 * ps.topo_nfree[tp] + 5 * nc) +
+                              (ps.topo_boundary[tp] ? 0 : 1);
                 int b = 0;
                 while (b < kBuckets && n > kBucketMax[b])
                     ++b;
@@ -1005,18 +1567,38 @@ namespace apf
         }
         DeviceBuffer<int> d_order(0, s);
         up(d_order, order);
-        const PatchTables ptab = make_patch_tables(make_est_tables());
+        const EstTables est = make_est_tables();
+        const PatchTables ptab = make_patch_tables(est);
         DeviceBuffer<double> d_ptab(kPatchTableDoubles, s);
         d_ptab.upload(reinterpret_cast<const double*>(&ptab), kPatchTableDoubles);
         const PatchTables* tables = reinterpret_cast<const PatchTables*>(d_ptab.get());
+        DeviceBuffer<double> d_rt2;
+        const Rt2Tables* tables2 = nullptr;
+        if (p2)
+        {
+            const Rt2Tables t2 = make_rt2_tables(est);
+            d_rt2.allocate(kRt2Doubles, s);
+            d_rt2.upload(reinterpret_cast<const double*>(&t2), kRt2Doubles);
+            tables2 = reinterpret_cast<const Rt2Tables*>(d_rt2.get());
+        }
         auto launch = [&](auto tag, int b) {
             constexpr int NMAX = decltype(tag)::value;
             const int count = bucket_count[b + 1] - bucket_count[b];
             if (count == 0)
                 return;
+            pa.nmax = NMAX;
+            if (p2)
+            {
+                constexpr std::size_t smem = patch2_smem_bytes<NMAX>();
+                APF_CUDA(cudaFuncSetAttribute(patch_solve2<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
+                const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32)));
+                APF_KERNEL("est_patch_solve", s);
+                patch_solve2<NMAX><<<grid, 32, smem, s>>>(pa, tables2, d_order.get() + bucket_count[b], count);
+                return;
+            }
             constexpr std::size_t smem = patch_smem_bytes<NMAX>();
             APF_CUDA(cudaFuncSetAttribute(patch_solve<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            pa.nmax = NMAX;
             const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
             const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32)));
             APF_KERNEL("est_patch_solve", s);
@@ -1042,6 +1624,23 @@ namespace apf
         DeviceBuffer<double> f2(ny, s), d2(ny, s), r2(ny, s), e2(ny, s);
         IndicatorArgs ia{ny, in.y_geo.get(), pa.m, pa.ell, theta.get(), ucell.get(), ldel.get(), ltil.get(), sigma.get(),
                          f2.get(), d2.get(), r2.get(), e2.get()};
+        if (p2)
+        {
+            {
+                APF_KERNEL("est_cell_indicators", s);
+                cell_indicators2<<<nb(ny, 128), 128, 0, s>>>(ia, tables2);
+            }
+            // ||lambda_delta - lambda~||^2 in the local A_y energy, eta = flux + that
+            DeviceBuffer<double> dl(nl, s);
+            copy(s, nl, S.solution.get(), dl.get());
+            axpby(s, nl, -1.0, lt.get(), 1.0, dl.get());
+            y_cell_energy(s, in, dl.get(), r2.get());
+            {
+                APF_KERNEL("est_eta", s);
+                add_kernel<<<nb(ny), 256, 0, s>>>(ny, f2.get(), r2.get(), e2.get());
+            }
+        }
+        else
         {
             APF_KERNEL("est_cell_indicators", s);
             cell_indicators<<<nb(ny, 128), 128, 0, s>>>(ia);

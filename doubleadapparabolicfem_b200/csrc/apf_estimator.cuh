@@ -35,6 +35,6 @@ namespace apf
 
     void build_patches(const std::vector<double>& geo, const std::vector<int>& vids, int n_cells, PatchSet& ps);
 
-    EstimatorTotals estimate_p1(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
+    EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
                                 double* recon, double* eta, bool out_on_device);
 }

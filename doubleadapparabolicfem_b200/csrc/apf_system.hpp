@@ -69,6 +69,9 @@ namespace apf
     // level separately (its low-energy modes are arbitrary in time, smooth in space)
     void dof_time_components(cudaStream_t s, const SystemInputs& in, bool y_space, DeviceBuffer<int>& comp);
     void prepare_inputs(cudaStream_t s, SystemInputs& in);
+    // per Y cell: v_K^T A_y,K v_K, the local A_y energy (int_K grad_x v . M grad_x v) of a
+    // Y-space true-DOF vector v (device)
+    void y_cell_energy(cudaStream_t s, const SystemInputs& in, const double* v, double* out);
     // X-marking indicators from lambda_delta (Y true DOFs) and u_delta (X true DOFs), all
     // device arrays: per Y cell lambda energy, per X cell its aggregate, the initial-trace
     // mismatch (0 off the t = 0 layer) and their sum

@@ -209,13 +209,13 @@ typedef struct apf_estimator_result
     double reconstruction_residual; /* relative residual of the slab reconstruction solve */
 } apf_estimator_result;
 
-/* The estimator of one inner iteration for p = 1, on the solution of the last
+/* The estimator of one inner iteration for p = 1 or 2, on the solution of the last
  * apf_solve_minres call:
  *   lambda~ : slab Riesz reconstruction, A_y lambda~ = f - B^T u (Y is broken in time, so
  *             this is every slab's reconstruction system at once), replacing
  *             TimeSlabReconstruction::solve_all_slabs (src/finite_element/time_slabs/
  *             time_slab_reconstruction.hpp:584);
- *   sigma_a : one mixed RT_1 x P_1 local problem per (time slab, spatial vertex) patch,
+ *   sigma_a : one mixed RT_p x P_p local problem per (time slab, spatial vertex) patch,
  *             replacing TimeSlabEquilibratedFluxReconstruction2plus1d::solve_all_patches
  *             (time_slab_equilibrated_flux_reconstruction.hpp:2515) with the bordered
  *             dense system of dense_local_error_blocks_2d.hpp:812-905;

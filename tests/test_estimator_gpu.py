@@ -1,4 +1,4 @@
-"""GPU parity tests of the equilibrated-flux estimator (p = 1) against the reference's
+"""GPU parity tests of the equilibrated-flux estimator (p = 1 and 2) against the reference's
 own per-cell indicators (fixtures written by the reference templates through the
 oracle driver) and the reference's published paper values.
 
@@ -17,6 +17,7 @@ from conftest import GOLDEN, load_golden, to_product_problem
 pytestmark = pytest.mark.gpu
 
 P1_CASES = ["p1_l1_smooth", "p1_l2_smooth", "p1_l3_smooth", "p1_l1_nonmatching"]
+P2_CASES = ["p2_l1_smooth"]
 
 
 def _solve_and_estimate(ctx, prob, tol=1e-13):
@@ -29,7 +30,7 @@ def _solve_and_estimate(ctx, prob, tol=1e-13):
     return blocks, estimate(blocks)
 
 
-@pytest.mark.parametrize("name", P1_CASES)
+@pytest.mark.parametrize("name", P1_CASES + P2_CASES)
 def test_indicators_match_reference(gpu_ctx, name):
     prob, ref, example = load_golden(name)
     z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
@@ -43,6 +44,20 @@ def test_indicators_match_reference(gpu_ctx, name):
     assert np.abs(cells["eta"] - z["est_eta"]).max() <= 1e-9 * scale
     assert abs(totals["flux_squared"] - ref_flux.sum()) <= 1e-10 * ref_flux.sum()
     assert totals["reconstruction_squared"] <= 1e-12 * ref_flux.sum()
+
+
+def test_p2_estimator_matches_published_paper_values(gpu_ctx):
+    """Uniform outer levels 1-3 of the smooth_initial P2 runs: y_flux_squared to the CSV's 6
+    digits (RT_2 x P_2 patches, P_2 time basis)."""
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    with open(os.path.join(GOLDEN, "paper_uniform_rows.json")) as fh:
+        rows = [r for r in json.load(fh) if r["dimension"] == "2d" and r["p"] == "p2"
+                and r["example"] == "smooth_initial"]
+    by_level = {int(r["outer_iteration"]): float(r["y_flux_squared"]) for r in rows}
+    for level in (1, 2, 3):
+        _, (_, totals) = _solve_and_estimate(gpu_ctx, uniform_problem(level, 2), tol=1e-11)
+        got = totals["flux_squared"]
+        assert abs(got - by_level[level]) <= 1e-5 * by_level[level], (level, got, by_level[level])
 
 
 def test_estimator_matches_published_paper_values(gpu_ctx):
