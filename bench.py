@@ -31,7 +31,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
@@ -64,7 +63,8 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region
+    (one nvidia-smi process in loop mode, started before and stopped after)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -73,35 +73,35 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.samples = []
-        self._stop = threading.Event()
-        self._t = None
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self._proc = None
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._proc = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        if self._t:
-            self._t.join(timeout=10)
+        if self._proc is None:
+            return
+        self._proc.terminate()
+        try:
+            out, _ = self._proc.communicate(timeout=10)
+        except Exception:
+            self._proc.kill()
+            out, _ = self._proc.communicate()
+        for line in (out or "").splitlines():
+            if line.strip():
+                self.samples.append([x.strip() for x in line.split(",")])
 
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        sm = [float(s[1]) for s in self.samples if len(s) > 1 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 5 + k and s[5 + k] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
@@ -348,13 +348,17 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize(dev)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    e_events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     e0.record(stream)
-    for _ in range(args.steps):
+    for k in range(args.steps):
         lib.apf_system_destroy(step(hprob, False))
+        e_events[k].record(stream)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
     e2e_elapsed = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e_step_ms = [round(e0.elapsed_time(e_events[0]), 2)] + [
+        round(e_events[k - 1].elapsed_time(e_events[k]), 2) for k in range(1, args.steps)]
     e2e_diags = solve_diags[-args.steps:]
 
     # one more device-resident step with per-kernel CUDA-event timing on the library's stream
@@ -418,6 +422,7 @@ def run_ours(args, world, rank, local):
                    "plain_preconditioner": plain,
                    "minres_iterations": [d["iterations"] for d in timed_diags],
                    "step_ms": step_ms,
+                   "e2e_step_ms": e2e_step_ms,
                    "final_true_residual_max": max(d["final_true_residual"] for d in timed_diags),
                    "e2e_final_true_residual_max": max(d["final_true_residual"] for d in e2e_diags),
                    "flux_squared": timed_est[-1]["flux_squared"] if timed_est else None,

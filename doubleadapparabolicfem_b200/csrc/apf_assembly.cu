@@ -9,8 +9,10 @@
 //      cell geometry (affine prisms, cell-constant M) and filtered with
 //      |a_ij| > zero_tol exactly like scatter.hpp:66-115 -- sorts the candidates
 //      in shared memory (bitonic, key = column | deterministic sequence number)
-//      and sums duplicates in a fixed order.  A count pass sizes the rows, a
-//      scan gives row_ptr, a fill pass writes columns and values once.
+//      and sums duplicates in a fixed order.  One sorting pass writes each row's
+//      distinct columns and values into its segment
+//      of staging arrays sized by the row's candidate count; a scan of the distinct counts
+//      gives row_ptr and a compaction writes the block.
 // The result is the reference's compressed pattern bit for bit (setFromTriplets
 // keeps summed explicit zeros, so does this) and deterministic values with no
 // floating-point atomics.
@@ -345,7 +347,7 @@ namespace apf
                 {
                     if (lane == 0)
                         atomicExch(A.status, APF_ERR_CAPACITY);
-                    if (!FILL && lane == 0)
+                    if (lane == 0)
                         A.row_count[row] = 0;
                     __syncwarp();
                     continue;
@@ -381,7 +383,7 @@ namespace apf
                     }
                     uniq += __popc(hm);
                 }
-                if (!FILL && lane == 0)
+                if (lane == 0)
                     A.row_count[row] = uniq;
                 __syncwarp();
             }
@@ -575,7 +577,8 @@ namespace apf
         };
 
         // max over rows of |C row| + sum_{c in B_dt row} |B_dt^T row c| + |A_x row|
-        __global__ void hhat_row_bound(HhatArgs A, int* __restrict__ out)
+        // candidates per row (cand[row]) and their maximum (*out)
+        __global__ void hhat_row_bound(HhatArgs A, int* __restrict__ out, int* __restrict__ cand)
         {
             int m = 0;
             for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.n_u; row += gridDim.x * blockDim.x)
@@ -587,6 +590,7 @@ namespace apf
                     n += A.bt_ptr[c + 1] - A.bt_ptr[c];
                 }
                 m = max(m, n);
+                cand[row] = n;
             }
             for (int o = 16; o > 0; o >>= 1)
                 m = max(m, __shfl_down_sync(0xffffffffu, m, o));
@@ -687,7 +691,7 @@ namespace apf
                 {
                     if (lane == 0)
                         atomicExch(A.status, APF_ERR_CAPACITY);
-                    if (!FILL && lane == 0)
+                    if (lane == 0)
                         A.row_count[row] = 0;
                     __syncwarp();
                     continue;
@@ -731,9 +735,28 @@ namespace apf
                     }
                     uniq += __popc(km);
                 }
-                if (!FILL && lane == 0)
+                if (lane == 0)
                     A.row_count[row] = uniq;
                 __syncwarp();
+            }
+        }
+
+        // one warp per row: the row's kept entries from its staging segment to the result
+        __global__ void hhat_compact(int rows, const int* __restrict__ cand_ptr, const int* __restrict__ tc,
+                                     const double* __restrict__ tv, const int* __restrict__ cp, int* __restrict__ cc,
+                                     double* __restrict__ cv)
+        {
+            const int lane = threadIdx.x & 31;
+            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            const int nw = (gridDim.x * blockDim.x) >> 5;
+            for (int r = warp; r < rows; r += nw)
+            {
+                const int src = cand_ptr[r], dst = cp[r], len = cp[r + 1] - dst;
+                for (int k = lane; k < len; k += 32)
+                {
+                    cc[dst + k] = tc[src + k];
+                    cv[dst + k] = tv[src + k];
+                }
             }
         }
 
@@ -850,6 +873,37 @@ namespace apf
             APF_CUDA(cudaGetLastError());
         }
 
+        // candidates of each row: incidences x local DOFs x restriction entries per term
+        __global__ void gather_candidates(int n_rows, Term t0, Term t1, int n_terms, int per_incidence,
+                                          int* __restrict__ cand)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += gridDim.x * blockDim.x)
+            {
+                int n = (t0.inc_ptr[r + 1] - t0.inc_ptr[r]);
+                if (n_terms > 1)
+                    n += t1.inc_ptr[r + 1] - t1.inc_ptr[r];
+                cand[r] = n * per_incidence;
+            }
+        }
+
+        __global__ void gather_compact(int rows, const int* __restrict__ cand_ptr, const int* __restrict__ tc,
+                                       const double* __restrict__ tv, const int* __restrict__ cp, int* __restrict__ cc,
+                                       double* __restrict__ cv)
+        {
+            const int lane = threadIdx.x & 31;
+            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            const int nw = (gridDim.x * blockDim.x) >> 5;
+            for (int r = warp; r < rows; r += nw)
+            {
+                const int src = cand_ptr[r], dst = cp[r], len = cp[r + 1] - dst;
+                for (int k = lane; k < len; k += 32)
+                {
+                    cc[dst + k] = tc[src + k];
+                    cv[dst + k] = tv[src + k];
+                }
+            }
+        }
+
         void dispatch_gather(cudaStream_t s, GatherArgs& a, int cap)
         {
             if (cap <= 512) run_gather<512>(s, a, a.status);
@@ -887,9 +941,24 @@ namespace apf
         DeviceBuffer<int> status(1, s);
         status.zero();
         a.status = status.get();
-        DeviceBuffer<int> counts(static_cast<std::size_t>(n_rows) + 1, s);
+        // one sorting pass: each row's distinct entries go to its candidate segment of
+        // staging arrays (sized by incidences x local DOFs x restriction entries), then a
+        // compaction into the CSR block
+        DeviceBuffer<int> counts(static_cast<std::size_t>(n_rows) + 1, s), cand(static_cast<std::size_t>(n_rows) + 1, s),
+            cand_ptr(static_cast<std::size_t>(n_rows) + 1, s);
+        if (n_rows > 0)
+        {
+            APF_KERNEL("gather_candidates", s);
+            gather_candidates<<<grid_for(n_rows, 256), 256, 0, s>>>(n_rows, a.term[0], a.term[n_terms > 1 ? 1 : 0],
+                                                                    n_terms, in.ndof * kmax, cand.get());
+        }
+        const long long total = exclusive_scan(cand.get(), cand_ptr.get(), n_rows, s);
+        DeviceBuffer<int> tc(static_cast<std::size_t>(std::max(total, 1ll)), s);
+        DeviceBuffer<double> tv(static_cast<std::size_t>(std::max(total, 1ll)), s);
         a.row_count = counts.get();
-        a.row_ptr = nullptr;
+        a.row_ptr = cand_ptr.get();
+        a.col_out = tc.get();
+        a.val_out = tv.get();
         if (n_rows > 0)
             dispatch_gather(s, a, cap);
         out.rows = n_rows;
@@ -900,13 +969,13 @@ namespace apf
             throw Error(APF_ERR_CAPACITY, "assembly: per-row candidate buffer overflow");
         out.col_idx.allocate(static_cast<std::size_t>(nnz), s);
         out.values.allocate(static_cast<std::size_t>(nnz), s);
-        a.row_ptr = out.row_ptr.get();
-        a.col_out = out.col_idx.get();
-        a.val_out = out.values.get();
         if (n_rows > 0)
-            dispatch_gather(s, a, cap);
-        if (check_status(status, s) != 0)
-            throw Error(APF_ERR_CAPACITY, "assembly: per-row candidate buffer overflow");
+        {
+            APF_KERNEL("gather_compact", s);
+            gather_compact<<<grid_for((long long)n_rows * 32, 256, 148 * 16), 256, 0, s>>>(
+                n_rows, cand_ptr.get(), tc.get(), tv.get(), out.row_ptr.get(), out.col_idx.get(), out.values.get());
+        }
+        APF_CUDA(cudaGetLastError());
     }
 
     void gather_vector_host(cudaStream_t s, const SystemInputs& in, double zero_tol, int which, const Incidence& inc,
@@ -990,14 +1059,19 @@ namespace apf
         a.status = status.get();
         DeviceBuffer<int> counts(static_cast<std::size_t>(n_u) + 1, s);
         a.row_count = counts.get();
-        // upper bound of the candidates of any row -> candidate buffer size
-        DeviceBuffer<int> bound(1, s);
+        // candidates per row -> shared-memory capacity and the staging segments of the one
+        // sorting pass (each row's kept entries land in its segment, then a compaction)
+        DeviceBuffer<int> bound(1, s), cand(static_cast<std::size_t>(n_u) + 1, s),
+            cand_ptr(static_cast<std::size_t>(n_u) + 1, s);
         bound.zero();
         if (n_u > 0)
         {
             APF_KERNEL("hhat_row_bound", s);
-            hhat_row_bound<<<grid_for(n_u, 256, 148 * 8), 256, 0, s>>>(a, bound.get());
+            hhat_row_bound<<<grid_for(n_u, 256, 148 * 8), 256, 0, s>>>(a, bound.get(), cand.get());
         }
+        const long long total = exclusive_scan(cand.get(), cand_ptr.get(), n_u, s);
+        DeviceBuffer<int> tc(static_cast<std::size_t>(std::max(total, 1ll)), s);
+        DeviceBuffer<double> tv(static_cast<std::size_t>(std::max(total, 1ll)), s);
         int cap = 0;
         APF_CUDA(cudaMemcpyAsync(&cap, bound.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         sync(s);
@@ -1030,7 +1104,10 @@ namespace apf
             else if (cap <= 4096) run(std::integral_constant<int, 4096>{}, fill);
             else throw Error(APF_ERR_CAPACITY, "graph norm: a row has more than 4096 candidates");
         };
-        dispatch(false);
+        a.row_ptr = cand_ptr.get();
+        a.col_out = tc.get();
+        a.val_out = tv.get();
+        dispatch(true);
         H.rows = H.cols = n_u;
         H.row_ptr.allocate(static_cast<std::size_t>(n_u) + 1, s);
         const long long nnz = exclusive_scan(counts.get(), H.row_ptr.get(), n_u, s);
@@ -1038,12 +1115,13 @@ namespace apf
             throw Error(APF_ERR_CAPACITY, "graph norm: per-row candidate buffer overflow");
         H.col_idx.allocate(static_cast<std::size_t>(nnz), s);
         H.values.allocate(static_cast<std::size_t>(nnz), s);
-        a.row_ptr = H.row_ptr.get();
-        a.col_out = H.col_idx.get();
-        a.val_out = H.values.get();
-        dispatch(true);
-        if (check_status(status, s) != 0)
-            throw Error(APF_ERR_CAPACITY, "graph norm: per-row candidate buffer overflow");
+        if (n_u > 0)
+        {
+            APF_KERNEL("hhat_compact", s);
+            hhat_compact<<<grid_for((long long)n_u * 32, 256, 148 * 16), 256, 0, s>>>(
+                n_u, cand_ptr.get(), tc.get(), tv.get(), H.row_ptr.get(), H.col_idx.get(), H.values.get());
+        }
+        APF_CUDA(cudaGetLastError());
     }
 
     // M per X cell, taken from the Y cells it contains (M is cell-constant).

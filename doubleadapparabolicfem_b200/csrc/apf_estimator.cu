@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <future>
 #include <numeric>
 #include <unordered_map>
 #include <vector>
@@ -1237,6 +1238,15 @@ namespace apf
             }
         }
 
+        __global__ void cell_times_kernel(int n, const double* __restrict__ geo, double* __restrict__ times)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+            {
+                times[2ll * c] = geo[8ll * c + 6];
+                times[2ll * c + 1] = geo[8ll * c + 7];
+            }
+        }
+
         __global__ void add_kernel(int n, const double* __restrict__ a, const double* __restrict__ b,
                                    double* __restrict__ y)
         {
@@ -1248,15 +1258,16 @@ namespace apf
     // ---------------------------------------------------------------------------
     // host-side patch topology (integer work; built once per distinct slab mesh)
     // ---------------------------------------------------------------------------
-    void build_patches(const std::vector<double>& geo, const std::vector<int>& vids, int n_cells, PatchSet& ps)
+    void build_patches(const std::vector<double>& times, const std::vector<int>& vids, int n_cells, PatchSet& ps)
     {
-        // slabs by the (exact, dyadic) start time of their cells
-        std::vector<std::int64_t> key(n_cells);
+        // slabs by the exact start time of their cells (mesh times are dyadic)
+        std::vector<double> key(n_cells);
         for (int c = 0; c < n_cells; ++c)
-            key[c] = std::llround(geo[8ll * c + 6] * 1099511627776.0);
+            key[c] = times[2ll * c];
         std::vector<int> order(n_cells);
         std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+        if (!std::is_sorted(key.begin(), key.end())) // cells usually come slab by slab
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
         ps.slab_ptr.assign(1, 0);
         ps.slab_cells.clear();
         ps.slab_cells.reserve(n_cells);
@@ -1270,9 +1281,9 @@ namespace apf
         const int n_slabs = static_cast<int>(ps.slab_ptr.size()) - 1;
         for (int s = 0; s < n_slabs; ++s)
         {
-            const double t1 = geo[8ll * ps.slab_cells[ps.slab_ptr[s]] + 7];
+            const double t1 = times[2ll * ps.slab_cells[ps.slab_ptr[s]] + 1];
             for (int i = ps.slab_ptr[s]; i < ps.slab_ptr[s + 1]; ++i)
-                require(geo[8ll * ps.slab_cells[i] + 7] == t1, APF_ERR_INVALID,
+                require(times[2ll * ps.slab_cells[i] + 1] == t1, APF_ERR_INVALID,
                         "estimator: the cells of a time slab must share their time interval");
         }
         // group slabs with identical spatial meshes (same vertex-id sequence)
@@ -1403,6 +1414,13 @@ namespace apf
         }
         ps.patch_slab.clear();
         ps.patch_topo.clear();
+        {
+            std::size_t total = 0;
+            for (int s = 0; s < n_slabs; ++s)
+                total += static_cast<std::size_t>(group_count[group_of[s]]);
+            ps.patch_slab.reserve(total);
+            ps.patch_topo.reserve(total);
+        }
         for (int s = 0; s < n_slabs; ++s)
         {
             const int g = group_of[s];
@@ -1436,7 +1454,25 @@ namespace apf
         require(in.n_x_cells == in.n_y_cells, APF_ERR_INVALID, "estimator: Y cells must coincide with X cells");
         upload_est_tables_once();
         EstimatorTotals tot{};
-        const int ny = in.n_y_cells, nl = in.n_lambda, nu = in.n_u;
+        const int ny = in.n_y_cells, nl = in.n_lambda;
+        // ---- patch topology: host integer work on the cells' time intervals and vertex ids,
+        // run on a host thread while the device solves the slab reconstruction
+        std::vector<double> times(2ll * ny);
+        {
+            DeviceBuffer<double> dt(2ll * ny, s);
+            if (ny)
+            {
+                APF_KERNEL("est_cell_times", s);
+                cell_times_kernel<<<nb(ny), 256, 0, s>>>(ny, in.y_geo.get(), dt.get());
+                APF_CUDA(cudaMemcpyAsync(times.data(), dt.get(), times.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+            }
+            sync(s);
+        }
+        std::future<PatchSet> patches = std::async(std::launch::async, [&times, &vids_host, ny]() {
+            PatchSet ps;
+            build_patches(times, vids_host, ny, ps);
+            return ps;
+        });
         // ---- lambda~ : A_y lambda~ = f - B^T u (PCG with the A_y AMG, start lambda_delta)
         DeviceBuffer<double> rhs(nl, s), lt(nl, s), r(nl, s), z(nl, s), pv(nl, s), q(nl, s);
         copy(s, nl, S.f.get(), rhs.get());
@@ -1470,6 +1506,7 @@ namespace apf
         }
         tot.recon_iterations = its;
         tot.recon_residual = bn > 0.0 ? rn / bn : 0.0;
+        PatchSet ps = patches.get();
         // ---- nodal data per cell
         const int nd = in.ndof;
         DeviceBuffer<double> theta((long long)nd * ny, s), ucell((long long)nd * ny, s), ldel((long long)nd * ny, s),
@@ -1492,15 +1529,6 @@ namespace apf
         }
         axpby(s, nd * ny, 1.0, ltil.get(), 0.0, theta.get());
         axpby(s, nd * ny, 1.0, ucell.get(), 1.0, theta.get());
-        // ---- patches (host topology)
-        std::vector<double> geo(8ll * ny);
-        APF_CUDA(cudaMemcpyAsync(geo.data(), in.y_geo.get(), geo.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-        sync(s);
-        PatchSet ps;
-        {
-            APF_HOST_RANGE("est_build_patches");
-            build_patches(geo, vids_host, ny, ps);
-        }
         tot.n_slabs = ps.n_slabs;
         tot.n_patches = static_cast<int>(ps.patch_slab.size());
         tot.max_patch_cells = ps.max_cells;

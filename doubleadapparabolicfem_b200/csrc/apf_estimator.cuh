@@ -33,7 +33,8 @@ namespace apf
         double recon_residual = 0.0;
     };
 
-    void build_patches(const std::vector<double>& geo, const std::vector<int>& vids, int n_cells, PatchSet& ps);
+    // times: [n_cells][2] (t0, t1) of every cell; vids: [n_cells][3] spatial vertex ids
+    void build_patches(const std::vector<double>& times, const std::vector<int>& vids, int n_cells, PatchSet& ps);
 
     EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
                                 double* recon, double* eta, bool out_on_device);

@@ -39,6 +39,12 @@ namespace apf
         if (!ok)
             throw Error(code, msg);
     }
+    // literal messages: no string is built unless the check fails (hot host loops)
+    inline void require(bool ok, int code, const char* msg)
+    {
+        if (!ok)
+            throw Error(code, msg);
+    }
 
     // Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on the owning stream).
     template<class T>

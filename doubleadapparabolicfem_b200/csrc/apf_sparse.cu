@@ -207,8 +207,9 @@ namespace apf
         }
 
         // ---- sparse product C = A B ---------------------------------------------
+        // candidate products per row of A B (cand[r]) and their maximum (*out)
         __global__ void spgemm_bound(int rows, const int* __restrict__ ap, const int* __restrict__ ac,
-                                     const int* __restrict__ bp, int* __restrict__ out)
+                                     const int* __restrict__ bp, int* __restrict__ out, int* __restrict__ cand)
         {
             int m = 0;
             for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
@@ -217,6 +218,7 @@ namespace apf
                 for (int k = ap[r]; k < ap[r + 1]; ++k)
                     n += bp[ac[k] + 1] - bp[ac[k]];
                 m = max(m, n);
+                cand[r] = n;
             }
             for (int o = 16; o > 0; o >>= 1)
                 m = max(m, __shfl_down_sync(0xffffffffu, m, o));
@@ -293,9 +295,29 @@ namespace apf
                     }
                     uniq += __popc(hm);
                 }
-                if (!FILL && lane == 0)
+                if (lane == 0)
                     A.count[row] = uniq;
                 __syncwarp();
+            }
+        }
+
+        // one warp per row: move the row's distinct entries from its candidate segment of
+        // the staging arrays to the compressed result
+        __global__ void spgemm_compact(int rows, const int* __restrict__ cand_ptr, const int* __restrict__ tc,
+                                       const double* __restrict__ tv, const int* __restrict__ cp, int* __restrict__ cc,
+                                       double* __restrict__ cv)
+        {
+            const int lane = threadIdx.x & 31;
+            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            const int nw = (gridDim.x * blockDim.x) >> 5;
+            for (int r = warp; r < rows; r += nw)
+            {
+                const int src = cand_ptr[r], dst = cp[r], len = cp[r + 1] - dst;
+                for (int k = lane; k < len; k += 32)
+                {
+                    cc[dst + k] = tc[src + k];
+                    cv[dst + k] = tv[src + k];
+                }
             }
         }
 
@@ -631,17 +653,22 @@ namespace apf
             APF_CUDA(cudaMemsetAsync(C.row_ptr.get(), 0, sizeof(int), s));
             return;
         }
-        DeviceBuffer<int> bound(1, s);
+        // one sorting pass: each row's distinct products go to its candidate segment of
+        // staging arrays (sized by the candidate counts), then a compaction
+        DeviceBuffer<int> bound(1, s), cand(static_cast<std::size_t>(A.rows) + 1, s),
+            cand_ptr(static_cast<std::size_t>(A.rows) + 1, s);
         bound.zero();
         {
             APF_KERNEL("spgemm_bound", s);
             spgemm_bound<<<blocks_for(A.rows, 256, 148 * 8), 256, 0, s>>>(A.rows, A.row_ptr.get(), A.col_idx.get(),
-                                                                           B.row_ptr.get(), bound.get());
+                                                                           B.row_ptr.get(), bound.get(), cand.get());
         }
+        const long long total = exclusive_scan(cand.get(), cand_ptr.get(), A.rows, s);
         const int cap = read_int(s, bound.get());
-        DeviceBuffer<int> count(static_cast<std::size_t>(A.rows) + 1, s);
+        DeviceBuffer<int> count(static_cast<std::size_t>(A.rows) + 1, s), tc(static_cast<std::size_t>(std::max(total, 1ll)), s);
+        DeviceBuffer<double> tv(static_cast<std::size_t>(std::max(total, 1ll)), s);
         GemmArgs g{A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(), B.row_ptr.get(), B.col_idx.get(),
-                   B.values.get(), count.get(), nullptr, nullptr, nullptr};
+                   B.values.get(), count.get(), cand_ptr.get(), tc.get(), tv.get()};
         auto launch = [&](auto tag, bool fill_pass) {
             constexpr int CAP = decltype(tag)::value;
             const int warps = warps_for_cap<CAP>();
@@ -661,14 +688,16 @@ namespace apf
             }
             APF_CUDA(cudaGetLastError());
         };
-        with_cap(std::max(cap, 1), [&](auto tag) { launch(tag, false); });
+        with_cap(std::max(cap, 1), [&](auto tag) { launch(tag, true); });
         const long long nnz = exclusive_scan(count.get(), C.row_ptr.get(), A.rows, s);
         C.col_idx.allocate(static_cast<std::size_t>(nnz), s);
         C.values.allocate(static_cast<std::size_t>(nnz), s);
-        g.cp = C.row_ptr.get();
-        g.cc = C.col_idx.get();
-        g.cv = C.values.get();
-        with_cap(std::max(cap, 1), [&](auto tag) { launch(tag, true); });
+        {
+            APF_KERNEL("spgemm_compact", s);
+            spgemm_compact<<<blocks_for((long long)A.rows * 32, 256, 148 * 16), 256, 0, s>>>(
+                A.rows, cand_ptr.get(), tc.get(), tv.get(), C.row_ptr.get(), C.col_idx.get(), C.values.get());
+        }
+        APF_CUDA(cudaGetLastError());
     }
 
     void transpose(cudaStream_t s, const DeviceCsr& A, DeviceCsr& T)
