@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-estimator", action="store_true")
     ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--pool-reserve-gb", type=float, default=0.0,
+                    help="grow the device memory pool to this size once before the warm-up")
     ap.add_argument("--precond", default="learned", choices=["learned", "plain"],
                     help="learned: the shipped model (plain block preconditioner as fallback), timed beside plain")
     return ap.parse_args()
@@ -63,49 +65,60 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region
-    (one nvidia-smi process in loop mode, started before and stopped after)."""
+    """SM clocks and throttle reasons sampled during the timed region by an in-process NVML
+    thread (every 0.5 s; an nvidia-smi process polling the driver every 200 ms was seen to
+    stall the library's launches)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, device):
+    def __init__(self, device, period=0.5):
         self.device = device
+        self.period = period
         self.samples = []
-        self._proc = None
+        self._stop = None
+        self._t = None
+        self._nvml = None
+
+    def _run(self):
+        nv = self._nvml
+        h = nv.nvmlDeviceGetHandleByIndex(self.device)
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                    nv.nvmlDeviceGetCurrentClocksThrottleReasons
+                reasons = get(h)
+                self.samples.append((sm, mx, reasons))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
+        import threading
         try:
-            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                                           "--format=csv,noheader,nounits", "-lms", "200"],
-                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self._nvml = pynvml
         except Exception:
-            self._proc = None
+            return self
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
         return self
 
     def __exit__(self, *a):
-        if self._proc is None:
-            return
-        self._proc.terminate()
-        try:
-            out, _ = self._proc.communicate(timeout=10)
-        except Exception:
-            self._proc.kill()
-            out, _ = self._proc.communicate()
-        for line in (out or "").splitlines():
-            if line.strip():
-                self.samples.append([x.strip() for x in line.split(",")])
+        if self._t:
+            self._stop.set()
+            self._t.join(timeout=10)
 
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if len(s) > 1 and s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 5 + k and s[5 + k] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({name for s in self.samples for name, bit in self.REASONS.items() if s[2] & bit})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(s[1] for s in self.samples), "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml"}
 
 
 def measured_peaks():
@@ -293,6 +306,13 @@ def run_ours(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    def pool_stats():
+        v = [C.c_int64() for _ in range(4)]
+        ctx.check(lib.apf_ctx_pool_stats(ctx.handle, *[C.byref(x) for x in v]))
+        return [round(x.value / 2 ** 30, 2) for x in v]
+
+    if args.pool_reserve_gb > 0:
+        ctx.check(lib.apf_ctx_reserve_pool(ctx.handle, int(args.pool_reserve_gb * 2 ** 30)))
     # warm-up
     for _ in range(args.warmup):
         lib.apf_system_destroy(step(dprob, True))
@@ -307,9 +327,16 @@ def run_ours(args, world, rank, local):
     step_events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with ClockSampler(local) as clocks:
         ev0.record(stream)
+        stage_ms = []
         for k in range(args.steps):
+            ctx.check(lib.apf_ctx_set_timing(ctx.handle, 2))
             lib.apf_system_destroy(step(dprob, True))
             step_events[k].record(stream)
+            rep = json.loads(lib.apf_ctx_timing_report(ctx.handle).decode())
+            st = {k2[5:]: round(v[1], 1) for k2, v in rep.items() if k2.startswith("host:")}
+            st["pool_gib_reserved_high_used_high"] = pool_stats()
+            stage_ms.append(st)
+        ctx.check(lib.apf_ctx_set_timing(ctx.handle, 0))
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     step_ms = [round(ev0.elapsed_time(step_events[0]), 2)] + [
@@ -329,9 +356,11 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize(dev)
         p0 = torch.cuda.Event(enable_timing=True)
         p1 = torch.cuda.Event(enable_timing=True)
+        p_events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         p0.record(stream)
-        for _ in range(args.steps):
+        for k in range(args.steps):
             lib.apf_system_destroy(step(dprob, True))
+            p_events[k].record(stream)
         p1.record(stream)
         torch.cuda.synchronize(dev)
         barrier()
@@ -340,7 +369,9 @@ def run_ours(args, world, rank, local):
         plain = {"value": args.steps * n_dofs * world / plain_elapsed, "ms_per_step": 1e3 * plain_elapsed / args.steps,
                  "minres_iterations": [d["iterations"] for d in pd],
                  "final_true_residual_max": max(d["final_true_residual"] for d in pd),
-                 "minres_solve_s_mean": sum(d["solve_seconds"] for d in pd) / len(pd)}
+                 "minres_solve_s_mean": sum(d["solve_seconds"] for d in pd) / len(pd),
+                 "step_ms": [round(p0.elapsed_time(p_events[0]), 2)] + [
+                     round(p_events[k - 1].elapsed_time(p_events[k]), 2) for k in range(1, args.steps)]}
         sopt.preconditioner = _lib.APF_PRECOND_LEARNED
 
     # e2e through the C ABI from pinned host buffers
@@ -370,6 +401,17 @@ def run_ours(args, world, rank, local):
     ctx.check(lib.apf_ctx_set_timing(ctx.handle, 0))
     kernels = {k: v for k, v in report.items() if not k.startswith("host:")}
     host_ranges = {k[5:]: round(v[1], 3) for k, v in report.items() if k.startswith("host:")}
+    amg_levels = {}
+    for block, name in ((0, "A_y"), (1, "Hhat_F")):
+        L, dc, sw, sm = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        ctx.check(lib.apf_amg_info(ctx.handle, h, block, C.byref(L), C.byref(dc), C.byref(sw), C.byref(sm)))
+        rows = []
+        for lv in range(L.value):
+            r, na, npp, om, al = C.c_int(), C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
+            ctx.check(lib.apf_amg_level_info(ctx.handle, h, block, lv, C.byref(r), C.byref(na), C.byref(npp),
+                                             C.byref(om), C.byref(al)))
+            rows.append([r.value, na.value, npp.value])
+        amg_levels[name] = {"rows_nnz_nnzP": rows, "dense_coarsest": bool(dc.value)}
     m = MainSystemBlocks(ctx, h, host)
     nnz_k = m.block_info("K")[2]
     nnz_h = m.block_info("Hhat")[2]
@@ -422,6 +464,7 @@ def run_ours(args, world, rank, local):
                    "plain_preconditioner": plain,
                    "minres_iterations": [d["iterations"] for d in timed_diags],
                    "step_ms": step_ms,
+                   "step_stage_wall_ms": stage_ms,
                    "e2e_step_ms": e2e_step_ms,
                    "final_true_residual_max": max(d["final_true_residual"] for d in timed_diags),
                    "e2e_final_true_residual_max": max(d["final_true_residual"] for d in e2e_diags),
@@ -440,7 +483,9 @@ def run_ours(args, world, rank, local):
                      "traffic": None, "dominant_kernel": dominant[0],
                      "dominant_share": dominant[1][1] / total_ms if total_ms else None},
         "kernel_times_ms_per_step": {k: round(v[1], 3) for k, v in
-                                     sorted(kernels.items(), key=lambda kv: -kv[1][1])[:25]},
+                                     sorted(kernels.items(), key=lambda kv: -kv[1][1])[:45]},
+        "kernel_launches_per_step": {k: v[0] for k, v in sorted(kernels.items(), key=lambda kv: -kv[1][1])[:45]},
+        "amg_levels": amg_levels,
         "kernel_ms_sum_per_step": round(total_ms, 3),
         "host_wall_ms_per_step": host_ranges,
         "clocks": clocks.summary(),

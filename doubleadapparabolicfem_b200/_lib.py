@@ -195,3 +195,7 @@ class XIndicatorTotals(C.Structure):
 
 SIGNATURES["apf_x_indicators"] = ([_P, _P, C.c_int, _P, _P, _P, _P, C.POINTER(XIndicatorTotals)], C.c_int)
 SIGNATURES["apf_y_estimator_threshold_squared"] = ([C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)], C.c_int)
+
+SIGNATURES["apf_ctx_reserve_pool"] = ([_P, C.c_int64], C.c_int)
+SIGNATURES["apf_ctx_pool_stats"] = ([_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                     C.POINTER(C.c_int64)], C.c_int)

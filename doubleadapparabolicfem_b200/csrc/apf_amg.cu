@@ -220,6 +220,21 @@ namespace apf
             }
         }
 
+        // kernel-timer names per operation and level (levels above 5 share one name)
+        const char* level_name(int op, int l)
+        {
+            static const char* names[4][7] = {
+                {"amg_sweep_l0", "amg_sweep_l1", "amg_sweep_l2", "amg_sweep_l3", "amg_sweep_l4", "amg_sweep_l5",
+                 "amg_sweep_l6+"},
+                {"amg_residual_l0", "amg_residual_l1", "amg_residual_l2", "amg_residual_l3", "amg_residual_l4",
+                 "amg_residual_l5", "amg_residual_l6+"},
+                {"amg_restrict_l0", "amg_restrict_l1", "amg_restrict_l2", "amg_restrict_l3", "amg_restrict_l4",
+                 "amg_restrict_l5", "amg_restrict_l6+"},
+                {"amg_prolong_l0", "amg_prolong_l1", "amg_prolong_l2", "amg_prolong_l3", "amg_prolong_l4",
+                 "amg_prolong_l5", "amg_prolong_l6+"}};
+            return names[op][l < 6 ? l : 6];
+        }
+
         __global__ void jacobi_first(int n, const double* b, const double* dinv, double omega, double* x)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -591,19 +606,19 @@ namespace apf
         const DeviceSell& A32 = *L.A32;
         for (int k = 1; k < pre; ++k)
         {
-            jacobi_sweep(s, A32, cur, b, weights(k), om, other);
+            jacobi_sweep(s, A32, cur, b, weights(k), om, other, coarsest ? "amg_coarse_sweep" : level_name(0, l));
             std::swap(cur, other);
         }
         if (coarsest)
             return;
-        residual(s, A32, cur, b, L.r.get());
+        residual(s, A32, cur, b, L.r.get(), level_name(1, l));
         AmgLevel& C = levels_[static_cast<std::size_t>(l) + 1];
-        spmv(s, *L.R32, L.r.get(), C.b.get());
+        spmv(s, *L.R32, L.r.get(), C.b.get(), 1.0, 0.0, level_name(2, l));
         vcycle(s, l + 1, C.b.get(), C.x.get());
-        spmv(s, *L.P32, C.x.get(), cur, L.alpha, 1.0);
+        spmv(s, *L.P32, C.x.get(), cur, L.alpha, 1.0, level_name(3, l));
         for (int k = 0; k < post; ++k)
         {
-            jacobi_sweep(s, A32, cur, b, weights(post - 1 - k), om, other);
+            jacobi_sweep(s, A32, cur, b, weights(post - 1 - k), om, other, level_name(0, l));
             std::swap(cur, other);
         }
     }

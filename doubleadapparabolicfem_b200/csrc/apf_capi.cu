@@ -74,6 +74,36 @@ namespace
         }
     }
 
+    // Keep the stream-ordered pool at 1.5x the largest footprint seen so far, reserved as one
+    // block: carving each call's buffers from one block avoids the pool mapping fresh memory
+    // for fragmented requests (seen as stalls of up to seconds between identical calls).
+    void ensure_pool(apf_ctx* ctx)
+    {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) != cudaSuccess)
+            return;
+        std::uint64_t reserved = 0, used_high = 0;
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &used_high);
+        const std::uint64_t gib = 1ull << 30;
+        std::uint64_t target = ((used_high + used_high / 2 + gib - 1) / gib) * gib;
+        std::size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+            target = std::min<std::uint64_t>(target, (total_b / 10) * 7);
+        if (used_high == 0 || reserved >= target)
+            return;
+        void* p = nullptr;
+        if (cudaMallocAsync(&p, target, ctx->stream) == cudaSuccess)
+        {
+            cudaFreeAsync(p, ctx->stream);
+            cudaStreamSynchronize(ctx->stream);
+            // the reservation is not footprint: measure the next calls from here
+            std::uint64_t zero = 0;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero);
+        }
+        cudaGetLastError(); // a failed reservation only costs the optimisation
+    }
+
     template<class T>
     void stage(apf::DeviceBuffer<T>& dst, const T* src, std::size_t n, bool on_device, cudaStream_t s)
     {
@@ -242,7 +272,43 @@ int apf_ctx_set_timing(apf_ctx* ctx, int enable)
     return guarded(ctx, [&] {
         ctx->profiler.flush();
         ctx->profiler.enabled = enable != 0;
+        ctx->profiler.kernels = enable != 2;
         ctx->profiler.totals.clear();
+    });
+}
+
+int apf_ctx_reserve_pool(apf_ctx* ctx, int64_t bytes)
+{
+    if (!ctx || bytes < 0)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        if (bytes == 0)
+            return;
+        void* p = nullptr;
+        APF_CUDA(cudaMallocAsync(&p, static_cast<std::size_t>(bytes), ctx->stream));
+        APF_CUDA(cudaFreeAsync(p, ctx->stream));
+        APF_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int apf_ctx_pool_stats(apf_ctx* ctx, int64_t* reserved, int64_t* reserved_high, int64_t* used, int64_t* used_high)
+{
+    if (!ctx)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        cudaMemPool_t pool;
+        APF_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+        auto get = [&](cudaMemPoolAttr attr, int64_t* out) {
+            if (!out)
+                return;
+            std::uint64_t v = 0;
+            APF_CUDA(cudaMemPoolGetAttribute(pool, attr, &v));
+            *out = static_cast<int64_t>(v);
+        };
+        get(cudaMemPoolAttrReservedMemCurrent, reserved);
+        get(cudaMemPoolAttrReservedMemHigh, reserved_high);
+        get(cudaMemPoolAttrUsedMemCurrent, used);
+        get(cudaMemPoolAttrUsedMemHigh, used_high);
     });
 }
 
@@ -274,6 +340,7 @@ int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs
     h->ctx = ctx;
     const int rc = guarded(ctx, [&] {
         APF_HOST_RANGE("call_assemble_main_system");
+        ensure_pool(ctx);
         apf::require(d->p == 1 || d->p == 2, APF_ERR_INVALID, "p must be 1 or 2");
         apf::require(d->n_y_cells >= 0 && d->n_x_cells >= 0 && d->n_lambda >= 0 && d->n_u >= 0, APF_ERR_INVALID,
                      "negative sizes");

@@ -105,13 +105,15 @@ namespace apf
         cudaStream_t s_ = nullptr;
     };
 
-    // Sliced-ELLPACK copy of a CSR matrix for the SpMV: slices of 32 consecutive rows, each
+    // Sliced-ELLPACK copy of a CSR matrix for the SpMV: rows sorted by decreasing length
+    // inside windows of 512 (perm: sorted position -> row), slices of 32 sorted rows, each
     // slice stored column-major at its own width (one thread per row, coalesced loads),
     // padding entries have value 0 and column 0.
     struct DeviceSell
     {
         int rows = 0;
         int slices = 0;
+        DeviceBuffer<int> perm;      // sorted position -> row
         DeviceBuffer<int> slice_ptr; // slices + 1 element offsets
         DeviceBuffer<int> col;
         DeviceBuffer<double> val;    // f64 values, or empty when val32 holds them
@@ -145,6 +147,7 @@ namespace apf
     struct Profiler
     {
         bool enabled = false;
+        bool kernels = true; // false: host ranges only (no per-launch events)
         struct Rec
         {
             const char* name;
@@ -181,7 +184,7 @@ namespace apf
         KernelTimer(const char* name, cudaStream_t s) : s_(s)
         {
             g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-            if (t_profiler && t_profiler->enabled)
+            if (t_profiler && t_profiler->enabled && t_profiler->kernels)
             {
                 rec_.name = name;
                 cudaEventCreate(&rec_.a);

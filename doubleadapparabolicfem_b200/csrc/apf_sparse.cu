@@ -59,7 +59,7 @@ namespace apf
                                                            const int* __restrict__ col, const V* __restrict__ val,
                                                            const double* __restrict__ x, const double* __restrict__ b,
                                                            double* __restrict__ y, double alpha, double beta,
-                                                           const double* __restrict__ dinv)
+                                                           const double* __restrict__ dinv, const int* __restrict__ perm)
         {
             const int lane = threadIdx.x & 31;
             const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -80,9 +80,10 @@ namespace apf
                 if (j < width)
                     s0 += static_cast<double>(v[32 * j]) * __ldg(x + c[32 * j]);
                 const double sum = s0 + s1;
-                const int r = sl * 32 + lane;
-                if (r < rows)
+                const int rs = sl * 32 + lane;
+                if (rs < rows)
                 {
+                    const int r = perm ? perm[rs] : rs;
                     if (MODE == 1)
                         y[r] = b[r] - sum;
                     else if (MODE == 2)
@@ -100,15 +101,56 @@ namespace apf
         }
 
         // slice widths x 32 (element counts per slice)
-        __global__ void sell_count(int rows, int slices, const int* __restrict__ rp, int* __restrict__ cnt)
+        // rows sorted by decreasing length inside windows of kSellWindow rows (ties by row
+        // index): perm[sorted position] = row.  One block of 256 threads per window, bitonic
+        // sort of (length, row) keys in shared memory.
+        constexpr int kSellWindow = 512;
+        __global__ void __launch_bounds__(256) sell_sort_rows(int rows, const int* __restrict__ rp, int* __restrict__ perm)
+        {
+            __shared__ unsigned long long key[kSellWindow];
+            const int w0 = blockIdx.x * kSellWindow;
+            for (int k = threadIdx.x; k < kSellWindow; k += blockDim.x)
+            {
+                const int r = w0 + k;
+                const unsigned len = r < rows ? static_cast<unsigned>(rp[r + 1] - rp[r]) : 0u;
+                // descending length first, real rows before the window's padding, then index
+                const unsigned hi = r < rows ? 0x7fffffffu - min(len, 0x7ffffffeu) : 0xffffffffu;
+                key[k] = (static_cast<unsigned long long>(hi) << 32) | static_cast<unsigned>(k);
+            }
+            __syncthreads();
+            for (int size = 2; size <= kSellWindow; size <<= 1)
+                for (int stride = size >> 1; stride > 0; stride >>= 1)
+                {
+                    for (int t = threadIdx.x; t < kSellWindow / 2; t += blockDim.x)
+                    {
+                        const int i = 2 * t - (t & (stride - 1));
+                        const int j = i + stride;
+                        const bool up = (i & size) == 0;
+                        const unsigned long long a = key[i], b = key[j];
+                        if ((a > b) == up)
+                        {
+                            key[i] = b;
+                            key[j] = a;
+                        }
+                    }
+                    __syncthreads();
+                }
+            for (int k = threadIdx.x; k < kSellWindow; k += blockDim.x)
+                if (w0 + k < rows)
+                    perm[w0 + k] = w0 + static_cast<int>(key[k] & 0xffffffffu);
+        }
+
+        __global__ void sell_count(int rows, int slices, const int* __restrict__ rp, const int* __restrict__ perm,
+                                   int* __restrict__ cnt)
         {
             const int lane = threadIdx.x & 31;
             const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
             const int nwarps = (gridDim.x * blockDim.x) >> 5;
             for (int sl = warp; sl < slices; sl += nwarps)
             {
-                const int r = sl * 32 + lane;
-                int len = r < rows ? rp[r + 1] - rp[r] : 0;
+                const int rs = sl * 32 + lane;
+                const int r = rs < rows ? perm[rs] : 0;
+                int len = rs < rows ? rp[r + 1] - rp[r] : 0;
                 for (int o = 16; o > 0; o >>= 1)
                     len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
                 if (lane == 0)
@@ -118,8 +160,8 @@ namespace apf
 
         template<class V>
         __global__ void sell_fill(int rows, int slices, const int* __restrict__ rp, const int* __restrict__ ci,
-                                  const double* __restrict__ va, const int* __restrict__ sp, int* __restrict__ col,
-                                  V* __restrict__ val)
+                                  const double* __restrict__ va, const int* __restrict__ sp, const int* __restrict__ perm,
+                                  int* __restrict__ col, V* __restrict__ val)
         {
             const int lane = threadIdx.x & 31;
             const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -128,9 +170,10 @@ namespace apf
             {
                 const int base = sp[sl];
                 const int width = (sp[sl + 1] - base) >> 5;
-                const int r = sl * 32 + lane;
-                const int b = r < rows ? rp[r] : 0;
-                const int len = r < rows ? rp[r + 1] - b : 0;
+                const int rs = sl * 32 + lane;
+                const int r = rs < rows ? perm[rs] : 0;
+                const int b = rs < rows ? rp[r] : 0;
+                const int len = rs < rows ? rp[r + 1] - b : 0;
                 for (int j = 0; j < width; ++j)
                 {
                     const int o = base + 32 * j + lane;
@@ -442,10 +485,10 @@ namespace apf
             const int grid = blocks_for((long long)S.slices * 32, 256, 148 * 64);
             if (S.val32.size())
                 sell_kernel<MODE, float><<<grid, 256, 0, s>>>(S.rows, S.slices, S.slice_ptr.get(), S.col.get(),
-                                                              S.val32.get(), x, b, y, alpha, beta, dinv);
+                                                              S.val32.get(), x, b, y, alpha, beta, dinv, S.perm.get());
             else
                 sell_kernel<MODE, double><<<grid, 256, 0, s>>>(S.rows, S.slices, S.slice_ptr.get(), S.col.get(),
-                                                               S.val.get(), x, b, y, alpha, beta, dinv);
+                                                               S.val.get(), x, b, y, alpha, beta, dinv, S.perm.get());
             APF_CUDA(cudaGetLastError());
         }
 
@@ -484,11 +527,16 @@ namespace apf
         const int slices = (A.rows + 31) / 32;
         DeviceBuffer<int> cnt(slices, s);
         const int grid = blocks_for((long long)slices * 32, 256, 148 * 32);
+        auto S = std::make_unique<DeviceSell>();
+        S->perm.allocate(static_cast<std::size_t>(A.rows), s);
+        {
+            APF_KERNEL("sell_sort_rows", s);
+            sell_sort_rows<<<(A.rows + kSellWindow - 1) / kSellWindow, 256, 0, s>>>(A.rows, A.row_ptr.get(), S->perm.get());
+        }
         {
             APF_KERNEL("sell_count", s);
-            sell_count<<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), cnt.get());
+            sell_count<<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), S->perm.get(), cnt.get());
         }
-        auto S = std::make_unique<DeviceSell>();
         S->rows = A.rows;
         S->slices = slices;
         S->slice_ptr.allocate(static_cast<std::size_t>(slices) + 1, s);
@@ -500,7 +548,7 @@ namespace apf
         {
             APF_KERNEL("sell_fill", s);
             sell_fill<double><<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), A.col_idx.get(), A.values.get(),
-                                                  S->slice_ptr.get(), S->col.get(), S->val.get());
+                                                  S->slice_ptr.get(), S->perm.get(), S->col.get(), S->val.get());
         }
         APF_CUDA(cudaGetLastError());
         A.sell = std::move(S);
@@ -533,9 +581,14 @@ namespace apf
             return S;
         DeviceBuffer<int> cnt(S->slices, s);
         const int grid = blocks_for((long long)S->slices * 32, 256, 148 * 32);
+        S->perm.allocate(static_cast<std::size_t>(A.rows), s);
+        {
+            APF_KERNEL("sell_sort_rows", s);
+            sell_sort_rows<<<(A.rows + kSellWindow - 1) / kSellWindow, 256, 0, s>>>(A.rows, A.row_ptr.get(), S->perm.get());
+        }
         {
             APF_KERNEL("sell_count", s);
-            sell_count<<<grid, 256, 0, s>>>(A.rows, S->slices, A.row_ptr.get(), cnt.get());
+            sell_count<<<grid, 256, 0, s>>>(A.rows, S->slices, A.row_ptr.get(), S->perm.get(), cnt.get());
         }
         const long long total = exclusive_scan(cnt.get(), S->slice_ptr.get(), S->slices, s);
         S->col.allocate(static_cast<std::size_t>(total), s);
@@ -544,7 +597,7 @@ namespace apf
         {
             APF_KERNEL("sell_fill", s);
             sell_fill<float><<<grid, 256, 0, s>>>(A.rows, S->slices, A.row_ptr.get(), A.col_idx.get(), A.values.get(),
-                                                 S->slice_ptr.get(), S->col.get(), S->val32.get());
+                                                 S->slice_ptr.get(), S->perm.get(), S->col.get(), S->val32.get());
         }
         APF_CUDA(cudaGetLastError());
         return S;
@@ -560,19 +613,19 @@ namespace apf
     }
 
     void jacobi_sweep(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, const double* dinv,
-                      double omega, double* y)
+                      double omega, double* y, const char* name)
     {
         if (A.rows == 0)
             return;
-        APF_KERNEL("jacobi_sweep", s);
+        APF_KERNEL(name ? name : "jacobi_sweep", s);
         sell_launch<2>(s, A, x, b, y, omega, 0.0, dinv);
     }
 
-    void residual(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, double* r)
+    void residual(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, double* r, const char* name)
     {
         if (A.rows == 0)
             return;
-        APF_KERNEL("residual", s);
+        APF_KERNEL(name ? name : "residual", s);
         sell_launch<1>(s, A, x, b, r, 1.0, 0.0, nullptr);
     }
 

@@ -33,8 +33,9 @@ namespace apf
     void spmv(cudaStream_t s, const DeviceSell& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0,
               const char* name = nullptr);
     void jacobi_sweep(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, const double* dinv,
-                      double omega, double* y);
-    void residual(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, double* r);
+                      double omega, double* y, const char* name = nullptr);
+    void residual(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, double* r,
+                  const char* name = nullptr);
     // y = alpha * A x + beta * y   (beta == 0 ignores y's old contents)
     void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0,
               const char* name = nullptr);

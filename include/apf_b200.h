@@ -97,12 +97,20 @@ const char* apf_ctx_last_error(const apf_ctx* ctx);
 int apf_ctx_synchronize(apf_ctx* ctx);
 /* Number of kernels the library has launched in this process. */
 int64_t apf_ctx_kernel_launches(const apf_ctx* ctx);
-/* Per-kernel CUDA-event timing on the context's stream (the GPU counterpart of the
- * reference's TimingRecorder, src/finite_element/detail/timing.hpp).  Enabling
- * resets the totals. */
+/* Per-kernel CUDA-event timing on the context's stream plus host wall time of the
+ * library's stages (the GPU counterpart of the reference's TimingRecorder,
+ * src/finite_element/detail/timing.hpp): enable 1 = kernels and stages, 2 = stages only
+ * (no per-launch events), 0 = off.  Every call resets the totals. */
 int apf_ctx_set_timing(apf_ctx* ctx, int enable);
 /* JSON object {"kernel": [launches, total_ms], ...}; valid until the next call. */
 const char* apf_ctx_timing_report(apf_ctx* ctx);
+/* The library allocates from the device's default stream-ordered pool and keeps freed
+ * memory there.  apf_ctx_reserve_pool grows the pool to at least `bytes` at once (one
+ * allocation, freed again on the context's stream) so that later allocations are carved
+ * from it rather than mapped one by one; apf_ctx_pool_stats reports the pool's reserved
+ * and used bytes (current and high-water marks; any pointer may be NULL). */
+int apf_ctx_reserve_pool(apf_ctx* ctx, int64_t bytes);
+int apf_ctx_pool_stats(apf_ctx* ctx, int64_t* reserved, int64_t* reserved_high, int64_t* used, int64_t* used_high);
 
 /* ---- assembly ------------------------------------------------------------------ */
 /* Replaces finite_element::system::assemble_main_system_blocks<QS,QT,Backend>
