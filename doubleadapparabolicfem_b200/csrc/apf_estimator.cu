@@ -280,6 +280,53 @@ namespace apf
             return p;
         }
 
+        // block-wide barrier of a patch team (one warp: __syncwarp)
+        template<int W>
+        __device__ __forceinline__ void team_sync()
+        {
+            if (W == 1)
+                __syncwarp();
+            else
+                __syncthreads();
+        }
+
+        // arg-max over the team: (best, bi) of every thread -> the team's (largest value,
+        // smallest index among ties), identical on every thread
+        template<int W>
+        __device__ __forceinline__ void team_argmax(double& best, int& bi)
+        {
+            for (int o = 16; o > 0; o >>= 1)
+            {
+                const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi))
+                {
+                    best = ov;
+                    bi = oi;
+                }
+            }
+            if (W == 1)
+                return;
+            __shared__ double s_v[W];
+            __shared__ int s_i[W];
+            const int warp = threadIdx.x >> 5;
+            if ((threadIdx.x & 31) == 0)
+            {
+                s_v[warp] = best;
+                s_i[warp] = bi;
+            }
+            __syncthreads();
+            best = s_v[0];
+            bi = s_i[0];
+            for (int w = 1; w < W; ++w)
+                if (s_v[w] > best || (s_v[w] == best && s_i[w] < bi))
+                {
+                    best = s_v[w];
+                    bi = s_i[w];
+                }
+            __syncthreads();
+        }
+
         // One warp per patch; the patch system (n rows, two right-hand-side columns at n and
         // n + 1) lives in this warp's slice of shared memory with an odd row stride, so
         // column walks (pivot search, back substitution) are free of bank conflicts.
@@ -289,8 +336,8 @@ namespace apf
         //              over columns, applied to both right-hand sides at once;
         //   solve    : column-oriented back substitution, lanes over rows.
         // Patches arrive sorted into size buckets; NMAX is the bucket's bound.
-        template<int NMAX>
-        __global__ void __launch_bounds__(32) patch_solve(PatchArgs A, const PatchTables* __restrict__ tables,
+        template<int NMAX, int W>
+        __global__ void __launch_bounds__(32 * W) patch_solve(PatchArgs A, const PatchTables* __restrict__ tables,
                                                           const int* __restrict__ order, int count)
         {
             constexpr int LD = NMAX + 3; // odd: NMAX is even
@@ -298,9 +345,10 @@ namespace apf
             PatchTables& T = *reinterpret_cast<PatchTables*>(sm);
             double* K = sm + kPatchTableDoubles + (kPatchTableDoubles & 1);
             const int lane = threadIdx.x;
-            for (int i = lane; i < kPatchTableDoubles; i += 32)
+            constexpr int NT = 32 * W; // threads of the patch team
+            for (int i = lane; i < kPatchTableDoubles; i += NT)
                 sm[i] = reinterpret_cast<const double*>(tables)[i];
-            __syncwarp();
+            team_sync<W>();
             for (int idx = blockIdx.x; idx < count; idx += gridDim.x)
             {
                 const int p = order[idx];
@@ -317,9 +365,9 @@ namespace apf
                     continue;
                 }
                 const int sb = A.slab_ptr[slab];
-                for (int i = lane; i < n * LD; i += 32)
+                for (int i = lane; i < n * LD; i += NT)
                     K[i] = 0.0;
-                __syncwarp();
+                team_sync<W>();
                 double ht = 0.0;
                 for (int ic = 0; ic < nc; ++ic)
                 {
@@ -371,7 +419,7 @@ namespace apf
                     double du[3];
                     for (int s2 = 0; s2 < 3; ++s2)
                         du[s2] = (uu[2 * s2 + 1] - uu[2 * s2]) / k.ht;
-                    for (int t = lane; t < 113; t += 32)
+                    for (int t = lane; t < 113; t += NT)
                     {
                         if (t < 64)
                         {
@@ -419,23 +467,23 @@ namespace apf
                             K[(sbase + r) * LD + n - 1] += v;
                         }
                     }
-                    __syncwarp();
+                    team_sync<W>();
                 }
                 // right-hand sides times Mt^-1 (Mt = ht [[1/3,1/6],[1/6,1/3]], inverse (1/ht) [[4,-2],[-2,4]])
-                for (int i = lane; i < n; i += 32)
+                for (int i = lane; i < n; i += NT)
                 {
                     const double b0 = K[i * LD + n], b1 = K[i * LD + n + 1];
                     K[i * LD + n] = (4.0 * b0 - 2.0 * b1) / ht;
                     K[i * LD + n + 1] = (-2.0 * b0 + 4.0 * b1) / ht;
                 }
-                __syncwarp();
+                team_sync<W>();
                 // LU with partial pivoting on the augmented n x (n + 2) system
                 bool singular = false;
                 for (int col = 0; col < n; ++col)
                 {
                     double best = -1.0;
                     int bi = n;
-                    for (int i = col + lane; i < n; i += 32)
+                    for (int i = col + lane; i < n; i += NT)
                     {
                         const double v = fabs(K[i * LD + col]);
                         if (v > best)
@@ -444,43 +492,34 @@ namespace apf
                             bi = i;
                         }
                     }
-                    for (int o = 16; o > 0; o >>= 1)
-                    {
-                        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-                        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                        if (ov > best || (ov == best && oi < bi))
-                        {
-                            best = ov;
-                            bi = oi;
-                        }
-                    }
+                    team_argmax<W>(best, bi);
                     if (bi >= n || !(best > 0.0) || !isfinite(best))
                     {
                         singular = true;
                         break;
                     }
                     if (bi != col)
-                        for (int j = col + lane; j < n + 2; j += 32)
+                        for (int j = col + lane; j < n + 2; j += NT)
                         {
                             const double t0 = K[col * LD + j];
                             K[col * LD + j] = K[bi * LD + j];
                             K[bi * LD + j] = t0;
                         }
-                    __syncwarp();
+                    team_sync<W>();
                     const double inv = 1.0 / K[col * LD + col];
-                    for (int j = col + 1 + lane; j < n + 2; j += 32)
+                    for (int j = col + 1 + lane; j < n + 2; j += NT)
                     {
                         const double u = K[col * LD + j] * inv;
                         for (int i = col + 1; i < n; ++i)
                             K[i * LD + j] -= K[i * LD + col] * u;
                     }
-                    __syncwarp();
+                    team_sync<W>();
                 }
                 if (singular)
                 {
                     if (lane == 0)
                         atomicExch(A.status, APF_ERR_NUMERIC);
-                    __syncwarp();
+                    team_sync<W>();
                     continue;
                 }
                 // back substitution, both right-hand sides, lanes over the rows above
@@ -488,22 +527,22 @@ namespace apf
                 {
                     const double d = K[i * LD + i];
                     const double x0 = K[i * LD + n] / d, x1 = K[i * LD + n + 1] / d;
-                    for (int r = lane; r < i; r += 32)
+                    for (int r = lane; r < i; r += NT)
                     {
                         const double kri = K[r * LD + i];
                         K[r * LD + n] -= kri * x0;
                         K[r * LD + n + 1] -= kri * x1;
                     }
-                    __syncwarp();
+                    team_sync<W>();
                     if (lane == 0)
                     {
                         K[i * LD + n] = x0;
                         K[i * LD + n + 1] = x1;
                     }
                 }
-                __syncwarp();
+                team_sync<W>();
                 // flux of this patch restricted to each of its cells -> slot of the patch vertex
-                for (int t = lane; t < nc * 16; t += 32)
+                for (int t = lane; t < nc * 16; t += NT)
                 {
                     const int ic = t >> 4, kk = (t >> 3) & 1, j = t & 7;
                     const int c = A.slab_cells[sb + A.topo_cell[cb + ic]];
@@ -528,7 +567,7 @@ namespace apf
                         val = K[(2 * nfree + 2 * ic + (j - 6)) * LD + n + kk];
                     A.sigma[((3ll * c + a) * 2 + kk) * 8 + j] = val;
                 }
-                __syncwarp();
+                team_sync<W>();
             }
         }
 
@@ -876,8 +915,8 @@ namespace apf
         // one warp per p = 2 patch (same structure as patch_solve): 3 edge moments per free
         // edge, 6 interior RT_2 moments and 6 scalars per patch cell, the mean-zero row, and
         // three right-hand-side columns (one per time DOF)
-        template<int NMAX>
-        __global__ void __launch_bounds__(32) patch_solve2(PatchArgs A, const Rt2Tables* __restrict__ tables,
+        template<int NMAX, int W>
+        __global__ void __launch_bounds__(32 * W) patch_solve2(PatchArgs A, const Rt2Tables* __restrict__ tables,
                                                            const int* __restrict__ order, int count)
         {
             constexpr int LD = NMAX + 3; // odd: NMAX is even; columns n, n+1, n+2 hold the rhs
@@ -885,9 +924,10 @@ namespace apf
             Rt2Tables& T = *reinterpret_cast<Rt2Tables*>(sm);
             double* K = sm + kRt2Doubles + (kRt2Doubles & 1);
             const int lane = threadIdx.x;
-            for (int i = lane; i < kRt2Doubles; i += 32)
+            constexpr int NT = 32 * W; // threads of the patch team
+            for (int i = lane; i < kRt2Doubles; i += NT)
                 sm[i] = reinterpret_cast<const double*>(tables)[i];
-            __syncwarp();
+            team_sync<W>();
             for (int idx = blockIdx.x; idx < count; idx += gridDim.x)
             {
                 const int p = order[idx];
@@ -904,9 +944,9 @@ namespace apf
                     continue;
                 }
                 const int sb = A.slab_ptr[slab];
-                for (int i = lane; i < n * LD; i += 32)
+                for (int i = lane; i < n * LD; i += NT)
                     K[i] = 0.0;
-                __syncwarp();
+                team_sync<W>();
                 double ht = 0.0;
                 for (int ic = 0; ic < nc; ++ic)
                 {
@@ -965,7 +1005,7 @@ namespace apf
                     const double id = 1.0 / k.det;
                     const double h0 = (mg0 * k.J11 - mg1 * k.J01) * id; // (M grad psi)^T G e_0
                     const double h1 = (-mg0 * k.J10 + mg1 * k.J00) * id; // (M grad psi)^T G e_1
-                    for (int t = lane; t < 384; t += 32)
+                    for (int t = lane; t < 384; t += NT)
                     {
                         if (t < 225)
                         {
@@ -1015,22 +1055,22 @@ namespace apf
                             K[(sbase + r) * LD + n - 1] += v;
                         }
                     }
-                    __syncwarp();
+                    team_sync<W>();
                 }
                 // right-hand sides times Mt^-1 = (1 / ht) mtinv
-                for (int i = lane; i < n; i += 32)
+                for (int i = lane; i < n; i += NT)
                 {
                     const double b0 = K[i * LD + n], b1 = K[i * LD + n + 1], b2 = K[i * LD + n + 2];
                     for (int kk = 0; kk < 3; ++kk)
                         K[i * LD + n + kk] = (T.mtinv[kk][0] * b0 + T.mtinv[kk][1] * b1 + T.mtinv[kk][2] * b2) / ht;
                 }
-                __syncwarp();
+                team_sync<W>();
                 bool singular = false;
                 for (int col = 0; col < n; ++col)
                 {
                     double best = -1.0;
                     int bi = n;
-                    for (int i = col + lane; i < n; i += 32)
+                    for (int i = col + lane; i < n; i += NT)
                     {
                         const double v = fabs(K[i * LD + col]);
                         if (v > best)
@@ -1039,57 +1079,48 @@ namespace apf
                             bi = i;
                         }
                     }
-                    for (int o = 16; o > 0; o >>= 1)
-                    {
-                        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-                        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                        if (ov > best || (ov == best && oi < bi))
-                        {
-                            best = ov;
-                            bi = oi;
-                        }
-                    }
+                    team_argmax<W>(best, bi);
                     if (bi >= n || !(best > 0.0) || !isfinite(best))
                     {
                         singular = true;
                         break;
                     }
                     if (bi != col)
-                        for (int j = col + lane; j < n + 3; j += 32)
+                        for (int j = col + lane; j < n + 3; j += NT)
                         {
                             const double t0 = K[col * LD + j];
                             K[col * LD + j] = K[bi * LD + j];
                             K[bi * LD + j] = t0;
                         }
-                    __syncwarp();
+                    team_sync<W>();
                     const double inv = 1.0 / K[col * LD + col];
-                    for (int j = col + 1 + lane; j < n + 3; j += 32)
+                    for (int j = col + 1 + lane; j < n + 3; j += NT)
                     {
                         const double u = K[col * LD + j] * inv;
                         for (int i = col + 1; i < n; ++i)
                             K[i * LD + j] -= K[i * LD + col] * u;
                     }
-                    __syncwarp();
+                    team_sync<W>();
                 }
                 if (singular)
                 {
                     if (lane == 0)
                         atomicExch(A.status, APF_ERR_NUMERIC);
-                    __syncwarp();
+                    team_sync<W>();
                     continue;
                 }
                 for (int i = n - 1; i >= 0; --i)
                 {
                     const double d = K[i * LD + i];
                     const double x0 = K[i * LD + n] / d, x1 = K[i * LD + n + 1] / d, x2 = K[i * LD + n + 2] / d;
-                    for (int r = lane; r < i; r += 32)
+                    for (int r = lane; r < i; r += NT)
                     {
                         const double kri = K[r * LD + i];
                         K[r * LD + n] -= kri * x0;
                         K[r * LD + n + 1] -= kri * x1;
                         K[r * LD + n + 2] -= kri * x2;
                     }
-                    __syncwarp();
+                    team_sync<W>();
                     if (lane == 0)
                     {
                         K[i * LD + n] = x0;
@@ -1097,11 +1128,11 @@ namespace apf
                         K[i * LD + n + 2] = x2;
                     }
                 }
-                __syncwarp();
+                team_sync<W>();
                 // flux of this patch on each of its cells -> slot of the patch vertex:
                 // sigma slots [cell][3 vertices][3 time][15], coefficients of the cell's own
                 // RT_2 basis with the orientation of its edges
-                for (int t = lane; t < nc * 45; t += 32)
+                for (int t = lane; t < nc * 45; t += NT)
                 {
                     const int ic = t / 45, kk = (t / 15) % 3, j = t % 15;
                     const int c = A.slab_cells[sb + A.topo_cell[cb + ic]];
@@ -1125,7 +1156,7 @@ namespace apf
                         val = K[(3 * nfree + 6 * ic + (j - 9)) * LD + n + kk];
                     A.sigma[((3ll * c + a) * 3 + kk) * 15 + j] = val;
                 }
-                __syncwarp();
+                team_sync<W>();
             }
         }
 
@@ -1609,8 +1640,12 @@ namespace apf
             d_rt2.upload(reinterpret_cast<const double*>(&t2), kRt2Doubles);
             tables2 = reinterpret_cast<const Rt2Tables*>(d_rt2.get());
         }
+        // one team of W warps per patch: larger patches get more warps (the LU's column
+        // updates and the assembly spread over 32 W threads; shared memory bounds the teams
+        // per SM)
         auto launch = [&](auto tag, int b) {
             constexpr int NMAX = decltype(tag)::value;
+            constexpr int W = NMAX <= 48 ? 1 : (NMAX <= 64 ? 2 : 4);
             const int count = bucket_count[b + 1] - bucket_count[b];
             if (count == 0)
                 return;
@@ -1618,19 +1653,19 @@ namespace apf
             if (p2)
             {
                 constexpr std::size_t smem = patch2_smem_bytes<NMAX>();
-                APF_CUDA(cudaFuncSetAttribute(patch_solve2<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                APF_CUDA(cudaFuncSetAttribute(patch_solve2<NMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
-                const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32)));
+                const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32 / W)));
                 APF_KERNEL("est_patch_solve", s);
-                patch_solve2<NMAX><<<grid, 32, smem, s>>>(pa, tables2, d_order.get() + bucket_count[b], count);
+                patch_solve2<NMAX, W><<<grid, 32 * W, smem, s>>>(pa, tables2, d_order.get() + bucket_count[b], count);
                 return;
             }
             constexpr std::size_t smem = patch_smem_bytes<NMAX>();
-            APF_CUDA(cudaFuncSetAttribute(patch_solve<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            APF_CUDA(cudaFuncSetAttribute(patch_solve<NMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
-            const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32)));
+            const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32 / W)));
             APF_KERNEL("est_patch_solve", s);
-            patch_solve<NMAX><<<grid, 32, smem, s>>>(pa, tables, d_order.get() + bucket_count[b], count);
+            patch_solve<NMAX, W><<<grid, 32 * W, smem, s>>>(pa, tables, d_order.get() + bucket_count[b], count);
         };
         if (tot.n_patches > 0)
         {
