@@ -213,6 +213,8 @@ namespace apf
             int* col_out;
             double* val_out;
             int* status;         // nonzero on overflow
+            const int* list;     // rows to process (null: all)
+            int nlist;
         };
 
         // One warp per row.  CAP candidates per warp in shared memory.
@@ -233,8 +235,10 @@ namespace apf
             int* counter = incs + 2 * kIncCap;
             const int ndof = A.ndof;
 
-            for (int row = blockIdx.x * warps + w; row < A.n_rows; row += gridDim.x * warps)
+            const int nrows = A.list ? A.nlist : A.n_rows;
+            for (int idx = blockIdx.x * warps + w; idx < nrows; idx += gridDim.x * warps)
             {
+                const int row = A.list ? A.list[idx] : idx;
                 if (lane == 0)
                     *counter = 0;
                 __syncwarp();
@@ -574,6 +578,8 @@ namespace apf
             int* col_out;
             double* val_out;
             int* status;
+            const int* list; // rows to process (null: all)
+            int nlist;
         };
 
         // max over rows of |C row| + sum_{c in B_dt row} |B_dt^T row c| + |A_x row|
@@ -611,8 +617,10 @@ namespace apf
             unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
             double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
                            (size_t)w * CAP;
-            for (int row = blockIdx.x * warps + w; row < A.n_u; row += gridDim.x * warps)
+            const int nrows = A.list ? A.nlist : A.n_u;
+            for (int idx = blockIdx.x * warps + w; idx < nrows; idx += gridDim.x * warps)
             {
+                const int row = A.list ? A.list[idx] : idx;
                 int n = 0;
                 bool overflow = false;
                 // -C row (seq region 0)
@@ -858,7 +866,7 @@ namespace apf
                 APF_CUDA(cudaFuncSetAttribute(gather_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 APF_CUDA(cudaFuncSetAttribute(gather_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             }
-            const int blocks = grid_for(a.n_rows, warps, 148 * 16);
+            const int blocks = grid_for(a.list ? a.nlist : a.n_rows, warps, 148 * 16);
             (void)status;
             if (a.row_ptr == nullptr)
                 {
@@ -906,7 +914,9 @@ namespace apf
 
         void dispatch_gather(cudaStream_t s, GatherArgs& a, int cap)
         {
-            if (cap <= 512) run_gather<512>(s, a, a.status);
+            if (cap <= 64) run_gather<64>(s, a, a.status);
+            else if (cap <= 256) run_gather<256>(s, a, a.status);
+            else if (cap <= 512) run_gather<512>(s, a, a.status);
             else if (cap <= 2048) run_gather<2048>(s, a, a.status);
             else if (cap <= 8192) run_gather<8192>(s, a, a.status);
             else throw Error(APF_ERR_CAPACITY, "row candidate count exceeds 8192");
@@ -959,8 +969,18 @@ namespace apf
         a.row_ptr = cand_ptr.get();
         a.col_out = tc.get();
         a.val_out = tv.get();
-        if (n_rows > 0)
-            dispatch_gather(s, a, cap);
+        // rows by candidate count, each class with its own shared-memory capacity
+        (void)cap;
+        static constexpr int kCaps[5] = {64, 256, 512, 2048, 8192};
+        RowBuckets rb;
+        bucket_rows(s, n_rows, cand.get(), kCaps, 5, rb);
+        for (int b = 0; b < 5; ++b)
+        {
+            a.list = rb.list.get() + rb.offsets[b];
+            a.nlist = rb.offsets[b + 1] - rb.offsets[b];
+            if (a.nlist > 0)
+                dispatch_gather(s, a, kCaps[b]);
+        }
         out.rows = n_rows;
         out.cols = n_cols;
         out.row_ptr.allocate(static_cast<std::size_t>(n_rows) + 1, s);
@@ -1080,7 +1100,7 @@ namespace apf
             const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 16)));
             const int threads = warps * 32;
             const size_t smem = (size_t)warps * CAP * 16;
-            const int blocks = grid_for(n_u, warps, 148 * 32);
+            const int blocks = grid_for(a.list ? a.nlist : n_u, warps, 148 * 32);
             if (fill)
             {
                 APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1107,7 +1127,26 @@ namespace apf
         a.row_ptr = cand_ptr.get();
         a.col_out = tc.get();
         a.val_out = tv.get();
-        dispatch(true);
+        // rows by candidate count, each class with its own shared-memory capacity
+        static constexpr int kCaps[5] = {256, 512, 1024, 2048, 4096};
+        RowBuckets rb;
+        if (n_u > 0 && cap <= 4096)
+        {
+            bucket_rows(s, n_u, cand.get(), kCaps, 5, rb);
+            for (int b = 0; b < 5; ++b)
+            {
+                a.list = rb.list.get() + rb.offsets[b];
+                a.nlist = rb.offsets[b + 1] - rb.offsets[b];
+                if (a.nlist == 0)
+                    continue;
+                const int keep = cap;
+                cap = kCaps[b];
+                dispatch(true);
+                cap = keep;
+            }
+        }
+        else
+            dispatch(true);
         H.rows = H.cols = n_u;
         H.row_ptr.allocate(static_cast<std::size_t>(n_u) + 1, s);
         const long long nnz = exclusive_scan(counts.get(), H.row_ptr.get(), n_u, s);

@@ -280,6 +280,8 @@ namespace apf
             const int* cp;
             int* cc;
             double* cv;
+            const int* list; // rows to process (null: all rows)
+            int nlist;
         };
 
         template<int CAP, bool FILL>
@@ -291,8 +293,10 @@ namespace apf
             unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
             double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
                            (size_t)w * CAP;
-            for (int row = blockIdx.x * warps + w; row < A.rows; row += gridDim.x * warps)
+            const int nrows = A.list ? A.nlist : A.rows;
+            for (int idx = blockIdx.x * warps + w; idx < nrows; idx += gridDim.x * warps)
             {
+                const int row = A.list ? A.list[idx] : idx;
                 int n = 0, seq = 0;
                 for (int k = A.ap[row]; k < A.ap[row + 1]; ++k)
                 {
@@ -341,6 +345,29 @@ namespace apf
                 if (lane == 0)
                     A.count[row] = uniq;
                 __syncwarp();
+            }
+        }
+
+        __global__ void bucket_count_kernel(int rows, const int* __restrict__ cand, const int* __restrict__ caps,
+                                            int ncaps, int* __restrict__ cls, int* __restrict__ counts)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+            {
+                int b = 0;
+                while (b < ncaps && cand[r] > caps[b])
+                    ++b;
+                cls[r] = b;
+                atomicAdd(counts + b, 1);
+            }
+        }
+
+        __global__ void bucket_fill_kernel(int rows, const int* __restrict__ cls, const int* __restrict__ base,
+                                           int* __restrict__ cursor, int* __restrict__ list)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+            {
+                const int b = cls[r];
+                list[base[b] + atomicAdd(cursor + b, 1)] = r;
             }
         }
 
@@ -695,6 +722,37 @@ namespace apf
                                                                  inv.get());
     }
 
+    void bucket_rows(cudaStream_t s, int rows, const int* cand, const int* caps, int ncaps, RowBuckets& out)
+    {
+        require(ncaps >= 1 && ncaps <= 16, APF_ERR_INVALID, "bucket_rows: 1 to 16 classes");
+        DeviceBuffer<int> dcaps(ncaps, s), cls(static_cast<std::size_t>(std::max(rows, 1)), s), counts(ncaps + 1, s),
+            base(ncaps + 1, s), cursor(ncaps + 1, s);
+        dcaps.upload(caps, ncaps);
+        counts.zero();
+        cursor.zero();
+        if (rows > 0)
+        {
+            APF_KERNEL("bucket_rows", s);
+            bucket_count_kernel<<<blocks_for(rows, 256), 256, 0, s>>>(rows, cand, dcaps.get(), ncaps, cls.get(), counts.get());
+        }
+        std::vector<int> h(ncaps + 1, 0);
+        APF_CUDA(cudaMemcpyAsync(h.data(), counts.get(), (ncaps + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        require(h[ncaps] == 0, APF_ERR_CAPACITY, "sparse product: a row has more candidates than the largest class");
+        out.offsets.assign(ncaps + 1, 0);
+        for (int b = 0; b < ncaps; ++b)
+            out.offsets[b + 1] = out.offsets[b] + h[b];
+        base.upload(out.offsets.data(), ncaps + 1);
+        out.list.allocate(static_cast<std::size_t>(std::max(rows, 1)), s);
+        if (rows > 0)
+        {
+            APF_KERNEL("bucket_rows", s);
+            bucket_fill_kernel<<<blocks_for(rows, 256), 256, 0, s>>>(rows, cls.get(), base.get(), cursor.get(),
+                                                                    out.list.get());
+        }
+        APF_CUDA(cudaGetLastError());
+    }
+
     void spgemm(cudaStream_t s, const DeviceCsr& A, const DeviceCsr& B, DeviceCsr& C)
     {
         require(A.cols == B.rows, APF_ERR_INVALID, "spgemm: inner dimensions differ");
@@ -717,16 +775,20 @@ namespace apf
                                                                            B.row_ptr.get(), bound.get(), cand.get());
         }
         const long long total = exclusive_scan(cand.get(), cand_ptr.get(), A.rows, s);
-        const int cap = read_int(s, bound.get());
         DeviceBuffer<int> count(static_cast<std::size_t>(A.rows) + 1, s), tc(static_cast<std::size_t>(std::max(total, 1ll)), s);
         DeviceBuffer<double> tv(static_cast<std::size_t>(std::max(total, 1ll)), s);
         GemmArgs g{A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(), B.row_ptr.get(), B.col_idx.get(),
-                   B.values.get(), count.get(), cand_ptr.get(), tc.get(), tv.get()};
+                   B.values.get(), count.get(), cand_ptr.get(), tc.get(), tv.get(), nullptr, 0};
+        // rows by candidate count: each class runs with its own shared-memory capacity, so
+        // the few long rows no longer set the occupancy of all the others
+        static constexpr int kCaps[5] = {64, 256, 1024, 4096, 8192};
+        RowBuckets rb;
+        bucket_rows(s, A.rows, cand.get(), kCaps, 5, rb);
         auto launch = [&](auto tag, bool fill_pass) {
             constexpr int CAP = decltype(tag)::value;
             const int warps = warps_for_cap<CAP>();
             const size_t smem = (size_t)warps * CAP * 16;
-            const int blocks = blocks_for(A.rows, warps, 148 * 32);
+            const int blocks = blocks_for(g.nlist, warps, 148 * 32);
             if (fill_pass)
             {
                 APF_CUDA(cudaFuncSetAttribute(spgemm_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -741,7 +803,13 @@ namespace apf
             }
             APF_CUDA(cudaGetLastError());
         };
-        with_cap(std::max(cap, 1), [&](auto tag) { launch(tag, true); });
+        for (int b = 0; b < 5; ++b)
+        {
+            g.list = rb.list.get() + rb.offsets[b];
+            g.nlist = rb.offsets[b + 1] - rb.offsets[b];
+            if (g.nlist > 0)
+                with_cap(kCaps[b], [&](auto tag) { launch(tag, true); });
+        }
         const long long nnz = exclusive_scan(count.get(), C.row_ptr.get(), A.rows, s);
         C.col_idx.allocate(static_cast<std::size_t>(nnz), s);
         C.values.allocate(static_cast<std::size_t>(nnz), s);

@@ -2,6 +2,8 @@
 // by per-row gather + warp sort, transposes, deterministic reductions.
 #pragma once
 
+#include <vector>
+
 #include "apf_internal.hpp"
 
 namespace apf
@@ -53,6 +55,15 @@ namespace apf
     void transpose(cudaStream_t s, const DeviceCsr& A, DeviceCsr& T);
     // inverse diagonal of a square CSR
     void inverse_diagonal(cudaStream_t s, const DeviceCsr& A, DeviceBuffer<double>& inv);
+    // Rows grouped by their candidate count into capacity classes caps[0] < caps[1] < ...:
+    // list holds the rows of class 0, then class 1, ...; offsets (host) has ncaps + 1 entries.
+    // Rows above the last class are an error (APF_ERR_CAPACITY).
+    struct RowBuckets
+    {
+        DeviceBuffer<int> list;
+        std::vector<int> offsets;
+    };
+    void bucket_rows(cudaStream_t s, int rows, const int* cand, const int* caps, int ncaps, RowBuckets& out);
     // vector helpers
     void axpby(cudaStream_t s, int n, double a, const double* x, double b, double* y); // y = a x + b y
     void copy(cudaStream_t s, int n, const double* x, double* y);
