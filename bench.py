@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-estimator", action="store_true")
     ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--profile-run", action="store_true",
+                    help="one device-resident step and exit (a short program for ncu captures); no JSON line")
     ap.add_argument("--pool-reserve-gb", type=float, default=0.0,
                     help="grow the device memory pool to this size once before the warm-up")
     ap.add_argument("--precond", default="learned", choices=["learned", "plain"],
@@ -313,6 +315,11 @@ def run_ours(args, world, rank, local):
 
     if args.pool_reserve_gb > 0:
         ctx.check(lib.apf_ctx_reserve_pool(ctx.handle, int(args.pool_reserve_gb * 2 ** 30)))
+    if args.profile_run:
+        lib.apf_system_destroy(step(dprob, True))
+        ctx.synchronize()
+        print(f"profile run: {solve_diags[-1]['iterations']} MINRES iterations, {ctx.kernel_launches()} launches")
+        return
     # warm-up
     for _ in range(args.warmup):
         lib.apf_system_destroy(step(dprob, True))
