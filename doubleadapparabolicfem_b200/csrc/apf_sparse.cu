@@ -70,16 +70,25 @@ namespace apf
                 const int width = (sp[sl + 1] - base) >> 5;
                 const V* v = val + base + lane;
                 const int* c = col + base + lane;
-                double s0 = 0.0, s1 = 0.0;
+                // four independent load chains in flight per thread; the matrix streams
+                // through once (evict-first loads), x stays cached for the gathers
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
                 int j = 0;
-                for (; j + 1 < width; j += 2)
+                for (; j + 3 < width; j += 4)
                 {
-                    s0 += static_cast<double>(v[32 * j]) * __ldg(x + c[32 * j]);
-                    s1 += static_cast<double>(v[32 * j + 32]) * __ldg(x + c[32 * j + 32]);
+                    const int c0 = __ldcs(c + 32 * j), c1 = __ldcs(c + 32 * j + 32);
+                    const int c2 = __ldcs(c + 32 * j + 64), c3 = __ldcs(c + 32 * j + 96);
+                    const V v0 = __ldcs(v + 32 * j), v1 = __ldcs(v + 32 * j + 32);
+                    const V v2 = __ldcs(v + 32 * j + 64), v3 = __ldcs(v + 32 * j + 96);
+                    const double x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+                    s0 += static_cast<double>(v0) * x0;
+                    s1 += static_cast<double>(v1) * x1;
+                    s2 += static_cast<double>(v2) * x2;
+                    s3 += static_cast<double>(v3) * x3;
                 }
-                if (j < width)
-                    s0 += static_cast<double>(v[32 * j]) * __ldg(x + c[32 * j]);
-                const double sum = s0 + s1;
+                for (; j < width; ++j)
+                    s0 += static_cast<double>(__ldcs(v + 32 * j)) * __ldg(x + __ldcs(c + 32 * j));
+                const double sum = (s0 + s1) + (s2 + s3);
                 const int rs = sl * 32 + lane;
                 if (rs < rows)
                 {
@@ -348,26 +357,51 @@ namespace apf
             }
         }
 
+        // class of every row; per-block histograms in shared memory, one global atomic per
+        // class and block
         __global__ void bucket_count_kernel(int rows, const int* __restrict__ cand, const int* __restrict__ caps,
                                             int ncaps, int* __restrict__ cls, int* __restrict__ counts)
         {
+            __shared__ int h[17];
+            if (threadIdx.x < 17)
+                h[threadIdx.x] = 0;
+            __syncthreads();
             for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
             {
                 int b = 0;
                 while (b < ncaps && cand[r] > caps[b])
                     ++b;
                 cls[r] = b;
-                atomicAdd(counts + b, 1);
+                atomicAdd(h + b, 1);
             }
+            __syncthreads();
+            if (threadIdx.x <= ncaps && h[threadIdx.x])
+                atomicAdd(counts + threadIdx.x, h[threadIdx.x]);
         }
 
+        // rows into their class ranges: each block reserves its slots per class with one
+        // global atomic, then places its rows through shared-memory cursors
         __global__ void bucket_fill_kernel(int rows, const int* __restrict__ cls, const int* __restrict__ base,
                                            int* __restrict__ cursor, int* __restrict__ list)
         {
-            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+            __shared__ int h[17], off[17];
+            const int r0 = blockIdx.x * blockDim.x * 8, r1 = min(rows, r0 + static_cast<int>(blockDim.x) * 8);
+            if (threadIdx.x < 17)
+                h[threadIdx.x] = 0;
+            __syncthreads();
+            for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+                atomicAdd(h + cls[r], 1);
+            __syncthreads();
+            if (threadIdx.x < 17)
+            {
+                off[threadIdx.x] = h[threadIdx.x] ? base[threadIdx.x] + atomicAdd(cursor + threadIdx.x, h[threadIdx.x]) : 0;
+                h[threadIdx.x] = 0;
+            }
+            __syncthreads();
+            for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x)
             {
                 const int b = cls[r];
-                list[base[b] + atomicAdd(cursor + b, 1)] = r;
+                list[off[b] + atomicAdd(h + b, 1)] = r;
             }
         }
 
@@ -747,8 +781,8 @@ namespace apf
         if (rows > 0)
         {
             APF_KERNEL("bucket_rows", s);
-            bucket_fill_kernel<<<blocks_for(rows, 256), 256, 0, s>>>(rows, cls.get(), base.get(), cursor.get(),
-                                                                    out.list.get());
+            bucket_fill_kernel<<<(rows + 256 * 8 - 1) / (256 * 8), 256, 0, s>>>(rows, cls.get(), base.get(), cursor.get(),
+                                                                                out.list.get());
         }
         APF_CUDA(cudaGetLastError());
     }
