@@ -295,10 +295,30 @@ namespace apf
         amg_h.setup(s, hhat_f, opt, w, x_component);
     }
 
+    BlockPreconditioner::~BlockPreconditioner()
+    {
+        if (side_)
+            cudaStreamDestroy(side_);
+        if (fork_)
+            cudaEventDestroy(fork_);
+        if (join_)
+            cudaEventDestroy(join_);
+    }
+
     void BlockPreconditioner::apply(cudaStream_t s, const double* r, double* z)
     {
+        if (!side_)
+        {
+            APF_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+            APF_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+            APF_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
+        }
+        APF_CUDA(cudaEventRecord(fork_, s));
+        APF_CUDA(cudaStreamWaitEvent(side_, fork_, 0));
+        amg_h.apply(side_, r + n_lambda, z + n_lambda);
         amg_a.apply(s, r, z);
-        amg_h.apply(s, r + n_lambda, z + n_lambda);
+        APF_CUDA(cudaEventRecord(join_, side_));
+        APF_CUDA(cudaStreamWaitEvent(s, join_, 0));
     }
 
     MinresSummary minres_solve(cudaStream_t s, const DeviceCsr& K, Preconditioner& P, const double* b, double* x,

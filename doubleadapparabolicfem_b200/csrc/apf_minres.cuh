@@ -13,10 +13,16 @@ namespace apf
         virtual void apply(cudaStream_t s, const double* r, double* z) = 0;
     };
 
-    // blkdiag(A_y, Hhat)^{-1} approximated by one AMG V-cycle per block.
+    // blkdiag(A_y, Hhat)^{-1} approximated by one AMG V-cycle per block.  The two V-cycles
+    // are independent: the Hhat one runs on a second stream forked from and joined back
+    // into the caller's stream, so the latency-bound coarse levels of both overlap.
     class BlockPreconditioner : public Preconditioner
     {
     public:
+        BlockPreconditioner() = default;
+        BlockPreconditioner(const BlockPreconditioner&) = delete;
+        BlockPreconditioner& operator=(const BlockPreconditioner&) = delete;
+        ~BlockPreconditioner() override;
         // y_component / x_component: time level of every Y / X DOF (device) or null
         void setup(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& Hhat, const AmgOptions& opt, Workspace& w,
                    const int* y_component = nullptr, const int* x_component = nullptr);
@@ -25,6 +31,10 @@ namespace apf
         Amg amg_a, amg_h;
         DeviceCsr hhat_f; // filtered SPD operator the Hhat hierarchy is built on
         static constexpr double kHhatDrop = 0.01;
+
+    private:
+        cudaStream_t side_ = nullptr;
+        cudaEvent_t fork_ = nullptr, join_ = nullptr;
     };
 
     struct MinresOptions

@@ -16,6 +16,9 @@ namespace apf
         }
 
         // G lanes per row; the row loop is warp-uniform so the shuffles see all 32 lanes.
+        // Each lane keeps four predicated loads of the row in flight per step (the row
+        // pointer, column, value and x gathers form one dependent chain per step, so the
+        // number of steps per row, not the bytes, sets the time on L2-resident levels).
         // MODE 0: y = alpha A x + beta y;  1: y = b - A x;  2: y = x + alpha dinv (b - A x)
         template<int G, int MODE, class V = double>
         __global__ void __launch_bounds__(256) spmv_kernel(int rows, const int* __restrict__ rp, const int* __restrict__ ci,
@@ -31,13 +34,31 @@ namespace apf
             for (long long base = warp * RPW; base < rows; base += nwarps * RPW)
             {
                 const long long r = base + sub;
-                double sum = 0.0;
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
                 if (r < rows)
                 {
-                    const int s0 = rp[r], e = rp[r + 1];
-                    for (int k = s0 + lane; k < e; k += G)
-                        sum += static_cast<double>(va[k]) * __ldg(x + ci[k]);
+                    const int e = rp[r + 1];
+                    for (int k = rp[r] + lane; k < e; k += 4 * G)
+                    {
+                        const bool p1 = k + G < e, p2 = k + 2 * G < e, p3 = k + 3 * G < e;
+                        const int c0 = ci[k];
+                        const int c1 = p1 ? ci[k + G] : 0;
+                        const int c2 = p2 ? ci[k + 2 * G] : 0;
+                        const int c3 = p3 ? ci[k + 3 * G] : 0;
+                        const double v0 = static_cast<double>(va[k]);
+                        const double v1 = p1 ? static_cast<double>(va[k + G]) : 0.0;
+                        const double v2 = p2 ? static_cast<double>(va[k + 2 * G]) : 0.0;
+                        const double v3 = p3 ? static_cast<double>(va[k + 3 * G]) : 0.0;
+                        s0 += v0 * __ldg(x + c0);
+                        if (p1)
+                            s1 += v1 * __ldg(x + c1);
+                        if (p2)
+                            s2 += v2 * __ldg(x + c2);
+                        if (p3)
+                            s3 += v3 * __ldg(x + c3);
+                    }
                 }
+                double sum = (s0 + s1) + (s2 + s3);
 #pragma unroll
                 for (int o = G / 2; o > 0; o >>= 1)
                     sum += __shfl_down_sync(0xffffffffu, sum, o, G);
@@ -518,13 +539,19 @@ namespace apf
 
     namespace
     {
-        // G lanes per row from the mean row length
+        // G lanes per row: about four to eight entries per lane (one or two unrolled steps
+        // per row), then more lanes while the launch would not fill the GPU once
         template<class F>
-        void with_lanes(double avg, F&& go)
+        void with_lanes(long long rows, double avg, F&& go)
         {
-            if (avg <= 6) go(std::integral_constant<int, 4>{});
-            else if (avg <= 14) go(std::integral_constant<int, 8>{});
-            else if (avg <= 40) go(std::integral_constant<int, 16>{});
+            int g = 4;
+            while (g < 32 && avg > 6.0 * g)
+                g *= 2;
+            while (g < 32 && rows * g < 148LL * 2048)
+                g *= 2;
+            if (g == 4) go(std::integral_constant<int, 4>{});
+            else if (g == 8) go(std::integral_constant<int, 8>{});
+            else if (g == 16) go(std::integral_constant<int, 16>{});
             else go(std::integral_constant<int, 32>{});
         }
 
@@ -535,7 +562,7 @@ namespace apf
             if (S.csr_rp)
             {
                 // CSR layout with f32 values (short or wide-row operators)
-                with_lanes(S.avg_row, [&](auto g) {
+                with_lanes(S.rows, S.avg_row, [&](auto g) {
                     constexpr int G = decltype(g)::value;
                     spmv_kernel<G, MODE, float><<<blocks_for((long long)S.rows * G, 256, 148 * 64), 256, 0, s>>>(
                         S.rows, S.csr_rp, S.csr_ci, S.val32.get(), x, b, y, alpha, beta, dinv);
@@ -567,15 +594,11 @@ namespace apf
                 sell_launch<MODE>(s, *A.sell, x, b, y, alpha, beta, dinv);
                 return;
             }
-            auto go = [&](auto g) {
+            with_lanes(A.rows, avg, [&](auto g) {
                 constexpr int G = decltype(g)::value;
                 spmv_kernel<G, MODE><<<blocks_for((long long)A.rows * G, threads, 148 * 64), threads, 0, s>>>(
                     A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(), x, b, y, alpha, beta, dinv);
-            };
-            if (avg <= 6) go(std::integral_constant<int, 4>{});
-            else if (avg <= 14) go(std::integral_constant<int, 8>{});
-            else if (avg <= 40) go(std::integral_constant<int, 16>{});
-            else go(std::integral_constant<int, 32>{});
+            });
             APF_CUDA(cudaGetLastError());
         }
     }
