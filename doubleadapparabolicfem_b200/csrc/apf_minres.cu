@@ -54,6 +54,68 @@ namespace apf
             return t;
         }
 
+        // One MINRES iteration as a CUDA graph: its ~100 launches (Lanczos step, K SpMV,
+        // both V-cycles on their two streams) are replayed with one launch.  The three
+        // Lanczos vectors rotate with period 3, so a solve needs at most four graphs
+        // (first iteration + three rotation phases).
+        struct IterationGraph
+        {
+            cudaGraphExec_t exec = nullptr;
+            long long kernels = 0;
+            int batch = -1;
+            ~IterationGraph()
+            {
+                if (exec)
+                    cudaGraphExecDestroy(exec);
+            }
+            void reset()
+            {
+                if (exec)
+                    cudaGraphExecDestroy(exec);
+                exec = nullptr;
+                kernels = 0;
+                batch = -1;
+            }
+        };
+
+        // Capture `body` (launches on s and streams forked from it) into g.
+        template<class F>
+        void capture_iteration(cudaStream_t s, IterationGraph& g, F&& body)
+        {
+            g.reset();
+            const long long before = g_kernel_launches.load();
+            APF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try
+            {
+                body();
+            }
+            catch (...)
+            {
+                cudaGraph_t partial = nullptr;
+                cudaStreamEndCapture(s, &partial);
+                if (partial)
+                    cudaGraphDestroy(partial);
+                cudaGetLastError();
+                throw;
+            }
+            cudaGraph_t graph = nullptr;
+            APF_CUDA(cudaStreamEndCapture(s, &graph));
+            g.kernels = g_kernel_launches.load() - before;
+            g_kernel_launches.fetch_sub(g.kernels);
+            const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            APF_CUDA(e);
+        }
+
+        // Graphs are used unless per-launch event timing is on (the events bracket single
+        // launches) or the caller's stream is the legacy default stream (not capturable).
+        bool graphs_enabled(cudaStream_t s)
+        {
+            if (s == nullptr || s == cudaStreamLegacy)
+                return false;
+            return !(t_profiler && t_profiler->enabled && t_profiler->kernels);
+        }
+
         __global__ void k_vscale(int n, const double* __restrict__ z, double* __restrict__ v, const MinresDev* S)
         {
             if (S->done)
@@ -267,6 +329,12 @@ namespace apf
     {
         n_lambda = A_y.rows;
         n_u = Hhat.rows;
+        if (!side_)
+        {
+            APF_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+            APF_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+            APF_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
+        }
         amg_a.setup(s, A_y, opt, w, y_component);
         // Hhat carries many couplings far below its diagonal scale (products of the
         // time-derivative columns that nearly cancel); the hierarchy is built on the
@@ -307,12 +375,7 @@ namespace apf
 
     void BlockPreconditioner::apply(cudaStream_t s, const double* r, double* z)
     {
-        if (!side_)
-        {
-            APF_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-            APF_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
-            APF_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
-        }
+        require(side_ != nullptr, APF_ERR_INVALID, "block preconditioner used before its setup");
         APF_CUDA(cudaEventRecord(fork_, s));
         APF_CUDA(cudaStreamWaitEvent(side_, fork_, 0));
         amg_h.apply(side_, r + n_lambda, z + n_lambda);
@@ -330,6 +393,8 @@ namespace apf
         DeviceBuffer<double> r1(n, s), r2(n, s), y(n, s), z(n, s), v(n, s), w1(n, s), w2(n, s), res(n, s);
         DeviceBuffer<MinresDev> S(1, s);
         DeviceBuffer<double> parts(kRedBlocks, s);
+        const bool use_graphs = graphs_enabled(s);
+        IterationGraph graphs[4];
         const double bn = std::sqrt(dot_host(s, w, n, b, b));
         if (bn == 0.0)
         {
@@ -394,45 +459,65 @@ namespace apf
                     for (int c = 0; c < chunk; ++c)
                     {
                         const int first = issued == 0;
+                        double* q1 = pr1;
+                        double* q2 = pr2;
+                        double* qy = py;
+                        // vectors before the step: r1 = q1, r2 = q2, y = qy; after it the
+                        // roles rotate (r1 <- r2, r2 <- y, y <- r1)
+                        auto step = [&]() {
+                            {
+                                APF_KERNEL("minres_vscale", s);
+                                k_vscale<<<nb(n), kThreads, 0, s>>>(n, z.get(), v.get(), S.get());
+                            }
+                            spmv(s, K, v.get(), qy, 1.0, 0.0, "minres_spmv_K");
+                            {
+                                APF_KERNEL("minres_t1", s);
+                                k_t1<<<kRedBlocks, kThreads, 0, s>>>(n, qy, q1, v.get(), S.get(), first, parts.get());
+                            }
+                            {
+                                APF_KERNEL("minres_alfa", s);
+                                k_alfa<<<1, 256, 0, s>>>(kRedBlocks, parts.get(), S.get());
+                            }
+                            {
+                                APF_KERNEL("minres_t2", s);
+                                k_t2<<<nb(n), kThreads, 0, s>>>(n, qy, q2, S.get());
+                            }
+                            P.apply(s, qy, z.get());
+                            {
+                                APF_KERNEL("minres_dot", s);
+                                k_dot_partials<<<kRedBlocks, kThreads, 0, s>>>(n, qy, z.get(), parts.get());
+                            }
+                            {
+                                APF_KERNEL("minres_scalars", s);
+                                k_scalars<<<1, 256, 0, s>>>(kRedBlocks, parts.get(), S.get());
+                            }
+                            {
+                                APF_KERNEL("minres_w", s);
+                                k_w<<<nb(n), kThreads, 0, s>>>(n, v.get(), w1.get(), w2.get(), x, S.get());
+                            }
+                            {
+                                APF_KERNEL("minres_check", s);
+                                k_check<<<1, 1, 0, s>>>(S.get(), this_batch);
+                            }
+                        };
+                        if (use_graphs)
                         {
-                            APF_KERNEL("minres_vscale", s);
-                            k_vscale<<<nb(n), kThreads, 0, s>>>(n, z.get(), v.get(), S.get());
+                            IterationGraph& g = first ? graphs[3] : graphs[issued % 3];
+                            if (!g.exec || g.batch != this_batch)
+                            {
+                                capture_iteration(s, g, step);
+                                g.batch = this_batch;
+                            }
+                            APF_CUDA(cudaGraphLaunch(g.exec, s));
+                            g_kernel_launches.fetch_add(g.kernels);
                         }
-                        spmv(s, K, v.get(), py, 1.0, 0.0, "minres_spmv_K");
+                        else
                         {
-                            APF_KERNEL("minres_t1", s);
-                            k_t1<<<kRedBlocks, kThreads, 0, s>>>(n, py, pr1, v.get(), S.get(), first, parts.get());
+                            step();
                         }
-                        {
-                            APF_KERNEL("minres_alfa", s);
-                            k_alfa<<<1, 256, 0, s>>>(kRedBlocks, parts.get(), S.get());
-                        }
-                        {
-                            APF_KERNEL("minres_t2", s);
-                            k_t2<<<nb(n), kThreads, 0, s>>>(n, py, pr2, S.get());
-                        }
-                        // rotate: r1 <- r2, r2 <- y
-                        double* t = pr1;
-                        pr1 = pr2;
-                        pr2 = py;
-                        py = t;
-                        P.apply(s, pr2, z.get());
-                        {
-                            APF_KERNEL("minres_dot", s);
-                            k_dot_partials<<<kRedBlocks, kThreads, 0, s>>>(n, pr2, z.get(), parts.get());
-                        }
-                        {
-                            APF_KERNEL("minres_scalars", s);
-                            k_scalars<<<1, 256, 0, s>>>(kRedBlocks, parts.get(), S.get());
-                        }
-                        {
-                            APF_KERNEL("minres_w", s);
-                            k_w<<<nb(n), kThreads, 0, s>>>(n, v.get(), w1.get(), w2.get(), x, S.get());
-                        }
-                        {
-                            APF_KERNEL("minres_check", s);
-                            k_check<<<1, 1, 0, s>>>(S.get(), this_batch);
-                        }
+                        pr1 = q2;
+                        pr2 = qy;
+                        py = q1;
                         ++issued;
                     }
                     APF_CUDA(cudaMemcpyAsync(&hs, S.get(), sizeof(hs), cudaMemcpyDeviceToHost, s));
