@@ -58,6 +58,7 @@ class ProblemDesc(C.Structure):
         ("u0_kind", C.c_int),
         ("zero_tol", C.c_double),
         ("g_scale", C.c_double),
+        ("dim_space", C.c_int),
     ]
 
 

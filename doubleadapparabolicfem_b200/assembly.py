@@ -122,6 +122,7 @@ def make_desc(problem: SpaceTimeProblem, zero_tol: float, g_scale: float, keep: 
     d.u0_kind = int(problem.u0_kind)
     d.zero_tol = float(zero_tol)
     d.g_scale = float(g_scale)
+    d.dim_space = int(getattr(problem, "dim_space", 2))
     return d
 
 

@@ -22,6 +22,7 @@
 #include <type_traits>
 
 #include "apf_device.cuh"
+#include "apf_quad1d.cuh"
 #include "apf_warpsort.cuh"
 #include "apf_internal.hpp"
 #include "apf_system.hpp"
@@ -109,6 +110,7 @@ namespace apf
         struct AsmData
         {
             int p;
+            int dim; // 1: quads (geometry rows x0 x1 t0 t1, one M value per cell), 2: prisms
             const double* y_geo;
             const double* x_geo;
             const int* y_to_x;
@@ -123,9 +125,41 @@ namespace apf
             double zero_tol;
         };
 
+        // 1+1D local entry (P1 x P1 quadrilaterals, see apf_quad1d.cuh)
+        __device__ double local_entry_1d(const AsmData& d, int kind, int c, int i, int j)
+        {
+            const int s = i >> 1, a = i & 1, r = j >> 1, b = j & 1;
+            if (kind == K_AY || kind == K_AX)
+            {
+                const q1d::Quad g = q1d::load(kind == K_AY ? d.y_geo : d.x_geo, c);
+                const double* m = kind == K_AY ? d.m_y : d.m_x;
+                const double mc = m ? m[c] : 1.0;
+                return mc * (g.k / g.h) * q1d::stiff(s, r) * q1d::mass(a, b);
+            }
+            if (kind == K_C)
+            {
+                const q1d::Quad g = q1d::load(d.x_geo, c);
+                return (a == 0 && b == 0) ? -(g.h * q1d::mass(s, r)) : 0.0;
+            }
+            int ix = i, jy = j;
+            if (kind == K_BT || kind == K_BDTT)
+            {
+                ix = j;
+                jy = i;
+            }
+            const int cx = d.y_to_x[c];
+            const q1d::Quad gy = q1d::load(d.y_geo, c);
+            const q1d::Quad gx = q1d::load(d.x_geo, cx);
+            const double mc = d.m_y ? d.m_y[c] : 1.0;
+            return q1d::mixed(gy, gx, q1d::same(d.y_geo, c, d.x_geo, cx), mc, ix, jy,
+                              kind == K_BDT || kind == K_BDTT);
+        }
+
         // local entry L_c(i, j) of block `kind` on assembly cell c
         __device__ double local_entry(const AsmData& d, int kind, int c, int i, int j)
         {
+            if (d.dim == 1)
+                return local_entry_1d(d, kind, c, i, j);
             const RefTables& t = c_tab[d.p - 1];
             if (kind == K_AY || kind == K_AX)
             {
@@ -429,8 +463,30 @@ namespace apf
             double *lam_y, *trace_x;
         };
 
+        __device__ double u0_value_1d(int kind, double x)
+        {
+            if (kind == APF_U0_SIN_SIN)
+                return sinpi(x);
+            if (kind == APF_U0_ONE)
+                return 1.0;
+            return 0.0;
+        }
+
         __device__ double local_vector(const VecArgs& A, int c, int i)
         {
+            if (A.d.dim == 1)
+            {
+                if (A.which == 0)
+                {
+                    if (!A.ell)
+                        return 0.0;
+                    const q1d::Quad g = q1d::load(A.d.y_geo, c);
+                    return A.ell[c] * g.h * g.k * 0.25;
+                }
+                const int kind = A.u0_kind;
+                return q1d::initial_load(q1d::load(A.d.x_geo, c), i, A.g_scale,
+                                         [kind](double x) { return u0_value_1d(kind, x); });
+            }
             const RefTables& t = c_tab[A.d.p - 1];
             const int s = i / t.nt, a = i % t.nt;
             if (A.which == 0)
@@ -839,6 +895,7 @@ namespace apf
         {
             AsmData d{};
             d.p = in.p;
+            d.dim = in.dim;
             d.y_geo = in.y_geo.get();
             d.x_geo = in.x_geo.get();
             d.y_to_x = in.y_to_x.get();
@@ -1166,22 +1223,23 @@ namespace apf
     // M per X cell, taken from the Y cells it contains (M is cell-constant).
     namespace
     {
-        __global__ void scatter_m_to_x(int ny, const int* __restrict__ y_to_x, const double* __restrict__ m_y,
+        // mw values of M per cell (3 in 2+1D: m00 m01 m11; 1 in 1+1D)
+        __global__ void scatter_m_to_x(int ny, int mw, const int* __restrict__ y_to_x, const double* __restrict__ m_y,
                                        double* __restrict__ m_x)
         {
             for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ny; c += gridDim.x * blockDim.x)
             {
                 const int x = y_to_x[c];
-                m_x[3ll * x + 0] = m_y[3ll * c + 0];
-                m_x[3ll * x + 1] = m_y[3ll * c + 1];
-                m_x[3ll * x + 2] = m_y[3ll * c + 2];
+                for (int k = 0; k < mw; ++k)
+                    m_x[(long long)mw * x + k] = m_y[(long long)mw * c + k];
             }
         }
 
-        __global__ void mark_bottom(int nx, const double* __restrict__ x_geo, int* __restrict__ flag)
+        // gw doubles per geometry row; t0 at offset gw - 2
+        __global__ void mark_bottom(int nx, int gw, const double* __restrict__ x_geo, int* __restrict__ flag)
         {
             for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nx; c += gridDim.x * blockDim.x)
-                flag[c] = x_geo[8ll * c + 6] == 0.0 ? 1 : 0;
+                flag[c] = x_geo[(long long)gw * c + gw - 2] == 0.0 ? 1 : 0;
         }
 
         __global__ void compact_flags(int n, const int* __restrict__ flag, const int* __restrict__ pos,
@@ -1208,14 +1266,14 @@ namespace apf
     {
         // time coordinate of every true DOF named by a restriction row, quantized to 2^-20
         // (dyadic mesh times are exact): DOFs on one time level share a component
-        __global__ void dof_time_component(int rows, int ndof, int p, const double* __restrict__ geo,
+        __global__ void dof_time_component(int rows, int ndof, int p, int gw, const double* __restrict__ geo,
                                            const int* __restrict__ off, const int* __restrict__ dofs,
                                            int* __restrict__ comp)
         {
             for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
             {
                 const int c = r / ndof, a = (r % ndof) % (p + 1);
-                const double t0 = geo[8ll * c + 6], t1 = geo[8ll * c + 7];
+                const double t0 = geo[(long long)gw * c + gw - 2], t1 = geo[(long long)gw * c + gw - 1];
                 const int level = static_cast<int>(llround((t0 + (t1 - t0) * a / p) * 1048576.0));
                 for (int e = off[r]; e < off[r + 1]; ++e)
                     comp[dofs[e]] = level;
@@ -1233,7 +1291,8 @@ namespace apf
         {
             APF_KERNEL("dof_time_component", s);
             dof_time_component<<<grid_for(rows, 256), 256, 0, s>>>(
-                rows, in.ndof, in.p, y_space ? in.y_geo.get() : in.x_geo.get(), y_space ? in.y_off.get() : in.x_off.get(),
+                rows, in.ndof, in.p, in.dim == 1 ? 4 : 8, y_space ? in.y_geo.get() : in.x_geo.get(),
+                y_space ? in.y_off.get() : in.x_off.get(),
                 y_space ? in.y_dofs.get() : in.x_dofs.get(), comp.get());
         }
         APF_CUDA(cudaGetLastError());
@@ -1242,20 +1301,27 @@ namespace apf
     void prepare_inputs(cudaStream_t s, SystemInputs& in)
     {
         // M on X cells
+        const int mw = in.dim == 1 ? 1 : 3, gw = in.dim == 1 ? 4 : 8;
         if (in.m_y.size())
         {
-            in.m_x.allocate(static_cast<std::size_t>(in.n_x_cells) * 3, s);
+            in.m_x.allocate(static_cast<std::size_t>(in.n_x_cells) * mw, s);
             std::vector<double> ident;
             // default identity for X cells not covered (should not happen for a valid Y/X pair)
-            ident.resize(static_cast<std::size_t>(in.n_x_cells) * 3);
+            ident.resize(static_cast<std::size_t>(in.n_x_cells) * mw);
             for (int c = 0; c < in.n_x_cells; ++c)
             {
-                ident[3 * c] = 1.0; ident[3 * c + 1] = 0.0; ident[3 * c + 2] = 1.0;
+                if (mw == 1)
+                    ident[c] = 1.0;
+                else
+                {
+                    ident[3 * c] = 1.0; ident[3 * c + 1] = 0.0; ident[3 * c + 2] = 1.0;
+                }
             }
             APF_CUDA(cudaMemcpyAsync(in.m_x.get(), ident.data(), ident.size() * sizeof(double), cudaMemcpyHostToDevice, s));
             {
                 APF_KERNEL("scatter_m_to_x", s);
-                scatter_m_to_x<<<grid_for(in.n_y_cells, 256), 256, 0, s>>>(in.n_y_cells, in.y_to_x.get(), in.m_y.get(), in.m_x.get());
+                scatter_m_to_x<<<grid_for(in.n_y_cells, 256), 256, 0, s>>>(in.n_y_cells, mw, in.y_to_x.get(), in.m_y.get(),
+                                                                           in.m_x.get());
             }
             APF_CUDA(cudaGetLastError());
             sync(s);
@@ -1267,7 +1333,7 @@ namespace apf
         {
             {
                 APF_KERNEL("mark_bottom", s);
-                mark_bottom<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, in.x_geo.get(), flag.get());
+                mark_bottom<<<grid_for(in.n_x_cells, 256), 256, 0, s>>>(in.n_x_cells, gw, in.x_geo.get(), flag.get());
             }
         }
         const long long nb = exclusive_scan(flag.get(), pos.get(), in.n_x_cells, s);
@@ -1378,6 +1444,49 @@ namespace apf
             }
         }
 
+        // 1+1D: lambda_y^2_K = m (k / h) sum_ij D_sr Mt_ab lambda_i lambda_j
+        __global__ void lambda_energy_1d_kernel(XIndArgs A)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n_y; c += gridDim.x * blockDim.x)
+            {
+                double lam[4];
+                for (int i = 0; i < 4; ++i)
+                    lam[i] = local_value(A.y_off, A.y_dofs, A.y_w, A.lambda, 4ll * c + i);
+                const q1d::Quad g = q1d::load(A.y_geo, c);
+                const double m = A.m_y ? A.m_y[c] : 1.0;
+                double e = 0.0;
+                for (int i = 0; i < 4; ++i)
+                {
+                    double row = 0.0;
+                    for (int j = 0; j < 4; ++j)
+                        row += q1d::stiff(i >> 1, j >> 1) * q1d::mass(i & 1, j & 1) * lam[j];
+                    e += lam[i] * row;
+                }
+                A.lam_y[c] = m * (g.k / g.h) * e;
+            }
+        }
+
+        // 1+1D: ||u0 - u_delta(., 0)||^2 on the bottom edge, 3-point Gauss rule
+        __global__ void initial_trace_1d_kernel(XIndArgs A)
+        {
+            for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < A.n_bottom; k += gridDim.x * blockDim.x)
+            {
+                const int c = A.bottom[k];
+                const double u0l = local_value(A.x_off, A.x_dofs, A.x_w, A.u, 4ll * c + 0);
+                const double u0r = local_value(A.x_off, A.x_dofs, A.x_w, A.u, 4ll * c + 2);
+                const q1d::Quad g = q1d::load(A.x_geo, c);
+                double acc = 0.0;
+                for (int q = 0; q < 3; ++q)
+                {
+                    const double xi = q1d::gauss_x(q);
+                    const double uh = u0l * (1.0 - xi) + u0r * xi;
+                    const double d = u0_value_1d(A.u0_kind, g.x0 + g.h * xi) - uh;
+                    acc += d * d * g.h * q1d::gauss_w(q);
+                }
+                A.trace_x[c] = acc;
+            }
+        }
+
         __global__ void child_count_kernel(int n_y, const int* __restrict__ y_to_x, int* __restrict__ cnt)
         {
             for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_y; c += gridDim.x * blockDim.x)
@@ -1438,7 +1547,10 @@ namespace apf
         if (in.n_y_cells > 0)
         {
             APF_KERNEL("y_cell_energy", s);
-            lambda_energy_kernel<<<grid_for(in.n_y_cells, 128), 128, 0, s>>>(a);
+            if (in.dim == 1)
+                lambda_energy_1d_kernel<<<grid_for(in.n_y_cells, 128), 128, 0, s>>>(a);
+            else
+                lambda_energy_kernel<<<grid_for(in.n_y_cells, 128), 128, 0, s>>>(a);
         }
         APF_CUDA(cudaGetLastError());
     }
@@ -1471,12 +1583,18 @@ namespace apf
         if (in.n_y_cells > 0)
         {
             APF_KERNEL("xind_lambda_energy", s);
-            lambda_energy_kernel<<<grid_for(in.n_y_cells, 128), 128, 0, s>>>(a);
+            if (in.dim == 1)
+                lambda_energy_1d_kernel<<<grid_for(in.n_y_cells, 128), 128, 0, s>>>(a);
+            else
+                lambda_energy_kernel<<<grid_for(in.n_y_cells, 128), 128, 0, s>>>(a);
         }
         if (in.n_bottom > 0)
         {
             APF_KERNEL("xind_initial_trace", s);
-            initial_trace_kernel<<<grid_for(in.n_bottom, 128), 128, 0, s>>>(a);
+            if (in.dim == 1)
+                initial_trace_1d_kernel<<<grid_for(in.n_bottom, 128), 128, 0, s>>>(a);
+            else
+                initial_trace_kernel<<<grid_for(in.n_bottom, 128), 128, 0, s>>>(a);
         }
         DeviceBuffer<int> cnt(static_cast<std::size_t>(in.n_x_cells) + 1, s), ptr(static_cast<std::size_t>(in.n_x_cells) + 1, s),
             cursor(static_cast<std::size_t>(in.n_x_cells) + 1, s), child(static_cast<std::size_t>(std::max(in.n_y_cells, 1)), s);

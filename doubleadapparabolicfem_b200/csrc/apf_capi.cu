@@ -341,7 +341,10 @@ int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs
     const int rc = guarded(ctx, [&] {
         APF_HOST_RANGE("call_assemble_main_system");
         ensure_pool(ctx);
-        apf::require(d->p == 1 || d->p == 2, APF_ERR_INVALID, "p must be 1 or 2");
+        const int dim = d->dim_space == 0 ? 2 : d->dim_space;
+        apf::require(dim == 1 || dim == 2, APF_ERR_INVALID, "dim_space must be 1 or 2");
+        apf::require(d->p == 1 || (d->p == 2 && dim == 2), APF_ERR_INVALID,
+                     "p must be 1 or 2 (2+1D) or 1 (1+1D)");
         apf::require(d->n_y_cells >= 0 && d->n_x_cells >= 0 && d->n_lambda >= 0 && d->n_u >= 0, APF_ERR_INVALID,
                      "negative sizes");
         apf::require(d->u0_kind >= 0 && d->u0_kind <= 2, APF_ERR_INVALID, "unknown u0_kind");
@@ -349,7 +352,8 @@ int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs
         S.stream = ctx->stream;
         auto& in = S.in;
         in.p = d->p;
-        in.ndof = (d->p + 1) * (d->p + 2) / 2 * (d->p + 1);
+        in.dim = dim;
+        in.ndof = dim == 1 ? (d->p + 1) * (d->p + 1) : (d->p + 1) * (d->p + 2) / 2 * (d->p + 1);
         in.n_y_cells = d->n_y_cells;
         in.n_x_cells = d->n_x_cells;
         in.n_lambda = d->n_lambda;
@@ -360,8 +364,9 @@ int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs
         const bool dev = inputs_on_device != 0;
         cudaStream_t s = ctx->stream;
         const std::size_t ny = static_cast<std::size_t>(d->n_y_cells), nx = static_cast<std::size_t>(d->n_x_cells);
-        stage(in.y_geo, d->y_geometry, ny * 8, dev, s);
-        stage(in.x_geo, d->x_geometry, nx * 8, dev, s);
+        const std::size_t gw = dim == 1 ? 4 : 8, mw = dim == 1 ? 1 : 3;
+        stage(in.y_geo, d->y_geometry, ny * gw, dev, s);
+        stage(in.x_geo, d->x_geometry, nx * gw, dev, s);
         stage(in.y_to_x, d->y_to_x, ny, dev, s);
         stage(in.y_off, d->y_restr_offsets, ny * in.ndof + 1, dev, s);
         stage(in.y_dofs, d->y_restr_dofs, static_cast<std::size_t>(d->y_restr_nnz), dev, s);
@@ -370,7 +375,7 @@ int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs
         stage(in.x_dofs, d->x_restr_dofs, static_cast<std::size_t>(d->x_restr_nnz), dev, s);
         stage(in.x_w, d->x_restr_weights, static_cast<std::size_t>(d->x_restr_nnz), dev, s);
         if (d->m_cells)
-            stage(in.m_y, d->m_cells, ny * 3, dev, s);
+            stage(in.m_y, d->m_cells, ny * mw, dev, s);
         if (d->ell_cells)
             stage(in.ell, d->ell_cells, ny, dev, s);
         apf::assemble_main(S);
@@ -643,19 +648,29 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
                  double* flux_squared, double* divergence_squared, double* reconstruction_squared, double* eta_squared,
                  apf_estimator_result* result)
 {
-    if (!ctx || !sys || !y_vertex_ids)
+    if (!ctx || !sys || (!y_vertex_ids && sys->sys.in.dim != 1))
         return APF_ERR_INVALID;
     return guarded(ctx, [&] {
         APF_HOST_RANGE("call_estimate");
         auto& S = sys->sys;
-        const std::size_t n = 3ull * static_cast<std::size_t>(S.in.n_y_cells);
-        std::vector<int> vids(n);
-        if (n)
-            APF_CUDA(cudaMemcpyAsync(vids.data(), y_vertex_ids, n * sizeof(int),
-                                     pointers_on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, ctx->stream));
-        apf::sync(ctx->stream);
-        const apf::EstimatorTotals t = apf::estimate(ctx->stream, S, vids, flux_squared, divergence_squared,
-                                                        reconstruction_squared, eta_squared, pointers_on_device != 0);
+        apf::EstimatorTotals t;
+        if (S.in.dim == 1)
+        {
+            t = apf::estimate_1d(ctx->stream, S, flux_squared, divergence_squared, reconstruction_squared, eta_squared,
+                                 pointers_on_device != 0);
+        }
+        else
+        {
+            const std::size_t n = 3ull * static_cast<std::size_t>(S.in.n_y_cells);
+            std::vector<int> vids(n);
+            if (n)
+                APF_CUDA(cudaMemcpyAsync(vids.data(), y_vertex_ids, n * sizeof(int),
+                                         pointers_on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost,
+                                         ctx->stream));
+            apf::sync(ctx->stream);
+            t = apf::estimate(ctx->stream, S, vids, flux_squared, divergence_squared, reconstruction_squared,
+                              eta_squared, pointers_on_device != 0);
+        }
         if (result)
         {
             result->flux_squared = t.flux;

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "apf_estimator.cuh"
+#include "apf_quad1d.cuh"
 
 namespace apf
 {
@@ -1474,38 +1475,10 @@ namespace apf
         done = true;
     }
 
-    EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
-                                double* recon, double* eta, bool out_on_device)
+    void reconstruct_lambda(cudaStream_t s, System& S, DeviceBuffer<double>& lt, EstimatorTotals& tot)
     {
-        SystemInputs& in = S.in;
-        require(in.p == 1 || in.p == 2, APF_ERR_INVALID, "estimator: p must be 1 or 2");
-        require(S.solution.size() == static_cast<std::size_t>(in.n_lambda + in.n_u), APF_ERR_INVALID,
-                "estimator: solve the main system first");
-        require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
-        require(in.n_x_cells == in.n_y_cells, APF_ERR_INVALID, "estimator: Y cells must coincide with X cells");
-        upload_est_tables_once();
-        EstimatorTotals tot{};
-        const int ny = in.n_y_cells, nl = in.n_lambda;
-        // ---- patch topology: host integer work on the cells' time intervals and vertex ids,
-        // run on a host thread while the device solves the slab reconstruction
-        std::vector<double> times(2ll * ny);
-        {
-            DeviceBuffer<double> dt(2ll * ny, s);
-            if (ny)
-            {
-                APF_KERNEL("est_cell_times", s);
-                cell_times_kernel<<<nb(ny), 256, 0, s>>>(ny, in.y_geo.get(), dt.get());
-                APF_CUDA(cudaMemcpyAsync(times.data(), dt.get(), times.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-            }
-            sync(s);
-        }
-        std::future<PatchSet> patches = std::async(std::launch::async, [&times, &vids_host, ny]() {
-            PatchSet ps;
-            build_patches(times, vids_host, ny, ps);
-            return ps;
-        });
-        // ---- lambda~ : A_y lambda~ = f - B^T u (PCG with the A_y AMG, start lambda_delta)
-        DeviceBuffer<double> rhs(nl, s), lt(nl, s), r(nl, s), z(nl, s), pv(nl, s), q(nl, s);
+        const int nl = S.in.n_lambda;
+        DeviceBuffer<double> rhs(nl, s), r(nl, s), z(nl, s), pv(nl, s), q(nl, s);
         copy(s, nl, S.f.get(), rhs.get());
         spmv(s, S.blocks[APF_BLOCK_BT], S.solution.get() + nl, rhs.get(), -1.0, 1.0);
         copy(s, nl, S.solution.get(), lt.get());
@@ -1537,6 +1510,41 @@ namespace apf
         }
         tot.recon_iterations = its;
         tot.recon_residual = bn > 0.0 ? rn / bn : 0.0;
+    }
+
+    EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
+                                double* recon, double* eta, bool out_on_device)
+    {
+        SystemInputs& in = S.in;
+        require(in.p == 1 || in.p == 2, APF_ERR_INVALID, "estimator: p must be 1 or 2");
+        require(S.solution.size() == static_cast<std::size_t>(in.n_lambda + in.n_u), APF_ERR_INVALID,
+                "estimator: solve the main system first");
+        require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
+        require(in.n_x_cells == in.n_y_cells, APF_ERR_INVALID, "estimator: Y cells must coincide with X cells");
+        upload_est_tables_once();
+        EstimatorTotals tot{};
+        const int ny = in.n_y_cells, nl = in.n_lambda;
+        // ---- patch topology: host integer work on the cells' time intervals and vertex ids,
+        // run on a host thread while the device solves the slab reconstruction
+        std::vector<double> times(2ll * ny);
+        {
+            DeviceBuffer<double> dt(2ll * ny, s);
+            if (ny)
+            {
+                APF_KERNEL("est_cell_times", s);
+                cell_times_kernel<<<nb(ny), 256, 0, s>>>(ny, in.y_geo.get(), dt.get());
+                APF_CUDA(cudaMemcpyAsync(times.data(), dt.get(), times.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+            }
+            sync(s);
+        }
+        std::future<PatchSet> patches = std::async(std::launch::async, [&times, &vids_host, ny]() {
+            PatchSet ps;
+            build_patches(times, vids_host, ny, ps);
+            return ps;
+        });
+        // ---- lambda~ : A_y lambda~ = f - B^T u
+        DeviceBuffer<double> lt(nl, s);
+        reconstruct_lambda(s, S, lt, tot);
         PatchSet ps = patches.get();
         // ---- nodal data per cell
         const int nd = in.ndof;
@@ -1707,6 +1715,427 @@ namespace apf
         {
             APF_KERNEL("est_cell_indicators", s);
             cell_indicators<<<nb(ny, 128), 128, 0, s>>>(ia);
+        }
+        APF_CUDA(cudaGetLastError());
+        tot.flux = device_sum(s, ny, f2.get());
+        tot.div = device_sum(s, ny, d2.get());
+        tot.recon = device_sum(s, ny, r2.get());
+        tot.eta = device_sum(s, ny, e2.get());
+        const cudaMemcpyKind kind = out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (flux) APF_CUDA(cudaMemcpyAsync(flux, f2.get(), ny * sizeof(double), kind, s));
+        if (div) APF_CUDA(cudaMemcpyAsync(div, d2.get(), ny * sizeof(double), kind, s));
+        if (recon) APF_CUDA(cudaMemcpyAsync(recon, r2.get(), ny * sizeof(double), kind, s));
+        if (eta) APF_CUDA(cudaMemcpyAsync(eta, e2.get(), ny * sizeof(double), kind, s));
+        sync(s);
+        return tot;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// 1+1D (P1) edge-patch estimator.
+//
+// Restates TimeSlabEquilibratedFluxReconstruction1plus1d
+// (src/finite_element/time_slabs/time_slab_equilibrated_flux_reconstruction.hpp:773-1880)
+// and compute_equilibrated_flux_error_squared_by_source_cell_1plus1d
+// (time_slab_equilibrated_flux_indicators.hpp:23-190):
+//   * patches (time_slab_edge_patch_builder.hpp:353-537): per time slab, its cells sorted
+//     by x; one boundary patch at each end (one cell) and one interior patch per shared
+//     spatial vertex (left cell, right cell);
+//   * flux space (patch_flux_space_1d.hpp): spatial functions {hat of the patch vertex,
+//     x(1-x) bubble of every patch cell} x shifted Legendre {1, 2 tau - 1} in time, index
+//     = i_space * 2 + i_time; scalar space (patch_scalar_space.hpp): boundary patch
+//     {1, 2 x - 1}, interior patch {2 x - 1 on the left cell, 2 x - 1 on the right cell,
+//     the weighted Haar function (h_R, -h_L) / (h_L + h_R)}, same time functions;
+//   * local forms on 3 x 3 Gauss points of every patch cell (local_error_bilinear_forms.hpp,
+//     local_error_linear_forms.hpp): A = (M^-1 sigma_j, sigma_i), B = (div sigma_j, q_i),
+//     f = -(psi_a d_x theta~, sigma_i), g = (psi_a (l - d_t u) - d_x psi_a M d_x theta~, q_i),
+//     entries of A and B with |a| <= zero_tol dropped (mat_A_1d.hpp, mat_B_1d.hpp), C = 0
+//     (mat_C_1d.hpp); [A B^T; B 0] solved exactly (partial-pivot LU), one thread per patch;
+//   * indicators per Y cell on 3 x 3 Gauss points: flux^2 = ((sigma + M d_x theta~)^2 / M),
+//     div^2 = (l - d_t u - d_x sigma)^2, plus the reconstruction energy of lambda_delta -
+//     lambda~ (time_slab_error_norms.hpp:946).
+// ---------------------------------------------------------------------------------------
+namespace apf
+{
+    namespace
+    {
+        constexpr int kEdgeMax = 12; // interior patch: 6 flux + 6 scalar unknowns
+
+        struct EdgeArgs
+        {
+            int n_patches;
+            const int* left;  // [patch] cell left of the patch vertex or -1
+            const int* right; // [patch] cell right of the patch vertex or -1
+            const double* geo;
+            const double* m;
+            const double* ell;
+            const double* lt; // [cell][4] lambda~ nodal values
+            const double* u;  // [cell][4] u_delta nodal values
+            double zero_tol;
+            double* sigma;    // [cell][2 slots][4]: hat L0, hat L1, bubble L0, bubble L1
+            int* status;
+        };
+
+        __device__ __forceinline__ double legendre1(int k, double x) { return k ? 2.0 * x - 1.0 : 1.0; }
+
+        // d_x and d_t of a P1 x P1 nodal function at (xi, tau) of cell g
+        __device__ __forceinline__ void nodal_grad(const double* v, const q1d::Quad& g, double xi, double tau,
+                                                   double& dx, double& dt)
+        {
+            dx = ((v[2] - v[0]) * (1.0 - tau) + (v[3] - v[1]) * tau) / g.h;
+            dt = ((v[1] - v[0]) * (1.0 - xi) + (v[3] - v[2]) * xi) / g.k;
+        }
+
+        __global__ void edge_patch_solve(EdgeArgs A)
+        {
+            for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < A.n_patches; p += gridDim.x * blockDim.x)
+            {
+                const int cl = A.left[p], cr = A.right[p];
+                const bool boundary = cl < 0 || cr < 0;
+                const int nc = boundary ? 1 : 2;
+                const int nfs = 1 + nc, nss = boundary ? 2 : 3;
+                const int nf = 2 * nfs, ns = 2 * nss, n = nf + ns;
+                double K[kEdgeMax][kEdgeMax + 1];
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j <= n; ++j)
+                        K[i][j] = 0.0;
+                double hl = 0.0, hr = 0.0;
+                if (!boundary)
+                {
+                    hl = q1d::load(A.geo, cl).h;
+                    hr = q1d::load(A.geo, cr).h;
+                }
+                double Aloc[6][6], Bloc[6][6];
+                for (int i = 0; i < nf; ++i)
+                    for (int j = 0; j < nf; ++j)
+                        Aloc[i][j] = 0.0;
+                for (int i = 0; i < ns; ++i)
+                    for (int j = 0; j < nf; ++j)
+                        Bloc[i][j] = 0.0;
+                for (int pc = 0; pc < nc; ++pc)
+                {
+                    // patch cell pc: the left cell lies left of the vertex (hat = x), the
+                    // right cell right of it (hat = 1 - x)
+                    const int c = boundary ? (cl >= 0 ? cl : cr) : (pc == 0 ? cl : cr);
+                    const bool left_of_vertex = boundary ? (cl >= 0) : (pc == 0);
+                    const q1d::Quad g = q1d::load(A.geo, c);
+                    const double m = A.m ? A.m[c] : 1.0;
+                    const double ell = A.ell ? A.ell[c] : 0.0;
+                    const int bub = boundary ? 1 : (left_of_vertex ? 1 : 2);
+                    const double* lt = A.lt + 4ll * c;
+                    const double* uu = A.u + 4ll * c;
+                    const double jac = g.h * g.k;
+                    for (int qx = 0; qx < 3; ++qx)
+                    {
+                        const double xi = q1d::gauss_x(qx), wx = q1d::gauss_w(qx);
+                        const double psi = left_of_vertex ? xi : 1.0 - xi;
+                        const double dpsi = (left_of_vertex ? 1.0 : -1.0) / g.h;
+                        // spatial flux functions on this cell: hat (0) and the cell's bubble
+                        const double sv[2] = {psi, xi * (1.0 - xi)};
+                        const double sd[2] = {(left_of_vertex ? 1.0 : -1.0) / g.h, (1.0 - 2.0 * xi) / g.h};
+                        const int sidx[2] = {0, bub};
+                        // spatial scalar functions (value at xi, index)
+                        double qv[3];
+                        int qn = 0;
+                        int qidx[3];
+                        if (boundary)
+                        {
+                            qv[0] = 1.0; qidx[0] = 0;
+                            qv[1] = 2.0 * xi - 1.0; qidx[1] = 1;
+                            qn = 2;
+                        }
+                        else
+                        {
+                            qv[0] = 2.0 * xi - 1.0; qidx[0] = left_of_vertex ? 0 : 1;
+                            qv[1] = left_of_vertex ? hr / (hl + hr) : -hl / (hl + hr); qidx[1] = 2;
+                            qn = 2;
+                        }
+                        for (int qt = 0; qt < 3; ++qt)
+                        {
+                            const double tau = q1d::gauss_x(qt), w = wx * q1d::gauss_w(qt) * jac;
+                            const double T[2] = {1.0, 2.0 * tau - 1.0};
+                            double dlx, dlt, dux, dut;
+                            nodal_grad(lt, g, xi, tau, dlx, dlt);
+                            nodal_grad(uu, g, xi, tau, dux, dut);
+                            const double gth = dlx + dux;
+                            const double frhs = -psi * gth * w;
+                            const double grhs = (psi * (ell - dut) - dpsi * m * gth) * w;
+                            for (int a = 0; a < 2; ++a)
+                                for (int ka = 0; ka < 2; ++ka)
+                                {
+                                    const int i = sidx[a] * 2 + ka;
+                                    const double si = sv[a] * T[ka];
+                                    K[i][n] += frhs * si;
+                                    for (int b = 0; b < 2; ++b)
+                                        for (int kb = 0; kb < 2; ++kb)
+                                            Aloc[i][sidx[b] * 2 + kb] += si * sv[b] * T[kb] / m * w;
+                                }
+                            for (int a = 0; a < qn; ++a)
+                                for (int ka = 0; ka < 2; ++ka)
+                                {
+                                    const int i = qidx[a] * 2 + ka;
+                                    const double qi = qv[a] * T[ka];
+                                    K[nf + i][n] += grhs * qi;
+                                    for (int b = 0; b < 2; ++b)
+                                        for (int kb = 0; kb < 2; ++kb)
+                                            Bloc[i][sidx[b] * 2 + kb] += qi * sd[b] * T[kb] * w;
+                                }
+                        }
+                    }
+                }
+                for (int i = 0; i < nf; ++i)
+                    for (int j = 0; j < nf; ++j)
+                        K[i][j] = fabs(Aloc[i][j]) > A.zero_tol ? Aloc[i][j] : 0.0;
+                for (int i = 0; i < ns; ++i)
+                    for (int j = 0; j < nf; ++j)
+                    {
+                        const double v = fabs(Bloc[i][j]) > A.zero_tol ? Bloc[i][j] : 0.0;
+                        K[nf + i][j] = v;
+                        K[j][nf + i] = v;
+                    }
+                // partial-pivot elimination on the augmented n x (n + 1) system
+                bool singular = false;
+                for (int col = 0; col < n; ++col)
+                {
+                    int piv = col;
+                    double best = fabs(K[col][col]);
+                    for (int i = col + 1; i < n; ++i)
+                        if (fabs(K[i][col]) > best)
+                        {
+                            best = fabs(K[i][col]);
+                            piv = i;
+                        }
+                    if (!(best > 0.0) || !isfinite(best))
+                    {
+                        singular = true;
+                        break;
+                    }
+                    if (piv != col)
+                        for (int j = col; j <= n; ++j)
+                        {
+                            const double t = K[col][j];
+                            K[col][j] = K[piv][j];
+                            K[piv][j] = t;
+                        }
+                    const double inv = 1.0 / K[col][col];
+                    for (int i = col + 1; i < n; ++i)
+                    {
+                        const double l = K[i][col] * inv;
+                        if (l != 0.0)
+                            for (int j = col + 1; j <= n; ++j)
+                                K[i][j] -= l * K[col][j];
+                    }
+                }
+                if (singular)
+                {
+                    atomicExch(A.status, APF_ERR_NUMERIC);
+                    continue;
+                }
+                double x[kEdgeMax];
+                for (int i = n - 1; i >= 0; --i)
+                {
+                    double v = K[i][n];
+                    for (int j = i + 1; j < n; ++j)
+                        v -= K[i][j] * x[j];
+                    x[i] = v / K[i][i];
+                }
+                // this patch's flux on each of its cells -> the cell's slot of the vertex
+                for (int pc = 0; pc < nc; ++pc)
+                {
+                    const int c = boundary ? (cl >= 0 ? cl : cr) : (pc == 0 ? cl : cr);
+                    const bool left_of_vertex = boundary ? (cl >= 0) : (pc == 0);
+                    const int bub = boundary ? 1 : (left_of_vertex ? 1 : 2);
+                    // slot 0: the patch at the cell's left vertex (cell right of it), 1: right
+                    double* out = A.sigma + 8ll * c + (left_of_vertex ? 4 : 0);
+                    out[0] = x[0];
+                    out[1] = x[1];
+                    out[2] = x[2 * bub];
+                    out[3] = x[2 * bub + 1];
+                }
+            }
+        }
+
+        struct EdgeIndArgs
+        {
+            int n_cells;
+            const double* geo;
+            const double* m;
+            const double* ell;
+            const double* lt;
+            const double* u;
+            const double* sigma;
+            double* flux;
+            double* div;
+        };
+
+        __global__ void edge_cell_indicators(EdgeIndArgs A)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n_cells; c += gridDim.x * blockDim.x)
+            {
+                const q1d::Quad g = q1d::load(A.geo, c);
+                const double m = A.m ? A.m[c] : 1.0;
+                const double ell = A.ell ? A.ell[c] : 0.0;
+                const double* sg = A.sigma + 8ll * c;
+                const double* lt = A.lt + 4ll * c;
+                const double* uu = A.u + 4ll * c;
+                double fl = 0.0, dv = 0.0;
+                for (int qx = 0; qx < 3; ++qx)
+                {
+                    const double xi = q1d::gauss_x(qx);
+                    for (int qt = 0; qt < 3; ++qt)
+                    {
+                        const double tau = q1d::gauss_x(qt);
+                        const double w = q1d::gauss_w(qx) * q1d::gauss_w(qt) * g.h * g.k;
+                        const double L1 = 2.0 * tau - 1.0, bub = xi * (1.0 - xi);
+                        double sigma = 0.0, dsig = 0.0;
+                        for (int slot = 0; slot < 2; ++slot)
+                        {
+                            const double* q = sg + 4 * slot;
+                            const double hat = slot == 0 ? 1.0 - xi : xi;
+                            const double dhat = (slot == 0 ? -1.0 : 1.0) / g.h;
+                            const double th = q[0] + q[1] * L1, tb = q[2] + q[3] * L1;
+                            sigma += th * hat + tb * bub;
+                            dsig += th * dhat + tb * (1.0 - 2.0 * xi) / g.h;
+                        }
+                        double dlx, dlt, dux, dut;
+                        nodal_grad(lt, g, xi, tau, dlx, dlt);
+                        nodal_grad(uu, g, xi, tau, dux, dut);
+                        const double e = sigma + m * (dlx + dux);
+                        fl += e * e / m * w;
+                        const double r = ell - dut - dsig;
+                        dv += r * r * w;
+                    }
+                }
+                A.flux[c] = fl;
+                A.div[c] = dv;
+            }
+        }
+    }
+
+    EstimatorTotals estimate_1d(cudaStream_t s, System& S, double* flux, double* div, double* recon, double* eta,
+                                bool out_on_device)
+    {
+        SystemInputs& in = S.in;
+        require(in.dim == 1 && in.p == 1, APF_ERR_INVALID, "1+1D estimator: P1 only");
+        require(S.solution.size() == static_cast<std::size_t>(in.n_lambda + in.n_u), APF_ERR_INVALID,
+                "estimator: solve the main system first");
+        require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
+        require(in.n_x_cells == in.n_y_cells, APF_ERR_INVALID, "estimator: Y cells must coincide with X cells");
+        EstimatorTotals tot{};
+        const int ny = in.n_y_cells, nl = in.n_lambda;
+        // ---- edge patches: host integer work on the cells' intervals
+        std::vector<double> geo(4ll * ny);
+        if (ny)
+            APF_CUDA(cudaMemcpyAsync(geo.data(), in.y_geo.get(), geo.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        std::vector<int> order(ny);
+        for (int c = 0; c < ny; ++c)
+            order[c] = c;
+        // slabs = distinct time intervals (in time order), cells of a slab by x
+        std::sort(order.begin(), order.end(), [&](int a, int b) {
+            const double* ga = &geo[4ll * a];
+            const double* gb = &geo[4ll * b];
+            if (ga[2] != gb[2]) return ga[2] < gb[2];
+            if (ga[3] != gb[3]) return ga[3] < gb[3];
+            if (ga[0] != gb[0]) return ga[0] < gb[0];
+            if (ga[1] != gb[1]) return ga[1] < gb[1];
+            return a < b;
+        });
+        std::vector<int> left, right;
+        left.reserve(static_cast<std::size_t>(ny) + 64);
+        right.reserve(static_cast<std::size_t>(ny) + 64);
+        int n_slabs = 0;
+        for (int b = 0; b < ny;)
+        {
+            int e = b + 1;
+            while (e < ny && geo[4ll * order[e] + 2] == geo[4ll * order[b] + 2] &&
+                   geo[4ll * order[e] + 3] == geo[4ll * order[b] + 3])
+                ++e;
+            ++n_slabs;
+            left.push_back(-1);
+            right.push_back(order[b]);
+            for (int i = b; i + 1 < e; ++i)
+            {
+                require(std::fabs(geo[4ll * order[i] + 1] - geo[4ll * order[i + 1]]) <= 1e-12, APF_ERR_INVALID,
+                        "1+1D estimator: adjacent slab cells are not spatially contiguous");
+                left.push_back(order[i]);
+                right.push_back(order[i + 1]);
+            }
+            left.push_back(order[e - 1]);
+            right.push_back(-1);
+            b = e;
+        }
+        const int np = static_cast<int>(left.size());
+        tot.n_slabs = n_slabs;
+        tot.n_patches = np;
+        tot.max_patch_cells = ny > 1 ? 2 : 1;
+        // ---- lambda~
+        DeviceBuffer<double> lt(nl, s);
+        reconstruct_lambda(s, S, lt, tot);
+        // ---- nodal data per cell
+        DeviceBuffer<double> ltil(4ll * ny, s), ucell(4ll * ny, s);
+        {
+            APF_KERNEL("est_gather_nodal", s);
+            gather_nodal<<<nb(4ll * ny), 256, 0, s>>>(ny, 4, in.y_off.get(), in.y_dofs.get(), in.y_w.get(), lt.get(),
+                                                     nullptr, ltil.get());
+        }
+        {
+            APF_KERNEL("est_gather_nodal", s);
+            gather_nodal<<<nb(4ll * ny), 256, 0, s>>>(ny, 4, in.x_off.get(), in.x_dofs.get(), in.x_w.get(),
+                                                     S.solution.get() + nl, nullptr, ucell.get());
+        }
+        DeviceBuffer<int> d_left(0, s), d_right(0, s), status(1, s);
+        d_left.upload(left.data(), left.size());
+        d_right.upload(right.data(), right.size());
+        status.zero();
+        DeviceBuffer<double> sigma(8ll * ny, s);
+        sigma.zero();
+        EdgeArgs ea{};
+        ea.n_patches = np;
+        ea.left = d_left.get();
+        ea.right = d_right.get();
+        ea.geo = in.y_geo.get();
+        ea.m = in.m_y.size() ? in.m_y.get() : nullptr;
+        ea.ell = in.ell.size() ? in.ell.get() : nullptr;
+        ea.lt = ltil.get();
+        ea.u = ucell.get();
+        ea.zero_tol = in.zero_tol;
+        ea.sigma = sigma.get();
+        ea.status = status.get();
+        if (np > 0)
+        {
+            APF_KERNEL("est_edge_patch_solve", s);
+            edge_patch_solve<<<nb(np, 64), 64, 0, s>>>(ea);
+        }
+        APF_CUDA(cudaGetLastError());
+        int hstat = 0;
+        APF_CUDA(cudaMemcpyAsync(&hstat, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        require(hstat == 0, APF_ERR_NUMERIC, "1+1D estimator: singular patch system");
+        DeviceBuffer<double> f2(ny, s), d2(ny, s), r2(ny, s), e2(ny, s);
+        EdgeIndArgs ia{};
+        ia.n_cells = ny;
+        ia.geo = in.y_geo.get();
+        ia.m = ea.m;
+        ia.ell = ea.ell;
+        ia.lt = ltil.get();
+        ia.u = ucell.get();
+        ia.sigma = sigma.get();
+        ia.flux = f2.get();
+        ia.div = d2.get();
+        if (ny > 0)
+        {
+            APF_KERNEL("est_cell_indicators", s);
+            edge_cell_indicators<<<nb(ny, 128), 128, 0, s>>>(ia);
+        }
+        DeviceBuffer<double> dl(nl, s);
+        copy(s, nl, S.solution.get(), dl.get());
+        axpby(s, nl, -1.0, lt.get(), 1.0, dl.get());
+        y_cell_energy(s, in, dl.get(), r2.get());
+        if (ny > 0)
+        {
+            APF_KERNEL("est_eta", s);
+            add_kernel<<<nb(ny), 256, 0, s>>>(ny, f2.get(), r2.get(), e2.get());
         }
         APF_CUDA(cudaGetLastError());
         tot.flux = device_sum(s, ny, f2.get());

@@ -38,4 +38,12 @@ namespace apf
 
     EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
                                 double* recon, double* eta, bool out_on_device);
+
+    // lambda~ of the slab reconstruction: A_y lambda~ = f - B^T u by PCG with the A_y
+    // V-cycle from lambda_delta (relative residual 1e-14, at most 400 iterations)
+    void reconstruct_lambda(cudaStream_t s, System& S, DeviceBuffer<double>& lt, EstimatorTotals& tot);
+
+    // 1+1D (P1) edge-patch estimator
+    EstimatorTotals estimate_1d(cudaStream_t s, System& S, double* flux, double* div, double* recon, double* eta,
+                                bool out_on_device);
 }

@@ -32,6 +32,7 @@ namespace apf
     struct SystemInputs
     {
         int p = 1, ndof = 6;
+        int dim = 2; // space dimension: 2 (prisms, geometry rows of 8) or 1 (quads, rows of 4)
         int n_y_cells = 0, n_x_cells = 0, n_lambda = 0, n_u = 0;
         DeviceBuffer<double> y_geo, x_geo;
         DeviceBuffer<int> y_to_x;

@@ -1,4 +1,4 @@
-"""Host-side mirror of the reference's estimator entry points (p = 1).
+"""Host-side mirror of the reference's estimator entry points (2+1D: p = 1, 2; 1+1D: p = 1).
 
 ``estimate(blocks)`` runs, on the solution of the last
 ``solver.solve_saddle_system_with_preconditioner`` call, what one inner iteration of
@@ -15,6 +15,12 @@ main solve:
   (time_slab_error_norms.hpp:946) and eta^2 = flux^2 + reconstruction^2
   (time_slab_estimator_combination.hpp).
 
+For 1+1D problems (``dim_space == 1``) the patches are the reference's edge patches
+(``TimeSlabEquilibratedFluxReconstruction1plus1d``,
+time_slab_equilibrated_flux_reconstruction.hpp:773) and the indicators those of
+``compute_equilibrated_flux_error_squared_by_source_cell_1plus1d``
+(time_slab_equilibrated_flux_indicators.hpp:23); no vertex ids are needed.
+
 Per-cell results are numpy arrays over the Y cells in input order.
 """
 from __future__ import annotations
@@ -28,15 +34,19 @@ from .assembly import MainSystemBlocks, _ptr
 
 
 def estimate(blocks: MainSystemBlocks, y_vertex_ids: np.ndarray | None = None):
-    vids = y_vertex_ids if y_vertex_ids is not None else blocks.problem.y_vertex_ids
-    if vids is None:
-        raise ValueError("the estimator needs the spatial vertex ids of the Y cells")
-    vids = np.ascontiguousarray(vids, dtype=np.int32)
+    if getattr(blocks.problem, "dim_space", 2) == 1:
+        vids = None  # 1+1D edge patches come from the cell intervals
+    else:
+        vids = y_vertex_ids if y_vertex_ids is not None else blocks.problem.y_vertex_ids
+        if vids is None:
+            raise ValueError("the estimator needs the spatial vertex ids of the Y cells")
+        vids = np.ascontiguousarray(vids, dtype=np.int32)
     n = blocks.problem.n_y_cells
     out = {k: np.empty(n) for k in ("flux", "divergence", "reconstruction", "eta")}
     res = _lib.EstimatorResult()
     ctx = blocks.ctx
-    ctx.check(ctx.lib.apf_estimate(ctx.handle, blocks.handle, _ptr(vids), 0, _ptr(out["flux"]),
+    ctx.check(ctx.lib.apf_estimate(ctx.handle, blocks.handle, _ptr(vids) if vids is not None else None, 0,
+                                   _ptr(out["flux"]),
                                    _ptr(out["divergence"]), _ptr(out["reconstruction"]), _ptr(out["eta"]),
                                    C.byref(res)))
     totals = {name: getattr(res, name) for name, _ in res._fields_}

@@ -54,9 +54,12 @@ class SpaceTimeProblem:
     u0_kind: int = 0                      # 0 sin(pi x) sin(pi y), 1 one, 2 zero
     y_vertex_ids: np.ndarray | None = None  # [n_y_cells, 3] spatial vertex ids (estimator patches)
     meta: dict = field(default_factory=dict)
+    dim_space: int = 2                    # 1: 1+1D quads, geometry rows x0 x1 t0 t1, m_cells [n_y_cells]
 
     @property
     def ndof(self) -> int:
+        if self.dim_space == 1:
+            return (self.p + 1) * (self.p + 1)
         return (self.p + 1) * (self.p + 2) // 2 * (self.p + 1)
 
     @property
@@ -151,6 +154,44 @@ def uniform_problem(level: int, p: int = 1, u0_kind: int = 0, m_cells=None) -> S
         n_lambda=int(n_lambda), n_u=int(n_u), m_cells=m_cells, u0_kind=u0_kind,
         y_vertex_ids=np.tile(vids, (nt, 1)),
         meta=dict(level=level, n=n, nt=nt, n_spatial_interior=n_sp))
+
+
+def uniform_problem_1d(level: int, u0_kind: int = 0, m_cells=None) -> SpaceTimeProblem:
+    """1+1D heat problem on (0,1) x (0,1), P1 x P1 quadrilaterals, after the example's
+    initial refinement and `level` uniform outer refinements: n = 2^(level+1) intervals in
+    space and in time (the reference's `uniform_standard` outer iteration `level`; X has
+    (n-1)(n+1) true DOFs, Y (n-1) 2n).  Homogeneous Dirichlet data at x = 0, 1: the
+    boundary nodes own no true DOF (empty restriction rows).  Cells are numbered time
+    slab by time slab, left to right; DOFs by spatial node, then time."""
+    n = 2 ** (level + 1)
+    h = 1.0 / n
+    m_idx, i_idx = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")  # time slab m, space cell i
+    m_idx = m_idx.ravel()
+    i_idx = i_idx.ravel()
+    geo = np.stack([i_idx * h, (i_idx + 1) * h, m_idx * h, (m_idx + 1) * h], axis=1).astype(np.float64)
+    n_cells = n * n
+
+    def restriction(dof_of):
+        offsets = np.zeros(n_cells * 4 + 1, dtype=np.int32)
+        dofs = []
+        k = 0
+        for c in range(n_cells):
+            for loc in range(4):
+                s_node, a = loc >> 1, loc & 1
+                node = i_idx[c] + s_node
+                if 0 < node < n:
+                    dofs.append(dof_of(node, m_idx[c], a))
+                k += 1
+                offsets[k] = len(dofs)
+        d = np.asarray(dofs, dtype=np.int32)
+        return Restriction(offsets, d, np.ones(len(d)), 4)
+
+    x_r = restriction(lambda node, m, a: (node - 1) * (n + 1) + m + a)
+    y_r = restriction(lambda node, m, a: (node - 1) * (2 * n) + 2 * m + a)
+    return SpaceTimeProblem(p=1, y_geometry=geo, x_geometry=geo.copy(), y_to_x=np.arange(n_cells, dtype=np.int32),
+                            y_restriction=y_r, x_restriction=x_r, n_lambda=(n - 1) * 2 * n, n_u=(n - 1) * (n + 1),
+                            m_cells=m_cells, u0_kind=u0_kind, dim_space=1,
+                            meta={"level": level, "intervals": n})
 
 
 def dof_coordinates(problem: SpaceTimeProblem, space: str):

@@ -29,8 +29,9 @@ extern "C" {
 #define APF_ERR_NO_DEVICE (-6)     /* no CUDA device */
 #define APF_ERR_INTERNAL (-7)
 
-/* ---- initial data u0 of the examples (algorithm/examples/space_time_2d/initial_data_2d_examples.hpp) */
-#define APF_U0_SIN_SIN 0 /* smooth_initial: sin(pi x) sin(pi y) */
+/* ---- initial data u0 of the examples (algorithm/examples/space_time_2d/initial_data_2d_examples.hpp,
+ *      algorithm/examples/space_time_1d/initial_data_1d_examples.hpp) */
+#define APF_U0_SIN_SIN 0 /* smooth_initial: sin(pi x) sin(pi y) in 2+1D, sin(pi x) in 1+1D */
 #define APF_U0_ONE 1     /* non_matching_initial: 1 */
 #define APF_U0_ZERO 2
 
@@ -63,7 +64,16 @@ typedef struct apf_system apf_system;
  * local i) owns entries [offsets[c*ndof+i], offsets[c*ndof+i+1]) of (dofs,
  * weights); ndof = (p+1)(p+2)/2 * (p+1); local index = i_space*(p+1) + i_time
  * (src/finite_element/basis/functions/triangular_prism_lagrange.hpp:27-30).
- * The diffusion tensor and the load are constant per Y cell. */
+ * The diffusion tensor and the load are constant per Y cell.
+ *
+ * dim_space = 1 selects the 1+1D path (P1 only, tensor P1 x P1 Lagrange quadrilaterals,
+ * the reference's generic assembly branch with the local forms of
+ * src/finite_element/assembly/detail/local_bilinear_forms.hpp:24-81,
+ * local_mixed_bilinear_forms.hpp:15-153 and local_trace_bilinear_forms.hpp:20-49, Gauss
+ * orders QSpace = QTime = 3): geometry row = x0 x1 t0 t1 (spatial vertices 0 and 1,
+ * temporal vertices 0 and 1), ndof = 4 with local index = i_space*2 + i_time
+ * (src/finite_element/tables/quadrilateral_basis_tables.hpp:33-35), m_cells one scalar per
+ * Y cell.  dim_space = 0 or 2 is the 2+1D path. */
 typedef struct apf_problem_desc
 {
     int p;
@@ -87,6 +97,7 @@ typedef struct apf_problem_desc
     int u0_kind;             /* APF_U0_* */
     double zero_tol;         /* per-local-entry filter, reference default 1e-15 */
     double g_scale;          /* reference default -1 */
+    int dim_space;           /* 1 = 1+1D, 2 (or 0) = 2+1D */
 } apf_problem_desc;
 
 /* ---- context ----------------------------------------------------------------- */
@@ -233,7 +244,14 @@ typedef struct apf_estimator_result
  *             their sum (time_slab_estimator_combination.hpp).
  * y_vertex_ids: [n_y_cells*3] spatial vertex ids of every Y cell (the reference mesh's
  * cell.spatial_vertex_ids); host or device per pointers_on_device.  Y cells must
- * coincide with their X ancestors.  Output arrays ([n_y_cells] each, host or device per
+ * coincide with their X ancestors.
+ * 1+1D systems (dim_space = 1, p = 1) use the edge-patch estimator instead:
+ * TimeSlabEquilibratedFluxReconstruction1plus1d (time_slab_equilibrated_flux_reconstruction.hpp:
+ * 773-1880; patches from time_slab_edge_patch_builder.hpp:353-537, flux space
+ * patch_flux_space_1d.hpp, scalar space patch_scalar_space.hpp, local forms
+ * local_error_bilinear_forms.hpp and local_error_linear_forms.hpp) and
+ * compute_equilibrated_flux_error_squared_by_source_cell_1plus1d
+ * (time_slab_equilibrated_flux_indicators.hpp:23-190); y_vertex_ids is not used (NULL).  Output arrays ([n_y_cells] each, host or device per
  * pointers_on_device) may be NULL. */
 int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int pointers_on_device,
                  double* flux_squared, double* divergence_squared, double* reconstruction_squared,

@@ -181,6 +181,7 @@ class MainProblem:
     n_lambda: int
     n_u: int
     m_cells: np.ndarray | None = None   # [ny, 3] (m00, m01, m11) per Y cell; None = identity
+    dim_space: int = 2                  # 1: quads, geometry rows x0 x1 t0 t1, m_cells [ny]
 
 
 def geometry_terms(geom):
@@ -370,6 +371,10 @@ def assemble_graph_norm(prob: MainProblem, A_y, C_signed, zero_tol=1e-15, diag_t
     gpsi = np.einsum("nab,qjb->nqja", gxx["invJT"], dphi_ref[:, :, :2])
     A_x_loc = np.einsum("nqia,nab,nqjb,nq->nij", gpsi, Mxt, gpsi, dmux)
     A_x = scatter_matrix(A_x_loc, prob.x_restr, prob.x_restr, (prob.n_u, prob.n_u), zero_tol)
+    return _hhat_from_blocks(A_y, C_signed, A_x, B_dt, diag_tol, prob.n_u)
+
+
+def _hhat_from_blocks(A_y, C_signed, A_x, B_dt, diag_tol, n_u):
     d = A_y.diagonal()
     if np.any(~(d > diag_tol)):
         raise RuntimeError("diagonal_schur_approximation: A_y diagonal must be positive.")
@@ -394,8 +399,99 @@ def assemble_graph_norm(prob: MainProblem, A_y, C_signed, zero_tol=1e-15, diag_t
     Cc = C_signed.tocoo()
     Ax = A_x.tocoo()
     rows += [Cc.row, Ax.row]; cols += [Cc.col, Ax.col]; vals += [-Cc.data, Ax.data]
-    H = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(prob.n_u, prob.n_u))
+    H = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n_u, n_u))
     return dict(Hhat=H, B_dt=B_dt, A_x=A_x)
+
+
+# ---------------------------------------------------------------------------------------
+# 1+1D (P1 x P1 quadrilaterals, QSpace = QTime = 3 Gauss points): the generic branch of
+# assemble_main_system_blocks with local_bilinear_forms.hpp:24-81,
+# local_mixed_bilinear_forms.hpp:15-153, local_trace_bilinear_forms.hpp:20-49; local index
+# i = i_space * 2 + i_time (quadrilateral_basis_tables.hpp:33-35).
+# ---------------------------------------------------------------------------------------
+def sin_initial_1d(x):
+    return np.sin(math.pi * x)
+
+
+def one_initial_1d(x):
+    return np.ones_like(x)
+
+
+def _quad_basis(xi, tau):
+    """P1 x P1 values, d/dxi, d/dtau at reference points -> three [nq, 4] arrays."""
+    N = np.stack([1.0 - xi, xi], -1)
+    dN = np.stack([-np.ones_like(xi), np.ones_like(xi)], -1)
+    T = np.stack([1.0 - tau, tau], -1)
+    dT = np.stack([-np.ones_like(tau), np.ones_like(tau)], -1)
+    v = (N[:, :, None] * T[:, None, :]).reshape(len(xi), 4)
+    vx = (dN[:, :, None] * T[:, None, :]).reshape(len(xi), 4)
+    vt = (N[:, :, None] * dT[:, None, :]).reshape(len(xi), 4)
+    return v, vx, vt
+
+
+def _quad_rule():
+    gx, gw = gauss_legendre01(3)
+    xi, tau = np.meshgrid(gx, gx, indexing="ij")
+    w = np.outer(gw, gw)
+    return xi.ravel(), tau.ravel(), w.ravel()
+
+
+def assemble_main_blocks_1d(prob: MainProblem, u0=sin_initial_1d, ell=None, zero_tol=1e-15, g_scale=-1.0):
+    """Restatement of assemble_main_system_blocks for 1+1D P1 (assemble_saddle_problem.hpp:131)."""
+    xi, tau, w = _quad_rule()
+    gy, gx = prob.y_geom, prob.x_geom[prob.y_to_x]
+    ny = gy.shape[0]
+    m = prob.m_cells if prob.m_cells is not None else np.ones(ny)
+    hy, ky = gy[:, 1] - gy[:, 0], gy[:, 3] - gy[:, 2]
+    v, vx, vt = _quad_basis(xi, tau)
+    dmu = (hy * ky)[:, None] * w[None, :]
+    phi_x = vx[None, :, :] / hy[:, None, None]
+    A = np.einsum("n,nqi,nqj,nq->nij", m, phi_x, phi_x, dmu)
+    # X basis at the Y points through the X cell's reference coordinates
+    xq = gy[:, 0:1] + hy[:, None] * xi[None, :]
+    tq = gy[:, 2:3] + ky[:, None] * tau[None, :]
+    hx, kx = gx[:, 1] - gx[:, 0], gx[:, 3] - gx[:, 2]
+    pv, pvx, pvt = _quad_basis(((xq - gx[:, 0:1]) / hx[:, None]).ravel(), ((tq - gx[:, 2:3]) / kx[:, None]).ravel())
+    psi_x = pvx.reshape(ny, -1, 4) / hx[:, None, None]
+    psi_t = pvt.reshape(ny, -1, 4) / kx[:, None, None]
+    B = np.einsum("nqi,qj,nq->nij", psi_t, v, dmu) + np.einsum("n,nqi,nqj,nq->nij", m, psi_x, phi_x, dmu)
+    f_loc = np.zeros((ny, 4)) if ell is None else np.einsum("nq,qj,nq->nj", ell(xq, tq), v, dmu)
+    A_y = scatter_matrix(A, prob.y_restr, prob.y_restr, (prob.n_lambda, prob.n_lambda), zero_tol)
+    Bm = scatter_matrix(B, prob.x_restr, prob.y_restr, (prob.n_u, prob.n_lambda), zero_tol, test_cells=prob.y_to_x)
+    f = scatter_vector(f_loc, prob.y_restr, prob.n_lambda, zero_tol)
+    # trace blocks on the X cells at t = 0 (3-point Gauss bottom rule)
+    cells = np.nonzero(prob.x_geom[:, 2] == 0.0)[0]
+    bx, bw = gauss_legendre01(3)
+    bv, _, _ = _quad_basis(bx, np.zeros_like(bx))
+    gc = prob.x_geom[cells]
+    hc = gc[:, 1] - gc[:, 0]
+    dg = hc[:, None] * bw[None, :]
+    C_loc = -np.einsum("qi,qj,nq->nij", bv, bv, dg)
+    g_loc = g_scale * np.einsum("nq,qi,nq->ni", u0(gc[:, 0:1] + hc[:, None] * bx[None, :]), bv, dg)
+    C = scatter_matrix(C_loc, prob.x_restr, prob.x_restr, (prob.n_u, prob.n_u), zero_tol,
+                       test_cells=cells, trial_cells=cells)
+    g = scatter_vector(g_loc, prob.x_restr, prob.n_u, zero_tol, cells=cells)
+    Bdt_loc = np.einsum("nqi,qj,nq->nij", psi_t, v, dmu)
+    return dict(A_y=A_y, B=Bm, C_signed=C, f=f, g=g, _Bdt_loc=Bdt_loc)
+
+
+def assemble_graph_norm_1d(prob: MainProblem, A_y, C_signed, zero_tol=1e-15, diag_tol=1e-14):
+    """Hhat = -C_signed + B_dt diag(A_y)^-1 B_dt^T + A_x for 1+1D P1 (parabolic_graph_norm.hpp:22-65)."""
+    blocks = assemble_main_blocks_1d(prob, zero_tol=zero_tol)
+    B_dt = scatter_matrix(blocks["_Bdt_loc"], prob.x_restr, prob.y_restr, (prob.n_u, prob.n_lambda), zero_tol,
+                          test_cells=prob.y_to_x)
+    xi, tau, w = _quad_rule()
+    gxx = prob.x_geom
+    nx = gxx.shape[0]
+    mx = np.ones(nx)
+    if prob.m_cells is not None:
+        mx[prob.y_to_x] = prob.m_cells
+    h, k = gxx[:, 1] - gxx[:, 0], gxx[:, 3] - gxx[:, 2]
+    _, vx, _ = _quad_basis(xi, tau)
+    px = vx[None, :, :] / h[:, None, None]
+    A_x_loc = np.einsum("n,nqi,nqj,nq->nij", mx, px, px, (h * k)[:, None] * w[None, :])
+    A_x = scatter_matrix(A_x_loc, prob.x_restr, prob.x_restr, (prob.n_u, prob.n_u), zero_tol)
+    return _hhat_from_blocks(A_y, C_signed, A_x, B_dt, diag_tol, prob.n_u)
 
 
 def load_csc(d, name):

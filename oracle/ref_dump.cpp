@@ -10,7 +10,7 @@
 //   * the parabolic graph-norm Schur approximation Hhat
 //     (src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:22).
 //
-// usage: apf_ref_dump <dim:2> <p:1|2> <uniform_levels> <example> <outdir>
+// usage: apf_ref_dump <dim:1|2> <p:1|2> <uniform_levels> <example> <outdir>
 //        apf_ref_dump bench <p:1|2> <uniform_levels> <example> <reps>
 
 #include <cstdio>
@@ -31,6 +31,7 @@
 #include "algorithm/example_registry.hpp"
 #include "algorithm/examples/space_time_2d/initial_data_2d_examples.hpp"
 #include "algorithm/examples/space_time_2d/space_time_2d_example.hpp"
+#include "algorithm/examples/space_time_1d/space_time_1d_example.hpp"
 #include "algorithm/support/space_time_1d.hpp"
 #include "algorithm/support/space_time_2d.hpp"
 #include "finite_element/fespace/fe_traits.hpp"
@@ -128,10 +129,12 @@ namespace
             const auto& sv = mesh.spatial_vertices();
             const auto& tv = mesh.temporal_vertices();
             double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300, mnt = 1e300, mxt = -1e300;
+            constexpr int dim = Space::GT::dim_space_v;
             for (const int v : cell.spatial_vertex_ids) {
                 mnx = std::min(mnx, sv[v][0]); mxx = std::max(mxx, sv[v][0]);
-                mny = std::min(mny, sv[v][1]); mxy = std::max(mxy, sv[v][1]);
+                if constexpr (dim > 1) { mny = std::min(mny, sv[v][dim > 1 ? 1 : 0]); mxy = std::max(mxy, sv[v][dim > 1 ? 1 : 0]); }
             }
+            if constexpr (dim == 1) { mny = 0.0; mxy = 1.0; }
             for (const int v : cell.temporal_vertex_ids) { mnt = std::min(mnt, tv[v][0]); mxt = std::max(mxt, tv[v][0]); }
             return Ext{mxx - mnx, mxy - mny, mxt - mnt};
         };
@@ -165,7 +168,8 @@ namespace
             for (const int c : space.active_cells()) {
                 const auto e = extents(c);
                 const auto& pe = parents.at(ancestor(c));
-                if (!(smaller(e.sx, pe.sx) && smaller(e.sy, pe.sy))) { all_smaller = false; break; }
+                const bool sy_ok = Space::GT::dim_space_v == 1 || smaller(e.sy, pe.sy);
+                if (!(smaller(e.sx, pe.sx) && sy_ok)) { all_smaller = false; break; }
             }
             const std::vector<int> targets(space.active_cells().begin(), space.active_cells().end());
             if (all_smaller) { refine_all(targets, mesh::RefinementType::temporal); return; }
@@ -349,6 +353,113 @@ namespace
         }
         return 0;
     }
+
+    // 1+1D: unit space-time square, the example's initial refinement, then `levels`
+    // uniform outer refinements (space and time halved), P = 1 elements with the
+    // runner's Gauss orders QSpace = QTime = 2P + 1
+    // (algorithm/runners/detail/runner_case_execution.hpp:27-33).  Geometry rows are
+    // x0 x1 t0 t1 (spatial vertices 0 and 1 of the cell, temporal vertices 0 and 1).
+    template<int P>
+    int run_1d(int levels, const std::string& example_name, const std::string& dir)
+    {
+        constexpr int QSpace = 2 * P + 1;
+        constexpr int QTime = 2 * P + 1;
+        using GT = mesh::MeshTraits<1>;
+        using FET = finite_element::FiniteElementTraits<GT, P, P>;
+        using XSpace = finite_element::FESpace<GT, FET, finite_element::SpaceTimePolicy>;
+        using YSpace = finite_element::FESpace<GT, FET, finite_element::SpaceOnlyPolicy>;
+
+        auto example = adaptive_algorithm::examples::make_1d_example(example_name);
+        auto mesh = adaptive_algorithm::support::make_unit_mesh<GT>();
+        XSpace x_space(mesh);
+        YSpace y_space(mesh);
+        adaptive_algorithm::examples::initialize_spaces_from_example(x_space, y_space, example);
+        for (int k = 0; k < levels; ++k)
+            uniform_isotropic_refine(x_space);
+        y_space.initialize(x_space.active_cells());
+
+        const auto& y_cells = y_space.active_cells();
+        const auto& x_cells = x_space.active_cells();
+        std::cerr << "1d p=" << P << " levels=" << levels << " x_cells=" << x_cells.size()
+                  << " y_cells=" << y_cells.size()
+                  << " n_x=" << x_space.dof_handler_ref().n_true_dofs()
+                  << " n_y=" << y_space.dof_handler_ref().n_true_dofs() << "\n";
+
+        std::filesystem::create_directories(dir);
+        auto dump_geometry_1d = [&](const std::string& name, const auto& cells) {
+            std::vector<double> g;
+            for (const int c : cells)
+            {
+                const auto& cell = mesh.cell(c);
+                g.push_back(mesh.spatial_vertices()[cell.spatial_vertex_ids[0]][0]);
+                g.push_back(mesh.spatial_vertices()[cell.spatial_vertex_ids[1]][0]);
+                g.push_back(mesh.temporal_vertices()[cell.temporal_vertex_ids[0]][0]);
+                g.push_back(mesh.temporal_vertices()[cell.temporal_vertex_ids[1]][0]);
+            }
+            apf_oracle::write_npy(dir + "/" + name + ".npy", g.data(), {cells.size(), 4u});
+        };
+        dump_geometry_1d("y_geometry", y_cells);
+        dump_geometry_1d("x_geometry", x_cells);
+        dump_restrictions(dir, "y_restriction", y_space, std::vector<int>(y_cells.begin(), y_cells.end()));
+        dump_restrictions(dir, "x_restriction", x_space, std::vector<int>(x_cells.begin(), x_cells.end()));
+        {
+            finite_element::assembly::detail::ActiveAncestorCache<XSpace> cache(x_space);
+            std::vector<int> x_pos(static_cast<std::size_t>(mesh.n_cells()), -1);
+            for (std::size_t k = 0; k < x_cells.size(); ++k)
+                x_pos[static_cast<std::size_t>(x_cells[k])] = static_cast<int>(k);
+            std::vector<int> anc;
+            for (const int c : y_cells)
+                anc.push_back(x_pos[static_cast<std::size_t>(cache.find(c))]);
+            apf_oracle::write_npy(dir + "/y_to_x_cell.npy", anc);
+            apf_oracle::write_npy(dir + "/y_cell_ids.npy", std::vector<int>(y_cells.begin(), y_cells.end()));
+            apf_oracle::write_npy(dir + "/x_cell_ids.npy", std::vector<int>(x_cells.begin(), x_cells.end()));
+        }
+
+        const auto blocks = finite_element::system::assemble_main_system_blocks<QSpace, QTime, Backend>(
+            y_space, x_space, example.problem, 1e-15, -1.0);
+        dump_csc(dir, "A_y", blocks.A_y());
+        dump_csc(dir, "B", blocks.lower_left_B());
+        dump_csc(dir, "C_signed", blocks.C_signed());
+        dump_vec(dir, "f", blocks.f());
+        dump_vec(dir, "g", blocks.g());
+        const auto gn = finite_element::assembly::assemble_parabolic_graph_norm_approximation<QSpace, QTime, Backend>(
+            y_space, x_space, example.problem.M, blocks.A_y(), blocks.C_signed(), 1e-15, 1e-14);
+        dump_csc(dir, "Hhat", gn.approximation.hhat);
+
+        if (std::getenv("APF_REF_ESTIMATE") != nullptr)
+        {
+            typename Backend::Solver solver;
+            la::concepts::SolverOptions opts;
+            finite_element::time_slabs::AdaptiveTestSpaceIterationParameters<Backend, XSpace, YSpace> params;
+            const auto state = finite_element::time_slabs::compute_adaptive_test_space_iteration<QSpace, QTime, Backend>(
+                y_space, x_space, example.problem, solver, opts, params);
+            dump_vec(dir, "lambda_delta", state.lambda_delta.true_coefficients());
+            dump_vec(dir, "u_delta", state.u_delta.true_coefficients());
+            auto dump_over = [&](const std::string& name, const auto& cells, const auto& m) {
+                std::vector<double> vals;
+                for (const int c : cells)
+                {
+                    const auto it = m.find(c);
+                    vals.push_back(it == m.end() ? std::numeric_limits<double>::quiet_NaN() : it->second);
+                }
+                apf_oracle::write_npy(dir + "/" + name + ".npy", vals);
+            };
+            const auto xi = adaptive_algorithm::detail::compute_x_marking_indicator_components<QSpace, QTime>(
+                x_space, state.lambda_delta, state.u_delta, example.problem.u0, example.problem.M);
+            dump_over("xind_lambda_by_y", y_cells, xi.lambda_y_squared_by_y_cell.by_source_cell);
+            dump_over("xind_lambda_by_x", x_cells, xi.lambda_y_squared_by_x_cell.by_source_cell);
+            dump_over("xind_trace_by_x", x_cells, xi.initial_trace_squared_by_x_cell.by_source_cell);
+            dump_over("xind_eta_by_x", x_cells, xi.eta_squared_by_x_cell.by_source_cell);
+            dump_over("est_flux", y_cells, state.flux_diagnostics.by_source_cell_flux);
+            dump_over("est_div", y_cells, state.flux_diagnostics.by_source_cell_residual);
+            dump_over("est_recon", y_cells, state.reconstruction_y_squared.by_source_cell);
+            dump_over("est_eta", y_cells, state.estimator.estimator_squared.by_source_cell);
+            std::fprintf(stderr, "estimate: flux=%.6e div=%.6e recon=%.6e eta=%.6e\n",
+                         state.flux_diagnostics.total_flux(), state.flux_diagnostics.total_residual(),
+                         state.reconstruction_y_squared.total(), state.estimator.total());
+        }
+        return 0;
+    }
 }
 
 int main(int argc, char** argv)
@@ -382,6 +493,8 @@ int main(int argc, char** argv)
     const std::string dir = argv[5];
     try
     {
+        if (dim == 1 && p == 1)
+            return run_1d<1>(levels, example, dir);
         if (dim == 2 && p == 1)
             return run_2d<1>(levels, example, dir);
         if (dim == 2 && p == 2)

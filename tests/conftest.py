@@ -16,6 +16,7 @@ def pytest_configure(config):
 
 
 GOLDEN_CASES = ["p1_l1_smooth", "p1_l2_smooth", "p2_l1_smooth", "p1_l1_nonmatching"]
+GOLDEN_CASES_1D = ["d1_l2_smooth", "d1_l2_nonmatching", "d1_l5_smooth"]
 
 
 def load_golden(name):
@@ -24,7 +25,8 @@ def load_golden(name):
     import scipy.sparse as sp
     z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     p = int(z["meta_p"][0])
-    ndof = (p + 1) * (p + 2) // 2 * (p + 1)
+    dim = int(z["meta_dim"][0]) if "meta_dim" in z else 2
+    ndof = (p + 1) * (p + 1) if dim == 1 else (p + 1) * (p + 2) // 2 * (p + 1)
 
     def restr(prefix):
         return O.Restriction(z[f"{prefix}_offsets"], z[f"{prefix}_dofs"], z[f"{prefix}_weights"], ndof)
@@ -38,7 +40,7 @@ def load_golden(name):
     out["g"] = z["g"]
     prob = O.MainProblem(p=p, y_geom=z["y_geometry"], x_geom=z["x_geometry"], y_to_x=z["y_to_x_cell"],
                          y_restr=restr("y_restriction"), x_restr=restr("x_restriction"),
-                         n_lambda=out["A_y"].shape[0], n_u=out["C_signed"].shape[0])
+                         n_lambda=out["A_y"].shape[0], n_u=out["C_signed"].shape[0], dim_space=dim)
     example = str(z["meta_example"][0])
     return prob, out, example
 
@@ -47,13 +49,16 @@ def to_product_problem(prob, example):
     """Oracle MainProblem -> product SpaceTimeProblem (same arrays)."""
     from doubleadapparabolicfem_b200.mesh import Restriction, SpaceTimeProblem
     u0 = 0 if example == "smooth_initial" else 1
+    ell = None
+    if prob.dim_space == 1 and example == "non_matching_initial":
+        ell = np.full(prob.y_geom.shape[0], 2.0)  # the 1+1D example's constant load
     return SpaceTimeProblem(
         p=prob.p, y_geometry=prob.y_geom, x_geometry=prob.x_geom, y_to_x=prob.y_to_x.astype(np.int32),
         y_restriction=Restriction(prob.y_restr.offsets.astype(np.int32), prob.y_restr.dofs.astype(np.int32),
                                   prob.y_restr.weights, prob.y_restr.ndof),
         x_restriction=Restriction(prob.x_restr.offsets.astype(np.int32), prob.x_restr.dofs.astype(np.int32),
                                   prob.x_restr.weights, prob.x_restr.ndof),
-        n_lambda=prob.n_lambda, n_u=prob.n_u, u0_kind=u0)
+        n_lambda=prob.n_lambda, n_u=prob.n_u, u0_kind=u0, ell_cells=ell, dim_space=prob.dim_space)
 
 
 def assert_same_sparse(ref, mine, rtol, what=""):

@@ -8,7 +8,7 @@ per-cell indicators) and the driver's X-marking indicators.  Also extracts the u
 6-significant-digit estimator values) of the reference's published paper data
 (algorithm_data_plot/{1d,2d}/*.csv) into paper_uniform_rows.json.
 
-usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+usage: python tests/golden/make_golden.py [REFERENCE_ROOT [CASE ...]]
 """
 from __future__ import annotations
 
@@ -33,6 +33,10 @@ CASES = [
     ("p2_l1_smooth", 2, 2, 1, "smooth_initial"),
     ("p1_l1_nonmatching", 2, 1, 1, "non_matching_initial"),
     ("p1_l3_smooth", 2, 1, 3, "smooth_initial"),
+    # 1+1D P1 (geometry rows x0 x1 t0 t1); level 5 is the 64 x 64 = 4,096-element mesh
+    ("d1_l2_smooth", 1, 1, 2, "smooth_initial"),
+    ("d1_l2_nonmatching", 1, 1, 2, "non_matching_initial"),
+    ("d1_l5_smooth", 1, 1, 5, "smooth_initial"),
 ]
 
 
@@ -48,9 +52,13 @@ def dump_case(dim, p, level, example, outdir):
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), f"REF={ref_root}"], check=True)
+    only = set(sys.argv[2:])
     for name, dim, p, level, example in CASES:
+        if only and name not in only:
+            continue
         with tempfile.TemporaryDirectory() as tmp:
             arrays = dump_case(dim, p, level, example, tmp)
+        arrays["meta_dim"] = np.array([dim])
         arrays["meta_p"] = np.array([p])
         arrays["meta_level"] = np.array([level])
         arrays["meta_example"] = np.array([example])
