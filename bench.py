@@ -419,6 +419,34 @@ def run_ours(args, world, rank, local):
                                              C.byref(om), C.byref(al)))
             rows.append([r.value, na.value, npp.value])
         amg_levels[name] = {"rows_nnz_nnzP": rows, "dense_coarsest": bool(dc.value)}
+    # the precision form of the patch solves on the same solution: FP64 (the bench line's
+    # path) against FP32 factorisation + one FP64 refinement step
+    patch_precision = None
+    if run_estimator and args.p == 1:
+        cells = {}
+        for prec_name, prec in (("fp64", _lib.APF_PATCH_FP64), ("fp32_refined", _lib.APF_PATCH_FP32_REFINED)):
+            ctx.check(lib.apf_ctx_set_patch_precision(ctx.handle, prec))
+            fl = torch.empty(ny, dtype=torch.float64, device=dev)
+            et = torch.empty(ny, dtype=torch.float64, device=dev)
+            res = _lib.EstimatorResult()
+            ctx.check(lib.apf_ctx_set_timing(ctx.handle, 1))
+            ctx.check(lib.apf_estimate(ctx.handle, h, C.c_void_p(dprob.y_vertex_ids.data_ptr()), 1,
+                                       C.c_void_p(fl.data_ptr()), None, None, C.c_void_p(et.data_ptr()),
+                                       C.byref(res)))
+            rep = json.loads(lib.apf_ctx_timing_report(ctx.handle).decode())
+            ctx.check(lib.apf_ctx_set_timing(ctx.handle, 0))
+            cells[prec_name] = (fl.cpu().numpy(), et.cpu().numpy(), res.flux_squared,
+                                rep.get("est_patch_solve", [0, float("nan")])[1],
+                                rep.get("host:call_estimate", [0, float("nan")])[1])
+        ctx.check(lib.apf_ctx_set_patch_precision(ctx.handle, _lib.APF_PATCH_FP64))
+        f64, f32 = cells["fp64"], cells["fp32_refined"]
+        scale = float(np.abs(f64[0]).max())
+        patch_precision = {
+            "patch_solve_ms_fp64": round(f64[3], 3), "patch_solve_ms_fp32_refined": round(f32[3], 3),
+            "estimate_ms_fp64": round(f64[4], 3), "estimate_ms_fp32_refined": round(f32[4], 3),
+            "max_cell_flux_err_over_max_cell": float(np.abs(f32[0] - f64[0]).max() / scale),
+            "max_cell_eta_err_over_max_cell": float(np.abs(f32[1] - f64[1]).max() / scale),
+            "flux_total_rel_err": float(abs(f32[2] - f64[2]) / f64[2])}
     m = MainSystemBlocks(ctx, h, host)
     nnz_k = m.block_info("K")[2]
     nnz_h = m.block_info("Hhat")[2]
@@ -469,6 +497,7 @@ def run_ours(args, world, rank, local):
                    "learned_fallbacks": sum(d["learned_fallback"] for d in timed_diags),
                    "minres_solve_s_mean": sum(d["solve_seconds"] for d in timed_diags) / len(timed_diags),
                    "plain_preconditioner": plain,
+                   "patch_precision_fp32_refined_vs_fp64": patch_precision,
                    "minres_iterations": [d["iterations"] for d in timed_diags],
                    "step_ms": step_ms,
                    "step_stage_wall_ms": stage_ms,

@@ -12,6 +12,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libapf_b200.so")
 
 APF_OK = 0
+APF_PATCH_FP64 = 0
+APF_PATCH_FP32_REFINED = 1
 APF_ERR_INVALID = -1
 APF_ERR_CUDA = -2
 APF_ERR_CAPACITY = -3
@@ -107,6 +109,7 @@ SIGNATURES = {
     "apf_ctx_synchronize": ([C.c_void_p], C.c_int),
     "apf_ctx_kernel_launches": ([C.c_void_p], C.c_int64),
     "apf_ctx_set_timing": ([C.c_void_p, C.c_int], C.c_int),
+    "apf_ctx_set_patch_precision": ([C.c_void_p, C.c_int], C.c_int),
     "apf_ctx_timing_report": ([C.c_void_p], C.c_char_p),
     "apf_assemble_main_system": ([C.c_void_p, C.POINTER(ProblemDesc), C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "apf_assemble_graph_norm": ([C.c_void_p, C.c_void_p, C.c_double], C.c_int),

@@ -23,6 +23,7 @@ struct apf_ctx
     std::string report;
     std::unique_ptr<apf::LearnedModel> learned; // model of APF_PRECOND_LEARNED set-ups
     unsigned long long learned_version = 0;
+    int patch_precision = APF_PATCH_FP64; // apf_ctx_set_patch_precision
 };
 
 struct apf_learned_model
@@ -644,6 +645,14 @@ int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const dou
     });
 }
 
+int apf_ctx_set_patch_precision(apf_ctx* ctx, int precision)
+{
+    if (!ctx || (precision != APF_PATCH_FP64 && precision != APF_PATCH_FP32_REFINED))
+        return APF_ERR_INVALID;
+    ctx->patch_precision = precision;
+    return APF_OK;
+}
+
 int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int pointers_on_device,
                  double* flux_squared, double* divergence_squared, double* reconstruction_squared, double* eta_squared,
                  apf_estimator_result* result)
@@ -669,7 +678,7 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
                                          ctx->stream));
             apf::sync(ctx->stream);
             t = apf::estimate(ctx->stream, S, vids, flux_squared, divergence_squared, reconstruction_squared,
-                              eta_squared, pointers_on_device != 0);
+                              eta_squared, pointers_on_device != 0, ctx->patch_precision);
         }
         if (result)
         {

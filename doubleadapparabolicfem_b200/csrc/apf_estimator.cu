@@ -337,14 +337,26 @@ namespace apf
         //              over columns, applied to both right-hand sides at once;
         //   solve    : column-oriented back substitution, lanes over rows.
         // Patches arrive sorted into size buckets; NMAX is the bucket's bound.
-        template<int NMAX, int W>
+        //
+        // F32 = true: the matrix is assembled and factored in FP32 (half the shared memory per
+        // team, so twice the teams per SM), followed by one FP64 iterative-refinement step:
+        // the FP64 residual Mt^-1 b - K x is formed matrix-free by a second pass over the
+        // patch cells' local entries (FP64 shared-memory atomics), solved with the FP32
+        // factors and pivots, and added to x in FP64.
+        template<int NMAX, int W, bool F32>
         __global__ void __launch_bounds__(32 * W) patch_solve(PatchArgs A, const PatchTables* __restrict__ tables,
                                                           const int* __restrict__ order, int count)
         {
+            using V = typename std::conditional<F32, float, double>::type;
             constexpr int LD = NMAX + 3; // odd: NMAX is even
             extern __shared__ double sm[];
             PatchTables& T = *reinterpret_cast<PatchTables*>(sm);
-            double* K = sm + kPatchTableDoubles + (kPatchTableDoubles & 1);
+            // F32: x [2][NMAX], b [2][NMAX], K x [2][NMAX] in FP64 ahead of the matrix
+            double* xd = sm + kPatchTableDoubles + (kPatchTableDoubles & 1);
+            double* bd = xd + 2 * NMAX;
+            double* kx = bd + 2 * NMAX;
+            V* K = reinterpret_cast<V*>(xd + (F32 ? 6 * NMAX : 0));
+            int* piv = reinterpret_cast<int*>(K + NMAX * LD);
             const int lane = threadIdx.x;
             constexpr int NT = 32 * W; // threads of the patch team
             for (int i = lane; i < kPatchTableDoubles; i += NT)
@@ -369,6 +381,9 @@ namespace apf
                 for (int i = lane; i < n * LD; i += NT)
                     K[i] = 0.0;
                 team_sync<W>();
+                // every local entry (row, col, value) of the patch system; cols n, n + 1 are
+                // the two right-hand sides
+                auto cell_entries = [&](auto&& sink) {
                 double ht = 0.0;
                 for (int ic = 0; ic < nc; ++ic)
                 {
@@ -411,10 +426,10 @@ namespace apf
                         gth[kk][0] = gth[kk][1] = 0.0;
                         for (int s2 = 0; s2 < 3; ++s2)
                         {
-                            const double W = k.ht * ((kk == 0 ? 1.0 / 3.0 : 1.0 / 6.0) * th[2 * s2] +
-                                                     (kk == 0 ? 1.0 / 6.0 : 1.0 / 3.0) * th[2 * s2 + 1]);
-                            gth[kk][0] += k.g[s2][0] * W;
-                            gth[kk][1] += k.g[s2][1] * W;
+                            const double wt = k.ht * ((kk == 0 ? 1.0 / 3.0 : 1.0 / 6.0) * th[2 * s2] +
+                                                      (kk == 0 ? 1.0 / 6.0 : 1.0 / 3.0) * th[2 * s2 + 1]);
+                            gth[kk][0] += k.g[s2][0] * wt;
+                            gth[kk][1] += k.g[s2][1] * wt;
                         }
                     }
                     double du[3];
@@ -428,7 +443,7 @@ namespace apf
                             if (pd[j] < 0 || pd[l] < 0)
                                 continue;
                             const double r = S00 * T.r00[j][l] + S01 * (T.r01[j][l] + T.r01[l][j]) + S11 * T.r11[j][l];
-                            K[pd[j] * LD + pd[l]] += e[j] * e[l] * adet * r;
+                            sink(pd[j], pd[l], e[j] * e[l] * adet * r);
                         }
                         else if (t < 88)
                         {
@@ -436,8 +451,8 @@ namespace apf
                             if (pd[l] < 0)
                                 continue;
                             const double v = e[l] * adet * T.rd[l][r];
-                            K[(sbase + r) * LD + pd[l]] += v;
-                            K[pd[l] * LD + sbase + r] += v;
+                            sink(sbase + r, pd[l], v);
+                            sink(pd[l], sbase + r, v);
                         }
                         else if (t < 104)
                         {
@@ -446,7 +461,7 @@ namespace apf
                                 continue;
                             const double gJ0 = gth[kk][0] * k.J00 + gth[kk][1] * k.J10;
                             const double gJ1 = gth[kk][0] * k.J01 + gth[kk][1] * k.J11;
-                            K[pd[j] * LD + n + kk] += -e[j] * adet * (gJ0 * T.rl[a][j][0] + gJ1 * T.rl[a][j][1]);
+                            sink(pd[j], n + kk, -e[j] * adet * (gJ0 * T.rl[a][j][0] + gJ1 * T.rl[a][j][1]));
                         }
                         else if (t < 110)
                         {
@@ -457,25 +472,28 @@ namespace apf
                             const double mg0 = k.m00 * gth[kk][0] + k.m01 * gth[kk][1];
                             const double mg1 = k.m01 * gth[kk][0] + k.m11 * gth[kk][1];
                             const double gpm = k.g[a][0] * mg0 + k.g[a][1] * mg1;
-                            K[(sbase + r) * LD + n + kk] += (0.5 * k.ht * acc - gpm / 6.0) * adet;
+                            sink(sbase + r, n + kk, (0.5 * k.ht * acc - gpm / 6.0) * adet);
                         }
                         else if (interior)
                         {
                             // mean-zero row: int_K lambda_r = |K| / 6 on the reference scale
                             const int r = t - 110;
                             const double v = adet / 6.0;
-                            K[(n - 1) * LD + sbase + r] += v;
-                            K[(sbase + r) * LD + n - 1] += v;
+                            sink(n - 1, sbase + r, v);
+                            sink(sbase + r, n - 1, v);
                         }
                     }
                     team_sync<W>();
                 }
+                return ht;
+                };
+                const double ht = cell_entries([&](int row, int col, double v) { K[row * LD + col] += static_cast<V>(v); });
                 // right-hand sides times Mt^-1 (Mt = ht [[1/3,1/6],[1/6,1/3]], inverse (1/ht) [[4,-2],[-2,4]])
                 for (int i = lane; i < n; i += NT)
                 {
                     const double b0 = K[i * LD + n], b1 = K[i * LD + n + 1];
-                    K[i * LD + n] = (4.0 * b0 - 2.0 * b1) / ht;
-                    K[i * LD + n + 1] = (-2.0 * b0 + 4.0 * b1) / ht;
+                    K[i * LD + n] = static_cast<V>((4.0 * b0 - 2.0 * b1) / ht);
+                    K[i * LD + n + 1] = static_cast<V>((-2.0 * b0 + 4.0 * b1) / ht);
                 }
                 team_sync<W>();
                 // LU with partial pivoting on the augmented n x (n + 2) system
@@ -499,18 +517,20 @@ namespace apf
                         singular = true;
                         break;
                     }
+                    if (F32 && lane == 0)
+                        piv[col] = bi;
                     if (bi != col)
                         for (int j = col + lane; j < n + 2; j += NT)
                         {
-                            const double t0 = K[col * LD + j];
+                            const V t0 = K[col * LD + j];
                             K[col * LD + j] = K[bi * LD + j];
                             K[bi * LD + j] = t0;
                         }
                     team_sync<W>();
-                    const double inv = 1.0 / K[col * LD + col];
+                    const V inv = V(1) / K[col * LD + col];
                     for (int j = col + 1 + lane; j < n + 2; j += NT)
                     {
-                        const double u = K[col * LD + j] * inv;
+                        const V u = K[col * LD + j] * inv;
                         for (int i = col + 1; i < n; ++i)
                             K[i * LD + j] -= K[i * LD + col] * u;
                     }
@@ -524,24 +544,86 @@ namespace apf
                     continue;
                 }
                 // back substitution, both right-hand sides, lanes over the rows above
-                for (int i = n - 1; i >= 0; --i)
-                {
-                    const double d = K[i * LD + i];
-                    const double x0 = K[i * LD + n] / d, x1 = K[i * LD + n + 1] / d;
-                    for (int r = lane; r < i; r += NT)
+                auto back_substitute = [&]() {
+                    for (int i = n - 1; i >= 0; --i)
                     {
-                        const double kri = K[r * LD + i];
-                        K[r * LD + n] -= kri * x0;
-                        K[r * LD + n + 1] -= kri * x1;
+                        const V d = K[i * LD + i];
+                        const V x0 = K[i * LD + n] / d, x1 = K[i * LD + n + 1] / d;
+                        for (int r = lane; r < i; r += NT)
+                        {
+                            const V kri = K[r * LD + i];
+                            K[r * LD + n] -= kri * x0;
+                            K[r * LD + n + 1] -= kri * x1;
+                        }
+                        team_sync<W>();
+                        if (lane == 0)
+                        {
+                            K[i * LD + n] = x0;
+                            K[i * LD + n + 1] = x1;
+                        }
                     }
                     team_sync<W>();
-                    if (lane == 0)
+                };
+                back_substitute();
+                if (F32)
+                {
+                    // one FP64 refinement step
+                    for (int i = lane; i < n; i += NT)
                     {
-                        K[i * LD + n] = x0;
-                        K[i * LD + n + 1] = x1;
+                        xd[i] = static_cast<double>(K[i * LD + n]);
+                        xd[NMAX + i] = static_cast<double>(K[i * LD + n + 1]);
+                        bd[i] = bd[NMAX + i] = kx[i] = kx[NMAX + i] = 0.0;
                     }
+                    team_sync<W>();
+                    cell_entries([&](int row, int col, double v) {
+                        if (col >= n)
+                            atomicAdd(bd + (col - n) * NMAX + row, v);
+                        else
+                        {
+                            atomicAdd(kx + row, v * xd[col]);
+                            atomicAdd(kx + NMAX + row, v * xd[NMAX + col]);
+                        }
+                    });
+                    for (int i = lane; i < n; i += NT)
+                    {
+                        const double b0 = bd[i], b1 = bd[NMAX + i];
+                        K[i * LD + n] = static_cast<V>((4.0 * b0 - 2.0 * b1) / ht - kx[i]);
+                        K[i * LD + n + 1] = static_cast<V>((-2.0 * b0 + 4.0 * b1) / ht - kx[NMAX + i]);
+                    }
+                    team_sync<W>();
+                    // forward elimination of the residual with the recorded pivots and the
+                    // multipliers K[i][col] / K[col][col] left below the diagonal
+                    for (int col = 0; col < n; ++col)
+                    {
+                        const int pr = piv[col];
+                        if (pr != col && lane < 2)
+                        {
+                            const V t0 = K[col * LD + n + lane];
+                            K[col * LD + n + lane] = K[pr * LD + n + lane];
+                            K[pr * LD + n + lane] = t0;
+                        }
+                        team_sync<W>();
+                        const V inv = V(1) / K[col * LD + col];
+                        const V r0 = K[col * LD + n] * inv, r1 = K[col * LD + n + 1] * inv;
+                        for (int i = col + 1 + lane; i < n; i += NT)
+                        {
+                            const V l = K[i * LD + col];
+                            K[i * LD + n] -= l * r0;
+                            K[i * LD + n + 1] -= l * r1;
+                        }
+                        team_sync<W>();
+                    }
+                    back_substitute();
+                    for (int i = lane; i < n; i += NT)
+                    {
+                        xd[i] += static_cast<double>(K[i * LD + n]);
+                        xd[NMAX + i] += static_cast<double>(K[i * LD + n + 1]);
+                    }
+                    team_sync<W>();
                 }
-                team_sync<W>();
+                auto solution = [&](int row, int kk) -> double {
+                    return F32 ? xd[kk * NMAX + row] : static_cast<double>(K[row * LD + n + kk]);
+                };
                 // flux of this patch restricted to each of its cells -> slot of the patch vertex
                 for (int t = lane; t < nc * 16; t += NT)
                 {
@@ -561,21 +643,23 @@ namespace apf
                             const double det = (g[2] - g[0]) * (g[5] - g[1]) - (g[4] - g[0]) * (g[3] - g[1]);
                             const double sn = (det < 0.0 ? -1.0 : 1.0) * sp;
                             const double cfj = m == 0 ? sn : sn * sp;
-                            val = cfj * K[(2 * pe + m) * LD + n + kk];
+                            val = cfj * solution(2 * pe + m, kk);
                         }
                     }
                     else
-                        val = K[(2 * nfree + 2 * ic + (j - 6)) * LD + n + kk];
+                        val = solution(2 * nfree + 2 * ic + (j - 6), kk);
                     A.sigma[((3ll * c + a) * 2 + kk) * 8 + j] = val;
                 }
                 team_sync<W>();
             }
         }
 
-        template<int NMAX>
+        template<int NMAX, bool F32>
         constexpr std::size_t patch_smem_bytes()
         {
-            return sizeof(double) * (kPatchTableDoubles + (kPatchTableDoubles & 1) + NMAX * (NMAX + 3));
+            return F32 ? sizeof(double) * (kPatchTableDoubles + (kPatchTableDoubles & 1) + 6 * NMAX) +
+                             sizeof(float) * NMAX * (NMAX + 3) + sizeof(int) * NMAX
+                       : sizeof(double) * (kPatchTableDoubles + (kPatchTableDoubles & 1) + NMAX * (NMAX + 3));
         }
 
         struct IndicatorArgs
@@ -1513,10 +1597,12 @@ namespace apf
     }
 
     EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
-                                double* recon, double* eta, bool out_on_device)
+                                double* recon, double* eta, bool out_on_device, int patch_precision)
     {
         SystemInputs& in = S.in;
         require(in.p == 1 || in.p == 2, APF_ERR_INVALID, "estimator: p must be 1 or 2");
+        require(patch_precision == APF_PATCH_FP64 || (patch_precision == APF_PATCH_FP32_REFINED && in.p == 1),
+                APF_ERR_INVALID, "estimator: FP32 patch solves are available for p = 1");
         require(S.solution.size() == static_cast<std::size_t>(in.n_lambda + in.n_u), APF_ERR_INVALID,
                 "estimator: solve the main system first");
         require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
@@ -1668,12 +1754,20 @@ namespace apf
                 patch_solve2<NMAX, W><<<grid, 32 * W, smem, s>>>(pa, tables2, d_order.get() + bucket_count[b], count);
                 return;
             }
-            constexpr std::size_t smem = patch_smem_bytes<NMAX>();
-            APF_CUDA(cudaFuncSetAttribute(patch_solve<NMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
-            const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32 / W)));
-            APF_KERNEL("est_patch_solve", s);
-            patch_solve<NMAX, W><<<grid, 32 * W, smem, s>>>(pa, tables, d_order.get() + bucket_count[b], count);
+            auto go = [&](auto f32) {
+                constexpr bool F32 = decltype(f32)::value;
+                constexpr std::size_t smem = patch_smem_bytes<NMAX, F32>();
+                APF_CUDA(cudaFuncSetAttribute(patch_solve<NMAX, W, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+                const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
+                const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32 / W)));
+                APF_KERNEL("est_patch_solve", s);
+                patch_solve<NMAX, W, F32><<<grid, 32 * W, smem, s>>>(pa, tables, d_order.get() + bucket_count[b], count);
+            };
+            if (patch_precision == APF_PATCH_FP32_REFINED)
+                go(std::true_type{});
+            else
+                go(std::false_type{});
         };
         if (tot.n_patches > 0)
         {
@@ -1775,8 +1869,6 @@ namespace apf
             double* sigma;    // [cell][2 slots][4]: hat L0, hat L1, bubble L0, bubble L1
             int* status;
         };
-
-        __device__ __forceinline__ double legendre1(int k, double x) { return k ? 2.0 * x - 1.0 : 1.0; }
 
         // d_x and d_t of a P1 x P1 nodal function at (xi, tau) of cell g
         __device__ __forceinline__ void nodal_grad(const double* v, const q1d::Quad& g, double xi, double tau,

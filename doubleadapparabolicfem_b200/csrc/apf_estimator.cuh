@@ -36,8 +36,9 @@ namespace apf
     // times: [n_cells][2] (t0, t1) of every cell; vids: [n_cells][3] spatial vertex ids
     void build_patches(const std::vector<double>& times, const std::vector<int>& vids, int n_cells, PatchSet& ps);
 
+    // patch_precision: APF_PATCH_FP64 or APF_PATCH_FP32_REFINED (p = 1)
     EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
-                                double* recon, double* eta, bool out_on_device);
+                                double* recon, double* eta, bool out_on_device, int patch_precision = APF_PATCH_FP64);
 
     // lambda~ of the slab reconstruction: A_y lambda~ = f - B^T u by PCG with the A_y
     // V-cycle from lambda_delta (relative residual 1e-14, at most 400 iterations)

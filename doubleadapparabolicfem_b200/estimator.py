@@ -33,7 +33,11 @@ from . import _lib
 from .assembly import MainSystemBlocks, _ptr
 
 
-def estimate(blocks: MainSystemBlocks, y_vertex_ids: np.ndarray | None = None):
+def estimate(blocks: MainSystemBlocks, y_vertex_ids: np.ndarray | None = None, patch_precision: str = "fp64"):
+    """patch_precision: "fp64" (the reference's arithmetic) or "fp32_refined" (2+1D P1:
+    FP32 patch factorisation plus one FP64 iterative-refinement step)."""
+    prec = {"fp64": _lib.APF_PATCH_FP64, "fp32_refined": _lib.APF_PATCH_FP32_REFINED}[patch_precision]
+    blocks.ctx.check(blocks.ctx.lib.apf_ctx_set_patch_precision(blocks.ctx.handle, prec))
     if getattr(blocks.problem, "dim_space", 2) == 1:
         vids = None  # 1+1D edge patches come from the cell intervals
     else:

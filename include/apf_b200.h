@@ -253,6 +253,17 @@ typedef struct apf_estimator_result
  * compute_equilibrated_flux_error_squared_by_source_cell_1plus1d
  * (time_slab_equilibrated_flux_indicators.hpp:23-190); y_vertex_ids is not used (NULL).  Output arrays ([n_y_cells] each, host or device per
  * pointers_on_device) may be NULL. */
+/* Precision of the 2+1D P1 patch solves of later apf_estimate calls on this context (no
+ * reference counterpart: the reference factors every patch in FP64):
+ *   APF_PATCH_FP64         FP64 assembly and partial-pivot LU (default);
+ *   APF_PATCH_FP32_REFINED the patch matrix assembled and factored in FP32, then one FP64
+ *                          iterative-refinement step (FP64 residual formed from the local
+ *                          entries, correction solved with the FP32 factors).
+ * p = 2 and 1+1D patches always use FP64 (APF_ERR_INVALID from apf_estimate otherwise). */
+#define APF_PATCH_FP64 0
+#define APF_PATCH_FP32_REFINED 1
+int apf_ctx_set_patch_precision(apf_ctx* ctx, int precision);
+
 int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int pointers_on_device,
                  double* flux_squared, double* divergence_squared, double* reconstruction_squared,
                  double* eta_squared, apf_estimator_result* result);

@@ -114,3 +114,23 @@ def test_x_indicators_match_published_paper_values(gpu_ctx):
         assert abs(totals["lambda_y_squared"] - lam) <= 1e-5 * lam, (level, totals, lam)
         assert abs(totals["eta_squared"] - eta) <= 1e-5 * eta, (level, totals, eta)
         blocks.close()
+
+
+def test_fp32_refined_patch_solves_match_fp64(gpu_ctx):
+    """The FP32 patch factorisation with one FP64 refinement step against the FP64 path on
+    the same solution (outer level 3 and 4, P1): per-cell flux^2 / div^2 / eta^2 within 1e-9 of
+    the largest cell value, totals within 1e-10 relative (measured errors are printed)."""
+    from doubleadapparabolicfem_b200.estimator import estimate
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    for level in (3, 4):
+        blocks, (c64, t64) = _solve_and_estimate(gpu_ctx, uniform_problem(level, 1), tol=1e-10)
+        c32, t32 = estimate(blocks, patch_precision="fp32_refined")
+        estimate(blocks)  # leave the context on FP64
+        for key in ("flux", "divergence", "eta"):
+            scale = np.abs(c64["flux"]).max()
+            err = np.abs(c32[key] - c64[key]).max() / scale
+            print(f"level {level} {key}: max |fp32_refined - fp64| / max cell = {err:.3e}")
+            assert err <= 1e-9, (level, key, err)
+        rel = abs(t32["flux_squared"] - t64["flux_squared"]) / t64["flux_squared"]
+        print(f"level {level} flux total relative difference {rel:.3e}")
+        assert rel <= 1e-10
