@@ -565,6 +565,7 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
         mo.tolerance = opt->tolerance;
         mo.max_iterations = opt->max_iterations;
         mo.batch = opt->use_true_residual_batching ? opt->true_residual_check_interval : opt->max_iterations;
+        mo.parts = S.partition.n_parts > 0 ? &S.partition : nullptr;
         const auto t0 = std::chrono::steady_clock::now();
         summary = apf::minres_solve(s, S.blocks[APF_BLOCK_K], *S.precond, S.rhs.get(), S.solution.get(), mo, S.ws);
         used = S.precond_kind;
@@ -589,6 +590,7 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
     if (diag)
     {
         *diag = apf_solver_diagnostics{};
+        sys->sys.part_residuals = summary.part_residuals;
         diag->iterations = summary.iterations;
         diag->residual_check_batches = summary.batches;
         diag->converged = summary.converged ? 1 : 0;
@@ -643,6 +645,45 @@ int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const dou
                                  pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
         apf::sync(s);
     });
+}
+
+int apf_system_set_partition(apf_ctx* ctx, apf_system* sys, int n_parts, const int32_t* lambda_offsets,
+                             const int32_t* u_offsets)
+{
+    if (!ctx || !sys || n_parts < 0 || (n_parts > 0 && (!lambda_offsets || !u_offsets)))
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        auto& S = sys->sys;
+        const int nl = S.in.n_lambda, nu = S.in.n_u;
+        std::vector<int2> segs(2 * static_cast<std::size_t>(n_parts));
+        if (n_parts > 0)
+            apf::require(lambda_offsets[0] == 0 && u_offsets[0] == 0 && lambda_offsets[n_parts] == nl &&
+                             u_offsets[n_parts] == nu,
+                         APF_ERR_INVALID, "partition offsets must start at 0 and end at n_lambda / n_u");
+        for (int p = 0; p < n_parts; ++p)
+        {
+            apf::require(lambda_offsets[p] <= lambda_offsets[p + 1] && u_offsets[p] <= u_offsets[p + 1],
+                         APF_ERR_INVALID, "partition offsets must not decrease");
+            segs[2 * p] = make_int2(lambda_offsets[p], lambda_offsets[p + 1]);
+            segs[2 * p + 1] = make_int2(nl + u_offsets[p], nl + u_offsets[p + 1]);
+        }
+        S.partition.n_parts = n_parts;
+        S.partition.segs.allocate(std::max<std::size_t>(segs.size(), 1), ctx->stream);
+        if (!segs.empty())
+            S.partition.segs.upload(segs.data(), segs.size());
+        S.part_residuals.clear();
+    });
+}
+
+int apf_system_part_residuals(apf_ctx* ctx, const apf_system* sys, double* out)
+{
+    if (!ctx || !sys || !out)
+        return APF_ERR_INVALID;
+    const auto& r = sys->sys.part_residuals;
+    if (static_cast<int>(r.size()) != sys->sys.partition.n_parts)
+        return APF_ERR_INVALID;
+    std::copy(r.begin(), r.end(), out);
+    return APF_OK;
 }
 
 int apf_ctx_set_patch_precision(apf_ctx* ctx, int precision)

@@ -1376,20 +1376,25 @@ namespace apf
     // ---------------------------------------------------------------------------
     void build_patches(const std::vector<double>& times, const std::vector<int>& vids, int n_cells, PatchSet& ps)
     {
-        // slabs by the exact start time of their cells (mesh times are dyadic)
-        std::vector<double> key(n_cells);
-        for (int c = 0; c < n_cells; ++c)
-            key[c] = times[2ll * c];
+        // slabs by the exact time interval of their cells (mesh times are dyadic; stacked
+        // independent problems may share a start time with different steps)
+        auto less = [&](int a, int b) {
+            const double a0 = times[2ll * a], b0 = times[2ll * b];
+            return a0 < b0 || (a0 == b0 && times[2ll * a + 1] < times[2ll * b + 1]);
+        };
+        auto same = [&](int a, int b) {
+            return times[2ll * a] == times[2ll * b] && times[2ll * a + 1] == times[2ll * b + 1];
+        };
         std::vector<int> order(n_cells);
         std::iota(order.begin(), order.end(), 0);
-        if (!std::is_sorted(key.begin(), key.end())) // cells usually come slab by slab
-            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+        if (!std::is_sorted(order.begin(), order.end(), less)) // cells usually come slab by slab
+            std::stable_sort(order.begin(), order.end(), less);
         ps.slab_ptr.assign(1, 0);
         ps.slab_cells.clear();
         ps.slab_cells.reserve(n_cells);
         for (int i = 0; i < n_cells; ++i)
         {
-            if (i > 0 && key[order[i]] != key[order[i - 1]])
+            if (i > 0 && !same(order[i], order[i - 1]))
                 ps.slab_ptr.push_back(i);
             ps.slab_cells.push_back(order[i]);
         }

@@ -116,6 +116,37 @@ namespace apf
             return !(t_profiler && t_profiler->enabled && t_profiler->kernels);
         }
 
+        // sum of squares of v over each segment (one block per segment, fixed order)
+        __global__ void k_segment_sumsq(const int2* __restrict__ segs, const double* __restrict__ v,
+                                        double* __restrict__ out)
+        {
+            const int2 r = segs[blockIdx.x];
+            double acc = 0.0;
+            for (int i = r.x + threadIdx.x; i < r.y; i += blockDim.x)
+                acc += v[i] * v[i];
+            const double t = block_sum(acc);
+            if (threadIdx.x == 0)
+                out[blockIdx.x] = t;
+        }
+
+        std::vector<double> part_norms2(cudaStream_t s, const Partition& P, const double* v, DeviceBuffer<double>& tmp)
+        {
+            const int nseg = 2 * P.n_parts;
+            std::vector<double> seg(static_cast<std::size_t>(nseg)), out(static_cast<std::size_t>(P.n_parts));
+            if (nseg == 0)
+                return out;
+            {
+                APF_KERNEL("minres_part_norms", s);
+                k_segment_sumsq<<<nseg, kThreads, 0, s>>>(P.segs.get(), v, tmp.get());
+            }
+            APF_CUDA(cudaGetLastError());
+            APF_CUDA(cudaMemcpyAsync(seg.data(), tmp.get(), nseg * sizeof(double), cudaMemcpyDeviceToHost, s));
+            sync(s);
+            for (int p = 0; p < P.n_parts; ++p)
+                out[p] = seg[2 * p] + seg[2 * p + 1];
+            return out;
+        }
+
         __global__ void k_vscale(int n, const double* __restrict__ z, double* __restrict__ v, const MinresDev* S)
         {
             if (S->done)
@@ -403,9 +434,26 @@ namespace apf
             sum.true_residual = 0.0;
             return sum;
         }
+        DeviceBuffer<double> seg_tmp(opt.parts ? 2 * std::max(1, opt.parts->n_parts) : 1, s);
+        std::vector<double> part_b2;
+        if (opt.parts)
+            part_b2 = part_norms2(s, *opt.parts, b, seg_tmp);
         auto true_residual = [&]() {
             residual(s, K, x, b, res.get());
-            return std::sqrt(dot_host(s, w, n, res.get(), res.get())) / bn;
+            const double rel = std::sqrt(dot_host(s, w, n, res.get(), res.get())) / bn;
+            if (!opt.parts)
+                return rel;
+            // every stacked problem must meet the tolerance on its own
+            const std::vector<double> r2 = part_norms2(s, *opt.parts, res.get(), seg_tmp);
+            sum.part_residuals.assign(r2.size(), 0.0);
+            double worst = 0.0;
+            for (std::size_t p = 0; p < r2.size(); ++p)
+            {
+                const double v = part_b2[p] > 0.0 ? std::sqrt(r2[p] / part_b2[p]) : std::sqrt(r2[p]);
+                sum.part_residuals[p] = v;
+                worst = std::max(worst, std::isfinite(v) ? v : std::numeric_limits<double>::infinity());
+            }
+            return std::max(rel, worst);
         };
         const int limit = std::max(1, opt.max_iterations);
         const int batch = std::min(limit, std::max(1, opt.batch));

@@ -1,6 +1,8 @@
 // Block-preconditioned MINRES on the device (see apf_minres.cu).
 #pragma once
 
+#include <vector>
+
 #include "apf_amg.cuh"
 
 namespace apf
@@ -37,11 +39,21 @@ namespace apf
         cudaEvent_t fork_ = nullptr, join_ = nullptr;
     };
 
+    // Independent problems stacked block-diagonally in K: segment 2p covers part p's lambda
+    // rows, segment 2p + 1 its u rows (offsets into the full vector).  With a partition the
+    // true-residual acceptance uses the largest per-part relative residual.
+    struct Partition
+    {
+        int n_parts = 0;
+        DeviceBuffer<int2> segs; // [2 n_parts] (begin, end)
+    };
+
     struct MinresOptions
     {
         double tolerance = 1e-8;
         int max_iterations = 20000;
         int batch = 100; // true_residual_check_interval (0 or negative: no batching)
+        const Partition* parts = nullptr;
     };
 
     struct MinresSummary
@@ -52,6 +64,7 @@ namespace apf
         bool backend_converged = false;
         double true_residual = 0.0;
         bool converged = false;
+        std::vector<double> part_residuals; // per part, with a partition
     };
 
     MinresSummary minres_solve(cudaStream_t s, const DeviceCsr& K, Preconditioner& P, const double* b, double* x,

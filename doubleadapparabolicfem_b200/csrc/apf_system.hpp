@@ -63,6 +63,8 @@ namespace apf
         double precond_setup_seconds = 0.0;
         int precond_kind = -1;                    // APF_PRECOND_* installed in precond's V-cycles
         unsigned long long precond_model_version = 0; // learned model the weights came from
+        Partition partition;                 // stacked independent problems (apf_system_set_partition)
+        std::vector<double> part_residuals;  // per-part true relative residuals of the last solve
     };
 
     void upload_tables_once(int device);

@@ -253,6 +253,20 @@ typedef struct apf_estimator_result
  * compute_equilibrated_flux_error_squared_by_source_cell_1plus1d
  * (time_slab_equilibrated_flux_indicators.hpp:23-190); y_vertex_ids is not used (NULL).  Output arrays ([n_y_cells] each, host or device per
  * pointers_on_device) may be NULL. */
+/* ---- batches of independent problems ----------------------------------------------- */
+/* Several independent problems assembled as one system (their cells, DOFs and vertex ids
+ * concatenated with offsets, so every stage runs over all of them in one launch): part p
+ * owns lambda rows [lambda_offsets[p], lambda_offsets[p+1]) and u rows
+ * [u_offsets[p], u_offsets[p+1]) (host arrays of n_parts + 1, starting at 0, ending at
+ * n_lambda / n_u).  No reference counterpart (a batching form; the reference solves one
+ * problem per call).  Later apf_solve_minres calls accept the solve only when every part's
+ * ||b_p - K_p x_p|| / ||b_p|| <= tolerance, the reference's acceptance test
+ * (iterative_residual_acceptance.hpp:32-54) per problem; apf_system_part_residuals copies
+ * those residuals of the last solve (n_parts doubles, host).  n_parts = 0 clears it. */
+int apf_system_set_partition(apf_ctx* ctx, apf_system* sys, int n_parts, const int32_t* lambda_offsets,
+                             const int32_t* u_offsets);
+int apf_system_part_residuals(apf_ctx* ctx, const apf_system* sys, double* out);
+
 /* Precision of the 2+1D P1 patch solves of later apf_estimate calls on this context (no
  * reference counterpart: the reference factors every patch in FP64):
  *   APF_PATCH_FP64         FP64 assembly and partial-pivot LU (default);

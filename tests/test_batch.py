@@ -1,0 +1,61 @@
+"""Batches of independent problems stacked into one system (doubleadapparabolicfem_b200/batch.py).
+
+CPU: the stacked problem assembles (oracle restatement) to the block-diagonal union of the
+problems' own blocks.  GPU: a seeded batch with piecewise-constant kappa, solved and
+estimated as one stacked system, against every problem solved on its own (FP64 path):
+each problem's own true relative residual meets the tolerance, per-cell indicators agree
+to 1e-9 of the problem's largest cell value; the FP32-refined patch solves agree with the
+FP64 path to 1e-9 of the largest cell value.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import assert_same_sparse
+
+import apf_oracle as O
+
+
+def _oracle(prob):
+    return O.MainProblem(p=prob.p, y_geom=prob.y_geometry, x_geom=prob.x_geometry, y_to_x=prob.y_to_x,
+                         y_restr=O.Restriction(prob.y_restriction.offsets, prob.y_restriction.dofs,
+                                               prob.y_restriction.weights, prob.ndof),
+                         x_restr=O.Restriction(prob.x_restriction.offsets, prob.x_restriction.dofs,
+                                               prob.x_restriction.weights, prob.ndof),
+                         n_lambda=prob.n_lambda, n_u=prob.n_u, m_cells=prob.m_cells)
+
+
+def test_stacked_problem_is_the_block_diagonal_union():
+    from doubleadapparabolicfem_b200.batch import random_batch, stack
+    problems = random_batch(3, seed=5, cells=(200, 5000))
+    stacked, off = stack(problems)
+    whole = O.assemble_main_blocks(_oracle(stacked))
+    parts = [O.assemble_main_blocks(_oracle(q)) for q in problems]
+    for nm in ("A_y", "B", "C_signed"):
+        assert_same_sparse(sp.block_diag([p[nm] for p in parts]), whole[nm], 1e-14, nm)
+    assert np.array_equal(np.concatenate([p["g"] for p in parts]), whole["g"])
+    assert off["lambda"][-1] == stacked.n_lambda and off["u"][-1] == stacked.n_u
+
+
+@pytest.mark.gpu
+def test_batched_solve_and_estimate_match_single_problems(gpu_ctx):
+    from doubleadapparabolicfem_b200.assembly import assemble_main_system_blocks
+    from doubleadapparabolicfem_b200.batch import random_batch, solve_batch
+    from doubleadapparabolicfem_b200.estimator import estimate
+    from doubleadapparabolicfem_b200.solver import SolverOptions, solve_saddle_system_with_preconditioner
+    problems = random_batch(5, seed=3, cells=(300, 40000))
+    tol = 1e-11
+    res, stats = solve_batch(problems, gpu_ctx, tol=tol, patch_precision="fp64", keep_cells=True)
+    assert len(stats) == 1 and stats[0]["problems"] == 5
+    res32, _ = solve_batch(problems, gpu_ctx, tol=tol, patch_precision="fp32_refined", keep_cells=True)
+    for q, r, r32 in zip(problems, res, res32):
+        assert r["residual"] <= tol
+        blocks = assemble_main_system_blocks(q, ctx=gpu_ctx)
+        blocks.assemble_parabolic_graph_norm_approximation()
+        _, diag = solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=tol), copy_out=False)
+        cells, _ = estimate(blocks)
+        blocks.close()
+        scale = np.abs(cells["flux"]).max()
+        for key in ("flux", "divergence", "eta"):
+            assert np.abs(r[key] - cells[key]).max() <= 1e-9 * scale, (q.meta, key)
+            assert np.abs(r32[key] - r[key]).max() <= 1e-9 * scale, (q.meta, key, "fp32")
