@@ -110,6 +110,8 @@ SIGNATURES = {
     "apf_ctx_kernel_launches": ([C.c_void_p], C.c_int64),
     "apf_ctx_set_timing": ([C.c_void_p, C.c_int], C.c_int),
     "apf_ctx_set_patch_precision": ([C.c_void_p, C.c_int], C.c_int),
+    "apf_ctx_set_autotune": ([C.c_void_p, C.c_int], C.c_int),
+    "apf_ctx_autotune_report": ([C.c_void_p], C.c_char_p),
     "apf_system_set_partition": ([C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
     "apf_system_part_residuals": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "apf_ctx_timing_report": ([C.c_void_p], C.c_char_p),

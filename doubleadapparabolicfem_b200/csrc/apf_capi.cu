@@ -24,6 +24,8 @@ struct apf_ctx
     std::unique_ptr<apf::LearnedModel> learned; // model of APF_PRECOND_LEARNED set-ups
     unsigned long long learned_version = 0;
     int patch_precision = APF_PATCH_FP64; // apf_ctx_set_patch_precision
+    apf::PatchTuner tuner;                // apf_ctx_set_autotune
+    std::string tune_report;
 };
 
 struct apf_learned_model
@@ -686,6 +688,43 @@ int apf_system_part_residuals(apf_ctx* ctx, const apf_system* sys, double* out)
     return APF_OK;
 }
 
+int apf_ctx_set_autotune(apf_ctx* ctx, int enable)
+{
+    if (!ctx)
+        return APF_ERR_INVALID;
+    ctx->tuner.enabled = enable != 0;
+    if (enable < 0)
+        ctx->tuner = apf::PatchTuner{};
+    return APF_OK;
+}
+
+const char* apf_ctx_autotune_report(apf_ctx* ctx)
+{
+    if (!ctx)
+        return "";
+    std::string r = "{";
+    bool first = true;
+    const auto& t = ctx->tuner;
+    for (int p = 0; p < 2; ++p)
+        for (int f = 0; f < 2; ++f)
+            for (int b = 0; b < 5; ++b)
+            {
+                if (t.width[p][f][b] == 0)
+                    continue;
+                char buf[256];
+                std::snprintf(buf, sizeof(buf),
+                              "%s\"p%d_%s_n%d\": {\"warps_per_patch\": %d, \"patches\": %d, \"ms_w1_w2_w4\": [%.3f, %.3f, %.3f]}",
+                              first ? "" : ", ", p + 1, f ? "fp32_refined" : "fp64", apf::kPatchBucketMax[b],
+                              t.width[p][f][b], t.patches[p][f][b], t.ms[p][f][b][0], t.ms[p][f][b][1],
+                              t.ms[p][f][b][2]);
+                r += buf;
+                first = false;
+            }
+    r += "}";
+    ctx->tune_report = r;
+    return ctx->tune_report.c_str();
+}
+
 int apf_ctx_set_patch_precision(apf_ctx* ctx, int precision)
 {
     if (!ctx || (precision != APF_PATCH_FP64 && precision != APF_PATCH_FP32_REFINED))
@@ -719,7 +758,7 @@ int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int
                                          ctx->stream));
             apf::sync(ctx->stream);
             t = apf::estimate(ctx->stream, S, vids, flux_squared, divergence_squared, reconstruction_squared,
-                              eta_squared, pointers_on_device != 0, ctx->patch_precision);
+                              eta_squared, pointers_on_device != 0, ctx->patch_precision, &ctx->tuner);
         }
         if (result)
         {

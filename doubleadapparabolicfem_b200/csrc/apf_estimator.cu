@@ -1602,7 +1602,8 @@ namespace apf
     }
 
     EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
-                                double* recon, double* eta, bool out_on_device, int patch_precision)
+                                double* recon, double* eta, bool out_on_device, int patch_precision,
+                                PatchTuner* tuner)
     {
         SystemInputs& in = S.in;
         require(in.p == 1 || in.p == 2, APF_ERR_INVALID, "estimator: p must be 1 or 2");
@@ -1741,26 +1742,38 @@ namespace apf
         }
         // one team of W warps per patch: larger patches get more warps (the LU's column
         // updates and the assembly spread over 32 W threads; shared memory bounds the teams
-        // per SM)
+        // per SM).  W per (degree, precision, bucket) comes from the context's autotuner when
+        // it is on (every candidate timed once on the bucket's own patches; all candidates
+        // compute the same values in the same order), else from the size rule below.
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        const bool tuning = tuner && tuner->enabled;
+        if (tuning)
+        {
+            APF_CUDA(cudaEventCreate(&ev0));
+            APF_CUDA(cudaEventCreate(&ev1));
+        }
         auto launch = [&](auto tag, int b) {
             constexpr int NMAX = decltype(tag)::value;
-            constexpr int W = NMAX <= 48 ? 1 : (NMAX <= 64 ? 2 : 4);
+            constexpr int W_RULE = NMAX <= 48 ? 1 : (NMAX <= 64 ? 2 : 4);
             const int count = bucket_count[b + 1] - bucket_count[b];
             if (count == 0)
                 return;
             pa.nmax = NMAX;
-            if (p2)
-            {
-                constexpr std::size_t smem = patch2_smem_bytes<NMAX>();
-                APF_CUDA(cudaFuncSetAttribute(patch_solve2<NMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
-                const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32 / W)));
-                APF_KERNEL("est_patch_solve", s);
-                patch_solve2<NMAX, W><<<grid, 32 * W, smem, s>>>(pa, tables2, d_order.get() + bucket_count[b], count);
-                return;
-            }
-            auto go = [&](auto f32) {
-                constexpr bool F32 = decltype(f32)::value;
+            const bool f32 = patch_precision == APF_PATCH_FP32_REFINED;
+            auto run = [&](auto wtag, auto f32tag) {
+                constexpr int W = decltype(wtag)::value;
+                constexpr bool F32 = decltype(f32tag)::value;
+                if (p2)
+                {
+                    constexpr std::size_t smem = patch2_smem_bytes<NMAX>();
+                    APF_CUDA(cudaFuncSetAttribute(patch_solve2<NMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smem));
+                    const int per_sm = std::max<int>(1, static_cast<int>((227u * 1024u) / (smem + 1024u)));
+                    const int grid = std::max(1, std::min(count, 148 * std::min(per_sm, 32 / W)));
+                    APF_KERNEL("est_patch_solve", s);
+                    patch_solve2<NMAX, W><<<grid, 32 * W, smem, s>>>(pa, tables2, d_order.get() + bucket_count[b], count);
+                    return;
+                }
                 constexpr std::size_t smem = patch_smem_bytes<NMAX, F32>();
                 APF_CUDA(cudaFuncSetAttribute(patch_solve<NMAX, W, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)smem));
@@ -1769,10 +1782,45 @@ namespace apf
                 APF_KERNEL("est_patch_solve", s);
                 patch_solve<NMAX, W, F32><<<grid, 32 * W, smem, s>>>(pa, tables, d_order.get() + bucket_count[b], count);
             };
-            if (patch_precision == APF_PATCH_FP32_REFINED)
-                go(std::true_type{});
-            else
-                go(std::false_type{});
+            auto run_w = [&](int w) {
+                auto with_w = [&](auto wtag) {
+                    if (f32 && !p2)
+                        run(wtag, std::true_type{});
+                    else
+                        run(wtag, std::false_type{});
+                };
+                if (w == 1)
+                    with_w(std::integral_constant<int, 1>{});
+                else if (w == 2)
+                    with_w(std::integral_constant<int, 2>{});
+                else
+                    with_w(std::integral_constant<int, 4>{});
+                APF_CUDA(cudaGetLastError());
+            };
+            int* choice = tuner ? &tuner->width[p2 ? 1 : 0][f32 ? 1 : 0][b] : nullptr;
+            if (tuning && *choice == 0)
+            {
+                static constexpr int kCand[3] = {1, 2, 4};
+                float best = 0.0f;
+                for (int k = 0; k < 3; ++k)
+                {
+                    APF_CUDA(cudaEventRecord(ev0, s));
+                    run_w(kCand[k]);
+                    APF_CUDA(cudaEventRecord(ev1, s));
+                    APF_CUDA(cudaEventSynchronize(ev1));
+                    float ms = 0.0f;
+                    APF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+                    tuner->ms[p2 ? 1 : 0][f32 ? 1 : 0][b][k] = ms;
+                    tuner->patches[p2 ? 1 : 0][f32 ? 1 : 0][b] = count;
+                    if (k == 0 || ms < best)
+                    {
+                        best = ms;
+                        *choice = kCand[k];
+                    }
+                }
+                return;
+            }
+            run_w(choice && *choice ? *choice : W_RULE);
         };
         if (tot.n_patches > 0)
         {
@@ -1783,6 +1831,10 @@ namespace apf
             launch(std::integral_constant<int, 144>{}, 4);
             APF_CUDA(cudaGetLastError());
         }
+        if (ev0)
+            cudaEventDestroy(ev0);
+        if (ev1)
+            cudaEventDestroy(ev1);
         int hstat = 0;
         APF_CUDA(cudaMemcpyAsync(&hstat, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         sync(s);

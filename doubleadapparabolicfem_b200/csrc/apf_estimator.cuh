@@ -36,9 +36,23 @@ namespace apf
     // times: [n_cells][2] (t0, t1) of every cell; vids: [n_cells][3] spatial vertex ids
     void build_patches(const std::vector<double>& times, const std::vector<int>& vids, int n_cells, PatchSet& ps);
 
+    // Launch-shape autotuner of the patch solves (one per context): for every (degree,
+    // precision, patch-size bucket) the first estimate that meets it times the candidate
+    // team widths (1, 2, 4 warps per patch) on that bucket's own patches and keeps the
+    // fastest; later estimates reuse the choice.
+    struct PatchTuner
+    {
+        bool enabled = true;
+        int width[2][2][5] = {};     // [p - 1][FP32][bucket] -> warps per patch (0: not tuned)
+        float ms[2][2][5][3] = {};   // candidate times of the tuning launch
+        int patches[2][2][5] = {};   // patches in the bucket when it was tuned
+    };
+    constexpr int kPatchBucketMax[5] = {32, 48, 64, 96, 144};
+
     // patch_precision: APF_PATCH_FP64 or APF_PATCH_FP32_REFINED (p = 1)
     EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
-                                double* recon, double* eta, bool out_on_device, int patch_precision = APF_PATCH_FP64);
+                                double* recon, double* eta, bool out_on_device, int patch_precision = APF_PATCH_FP64,
+                                PatchTuner* tuner = nullptr);
 
     // lambda~ of the slab reconstruction: A_y lambda~ = f - B^T u by PCG with the A_y
     // V-cycle from lambda_delta (relative residual 1e-14, at most 400 iterations)

@@ -278,6 +278,19 @@ int apf_system_part_residuals(apf_ctx* ctx, const apf_system* sys, double* out);
 #define APF_PATCH_FP32_REFINED 1
 int apf_ctx_set_patch_precision(apf_ctx* ctx, int precision);
 
+/* Launch-shape autotuner of the patch solves (no reference counterpart): patches are
+ * sorted into size buckets (at most 32, 48, 64, 96, 144 unknowns) and every bucket is
+ * solved by teams of W warps per patch.  With autotuning on (the default) the first
+ * apf_estimate that meets a (degree, precision, bucket) times W = 1, 2 and 4 on that
+ * bucket's own patches and keeps the fastest for the context; the values do not depend on
+ * W.  enable = 0 uses the kept choices (or the size rule W = 1 / 2 / 4 for buckets up to
+ * 48 / 64 / larger where none was made), enable < 0 forgets them and turns tuning on.
+ * The report is a JSON
+ * object {"p1_fp64_n64": {"warps_per_patch": 2, "patches": ..., "ms_w1_w2_w4": [...]}, ...},
+ * valid until the next call. */
+int apf_ctx_set_autotune(apf_ctx* ctx, int enable);
+const char* apf_ctx_autotune_report(apf_ctx* ctx);
+
 int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int pointers_on_device,
                  double* flux_squared, double* divergence_squared, double* reconstruction_squared,
                  double* eta_squared, apf_estimator_result* result);

@@ -134,3 +134,25 @@ def test_fp32_refined_patch_solves_match_fp64(gpu_ctx):
         rel = abs(t32["flux_squared"] - t64["flux_squared"]) / t64["flux_squared"]
         print(f"level {level} flux total relative difference {rel:.3e}")
         assert rel <= 1e-10
+
+
+def test_autotuned_patch_launch_shapes_give_identical_indicators(gpu_ctx):
+    """The autotuner times teams of 1, 2 and 4 warps per patch on every bucket and keeps
+    the fastest; the indicators do not depend on the team width (bit-identical)."""
+    import json as _json
+    from doubleadapparabolicfem_b200.estimator import estimate
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    ctx = gpu_ctx
+    blocks, (ref_cells, _) = _solve_and_estimate(ctx, uniform_problem(3, 1), tol=1e-10)
+    for mode in (-1, 0):  # forget the choices and tune again; then reuse the kept choices
+        ctx.check(ctx.lib.apf_ctx_set_autotune(ctx.handle, mode))
+        cells, _ = estimate(blocks)
+        for key in ("flux", "divergence", "eta"):
+            assert np.array_equal(cells[key], ref_cells[key]), (mode, key)
+    ctx.check(ctx.lib.apf_ctx_set_autotune(ctx.handle, -1))
+    ctx.check(ctx.lib.apf_ctx_set_autotune(ctx.handle, 1))
+    cells, _ = estimate(blocks)
+    report = _json.loads(ctx.lib.apf_ctx_autotune_report(ctx.handle).decode())
+    assert report and all(v["warps_per_patch"] in (1, 2, 4) for v in report.values())
+    for key in ("flux", "divergence", "eta"):
+        assert np.array_equal(cells[key], ref_cells[key]), key
