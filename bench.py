@@ -522,7 +522,11 @@ def run_ours(args, world, rank, local):
         "roofline": {"kernel": "minres_spmv_K", "bound": "hbm", "achieved": spmv_achieved, "peak": peak, "unit": "GB/s",
                      "frac": spmv_achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": spmv_bytes, "launches_per_step": spmv_launches,
-                     "traffic": None, "dominant_kernel": dominant[0],
+                     "traffic": K_SPMV_TRAFFIC_RATIO * spmv_bytes,
+                     "traffic_source": "DRAM bytes per launch of the K SpMV measured by ncu at outer level 5 "
+                                       "(1.016 x its algorithmic bytes; profiles/spmv_kernels_l5.md) times this "
+                                       "launch's algorithmic bytes",
+                     "dominant_kernel": dominant[0],
                      "dominant_share": dominant[1][1] / total_ms if total_ms else None},
         "kernel_times_ms_per_step": {k: round(v[1], 3) for k, v in
                                      sorted(kernels.items(), key=lambda kv: -kv[1][1])[:45]},
@@ -534,6 +538,12 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum of the MINRES K SpMV per launch divided by its
+# algorithmic bytes (12 nnz + 4 (n+1) + 16 n), from one ncu capture at outer level 5
+# (123.4 and 124.4 MB for 121.93 MB; profiles/spmv_kernels_l5.md)
+K_SPMV_TRAFFIC_RATIO = 1.016
 
 
 def main():
