@@ -524,8 +524,7 @@ def run_ours(args, world, rank, local):
                      "algorithmic_bytes_per_launch": spmv_bytes, "launches_per_step": spmv_launches,
                      "traffic": K_SPMV_TRAFFIC_RATIO * spmv_bytes,
                      "traffic_source": "DRAM bytes per launch of the K SpMV measured by ncu at outer level 5 "
-                                       "(1.016 x its algorithmic bytes; profiles/spmv_kernels_l5.md) times this "
-                                       "launch's algorithmic bytes",
+                                       "(1.016 x its algorithmic bytes) times this launch's algorithmic bytes",
                      "dominant_kernel": dominant[0],
                      "dominant_share": dominant[1][1] / total_ms if total_ms else None},
         "kernel_times_ms_per_step": {k: round(v[1], 3) for k, v in
@@ -542,7 +541,7 @@ def run_ours(args, world, rank, local):
 
 # dram__bytes_read.sum + dram__bytes_write.sum of the MINRES K SpMV per launch divided by its
 # algorithmic bytes (12 nnz + 4 (n+1) + 16 n), from one ncu capture at outer level 5
-# (123.4 and 124.4 MB for 121.93 MB; profiles/spmv_kernels_l5.md)
+# (123.4 and 124.4 MB for 121.93 MB)
 K_SPMV_TRAFFIC_RATIO = 1.016
 
 
