@@ -314,66 +314,111 @@ namespace apf
             int nlist;
         };
 
-        template<int CAP, bool FILL>
+        // One warp per row of A B with at most CAP candidate products.  The distinct columns
+        // are collected in a shared-memory hash set (open addressing, at most half full), only
+        // those are sorted, and each product is then added to its column's accumulator in
+        // generation order (A's row order, then B's row order: one product per column per A
+        // entry, so lanes never collide), which is the order a stable sort of the candidates
+        // would sum them in.  Output: the row's sorted distinct columns and sums at cp[row],
+        // their number in count[row].
+        // shared memory per warp: table keys int[2 CAP], ranks int[2 CAP], sorted keys /
+        // accumulators 8 B x CAP
+        __device__ __forceinline__ unsigned hash_slot(int col, int hbits)
+        {
+            return (static_cast<unsigned>(col) * 2654435761u) >> (32 - hbits);
+        }
+
+        template<int CAP>
         __global__ void __launch_bounds__(256) spgemm_rows(GemmArgs A)
         {
             extern __shared__ unsigned char smem_raw[];
             const int warps = blockDim.x >> 5;
             const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-            unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
-            double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
-                           (size_t)w * CAP;
+            int* tkeys = reinterpret_cast<int*>(smem_raw) + (size_t)w * (2 * CAP);
+            int* tranks = reinterpret_cast<int*>(smem_raw) + (size_t)warps * (2 * CAP) + (size_t)w * (2 * CAP);
+            unsigned long long* ukeys =
+                reinterpret_cast<unsigned long long*>(reinterpret_cast<int*>(smem_raw) + (size_t)warps * (4 * CAP)) +
+                (size_t)w * CAP;
+            double* acc = reinterpret_cast<double*>(ukeys);
             const int nrows = A.list ? A.nlist : A.rows;
             for (int idx = blockIdx.x * warps + w; idx < nrows; idx += gridDim.x * warps)
             {
                 const int row = A.list ? A.list[idx] : idx;
-                int n = 0, seq = 0;
+                int n = 0;
+                for (int k = A.ap[row]; k < A.ap[row + 1]; ++k)
+                    n += A.bp[A.ac[k] + 1] - A.bp[A.ac[k]];
+                int hbits = 6;
+                while ((1 << hbits) < 2 * n)
+                    ++hbits;
+                const int H = 1 << hbits;
+                for (int t = lane; t < H; t += 32)
+                    tkeys[t] = -1;
+                __syncwarp();
+                // distinct columns
+                for (int k = A.ap[row]; k < A.ap[row + 1]; ++k)
+                {
+                    const int j = A.ac[k];
+                    for (int q = A.bp[j] + lane; q < A.bp[j + 1]; q += 32)
+                    {
+                        const int col = A.bc[q];
+                        unsigned h = hash_slot(col, hbits);
+                        while (true)
+                        {
+                            const int prev = atomicCAS(tkeys + h, -1, col);
+                            if (prev == -1 || prev == col)
+                                break;
+                            h = (h + 1) & (H - 1);
+                        }
+                    }
+                }
+                __syncwarp();
+                // compact and sort them: key = column (high) | table slot (low)
+                int u = 0;
+                for (int t0 = 0; t0 < H; t0 += 32)
+                {
+                    const int t = t0 + lane;
+                    const int key = tkeys[t];
+                    const unsigned m = __ballot_sync(0xffffffffu, key != -1);
+                    if (key != -1)
+                        ukeys[u + __popc(m & ((1u << lane) - 1))] =
+                            (static_cast<unsigned long long>(static_cast<unsigned>(key)) << 32) | static_cast<unsigned>(t);
+                    u += __popc(m);
+                }
+                const int np = next_pow2(u);
+                for (int k = u + lane; k < np; k += 32)
+                    ukeys[k] = ~0ull;
+                __syncwarp();
+                warp_bitonic_sort(ukeys, np);
+                const int base = A.cp[row];
+                for (int k = lane; k < u; k += 32)
+                {
+                    const unsigned long long key = ukeys[k];
+                    tranks[static_cast<unsigned>(key)] = k;
+                    A.cc[base + k] = static_cast<int>(key >> 32);
+                }
+                __syncwarp();
+                for (int k = lane; k < u; k += 32)
+                    acc[k] = 0.0;
+                __syncwarp();
+                // sums in generation order
                 for (int k = A.ap[row]; k < A.ap[row + 1]; ++k)
                 {
                     const int j = A.ac[k];
                     const double a = A.av[k];
-                    const int b = A.bp[j], e = A.bp[j + 1];
-                    for (int q = b + lane; q < e; q += 32)
+                    for (int q = A.bp[j] + lane; q < A.bp[j + 1]; q += 32)
                     {
-                        const int slot = n + (q - b);
-                        keys[slot] = make_key(A.bc[q], seq + (q - b), slot);
-                        vals[slot] = a * A.bv[q];
+                        const int col = A.bc[q];
+                        unsigned h = hash_slot(col, hbits);
+                        while (tkeys[h] != col)
+                            h = (h + 1) & (H - 1);
+                        acc[tranks[h]] += a * A.bv[q];
                     }
-                    n += e - b;
-                    seq += e - b;
+                    __syncwarp();
                 }
-                __syncwarp();
-                const int np = next_pow2(n);
-                for (int k = n + lane; k < np; k += 32)
-                    keys[k] = ~0ull;
-                __syncwarp();
-                warp_bitonic_sort(keys, np);
-                const int base = FILL ? A.cp[row] : 0;
-                int uniq = 0;
-                for (int k0 = 0; k0 < n; k0 += 32)
-                {
-                    const int k = k0 + lane;
-                    bool head = false;
-                    unsigned col = 0;
-                    if (k < n)
-                    {
-                        col = static_cast<unsigned>(keys[k] >> 32);
-                        head = k == 0 || static_cast<unsigned>(keys[k - 1] >> 32) != col;
-                    }
-                    const unsigned hm = __ballot_sync(0xffffffffu, head);
-                    if (FILL && head)
-                    {
-                        double s = 0.0;
-                        for (int q = k; q < n && static_cast<unsigned>(keys[q] >> 32) == col; ++q)
-                            s += vals[keys[q] & ((1u << kSlotBits) - 1)];
-                        const int pos = base + uniq + __popc(hm & ((1u << lane) - 1));
-                        A.cc[pos] = static_cast<int>(col);
-                        A.cv[pos] = s;
-                    }
-                    uniq += __popc(hm);
-                }
+                for (int k = lane; k < u; k += 32)
+                    A.cv[base + k] = acc[k];
                 if (lane == 0)
-                    A.count[row] = uniq;
+                    A.count[row] = u;
                 __syncwarp();
             }
         }
@@ -841,23 +886,14 @@ namespace apf
         static constexpr int kCaps[5] = {64, 256, 1024, 4096, 8192};
         RowBuckets rb;
         bucket_rows(s, A.rows, cand.get(), kCaps, 5, rb);
-        auto launch = [&](auto tag, bool fill_pass) {
+        auto launch = [&](auto tag) {
             constexpr int CAP = decltype(tag)::value;
-            const int warps = warps_for_cap<CAP>();
-            const size_t smem = (size_t)warps * CAP * 16;
+            const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 24)));
+            const size_t smem = (size_t)warps * CAP * 24;
             const int blocks = blocks_for(g.nlist, warps, 148 * 32);
-            if (fill_pass)
-            {
-                APF_CUDA(cudaFuncSetAttribute(spgemm_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                APF_KERNEL("spgemm_fill", s);
-                spgemm_rows<CAP, true><<<blocks, warps * 32, smem, s>>>(g);
-            }
-            else
-            {
-                APF_CUDA(cudaFuncSetAttribute(spgemm_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                APF_KERNEL("spgemm_count", s);
-                spgemm_rows<CAP, false><<<blocks, warps * 32, smem, s>>>(g);
-            }
+            APF_CUDA(cudaFuncSetAttribute(spgemm_rows<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            APF_KERNEL("spgemm_fill", s);
+            spgemm_rows<CAP><<<blocks, warps * 32, smem, s>>>(g);
             APF_CUDA(cudaGetLastError());
         };
         for (int b = 0; b < 5; ++b)
@@ -865,7 +901,7 @@ namespace apf
             g.list = rb.list.get() + rb.offsets[b];
             g.nlist = rb.offsets[b + 1] - rb.offsets[b];
             if (g.nlist > 0)
-                with_cap(kCaps[b], [&](auto tag) { launch(tag, true); });
+                with_cap(kCaps[b], [&](auto tag) { launch(tag); });
         }
         const long long nnz = exclusive_scan(count.get(), C.row_ptr.get(), A.rows, s);
         C.col_idx.allocate(static_cast<std::size_t>(nnz), s);
