@@ -664,143 +664,152 @@ namespace apf
         // (schur_approximations.hpp:107-200, sparse_matrix_ops.hpp:286-316 with zero_tol 0):
         //   hpar = setFromTriplets(-C[nz], (1/A_cc * B_ic) * B_jc for B_ic, B_jc != 0)
         //   Hhat = setFromTriplets(hpar[nz], A_x[nz])
-        template<int CAP, bool FILL>
+        __device__ __forceinline__ unsigned hhat_hash(int col, int hbits)
+        {
+            return (static_cast<unsigned>(col) * 2654435761u) >> (32 - hbits);
+        }
+
+        // One warp per row with at most CAP candidates.  The distinct columns of the kept
+        // candidates go through a shared-memory hash set (at most half full); only those are
+        // sorted; then every candidate is added to its column's two accumulators in
+        // generation order (-C row, the Schur terms in B_dt's row order, then A_x), the
+        // order in which the reference's setFromTriplets passes sum them.  Shared memory per
+        // warp: table keys int[2 CAP], ranks int[2 CAP], sorted keys / (hs, as)
+        // accumulators 16 B x CAP, sorted columns int[CAP].
+        template<int CAP>
         __global__ void __launch_bounds__(256) hhat_rows(HhatArgs A)
         {
             extern __shared__ unsigned char smem_raw[];
             const int warps = blockDim.x >> 5;
             const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-            unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
-            double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
-                           (size_t)w * CAP;
+            unsigned char* mine = smem_raw + (size_t)w * CAP * 36;
+            int* tkeys = reinterpret_cast<int*>(mine);
+            int* tranks = tkeys + 2 * CAP;
+            unsigned long long* ukeys = reinterpret_cast<unsigned long long*>(tranks + 2 * CAP);
+            double2* acc = reinterpret_cast<double2*>(ukeys);
+            int* ucols = reinterpret_cast<int*>(acc + CAP);
+            (void)warps;
             const int nrows = A.list ? A.nlist : A.n_u;
-            for (int idx = blockIdx.x * warps + w; idx < nrows; idx += gridDim.x * warps)
+            for (int idx = blockIdx.x * (blockDim.x >> 5) + w; idx < nrows; idx += gridDim.x * (blockDim.x >> 5))
             {
                 const int row = A.list ? A.list[idx] : idx;
-                int n = 0;
-                bool overflow = false;
-                // -C row (seq region 0)
-                {
-                    const int b = A.c_ptr[row], e = A.c_ptr[row + 1];
-                    for (int k0 = b; k0 < e; k0 += 32)
-                    {
-                        const int k = k0 + lane;
-                        const bool ok = k < e && A.c_val[k] != 0.0;
-                        const unsigned m = __ballot_sync(0xffffffffu, ok);
-                        const int slot = n + __popc(m & ((1u << lane) - 1));
-                        if (ok && slot < CAP)
-                        {
-                            keys[slot] = make_key(A.c_col[k], k - b, slot);
-                            vals[slot] = -A.c_val[k];
-                        }
-                        n += __popc(m);
-                    }
-                }
-                // Schur part: for each nonzero B_dt(row, c): (inv_c * B(row,c)) * B(j, c)
-                int seq = 4096;
-                {
-                    const int b = A.bd_ptr[row], e = A.bd_ptr[row + 1];
-                    for (int k = b; k < e; ++k)
+                // the three candidate sources, in generation order; f(col, value, is_ax)
+                auto for_each = [&](auto&& f) {
+                    for (int k = A.c_ptr[row] + lane; k < A.c_ptr[row + 1]; k += 32)
+                        if (A.c_val[k] != 0.0)
+                            f(A.c_col[k], -A.c_val[k], false);
+                    __syncwarp();
+                    for (int k = A.bd_ptr[row]; k < A.bd_ptr[row + 1]; ++k)
                     {
                         const double vi = A.bd_val[k];
+                        if (vi == 0.0)
+                            continue;
                         const int c = A.bd_col[k];
-                        const int tb = A.bt_ptr[c], te = A.bt_ptr[c + 1];
-                        if (vi != 0.0)
+                        const double sv = A.inv_diag[c] * vi;
+                        for (int q = A.bt_ptr[c] + lane; q < A.bt_ptr[c + 1]; q += 32)
                         {
-                            const double sv = A.inv_diag[c] * vi;
-                            for (int q0 = tb; q0 < te; q0 += 32)
-                            {
-                                const int q = q0 + lane;
-                                double contrib = 0.0;
-                                bool ok = false;
-                                if (q < te)
-                                {
-                                    const double vj = A.bt_val[q];
-                                    contrib = sv * vj;
-                                    ok = vj != 0.0 && fabs(contrib) > 0.0;
-                                }
-                                const unsigned m = __ballot_sync(0xffffffffu, ok);
-                                const int slot = n + __popc(m & ((1u << lane) - 1));
-                                if (ok && slot < CAP)
-                                {
-                                    keys[slot] = make_key(A.bt_col[q], seq + (q - tb), slot);
-                                    vals[slot] = contrib;
-                                }
-                                n += __popc(m);
-                            }
+                            const double vj = A.bt_val[q];
+                            const double contrib = sv * vj;
+                            if (vj != 0.0 && fabs(contrib) > 0.0)
+                                f(A.bt_col[q], contrib, false);
                         }
-                        seq += te - tb;
+                        __syncwarp();
                     }
-                }
-                const int n_h = n;
-                // A_x row: flagged by seq region >= (1 << 16)
+                    for (int k = A.ax_ptr[row] + lane; k < A.ax_ptr[row + 1]; k += 32)
+                        if (A.ax_val[k] != 0.0)
+                            f(A.ax_col[k], A.ax_val[k], true);
+                    __syncwarp();
+                };
+                int n = (A.c_ptr[row + 1] - A.c_ptr[row]) + (A.ax_ptr[row + 1] - A.ax_ptr[row]);
+                for (int k = A.bd_ptr[row]; k < A.bd_ptr[row + 1]; ++k)
+                    n += A.bt_ptr[A.bd_col[k] + 1] - A.bt_ptr[A.bd_col[k]];
+                if (n > CAP)
                 {
-                    const int b = A.ax_ptr[row], e = A.ax_ptr[row + 1];
-                    for (int k0 = b; k0 < e; k0 += 32)
+                    if (lane == 0)
                     {
-                        const int k = k0 + lane;
-                        const bool ok = k < e && A.ax_val[k] != 0.0;
-                        const unsigned m = __ballot_sync(0xffffffffu, ok);
-                        const int slot = n + __popc(m & ((1u << lane) - 1));
-                        if (ok && slot < CAP)
-                        {
-                            keys[slot] = make_key(A.ax_col[k], (1 << 16) + (k - b), slot);
-                            vals[slot] = A.ax_val[k];
-                        }
-                        n += __popc(m);
-                    }
-                }
-                (void)n_h;
-                if (n > CAP || seq >= (1 << 16) || overflow)
-                {
-                    if (lane == 0)
                         atomicExch(A.status, APF_ERR_CAPACITY);
-                    if (lane == 0)
                         A.row_count[row] = 0;
+                    }
                     __syncwarp();
                     continue;
                 }
-                int np = 1;
-                while (np < n) np <<= 1;
-                for (int k = n + lane; k < np; k += 32)
-                    keys[k] = ~0ull;
+                int hbits = 6;
+                while ((1 << hbits) < 2 * n)
+                    ++hbits;
+                const int H = 1 << hbits;
+                for (int t = lane; t < H; t += 32)
+                    tkeys[t] = -1;
                 __syncwarp();
-                warp_bitonic_sort(keys, np);
-                const int out_base = FILL ? A.row_ptr[row] : 0;
-                int uniq = 0;
-                for (int k0 = 0; k0 < n; k0 += 32)
+                for_each([&](int col, double, bool) {
+                    unsigned h = hhat_hash(col, hbits);
+                    while (true)
+                    {
+                        const int prev = atomicCAS(tkeys + h, -1, col);
+                        if (prev == -1 || prev == col)
+                            break;
+                        h = (h + 1) & (H - 1);
+                    }
+                });
+                int u = 0;
+                for (int t0 = 0; t0 < H; t0 += 32)
+                {
+                    const int t = t0 + lane;
+                    const int key = tkeys[t];
+                    const unsigned m = __ballot_sync(0xffffffffu, key != -1);
+                    if (key != -1)
+                        ukeys[u + __popc(m & ((1u << lane) - 1))] =
+                            (static_cast<unsigned long long>(static_cast<unsigned>(key)) << 32) | static_cast<unsigned>(t);
+                    u += __popc(m);
+                }
+                const int np = next_pow2(u);
+                for (int k = u + lane; k < np; k += 32)
+                    ukeys[k] = ~0ull;
+                __syncwarp();
+                warp_bitonic_sort(ukeys, np);
+                for (int k = lane; k < u; k += 32)
+                {
+                    const unsigned long long key = ukeys[k];
+                    tranks[static_cast<unsigned>(key)] = k;
+                    ucols[k] = static_cast<int>(key >> 32);
+                }
+                __syncwarp();
+                for (int k = lane; k < u; k += 32)
+                    acc[k] = make_double2(0.0, 0.0);
+                __syncwarp();
+                for_each([&](int col, double v, bool is_ax) {
+                    unsigned h = hhat_hash(col, hbits);
+                    while (tkeys[h] != col)
+                        h = (h + 1) & (H - 1);
+                    double2& a2 = acc[tranks[h]];
+                    if (is_ax)
+                        a2.y += v;
+                    else
+                        a2.x += v;
+                });
+                // kept entries (hpar or A_x nonzero) in column order to the row's segment
+                const int out_base = A.row_ptr[row];
+                int kept = 0;
+                for (int k0 = 0; k0 < u; k0 += 32)
                 {
                     const int k = k0 + lane;
-                    bool head = false, keep = false;
-                    unsigned col = 0;
                     double hs = 0.0, as = 0.0;
-                    if (k < n)
+                    if (k < u)
                     {
-                        col = static_cast<unsigned>(keys[k] >> 32);
-                        head = (k == 0) || (static_cast<unsigned>(keys[k - 1] >> 32) != col);
-                        if (head)
-                        {
-                            for (int q = k; q < n && static_cast<unsigned>(keys[q] >> 32) == col; ++q)
-                            {
-                                const unsigned long long kk = keys[q];
-                                const int sq = static_cast<int>((kk >> kSlotBits) & ((1u << kSeqBits) - 1));
-                                const double v = vals[kk & ((1u << kSlotBits) - 1)];
-                                if (sq >= (1 << 16)) as += v; else hs += v;
-                            }
-                            keep = (hs != 0.0) || (as != 0.0);
-                        }
+                        hs = acc[k].x;
+                        as = acc[k].y;
                     }
+                    const bool keep = k < u && (hs != 0.0 || as != 0.0);
                     const unsigned km = __ballot_sync(0xffffffffu, keep);
-                    if (FILL && keep)
+                    if (keep)
                     {
-                        const int pos = out_base + uniq + __popc(km & ((1u << lane) - 1));
-                        A.col_out[pos] = static_cast<int>(col);
-                        A.val_out[pos] = (hs != 0.0 ? hs : 0.0) + (as != 0.0 ? as : 0.0);
+                        const int pos = out_base + kept + __popc(km & ((1u << lane) - 1));
+                        A.col_out[pos] = ucols[k];
+                        A.val_out[pos] = hs + as;
                     }
-                    uniq += __popc(km);
+                    kept += __popc(km);
                 }
                 if (lane == 0)
-                    A.row_count[row] = uniq;
+                    A.row_count[row] = kept;
                 __syncwarp();
             }
         }
@@ -1152,24 +1161,15 @@ namespace apf
         int cap = 0;
         APF_CUDA(cudaMemcpyAsync(&cap, bound.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         sync(s);
-        auto run = [&](auto cap_tag, bool fill) {
+        auto run = [&](auto cap_tag, bool) {
             constexpr int CAP = decltype(cap_tag)::value;
-            const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 16)));
+            const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 36)));
             const int threads = warps * 32;
-            const size_t smem = (size_t)warps * CAP * 16;
+            const size_t smem = (size_t)warps * CAP * 36;
             const int blocks = grid_for(a.list ? a.nlist : n_u, warps, 148 * 32);
-            if (fill)
-            {
-                APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                APF_KERNEL("hhat_rows_fill", s);
-                hhat_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
-            }
-            else
-            {
-                APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                APF_KERNEL("hhat_rows_count", s);
-                hhat_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
-            }
+            APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            APF_KERNEL("hhat_rows_fill", s);
+            hhat_rows<CAP><<<blocks, threads, smem, s>>>(a);
             APF_CUDA(cudaGetLastError());
         };
         auto dispatch = [&](bool fill) {
