@@ -291,6 +291,28 @@ namespace apf
                 __syncthreads();
         }
 
+        // K[i][j] -= K[i][col] u for rows col < i < n (one thread per column j > col): four
+        // rows per step, loads before stores, so four shared-memory round trips overlap (the
+        // column col is read only, the column j belongs to this thread)
+        template<class V>
+        __device__ __forceinline__ void lu_column_update(V* K, int LD, int col, int j, int n, V u)
+        {
+            int i = col + 1;
+            for (; i + 3 < n; i += 4)
+            {
+                const V l0 = K[i * LD + col], l1 = K[(i + 1) * LD + col];
+                const V l2 = K[(i + 2) * LD + col], l3 = K[(i + 3) * LD + col];
+                const V a0 = K[i * LD + j], a1 = K[(i + 1) * LD + j];
+                const V a2 = K[(i + 2) * LD + j], a3 = K[(i + 3) * LD + j];
+                K[i * LD + j] = a0 - l0 * u;
+                K[(i + 1) * LD + j] = a1 - l1 * u;
+                K[(i + 2) * LD + j] = a2 - l2 * u;
+                K[(i + 3) * LD + j] = a3 - l3 * u;
+            }
+            for (; i < n; ++i)
+                K[i * LD + j] -= K[i * LD + col] * u;
+        }
+
         // arg-max over the team: (best, bi) of every thread -> the team's (largest value,
         // smallest index among ties), identical on every thread
         template<int W>
@@ -531,8 +553,7 @@ namespace apf
                     for (int j = col + 1 + lane; j < n + 2; j += NT)
                     {
                         const V u = K[col * LD + j] * inv;
-                        for (int i = col + 1; i < n; ++i)
-                            K[i * LD + j] -= K[i * LD + col] * u;
+                        lu_column_update(K, LD, col, j, n, u);
                     }
                     team_sync<W>();
                 }
@@ -1182,8 +1203,7 @@ namespace apf
                     for (int j = col + 1 + lane; j < n + 3; j += NT)
                     {
                         const double u = K[col * LD + j] * inv;
-                        for (int i = col + 1; i < n; ++i)
-                            K[i * LD + j] -= K[i * LD + col] * u;
+                        lu_column_update(K, LD, col, j, n, u);
                     }
                     team_sync<W>();
                 }
