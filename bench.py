@@ -54,6 +54,8 @@ def parse():
                     help="one device-resident step and exit (a short program for ncu captures); no JSON line")
     ap.add_argument("--pool-reserve-gb", type=float, default=0.0,
                     help="grow the device memory pool to this size once before the warm-up")
+    ap.add_argument("--amg-aggressive-levels", type=int, default=None,
+                    help="finest AMG levels aggregated from a distance-2 independent set (default: the library's)")
     ap.add_argument("--precond", default="learned", choices=["learned", "plain"],
                     help="learned: the shipped model (plain block preconditioner as fallback), timed beside plain")
     return ap.parse_args()
@@ -257,6 +259,8 @@ def run_ours(args, world, rank, local):
     sopt = _lib.SolverOptions()
     lib.apf_solver_options_default(C.byref(sopt))
     sopt.tolerance = args.tol
+    if args.amg_aggressive_levels is not None:
+        sopt.amg_aggressive_levels = args.amg_aggressive_levels
     from doubleadapparabolicfem_b200 import learned as LM
     learned_model = None
     if args.precond == "learned" and os.path.exists(LM.DEFAULT_WEIGHTS):
@@ -496,6 +500,7 @@ def run_ours(args, world, rank, local):
                              (["slab_reconstruction", "patch_fluxes", "indicators", "x_indicators"]
                               if run_estimator else []),
                    "tolerance": args.tol,
+                   "amg_aggressive_levels": sopt.amg_aggressive_levels,
                    "preconditioner": ("learned smoother weights in the blkdiag(A_y, Hhat) SA-AMG V-cycles "
                                       "(plain fallback)" if plain else
                                       "plain: blkdiag(A_y, Hhat) by SA-AMG V-cycles"),

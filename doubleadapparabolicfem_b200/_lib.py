@@ -74,6 +74,7 @@ class SolverOptions(C.Structure):
         ("amg_smooth_steps", C.c_int),
         ("amg_strength", C.c_double),
         ("amg_coarse_size", C.c_int),
+        ("amg_aggressive_levels", C.c_int),
     ]
 
 

@@ -112,6 +112,107 @@ namespace apf
                 atomicAdd(undecided, cnt);
         }
 
+        // distance-2 independent set (aggressive coarsening): a node is a root when its
+        // priority key is the largest among the undecided nodes within two strong edges, out
+        // when a root lies within two strong edges.  Pass A: per node, the largest undecided
+        // key and whether a root is among itself and its strong neighbours; pass B: the same
+        // over the strong neighbours' pass-A values.
+        __device__ __forceinline__ unsigned long long mis_key(int i)
+        {
+            return (static_cast<unsigned long long>(hash_u32(static_cast<unsigned>(i))) << 32) | static_cast<unsigned>(i);
+        }
+
+        __global__ void mis2_pass_a(int n, const int* rp, const int* ci, const double* va, Strength st, const int* state,
+                                    unsigned long long* m1, int* r1)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            {
+                unsigned long long m = state[i] == UNDECIDED ? mis_key(i) : 0ull;
+                int r = state[i] == ROOT;
+                for (int k = rp[i]; k < rp[i + 1]; ++k)
+                {
+                    const int j = ci[k];
+                    if (!st(i, j, va[k]))
+                        continue;
+                    const int sj = state[j];
+                    if (sj == UNDECIDED)
+                        m = max(m, mis_key(j));
+                    r |= sj == ROOT;
+                }
+                m1[i] = m;
+                r1[i] = r;
+            }
+        }
+
+        __global__ void mis2_pass_b(int n, const int* rp, const int* ci, const double* va, Strength st, const int* sin,
+                                    const unsigned long long* m1, const int* r1, int* sout, int* undecided)
+        {
+            int cnt = 0;
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            {
+                const int s0 = sin[i];
+                if (s0 != UNDECIDED)
+                {
+                    sout[i] = s0;
+                    continue;
+                }
+                unsigned long long m = m1[i];
+                int r = r1[i];
+                for (int k = rp[i]; k < rp[i + 1]; ++k)
+                {
+                    const int j = ci[k];
+                    if (!st(i, j, va[k]))
+                        continue;
+                    m = max(m, m1[j]);
+                    r |= r1[j];
+                }
+                const int ns = r ? OUT : (m == mis_key(i) ? ROOT : UNDECIDED);
+                sout[i] = ns;
+                cnt += ns == UNDECIDED;
+            }
+            for (int o = 16; o > 0; o >>= 1)
+                cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+            if ((threadIdx.x & 31) == 0 && cnt)
+                atomicAdd(undecided, cnt);
+        }
+
+        // second aggregation pass after distance-2 selection: a node without a strong root
+        // neighbour joins the aggregate of its strongest assigned neighbour (ties: smallest
+        // index); agg_in holds the first pass (-1: unassigned)
+        __global__ void assign_aggregates2(int n, const int* rp, const int* ci, const double* va, Strength st,
+                                           const int* agg_in, int* agg_out, int* status)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            {
+                if (agg_in[i] >= 0)
+                {
+                    agg_out[i] = agg_in[i];
+                    continue;
+                }
+                int best = -1;
+                double bv = -1.0;
+                for (int k = rp[i]; k < rp[i + 1]; ++k)
+                {
+                    const int j = ci[k];
+                    if (agg_in[j] < 0 || !st(i, j, va[k]))
+                        continue;
+                    const double v = fabs(va[k]);
+                    if (v > bv || (v == bv && j < best))
+                    {
+                        bv = v;
+                        best = j;
+                    }
+                }
+                if (best < 0)
+                {
+                    atomicExch(status, APF_ERR_INTERNAL);
+                    agg_out[i] = 0;
+                }
+                else
+                    agg_out[i] = agg_in[best];
+            }
+        }
+
         __global__ void root_flags(int n, const int* state, int* flag)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -120,7 +221,8 @@ namespace apf
 
         // each non-root joins its strongest root neighbour (ties: smallest index)
         __global__ void assign_aggregates(int n, const int* rp, const int* ci, const double* va, Strength st,
-                                          const int* state, const int* root_pos, int* agg, int* comp_coarse, int* status)
+                                          const int* state, const int* root_pos, int* agg, int* comp_coarse, int* status,
+                                          bool allow_unassigned)
         {
             for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             {
@@ -147,8 +249,9 @@ namespace apf
                 }
                 if (best < 0)
                 {
-                    atomicExch(status, APF_ERR_INTERNAL);
-                    agg[i] = 0;
+                    if (!allow_unassigned)
+                        atomicExch(status, APF_ERR_INTERNAL);
+                    agg[i] = allow_unassigned ? -1 : 0;
                 }
                 else
                     agg[i] = root_pos[best];
@@ -388,6 +491,13 @@ namespace apf
             }
             if (force_dense || n <= opt.coarse_size)
             {
+                // the level's diagonal and damping too, so every level carries the same data
+                // for inspection (the dense solve itself needs neither)
+                if (L.dinv.size() != static_cast<std::size_t>(n))
+                {
+                    inverse_diagonal(s, Al, L.dinv);
+                    L.omega = 4.0 / (3.0 * spectral_radius(s, Al));
+                }
                 // dense inverse on the device: scatter, then n Gauss-Jordan exchange steps
                 const std::size_t nn = static_cast<std::size_t>(n) * n;
                 coarse_inv_.allocate(nn, s);
@@ -437,10 +547,25 @@ namespace apf
             }
             int* cur = st0.get();
             int* nxt = st1.get();
+            const bool aggressive = l < opt.aggressive_levels;
+            DeviceBuffer<unsigned long long> m1(aggressive ? n : 1, s);
+            DeviceBuffer<int> r1(aggressive ? n : 1, s);
             for (int it = 0;; ++it)
             {
                 require(it < 200, APF_ERR_INTERNAL, "AMG: independent-set selection did not finish");
                 cnt.zero();
+                if (aggressive)
+                {
+                    {
+                        APF_KERNEL("amg_mis_select", s);
+                        mis2_pass_a<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(),
+                                                                    Al.values.get(), st, cur, m1.get(), r1.get());
+                    }
+                    APF_KERNEL("amg_mis_select", s);
+                    mis2_pass_b<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), st,
+                                                                cur, m1.get(), r1.get(), nxt, cnt.get());
+                }
+                else
                 {
                     APF_KERNEL("amg_mis_select", s);
                     mis_select<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), st,
@@ -474,7 +599,18 @@ namespace apf
                 APF_KERNEL("amg_assign", s);
                 assign_aggregates<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), st,
                                                                   cur, pos.get(), agg.get(),
-                                                                  st.comp ? comp_c.get() : nullptr, status.get());
+                                                                  st.comp ? comp_c.get() : nullptr, status.get(), aggressive);
+            }
+            if (aggressive)
+            {
+                DeviceBuffer<int> agg2(n, s);
+                {
+                    APF_KERNEL("amg_assign", s);
+                    assign_aggregates2<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(),
+                                                                       Al.values.get(), st, agg.get(), agg2.get(),
+                                                                       status.get());
+                }
+                agg = std::move(agg2);
             }
             require(read_int(s, status.get()) == 0, APF_ERR_INTERNAL, "AMG: a node has no aggregate");
             // tentative prolongator

@@ -15,6 +15,9 @@ namespace apf
         int smooth_steps = 2;     // damped-Jacobi sweeps before and after the coarse correction
         int coarse_size = 1024;   // dense solve at or below this size
         int max_levels = 20;
+        // levels (from the finest) whose aggregates come from a distance-2 independent set
+        // (roots two strong edges apart: larger aggregates, fewer coarse unknowns)
+        int aggressive_levels = 0;
     };
 
     struct AmgLevel

@@ -465,6 +465,7 @@ void apf_solver_options_default(apf_solver_options* opt)
     opt->amg_smooth_steps = 2;
     opt->amg_strength = 0.08;
     opt->amg_coarse_size = 256;
+    opt->amg_aggressive_levels = 1;
 }
 
 namespace
@@ -475,6 +476,7 @@ namespace
         a.smooth_steps = std::max(1, o->amg_smooth_steps);
         a.strength = o->amg_strength;
         a.coarse_size = std::max(16, o->amg_coarse_size);
+        a.aggressive_levels = std::max(0, o->amg_aggressive_levels);
         return a;
     }
 
@@ -1030,6 +1032,7 @@ int apf_amg_level_weights(apf_ctx* ctx, apf_system* sys, int block, int level, i
         apf::AmgLevel& L = level_of(sys, block, level);
         cudaStream_t s = ctx->stream;
         const int n = L.A->rows;
+        apf::require(L.dinv.size() == static_cast<std::size_t>(n), APF_ERR_INTERNAL, "AMG level without its diagonal");
         const apf::DeviceBuffer<double>& W = (o == 1 && L.w2.size()) ? L.w2 : L.w;
         if (W.size())
             APF_CUDA(cudaMemcpyAsync(weights, W.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1051,6 +1054,7 @@ int apf_amg_level_features(apf_ctx* ctx, apf_system* sys, int block, int level, 
         apf::AmgLevel& L = level_of(sys, block, level);
         cudaStream_t s = ctx->stream;
         const int n = L.A->rows;
+        apf::require(L.dinv.size() == static_cast<std::size_t>(n), APF_ERR_INTERNAL, "AMG level without its diagonal");
         apf::DeviceBuffer<float> f(static_cast<std::size_t>(n) * apf::learned::kFeatures, s);
         apf::learned_features(s, *L.A, L.dinv.get(), level, block, f.get());
         if (n)

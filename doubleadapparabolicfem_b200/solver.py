@@ -31,6 +31,7 @@ class SolverOptions:
     amg_smooth_steps: int = 2
     amg_strength: float = 0.08
     amg_coarse_size: int = 256
+    amg_aggressive_levels: int = 1
 
     def to_c(self) -> _lib.SolverOptions:
         o = _lib.SolverOptions()
@@ -42,6 +43,7 @@ class SolverOptions:
         o.amg_smooth_steps = self.amg_smooth_steps
         o.amg_strength = self.amg_strength
         o.amg_coarse_size = self.amg_coarse_size
+        o.amg_aggressive_levels = self.amg_aggressive_levels
         return o
 
 

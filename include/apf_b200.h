@@ -170,6 +170,8 @@ typedef struct apf_solver_options
     int amg_smooth_steps;             /* damped-Jacobi sweeps per side of the V-cycle (>= 1) */
     double amg_strength;              /* strength-of-connection threshold (e.g. 0.08) */
     int amg_coarse_size;              /* dense coarsest solve at or below this size */
+    int amg_aggressive_levels;        /* finest levels aggregated from a distance-2 independent set
+                                         (larger aggregates, cheaper V-cycles); default 1, 0 = distance 1 */
 } apf_solver_options;
 
 /* Mirrors SolverDiagnostics.iterative_stats (src/linear_algebra/concepts/solver.hpp:186-197). */
