@@ -54,6 +54,10 @@ def parse():
                     help="one device-resident step and exit (a short program for ncu captures); no JSON line")
     ap.add_argument("--pool-reserve-gb", type=float, default=0.0,
                     help="grow the device memory pool to this size once before the warm-up")
+    ap.add_argument("--amg-smooth-steps", type=int, default=None,
+                    help="damped-Jacobi sweeps per side of the V-cycle (default: the library's)")
+    ap.add_argument("--amg-strength", type=float, default=None,
+                    help="AMG strength-of-connection threshold (default: the library's)")
     ap.add_argument("--amg-aggressive-levels", type=int, default=None,
                     help="finest AMG levels aggregated from a distance-2 independent set (default: the library's)")
     ap.add_argument("--precond", default="learned", choices=["learned", "plain"],
@@ -261,6 +265,10 @@ def run_ours(args, world, rank, local):
     sopt.tolerance = args.tol
     if args.amg_aggressive_levels is not None:
         sopt.amg_aggressive_levels = args.amg_aggressive_levels
+    if args.amg_smooth_steps is not None:
+        sopt.amg_smooth_steps = args.amg_smooth_steps
+    if args.amg_strength is not None:
+        sopt.amg_strength = args.amg_strength
     from doubleadapparabolicfem_b200 import learned as LM
     learned_model = None
     if args.precond == "learned" and os.path.exists(LM.DEFAULT_WEIGHTS):
@@ -501,6 +509,7 @@ def run_ours(args, world, rank, local):
                               if run_estimator else []),
                    "tolerance": args.tol,
                    "amg_aggressive_levels": sopt.amg_aggressive_levels,
+                   "amg_smooth_steps": sopt.amg_smooth_steps, "amg_strength": sopt.amg_strength,
                    "preconditioner": ("learned smoother weights in the blkdiag(A_y, Hhat) SA-AMG V-cycles "
                                       "(plain fallback)" if plain else
                                       "plain: blkdiag(A_y, Hhat) by SA-AMG V-cycles"),
