@@ -707,7 +707,18 @@ namespace apf
         return r;
     }
 
-    void Amg::vcycle(cudaStream_t s, int l, const double* b, double* x)
+    // where level l's first smoothing iterate goes: x or the scratch t, chosen so that the
+    // last of its pre + post sweeps writes x
+    double* Amg::first_iterate(int l, double* x)
+    {
+        AmgLevel& L = levels_[static_cast<std::size_t>(l)];
+        const bool coarsest = l == static_cast<int>(levels_.size()) - 1;
+        const int pre = coarsest ? kCoarseSweeps : opt_.smooth_steps;
+        const int post = coarsest ? 0 : opt_.smooth_steps;
+        return (pre + post) % 2 == 1 ? x : L.t.get();
+    }
+
+    void Amg::vcycle(cudaStream_t s, int l, const double* b, double* x, bool first_done)
     {
         AmgLevel& L = levels_[static_cast<std::size_t>(l)];
         const DeviceCsr& A = *L.A;
@@ -733,8 +744,9 @@ namespace apf
         };
         // the iterate alternates between x and the level's scratch t; starting in the right
         // one makes the last of the pre + post smoothing writes land in x (no copies)
-        double* cur = (pre + post) % 2 == 1 ? x : L.t.get();
+        double* cur = first_iterate(l, x);
         double* other = cur == x ? L.t.get() : x;
+        if (!first_done)
         {
             APF_KERNEL("amg_jacobi_first", s);
             jacobi_first<<<nblocks(n, 256), 256, 0, s>>>(n, b, weights(0), om, cur);
@@ -749,8 +761,20 @@ namespace apf
             return;
         residual(s, A32, cur, b, L.r.get(), level_name(1, l));
         AmgLevel& C = levels_[static_cast<std::size_t>(l) + 1];
-        spmv(s, *L.R32, L.r.get(), C.b.get(), 1.0, 0.0, level_name(2, l));
-        vcycle(s, l + 1, C.b.get(), C.x.get());
+        const bool c_dense = l + 2 == static_cast<int>(levels_.size()) && !jacobi_coarse_;
+        if (c_dense)
+        {
+            spmv(s, *L.R32, L.r.get(), C.b.get(), 1.0, 0.0, level_name(2, l));
+            vcycle(s, l + 1, C.b.get(), C.x.get());
+        }
+        else
+        {
+            // restriction fused with the coarse level's first damped-Jacobi step from zero
+            const bool cown = C.w.size() != 0;
+            spmv_jacobi_first(s, *L.R32, L.r.get(), C.b.get(), cown ? C.w.get() : C.dinv.get(),
+                              cown ? 1.0 : C.omega, first_iterate(l + 1, C.x.get()), level_name(2, l));
+            vcycle(s, l + 1, C.b.get(), C.x.get(), true);
+        }
         spmv(s, *L.P32, C.x.get(), cur, L.alpha, 1.0, level_name(3, l));
         for (int k = 0; k < post; ++k)
         {

@@ -68,7 +68,10 @@ namespace apf
         void coarse_apply(cudaStream_t s, const double* b, double* x) { vcycle(s, levels() - 1, b, x); }
 
     private:
-        void vcycle(cudaStream_t s, int l, const double* b, double* x);
+        // first_done: the caller already wrote level l's first damped-Jacobi iterate from
+        // zero (a restriction fused with it)
+        void vcycle(cudaStream_t s, int l, const double* b, double* x, bool first_done = false);
+        double* first_iterate(int l, double* x);
         std::vector<AmgLevel> levels_;
         DeviceBuffer<double> coarse_inv_; // dense inverse of the coarsest operator, row-major
         int n_coarse_ = 0;

@@ -1657,7 +1657,11 @@ namespace apf
         // ---- lambda~ : A_y lambda~ = f - B^T u
         DeviceBuffer<double> lt(nl, s);
         reconstruct_lambda(s, S, lt, tot);
-        PatchSet ps = patches.get();
+        PatchSet ps;
+        {
+            APF_HOST_RANGE("est_patch_topology_wait");
+            ps = patches.get();
+        }
         // ---- nodal data per cell
         const int nd = in.ndof;
         DeviceBuffer<double> theta((long long)nd * ny, s), ucell((long long)nd * ny, s), ldel((long long)nd * ny, s),
@@ -1842,6 +1846,7 @@ namespace apf
             }
             run_w(choice && *choice ? *choice : W_RULE);
         };
+        APF_HOST_RANGE("est_patch_solves");
         if (tot.n_patches > 0)
         {
             launch(std::integral_constant<int, 32>{}, 0);

@@ -19,12 +19,15 @@ namespace apf
         // Each lane keeps four predicated loads of the row in flight per step (the row
         // pointer, column, value and x gathers form one dependent chain per step, so the
         // number of steps per row, not the bytes, sets the time on L2-resident levels).
-        // MODE 0: y = alpha A x + beta y;  1: y = b - A x;  2: y = x + alpha dinv (b - A x)
+        // MODE 0: y = alpha A x + beta y;  1: y = b - A x;  2: y = x + alpha dinv (b - A x);
+        // 3: y = alpha A x and z = beta dinv y (a restriction fused with the coarse level's
+        // first damped-Jacobi step from zero)
         template<int G, int MODE, class V = double>
         __global__ void __launch_bounds__(256) spmv_kernel(int rows, const int* __restrict__ rp, const int* __restrict__ ci,
                                                            const V* __restrict__ va, const double* __restrict__ x,
                                                            const double* __restrict__ b, double* __restrict__ y,
-                                                           double alpha, double beta, const double* __restrict__ dinv)
+                                                           double alpha, double beta, const double* __restrict__ dinv,
+                                                           double* __restrict__ z)
         {
             constexpr int RPW = 32 / G; // rows per warp and step
             const int lane = threadIdx.x & (G - 1);
@@ -68,6 +71,12 @@ namespace apf
                         y[r] = b[r] - sum;
                     else if (MODE == 2)
                         y[r] = x[r] + alpha * dinv[r] * (b[r] - sum);
+                    else if (MODE == 3)
+                    {
+                        const double v = alpha * sum;
+                        y[r] = v;
+                        z[r] = beta * dinv[r] * v;
+                    }
                     else
                         y[r] = beta == 0.0 ? alpha * sum : alpha * sum + beta * y[r];
                 }
@@ -80,7 +89,8 @@ namespace apf
                                                            const int* __restrict__ col, const V* __restrict__ val,
                                                            const double* __restrict__ x, const double* __restrict__ b,
                                                            double* __restrict__ y, double alpha, double beta,
-                                                           const double* __restrict__ dinv, const int* __restrict__ perm)
+                                                           const double* __restrict__ dinv, const int* __restrict__ perm,
+                                                           double* __restrict__ z)
         {
             const int lane = threadIdx.x & 31;
             const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -118,6 +128,12 @@ namespace apf
                         y[r] = b[r] - sum;
                     else if (MODE == 2)
                         y[r] = x[r] + alpha * dinv[r] * (b[r] - sum);
+                    else if (MODE == 3)
+                    {
+                        const double v = alpha * sum;
+                        y[r] = v;
+                        z[r] = beta * dinv[r] * v;
+                    }
                     else
                         y[r] = beta == 0.0 ? alpha * sum : alpha * sum + beta * y[r];
                 }
@@ -602,7 +618,7 @@ namespace apf
 
         template<int MODE>
         void sell_launch(cudaStream_t s, const DeviceSell& S, const double* x, const double* b, double* y, double alpha,
-                         double beta, const double* dinv)
+                         double beta, const double* dinv, double* z = nullptr)
         {
             if (S.csr_rp)
             {
@@ -610,7 +626,7 @@ namespace apf
                 with_lanes(S.rows, S.avg_row, [&](auto g) {
                     constexpr int G = decltype(g)::value;
                     spmv_kernel<G, MODE, float><<<blocks_for((long long)S.rows * G, 256, 148 * 64), 256, 0, s>>>(
-                        S.rows, S.csr_rp, S.csr_ci, S.val32.get(), x, b, y, alpha, beta, dinv);
+                        S.rows, S.csr_rp, S.csr_ci, S.val32.get(), x, b, y, alpha, beta, dinv, z);
                 });
                 APF_CUDA(cudaGetLastError());
                 return;
@@ -618,10 +634,10 @@ namespace apf
             const int grid = blocks_for((long long)S.slices * 32, 256, 148 * 64);
             if (S.val32.size())
                 sell_kernel<MODE, float><<<grid, 256, 0, s>>>(S.rows, S.slices, S.slice_ptr.get(), S.col.get(),
-                                                              S.val32.get(), x, b, y, alpha, beta, dinv, S.perm.get());
+                                                              S.val32.get(), x, b, y, alpha, beta, dinv, S.perm.get(), z);
             else
                 sell_kernel<MODE, double><<<grid, 256, 0, s>>>(S.rows, S.slices, S.slice_ptr.get(), S.col.get(),
-                                                               S.val.get(), x, b, y, alpha, beta, dinv, S.perm.get());
+                                                               S.val.get(), x, b, y, alpha, beta, dinv, S.perm.get(), z);
             APF_CUDA(cudaGetLastError());
         }
 
@@ -642,7 +658,7 @@ namespace apf
             with_lanes(A.rows, avg, [&](auto g) {
                 constexpr int G = decltype(g)::value;
                 spmv_kernel<G, MODE><<<blocks_for((long long)A.rows * G, threads, 148 * 64), threads, 0, s>>>(
-                    A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(), x, b, y, alpha, beta, dinv);
+                    A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(), x, b, y, alpha, beta, dinv, nullptr);
             });
             APF_CUDA(cudaGetLastError());
         }
@@ -739,6 +755,15 @@ namespace apf
             return;
         APF_KERNEL(name ? name : "spmv", s);
         sell_launch<0>(s, A, x, nullptr, y, alpha, beta, nullptr);
+    }
+
+    void spmv_jacobi_first(cudaStream_t s, const DeviceSell& A, const double* x, double* y, const double* w,
+                           double omega, double* z, const char* name)
+    {
+        if (A.rows == 0)
+            return;
+        APF_KERNEL(name ? name : "spmv", s);
+        sell_launch<3>(s, A, x, nullptr, y, 1.0, omega, w, z);
     }
 
     void jacobi_sweep(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, const double* dinv,

@@ -38,6 +38,10 @@ namespace apf
                       double omega, double* y, const char* name = nullptr);
     void residual(cudaStream_t s, const DeviceSell& A, const double* x, const double* b, double* r,
                   const char* name = nullptr);
+    // y = A x and z = omega w y in one pass (a restriction fused with the first damped-Jacobi
+    // step from zero on the coarse level)
+    void spmv_jacobi_first(cudaStream_t s, const DeviceSell& A, const double* x, double* y, const double* w,
+                           double omega, double* z, const char* name = nullptr);
     // y = alpha * A x + beta * y   (beta == 0 ignores y's old contents)
     void spmv(cudaStream_t s, const DeviceCsr& A, const double* x, double* y, double alpha = 1.0, double beta = 0.0,
               const char* name = nullptr);
