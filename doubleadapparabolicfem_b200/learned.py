@@ -278,6 +278,36 @@ def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, leve
     return model, hist
 
 
+def evaluate(level: int = 6, seeds=(1, 2), tol: float = 1e-8, device: int = 0, blocks_per_side: int = 8):
+    """Learned vs plain block preconditioner on held-out systems of the learned-preconditioner
+    configuration: uniform outer level ``level`` with seeded piecewise-constant diffusivity
+    log-uniform in [0.01, 100] on blocks_per_side^2 blocks, MINRES to the FP64 true residual
+    ``tol``.  Returns one record per system (iterations, solve seconds, true residuals)."""
+    from .assembly import assemble_main_system_blocks
+    from .solver import SolverOptions, solve_saddle_system_with_preconditioner
+    ctx = Context(device)
+    model = LearnedModel.load()
+    use_model(ctx, model)
+    out = []
+    for seed in seeds:
+        prob = random_kappa_problem(level, seed=seed, blocks_per_side=blocks_per_side)
+        rec = {"level": level, "seed": seed, "dofs": prob.n_lambda + prob.n_u}
+        for name, prec in (("plain", "amg_block"), ("learned", "learned")):
+            b = assemble_main_system_blocks(prob, ctx=ctx)
+            b.assemble_parabolic_graph_norm_approximation()
+            solve_saddle_system_with_preconditioner(b, SolverOptions(tolerance=tol, preconditioner=prec),
+                                                    copy_out=False)  # warm-up (set-up, graphs)
+            _, d = solve_saddle_system_with_preconditioner(b, SolverOptions(tolerance=tol, preconditioner=prec),
+                                                           copy_out=False)
+            rec[name] = {"iterations": d["iterations"], "solve_s": d["solve_seconds"],
+                         "true_residual": d["final_true_residual"], "fallback": d["learned_fallback"]}
+            b.close()
+        rec["iteration_gain"] = rec["plain"]["iterations"] / max(1, rec["learned"]["iterations"])
+        rec["time_gain"] = rec["plain"]["solve_s"] / rec["learned"]["solve_s"]
+        out.append(rec)
+    return out
+
+
 if __name__ == "__main__":
     import argparse
     ap = argparse.ArgumentParser(description="train the learned MINRES preconditioner on method-generated systems")
@@ -289,6 +319,12 @@ if __name__ == "__main__":
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--burn-in", type=int, default=8)
+    ap.add_argument("--evaluate", type=int, default=None, metavar="LEVEL",
+                    help="instead of training: learned vs plain on seeded random-kappa systems of this level")
     a = ap.parse_args()
+    if a.evaluate is not None:
+        import json
+        print(json.dumps(evaluate(a.evaluate)))
+        raise SystemExit(0)
     train_default_model(a.out, a.n_train, tuple(int(x) for x in a.levels.split(",")), a.epochs, a.lr, a.seed,
                         steps=a.steps, burn_in=a.burn_in)
