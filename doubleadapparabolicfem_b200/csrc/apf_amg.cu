@@ -112,6 +112,19 @@ namespace apf
                 atomicAdd(undecided, cnt);
         }
 
+        // candidate (v, j) beats (bv, best): larger magnitude, values within a relative 1e-10
+        // counting as equal (ties: smaller index), so that rounding-level differences between
+        // couplings that are equal in exact arithmetic do not change the aggregates
+        __device__ __forceinline__ bool stronger(double v, int j, double bv, int best)
+        {
+            if (best < 0)
+                return true;
+            const double tol = 1e-10 * fmax(v, bv);
+            if (v > bv + tol)
+                return true;
+            return v >= bv - tol && j < best;
+        }
+
         // distance-2 independent set (aggressive coarsening): a node is a root when its
         // priority key is the largest among the undecided nodes within two strong edges, out
         // when a root lies within two strong edges.  Pass A: per node, the largest undecided
@@ -197,7 +210,7 @@ namespace apf
                     if (agg_in[j] < 0 || !st(i, j, va[k]))
                         continue;
                     const double v = fabs(va[k]);
-                    if (v > bv || (v == bv && j < best))
+                    if (stronger(v, j, bv, best))
                     {
                         bv = v;
                         best = j;
@@ -241,7 +254,7 @@ namespace apf
                     if (state[j] != ROOT || !st(i, j, va[k]))
                         continue;
                     const double v = fabs(va[k]);
-                    if (v > bv || (v == bv && j < best))
+                    if (stronger(v, j, bv, best))
                     {
                         bv = v;
                         best = j;

@@ -24,6 +24,7 @@
 #include "apf_device.cuh"
 #include "apf_quad1d.cuh"
 #include "apf_warpsort.cuh"
+#include "apf_rowhash.cuh"
 #include "apf_internal.hpp"
 #include "apf_system.hpp"
 
@@ -664,61 +665,103 @@ namespace apf
         // (schur_approximations.hpp:107-200, sparse_matrix_ops.hpp:286-316 with zero_tol 0):
         //   hpar = setFromTriplets(-C[nz], (1/A_cc * B_ic) * B_jc for B_ic, B_jc != 0)
         //   Hhat = setFromTriplets(hpar[nz], A_x[nz])
-        __device__ __forceinline__ unsigned hhat_hash(int col, int hbits)
-        {
-            return (static_cast<unsigned>(col) * 2654435761u) >> (32 - hbits);
-        }
-
-        // One warp per row with at most CAP candidates.  The distinct columns of the kept
-        // candidates go through a shared-memory hash set (at most half full); only those are
-        // sorted; then every candidate is added to its column's two accumulators in
-        // generation order (-C row, the Schur terms in B_dt's row order, then A_x), the
-        // order in which the reference's setFromTriplets passes sum them.  Shared memory per
-        // warp: table keys int[2 CAP], ranks int[2 CAP], sorted keys / (hs, as)
-        // accumulators 16 B x CAP, sorted columns int[CAP].
+        // One warp per row with at most CAP candidates: the -C row, the Schur terms
+        // (inv_c B_dt(row, c)) B_dt(j, c) for the nonzero B_dt entries of the row (the B_dt^T
+        // rows of up to kSeg of them flattened through a prefix sum of their lengths), then
+        // the A_x row, 32 at a time in that order.  Distinct columns of the kept candidates
+        // go through a shared-memory hash set; only those are sorted; every candidate is then
+        // added to its column's two accumulators (-C and Schur: hpar; A_x) in generation
+        // order, the order in which the reference's setFromTriplets passes sum them.  Shared
+        // memory per warp: table keys int[2 CAP], ranks int[2 CAP], sorted keys / (hpar, A_x)
+        // accumulators 16 B x CAP, sorted columns int[CAP], then kRowExtra.
         template<int CAP>
         __global__ void __launch_bounds__(256) hhat_rows(HhatArgs A)
         {
             extern __shared__ unsigned char smem_raw[];
-            const int warps = blockDim.x >> 5;
             const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-            unsigned char* mine = smem_raw + (size_t)w * CAP * 36;
+            unsigned char* mine = smem_raw + (size_t)w * (CAP * 36 + kRowExtra);
             int* tkeys = reinterpret_cast<int*>(mine);
             int* tranks = tkeys + 2 * CAP;
             unsigned long long* ukeys = reinterpret_cast<unsigned long long*>(tranks + 2 * CAP);
             double2* acc = reinterpret_cast<double2*>(ukeys);
             int* ucols = reinterpret_cast<int*>(acc + CAP);
-            (void)warps;
+            int* seg = ucols + CAP;
+            double* stage = reinterpret_cast<double*>(seg + kSeg + 2);
+            double* hs = reinterpret_cast<double*>(acc);
             const int nrows = A.list ? A.nlist : A.n_u;
             for (int idx = blockIdx.x * (blockDim.x >> 5) + w; idx < nrows; idx += gridDim.x * (blockDim.x >> 5))
             {
                 const int row = A.list ? A.list[idx] : idx;
-                // the three candidate sources, in generation order; f(col, value, is_ax)
+                // every candidate (ok, column, value, is_ax) in generation order, 32 lanes at a time
                 auto for_each = [&](auto&& f) {
-                    for (int k = A.c_ptr[row] + lane; k < A.c_ptr[row + 1]; k += 32)
-                        if (A.c_val[k] != 0.0)
-                            f(A.c_col[k], -A.c_val[k], false);
-                    __syncwarp();
-                    for (int k = A.bd_ptr[row]; k < A.bd_ptr[row + 1]; ++k)
                     {
-                        const double vi = A.bd_val[k];
-                        if (vi == 0.0)
-                            continue;
-                        const int c = A.bd_col[k];
-                        const double sv = A.inv_diag[c] * vi;
-                        for (int q = A.bt_ptr[c] + lane; q < A.bt_ptr[c + 1]; q += 32)
+                        const int b = A.c_ptr[row], e = A.c_ptr[row + 1];
+                        for (int k0 = b; k0 < e; k0 += 32)
                         {
-                            const double vj = A.bt_val[q];
-                            const double contrib = sv * vj;
-                            if (vj != 0.0 && fabs(contrib) > 0.0)
-                                f(A.bt_col[q], contrib, false);
+                            const int k = k0 + lane;
+                            const bool ok = k < e && A.c_val[k] != 0.0;
+                            f(ok, ok ? A.c_col[k] : 0, ok ? -A.c_val[k] : 0.0, false);
+                        }
+                    }
+                    const int db = A.bd_ptr[row], de = A.bd_ptr[row + 1];
+                    for (int kb = db; kb < de; kb += kSeg)
+                    {
+                        const int cnt = min(de - kb, kSeg);
+                        for (int i = lane; i < cnt; i += 32)
+                        {
+                            const int c = A.bd_col[kb + i];
+                            seg[i + 1] = A.bd_val[kb + i] != 0.0 ? A.bt_ptr[c + 1] - A.bt_ptr[c] : 0;
+                        }
+                        __syncwarp();
+                        for (int i0 = 0, carry = 0; i0 < cnt; i0 += 32)
+                        {
+                            int v = i0 + lane < cnt ? seg[i0 + lane + 1] : 0;
+                            for (int o = 1; o < 32; o <<= 1)
+                            {
+                                const int u = __shfl_up_sync(0xffffffffu, v, o);
+                                if (lane >= o)
+                                    v += u;
+                            }
+                            __syncwarp();
+                            if (i0 + lane < cnt)
+                                seg[i0 + lane + 1] = carry + v;
+                            carry += __shfl_sync(0xffffffffu, v, 31);
+                            __syncwarp();
+                        }
+                        if (lane == 0)
+                            seg[0] = 0;
+                        __syncwarp();
+                        const int nb = seg[cnt];
+                        for (int t0 = 0; t0 < nb; t0 += 32)
+                        {
+                            const int t = t0 + lane;
+                            bool ok = false;
+                            int col = 0;
+                            double contrib = 0.0;
+                            if (t < nb)
+                            {
+                                const int i = find_segment(seg, cnt, t);
+                                const int k = kb + i;
+                                const int c = A.bd_col[k];
+                                const int q = A.bt_ptr[c] + (t - seg[i]);
+                                const double vj = A.bt_val[q];
+                                contrib = (A.inv_diag[c] * A.bd_val[k]) * vj;
+                                ok = vj != 0.0 && fabs(contrib) > 0.0;
+                                col = A.bt_col[q];
+                            }
+                            f(ok, col, contrib, false);
                         }
                         __syncwarp();
                     }
-                    for (int k = A.ax_ptr[row] + lane; k < A.ax_ptr[row + 1]; k += 32)
-                        if (A.ax_val[k] != 0.0)
-                            f(A.ax_col[k], A.ax_val[k], true);
-                    __syncwarp();
+                    {
+                        const int b = A.ax_ptr[row], e = A.ax_ptr[row + 1];
+                        for (int k0 = b; k0 < e; k0 += 32)
+                        {
+                            const int k = k0 + lane;
+                            const bool ok = k < e && A.ax_val[k] != 0.0;
+                            f(ok, ok ? A.ax_col[k] : 0, ok ? A.ax_val[k] : 0.0, true);
+                        }
+                    }
                 };
                 int n = (A.c_ptr[row + 1] - A.c_ptr[row]) + (A.ax_ptr[row + 1] - A.ax_ptr[row]);
                 for (int k = A.bd_ptr[row]; k < A.bd_ptr[row + 1]; ++k)
@@ -740,16 +783,11 @@ namespace apf
                 for (int t = lane; t < H; t += 32)
                     tkeys[t] = -1;
                 __syncwarp();
-                for_each([&](int col, double, bool) {
-                    unsigned h = hhat_hash(col, hbits);
-                    while (true)
-                    {
-                        const int prev = atomicCAS(tkeys + h, -1, col);
-                        if (prev == -1 || prev == col)
-                            break;
-                        h = (h + 1) & (H - 1);
-                    }
+                for_each([&](bool ok, int col, double, bool) {
+                    if (ok)
+                        hash_insert(tkeys, col, hbits);
                 });
+                __syncwarp();
                 int u = 0;
                 for (int t0 = 0; t0 < H; t0 += 32)
                 {
@@ -776,15 +814,10 @@ namespace apf
                 for (int k = lane; k < u; k += 32)
                     acc[k] = make_double2(0.0, 0.0);
                 __syncwarp();
-                for_each([&](int col, double v, bool is_ax) {
-                    unsigned h = hhat_hash(col, hbits);
-                    while (tkeys[h] != col)
-                        h = (h + 1) & (H - 1);
-                    double2& a2 = acc[tranks[h]];
-                    if (is_ax)
-                        a2.y += v;
-                    else
-                        a2.x += v;
+                // hpar and A_x sums of each column live side by side: rank r -> hs[2 r] / hs[2 r + 1]
+                for_each([&](bool ok, int col, double v, bool is_ax) {
+                    const int r = ok ? hash_rank(tkeys, tranks, col, hbits) : 0;
+                    ordered_add(hs, stage, ok, 2 * r + (is_ax ? 1 : 0), v, lane);
                 });
                 // kept entries (hpar or A_x nonzero) in column order to the row's segment
                 const int out_base = A.row_ptr[row];
@@ -792,19 +825,19 @@ namespace apf
                 for (int k0 = 0; k0 < u; k0 += 32)
                 {
                     const int k = k0 + lane;
-                    double hs = 0.0, as = 0.0;
+                    double h = 0.0, a = 0.0;
                     if (k < u)
                     {
-                        hs = acc[k].x;
-                        as = acc[k].y;
+                        h = acc[k].x;
+                        a = acc[k].y;
                     }
-                    const bool keep = k < u && (hs != 0.0 || as != 0.0);
+                    const bool keep = k < u && (h != 0.0 || a != 0.0);
                     const unsigned km = __ballot_sync(0xffffffffu, keep);
                     if (keep)
                     {
                         const int pos = out_base + kept + __popc(km & ((1u << lane) - 1));
                         A.col_out[pos] = ucols[k];
-                        A.val_out[pos] = hs + as;
+                        A.val_out[pos] = h + a;
                     }
                     kept += __popc(km);
                 }
@@ -1163,9 +1196,9 @@ namespace apf
         sync(s);
         auto run = [&](auto cap_tag, bool) {
             constexpr int CAP = decltype(cap_tag)::value;
-            const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 36)));
+            const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 36 + kRowExtra)));
             const int threads = warps * 32;
-            const size_t smem = (size_t)warps * CAP * 36;
+            const size_t smem = (size_t)warps * (CAP * 36 + kRowExtra);
             const int blocks = grid_for(a.list ? a.nlist : n_u, warps, 148 * 32);
             APF_CUDA(cudaFuncSetAttribute(hhat_rows<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             APF_KERNEL("hhat_rows_fill", s);

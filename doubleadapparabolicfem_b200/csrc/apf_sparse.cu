@@ -4,6 +4,7 @@
 
 #include "apf_sparse.cuh"
 #include "apf_warpsort.cuh"
+#include "apf_rowhash.cuh"
 
 namespace apf
 {
@@ -330,19 +331,17 @@ namespace apf
             int nlist;
         };
 
-        // One warp per row of A B with at most CAP candidate products.  The distinct columns
-        // are collected in a shared-memory hash set (open addressing, at most half full), only
-        // those are sorted, and each product is then added to its column's accumulator in
-        // generation order (A's row order, then B's row order: one product per column per A
-        // entry, so lanes never collide), which is the order a stable sort of the candidates
-        // would sum them in.  Output: the row's sorted distinct columns and sums at cp[row],
-        // their number in count[row].
-        // shared memory per warp: table keys int[2 CAP], ranks int[2 CAP], sorted keys /
-        // accumulators 8 B x CAP
-        __device__ __forceinline__ unsigned hash_slot(int col, int hbits)
-        {
-            return (static_cast<unsigned>(col) * 2654435761u) >> (32 - hbits);
-        }
+        // One warp per row of A B with at most CAP candidate products, processed 32 at a time
+        // in generation order (A's row order, then B's row order) with the warp's lanes spread
+        // over all of them (the B rows of up to kSeg A entries are flattened through a
+        // prefix sum of their lengths).  The distinct columns go through a shared-memory hash
+        // set (at most half full) and only those are sorted; each product is then added to
+        // its column's accumulator in generation order (within a group of 32, the lowest lane
+        // of each column adds its group's products in lane order), so the sums are those of a
+        // stable sort of the candidates.  Output: the row's sorted distinct columns and sums
+        // at cp[row], their number in count[row].
+        // Shared memory per warp: table keys int[2 CAP], ranks int[2 CAP], sorted keys /
+        // accumulators 8 B x CAP, segment offsets int[kSeg + 2], staged products double[32].
 
         template<int CAP>
         __global__ void __launch_bounds__(256) spgemm_rows(GemmArgs A)
@@ -350,18 +349,20 @@ namespace apf
             extern __shared__ unsigned char smem_raw[];
             const int warps = blockDim.x >> 5;
             const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-            int* tkeys = reinterpret_cast<int*>(smem_raw) + (size_t)w * (2 * CAP);
-            int* tranks = reinterpret_cast<int*>(smem_raw) + (size_t)warps * (2 * CAP) + (size_t)w * (2 * CAP);
-            unsigned long long* ukeys =
-                reinterpret_cast<unsigned long long*>(reinterpret_cast<int*>(smem_raw) + (size_t)warps * (4 * CAP)) +
-                (size_t)w * CAP;
+            unsigned char* mine = smem_raw + (size_t)w * (24 * CAP + kRowExtra);
+            int* tkeys = reinterpret_cast<int*>(mine);
+            int* tranks = tkeys + 2 * CAP;
+            unsigned long long* ukeys = reinterpret_cast<unsigned long long*>(tranks + 2 * CAP);
             double* acc = reinterpret_cast<double*>(ukeys);
+            int* seg = reinterpret_cast<int*>(ukeys + CAP);
+            double* stage = reinterpret_cast<double*>(seg + kSeg + 2);
             const int nrows = A.list ? A.nlist : A.rows;
             for (int idx = blockIdx.x * warps + w; idx < nrows; idx += gridDim.x * warps)
             {
                 const int row = A.list ? A.list[idx] : idx;
+                const int ab = A.ap[row], ae = A.ap[row + 1];
                 int n = 0;
-                for (int k = A.ap[row]; k < A.ap[row + 1]; ++k)
+                for (int k = ab; k < ae; ++k)
                     n += A.bp[A.ac[k] + 1] - A.bp[A.ac[k]];
                 int hbits = 6;
                 while ((1 << hbits) < 2 * n)
@@ -370,25 +371,58 @@ namespace apf
                 for (int t = lane; t < H; t += 32)
                     tkeys[t] = -1;
                 __syncwarp();
-                // distinct columns
-                for (int k = A.ap[row]; k < A.ap[row + 1]; ++k)
-                {
-                    const int j = A.ac[k];
-                    for (int q = A.bp[j] + lane; q < A.bp[j + 1]; q += 32)
+                // every product (ok, column, value) in generation order, 32 lanes at a time
+                auto for_each = [&](auto&& f) {
+                    for (int kb = ab; kb < ae; kb += kSeg)
                     {
-                        const int col = A.bc[q];
-                        unsigned h = hash_slot(col, hbits);
-                        while (true)
+                        const int cnt = min(ae - kb, kSeg);
+                        for (int i = lane; i < cnt; i += 32)
+                            seg[i + 1] = A.bp[A.ac[kb + i] + 1] - A.bp[A.ac[kb + i]];
+                        __syncwarp();
+                        for (int i0 = 0, carry = 0; i0 < cnt; i0 += 32)
                         {
-                            const int prev = atomicCAS(tkeys + h, -1, col);
-                            if (prev == -1 || prev == col)
-                                break;
-                            h = (h + 1) & (H - 1);
+                            int v = i0 + lane < cnt ? seg[i0 + lane + 1] : 0;
+                            for (int o = 1; o < 32; o <<= 1)
+                            {
+                                const int u = __shfl_up_sync(0xffffffffu, v, o);
+                                if (lane >= o)
+                                    v += u;
+                            }
+                            __syncwarp();
+                            if (i0 + lane < cnt)
+                                seg[i0 + lane + 1] = carry + v;
+                            carry += __shfl_sync(0xffffffffu, v, 31);
+                            __syncwarp();
                         }
+                        if (lane == 0)
+                            seg[0] = 0;
+                        __syncwarp();
+                        const int nb = seg[cnt];
+                        for (int t0 = 0; t0 < nb; t0 += 32)
+                        {
+                            const int t = t0 + lane;
+                            const bool ok = t < nb;
+                            int col = 0;
+                            double v = 0.0;
+                            if (ok)
+                            {
+                                const int i = find_segment(seg, cnt, t);
+                                const int k = kb + i;
+                                const int q = A.bp[A.ac[k]] + (t - seg[i]);
+                                col = A.bc[q];
+                                v = A.av[k] * A.bv[q];
+                            }
+                            f(ok, col, v);
+                        }
+                        __syncwarp();
                     }
-                }
+                };
+                for_each([&](bool ok, int col, double) {
+                    if (ok)
+                        hash_insert(tkeys, col, hbits);
+                });
                 __syncwarp();
-                // compact and sort them: key = column (high) | table slot (low)
+                // compact and sort the distinct columns: key = column (high) | table slot (low)
                 int u = 0;
                 for (int t0 = 0; t0 < H; t0 += 32)
                 {
@@ -416,21 +450,10 @@ namespace apf
                 for (int k = lane; k < u; k += 32)
                     acc[k] = 0.0;
                 __syncwarp();
-                // sums in generation order
-                for (int k = A.ap[row]; k < A.ap[row + 1]; ++k)
-                {
-                    const int j = A.ac[k];
-                    const double a = A.av[k];
-                    for (int q = A.bp[j] + lane; q < A.bp[j + 1]; q += 32)
-                    {
-                        const int col = A.bc[q];
-                        unsigned h = hash_slot(col, hbits);
-                        while (tkeys[h] != col)
-                            h = (h + 1) & (H - 1);
-                        acc[tranks[h]] += a * A.bv[q];
-                    }
-                    __syncwarp();
-                }
+                for_each([&](bool ok, int col, double v) {
+                    const int r = ok ? hash_rank(tkeys, tranks, col, hbits) : 0;
+                    ordered_add(acc, stage, ok, r, v, lane);
+                });
                 for (int k = lane; k < u; k += 32)
                     A.cv[base + k] = acc[k];
                 if (lane == 0)
@@ -913,8 +936,8 @@ namespace apf
         bucket_rows(s, A.rows, cand.get(), kCaps, 5, rb);
         auto launch = [&](auto tag) {
             constexpr int CAP = decltype(tag)::value;
-            const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 24)));
-            const size_t smem = (size_t)warps * CAP * 24;
+            const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 24 + kRowExtra)));
+            const size_t smem = (size_t)warps * (CAP * 24 + kRowExtra);
             const int blocks = blocks_for(g.nlist, warps, 148 * 32);
             APF_CUDA(cudaFuncSetAttribute(spgemm_rows<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             APF_KERNEL("spgemm_fill", s);
