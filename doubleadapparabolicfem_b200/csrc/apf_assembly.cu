@@ -677,6 +677,8 @@ namespace apf
         template<int CAP>
         __global__ void __launch_bounds__(256) hhat_rows(HhatArgs A)
         {
+            // CAP bounds the row's distinct columns (not its candidates, which stream through):
+            // a row with more is marked (row_count = -1) and left for a larger CAP
             extern __shared__ unsigned char smem_raw[];
             const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
             unsigned char* mine = smem_raw + (size_t)w * (CAP * 36 + kRowExtra);
@@ -766,28 +768,30 @@ namespace apf
                 int n = (A.c_ptr[row + 1] - A.c_ptr[row]) + (A.ax_ptr[row + 1] - A.ax_ptr[row]);
                 for (int k = A.bd_ptr[row]; k < A.bd_ptr[row + 1]; ++k)
                     n += A.bt_ptr[A.bd_col[k] + 1] - A.bt_ptr[A.bd_col[k]];
-                if (n > CAP)
-                {
-                    if (lane == 0)
-                    {
-                        atomicExch(A.status, APF_ERR_CAPACITY);
-                        A.row_count[row] = 0;
-                    }
-                    __syncwarp();
-                    continue;
-                }
+                // table at most half full: 2 min(n, CAP) slots (+ one group of 32 beyond CAP
+                // before the overflow is seen)
                 int hbits = 6;
-                while ((1 << hbits) < 2 * n)
+                while ((1 << hbits) < 2 * min(n, CAP))
                     ++hbits;
                 const int H = 1 << hbits;
                 for (int t = lane; t < H; t += 32)
                     tkeys[t] = -1;
                 __syncwarp();
+                int distinct = 0;
+                bool overflow = false;
                 for_each([&](bool ok, int col, double, bool) {
-                    if (ok)
-                        hash_insert(tkeys, col, hbits);
+                    const bool fresh = ok && !overflow && hash_insert_new(tkeys, col, hbits);
+                    distinct += __popc(__ballot_sync(0xffffffffu, fresh));
+                    overflow = overflow || distinct > CAP;
                 });
                 __syncwarp();
+                if (overflow)
+                {
+                    if (lane == 0)
+                        A.row_count[row] = -1;
+                    __syncwarp();
+                    continue;
+                }
                 int u = 0;
                 for (int t0 = 0; t0 < H; t0 += 32)
                 {
@@ -845,6 +849,22 @@ namespace apf
                     A.row_count[row] = kept;
                 __syncwarp();
             }
+        }
+
+        // rows (of list, or all) whose count is the overflow mark -1
+        __global__ void overflow_flags(int n, const int* __restrict__ list, const int* __restrict__ counts,
+                                       int* __restrict__ flag)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                flag[i] = counts[list ? list[i] : i] < 0 ? 1 : 0;
+        }
+
+        __global__ void overflow_compact(int n, const int* __restrict__ list, const int* __restrict__ flag,
+                                         const int* __restrict__ pos, int* __restrict__ out)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                if (flag[i])
+                    out[pos[i]] = list ? list[i] : i;
         }
 
         // one warp per row: the row's kept entries from its staging segment to the result
@@ -1191,10 +1211,7 @@ namespace apf
         const long long total = exclusive_scan(cand.get(), cand_ptr.get(), n_u, s);
         DeviceBuffer<int> tc(static_cast<std::size_t>(std::max(total, 1ll)), s);
         DeviceBuffer<double> tv(static_cast<std::size_t>(std::max(total, 1ll)), s);
-        int cap = 0;
-        APF_CUDA(cudaMemcpyAsync(&cap, bound.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-        sync(s);
-        auto run = [&](auto cap_tag, bool) {
+        auto run = [&](auto cap_tag) {
             constexpr int CAP = decltype(cap_tag)::value;
             const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 36 + kRowExtra)));
             const int threads = warps * 32;
@@ -1205,38 +1222,48 @@ namespace apf
             hhat_rows<CAP><<<blocks, threads, smem, s>>>(a);
             APF_CUDA(cudaGetLastError());
         };
-        auto dispatch = [&](bool fill) {
-            if (n_u == 0) return;
-            if (cap <= 256) run(std::integral_constant<int, 256>{}, fill);
-            else if (cap <= 512) run(std::integral_constant<int, 512>{}, fill);
-            else if (cap <= 1024) run(std::integral_constant<int, 1024>{}, fill);
-            else if (cap <= 2048) run(std::integral_constant<int, 2048>{}, fill);
-            else if (cap <= 4096) run(std::integral_constant<int, 4096>{}, fill);
-            else throw Error(APF_ERR_CAPACITY, "graph norm: a row has more than 4096 candidates");
-        };
         a.row_ptr = cand_ptr.get();
         a.col_out = tc.get();
         a.val_out = tv.get();
-        // rows by candidate count, each class with its own shared-memory capacity
-        static constexpr int kCaps[5] = {256, 512, 1024, 2048, 4096};
-        RowBuckets rb;
-        if (n_u > 0 && cap <= 4096)
+        // every row with room for 128 distinct columns (the candidates stream through), then
+        // the rows that had more with 1024, then 4096
+        a.list = nullptr;
+        a.nlist = n_u;
+        if (n_u > 0)
+            run(std::integral_constant<int, 128>{});
+        DeviceBuffer<int> oflag(static_cast<std::size_t>(n_u) + 1, s), opos(static_cast<std::size_t>(n_u) + 1, s),
+            olist(static_cast<std::size_t>(std::max(n_u, 1)), s);
+        for (int pass = 0; pass < 2 && n_u > 0; ++pass)
         {
-            bucket_rows(s, n_u, cand.get(), kCaps, 5, rb);
-            for (int b = 0; b < 5; ++b)
             {
-                a.list = rb.list.get() + rb.offsets[b];
-                a.nlist = rb.offsets[b + 1] - rb.offsets[b];
-                if (a.nlist == 0)
-                    continue;
-                const int keep = cap;
-                cap = kCaps[b];
-                dispatch(true);
-                cap = keep;
+                APF_KERNEL("hhat_overflow_rows", s);
+                overflow_flags<<<grid_for(n_u, 256), 256, 0, s>>>(a.list ? a.nlist : n_u, a.list, counts.get(),
+                                                                 oflag.get());
             }
+            const int nover = static_cast<int>(exclusive_scan(oflag.get(), opos.get(), a.list ? a.nlist : n_u, s));
+            if (nover == 0)
+                break;
+            DeviceBuffer<int> next(static_cast<std::size_t>(nover), s);
+            {
+                APF_KERNEL("hhat_overflow_rows", s);
+                overflow_compact<<<grid_for(n_u, 256), 256, 0, s>>>(a.list ? a.nlist : n_u, a.list, oflag.get(),
+                                                                   opos.get(), next.get());
+            }
+            olist = std::move(next);
+            a.list = olist.get();
+            a.nlist = nover;
+            if (pass == 0)
+                run(std::integral_constant<int, 1024>{});
+            else
+                run(std::integral_constant<int, 4096>{});
         }
-        else
-            dispatch(true);
+        if (n_u > 0 && a.list)
+        {
+            APF_KERNEL("hhat_overflow_rows", s);
+            overflow_flags<<<grid_for(n_u, 256), 256, 0, s>>>(a.nlist, a.list, counts.get(), oflag.get());
+            if (exclusive_scan(oflag.get(), opos.get(), a.nlist, s) != 0)
+                throw Error(APF_ERR_CAPACITY, "graph norm: a row has more than 4096 distinct columns");
+        }
         H.rows = H.cols = n_u;
         H.row_ptr.allocate(static_cast<std::size_t>(n_u) + 1, s);
         const long long nnz = exclusive_scan(counts.get(), H.row_ptr.get(), n_u, s);

@@ -30,6 +30,22 @@ namespace apf
         }
     }
 
+    // insert col; true when it was not in the table yet
+    __device__ __forceinline__ bool hash_insert_new(int* tkeys, int col, int hbits)
+    {
+        const int H = 1 << hbits;
+        unsigned h = hash_slot(col, hbits);
+        while (true)
+        {
+            const int prev = atomicCAS(tkeys + h, -1, col);
+            if (prev == -1)
+                return true;
+            if (prev == col)
+                return false;
+            h = (h + 1) & (H - 1);
+        }
+    }
+
     __device__ __forceinline__ int hash_rank(const int* tkeys, const int* tranks, int col, int hbits)
     {
         const int H = 1 << hbits;
