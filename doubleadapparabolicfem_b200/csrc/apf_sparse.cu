@@ -364,8 +364,10 @@ namespace apf
                 int n = 0;
                 for (int k = ab; k < ae; ++k)
                     n += A.bp[A.ac[k] + 1] - A.bp[A.ac[k]];
+                // table at most half full: 2 min(n, CAP) slots (CAP bounds the distinct columns;
+                // a row with more is marked count = -1 and left for a larger CAP)
                 int hbits = 6;
-                while ((1 << hbits) < 2 * n)
+                while ((1 << hbits) < 2 * min(n, CAP))
                     ++hbits;
                 const int H = 1 << hbits;
                 for (int t = lane; t < H; t += 32)
@@ -417,11 +419,21 @@ namespace apf
                         __syncwarp();
                     }
                 };
+                int distinct = 0;
+                bool overflow = false;
                 for_each([&](bool ok, int col, double) {
-                    if (ok)
-                        hash_insert(tkeys, col, hbits);
+                    const bool fresh = ok && !overflow && hash_insert_new(tkeys, col, hbits);
+                    distinct += __popc(__ballot_sync(0xffffffffu, fresh));
+                    overflow = overflow || distinct > CAP;
                 });
                 __syncwarp();
+                if (overflow)
+                {
+                    if (lane == 0)
+                        A.count[row] = -1;
+                    __syncwarp();
+                    continue;
+                }
                 // compact and sort the distinct columns: key = column (high) | table slot (low)
                 int u = 0;
                 for (int t0 = 0; t0 < H; t0 += 32)
@@ -460,6 +472,22 @@ namespace apf
                     A.count[row] = u;
                 __syncwarp();
             }
+        }
+
+        // rows (of list, or all) whose count is the overflow mark -1, and their list
+        __global__ void overflow_rows(int n, const int* __restrict__ list, const int* __restrict__ counts,
+                                      int* __restrict__ flag)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                flag[i] = counts[list ? list[i] : i] < 0 ? 1 : 0;
+        }
+
+        __global__ void overflow_list(int n, const int* __restrict__ list, const int* __restrict__ flag,
+                                      const int* __restrict__ pos, int* __restrict__ out)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                if (flag[i])
+                    out[pos[i]] = list ? list[i] : i;
         }
 
         // class of every row; per-block histograms in shared memory, one global atomic per
@@ -929,27 +957,46 @@ namespace apf
         DeviceBuffer<double> tv(static_cast<std::size_t>(std::max(total, 1ll)), s);
         GemmArgs g{A.rows, A.row_ptr.get(), A.col_idx.get(), A.values.get(), B.row_ptr.get(), B.col_idx.get(),
                    B.values.get(), count.get(), cand_ptr.get(), tc.get(), tv.get(), nullptr, 0};
-        // rows by candidate count: each class runs with its own shared-memory capacity, so
-        // the few long rows no longer set the occupancy of all the others
-        static constexpr int kCaps[5] = {64, 256, 1024, 4096, 8192};
-        RowBuckets rb;
-        bucket_rows(s, A.rows, cand.get(), kCaps, 5, rb);
+        // every row with room for 128 distinct columns (the candidates stream through), then
+        // the rows that had more with 1024, then 8192
         auto launch = [&](auto tag) {
             constexpr int CAP = decltype(tag)::value;
             const int warps = std::max(1, std::min(8, (96 * 1024) / (CAP * 24 + kRowExtra)));
             const size_t smem = (size_t)warps * (CAP * 24 + kRowExtra);
-            const int blocks = blocks_for(g.nlist, warps, 148 * 32);
+            const int blocks = blocks_for(g.list ? g.nlist : A.rows, warps, 148 * 32);
             APF_CUDA(cudaFuncSetAttribute(spgemm_rows<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             APF_KERNEL("spgemm_fill", s);
             spgemm_rows<CAP><<<blocks, warps * 32, smem, s>>>(g);
             APF_CUDA(cudaGetLastError());
         };
-        for (int b = 0; b < 5; ++b)
+        g.list = nullptr;
+        g.nlist = A.rows;
+        launch(std::integral_constant<int, 128>{});
+        DeviceBuffer<int> oflag(static_cast<std::size_t>(A.rows) + 1, s), opos(static_cast<std::size_t>(A.rows) + 1, s),
+            olist(1, s);
+        for (int pass = 0; pass < 3; ++pass)
         {
-            g.list = rb.list.get() + rb.offsets[b];
-            g.nlist = rb.offsets[b + 1] - rb.offsets[b];
-            if (g.nlist > 0)
-                with_cap(kCaps[b], [&](auto tag) { launch(tag); });
+            const int nin = g.list ? g.nlist : A.rows;
+            {
+                APF_KERNEL("spgemm_overflow_rows", s);
+                overflow_rows<<<blocks_for(nin, 256), 256, 0, s>>>(nin, g.list, count.get(), oflag.get());
+            }
+            const int nover = static_cast<int>(exclusive_scan(oflag.get(), opos.get(), nin, s));
+            if (nover == 0)
+                break;
+            require(pass < 2, APF_ERR_CAPACITY, "sparse product: a row has more than 8192 distinct columns");
+            DeviceBuffer<int> next(static_cast<std::size_t>(nover), s);
+            {
+                APF_KERNEL("spgemm_overflow_rows", s);
+                overflow_list<<<blocks_for(nin, 256), 256, 0, s>>>(nin, g.list, oflag.get(), opos.get(), next.get());
+            }
+            olist = std::move(next);
+            g.list = olist.get();
+            g.nlist = nover;
+            if (pass == 0)
+                launch(std::integral_constant<int, 1024>{});
+            else
+                launch(std::integral_constant<int, 8192>{});
         }
         const long long nnz = exclusive_scan(count.get(), C.row_ptr.get(), A.rows, s);
         C.col_idx.allocate(static_cast<std::size_t>(nnz), s);
