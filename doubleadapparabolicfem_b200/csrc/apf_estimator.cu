@@ -26,6 +26,7 @@
 #include <cstring>
 #include <future>
 #include <numeric>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -1397,70 +1398,146 @@ namespace apf
     void build_patches(const std::vector<double>& times, const std::vector<int>& vids, int n_cells, PatchSet& ps)
     {
         // slabs by the exact time interval of their cells (mesh times are dyadic; stacked
-        // independent problems may share a start time with different steps)
-        auto less = [&](int a, int b) {
-            const double a0 = times[2ll * a], b0 = times[2ll * b];
-            return a0 < b0 || (a0 == b0 && times[2ll * a + 1] < times[2ll * b + 1]);
-        };
-        auto same = [&](int a, int b) {
-            return times[2ll * a] == times[2ll * b] && times[2ll * a + 1] == times[2ll * b + 1];
-        };
-        std::vector<int> order(n_cells);
-        std::iota(order.begin(), order.end(), 0);
-        if (!std::is_sorted(order.begin(), order.end(), less)) // cells usually come slab by slab
-            std::stable_sort(order.begin(), order.end(), less);
-        ps.slab_ptr.assign(1, 0);
-        ps.slab_cells.clear();
-        ps.slab_cells.reserve(n_cells);
-        for (int i = 0; i < n_cells; ++i)
+        // independent problems may share a start time with different steps): the distinct
+        // intervals in time order, then a stable counting sort of the cells into them
+        struct PairHash
         {
-            if (i > 0 && !same(order[i], order[i - 1]))
-                ps.slab_ptr.push_back(i);
-            ps.slab_cells.push_back(order[i]);
+            std::size_t operator()(const std::pair<double, double>& p) const noexcept
+            {
+                std::uint64_t a, b;
+                std::memcpy(&a, &p.first, 8);
+                std::memcpy(&b, &p.second, 8);
+                return static_cast<std::size_t>((a * 0x9E3779B97F4A7C15ull) ^ (b + 0x632BE59BD9B4E019ull + (a << 6)));
+            }
+        };
+        std::vector<int> cell_slab(n_cells);
+        {
+            // open-addressing table of the distinct intervals (at most half full, grown by doubling)
+            std::vector<std::pair<double, double>> intervals;
+            std::vector<int> table(64, -1);
+            const PairHash hasher;
+            auto find_or_add = [&](const std::pair<double, double>& key) {
+                std::size_t mask = table.size() - 1, h = hasher(key) & mask;
+                while (table[h] >= 0 && intervals[table[h]] != key)
+                    h = (h + 1) & mask;
+                if (table[h] >= 0)
+                    return table[h];
+                const int id = static_cast<int>(intervals.size());
+                intervals.push_back(key);
+                table[h] = id;
+                if (2 * intervals.size() > table.size())
+                {
+                    std::vector<int> bigger(table.size() * 2, -1);
+                    const std::size_t m2 = bigger.size() - 1;
+                    for (std::size_t q = 0; q < intervals.size(); ++q)
+                    {
+                        std::size_t g = hasher(intervals[q]) & m2;
+                        while (bigger[g] >= 0)
+                            g = (g + 1) & m2;
+                        bigger[g] = static_cast<int>(q);
+                    }
+                    table.swap(bigger);
+                }
+                return id;
+            };
+            int last = -1;
+            std::pair<double, double> last_key{0.0, 0.0};
+            for (int c = 0; c < n_cells; ++c)
+            {
+                const std::pair<double, double> key{times[2ll * c], times[2ll * c + 1]};
+                if (last < 0 || key != last_key)
+                {
+                    last = find_or_add(key);
+                    last_key = key;
+                }
+                cell_slab[c] = last;
+            }
+            // renumber the intervals in time order
+            std::vector<int> by_time(intervals.size());
+            std::iota(by_time.begin(), by_time.end(), 0);
+            std::sort(by_time.begin(), by_time.end(), [&](int a, int b) { return intervals[a] < intervals[b]; });
+            std::vector<int> rank(intervals.size());
+            for (std::size_t k = 0; k < by_time.size(); ++k)
+                rank[by_time[k]] = static_cast<int>(k);
+            for (int c = 0; c < n_cells; ++c)
+                cell_slab[c] = rank[cell_slab[c]];
+            ps.slab_ptr.assign(intervals.size() + 1, 0);
         }
-        ps.slab_ptr.push_back(n_cells);
+        for (int c = 0; c < n_cells; ++c)
+            ++ps.slab_ptr[cell_slab[c] + 1];
+        for (std::size_t k = 1; k < ps.slab_ptr.size(); ++k)
+            ps.slab_ptr[k] += ps.slab_ptr[k - 1];
+        ps.slab_cells.assign(n_cells, 0);
+        {
+            std::vector<int> cursor(ps.slab_ptr.begin(), ps.slab_ptr.end() - 1);
+            for (int c = 0; c < n_cells; ++c)
+                ps.slab_cells[cursor[cell_slab[c]]++] = c;
+        }
         const int n_slabs = static_cast<int>(ps.slab_ptr.size()) - 1;
-        for (int s = 0; s < n_slabs; ++s)
-        {
-            const double t1 = times[2ll * ps.slab_cells[ps.slab_ptr[s]] + 1];
-            for (int i = ps.slab_ptr[s]; i < ps.slab_ptr[s + 1]; ++i)
-                require(times[2ll * ps.slab_cells[i] + 1] == t1, APF_ERR_INVALID,
-                        "estimator: the cells of a time slab must share their time interval");
-        }
         // group slabs with identical spatial meshes (same vertex-id sequence)
         std::vector<int> group_of(n_slabs, -1);
         std::vector<int> group_rep;
-        std::unordered_map<std::uint64_t, std::vector<int>> by_hash;
-        for (int s = 0; s < n_slabs; ++s)
-        {
+        // slab fingerprints on a few host threads, then groups by fingerprint with an exact
+        // comparison against each group's first slab (also threaded)
+        const int nthreads = std::max(1, std::min<int>(8, static_cast<int>(std::thread::hardware_concurrency())));
+        auto parallel_slabs = [&](auto&& body) {
+            std::vector<std::thread> pool;
+            for (int t = 0; t < nthreads; ++t)
+                pool.emplace_back([&, t]() {
+                    for (int sl = t; sl < n_slabs; sl += nthreads)
+                        body(sl);
+                });
+            for (auto& th : pool)
+                th.join();
+        };
+        std::vector<std::uint64_t> fp(n_slabs);
+        parallel_slabs([&](int sl) {
             std::uint64_t h = 1469598103934665603ull;
-            for (int i = ps.slab_ptr[s]; i < ps.slab_ptr[s + 1]; ++i)
+            for (int i = ps.slab_ptr[sl]; i < ps.slab_ptr[sl + 1]; ++i)
                 for (int k = 0; k < 3; ++k)
                     h = (h ^ static_cast<std::uint64_t>(vids[3ll * ps.slab_cells[i] + k])) * 1099511628211ull;
-            auto& cand = by_hash[h];
-            for (int g : cand)
+            fp[sl] = h;
+        });
+        auto same_mesh = [&](int a, int r) {
+            const int len = ps.slab_ptr[a + 1] - ps.slab_ptr[a];
+            if (len != ps.slab_ptr[r + 1] - ps.slab_ptr[r])
+                return false;
+            for (int i = 0; i < len; ++i)
+                for (int k = 0; k < 3; ++k)
+                    if (vids[3ll * ps.slab_cells[ps.slab_ptr[a] + i] + k] != vids[3ll * ps.slab_cells[ps.slab_ptr[r] + i] + k])
+                        return false;
+            return true;
+        };
+        std::unordered_map<std::uint64_t, int> first_of;
+        std::vector<int> tentative(n_slabs);
+        for (int sl = 0; sl < n_slabs; ++sl)
+            tentative[sl] = first_of.emplace(fp[sl], sl).first->second;
+        std::vector<char> confirmed(n_slabs, 1);
+        parallel_slabs([&](int sl) {
+            if (tentative[sl] != sl)
+                confirmed[sl] = same_mesh(sl, tentative[sl]) ? 1 : 0;
+        });
+        std::vector<int> group_of_rep(n_slabs, -1);
+        for (int sl = 0; sl < n_slabs; ++sl)
+        {
+            int r = tentative[sl];
+            if (r != sl && !confirmed[sl])
             {
-                const int r = group_rep[g];
-                const int len = ps.slab_ptr[s + 1] - ps.slab_ptr[s];
-                if (len != ps.slab_ptr[r + 1] - ps.slab_ptr[r])
-                    continue;
-                bool same = true;
-                for (int i = 0; i < len && same; ++i)
-                    for (int k = 0; k < 3 && same; ++k)
-                        same = vids[3ll * ps.slab_cells[ps.slab_ptr[s] + i] + k] ==
-                               vids[3ll * ps.slab_cells[ps.slab_ptr[r] + i] + k];
-                if (same)
-                {
-                    group_of[s] = g;
-                    break;
-                }
+                // equal fingerprints of different meshes: compare with every group so far
+                r = sl;
+                for (std::size_t g = 0; g < group_rep.size(); ++g)
+                    if (same_mesh(sl, group_rep[g]))
+                    {
+                        r = group_rep[g];
+                        break;
+                    }
             }
-            if (group_of[s] < 0)
+            if (r == sl)
             {
-                group_of[s] = static_cast<int>(group_rep.size());
-                cand.push_back(group_of[s]);
-                group_rep.push_back(s);
+                group_of_rep[sl] = static_cast<int>(group_rep.size());
+                group_rep.push_back(sl);
             }
+            group_of[sl] = group_of_rep[r];
         }
         // topology patches of every group
         ps.topo_ptr.assign(1, 0);
@@ -1477,49 +1554,82 @@ namespace apf
             const int s = group_rep[g];
             const int b = ps.slab_ptr[s], len = ps.slab_ptr[s + 1] - b;
             auto vid = [&](int local, int k) { return vids[3ll * ps.slab_cells[b + local] + k]; };
-            // edge multiplicity in the slab mesh
-            std::unordered_map<std::uint64_t, int> edge_count;
-            edge_count.reserve(static_cast<std::size_t>(len) * 3);
+            // edge multiplicity in the slab mesh: all edge keys sorted, counts by run length
             auto ekey = [](int p, int q) {
                 const std::uint32_t lo = static_cast<std::uint32_t>(std::min(p, q)), hi = static_cast<std::uint32_t>(std::max(p, q));
                 return (static_cast<std::uint64_t>(lo) << 32) | hi;
             };
+            std::vector<std::uint64_t> ekeys(3ll * len);
+            std::vector<int> eorder(3ll * len), ecount(3ll * len);
             for (int i = 0; i < len; ++i)
                 for (int k = 0; k < 3; ++k)
-                    ++edge_count[ekey(vid(i, (k + 1) % 3), vid(i, (k + 2) % 3))];
+                    ekeys[3ll * i + k] = ekey(vid(i, (k + 1) % 3), vid(i, (k + 2) % 3));
+            std::iota(eorder.begin(), eorder.end(), 0);
+            std::sort(eorder.begin(), eorder.end(), [&](int a, int b) { return ekeys[a] < ekeys[b]; });
+            for (std::size_t e = 0; e < eorder.size();)
+            {
+                std::size_t f = e + 1;
+                while (f < eorder.size() && ekeys[eorder[f]] == ekeys[eorder[e]])
+                    ++f;
+                for (std::size_t q = e; q < f; ++q)
+                    ecount[eorder[q]] = static_cast<int>(f - e);
+                e = f;
+            }
             // vertex -> incident (local cell, local vertex), vertices in first-appearance order
-            std::unordered_map<int, int> vindex;
-            std::vector<std::vector<std::pair<int, int>>> inc;
-            std::vector<char> vbound;
+            int vmax = -1;
+            for (int i = 0; i < len; ++i)
+                for (int k = 0; k < 3; ++k)
+                    vmax = std::max(vmax, vid(i, k));
+            std::vector<int> vindex(static_cast<std::size_t>(vmax) + 1, -1);
+            std::vector<int> vfirst; // first incidence of each vertex, then counting sort
+            std::vector<int> vcount;
             for (int i = 0; i < len; ++i)
                 for (int k = 0; k < 3; ++k)
                 {
-                    auto it = vindex.find(vid(i, k));
-                    int vi;
-                    if (it == vindex.end())
+                    int& vi = vindex[vid(i, k)];
+                    if (vi < 0)
                     {
-                        vi = static_cast<int>(inc.size());
-                        vindex.emplace(vid(i, k), vi);
-                        inc.emplace_back();
-                        vbound.push_back(0);
+                        vi = static_cast<int>(vcount.size());
+                        vcount.push_back(0);
                     }
-                    else
-                        vi = it->second;
-                    inc[vi].emplace_back(i, k);
+                    ++vcount[vi];
                 }
-            for (int i = 0; i < len; ++i)
-                for (int k = 0; k < 3; ++k)
-                    if (edge_count[ekey(vid(i, (k + 1) % 3), vid(i, (k + 2) % 3))] == 1)
-                    {
-                        vbound[vindex[vid(i, (k + 1) % 3)]] = 1;
-                        vbound[vindex[vid(i, (k + 2) % 3)]] = 1;
-                    }
+            const int nv = static_cast<int>(vcount.size());
+            std::vector<int> vptr(nv + 1, 0);
+            for (int v = 0; v < nv; ++v)
+                vptr[v + 1] = vptr[v] + vcount[v];
+            std::vector<std::pair<int, int>> incs(vptr[nv]);
+            {
+                std::vector<int> cur(vptr.begin(), vptr.end() - 1);
+                for (int i = 0; i < len; ++i)
+                    for (int k = 0; k < 3; ++k)
+                        incs[cur[vindex[vid(i, k)]]++] = {i, k};
+            }
+            std::vector<char> vbound(nv, 0);
+            for (std::size_t e = 0; e < ekeys.size(); ++e)
+                if (ecount[e] == 1)
+                {
+                    vbound[vindex[static_cast<int>(ekeys[e] >> 32)]] = 1;
+                    vbound[vindex[static_cast<int>(ekeys[e] & 0xffffffffu)]] = 1;
+                }
+            struct IncRange
+            {
+                const std::pair<int, int>* b;
+                const std::pair<int, int>* e;
+                const std::pair<int, int>* begin() const { return b; }
+                const std::pair<int, int>* end() const { return e; }
+                std::size_t size() const { return static_cast<std::size_t>(e - b); }
+            };
+            std::vector<IncRange> inc(nv);
+            for (int v = 0; v < nv; ++v)
+                inc[v] = IncRange{incs.data() + vptr[v], incs.data() + vptr[v + 1]};
             group_first[g] = static_cast<int>(ps.topo_nfree.size());
             group_count[g] = static_cast<int>(inc.size());
             for (std::size_t v = 0; v < inc.size(); ++v)
             {
                 const bool boundary = vbound[v] != 0;
-                std::unordered_map<std::uint64_t, int> free_id;
+                std::vector<std::uint64_t> free_id; // free edges of the patch, in first-seen order
+                free_id.reserve(16);
                 int nfree = 0;
                 for (const auto& [i, a] : inc[v])
                 {
@@ -1529,17 +1639,22 @@ namespace apf
                     for (int k = 0; k < 3; ++k)
                     {
                         const int P = vid(i, (k + 1) % 3), Q = vid(i, (k + 2) % 3);
-                        const std::uint64_t ek = ekey(P, Q);
-                        const int cnt = edge_count[ek];
+                        const std::uint64_t ek = ekeys[3ll * i + k];
+                        const int cnt = ecount[3ll * i + k];
                         const bool touches = P == va || Q == va;
                         const bool is_free = (touches && cnt == 2) || (boundary && cnt == 1);
                         int code = 0xffff;
                         if (is_free)
                         {
-                            auto it = free_id.find(ek);
-                            if (it == free_id.end())
-                                it = free_id.emplace(ek, nfree++).first;
-                            code = it->second;
+                            int id = 0;
+                            while (id < nfree && free_id[id] != ek)
+                                ++id;
+                            if (id == nfree)
+                            {
+                                free_id.push_back(ek);
+                                ++nfree;
+                            }
+                            code = id;
                         }
                         if (P > Q)
                             code |= 1 << 30; // local parameterisation runs from the higher to the lower id
