@@ -250,180 +250,178 @@ namespace apf
             int* status;         // nonzero on overflow
             const int* list;     // rows to process (null: all)
             int nlist;
+            int kmax;            // restriction entries per local row (at most 4)
         };
 
-        // One warp per row.  CAP candidates per warp in shared memory.
-        template<int CAP, bool FILL>
-        __global__ void __launch_bounds__(128) gather_rows(GatherArgs A)
+        // One warp per row with at most UCAP distinct columns, in one pass over the candidates:
+        // per term, the row's incidences staged and ordered by (cell * ndof + i); then every
+        // (incidence, local column j, restriction entry q) candidate with |local| > zero_tol,
+        // 32 items at a time, is added to its column's slot of a shared-memory hash table
+        // (at most half full) in generation order (within 32 items: by restriction entry,
+        // then lane); at the end only the distinct columns are sorted.  A row with more than
+        // UCAP distinct columns is marked row_count = -1 and left for a larger UCAP.
+        // Shared memory per warp: incidences int[2 kIncCap + 2], table keys int[2 UCAP],
+        // table sums double[2 UCAP], sorted keys 8 B x UCAP, staged values double[32].
+        constexpr int kGatherIncCap = 256;
+
+        template<int UCAP>
+        __host__ __device__ constexpr std::size_t gather_u_warp_bytes()
         {
-            constexpr int kIncCap = 256;
+            return ((sizeof(int) * (2 * kGatherIncCap + 2) + 32 * UCAP + 32 * 8) + 15) / 16 * 16;
+        }
+
+        template<int UCAP>
+        __global__ void __launch_bounds__(128) gather_rows_u(GatherArgs A)
+        {
             extern __shared__ unsigned char smem_raw[];
             const int warps = blockDim.x >> 5;
             const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-            unsigned long long* keys = reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)w * CAP;
-            double* vals = reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) + (size_t)warps * CAP) +
-                           (size_t)w * CAP;
-            int* incs = reinterpret_cast<int*>(reinterpret_cast<double*>(reinterpret_cast<unsigned long long*>(smem_raw) +
-                                                                         (size_t)warps * CAP) +
-                                               (size_t)warps * CAP) +
-                        (size_t)w * (2 * kIncCap + 1);
-            int* counter = incs + 2 * kIncCap;
+            unsigned char* mine = smem_raw + (size_t)w * gather_u_warp_bytes<UCAP>();
+            int* incs = reinterpret_cast<int*>(mine);
+            int* tkeys = incs + 2 * kGatherIncCap + 2;
+            double* tvals = reinterpret_cast<double*>(tkeys + 2 * UCAP);
+            unsigned long long* ukeys = reinterpret_cast<unsigned long long*>(tvals + 2 * UCAP);
+            double* stage = reinterpret_cast<double*>(ukeys + UCAP);
             const int ndof = A.ndof;
-
             const int nrows = A.list ? A.nlist : A.n_rows;
             for (int idx = blockIdx.x * warps + w; idx < nrows; idx += gridDim.x * warps)
             {
                 const int row = A.list ? A.list[idx] : idx;
-                if (lane == 0)
-                    *counter = 0;
-                __syncwarp();
-                int seq_base = 0;
-                bool overflow = false;
+                bool too_many_inc = false;
+                // every candidate (ok, column, value) in generation order; all lanes call f
+                auto for_each = [&](auto&& f) {
+                    for (int tt = 0; tt < A.n_terms; ++tt)
+                    {
+                        const Term T = A.term[tt];
+                        const int ib = T.inc_ptr[row], ie = T.inc_ptr[row + 1];
+                        const int n_inc = ie - ib;
+                        if (n_inc > kGatherIncCap)
+                        {
+                            too_many_inc = true;
+                            return;
+                        }
+                        for (int k = lane; k < n_inc; k += 32)
+                        {
+                            const int2 v = T.inc[ib + k];
+                            incs[k] = v.x;
+                            incs[kGatherIncCap + k] = v.y;
+                        }
+                        __syncwarp();
+                        int my_ci[8], my_e[8], my_rank[8];
+                        int nm = 0;
+                        for (int k = lane; k < n_inc; k += 32, ++nm)
+                        {
+                            const int ci = incs[k];
+                            int rank = 0;
+                            for (int q = 0; q < n_inc; ++q)
+                                rank += incs[q] < ci;
+                            my_ci[nm] = ci;
+                            my_e[nm] = incs[kGatherIncCap + k];
+                            my_rank[nm] = rank;
+                        }
+                        __syncwarp();
+                        for (int q = 0; q < nm; ++q)
+                        {
+                            incs[my_rank[q]] = my_ci[q];
+                            incs[kGatherIncCap + my_rank[q]] = my_e[q];
+                        }
+                        __syncwarp();
+                        const double* rw = row_weights(A.d, T.kind);
+                        const int items = n_inc * ndof;
+                        for (int it0 = 0; it0 < items; it0 += 32)
+                        {
+                            const int it = it0 + lane;
+                            bool ok = false;
+                            double v = 0.0, wi = 0.0;
+                            const int* cd = nullptr;
+                            const double* cw = nullptr;
+                            int b = 0, e = 0;
+                            if (it < items)
+                            {
+                                const int t_idx = it / ndof, j = it % ndof;
+                                const int ci = incs[t_idx];
+                                const int c = ci / ndof, i = ci % ndof;
+                                wi = rw[incs[kGatherIncCap + t_idx]];
+                                v = local_entry(A.d, T.kind, c, i, j);
+                                ok = fabs(v) > A.d.zero_tol;
+                                if (ok)
+                                    col_restriction(A.d, T.kind, c, j, ndof, cd, cw, b, e);
+                            }
+                            for (int q = 0; q < A.kmax; ++q)
+                            {
+                                const bool has = ok && b + q < e;
+                                f(has, has ? cd[b + q] + T.col_offset : 0, has ? wi * cw[b + q] * v : 0.0);
+                            }
+                        }
+                        __syncwarp();
+                    }
+                };
+                int n = 0;
                 for (int tt = 0; tt < A.n_terms; ++tt)
+                    n += (A.term[tt].inc_ptr[row + 1] - A.term[tt].inc_ptr[row]) * ndof * A.kmax;
+                int hbits = 6;
+                while ((1 << hbits) < 2 * min(n, UCAP))
+                    ++hbits;
+                const int H = 1 << hbits;
+                for (int t = lane; t < H; t += 32)
                 {
-                    const Term T = A.term[tt];
-                    const int ib = T.inc_ptr[row], ie = T.inc_ptr[row + 1];
-                    const int n_inc = ie - ib;
-                    if (n_inc > kIncCap)
-                    {
-                        overflow = true;
-                        break;
-                    }
-                    // stage the incidence list and sort it by (cell*ndof+i) -> deterministic order
-                    for (int k = lane; k < n_inc; k += 32)
-                    {
-                        const int2 v = T.inc[ib + k];
-                        incs[k] = v.x;
-                        incs[kIncCap + k] = v.y;
-                    }
-                    __syncwarp();
-                    int my_ci[8], my_e[8], my_rank[8];
-                    int nm = 0;
-                    for (int k = lane; k < n_inc; k += 32, ++nm)
-                    {
-                        const int ci = incs[k];
-                        int rank = 0;
-                        for (int q = 0; q < n_inc; ++q)
-                            rank += incs[q] < ci;
-                        my_ci[nm] = ci;
-                        my_e[nm] = incs[kIncCap + k];
-                        my_rank[nm] = rank;
-                    }
-                    __syncwarp();
-                    for (int q = 0; q < nm; ++q)
-                    {
-                        incs[my_rank[q]] = my_ci[q];
-                        incs[kIncCap + my_rank[q]] = my_e[q];
-                    }
-                    __syncwarp();
-                    const double* rw = row_weights(A.d, T.kind);
-                    const int items = n_inc * ndof;
-                    for (int it = lane; it < items + ((32 - items % 32) % 32); it += 32)
-                    {
-                        const bool active = it < items;
-                        int nloc = 0;
-                        int cols_l[4];
-                        double vals_l[4];
-                        int seqs_l[4];
-                        int more = 0;
-                        if (active)
-                        {
-                            const int t_idx = it / ndof, j = it % ndof;
-                            const int ci = incs[t_idx];
-                            const int c = ci / ndof, i = ci % ndof;
-                            const double wi = rw[incs[kIncCap + t_idx]];
-                            const double v = local_entry(A.d, T.kind, c, i, j);
-                            if (fabs(v) > A.d.zero_tol)
-                            {
-                                const int* cd;
-                                const double* cw;
-                                int b, e;
-                                col_restriction(A.d, T.kind, c, j, ndof, cd, cw, b, e);
-                                for (int q = b; q < e; ++q)
-                                {
-                                    if (nloc < 4)
-                                    {
-                                        cols_l[nloc] = cd[q] + T.col_offset;
-                                        vals_l[nloc] = wi * cw[q] * v;
-                                        seqs_l[nloc] = seq_base + it * 4 + (q - b);
-                                        ++nloc;
-                                    }
-                                    else
-                                        more = 1;
-                                }
-                            }
-                        }
-                        if (__any_sync(0xffffffffu, more))
-                            overflow = true;
-                        // warp-aggregated append
-                        int incl = nloc;
-                        for (int o = 1; o < 32; o <<= 1)
-                        {
-                            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                            if (lane >= o) incl += y;
-                        }
-                        const int base = *counter;
-                        const int total = __shfl_sync(0xffffffffu, incl, 31);
-                        const int start = base + incl - nloc;
-                        for (int q = 0; q < nloc; ++q)
-                        {
-                            const int slot = start + q;
-                            if (slot < CAP)
-                            {
-                                keys[slot] = make_key(cols_l[q], seqs_l[q], slot);
-                                vals[slot] = vals_l[q];
-                            }
-                        }
-                        __syncwarp();
-                        if (lane == 0)
-                            *counter = base + total;
-                        __syncwarp();
-                    }
-                    seq_base += items * 4;
+                    tkeys[t] = -1;
+                    tvals[t] = 0.0;
                 }
-                const int n = *counter;
-                if (n > CAP || overflow || seq_base >= (1 << kSeqBits))
+                __syncwarp();
+                int distinct = 0;
+                bool overflow = false;
+                for_each([&](bool ok, int col, double v) {
+                    bool fresh = false;
+                    const bool live = ok && !overflow;
+                    const int h = live ? hash_slot_of(tkeys, col, hbits, fresh) : 0;
+                    distinct += __popc(__ballot_sync(0xffffffffu, fresh));
+                    ordered_add(tvals, stage, live, h, v, lane);
+                    overflow = overflow || distinct > UCAP;
+                });
+                __syncwarp();
+                if (too_many_inc)
                 {
                     if (lane == 0)
+                    {
                         atomicExch(A.status, APF_ERR_CAPACITY);
-                    if (lane == 0)
                         A.row_count[row] = 0;
+                    }
                     __syncwarp();
                     continue;
                 }
-                int np = 1;
-                while (np < n) np <<= 1;
-                for (int k = n + lane; k < np; k += 32)
-                    keys[k] = ~0ull;
-                __syncwarp();
-                warp_bitonic_sort(keys, np);
-                // heads of equal-column runs
-                int out_base = FILL ? A.row_ptr[row] : 0;
-                int uniq = 0;
-                for (int k0 = 0; k0 < n; k0 += 32)
+                if (overflow)
                 {
-                    const int k = k0 + lane;
-                    bool head = false;
-                    unsigned col = 0;
-                    if (k < n)
-                    {
-                        col = static_cast<unsigned>(keys[k] >> 32);
-                        head = (k == 0) || (static_cast<unsigned>(keys[k - 1] >> 32) != col);
-                    }
-                    const unsigned hm = __ballot_sync(0xffffffffu, head);
-                    if (FILL && head)
-                    {
-                        double s = 0.0;
-                        for (int q = k; q < n && static_cast<unsigned>(keys[q] >> 32) == col; ++q)
-                            s += vals[keys[q] & ((1u << kSlotBits) - 1)];
-                        const int pos = out_base + uniq + __popc(hm & ((1u << lane) - 1));
-                        A.col_out[pos] = static_cast<int>(col);
-                        A.val_out[pos] = s;
-                    }
-                    uniq += __popc(hm);
+                    if (lane == 0)
+                        A.row_count[row] = -1;
+                    __syncwarp();
+                    continue;
+                }
+                int u = 0;
+                for (int t0 = 0; t0 < H; t0 += 32)
+                {
+                    const int t = t0 + lane;
+                    const int key = tkeys[t];
+                    const unsigned m = __ballot_sync(0xffffffffu, key != -1);
+                    if (key != -1)
+                        ukeys[u + __popc(m & ((1u << lane) - 1))] =
+                            (static_cast<unsigned long long>(static_cast<unsigned>(key)) << 32) | static_cast<unsigned>(t);
+                    u += __popc(m);
+                }
+                const int np = next_pow2(u);
+                for (int k = u + lane; k < np; k += 32)
+                    ukeys[k] = ~0ull;
+                __syncwarp();
+                warp_bitonic_sort(ukeys, np);
+                const int out_base = A.row_ptr[row];
+                for (int k = lane; k < u; k += 32)
+                {
+                    const unsigned long long key = ukeys[k];
+                    A.col_out[out_base + k] = static_cast<int>(key >> 32);
+                    A.val_out[out_base + k] = tvals[static_cast<unsigned>(key)];
                 }
                 if (lane == 0)
-                    A.row_count[row] = uniq;
+                    A.row_count[row] = u;
                 __syncwarp();
             }
         }
@@ -973,33 +971,6 @@ namespace apf
             return d;
         }
 
-        template<int CAP>
-        void run_gather(cudaStream_t s, GatherArgs& a, int* status)
-        {
-            // shared memory per warp: CAP keys + CAP values + staged incidences
-            const int warps = CAP <= 2048 ? 4 : 1;
-            const int threads = warps * 32;
-            const size_t smem = (size_t)warps * CAP * 16 + (size_t)warps * (2 * 256 + 1) * sizeof(int);
-            if (smem > 48 * 1024)
-            {
-                APF_CUDA(cudaFuncSetAttribute(gather_rows<CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                APF_CUDA(cudaFuncSetAttribute(gather_rows<CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            }
-            const int blocks = grid_for(a.list ? a.nlist : a.n_rows, warps, 148 * 16);
-            (void)status;
-            if (a.row_ptr == nullptr)
-                {
-                    APF_KERNEL("gather_rows_count", s);
-                    gather_rows<CAP, false><<<blocks, threads, smem, s>>>(a);
-                }
-            else
-                {
-                    APF_KERNEL("gather_rows_fill", s);
-                    gather_rows<CAP, true><<<blocks, threads, smem, s>>>(a);
-                }
-            APF_CUDA(cudaGetLastError());
-        }
-
         // candidates of each row: incidences x local DOFs x restriction entries per term
         __global__ void gather_candidates(int n_rows, Term t0, Term t1, int n_terms, int per_incidence,
                                           int* __restrict__ cand)
@@ -1029,16 +1000,6 @@ namespace apf
                     cv[dst + k] = tv[src + k];
                 }
             }
-        }
-
-        void dispatch_gather(cudaStream_t s, GatherArgs& a, int cap)
-        {
-            if (cap <= 64) run_gather<64>(s, a, a.status);
-            else if (cap <= 256) run_gather<256>(s, a, a.status);
-            else if (cap <= 512) run_gather<512>(s, a, a.status);
-            else if (cap <= 2048) run_gather<2048>(s, a, a.status);
-            else if (cap <= 8192) run_gather<8192>(s, a, a.status);
-            else throw Error(APF_ERR_CAPACITY, "row candidate count exceeds 8192");
         }
 
         int check_status(DeviceBuffer<int>& st, cudaStream_t s)
@@ -1088,17 +1049,49 @@ namespace apf
         a.row_ptr = cand_ptr.get();
         a.col_out = tc.get();
         a.val_out = tv.get();
-        // rows by candidate count, each class with its own shared-memory capacity
+        // every row with room for 128 distinct columns (the candidates stream through), then
+        // the rows that had more with 1024, then 4096
         (void)cap;
-        static constexpr int kCaps[5] = {64, 256, 512, 2048, 8192};
-        RowBuckets rb;
-        bucket_rows(s, n_rows, cand.get(), kCaps, 5, rb);
-        for (int b = 0; b < 5; ++b)
+        a.kmax = kmax;
+        auto run = [&](auto tag) {
+            constexpr int UCAP = decltype(tag)::value;
+            const int warps = std::max(1, std::min(4, static_cast<int>((96 * 1024) / gather_u_warp_bytes<UCAP>())));
+            const size_t smem = warps * gather_u_warp_bytes<UCAP>();
+            const int blocks = grid_for(a.list ? a.nlist : n_rows, warps, 148 * 64);
+            APF_CUDA(cudaFuncSetAttribute(gather_rows_u<UCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            APF_KERNEL("gather_rows_fill", s);
+            gather_rows_u<UCAP><<<blocks, warps * 32, smem, s>>>(a);
+            APF_CUDA(cudaGetLastError());
+        };
+        a.list = nullptr;
+        a.nlist = n_rows;
+        if (n_rows > 0)
+            run(std::integral_constant<int, 128>{});
+        DeviceBuffer<int> oflag(static_cast<std::size_t>(n_rows) + 1, s), opos(static_cast<std::size_t>(n_rows) + 1, s),
+            olist(1, s);
+        for (int pass = 0; pass < 3 && n_rows > 0; ++pass)
         {
-            a.list = rb.list.get() + rb.offsets[b];
-            a.nlist = rb.offsets[b + 1] - rb.offsets[b];
-            if (a.nlist > 0)
-                dispatch_gather(s, a, kCaps[b]);
+            const int nin = a.list ? a.nlist : n_rows;
+            {
+                APF_KERNEL("gather_overflow_rows", s);
+                overflow_flags<<<grid_for(nin, 256), 256, 0, s>>>(nin, a.list, counts.get(), oflag.get());
+            }
+            const int nover = static_cast<int>(exclusive_scan(oflag.get(), opos.get(), nin, s));
+            if (nover == 0)
+                break;
+            require(pass < 2, APF_ERR_CAPACITY, "assembly: a row has more than 4096 distinct columns");
+            DeviceBuffer<int> next(static_cast<std::size_t>(nover), s);
+            {
+                APF_KERNEL("gather_overflow_rows", s);
+                overflow_compact<<<grid_for(nin, 256), 256, 0, s>>>(nin, a.list, oflag.get(), opos.get(), next.get());
+            }
+            olist = std::move(next);
+            a.list = olist.get();
+            a.nlist = nover;
+            if (pass == 0)
+                run(std::integral_constant<int, 1024>{});
+            else
+                run(std::integral_constant<int, 4096>{});
         }
         out.rows = n_rows;
         out.cols = n_cols;

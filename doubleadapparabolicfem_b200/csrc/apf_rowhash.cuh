@@ -46,6 +46,23 @@ namespace apf
         }
     }
 
+    // slot of col in the table, inserting it when absent (fresh = it was absent)
+    __device__ __forceinline__ int hash_slot_of(int* tkeys, int col, int hbits, bool& fresh)
+    {
+        const int H = 1 << hbits;
+        unsigned h = hash_slot(col, hbits);
+        while (true)
+        {
+            const int prev = atomicCAS(tkeys + h, -1, col);
+            if (prev == -1 || prev == col)
+            {
+                fresh = prev == -1;
+                return static_cast<int>(h);
+            }
+            h = (h + 1) & (H - 1);
+        }
+    }
+
     __device__ __forceinline__ int hash_rank(const int* tkeys, const int* tranks, int col, int hbits)
     {
         const int H = 1 << hbits;
