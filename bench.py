@@ -464,6 +464,34 @@ def run_ours(args, world, rank, local):
             "max_cell_flux_err_over_max_cell": float(np.abs(f32[0] - f64[0]).max() / scale),
             "max_cell_eta_err_over_max_cell": float(np.abs(f32[1] - f64[1]).max() / scale),
             "flux_total_rel_err": float(abs(f32[2] - f64[2]) / f64[2])}
+    # the direct-solver path's two-pass full saddle assembly on the same mesh (not part of
+    # the step): pattern + numeric pass, then the numeric pass alone on the cached pattern
+    two_pass = None
+    if args.p in (1, 2):
+        keep = _Keep()
+        desc = make_desc(dprob, 1e-15, -1.0, keep)
+        cache = C.c_void_p()
+        ctx.check(lib.apf_two_pass_cache_create(ctx.handle, C.byref(cache)))
+        times = []
+        for _ in range(3):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            h2 = C.c_void_p()
+            ctx.check(lib.apf_assemble_full_saddle_two_pass(ctx.handle, C.byref(desc), 1, cache, C.byref(h2)))
+            t1.record(stream)
+            torch.cuda.synchronize(dev)
+            times.append(t0.elapsed_time(t1))
+            r2, c2, n2 = C.c_int32(), C.c_int32(), C.c_int64()
+            ctx.check(lib.apf_system_block_info(h2, _lib.BLOCKS["K"], C.byref(r2), C.byref(c2), C.byref(n2)))
+            lib.apf_system_destroy(h2)
+        nb, nr, ne = C.c_int64(), C.c_int64(), C.c_int64()
+        ctx.check(lib.apf_two_pass_cache_stats(cache, C.byref(nb), C.byref(nr), C.byref(ne)))
+        lib.apf_two_pass_cache_destroy(cache)
+        two_pass = {"pattern_and_numeric_ms": round(times[0], 3),
+                    "numeric_on_cached_pattern_ms": round(min(times[1:]), 3),
+                    "pattern_entries": ne.value, "K_nnz_after_prune": n2.value,
+                    "pattern_builds": nb.value, "pattern_reuse_count": nr.value}
     m = MainSystemBlocks(ctx, h, host)
     nnz_k = m.block_info("K")[2]
     nnz_h = m.block_info("Hhat")[2]
@@ -517,6 +545,7 @@ def run_ours(args, world, rank, local):
                    "minres_solve_s_mean": sum(d["solve_seconds"] for d in timed_diags) / len(timed_diags),
                    "plain_preconditioner": plain,
                    "patch_precision_fp32_refined_vs_fp64": patch_precision,
+                   "two_pass_full_saddle_assembly": two_pass,
                    "patch_launch_autotune": json.loads(lib.apf_ctx_autotune_report(ctx.handle).decode() or "{}"),
                    "minres_iterations": [d["iterations"] for d in timed_diags],
                    "step_ms": step_ms,

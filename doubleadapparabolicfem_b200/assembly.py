@@ -220,3 +220,77 @@ def assemble_main_system_blocks(problem: SpaceTimeProblem, zero_tol: float = 1e-
     h = C.c_void_p()
     ctx.check(ctx.lib.apf_assemble_main_system(ctx.handle, C.byref(desc), 1 if inputs_on_device else 0, C.byref(h)))
     return MainSystemBlocks(ctx, h, problem)
+
+
+class TwoPassFullSaddleAssemblyCache:
+    """Pattern cache of the two-pass full saddle assembly
+    (TwoPassFullSaddleAssemblyCache2D, two_pass_full_saddle_2d.hpp:325-373): the pattern
+    is kept on the device while the mesh and its DOF maps are unchanged."""
+
+    def __init__(self, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.apf_two_pass_cache_create(self.ctx.handle, C.byref(h)))
+        self.handle = h
+
+    def stats(self) -> dict:
+        b, r, e = C.c_int64(), C.c_int64(), C.c_int64()
+        self.ctx.check(self.ctx.lib.apf_two_pass_cache_stats(self.handle, C.byref(b), C.byref(r), C.byref(e)))
+        return {"pattern_builds": b.value, "pattern_reuse_count": r.value, "pattern_entries": e.value}
+
+    @property
+    def pattern_reuse_count(self) -> int:
+        return self.stats()["pattern_reuse_count"]
+
+    def close(self):
+        if self.handle:
+            self.ctx.lib.apf_two_pass_cache_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        if sys.is_finalizing():
+            return
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LinearSystem:
+    """The direct-solver path's system (la::linear::LinearSystem,
+    src/linear_algebra/system/linear_system.hpp:6-14): the full saddle matrix and
+    rhs = [f; g], device-resident."""
+
+    def __init__(self, blocks: MainSystemBlocks):
+        self.blocks = blocks
+
+    @property
+    def matrix(self):
+        return self.blocks.block("K")
+
+    @property
+    def rhs(self) -> np.ndarray:
+        return np.concatenate([self.blocks.f(), self.blocks.g()])
+
+    def matrix_device_ptrs(self):
+        return self.blocks.block_device_ptrs("K")
+
+    def close(self):
+        self.blocks.close()
+
+
+def assemble_main_full_saddle_two_pass(problem: SpaceTimeProblem, zero_tol: float = 1e-15, g_scale: float = -1.0,
+                                       ctx: Context | None = None,
+                                       assembly_cache: TwoPassFullSaddleAssemblyCache | None = None,
+                                       inputs_on_device: bool = False) -> LinearSystem:
+    """GPU two-pass full saddle assembly (assemble_main_full_saddle_two_pass_2d,
+    two_pass_full_saddle_2d.hpp:468): structural pattern (kept in ``assembly_cache``
+    while the mesh is unchanged), numeric pass, prune of |value| <= zero_tol.  2+1D."""
+    ctx = ctx or (assembly_cache.ctx if assembly_cache is not None else default_context())
+    keep = _Keep()
+    desc = make_desc(problem, zero_tol, g_scale, keep)
+    h = C.c_void_p()
+    ctx.check(ctx.lib.apf_assemble_full_saddle_two_pass(ctx.handle, C.byref(desc), 1 if inputs_on_device else 0,
+                                                        assembly_cache.handle if assembly_cache is not None else None,
+                                                        C.byref(h)))
+    return LinearSystem(MainSystemBlocks(ctx, h, problem))

@@ -270,6 +270,188 @@ namespace apf
             return ((sizeof(int) * (2 * kGatherIncCap + 2) + 32 * UCAP + 32 * 8) + 15) / 16 * 16;
         }
 
+        // Every candidate (ok, column, value) of one row in generation order: per term, the
+        // row's incidences staged in incs and ordered by (cell * ndof + i); then every
+        // (incidence, local column j, restriction entry q) item, 32 at a time (within a
+        // batch: by restriction entry, then lane), ok = |local| > zero_tol.  All lanes of
+        // the warp call f with the same sequence.  A row with more than kGatherIncCap
+        // incidences in a term sets too_many_inc and stops.
+        template<class F>
+        __device__ __forceinline__ void row_candidates(const GatherArgs& A, int row, int lane, int* incs,
+                                                       bool& too_many_inc, F&& f)
+        {
+            const int ndof = A.ndof;
+            for (int tt = 0; tt < A.n_terms; ++tt)
+            {
+                const Term T = A.term[tt];
+                const int ib = T.inc_ptr[row], ie = T.inc_ptr[row + 1];
+                const int n_inc = ie - ib;
+                if (n_inc > kGatherIncCap)
+                {
+                    too_many_inc = true;
+                    return;
+                }
+                for (int k = lane; k < n_inc; k += 32)
+                {
+                    const int2 v = T.inc[ib + k];
+                    incs[k] = v.x;
+                    incs[kGatherIncCap + k] = v.y;
+                }
+                __syncwarp();
+                int my_ci[8], my_e[8], my_rank[8];
+                int nm = 0;
+                for (int k = lane; k < n_inc; k += 32, ++nm)
+                {
+                    const int ci = incs[k];
+                    int rank = 0;
+                    for (int q = 0; q < n_inc; ++q)
+                        rank += incs[q] < ci;
+                    my_ci[nm] = ci;
+                    my_e[nm] = incs[kGatherIncCap + k];
+                    my_rank[nm] = rank;
+                }
+                __syncwarp();
+                for (int q = 0; q < nm; ++q)
+                {
+                    incs[my_rank[q]] = my_ci[q];
+                    incs[kGatherIncCap + my_rank[q]] = my_e[q];
+                }
+                __syncwarp();
+                const double* rw = row_weights(A.d, T.kind);
+                const int items = n_inc * ndof;
+                for (int it0 = 0; it0 < items; it0 += 32)
+                {
+                    const int it = it0 + lane;
+                    bool ok = false;
+                    double v = 0.0, wi = 0.0;
+                    const int* cd = nullptr;
+                    const double* cw = nullptr;
+                    int b = 0, e = 0;
+                    if (it < items)
+                    {
+                        const int t_idx = it / ndof, j = it % ndof;
+                        const int ci = incs[t_idx];
+                        const int c = ci / ndof, i = ci % ndof;
+                        wi = rw[incs[kGatherIncCap + t_idx]];
+                        v = local_entry(A.d, T.kind, c, i, j);
+                        ok = fabs(v) > A.d.zero_tol;
+                        if (ok)
+                            col_restriction(A.d, T.kind, c, j, ndof, cd, cw, b, e);
+                    }
+                    for (int q = 0; q < A.kmax; ++q)
+                    {
+                        const bool has = ok && b + q < e;
+                        f(has, has ? cd[b + q] + T.col_offset : 0, has ? wi * cw[b + q] * v : 0.0);
+                    }
+                }
+                __syncwarp();
+            }
+        }
+
+        // Numeric pass on a kept pattern (the two-pass full saddle assembly): one warp per
+        // row; the row's candidates, in row_candidates' order and with its zero_tol filter,
+        // are added into the pattern's slots (the column's position among the row's sorted
+        // columns) with ordered_add, so each slot receives exactly the sum the gather forms
+        // for that column.  Slots that no candidate reaches stay 0.  A candidate whose column
+        // is missing from the pattern sets status APF_ERR_INVALID.
+        constexpr int kFillWarps = 4;
+        constexpr int kFillWarpBytes = sizeof(int) * (2 * kGatherIncCap + 2) + 32 * sizeof(double);
+
+        __global__ void __launch_bounds__(kFillWarps * 32) fill_rows_on_pattern(GatherArgs A, int row_base,
+                                                                                const int* __restrict__ prow,
+                                                                                const int* __restrict__ pcol,
+                                                                                double* __restrict__ pval)
+        {
+            __shared__ __align__(16) unsigned char smem[kFillWarps * kFillWarpBytes];
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            int* incs = reinterpret_cast<int*>(smem + w * kFillWarpBytes);
+            double* stage = reinterpret_cast<double*>(incs + 2 * kGatherIncCap + 2);
+            for (int row = blockIdx.x * kFillWarps + w; row < A.n_rows; row += gridDim.x * kFillWarps)
+            {
+                const int b = prow[row_base + row], e = prow[row_base + row + 1];
+                for (int k = b + lane; k < e; k += 32)
+                    pval[k] = 0.0;
+                __syncwarp();
+                bool too_many_inc = false;
+                row_candidates(A, row, lane, incs, too_many_inc, [&](bool ok, int col, double v) {
+                    int slot = 0;
+                    bool live = ok;
+                    if (ok)
+                    {
+                        int lo = b, hi = e;
+                        while (lo < hi)
+                        {
+                            const int mid = (lo + hi) >> 1;
+                            if (pcol[mid] < col)
+                                lo = mid + 1;
+                            else
+                                hi = mid;
+                        }
+                        if (lo < e && pcol[lo] == col)
+                            slot = lo - b;
+                        else
+                        {
+                            live = false;
+                            atomicExch(A.status, APF_ERR_INVALID);
+                        }
+                    }
+                    ordered_add(pval + b, stage, live, slot, v, lane);
+                });
+                if (too_many_inc && lane == 0)
+                    atomicExch(A.status, APF_ERR_CAPACITY);
+                __syncwarp();
+            }
+        }
+
+        // entries with |value| > tol per row (prune(1.0, tol) keeps exactly those)
+        __global__ void prune_count(int rows, const int* __restrict__ rp, const double* __restrict__ val, double tol,
+                                    int* __restrict__ cnt)
+        {
+            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+            {
+                int c = 0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k)
+                    c += fabs(val[k]) > tol;
+                cnt[r] = c;
+            }
+        }
+
+        // one warp per row: the kept entries in order (ballot compaction)
+        __global__ void prune_fill(int rows, const int* __restrict__ rp, const int* __restrict__ ci,
+                                   const double* __restrict__ val, double tol, const int* __restrict__ out_rp,
+                                   int* __restrict__ out_ci, double* __restrict__ out_val)
+        {
+            const int lane = threadIdx.x & 31;
+            const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            const int nwarps = (gridDim.x * blockDim.x) >> 5;
+            for (int r = warp; r < rows; r += nwarps)
+            {
+                int o = out_rp[r];
+                for (int k0 = rp[r]; k0 < rp[r + 1]; k0 += 32)
+                {
+                    const int k = k0 + lane;
+                    const bool keep = k < rp[r + 1] && fabs(val[k]) > tol;
+                    const unsigned m = __ballot_sync(0xffffffffu, keep);
+                    if (keep)
+                    {
+                        const int at = o + __popc(m & ((1u << lane) - 1));
+                        out_ci[at] = ci[k];
+                        out_val[at] = val[k];
+                    }
+                    o += __popc(m);
+                }
+            }
+        }
+
+        // row pointers of two CSR row blocks stacked (the second block's shifted by the
+        // first's nonzeros)
+        __global__ void stack_row_ptr(int n_top, const int* __restrict__ top, int n_bottom,
+                                      const int* __restrict__ bottom, int* __restrict__ out)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n_top + n_bottom; i += gridDim.x * blockDim.x)
+                out[i] = i <= n_top ? top[i] : top[n_top] + bottom[i - n_top];
+        }
+
         template<int UCAP>
         __global__ void __launch_bounds__(128) gather_rows_u(GatherArgs A)
         {
@@ -288,74 +470,7 @@ namespace apf
             {
                 const int row = A.list ? A.list[idx] : idx;
                 bool too_many_inc = false;
-                // every candidate (ok, column, value) in generation order; all lanes call f
-                auto for_each = [&](auto&& f) {
-                    for (int tt = 0; tt < A.n_terms; ++tt)
-                    {
-                        const Term T = A.term[tt];
-                        const int ib = T.inc_ptr[row], ie = T.inc_ptr[row + 1];
-                        const int n_inc = ie - ib;
-                        if (n_inc > kGatherIncCap)
-                        {
-                            too_many_inc = true;
-                            return;
-                        }
-                        for (int k = lane; k < n_inc; k += 32)
-                        {
-                            const int2 v = T.inc[ib + k];
-                            incs[k] = v.x;
-                            incs[kGatherIncCap + k] = v.y;
-                        }
-                        __syncwarp();
-                        int my_ci[8], my_e[8], my_rank[8];
-                        int nm = 0;
-                        for (int k = lane; k < n_inc; k += 32, ++nm)
-                        {
-                            const int ci = incs[k];
-                            int rank = 0;
-                            for (int q = 0; q < n_inc; ++q)
-                                rank += incs[q] < ci;
-                            my_ci[nm] = ci;
-                            my_e[nm] = incs[kGatherIncCap + k];
-                            my_rank[nm] = rank;
-                        }
-                        __syncwarp();
-                        for (int q = 0; q < nm; ++q)
-                        {
-                            incs[my_rank[q]] = my_ci[q];
-                            incs[kGatherIncCap + my_rank[q]] = my_e[q];
-                        }
-                        __syncwarp();
-                        const double* rw = row_weights(A.d, T.kind);
-                        const int items = n_inc * ndof;
-                        for (int it0 = 0; it0 < items; it0 += 32)
-                        {
-                            const int it = it0 + lane;
-                            bool ok = false;
-                            double v = 0.0, wi = 0.0;
-                            const int* cd = nullptr;
-                            const double* cw = nullptr;
-                            int b = 0, e = 0;
-                            if (it < items)
-                            {
-                                const int t_idx = it / ndof, j = it % ndof;
-                                const int ci = incs[t_idx];
-                                const int c = ci / ndof, i = ci % ndof;
-                                wi = rw[incs[kGatherIncCap + t_idx]];
-                                v = local_entry(A.d, T.kind, c, i, j);
-                                ok = fabs(v) > A.d.zero_tol;
-                                if (ok)
-                                    col_restriction(A.d, T.kind, c, j, ndof, cd, cw, b, e);
-                            }
-                            for (int q = 0; q < A.kmax; ++q)
-                            {
-                                const bool has = ok && b + q < e;
-                                f(has, has ? cd[b + q] + T.col_offset : 0, has ? wi * cw[b + q] * v : 0.0);
-                            }
-                        }
-                        __syncwarp();
-                    }
-                };
+                auto for_each = [&](auto&& f) { row_candidates(A, row, lane, incs, too_many_inc, f); };
                 int n = 0;
                 for (int tt = 0; tt < A.n_terms; ++tt)
                     n += (A.term[tt].inc_ptr[row + 1] - A.term[tt].inc_ptr[row]) * ndof * A.kmax;
@@ -1164,6 +1279,99 @@ namespace apf
                 c.col_idx.get(), c.values.get(), k.col_idx.get(), k.values.get());
         }
         APF_CUDA(cudaGetLastError());
+    }
+
+    void full_saddle_pattern(cudaStream_t s, const SystemInputs& in, const Incidence& inc_y, const Incidence& inc_xy,
+                             const Incidence& inc_xb, DeviceBuffer<int>& row_ptr, DeviceBuffer<int>& col_idx)
+    {
+        const int n_lambda = in.n_lambda, n_u = in.n_u, n = n_lambda + n_u;
+        // a negative filter keeps every candidate: the structural union of the restricted
+        // couplings (the values of this pass are not used)
+        DeviceCsr top, bottom;
+        {
+            const int kinds[2] = {K_AY, K_BT};
+            const Incidence* incs[2] = {&inc_y, &inc_y};
+            const int offs[2] = {0, n_lambda};
+            gather_csr(s, in, -1.0, n_lambda, n, 2, kinds, incs, offs, in.kmax, top);
+        }
+        {
+            const int kinds[2] = {K_B, K_C};
+            const Incidence* incs[2] = {&inc_xy, &inc_xb};
+            const int offs[2] = {0, n_lambda};
+            gather_csr(s, in, -1.0, n_u, n, 2, kinds, incs, offs, in.kmax, bottom);
+        }
+        row_ptr.allocate(static_cast<std::size_t>(n) + 1, s);
+        {
+            APF_KERNEL("stack_row_ptr", s);
+            stack_row_ptr<<<grid_for(n + 1, 256), 256, 0, s>>>(n_lambda, top.row_ptr.get(), n_u, bottom.row_ptr.get(),
+                                                               row_ptr.get());
+        }
+        APF_CUDA(cudaGetLastError());
+        const std::size_t nt = top.col_idx.size(), nb = bottom.col_idx.size();
+        col_idx.allocate(nt + nb, s);
+        if (nt)
+            APF_CUDA(cudaMemcpyAsync(col_idx.get(), top.col_idx.get(), nt * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        if (nb)
+            APF_CUDA(cudaMemcpyAsync(col_idx.get() + nt, bottom.col_idx.get(), nb * sizeof(int),
+                                     cudaMemcpyDeviceToDevice, s));
+    }
+
+    void full_saddle_numeric(cudaStream_t s, const SystemInputs& in, const Incidence& inc_y, const Incidence& inc_xy,
+                             const Incidence& inc_xb, const int* row_ptr, const int* col_idx, long long nnz_pattern,
+                             DeviceCsr& K)
+    {
+        const int n_lambda = in.n_lambda, n_u = in.n_u, n = n_lambda + n_u;
+        require(in.kmax <= 4, APF_ERR_CAPACITY, "restriction rows with more than 4 entries are not supported");
+        DeviceBuffer<double> vals(static_cast<std::size_t>(std::max(nnz_pattern, 1ll)), s);
+        DeviceBuffer<int> status(1, s);
+        status.zero();
+        auto fill = [&](int n_rows, int row_base, int k0, const Incidence& i0, int k1, const Incidence& i1) {
+            if (n_rows == 0)
+                return;
+            require(i0.max_len <= kGatherIncCap && i1.max_len <= kGatherIncCap, APF_ERR_CAPACITY,
+                    "a DOF has more than 256 cell incidences");
+            GatherArgs a{};
+            a.d = make_asm_data(in, in.zero_tol);
+            a.n_rows = n_rows;
+            a.ndof = in.ndof;
+            a.n_terms = 2;
+            a.term[0] = Term{k0, i0.ptr.get(), i0.entries.get(), 0};
+            a.term[1] = Term{k1, i1.ptr.get(), i1.entries.get(), n_lambda};
+            a.status = status.get();
+            a.kmax = in.kmax;
+            APF_KERNEL("fill_rows_on_pattern", s);
+            fill_rows_on_pattern<<<grid_for(n_rows, kFillWarps, 148 * 64), kFillWarps * 32, 0, s>>>(
+                a, row_base, row_ptr, col_idx, vals.get());
+            APF_CUDA(cudaGetLastError());
+        };
+        fill(n_lambda, 0, K_AY, inc_y, K_BT, inc_y);
+        fill(n_u, n_lambda, K_B, inc_xy, K_C, inc_xb);
+        const int st = check_status(status, s);
+        if (st == APF_ERR_INVALID)
+            throw Error(APF_ERR_INVALID, "two-pass assembly: a coupling lies outside the cached pattern "
+                                         "(the pattern belongs to another mesh)");
+        if (st != 0)
+            throw Error(APF_ERR_CAPACITY, "two-pass assembly: more than 256 cell incidences for a DOF");
+        // prune(1.0, zero_tol): keep |value| > zero_tol
+        DeviceBuffer<int> cnt(static_cast<std::size_t>(n) + 1, s);
+        if (n > 0)
+        {
+            APF_KERNEL("prune_count", s);
+            prune_count<<<grid_for(n, 256), 256, 0, s>>>(n, row_ptr, vals.get(), in.zero_tol, cnt.get());
+            APF_CUDA(cudaGetLastError());
+        }
+        K.rows = K.cols = n;
+        K.row_ptr.allocate(static_cast<std::size_t>(n) + 1, s);
+        const long long nnz = exclusive_scan(cnt.get(), K.row_ptr.get(), n, s);
+        K.col_idx.allocate(static_cast<std::size_t>(nnz), s);
+        K.values.allocate(static_cast<std::size_t>(nnz), s);
+        if (n > 0)
+        {
+            APF_KERNEL("prune_fill", s);
+            prune_fill<<<grid_for((long long)n * 32, 256, 148 * 16), 256, 0, s>>>(
+                n, row_ptr, col_idx, vals.get(), in.zero_tol, K.row_ptr.get(), K.col_idx.get(), K.values.get());
+            APF_CUDA(cudaGetLastError());
+        }
     }
 
     void build_hhat(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& C, const DeviceCsr& A_x, const DeviceCsr& B_dt,

@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <array>
 #include <memory>
 #include <new>
 #include <string>
@@ -116,6 +117,108 @@ namespace
         apf::require(src != nullptr, APF_ERR_INVALID, "null input array");
         APF_CUDA(cudaMemcpyAsync(dst.get(), src, n * sizeof(T),
                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    }
+}
+
+struct apf_two_pass_cache
+{
+    apf_ctx* ctx = nullptr;
+    bool valid = false;
+    std::array<long long, 12> key{};
+    apf::DeviceBuffer<int> row_ptr, col_idx;
+    long long pattern_builds = 0, pattern_reuses = 0;
+};
+
+namespace
+{
+    using TwoPassKey = std::array<long long, 12>;
+
+    __device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+    {
+        // splitmix64 finaliser
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        return z ^ (z >> 31);
+    }
+
+    // order-independent fingerprint of an int array: sum over i of mix(tag, i, a[i])
+    __global__ void fingerprint_add(const int* __restrict__ a, long long n, unsigned tag,
+                                    unsigned long long* __restrict__ acc)
+    {
+        unsigned long long h = 0;
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+            h += mix64((static_cast<unsigned long long>(tag) << 56) ^ (static_cast<unsigned long long>(i) << 24) ^
+                       static_cast<unsigned long long>(static_cast<unsigned>(a[i])) * 0x9e3779b97f4a7c15ull);
+        for (int o = 16; o > 0; o >>= 1)
+            h += __shfl_xor_sync(0xffffffffu, h, o);
+        if ((threadIdx.x & 31) == 0)
+            atomicAdd(acc, h);
+    }
+
+    TwoPassKey two_pass_key(cudaStream_t s, const apf::SystemInputs& in)
+    {
+        apf::DeviceBuffer<unsigned long long> acc(1, s);
+        APF_CUDA(cudaMemsetAsync(acc.get(), 0, sizeof(unsigned long long), s));
+        const apf::DeviceBuffer<int>* arrays[6] = {&in.y_off, &in.y_dofs, &in.x_off, &in.x_dofs, &in.y_to_x,
+                                                   &in.bottom_list};
+        for (unsigned t = 0; t < 6; ++t)
+        {
+            const long long n = static_cast<long long>(arrays[t]->size());
+            if (n == 0)
+                continue;
+            APF_KERNEL("pattern_fingerprint", s);
+            fingerprint_add<<<static_cast<int>(std::min<long long>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(
+                arrays[t]->get(), n, t + 1, acc.get());
+            APF_CUDA(cudaGetLastError());
+        }
+        unsigned long long h = 0;
+        APF_CUDA(cudaMemcpyAsync(&h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+        apf::sync(s);
+        return TwoPassKey{in.p, in.dim, in.ndof, in.n_y_cells, in.n_x_cells, in.n_lambda, in.n_u,
+                          static_cast<long long>(in.y_dofs.size()), static_cast<long long>(in.x_dofs.size()),
+                          in.n_bottom, static_cast<long long>(h >> 1), static_cast<long long>(h & 1)};
+    }
+
+    // problem descriptor -> device inputs of a system (validation as the reference's
+    // assembly preconditions)
+    void stage_problem(apf_ctx* ctx, const apf_problem_desc* d, int inputs_on_device, apf::System& S)
+    {
+        const int dim = d->dim_space == 0 ? 2 : d->dim_space;
+        apf::require(dim == 1 || dim == 2, APF_ERR_INVALID, "dim_space must be 1 or 2");
+        apf::require(d->p == 1 || (d->p == 2 && dim == 2), APF_ERR_INVALID,
+                     "p must be 1 or 2 (2+1D) or 1 (1+1D)");
+        apf::require(d->n_y_cells >= 0 && d->n_x_cells >= 0 && d->n_lambda >= 0 && d->n_u >= 0, APF_ERR_INVALID,
+                     "negative sizes");
+        apf::require(d->u0_kind >= 0 && d->u0_kind <= 2, APF_ERR_INVALID, "unknown u0_kind");
+        S.stream = ctx->stream;
+        auto& in = S.in;
+        in.p = d->p;
+        in.dim = dim;
+        in.ndof = dim == 1 ? (d->p + 1) * (d->p + 1) : (d->p + 1) * (d->p + 2) / 2 * (d->p + 1);
+        in.n_y_cells = d->n_y_cells;
+        in.n_x_cells = d->n_x_cells;
+        in.n_lambda = d->n_lambda;
+        in.n_u = d->n_u;
+        in.u0_kind = d->u0_kind;
+        in.zero_tol = d->zero_tol;
+        in.g_scale = d->g_scale;
+        const bool dev = inputs_on_device != 0;
+        cudaStream_t s = ctx->stream;
+        const std::size_t ny = static_cast<std::size_t>(d->n_y_cells), nx = static_cast<std::size_t>(d->n_x_cells);
+        const std::size_t gw = dim == 1 ? 4 : 8, mw = dim == 1 ? 1 : 3;
+        stage(in.y_geo, d->y_geometry, ny * gw, dev, s);
+        stage(in.x_geo, d->x_geometry, nx * gw, dev, s);
+        stage(in.y_to_x, d->y_to_x, ny, dev, s);
+        stage(in.y_off, d->y_restr_offsets, ny * in.ndof + 1, dev, s);
+        stage(in.y_dofs, d->y_restr_dofs, static_cast<std::size_t>(d->y_restr_nnz), dev, s);
+        stage(in.y_w, d->y_restr_weights, static_cast<std::size_t>(d->y_restr_nnz), dev, s);
+        stage(in.x_off, d->x_restr_offsets, nx * in.ndof + 1, dev, s);
+        stage(in.x_dofs, d->x_restr_dofs, static_cast<std::size_t>(d->x_restr_nnz), dev, s);
+        stage(in.x_w, d->x_restr_weights, static_cast<std::size_t>(d->x_restr_nnz), dev, s);
+        if (d->m_cells)
+            stage(in.m_y, d->m_cells, ny * mw, dev, s);
+        if (d->ell_cells)
+            stage(in.ell, d->ell_cells, ny, dev, s);
     }
 }
 
@@ -344,44 +447,108 @@ int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* d, int inputs
     const int rc = guarded(ctx, [&] {
         APF_HOST_RANGE("call_assemble_main_system");
         ensure_pool(ctx);
-        const int dim = d->dim_space == 0 ? 2 : d->dim_space;
-        apf::require(dim == 1 || dim == 2, APF_ERR_INVALID, "dim_space must be 1 or 2");
-        apf::require(d->p == 1 || (d->p == 2 && dim == 2), APF_ERR_INVALID,
-                     "p must be 1 or 2 (2+1D) or 1 (1+1D)");
-        apf::require(d->n_y_cells >= 0 && d->n_x_cells >= 0 && d->n_lambda >= 0 && d->n_u >= 0, APF_ERR_INVALID,
-                     "negative sizes");
-        apf::require(d->u0_kind >= 0 && d->u0_kind <= 2, APF_ERR_INVALID, "unknown u0_kind");
+        stage_problem(ctx, d, inputs_on_device, h->sys);
+        apf::assemble_main(h->sys);
+    });
+    if (rc != APF_OK)
+        return rc;
+    *out = h.release();
+    return APF_OK;
+}
+
+int apf_two_pass_cache_create(apf_ctx* ctx, apf_two_pass_cache** out)
+{
+    if (!ctx || !out)
+        return APF_ERR_INVALID;
+    *out = new apf_two_pass_cache;
+    (*out)->ctx = ctx;
+    return APF_OK;
+}
+
+void apf_two_pass_cache_destroy(apf_two_pass_cache* cache)
+{
+    if (!cache)
+        return;
+    cudaSetDevice(cache->ctx->device);
+    cudaStreamSynchronize(cache->ctx->stream);
+    delete cache;
+}
+
+int apf_two_pass_cache_stats(const apf_two_pass_cache* cache, int64_t* pattern_builds, int64_t* pattern_reuses,
+                             int64_t* pattern_entries)
+{
+    if (!cache)
+        return APF_ERR_INVALID;
+    if (pattern_builds)
+        *pattern_builds = cache->pattern_builds;
+    if (pattern_reuses)
+        *pattern_reuses = cache->pattern_reuses;
+    if (pattern_entries)
+        *pattern_entries = cache->valid ? static_cast<int64_t>(cache->col_idx.size()) : 0;
+    return APF_OK;
+}
+
+int apf_assemble_full_saddle_two_pass(apf_ctx* ctx, const apf_problem_desc* d, int inputs_on_device,
+                                      apf_two_pass_cache* cache, apf_system** out)
+{
+    if (!ctx || !d || !out || (cache && cache->ctx != ctx))
+        return APF_ERR_INVALID;
+    *out = nullptr;
+    auto h = std::make_unique<apf_system>();
+    h->ctx = ctx;
+    const int rc = guarded(ctx, [&] {
+        APF_HOST_RANGE("call_assemble_full_saddle_two_pass");
+        ensure_pool(ctx);
         auto& S = h->sys;
-        S.stream = ctx->stream;
+        apf::require(d->dim_space == 0 || d->dim_space == 2, APF_ERR_INVALID,
+                     "the two-pass full saddle assembly is for 2+1D problems");
+        stage_problem(ctx, d, inputs_on_device, S);
+        cudaStream_t s = S.stream;
         auto& in = S.in;
-        in.p = d->p;
-        in.dim = dim;
-        in.ndof = dim == 1 ? (d->p + 1) * (d->p + 1) : (d->p + 1) * (d->p + 2) / 2 * (d->p + 1);
-        in.n_y_cells = d->n_y_cells;
-        in.n_x_cells = d->n_x_cells;
-        in.n_lambda = d->n_lambda;
-        in.n_u = d->n_u;
-        in.u0_kind = d->u0_kind;
-        in.zero_tol = d->zero_tol;
-        in.g_scale = d->g_scale;
-        const bool dev = inputs_on_device != 0;
-        cudaStream_t s = ctx->stream;
-        const std::size_t ny = static_cast<std::size_t>(d->n_y_cells), nx = static_cast<std::size_t>(d->n_x_cells);
-        const std::size_t gw = dim == 1 ? 4 : 8, mw = dim == 1 ? 1 : 3;
-        stage(in.y_geo, d->y_geometry, ny * gw, dev, s);
-        stage(in.x_geo, d->x_geometry, nx * gw, dev, s);
-        stage(in.y_to_x, d->y_to_x, ny, dev, s);
-        stage(in.y_off, d->y_restr_offsets, ny * in.ndof + 1, dev, s);
-        stage(in.y_dofs, d->y_restr_dofs, static_cast<std::size_t>(d->y_restr_nnz), dev, s);
-        stage(in.y_w, d->y_restr_weights, static_cast<std::size_t>(d->y_restr_nnz), dev, s);
-        stage(in.x_off, d->x_restr_offsets, nx * in.ndof + 1, dev, s);
-        stage(in.x_dofs, d->x_restr_dofs, static_cast<std::size_t>(d->x_restr_nnz), dev, s);
-        stage(in.x_w, d->x_restr_weights, static_cast<std::size_t>(d->x_restr_nnz), dev, s);
-        if (d->m_cells)
-            stage(in.m_y, d->m_cells, ny * mw, dev, s);
-        if (d->ell_cells)
-            stage(in.ell, d->ell_cells, ny, dev, s);
-        apf::assemble_main(S);
+        apf::prepare_inputs(s, in);
+        const int nd = in.ndof;
+        S.inc_y = apf::build_incidence(s, in.n_lambda, in.n_y_cells, nullptr, nullptr, in.y_off.get(), in.y_dofs.get(), nd);
+        S.inc_xy = apf::build_incidence(s, in.n_u, in.n_y_cells, nullptr, in.y_to_x.get(), in.x_off.get(),
+                                        in.x_dofs.get(), nd);
+        S.inc_xb = apf::build_incidence(s, in.n_u, in.n_bottom, in.bottom_list.get(), nullptr, in.x_off.get(),
+                                        in.x_dofs.get(), nd);
+        apf::DeviceBuffer<int> own_rp, own_ci;
+        const int* rp = nullptr;
+        const int* ci = nullptr;
+        long long nnz_pattern = 0;
+        // the pattern is kept while the mesh and its DOF maps are unchanged: sizes plus a
+        // fingerprint of the restriction rows, the Y -> X map and the bottom-cell list
+        // (the reference keys its cache on the spaces' version counters)
+        TwoPassKey key{};
+        if (cache)
+            key = two_pass_key(s, in);
+        if (cache && cache->valid && cache->key == key)
+        {
+            ++cache->pattern_reuses;
+        }
+        else
+        {
+            if (cache)
+                cache->valid = false; // a pass that throws leaves no stale pattern behind
+            apf::DeviceBuffer<int>& prp = cache ? cache->row_ptr : own_rp;
+            apf::DeviceBuffer<int>& pci = cache ? cache->col_idx : own_ci;
+            apf::full_saddle_pattern(s, in, S.inc_y, S.inc_xy, S.inc_xb, prp, pci);
+            if (cache)
+            {
+                cache->key = key;
+                cache->valid = true;
+                ++cache->pattern_builds;
+            }
+        }
+        rp = cache ? cache->row_ptr.get() : own_rp.get();
+        ci = cache ? cache->col_idx.get() : own_ci.get();
+        nnz_pattern = static_cast<long long>(cache ? cache->col_idx.size() : own_ci.size());
+        apf::full_saddle_numeric(s, in, S.inc_y, S.inc_xy, S.inc_xb, rp, ci, nnz_pattern, S.blocks[APF_BLOCK_K]);
+        S.have[APF_BLOCK_K] = true;
+        apf::gather_vector_host(s, in, in.zero_tol, 0, S.inc_y, in.n_lambda, in.ell.size() ? in.ell.get() : nullptr,
+                                in.u0_kind, in.g_scale, S.f);
+        apf::gather_vector_host(s, in, in.zero_tol, 1, S.inc_xb, in.n_u, nullptr, in.u0_kind, in.g_scale, S.g);
+        apf::sync(s);
     });
     if (rc != APF_OK)
         return rc;

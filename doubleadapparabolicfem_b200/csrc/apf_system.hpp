@@ -88,6 +88,14 @@ namespace apf
                             int n_rows, const double* ell, int u0_kind, double g_scale, DeviceBuffer<double>& out);
     void build_k(cudaStream_t s, int n_lambda, int n_u, const DeviceCsr& a, const DeviceCsr& bt, const DeviceCsr& b,
                  const DeviceCsr& c, DeviceCsr& k);
+    // Two-pass full saddle assembly (the direct-solver path's K = [A_y B^T; B C_signed]):
+    // the structural pattern (union of the restricted couplings, no value filter), then
+    // the numeric pass into that pattern and the prune of |value| <= zero_tol
+    void full_saddle_pattern(cudaStream_t s, const SystemInputs& in, const Incidence& inc_y, const Incidence& inc_xy,
+                             const Incidence& inc_xb, DeviceBuffer<int>& row_ptr, DeviceBuffer<int>& col_idx);
+    void full_saddle_numeric(cudaStream_t s, const SystemInputs& in, const Incidence& inc_y, const Incidence& inc_xy,
+                             const Incidence& inc_xb, const int* row_ptr, const int* col_idx, long long nnz_pattern,
+                             DeviceCsr& K);
     void build_hhat(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& C, const DeviceCsr& A_x, const DeviceCsr& B_dt,
                     const DeviceCsr& B_dtT, double diag_tol, DeviceCsr& H, DeviceBuffer<double>& inv_diag);
 

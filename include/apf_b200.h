@@ -143,6 +143,32 @@ int apf_assemble_main_system(apf_ctx* ctx, const apf_problem_desc* desc, int inp
  * Hhat = -C_signed + B_dt diag(A_y)^-1 B_dt^T + A_x.  Also keeps B_dt and A_x. */
 int apf_assemble_graph_norm(apf_ctx* ctx, apf_system* sys, double diagonal_tolerance);
 
+/* Two-pass full saddle assembly of the direct-solver path.  Replaces
+ * finite_element::assembly::assemble_main_full_saddle_two_pass_2d
+ * (src/finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp:468), called from
+ * solve_main_system.hpp:1855-1942, with its pattern cache TwoPassFullSaddleAssemblyCache2D
+ * (same file :325-373).  2+1D only, as the reference (static_assert at :520).
+ * Pattern pass (:740-790): the structural union over Y cells of the restricted (Y x Y),
+ * (X ancestor x Y) and transposed couplings and over bottom X cells of (X x X).  Numeric
+ * pass (scatter_matrix_by_slots, :431-459): the local entries with |a_ij| > zero_tol added
+ * into that pattern in cell order.  Then prune(1.0, zero_tol) (:1720): every entry with
+ * |value| <= zero_tol is dropped.  The result is block APF_BLOCK_K of *out (the only block
+ * it holds) and the right-hand side [f; g] (APF_VEC_F, APF_VEC_G).
+ * cache (NULL = none): the pattern of the last call is reused while the mesh and its DOF
+ * maps are unchanged (sizes and a fingerprint of the restriction rows, the Y -> X map and
+ * the bottom cells; the reference keys on the spaces' version counters), so a later call
+ * with new coefficients (m_cells, ell_cells, u0_kind, geometry of the same topology) runs
+ * the numeric pass only.  A cache belongs to one context and is destroyed before it. */
+typedef struct apf_two_pass_cache apf_two_pass_cache;
+int apf_two_pass_cache_create(apf_ctx* ctx, apf_two_pass_cache** out);
+void apf_two_pass_cache_destroy(apf_two_pass_cache* cache);
+/* pattern passes run, pattern reuses (the reference's pattern_reuse_count), entries of the
+ * kept pattern (any pointer may be NULL) */
+int apf_two_pass_cache_stats(const apf_two_pass_cache* cache, int64_t* pattern_builds, int64_t* pattern_reuses,
+                             int64_t* pattern_entries);
+int apf_assemble_full_saddle_two_pass(apf_ctx* ctx, const apf_problem_desc* desc, int inputs_on_device,
+                                      apf_two_pass_cache* cache, apf_system** out);
+
 /* Block sizes; nnz counts stored entries (explicit zeros included). */
 int apf_system_block_info(const apf_system* sys, int block, int32_t* rows, int32_t* cols, int64_t* nnz);
 /* Copy a block in CSR form.  to_device: 1 = destination pointers are device memory. */

@@ -25,7 +25,9 @@ Restated reference code (paths relative to the reference project root):
   scatter with the per-local-entry ``zero_tol`` filter
   ``src/finite_element/assembly/scatter.hpp:66-115,227-254``;
 * graph-norm preconditioner block — ``src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:22-65``
-  and ``src/linear_algebra/preconditioners/schur_approximations.hpp:79-287``.
+  and ``src/linear_algebra/preconditioners/schur_approximations.hpp:79-287``;
+* full saddle matrix of the direct-solver path — ``src/finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp:468``
+  (structural pattern, numeric fill, ``prune(1.0, zero_tol)``).
 """
 from __future__ import annotations
 
@@ -304,6 +306,27 @@ def assemble_main_blocks(prob: MainProblem, u0=sin_initial, ell=None, zero_tol=1
     f = scatter_vector(f_loc, prob.y_restr, prob.n_lambda, zero_tol)
     C, g = assemble_trace_blocks(prob, u0, zero_tol, g_scale)
     return dict(A_y=A_y, B=Bm, C_signed=C, f=f, g=g)
+
+
+def assemble_main_full_saddle_two_pass(prob: MainProblem, u0=sin_initial, ell=None, zero_tol=1e-15, g_scale=-1.0):
+    """Restatement of assemble_main_full_saddle_two_pass_2d
+    (src/finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp:468): the full
+    saddle matrix K = [A_y B^T; B C_signed] of the direct-solver path and rhs = [f; g].
+
+    Pattern pass (:740-790): the union over Y cells of the restricted (Y x Y), (X ancestor
+    x Y) and transposed couplings and over bottom X cells of (X x X), with no value filter.
+    Numeric pass (scatter_matrix_by_slots, :431-459): the local entries with |a_ij| >
+    zero_tol added into those slots in cell order, so every slot holds the block path's
+    sum.  Then ``prune(1.0, zero_tol)`` (:1720) drops every entry with |value| <= zero_tol,
+    structural slots no entry reached included.  The local vectors keep the per-entry
+    filter (:93-122)."""
+    blocks = assemble_main_blocks(prob, u0, ell, zero_tol, g_scale)
+    K = sp.bmat([[blocks["A_y"], blocks["B"].T], [blocks["B"], blocks["C_signed"]]], format="csr")
+    K.sum_duplicates()
+    K.data[np.abs(K.data) <= zero_tol] = 0.0
+    K.eliminate_zeros()
+    K.sort_indices()
+    return K, np.concatenate([blocks["f"], blocks["g"]])
 
 
 def bottom_cells(x_geom):

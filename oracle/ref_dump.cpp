@@ -8,7 +8,12 @@
 //     (finite_element::system::assemble_main_system_blocks,
 //      src/finite_element/system/assemble_saddle_problem.hpp:131),
 //   * the parabolic graph-norm Schur approximation Hhat
-//     (src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:22).
+//     (src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:22),
+//   * 2+1D: the direct-solver path's full saddle matrix and right-hand side by the
+//     two-pass pattern + numeric assembly
+//     (src/finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp:468), twice
+//     through one pattern cache: the example's coefficients, then a constant anisotropic
+//     M = [[2, 0.5], [0.5, 1]] on the reused pattern.
 //
 // usage: apf_ref_dump <dim:1|2> <p:1|2> <uniform_levels> <example> <outdir>
 //        apf_ref_dump bench <p:1|2> <uniform_levels> <example> <reps>
@@ -39,6 +44,7 @@
 #include "finite_element/fespace/policies.hpp"
 #include "finite_element/system/assemble_saddle_problem.hpp"
 #include "finite_element/assembly/main_system/parabolic_graph_norm.hpp"
+#include "finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp"
 #include "finite_element/assembly/constrained_dofs.hpp"
 #include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
 #include "algorithm/detail/indicator_utilities.hpp"
@@ -304,6 +310,31 @@ namespace
         const auto gn = finite_element::assembly::assemble_parabolic_graph_norm_approximation<QSpace, QTime, Backend>(
             y_space, x_space, example.problem.M, blocks.A_y(), blocks.C_signed(), 1e-15, 1e-14);
         dump_csc(dir, "Hhat", gn.approximation.hhat);
+
+        {
+            namespace fa = finite_element::assembly;
+            fa::detail::AssemblySpaceCache<YSpace> y_cache(y_space);
+            fa::detail::AssemblySpaceCache<XSpace> x_cache(x_space);
+            fa::detail::ActiveAncestorCache<XSpace> ancestors(x_space);
+            fa::TwoPassFullSaddleAssemblyCache2D<Backend, XSpace, YSpace> cache;
+            const finite_element::detail::TimingRecorder timing{};
+            const auto full = fa::assemble_main_full_saddle_two_pass_2d<QSpace, QTime, Backend>(
+                x_space, y_space, x_cache, y_cache, ancestors, example.problem.M, example.problem.ell,
+                example.problem.u0, 1e-15, -1.0, timing, nullptr, 1, 0.0, &cache);
+            dump_csc(dir, "K2p", full.matrix);
+            dump_vec(dir, "K2p_rhs", full.rhs);
+            const adaptive_algorithm::examples::SpaceTime2DDiffusionFunctionM m_aniso =
+                [](const adaptive_algorithm::examples::SpaceTime2DPoint&) {
+                    return finite_element::coefficients::DiffusionTensor<2>{{{2.0, 0.5}, {0.5, 1.0}}};
+                };
+            const auto aniso = fa::assemble_main_full_saddle_two_pass_2d<QSpace, QTime, Backend>(
+                x_space, y_space, x_cache, y_cache, ancestors, m_aniso, example.problem.ell, example.problem.u0,
+                1e-15, -1.0, timing, nullptr, 1, 0.0, &cache);
+            dump_csc(dir, "K2p_aniso", aniso.matrix);
+            dump_vec(dir, "K2p_aniso_rhs", aniso.rhs);
+            const std::vector<int> reuse{static_cast<int>(cache.pattern_reuse_count)};
+            apf_oracle::write_npy(dir + "/K2p_pattern_reuse_count.npy", reuse);
+        }
 
         if (std::getenv("APF_REF_ESTIMATE") != nullptr)
         {

@@ -38,6 +38,13 @@ def load_golden(name):
     out = {nm: csc(nm) for nm in ("A_y", "B", "C_signed", "Hhat")}
     out["f"] = z["f"]
     out["g"] = z["g"]
+    if "K2p_values" in z:
+        # the reference's two-pass full saddle matrix: example coefficients, then the
+        # constant anisotropic M = [[2, 0.5], [0.5, 1]] on the cached pattern
+        for nm in ("K2p", "K2p_aniso"):
+            out[nm] = csc(nm)
+            out[nm + "_rhs"] = z[nm + "_rhs"]
+        out["K2p_pattern_reuse_count"] = int(z["K2p_pattern_reuse_count"][0])
     prob = O.MainProblem(p=p, y_geom=z["y_geometry"], x_geom=z["x_geometry"], y_to_x=z["y_to_x_cell"],
                          y_restr=restr("y_restriction"), x_restr=restr("x_restriction"),
                          n_lambda=out["A_y"].shape[0], n_u=out["C_signed"].shape[0], dim_space=dim)

@@ -29,6 +29,24 @@ def test_oracle_graph_norm_matches_reference(name):
     assert_same_sparse(ref["Hhat"], gn["Hhat"], 1e-12, "Hhat")
 
 
+M_ANISO = (2.0, 0.5, 1.0)  # (m00, m01, m11) of the fixtures' second two-pass call
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_two_pass_full_saddle_matches_reference(name):
+    prob, ref, example = load_golden(name)
+    u0 = O.sin_initial if example == "smooth_initial" else O.one_initial
+    assert ref["K2p_pattern_reuse_count"] == 1
+    for key, m in (("K2p", None), ("K2p_aniso", M_ANISO)):
+        prob.m_cells = None if m is None else np.tile(m, (prob.y_geom.shape[0], 1))
+        K, rhs = O.assemble_main_full_saddle_two_pass(prob, u0=u0)
+        assert_same_sparse(ref[key], K, 1e-12, key)
+        assert np.abs(rhs - ref[key + "_rhs"]).max() <= 1e-12 * np.abs(ref[key + "_rhs"]).max()
+    # the identity coefficient's right-angle couplings cancel to zero and are pruned; the
+    # anisotropic one keeps them, so the two patterns differ
+    assert ref["K2p"].nnz < ref["K2p_aniso"].nnz
+
+
 def _paper_rows():
     with open(os.path.join(GOLDEN, "paper_uniform_rows.json")) as fh:
         return json.load(fh)
