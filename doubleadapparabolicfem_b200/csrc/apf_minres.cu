@@ -407,6 +407,15 @@ namespace apf
     void BlockPreconditioner::apply(cudaStream_t s, const double* r, double* z)
     {
         require(side_ != nullptr, APF_ERR_INVALID, "block preconditioner used before its setup");
+        if (t_profiler && t_profiler->enabled && t_profiler->kernels)
+        {
+            // per-launch event timing: both V-cycles on the caller's stream, one after the
+            // other, so that each launch's duration is its own (no overlap with the other
+            // block's launches sharing the GPU)
+            amg_h.apply(s, r + n_lambda, z + n_lambda);
+            amg_a.apply(s, r, z);
+            return;
+        }
         APF_CUDA(cudaEventRecord(fork_, s));
         APF_CUDA(cudaStreamWaitEvent(side_, fork_, 0));
         amg_h.apply(side_, r + n_lambda, z + n_lambda);

@@ -102,6 +102,16 @@ namespace apf
                 const int width = (sp[sl + 1] - base) >> 5;
                 const V* v = val + base + lane;
                 const int* c = col + base + lane;
+                // the row index (and, for y = a A x + b y, the old y) is requested before
+                // the loop, so its latency overlaps the matrix loads; the sweeps' operands
+                // b, x and the weights are read after it (hoisting them too cost the
+                // sweeps more in registers than it saved in latency)
+                const int rs = sl * 32 + lane;
+                const bool live = rs < rows;
+                const int r = live ? (perm ? __ldg(perm + rs) : rs) : 0;
+                double pre_y = 0.0;
+                if (MODE == 0 && live && beta != 0.0)
+                    pre_y = y[r];
                 // four independent load chains in flight per thread; the matrix streams
                 // through once (evict-first loads), x stays cached for the gathers
                 double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
@@ -121,10 +131,8 @@ namespace apf
                 for (; j < width; ++j)
                     s0 += static_cast<double>(__ldcs(v + 32 * j)) * __ldg(x + __ldcs(c + 32 * j));
                 const double sum = (s0 + s1) + (s2 + s3);
-                const int rs = sl * 32 + lane;
-                if (rs < rows)
+                if (live)
                 {
-                    const int r = perm ? perm[rs] : rs;
                     if (MODE == 1)
                         y[r] = b[r] - sum;
                     else if (MODE == 2)
@@ -136,7 +144,7 @@ namespace apf
                         z[r] = beta * dinv[r] * v;
                     }
                     else
-                        y[r] = beta == 0.0 ? alpha * sum : alpha * sum + beta * y[r];
+                        y[r] = beta == 0.0 ? alpha * sum : alpha * sum + beta * pre_y;
                 }
             }
         }
