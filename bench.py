@@ -408,9 +408,14 @@ def run_ours(args, world, rank, local):
     e1 = torch.cuda.Event(enable_timing=True)
     e_events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     e0.record(stream)
+    e2e_stage_ms = []
     for k in range(args.steps):
+        ctx.check(lib.apf_ctx_set_timing(ctx.handle, 2))
         lib.apf_system_destroy(step(hprob, False))
         e_events[k].record(stream)
+        rep = json.loads(lib.apf_ctx_timing_report(ctx.handle).decode())
+        e2e_stage_ms.append({k2[5:]: round(v[1], 1) for k2, v in rep.items() if k2.startswith("host:")})
+    ctx.check(lib.apf_ctx_set_timing(ctx.handle, 0))
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
@@ -593,6 +598,7 @@ def run_ours(args, world, rank, local):
                    "step_ms": step_ms,
                    "step_stage_wall_ms": stage_ms,
                    "e2e_step_ms": e2e_step_ms,
+                   "e2e_step_stage_wall_ms": e2e_stage_ms[-1] if e2e_stage_ms else None,
                    "final_true_residual_max": max(d["final_true_residual"] for d in timed_diags),
                    "e2e_final_true_residual_max": max(d["final_true_residual"] for d in e2e_diags),
                    "flux_squared": timed_est[-1]["flux_squared"] if timed_est else None,
