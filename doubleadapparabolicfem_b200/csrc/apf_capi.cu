@@ -876,7 +876,7 @@ const char* apf_ctx_autotune_report(apf_ctx* ctx)
     const auto& t = ctx->tuner;
     for (int p = 0; p < 2; ++p)
         for (int f = 0; f < 2; ++f)
-            for (int b = 0; b < 5; ++b)
+            for (int b = 0; b < apf::kPatchBuckets; ++b)
             {
                 if (t.width[p][f][b] == 0)
                     continue;

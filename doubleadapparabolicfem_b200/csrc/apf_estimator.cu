@@ -1839,8 +1839,8 @@ namespace apf
         pa.sigma = sigma.get();
         pa.status = status.get();
         // patches sorted into size buckets (one warp each; shared memory sized per bucket)
-        constexpr int kBuckets = 5;
-        static constexpr int kBucketMax[kBuckets] = {32, 48, 64, 96, 144};
+        constexpr int kBuckets = kPatchBuckets;
+        const int* kBucketMax = kPatchBucketMax;
         std::vector<int> bucket_count(kBuckets + 1, 0), order(tot.n_patches);
         {
             std::vector<signed char> bucket_of(tot.n_patches);
@@ -1964,11 +1964,17 @@ namespace apf
         APF_HOST_RANGE("est_patch_solves");
         if (tot.n_patches > 0)
         {
-            launch(std::integral_constant<int, 32>{}, 0);
-            launch(std::integral_constant<int, 48>{}, 1);
-            launch(std::integral_constant<int, 64>{}, 2);
-            launch(std::integral_constant<int, 96>{}, 3);
-            launch(std::integral_constant<int, 144>{}, 4);
+            static_assert(kPatchBuckets == 7 && kPatchBucketMax[0] == 30 && kPatchBucketMax[1] == 40 &&
+                              kPatchBucketMax[2] == 48 && kPatchBucketMax[3] == 58 && kPatchBucketMax[4] == 64 &&
+                              kPatchBucketMax[5] == 96 && kPatchBucketMax[6] == 144,
+                          "bucket launches follow kPatchBucketMax");
+            launch(std::integral_constant<int, 30>{}, 0);
+            launch(std::integral_constant<int, 40>{}, 1);
+            launch(std::integral_constant<int, 48>{}, 2);
+            launch(std::integral_constant<int, 58>{}, 3);
+            launch(std::integral_constant<int, 64>{}, 4);
+            launch(std::integral_constant<int, 96>{}, 5);
+            launch(std::integral_constant<int, 144>{}, 6);
             APF_CUDA(cudaGetLastError());
         }
         if (ev0)

@@ -43,11 +43,15 @@ namespace apf
     struct PatchTuner
     {
         bool enabled = true;
-        int width[2][2][5] = {};     // [p - 1][FP32][bucket] -> warps per patch (0: not tuned)
-        float ms[2][2][5][3] = {};   // candidate times of the tuning launch
-        int patches[2][2][5] = {};   // patches in the bucket when it was tuned
+        int width[2][2][7] = {};     // [p - 1][FP32][bucket] -> warps per patch (0: not tuned)
+        float ms[2][2][7][3] = {};   // candidate times of the tuning launch
+        int patches[2][2][7] = {};   // patches in the bucket when it was tuned
     };
-    constexpr int kPatchBucketMax[5] = {32, 48, 64, 96, 144};
+    // patch-size buckets (largest system size of each): the patch matrix's shared-memory
+    // slice, and so the teams per SM, follows the bucket, so the ladder is fine where the
+    // common sizes lie (P1: 29 unknowns at valence-4 vertices, 57 at valence 8)
+    constexpr int kPatchBuckets = 7;
+    constexpr int kPatchBucketMax[kPatchBuckets] = {30, 40, 48, 58, 64, 96, 144};
 
     // patch_precision: APF_PATCH_FP64 or APF_PATCH_FP32_REFINED (p = 1)
     EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
