@@ -4,6 +4,9 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <numeric>
+#include <vector>
 #include <array>
 #include <memory>
 #include <new>
@@ -301,6 +304,85 @@ namespace apf
                    bdtT, diag_tol, S.blocks[APF_BLOCK_HHAT], S.inv_diag_ay);
         S.have[APF_BLOCK_HHAT] = true;
         sync(s);
+    }
+}
+
+namespace
+{
+    // n values of one array into host memory (a device array through the context's stream)
+    template<class T>
+    std::vector<T> fetch_host(apf_ctx* ctx, const T* p, int n, bool on_device)
+    {
+        std::vector<T> h(static_cast<std::size_t>(n));
+        if (n == 0)
+            return h;
+        apf::require(p != nullptr, APF_ERR_INVALID, "artifact writer: null array");
+        if (on_device)
+        {
+            APF_CUDA(cudaMemcpyAsync(h.data(), p, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->stream));
+            APF_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+        else
+            std::memcpy(h.data(), p, sizeof(T) * n);
+        return h;
+    }
+
+    // entry order of the reference's writers: decreasing total, ties by increasing cell id
+    // (CellwiseSquaredError::sorted_descending), or the given order
+    std::vector<int> artifact_order(const std::vector<int32_t>& ids, const std::vector<double>& key, bool sort)
+    {
+        std::vector<int> order(ids.size());
+        std::iota(order.begin(), order.end(), 0);
+        if (sort)
+            std::sort(order.begin(), order.end(), [&](int a, int b) {
+                if (key[a] != key[b])
+                    return key[a] > key[b];
+                return ids[a] < ids[b];
+            });
+        return order;
+    }
+
+    void write_artifact(const char* path, const std::vector<int32_t>& header, const std::vector<int32_t>& ids,
+                        const std::vector<const std::vector<double>*>& columns, const std::vector<int>& order)
+    {
+        std::ofstream f(path, std::ios::binary | std::ios::trunc);
+        apf::require(f.is_open(), APF_ERR_INVALID, std::string("artifact writer: cannot open ") + path);
+        f.write(reinterpret_cast<const char*>(header.data()), static_cast<std::streamsize>(header.size() * 4));
+        std::vector<int32_t> oid(order.size());
+        for (std::size_t k = 0; k < order.size(); ++k)
+            oid[k] = ids[static_cast<std::size_t>(order[k])];
+        // empty blocks are not written (write_binary_block skips empty vectors)
+        if (!oid.empty())
+            f.write(reinterpret_cast<const char*>(oid.data()), static_cast<std::streamsize>(oid.size() * 4));
+        std::vector<double> col(order.size());
+        for (const auto* c : columns)
+        {
+            for (std::size_t k = 0; k < order.size(); ++k)
+                col[k] = (*c)[static_cast<std::size_t>(order[k])];
+            if (!col.empty())
+                f.write(reinterpret_cast<const char*>(col.data()), static_cast<std::streamsize>(col.size() * 8));
+        }
+        apf::require(static_cast<bool>(f), APF_ERR_INTERNAL, std::string("artifact writer: write failed: ") + path);
+    }
+
+    template<class F>
+    int host_guarded(apf_ctx* ctx, F&& f)
+    {
+        if (ctx)
+            return guarded(ctx, std::forward<F>(f));
+        try
+        {
+            f();
+            return APF_OK;
+        }
+        catch (const apf::Error& e)
+        {
+            return e.code;
+        }
+        catch (const std::exception&)
+        {
+            return APF_ERR_INTERNAL;
+        }
     }
 }
 
@@ -983,6 +1065,38 @@ int apf_y_estimator_threshold_squared(double rho, double lambda_y_squared, doubl
     const double shifted = rho + 0.5;
     *threshold_squared = rho * rho * (lambda_y_squared + (1.0 + 1.0 / (shifted * shifted)) * initial_trace_squared);
     return APF_OK;
+}
+
+int apf_write_cellwise_error_binary(apf_ctx* ctx, const char* path, int32_t n_cells, const int32_t* cell_ids,
+                                    const double* values, int pointers_on_device, int sort_descending)
+{
+    if (!path || n_cells < 0 || (pointers_on_device && !ctx))
+        return APF_ERR_INVALID;
+    return host_guarded(ctx, [&] {
+        const auto ids = fetch_host(ctx, cell_ids, n_cells, pointers_on_device != 0);
+        const auto v = fetch_host(ctx, values, n_cells, pointers_on_device != 0);
+        // header: format version 1, entry count
+        write_artifact(path, {1, n_cells}, ids, {&v}, artifact_order(ids, v, sort_descending != 0));
+    });
+}
+
+int apf_write_cellwise_error_components_binary(apf_ctx* ctx, const char* path, int32_t n_cells,
+                                               const int32_t* cell_ids, const double* flux, const double* recon,
+                                               const double* divergence, const double* eta, int pointers_on_device,
+                                               int sort_descending)
+{
+    if (!path || n_cells < 0 || (pointers_on_device && !ctx))
+        return APF_ERR_INVALID;
+    return host_guarded(ctx, [&] {
+        const bool dev = pointers_on_device != 0;
+        const auto ids = fetch_host(ctx, cell_ids, n_cells, dev);
+        const auto f = fetch_host(ctx, flux, n_cells, dev);
+        const auto r = fetch_host(ctx, recon, n_cells, dev);
+        const auto d = fetch_host(ctx, divergence, n_cells, dev);
+        const auto e = fetch_host(ctx, eta, n_cells, dev);
+        // header: format version 1, entry count, 4 components
+        write_artifact(path, {1, n_cells, 4}, ids, {&f, &r, &d, &e}, artifact_order(ids, e, sort_descending != 0));
+    });
 }
 
 int apf_true_residual_noalloc(apf_ctx* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_idx,

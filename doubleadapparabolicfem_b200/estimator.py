@@ -85,3 +85,36 @@ def y_estimator_threshold_squared(rho: float, lambda_y_squared: float, initial_t
     if rc != _lib.APF_OK:
         raise _lib.ApfError(rc, "compute_y_estimator_threshold_squared: rho must be positive.")
     return out.value
+
+
+def write_cellwise_error_binary(path: str, cell_ids: np.ndarray, values: np.ndarray, sort_descending: bool = True):
+    """The reference's cellwise_error.bin (write_cellwise_error_binary,
+    src/finite_element/io/write_cellwise_error_binary.hpp:24-79) from host arrays: int32
+    [1, n], int32 cell ids, float64 values, entries by decreasing value (ties by cell id)."""
+    lib = _lib.load()
+    ids = np.ascontiguousarray(cell_ids, dtype=np.int32)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    if ids.size != v.size:
+        raise ValueError("one value per cell id")
+    rc = lib.apf_write_cellwise_error_binary(None, str(path).encode(), ids.size, _ptr(ids), _ptr(v), 0,
+                                             1 if sort_descending else 0)
+    if rc != _lib.APF_OK:
+        raise _lib.ApfError(rc, f"write_cellwise_error_binary: cannot write {path}")
+
+
+def write_cellwise_error_components_binary(path: str, cell_ids: np.ndarray, cells: dict,
+                                           sort_descending: bool = True):
+    """The reference's cellwise_error_components.bin
+    (write_cellwise_error_components_binary,
+    src/finite_element/io/write_cellwise_error_components_binary.hpp:12-88) from the per-cell
+    arrays ``estimate`` returns (flux, reconstruction, divergence, eta): int32 [1, n, 4],
+    int32 cell ids, then the four float64 columns, entries by decreasing eta."""
+    lib = _lib.load()
+    ids = np.ascontiguousarray(cell_ids, dtype=np.int32)
+    cols = [np.ascontiguousarray(cells[k], dtype=np.float64) for k in ("flux", "reconstruction", "divergence", "eta")]
+    if any(c.size != ids.size for c in cols):
+        raise ValueError("one value per cell id in every column")
+    rc = lib.apf_write_cellwise_error_components_binary(None, str(path).encode(), ids.size, _ptr(ids),
+                                                        *[_ptr(c) for c in cols], 0, 1 if sort_descending else 0)
+    if rc != _lib.APF_OK:
+        raise _lib.ApfError(rc, f"write_cellwise_error_components_binary: cannot write {path}")

@@ -349,6 +349,28 @@ int apf_x_indicators(apf_ctx* ctx, apf_system* sys, int pointers_on_device, doub
 int apf_y_estimator_threshold_squared(double rho, double lambda_y_squared, double initial_trace_squared,
                                       double* threshold_squared);
 
+/* ---- estimator artifacts ---------------------------------------------------------- */
+/* The reference's binary files of an estimate, written from per-cell arrays (host, or
+ * device with pointers_on_device = 1 and a context; ctx may be NULL for host arrays).
+ * cell_ids are the mesh ids of the source (Y) cells, one per value.  Entry order: by
+ * decreasing value (eta for the components file), ties by increasing cell id, as
+ * CellwiseSquaredError::sorted_descending (src/finite_element/time_slabs/
+ * time_slab_cellwise_errors.hpp:54-68); sort_descending = 0 keeps the given order (the
+ * reference then writes its hash map's order).  Replaces
+ * write_cellwise_error_binary (src/finite_element/io/write_cellwise_error_binary.hpp:24-79):
+ *   int32 [version 1, n], int32 cell_ids[n], float64 values[n];
+ * and write_cellwise_error_components_binary
+ * (src/finite_element/io/write_cellwise_error_components_binary.hpp:12-88):
+ *   int32 [version 1, n, 4], int32 cell_ids[n], float64 flux[n], recon[n], divergence[n],
+ *   eta[n]  (the equilibrated-flux, reconstruction, divergence-residual and total
+ *   indicators squared, as apf_estimate returns them). */
+int apf_write_cellwise_error_binary(apf_ctx* ctx, const char* path, int32_t n_cells, const int32_t* cell_ids,
+                                    const double* values, int pointers_on_device, int sort_descending);
+int apf_write_cellwise_error_components_binary(apf_ctx* ctx, const char* path, int32_t n_cells,
+                                               const int32_t* cell_ids, const double* flux, const double* recon,
+                                               const double* divergence, const double* eta, int pointers_on_device,
+                                               int sort_descending);
+
 /* ---- allocation-free residual check ---------------------------------------------- */
 /* No counterpart in the reference: an addition for callers that cannot allocate device
  * memory where they need the check -- e.g. a solver loop whose device memory is all owned

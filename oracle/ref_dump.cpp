@@ -13,7 +13,11 @@
 //     two-pass pattern + numeric assembly
 //     (src/finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp:468), twice
 //     through one pattern cache: the example's coefficients, then a constant anisotropic
-//     M = [[2, 0.5], [0.5, 1]] on the reused pattern.
+//     M = [[2, 0.5], [0.5, 1]] on the reused pattern,
+//   * 2+1D with APF_REF_ESTIMATE: the reference's binary artifacts of the estimate,
+//     cellwise_error.bin and cellwise_error_components.bin
+//     (src/finite_element/io/write_cellwise_error_binary.hpp,
+//      src/finite_element/io/write_cellwise_error_components_binary.hpp).
 //
 // usage: apf_ref_dump <dim:1|2> <p:1|2> <uniform_levels> <example> <outdir>
 //        apf_ref_dump bench <p:1|2> <uniform_levels> <example> <reps>
@@ -45,6 +49,8 @@
 #include "finite_element/system/assemble_saddle_problem.hpp"
 #include "finite_element/assembly/main_system/parabolic_graph_norm.hpp"
 #include "finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp"
+#include "finite_element/io/write_cellwise_error_binary.hpp"
+#include "finite_element/io/write_cellwise_error_components_binary.hpp"
 #include "finite_element/assembly/constrained_dofs.hpp"
 #include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
 #include "algorithm/detail/indicator_utilities.hpp"
@@ -378,6 +384,11 @@ namespace
             dump_map("est_div", state.flux_diagnostics.by_source_cell_residual);
             dump_map("est_recon", state.reconstruction_y_squared.by_source_cell);
             dump_map("est_eta", state.estimator.estimator_squared.by_source_cell);
+            // the reference's binary artifacts of the estimate (sorted by decreasing value)
+            finite_element::io::write_cellwise_error_binary(state.estimator.estimator_squared, dir,
+                                                            "cellwise_error.bin");
+            finite_element::io::write_cellwise_error_components_binary(state.estimator, dir,
+                                                                       "cellwise_error_components.bin");
             std::fprintf(stderr, "estimate: flux=%.6e div=%.6e recon=%.6e eta=%.6e\n",
                          state.flux_diagnostics.total_flux(), state.flux_diagnostics.total_residual(),
                          state.reconstruction_y_squared.total(), state.estimator.total());

@@ -4,7 +4,8 @@ Runs oracle/_ref/apf_ref_dump (the reference's own templates compiled by
 oracle/Makefile against oracle/shim) on small uniform meshes and packs each case
 into one .npz: mesh and DOF maps, assembled blocks, and the reference's whole inner
 iteration (direct main solve, slab reconstruction, vertex-patch flux solves,
-per-cell indicators) and the driver's X-marking indicators.  Also extracts the uniform-refinement rows (exact DOF counts and
+per-cell indicators), the driver's X-marking indicators and the reference's binary
+artifacts of the estimate (cellwise_error.bin, cellwise_error_components.bin, as bytes).  Also extracts the uniform-refinement rows (exact DOF counts and
 6-significant-digit estimator values) of the reference's published paper data
 (algorithm_data_plot/{1d,2d}/*.csv) into paper_uniform_rows.json.
 
@@ -46,6 +47,9 @@ def dump_case(dim, p, level, example, outdir):
     arrays = {}
     for f in sorted(glob.glob(os.path.join(outdir, "*.npy"))):
         arrays[os.path.basename(f)[:-4]] = np.load(f)
+    # the reference's binary artifacts, byte for byte
+    for f in sorted(glob.glob(os.path.join(outdir, "*.bin"))):
+        arrays["bin_" + os.path.basename(f)[:-4]] = np.fromfile(f, dtype=np.uint8)
     return arrays
 
 

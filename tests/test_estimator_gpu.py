@@ -156,3 +156,41 @@ def test_autotuned_patch_launch_shapes_give_identical_indicators(gpu_ctx):
     assert report and all(v["warps_per_patch"] in (1, 2, 4) for v in report.values())
     for key in ("flux", "divergence", "eta"):
         assert np.array_equal(cells[key], ref_cells[key]), key
+
+
+@pytest.mark.parametrize("name", ["p1_l2_smooth", "p2_l1_smooth"])
+def test_cellwise_error_artifacts_from_device_estimate(gpu_ctx, name, tmp_path):
+    """The estimate's per-cell arrays written as the reference's binary artifacts from
+    device buffers (pointers_on_device = 1) equal the same arrays written from the host,
+    byte for byte, and hold the reference's own file's cells with values within 1e-9 of
+    its largest."""
+    import ctypes as C
+    import torch
+    from doubleadapparabolicfem_b200.estimator import write_cellwise_error_components_binary
+    prob, ref, example = load_golden(name)
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    product = to_product_problem(prob, example)
+    product.y_vertex_ids = z["y_vertex_ids"]
+    _, (cells, _) = _solve_and_estimate(gpu_ctx, product)
+    ids = z["y_cell_ids"].astype(np.int32)
+    host = tmp_path / "host.bin"
+    write_cellwise_error_components_binary(host, ids, cells)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in cells.items()}
+    dids = torch.from_numpy(ids).cuda()
+    torch.cuda.synchronize()
+    rc = gpu_ctx.lib.apf_write_cellwise_error_components_binary(
+        gpu_ctx.handle, str(tmp_path / "dev.bin").encode(), ids.size, C.c_void_p(dids.data_ptr()),
+        *[C.c_void_p(dev[k].data_ptr()) for k in ("flux", "reconstruction", "divergence", "eta")], 1, 1)
+    gpu_ctx.check(rc)
+    assert (tmp_path / "dev.bin").read_bytes() == host.read_bytes()
+    raw = z["bin_cellwise_error_components"].tobytes()
+    n = int(np.frombuffer(raw, dtype=np.int32, count=3)[1])
+    ref_ids = np.frombuffer(raw, dtype=np.int32, count=n, offset=12)
+    ref_eta = np.frombuffer(raw, dtype=np.float64, count=n, offset=12 + 4 * n + 24 * n)
+    mine = np.fromfile(host, dtype=np.uint8).tobytes()
+    my_ids = np.frombuffer(mine, dtype=np.int32, count=n, offset=12)
+    my_eta = np.frombuffer(mine, dtype=np.float64, count=n, offset=12 + 4 * n + 24 * n)
+    assert np.array_equal(np.sort(my_ids), np.sort(ref_ids))
+    a, b = np.argsort(my_ids), np.argsort(ref_ids)
+    assert np.abs(my_eta[a] - ref_eta[b]).max() <= 1e-9 * np.abs(ref_eta).max()
+    assert np.all(np.diff(my_eta) <= 0.0)
