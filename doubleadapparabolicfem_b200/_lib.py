@@ -122,6 +122,8 @@ SIGNATURES = {
                                         C.c_int),
     "apf_write_cellwise_error_components_binary": ([C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "apf_write_x_indicator_components_binary": ([C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "apf_two_pass_cache_create": ([C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
     "apf_two_pass_cache_destroy": ([C.c_void_p], None),
     "apf_two_pass_cache_stats": ([C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)],

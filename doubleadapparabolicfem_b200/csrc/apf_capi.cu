@@ -1099,6 +1099,23 @@ int apf_write_cellwise_error_components_binary(apf_ctx* ctx, const char* path, i
     });
 }
 
+int apf_write_x_indicator_components_binary(apf_ctx* ctx, const char* path, int32_t n_x_cells,
+                                            const int32_t* x_cell_ids, const double* lambda_by_x,
+                                            const double* trace_by_x, const double* eta_by_x, int pointers_on_device)
+{
+    if (!path || n_x_cells < 0 || (pointers_on_device && !ctx))
+        return APF_ERR_INVALID;
+    return host_guarded(ctx, [&] {
+        const bool dev = pointers_on_device != 0;
+        const auto ids = fetch_host(ctx, x_cell_ids, n_x_cells, dev);
+        const auto l = fetch_host(ctx, lambda_by_x, n_x_cells, dev);
+        const auto t = fetch_host(ctx, trace_by_x, n_x_cells, dev);
+        const auto e = fetch_host(ctx, eta_by_x, n_x_cells, dev);
+        // header: format version 1, entry count, 3 components; always by decreasing eta
+        write_artifact(path, {1, n_x_cells, 3}, ids, {&l, &t, &e}, artifact_order(ids, e, true));
+    });
+}
+
 int apf_true_residual_noalloc(apf_ctx* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_idx,
                               const double* values, const double* x, const double* b, double* absolute_residual,
                               double* relative_residual)

@@ -118,3 +118,19 @@ def write_cellwise_error_components_binary(path: str, cell_ids: np.ndarray, cell
                                                         *[_ptr(c) for c in cols], 0, 1 if sort_descending else 0)
     if rc != _lib.APF_OK:
         raise _lib.ApfError(rc, f"write_cellwise_error_components_binary: cannot write {path}")
+
+
+def write_x_indicator_components_binary(path: str, x_cell_ids: np.ndarray, lambda_by_x: np.ndarray,
+                                        trace_by_x: np.ndarray, eta_by_x: np.ndarray):
+    """The driver's x_indicator_components.bin (write_x_indicator_components_binary,
+    algorithm/output/iteration_snapshot_writer.hpp:173-233) from host arrays: int32
+    [1, n, 3], int32 X cell ids, float64 lambda_y, initial_trace, eta, by decreasing eta."""
+    lib = _lib.load()
+    ids = np.ascontiguousarray(x_cell_ids, dtype=np.int32)
+    cols = [np.ascontiguousarray(c, dtype=np.float64) for c in (lambda_by_x, trace_by_x, eta_by_x)]
+    if any(c.size != ids.size for c in cols):
+        raise ValueError("one value per X cell id in every column")
+    rc = lib.apf_write_x_indicator_components_binary(None, str(path).encode(), ids.size, _ptr(ids),
+                                                     *[_ptr(c) for c in cols], 0)
+    if rc != _lib.APF_OK:
+        raise _lib.ApfError(rc, f"write_x_indicator_components_binary: cannot write {path}")

@@ -370,6 +370,15 @@ int apf_write_cellwise_error_components_binary(apf_ctx* ctx, const char* path, i
                                                const int32_t* cell_ids, const double* flux, const double* recon,
                                                const double* divergence, const double* eta, int pointers_on_device,
                                                int sort_descending);
+/* The driver's x_indicator_components.bin from the X-marking indicators (apf_x_indicators'
+ * per-X-cell arrays; x_cell_ids = mesh ids of the active X cells).  Replaces
+ * adaptive_algorithm::output::detail::write_x_indicator_components_binary
+ * (algorithm/output/iteration_snapshot_writer.hpp:173-233):
+ *   int32 [version 1, n, 3], int32 cell_ids[n], float64 lambda_y[n], initial_trace[n],
+ *   eta[n], entries by decreasing eta, ties by increasing cell id. */
+int apf_write_x_indicator_components_binary(apf_ctx* ctx, const char* path, int32_t n_x_cells,
+                                            const int32_t* x_cell_ids, const double* lambda_by_x,
+                                            const double* trace_by_x, const double* eta_by_x, int pointers_on_device);
 
 /* ---- allocation-free residual check ---------------------------------------------- */
 /* No counterpart in the reference: an addition for callers that cannot allocate device

@@ -15,9 +15,10 @@
 //     through one pattern cache: the example's coefficients, then a constant anisotropic
 //     M = [[2, 0.5], [0.5, 1]] on the reused pattern,
 //   * 2+1D with APF_REF_ESTIMATE: the reference's binary artifacts of the estimate,
-//     cellwise_error.bin and cellwise_error_components.bin
+//     cellwise_error.bin, cellwise_error_components.bin and x_indicator_components.bin
 //     (src/finite_element/io/write_cellwise_error_binary.hpp,
-//      src/finite_element/io/write_cellwise_error_components_binary.hpp).
+//      src/finite_element/io/write_cellwise_error_components_binary.hpp,
+//      algorithm/output/iteration_snapshot_writer.hpp:173-233).
 //
 // usage: apf_ref_dump <dim:1|2> <p:1|2> <uniform_levels> <example> <outdir>
 //        apf_ref_dump bench <p:1|2> <uniform_levels> <example> <reps>
@@ -51,6 +52,7 @@
 #include "finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp"
 #include "finite_element/io/write_cellwise_error_binary.hpp"
 #include "finite_element/io/write_cellwise_error_components_binary.hpp"
+#include "algorithm/output/iteration_snapshot_writer.hpp"
 #include "finite_element/assembly/constrained_dofs.hpp"
 #include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
 #include "algorithm/detail/indicator_utilities.hpp"
@@ -389,6 +391,8 @@ namespace
                                                             "cellwise_error.bin");
             finite_element::io::write_cellwise_error_components_binary(state.estimator, dir,
                                                                        "cellwise_error_components.bin");
+            adaptive_algorithm::output::detail::write_x_indicator_components_binary(xi, dir,
+                                                                                    "x_indicator_components.bin");
             std::fprintf(stderr, "estimate: flux=%.6e div=%.6e recon=%.6e eta=%.6e\n",
                          state.flux_diagnostics.total_flux(), state.flux_diagnostics.total_residual(),
                          state.reconstruction_y_squared.total(), state.estimator.total());

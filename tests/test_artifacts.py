@@ -1,5 +1,5 @@
 """The reference's binary artifacts of an estimate (cellwise_error.bin,
-cellwise_error_components.bin), written by the library through the C ABI from host
+cellwise_error_components.bin, x_indicator_components.bin), written by the library through the C ABI from host
 arrays (no GPU): byte for byte against the files the reference's own writers produced
 for the golden cases (fixtures ``bin_*``, by ``tests/golden/make_golden.py``).  The values
 are taken from the reference's files, given to the writer in mesh-cell order, so the
@@ -59,3 +59,16 @@ def test_cellwise_error_binary_ties_break_by_cell_id(tmp_path):
     write_cellwise_error_binary(out, ids, vals)
     _, ids2, (vals2,) = _parse(np.fromfile(out, dtype=np.uint8), 2, 1)
     assert list(ids2) == [1, 3, 5, 7] and list(vals2) == [2.0, 2.0, 1.0, 1.0]
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_x_indicator_components_binary_matches_reference_bytes(name, tmp_path):
+    from doubleadapparabolicfem_b200.estimator import write_x_indicator_components_binary
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    ref = z["bin_x_indicator_components"]
+    head, ids, (lam, trace, eta) = _parse(ref, 3, 3)
+    assert list(head) == [1, len(ids), 3]
+    order = np.argsort(ids, kind="stable")
+    out = tmp_path / "x_indicator_components.bin"
+    write_x_indicator_components_binary(out, ids[order], lam[order], trace[order], eta[order])
+    assert out.read_bytes() == ref.tobytes()
