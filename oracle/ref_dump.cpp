@@ -14,7 +14,7 @@
 //     (src/finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp:468), twice
 //     through one pattern cache: the example's coefficients, then a constant anisotropic
 //     M = [[2, 0.5], [0.5, 1]] on the reused pattern,
-//   * 2+1D with APF_REF_ESTIMATE: the reference's binary artifacts of the estimate,
+//   * with APF_REF_ESTIMATE (2+1D and 1+1D): the reference's binary artifacts of the estimate,
 //     cellwise_error.bin, cellwise_error_components.bin and x_indicator_components.bin
 //     (src/finite_element/io/write_cellwise_error_binary.hpp,
 //      src/finite_element/io/write_cellwise_error_components_binary.hpp,
@@ -498,6 +498,12 @@ namespace
             dump_over("xind_eta_by_x", x_cells, xi.eta_squared_by_x_cell.by_source_cell);
             dump_over("est_flux", y_cells, state.flux_diagnostics.by_source_cell_flux);
             dump_over("est_div", y_cells, state.flux_diagnostics.by_source_cell_residual);
+            finite_element::io::write_cellwise_error_binary(state.estimator.estimator_squared, dir,
+                                                            "cellwise_error.bin");
+            finite_element::io::write_cellwise_error_components_binary(state.estimator, dir,
+                                                                       "cellwise_error_components.bin");
+            adaptive_algorithm::output::detail::write_x_indicator_components_binary(xi, dir,
+                                                                                    "x_indicator_components.bin");
             dump_over("est_recon", y_cells, state.reconstruction_y_squared.by_source_cell);
             dump_over("est_eta", y_cells, state.estimator.estimator_squared.by_source_cell);
             std::fprintf(stderr, "estimate: flux=%.6e div=%.6e recon=%.6e eta=%.6e\n",

@@ -1,7 +1,7 @@
 """The reference's binary artifacts of an estimate (cellwise_error.bin,
 cellwise_error_components.bin, x_indicator_components.bin), written by the library through the C ABI from host
 arrays (no GPU): byte for byte against the files the reference's own writers produced
-for the golden cases (fixtures ``bin_*``, by ``tests/golden/make_golden.py``).  The values
+for the golden cases, 2+1D and 1+1D (fixtures ``bin_*``, by ``tests/golden/make_golden.py``).  The values
 are taken from the reference's files, given to the writer in mesh-cell order, so the
 comparison pins the header, the block layout and the entry order (decreasing value,
 ties by increasing cell id)."""
@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, GOLDEN_CASES
+from conftest import GOLDEN, GOLDEN_CASES, GOLDEN_CASES_1D
 
 
 def _parse(raw: np.ndarray, n_header: int, n_cols: int):
@@ -24,7 +24,7 @@ def _parse(raw: np.ndarray, n_header: int, n_cols: int):
     return head, ids, cols
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", GOLDEN_CASES + GOLDEN_CASES_1D)
 def test_cellwise_error_binaries_match_reference_bytes(name, tmp_path):
     from doubleadapparabolicfem_b200.estimator import (write_cellwise_error_binary,
                                                        write_cellwise_error_components_binary)
@@ -61,7 +61,7 @@ def test_cellwise_error_binary_ties_break_by_cell_id(tmp_path):
     assert list(ids2) == [1, 3, 5, 7] and list(vals2) == [2.0, 2.0, 1.0, 1.0]
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", GOLDEN_CASES + GOLDEN_CASES_1D)
 def test_x_indicator_components_binary_matches_reference_bytes(name, tmp_path):
     from doubleadapparabolicfem_b200.estimator import write_x_indicator_components_binary
     z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
