@@ -18,7 +18,9 @@ element, log-uniform in [0.1, 10] (M = kappa I).
     python -m doubleadapparabolicfem_b200.batch --problems 256 --seed 0
 
 prints one JSON line with the batch throughput and the FP32-refined patch solves' error
-against the FP64 path.
+against the FP64 path.  Under ``torchrun --nproc-per-node N`` each GPU solves its ``shard``
+of the batch (no exchange between GPUs); rank 0 prints the totals (elements summed, wall
+time of the slowest rank).
 """
 from __future__ import annotations
 
@@ -27,6 +29,7 @@ import ctypes as C
 import dataclasses
 import json
 import math
+import os
 import time
 
 import numpy as np
@@ -60,6 +63,23 @@ def random_batch(n_problems: int, seed: int = 0, cells=(1e4, 5e5), kappa=(0.1, 1
         m[:, 2] = kap
         out.append(dataclasses.replace(base, m_cells=m, meta={"level": level, "target_cells": target, "index": i}))
     return out
+
+
+def shard(problems: list[SpaceTimeProblem], rank: int, world: int) -> list[SpaceTimeProblem]:
+    """The problems one of ``world`` GPUs solves when a batch is spread over several: the
+    problems are independent, so each GPU stacks and solves its own share with no exchange
+    between GPUs.  Greedy by decreasing cell count onto the GPU with the fewest cells so far
+    (ties: the lower problem index, the lower rank), so every rank computes the same split
+    from the same batch and every problem lands on exactly one rank."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must lie in [0, world)")
+    loads = [0] * world
+    owner = [0] * len(problems)
+    for i in sorted(range(len(problems)), key=lambda k: (-problems[k].n_y_cells, k)):
+        r = min(range(world), key=lambda k: (loads[k], k))
+        owner[i] = r
+        loads[r] += problems[i].n_y_cells
+    return [q for q, r in zip(problems, owner) if r == rank]
 
 
 def stack(problems: list[SpaceTimeProblem]):
@@ -212,20 +232,46 @@ def main():
     ap.add_argument("--patch-precision", default="fp32_refined", choices=["fp64", "fp32_refined"])
     args = ap.parse_args()
     from .assembly import Context
-    ctx = Context(0)
+    # one process per GPU (torchrun): each rank solves its shard of the batch; only the
+    # scalar totals are combined (elements summed, wall time the slowest rank's)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("gloo", rank=rank, world_size=world)
+    ctx = Context(local)
     t0 = time.perf_counter()
-    problems = random_batch(args.problems, args.seed)
+    problems = shard(random_batch(args.problems, args.seed), rank, world)
     t_gen = time.perf_counter() - t0
     # warm-up on the smallest problem (kernel loading, pool growth)
     solve_batch(sorted(problems, key=lambda q: q.n_y_cells)[:1], ctx, args.tol, args.patch_precision)
     t1 = time.perf_counter()
+    if dist:
+        dist.barrier()
+        t1 = time.perf_counter()
     res, stats = solve_batch(problems, ctx, args.tol, args.patch_precision, args.max_cells_per_wave)
     wall = time.perf_counter() - t1
+    if dist:
+        totals = torch.tensor([float(sum(r["n_cells"] for r in res)), float(sum(r["n_dofs"] for r in res)), wall],
+                              dtype=torch.float64)
+        sums = totals[:2].clone()
+        dist.all_reduce(sums)
+        worst = totals[2:].clone()
+        dist.all_reduce(worst, op=dist.ReduceOp.MAX)
     # the FP32-refined patch solves against the FP64 path on the first wave
     first = next(waves(problems, args.max_cells_per_wave))
     cmp, _ = solve_batch(first, ctx, args.tol, "fp32_refined", args.max_cells_per_wave, compare_fp64=True)
     cells = sum(r["n_cells"] for r in res)
     dofs = sum(r["n_dofs"] for r in res)
+    if dist:
+        cells, dofs, wall = int(sums[0]), int(sums[1]), float(worst[0])
+        dist.destroy_process_group()
+        if rank != 0:
+            return
     device_s = sum(w["device_s"] for w in stats)
     levels = {}
     for q in problems:
@@ -233,6 +279,7 @@ def main():
     print(json.dumps({
         "workload": f"{args.problems} independent 2+1D P1 problems (seed {args.seed}), kappa log-uniform [0.1, 10] "
                     f"per element, tol {args.tol}, patch solves {args.patch_precision}",
+        "n_gpus": world, "scaling": "strong (one batch split over the GPUs)",
         "problems_per_level": {str(k): v for k, v in sorted(levels.items())},
         "cells": cells, "dofs": dofs, "waves": len(stats),
         "elements_per_s": cells / wall, "dofs_per_s": dofs / wall,

@@ -37,6 +37,49 @@ def test_stacked_problem_is_the_block_diagonal_union():
     assert off["lambda"][-1] == stacked.n_lambda and off["u"][-1] == stacked.n_u
 
 
+def _shard_rank(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    from doubleadapparabolicfem_b200.batch import random_batch, shard, stack
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    problems = random_batch(12, seed=4, cells=(200, 5000))
+    mine = shard(problems, rank, world)
+    stacked, _ = stack(mine) if mine else (None, None)
+    got = [None] * world
+    dist.all_gather_object(got, [q.meta["index"] for q in mine])
+    cells = torch.tensor([float(sum(q.n_y_cells for q in mine))], dtype=torch.float64)
+    dist.all_reduce(cells)
+    if rank == 0:
+        out.put((got, float(cells[0]), [sum(problems[i].n_y_cells for i in g) for g in got],
+                 max(q.n_y_cells for q in problems), sum(q.n_y_cells for q in problems),
+                 stacked.n_y_cells if stacked is not None else 0, sum(q.n_y_cells for q in mine)))
+    dist.destroy_process_group()
+
+
+def test_batch_shards_over_two_ranks_without_overlap():
+    """The multi-GPU form of a batch on two gloo ranks (CPU): every problem on exactly one
+    rank, the cell loads within one problem of each other, each rank's stack holding its
+    shard, and the scalar totals combined by one reduction."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shard_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got, total, loads, biggest, all_cells, stacked_cells, mine_cells = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert sorted(got[0] + got[1]) == list(range(12)) and not set(got[0]) & set(got[1])
+    assert total == all_cells
+    assert abs(loads[0] - loads[1]) <= biggest
+    assert stacked_cells == mine_cells
+
+
 @pytest.mark.gpu
 def test_batched_solve_and_estimate_match_single_problems(gpu_ctx):
     from doubleadapparabolicfem_b200.assembly import assemble_main_system_blocks
