@@ -248,34 +248,40 @@ def main():
     problems = shard(random_batch(args.problems, args.seed), rank, world)
     t_gen = time.perf_counter() - t0
     # warm-up on the smallest problem (kernel loading, pool growth)
-    solve_batch(sorted(problems, key=lambda q: q.n_y_cells)[:1], ctx, args.tol, args.patch_precision)
+    if problems:
+        solve_batch(sorted(problems, key=lambda q: q.n_y_cells)[:1], ctx, args.tol, args.patch_precision)
     t1 = time.perf_counter()
     if dist:
         dist.barrier()
         t1 = time.perf_counter()
     res, stats = solve_batch(problems, ctx, args.tol, args.patch_precision, args.max_cells_per_wave)
     wall = time.perf_counter() - t1
+    # the FP32-refined patch solves against the FP64 path on the first wave (a rank with an
+    # empty shard has none)
+    cmp = []
+    if problems:
+        first = next(waves(problems, args.max_cells_per_wave))
+        cmp, _ = solve_batch(first, ctx, args.tol, "fp32_refined", args.max_cells_per_wave, compare_fp64=True)
+    level_ids = list(range(16))
+    counts = [sum(1 for q in problems if int(q.meta["level"]) == lv) for lv in level_ids]
+    summed = [float(sum(r["n_cells"] for r in res)), float(sum(r["n_dofs"] for r in res))] + [float(c) for c in counts]
+    worst = [wall, sum(w["device_s"] for w in stats), max((r["residual"] for r in res), default=0.0),
+             max((r["fp32_refined_max_cell_err"] for r in cmp), default=0.0),
+             max((r["fp32_refined_total_rel_err"] for r in cmp), default=0.0)]
     if dist:
-        totals = torch.tensor([float(sum(r["n_cells"] for r in res)), float(sum(r["n_dofs"] for r in res)), wall],
-                              dtype=torch.float64)
-        sums = totals[:2].clone()
-        dist.all_reduce(sums)
-        worst = totals[2:].clone()
-        dist.all_reduce(worst, op=dist.ReduceOp.MAX)
-    # the FP32-refined patch solves against the FP64 path on the first wave
-    first = next(waves(problems, args.max_cells_per_wave))
-    cmp, _ = solve_batch(first, ctx, args.tol, "fp32_refined", args.max_cells_per_wave, compare_fp64=True)
-    cells = sum(r["n_cells"] for r in res)
-    dofs = sum(r["n_dofs"] for r in res)
-    if dist:
-        cells, dofs, wall = int(sums[0]), int(sums[1]), float(worst[0])
+        # every rank's totals: elements, DOFs and problems per level summed; wall time, device
+        # time, the largest per-problem residual and the FP32 errors the worst over the ranks
+        ts = torch.tensor(summed, dtype=torch.float64)
+        dist.all_reduce(ts)
+        tw = torch.tensor(worst, dtype=torch.float64)
+        dist.all_reduce(tw, op=dist.ReduceOp.MAX)
+        summed, worst = ts.tolist(), tw.tolist()
         dist.destroy_process_group()
         if rank != 0:
             return
-    device_s = sum(w["device_s"] for w in stats)
-    levels = {}
-    for q in problems:
-        levels[q.meta["level"]] = levels.get(q.meta["level"], 0) + 1
+    cells, dofs = int(summed[0]), int(summed[1])
+    levels = {lv: int(c) for lv, c in zip(level_ids, summed[2:]) if c > 0}
+    wall, device_s = worst[0], worst[1]
     print(json.dumps({
         "workload": f"{args.problems} independent 2+1D P1 problems (seed {args.seed}), kappa log-uniform [0.1, 10] "
                     f"per element, tol {args.tol}, patch solves {args.patch_precision}",
@@ -283,13 +289,14 @@ def main():
         "problems_per_level": {str(k): v for k, v in sorted(levels.items())},
         "cells": cells, "dofs": dofs, "waves": len(stats),
         "elements_per_s": cells / wall, "dofs_per_s": dofs / wall,
-        "device_elements_per_s": cells / device_s, "wall_s": wall, "device_s": device_s,
-        "host_stack_wait_s": sum(w["host_stack_wait_s"] for w in stats), "host_generate_s": t_gen,
-        "max_part_residual": max(r["residual"] for r in res),
-        "minres_iterations_per_wave": [w["minres_iterations"] for w in stats],
+        "device_elements_per_s": cells / device_s if device_s > 0 else None, "wall_s": wall,
+        "device_s_slowest_rank": device_s,
+        "host_stack_wait_s_rank0": sum(w["host_stack_wait_s"] for w in stats), "host_generate_s_rank0": t_gen,
+        "max_part_residual": worst[2],
+        "minres_iterations_per_wave_rank0": [w["minres_iterations"] for w in stats],
         "fp32_refined_vs_fp64_first_wave": {
-            "max_cell_err_over_max_cell": max(r["fp32_refined_max_cell_err"] for r in cmp),
-            "max_total_rel_err": max(r["fp32_refined_total_rel_err"] for r in cmp)},
+            "max_cell_err_over_max_cell": worst[3],
+            "max_total_rel_err": worst[4]},
     }))
 
 

@@ -7,8 +7,9 @@
 // aggregates from a distance-1 maximal independent set (hash priorities, deterministic);
 // tentative prolongator T (one 1 per row); P = (I - omega D_F^-1 A_F) T with the filtered
 // operator A_F (weak entries lumped onto the diagonal); A_c = P^T A P.  The coarsest
-// operator is inverted densely on the host once per setup (or, when coarsening stalls
-// above the dense size, smoothed with a fixed number of Jacobi sweeps).  The V-cycle uses
+// operator is inverted densely on the device once per setup (Gauss-Jordan, one launch per
+// pivot; or, when coarsening stalls above the dense size, smoothed with a fixed number of
+// Jacobi sweeps).  The V-cycle uses
 // the same damped-Jacobi sweeps before and after the coarse correction, so it is a
 // symmetric positive definite linear operator.
 #include <algorithm>

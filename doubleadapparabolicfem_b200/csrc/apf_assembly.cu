@@ -1816,6 +1816,86 @@ namespace apf
         APF_CUDA(cudaGetLastError());
     }
 
+    namespace
+    {
+        // dst[c][k] = sum_i src[src_index[c]][i] phi_i(node_k of dst cell c): the local
+        // function of the source prism evaluated at the nodes of the destination prism (the
+        // destination lies inside the source, so this represents it exactly)
+        __global__ void nodal_transfer_kernel(int p, int n, const double* __restrict__ dst_geo,
+                                              const int* __restrict__ src_index, const double* __restrict__ src_geo,
+                                              const double* __restrict__ src, double* __restrict__ dst)
+        {
+            const RefTables& t = c_tab[p - 1];
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+            {
+                const int sc = src_index ? src_index[c] : c;
+                const double* in = src + static_cast<long long>(sc) * t.ndof;
+                double* out = dst + static_cast<long long>(c) * t.ndof;
+                if (same_geometry(dst_geo, c, src_geo, sc))
+                {
+                    for (int k = 0; k < t.ndof; ++k)
+                        out[k] = in[k];
+                    continue;
+                }
+                const CellGeo gd = load_geo(dst_geo, c);
+                const CellGeo gs = load_geo(src_geo, sc);
+                for (int k = 0; k < t.ndof; ++k)
+                {
+                    double v = 0.0;
+                    for (int i = 0; i < t.ndof; ++i)
+                        v += transfer(t, gd, gs, i, k) * in[i];
+                    out[k] = v;
+                }
+            }
+        }
+
+        // out[c] = v_c^T A_c v_c with the local A_y block of prism c and nodal values v_c
+        __global__ void nodal_energy_kernel(int p, int n, const double* __restrict__ geo, const double* __restrict__ m,
+                                            const double* __restrict__ v, double* __restrict__ out)
+        {
+            const RefTables& t = c_tab[p - 1];
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+            {
+                const double* lam = v + static_cast<long long>(c) * t.ndof;
+                const CellGeo g = load_geo(geo, c);
+                double q00, q01, q11;
+                q_form(g, m, c, q00, q01, q11);
+                double e = 0.0;
+                for (int i = 0; i < t.ndof; ++i)
+                {
+                    const int s = i / t.nt, a = i % t.nt;
+                    double row = 0.0;
+                    for (int j = 0; j < t.ndof; ++j)
+                    {
+                        const int r = j / t.nt, b = j % t.nt;
+                        row += t.Mt[a][b] * ks(t, q00, q01, q11, s, r) * lam[j];
+                    }
+                    e += lam[i] * row;
+                }
+                out[c] = g.det * g.ht * e;
+            }
+        }
+    }
+
+    void nodal_transfer(cudaStream_t s, int p, int n, const double* dst_geo, const int* src_index, const double* src_geo,
+                        const double* src, double* dst)
+    {
+        if (n <= 0)
+            return;
+        APF_KERNEL("nodal_transfer", s);
+        nodal_transfer_kernel<<<grid_for(n, 128), 128, 0, s>>>(p, n, dst_geo, src_index, src_geo, src, dst);
+        APF_CUDA(cudaGetLastError());
+    }
+
+    void nodal_energy(cudaStream_t s, int p, int n, const double* geo, const double* m, const double* v, double* out)
+    {
+        if (n <= 0)
+            return;
+        APF_KERNEL("nodal_energy", s);
+        nodal_energy_kernel<<<grid_for(n, 128), 128, 0, s>>>(p, n, geo, m, v, out);
+        APF_CUDA(cudaGetLastError());
+    }
+
     void x_indicators(cudaStream_t s, const SystemInputs& in, const double* lambda, const double* u, double* lam_y,
                       double* lam_x, double* trace_x, double* eta_x)
     {

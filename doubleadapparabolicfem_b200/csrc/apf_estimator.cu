@@ -1699,6 +1699,355 @@ namespace apf
         done = true;
     }
 
+    // ---------------------------------------------------------------------------
+    // time-slab space of an adaptive Y (time_slab_builder.hpp:53-215): the slab times are
+    // the distinct time endpoints of the active Y cells; every Y cell is cut into one slab
+    // cell per slab it spans (slabs in time order, each slab's cells in Y order); the slab
+    // space is P_p x P_p on each slab, continuous in space inside the slab (the reference's
+    // refinement keeps each slab's spatial mesh conforming), broken between slabs, zero on
+    // the Dirichlet boundary (the spatial nodes whose Y restriction rows are empty).
+    // ---------------------------------------------------------------------------
+    namespace
+    {
+        // per (Y cell, spatial node): 1 when the restriction rows of all its time nodes are empty
+        __global__ void dirichlet_nodes_kernel(int n, int ns, int nt, const int* __restrict__ off,
+                                               unsigned char* __restrict__ out)
+        {
+            for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < (long long)n * ns;
+                 r += (long long)gridDim.x * blockDim.x)
+            {
+                bool empty = true;
+                for (int a = 0; a < nt; ++a)
+                    empty = empty && off[r * nt + a] == off[r * nt + a + 1];
+                out[r] = empty ? 1 : 0;
+            }
+        }
+
+        // flag = 1 when some restriction row has more than one entry or a weight other than 1
+        __global__ void nontrivial_restriction_kernel(long long rows, const int* __restrict__ off,
+                                                      const double* __restrict__ w, int* __restrict__ flag)
+        {
+            for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows;
+                 r += (long long)gridDim.x * blockDim.x)
+            {
+                const int b = off[r], e = off[r + 1];
+                if (e - b > 1 || (e - b == 1 && w[b] != 1.0))
+                    *flag = 1;
+            }
+        }
+
+        // per slab cell: the source Y cell's geometry with the slab's time interval, its M,
+        // load and X ancestor
+        __global__ void slab_cells_kernel(int n, const int* __restrict__ source, const int* __restrict__ slab,
+                                          const double* __restrict__ slab_times, const double* __restrict__ y_geo,
+                                          const double* __restrict__ m_y, const double* __restrict__ ell_y,
+                                          const int* __restrict__ y_to_x, double* __restrict__ geo,
+                                          double* __restrict__ m, double* __restrict__ ell, int* __restrict__ to_x)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+            {
+                const int y = source[c], k = slab[c];
+                for (int j = 0; j < 6; ++j)
+                    geo[8ll * c + j] = y_geo[8ll * y + j];
+                geo[8ll * c + 6] = slab_times[k];
+                geo[8ll * c + 7] = slab_times[k + 1];
+                if (m)
+                    for (int j = 0; j < 3; ++j)
+                        m[3ll * c + j] = m_y[3ll * y + j];
+                if (ell)
+                    ell[c] = ell_y[y];
+                to_x[c] = y_to_x[y];
+            }
+        }
+
+        // out[y] = sum of a over the slab cells of Y cell y (in slab order)
+        __global__ void reduce_to_source_kernel(int n, const int* __restrict__ ptr, const int* __restrict__ list,
+                                                const double* __restrict__ a, double* __restrict__ out)
+        {
+            for (int y = blockIdx.x * blockDim.x + threadIdx.x; y < n; y += gridDim.x * blockDim.x)
+            {
+                double s = 0.0;
+                for (int i = ptr[y]; i < ptr[y + 1]; ++i)
+                    s += a[list[i]];
+                out[y] = s;
+            }
+        }
+    }
+
+    struct SlabSpace
+    {
+        bool identity = true;        // slab space == Y (every Y cell in one slab, no hanging rows)
+        int n_cells = 0;             // slab cells
+        int n_slabs = 0;
+        int n_dofs = 0;
+        std::vector<double> slab_times;
+        std::vector<int> source, slab; // per slab cell
+        std::vector<double> times;     // per slab cell: t0 t1
+        std::vector<int> vids;         // per slab cell: 3 spatial vertex ids
+        std::vector<int> dof;          // per slab cell and local node: slab DOF or -1
+        std::vector<int> src_ptr, src_list; // Y cell -> its slab cells
+    };
+
+    // host integer work: slabs, slab cells, slab DOFs (bnode: Dirichlet flag per Y cell and
+    // spatial node)
+    void build_slab_space(int p, int ny, const std::vector<double>& ytimes, const std::vector<int>& yvids,
+                          const std::vector<unsigned char>& bnode, SlabSpace& sp)
+    {
+        const int ns = p == 1 ? 3 : 6, nt = p + 1, nd = ns * nt;
+        std::vector<double>& T = sp.slab_times;
+        T.assign(ytimes.begin(), ytimes.end());
+        std::sort(T.begin(), T.end());
+        T.erase(std::unique(T.begin(), T.end()), T.end());
+        sp.n_slabs = std::max<int>(0, static_cast<int>(T.size()) - 1);
+        auto index_of = [&](double t) {
+            const auto it = std::lower_bound(T.begin(), T.end(), t);
+            return static_cast<int>(it - T.begin());
+        };
+        std::vector<int> kb(ny), ke(ny), count(sp.n_slabs + 1, 0);
+        for (int c = 0; c < ny; ++c)
+        {
+            kb[c] = index_of(ytimes[2ll * c]);
+            ke[c] = index_of(ytimes[2ll * c + 1]);
+            require(kb[c] < ke[c], APF_ERR_INVALID, "estimator: Y cell with an empty time interval");
+            for (int k = kb[c]; k < ke[c]; ++k)
+                ++count[k + 1];
+        }
+        for (int k = 0; k < sp.n_slabs; ++k)
+            count[k + 1] += count[k];
+        const int nsc = count[sp.n_slabs];
+        sp.n_cells = nsc;
+        sp.source.assign(nsc, 0);
+        sp.slab.assign(nsc, 0);
+        {
+            std::vector<int> cur(count.begin(), count.end() - 1);
+            for (int c = 0; c < ny; ++c)
+                for (int k = kb[c]; k < ke[c]; ++k)
+                {
+                    const int i = cur[k]++;
+                    sp.source[i] = c;
+                    sp.slab[i] = k;
+                }
+        }
+        sp.times.resize(2ll * nsc);
+        sp.vids.resize(3ll * nsc);
+        for (int i = 0; i < nsc; ++i)
+        {
+            sp.times[2ll * i] = T[sp.slab[i]];
+            sp.times[2ll * i + 1] = T[sp.slab[i] + 1];
+            for (int v = 0; v < 3; ++v)
+                sp.vids[3ll * i + v] = yvids[3ll * sp.source[i] + v];
+        }
+        // spatial nodes of slab cell i: vertex nodes keyed by their vertex id, P2 edge nodes
+        // by their two vertex ids (node order v0 m01 v1 m02 m12 v2)
+        static const int kNodeVerts[2][6][2] = {{{0, 0}, {1, 1}, {2, 2}, {0, 0}, {0, 0}, {0, 0}},
+                                                {{0, 0}, {0, 1}, {1, 1}, {0, 2}, {1, 2}, {2, 2}}};
+        auto node_key = [&](int i, int s) {
+            const int a = sp.vids[3ll * i + kNodeVerts[p - 1][s][0]], b = sp.vids[3ll * i + kNodeVerts[p - 1][s][1]];
+            const std::uint32_t lo = static_cast<std::uint32_t>(std::min(a, b)), hi = static_cast<std::uint32_t>(std::max(a, b));
+            return (static_cast<std::uint64_t>(lo) << 32) | hi;
+        };
+        // per slab (host threads): spatial node numbering in first-appearance order
+        std::vector<int> local(static_cast<std::size_t>(nsc) * ns, -1), n_spatial(sp.n_slabs, 0);
+        const int nthreads = std::max(1, std::min<int>(8, static_cast<int>(std::thread::hardware_concurrency())));
+        {
+            std::vector<std::thread> pool;
+            for (int t = 0; t < nthreads; ++t)
+                pool.emplace_back([&, t]() {
+                    std::unordered_map<std::uint64_t, int> ids;
+                    for (int k = t; k < sp.n_slabs; k += nthreads)
+                    {
+                        ids.clear();
+                        for (int i = count[k]; i < count[k + 1]; ++i)
+                            for (int s = 0; s < ns; ++s)
+                            {
+                                if (bnode[static_cast<std::size_t>(sp.source[i]) * ns + s])
+                                    continue;
+                                const auto it = ids.emplace(node_key(i, s), static_cast<int>(ids.size())).first;
+                                local[static_cast<std::size_t>(i) * ns + s] = it->second;
+                            }
+                        n_spatial[k] = static_cast<int>(ids.size());
+                    }
+                });
+            for (auto& th : pool)
+                th.join();
+        }
+        std::vector<long long> base(sp.n_slabs + 1, 0);
+        for (int k = 0; k < sp.n_slabs; ++k)
+            base[k + 1] = base[k] + static_cast<long long>(n_spatial[k]) * nt;
+        require(base[sp.n_slabs] < (1ll << 31), APF_ERR_CAPACITY, "estimator: slab space too large");
+        sp.n_dofs = static_cast<int>(base[sp.n_slabs]);
+        sp.dof.assign(static_cast<std::size_t>(nsc) * nd, -1);
+        for (int i = 0; i < nsc; ++i)
+            for (int s = 0; s < ns; ++s)
+            {
+                const int l = local[static_cast<std::size_t>(i) * ns + s];
+                if (l < 0)
+                    continue;
+                for (int a = 0; a < nt; ++a)
+                    sp.dof[static_cast<std::size_t>(i) * nd + s * nt + a] =
+                        static_cast<int>(base[sp.slab[i]] + static_cast<long long>(l) * nt + a);
+            }
+        // Y cell -> slab cells
+        sp.src_ptr.assign(ny + 1, 0);
+        for (int i = 0; i < nsc; ++i)
+            ++sp.src_ptr[sp.source[i] + 1];
+        for (int c = 0; c < ny; ++c)
+            sp.src_ptr[c + 1] += sp.src_ptr[c];
+        sp.src_list.assign(nsc, 0);
+        {
+            std::vector<int> cur(sp.src_ptr.begin(), sp.src_ptr.end() - 1);
+            for (int i = 0; i < nsc; ++i)
+                sp.src_list[cur[sp.source[i]]++] = i;
+        }
+    }
+
+    // the slab space's inputs as a main-system SystemInputs (Y := slab space, X borrowed
+    // from the main system while the slab blocks are assembled)
+    struct SlabSystem
+    {
+        SystemInputs in;
+        DeviceBuffer<int> src_ptr, src_list;
+    };
+
+    void upload_slab_system(cudaStream_t s, const SystemInputs& yin, const SlabSpace& sp, SlabSystem& out)
+    {
+        SystemInputs& in = out.in;
+        in.p = yin.p;
+        in.ndof = yin.ndof;
+        in.dim = 2;
+        in.n_y_cells = sp.n_cells;
+        in.n_x_cells = yin.n_x_cells;
+        in.n_lambda = sp.n_dofs;
+        in.n_u = yin.n_u;
+        in.u0_kind = yin.u0_kind;
+        in.zero_tol = yin.zero_tol;
+        in.g_scale = yin.g_scale;
+        const int n = sp.n_cells, nd = yin.ndof;
+        DeviceBuffer<int> d_source(0, s), d_slab(0, s);
+        DeviceBuffer<double> d_times(0, s);
+        d_source.upload(sp.source.data(), sp.source.size());
+        d_slab.upload(sp.slab.data(), sp.slab.size());
+        d_times.upload(sp.slab_times.data(), sp.slab_times.size());
+        in.y_geo.allocate(8ll * n, s);
+        in.y_to_x.allocate(n, s);
+        if (yin.m_y.size())
+            in.m_y.allocate(3ll * n, s);
+        if (yin.ell.size())
+            in.ell.allocate(n, s);
+        if (n > 0)
+        {
+            APF_KERNEL("est_slab_cells", s);
+            slab_cells_kernel<<<nb(n), 256, 0, s>>>(n, d_source.get(), d_slab.get(), d_times.get(), yin.y_geo.get(),
+                                                     yin.m_y.size() ? yin.m_y.get() : nullptr,
+                                                     yin.ell.size() ? yin.ell.get() : nullptr, yin.y_to_x.get(),
+                                                     in.y_geo.get(), in.m_y.size() ? in.m_y.get() : nullptr,
+                                                     in.ell.size() ? in.ell.get() : nullptr, in.y_to_x.get());
+        }
+        // restriction: one entry of weight 1 per non-Dirichlet node
+        std::vector<int> off(static_cast<std::size_t>(n) * nd + 1, 0), dofs;
+        dofs.reserve(sp.dof.size());
+        for (std::size_t r = 0; r < sp.dof.size(); ++r)
+        {
+            if (sp.dof[r] >= 0)
+                dofs.push_back(sp.dof[r]);
+            off[r + 1] = static_cast<int>(dofs.size());
+        }
+        const std::vector<double> w(dofs.size(), 1.0);
+        in.y_off.upload(off.data(), off.size());
+        in.y_dofs.upload(dofs.data(), dofs.size());
+        in.y_w.upload(w.data(), w.size());
+        out.src_ptr.upload(sp.src_ptr.data(), sp.src_ptr.size());
+        out.src_list.upload(sp.src_list.data(), sp.src_list.size());
+        APF_CUDA(cudaGetLastError());
+    }
+
+    // swaps the main system's X inputs into a slab system for the lifetime of the guard
+    struct BorrowX
+    {
+        SystemInputs& a;
+        SystemInputs& b;
+        BorrowX(SystemInputs& main, SystemInputs& slab) : a(main), b(slab) { swap_x(); }
+        ~BorrowX() { swap_x(); }
+        void swap_x()
+        {
+            std::swap(a.x_geo, b.x_geo);
+            std::swap(a.x_off, b.x_off);
+            std::swap(a.x_dofs, b.x_dofs);
+            std::swap(a.x_w, b.x_w);
+        }
+    };
+
+    // lambda~ on the slab space: A_slab lambda~ = f_slab - B_slab^T u, the slab Riesz
+    // reconstruction of every slab at once (the slab blocks are the main-system A_y, B^T and
+    // f with the slab space as test space: time_slab_reconstruction_operator.hpp:686-830
+    // assembles the same forms), solved by CG with an SA-AMG V-cycle to 1e-14
+    void reconstruct_lambda_slabs(cudaStream_t s, System& S, SlabSystem& sl, DeviceBuffer<double>& lt,
+                                  EstimatorTotals& tot)
+    {
+        SystemInputs& in = sl.in;
+        const int nl = in.n_lambda, nd = in.ndof;
+        DeviceCsr A, Bt;
+        DeviceBuffer<double> f;
+        {
+            APF_HOST_RANGE("est_slab_assembly");
+            BorrowX borrow(S.in, in);
+            prepare_inputs(s, in);
+            const Incidence inc =
+                build_incidence(s, nl, in.n_y_cells, nullptr, nullptr, in.y_off.get(), in.y_dofs.get(), nd);
+            const int offs[1] = {0};
+            const Incidence* incs[1] = {&inc};
+            const int ka[1] = {K_AY};
+            gather_csr(s, in, in.zero_tol, nl, nl, 1, ka, incs, offs, in.kmax, A);
+            const int kbt[1] = {K_BT};
+            gather_csr(s, in, in.zero_tol, nl, in.n_u, 1, kbt, incs, offs, in.kmax, Bt);
+            gather_vector_host(s, in, in.zero_tol, 0, inc, nl, in.ell.size() ? in.ell.get() : nullptr, in.u0_kind,
+                               in.g_scale, f);
+            sync(s);
+        }
+        lt.allocate(static_cast<std::size_t>(nl), s);
+        lt.zero();
+        if (nl == 0)
+            return;
+        DeviceBuffer<double> rhs(nl, s), r(nl, s), z(nl, s), pv(nl, s), q(nl, s);
+        copy(s, nl, f.get(), rhs.get());
+        spmv(s, Bt, S.solution.get() + S.in.n_lambda, rhs.get(), -1.0, 1.0);
+        Amg amg;
+        {
+            APF_HOST_RANGE("est_slab_amg_setup");
+            DeviceBuffer<int> comp;
+            dof_time_components(s, in, true, comp);
+            AmgOptions o = S.precond_opts;
+            amg.setup(s, A, o, S.ws, comp.get());
+        }
+        copy(s, nl, rhs.get(), r.get());
+        const double bn = std::sqrt(dot_host(s, S.ws, nl, rhs.get(), rhs.get()));
+        double rn = bn;
+        int its = 0;
+        if (bn > 0.0)
+        {
+            APF_HOST_RANGE("est_reconstruction_pcg");
+            amg.apply(s, r.get(), z.get());
+            copy(s, nl, z.get(), pv.get());
+            double rz = dot_host(s, S.ws, nl, r.get(), z.get());
+            for (its = 1; its <= 400; ++its)
+            {
+                spmv(s, A, pv.get(), q.get());
+                const double alpha = rz / dot_host(s, S.ws, nl, pv.get(), q.get());
+                axpby(s, nl, alpha, pv.get(), 1.0, lt.get());
+                axpby(s, nl, -alpha, q.get(), 1.0, r.get());
+                rn = std::sqrt(dot_host(s, S.ws, nl, r.get(), r.get()));
+                if (!(rn > 1e-14 * bn))
+                    break;
+                amg.apply(s, r.get(), z.get());
+                const double rz2 = dot_host(s, S.ws, nl, r.get(), z.get());
+                axpby(s, nl, 1.0, z.get(), rz2 / rz, pv.get());
+                rz = rz2;
+            }
+        }
+        tot.recon_iterations = its;
+        tot.recon_residual = bn > 0.0 ? rn / bn : 0.0;
+    }
+
     void reconstruct_lambda(cudaStream_t s, System& S, DeviceBuffer<double>& lt, EstimatorTotals& tot)
     {
         const int nl = S.in.n_lambda;
@@ -1747,58 +2096,137 @@ namespace apf
         require(S.solution.size() == static_cast<std::size_t>(in.n_lambda + in.n_u), APF_ERR_INVALID,
                 "estimator: solve the main system first");
         require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
-        require(in.n_x_cells == in.n_y_cells, APF_ERR_INVALID, "estimator: Y cells must coincide with X cells");
         upload_est_tables_once();
         EstimatorTotals tot{};
-        const int ny = in.n_y_cells, nl = in.n_lambda;
-        // ---- patch topology: host integer work on the cells' time intervals and vertex ids,
-        // run on a host thread while the device solves the slab reconstruction
-        std::vector<double> times(2ll * ny);
+        const int ny = in.n_y_cells, nl = in.n_lambda, nd = in.ndof;
+        const int ns = in.p == 1 ? 3 : 6, nt = in.p + 1;
+        // ---- Y cell time intervals (host) and whether the Y restriction is trivial
+        std::vector<double> ytimes(2ll * ny);
+        int nontrivial = 0;
         {
             DeviceBuffer<double> dt(2ll * ny, s);
+            DeviceBuffer<int> flag(1, s);
+            flag.zero();
             if (ny)
             {
-                APF_KERNEL("est_cell_times", s);
-                cell_times_kernel<<<nb(ny), 256, 0, s>>>(ny, in.y_geo.get(), dt.get());
-                APF_CUDA(cudaMemcpyAsync(times.data(), dt.get(), times.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+                {
+                    APF_KERNEL("est_cell_times", s);
+                    cell_times_kernel<<<nb(ny), 256, 0, s>>>(ny, in.y_geo.get(), dt.get());
+                }
+                {
+                    APF_KERNEL("est_restriction_check", s);
+                    nontrivial_restriction_kernel<<<nb((long long)ny * nd), 256, 0, s>>>((long long)ny * nd,
+                                                                                       in.y_off.get(), in.y_w.get(),
+                                                                                       flag.get());
+                }
+                APF_CUDA(cudaMemcpyAsync(ytimes.data(), dt.get(), ytimes.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+                APF_CUDA(cudaMemcpyAsync(&nontrivial, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
             }
             sync(s);
         }
-        std::future<PatchSet> patches = std::async(std::launch::async, [&times, &vids_host, ny]() {
+        // ---- time slabs: when every Y cell lies in one slab and Y has no hanging rows the
+        // slab space is Y itself (uniform and space-only adaptive meshes); otherwise Y cells are
+        // cut into slab cells and lambda~ lives on the slab space
+        SlabSpace sp;
+        {
+            APF_HOST_RANGE("est_slab_space");
+            std::vector<double> T(ytimes);
+            std::sort(T.begin(), T.end());
+            T.erase(std::unique(T.begin(), T.end()), T.end());
+            bool one_slab_each = true;
+            for (int c = 0; c < ny && one_slab_each; ++c)
+            {
+                const auto a = std::upper_bound(T.begin(), T.end(), ytimes[2ll * c]);
+                one_slab_each = a != T.end() && *a == ytimes[2ll * c + 1];
+            }
+            sp.identity = one_slab_each && nontrivial == 0;
+        }
+        SlabSystem sl;
+        if (!sp.identity)
+        {
+            APF_HOST_RANGE("est_slab_space");
+            std::vector<unsigned char> bnode(static_cast<std::size_t>(ny) * ns);
+            if (ny)
+            {
+                DeviceBuffer<unsigned char> d_bnode(bnode.size(), s);
+                {
+                    APF_KERNEL("est_dirichlet_nodes", s);
+                    dirichlet_nodes_kernel<<<nb((long long)ny * ns), 256, 0, s>>>(ny, ns, nt, in.y_off.get(), d_bnode.get());
+                }
+                APF_CUDA(cudaMemcpyAsync(bnode.data(), d_bnode.get(), bnode.size(), cudaMemcpyDeviceToHost, s));
+                sync(s);
+            }
+            build_slab_space(in.p, ny, ytimes, vids_host, bnode, sp);
+            upload_slab_system(s, in, sp, sl);
+        }
+        // the cells the patches and indicators run on: Y cells, or slab cells
+        const int nc = sp.identity ? ny : sp.n_cells;
+        const double* cgeo = sp.identity ? in.y_geo.get() : sl.in.y_geo.get();
+        const double* cm = sp.identity ? (in.m_y.size() ? in.m_y.get() : nullptr)
+                                       : (sl.in.m_y.size() ? sl.in.m_y.get() : nullptr);
+        const double* cell = sp.identity ? (in.ell.size() ? in.ell.get() : nullptr)
+                                         : (sl.in.ell.size() ? sl.in.ell.get() : nullptr);
+        const int* cx = sp.identity ? in.y_to_x.get() : sl.in.y_to_x.get();
+        // ---- patch topology: host integer work on the cells' time intervals and vertex ids,
+        // run on a host thread while the device solves the slab reconstruction
+        std::future<PatchSet> patches = std::async(std::launch::async, [&sp, &ytimes, &vids_host, ny, nc]() {
             PatchSet ps;
-            build_patches(times, vids_host, ny, ps);
+            if (sp.identity)
+                build_patches(ytimes, vids_host, ny, ps);
+            else
+                build_patches(sp.times, sp.vids, nc, ps);
             return ps;
         });
-        // ---- lambda~ : A_y lambda~ = f - B^T u
-        DeviceBuffer<double> lt(nl, s);
-        reconstruct_lambda(s, S, lt, tot);
+        // ---- lambda~
+        DeviceBuffer<double> lt(sp.identity ? nl : 0, s);
+        if (sp.identity)
+            reconstruct_lambda(s, S, lt, tot);
+        else
+            reconstruct_lambda_slabs(s, S, sl, lt, tot);
         PatchSet ps;
         {
             APF_HOST_RANGE("est_patch_topology_wait");
             ps = patches.get();
         }
-        // ---- nodal data per cell
-        const int nd = in.ndof;
-        DeviceBuffer<double> theta((long long)nd * ny, s), ucell((long long)nd * ny, s), ldel((long long)nd * ny, s),
-            ltil((long long)nd * ny, s);
+        // ---- nodal data per cell: lambda~ through the slab restriction; lambda_delta and u
+        // as the local functions of the cell's Y cell and X ancestor at its nodes
+        DeviceBuffer<double> theta((long long)nd * nc, s), ucell((long long)nd * nc, s), ldel((long long)nd * nc, s),
+            ltil((long long)nd * nc, s);
         const double* u = S.solution.get() + nl;
         {
+            const SystemInputs& li = sp.identity ? in : sl.in;
             APF_KERNEL("est_gather_nodal", s);
-            gather_nodal<<<nb((long long)ny * nd), 256, 0, s>>>(ny, nd, in.y_off.get(), in.y_dofs.get(), in.y_w.get(),
+            gather_nodal<<<nb((long long)nc * nd), 256, 0, s>>>(nc, nd, li.y_off.get(), li.y_dofs.get(), li.y_w.get(),
                                                                 lt.get(), nullptr, ltil.get());
         }
         {
-            APF_KERNEL("est_gather_nodal", s);
-            gather_nodal<<<nb((long long)ny * nd), 256, 0, s>>>(ny, nd, in.y_off.get(), in.y_dofs.get(), in.y_w.get(),
-                                                                S.solution.get(), nullptr, ldel.get());
+            DeviceBuffer<double> ly((long long)nd * ny, s);
+            {
+                APF_KERNEL("est_gather_nodal", s);
+                gather_nodal<<<nb((long long)ny * nd), 256, 0, s>>>(ny, nd, in.y_off.get(), in.y_dofs.get(),
+                                                                    in.y_w.get(), S.solution.get(), nullptr, ly.get());
+            }
+            if (sp.identity)
+                copy(s, nd * ny, ly.get(), ldel.get());
+            else
+            {
+                DeviceBuffer<int> d_src(0, s);
+                d_src.upload(sp.source.data(), sp.source.size());
+                nodal_transfer(s, in.p, nc, cgeo, d_src.get(), in.y_geo.get(), ly.get(), ldel.get());
+            }
         }
         {
-            APF_KERNEL("est_gather_nodal", s);
-            gather_nodal<<<nb((long long)ny * nd), 256, 0, s>>>(ny, nd, in.x_off.get(), in.x_dofs.get(), in.x_w.get(), u,
-                                                                nullptr, ucell.get());
+            const int nx = in.n_x_cells;
+            DeviceBuffer<double> ux((long long)nd * nx, s);
+            {
+                APF_KERNEL("est_gather_nodal", s);
+                gather_nodal<<<nb((long long)nx * nd), 256, 0, s>>>(nx, nd, in.x_off.get(), in.x_dofs.get(),
+                                                                    in.x_w.get(), u, nullptr, ux.get());
+            }
+            nodal_transfer(s, in.p, nc, cgeo, cx, in.x_geo.get(), ux.get(), ucell.get());
         }
-        axpby(s, nd * ny, 1.0, ltil.get(), 0.0, theta.get());
-        axpby(s, nd * ny, 1.0, ucell.get(), 1.0, theta.get());
+        axpby(s, nd * nc, 1.0, ltil.get(), 0.0, theta.get());
+        axpby(s, nd * nc, 1.0, ucell.get(), 1.0, theta.get());
         tot.n_slabs = ps.n_slabs;
         tot.n_patches = static_cast<int>(ps.patch_slab.size());
         tot.max_patch_cells = ps.max_cells;
@@ -1817,7 +2245,7 @@ namespace apf
         up(d_scell, ps.slab_cells);
         status.zero();
         const bool p2 = in.p == 2;
-        DeviceBuffer<double> sigma((p2 ? 135ll : 48ll) * ny, s);
+        DeviceBuffer<double> sigma((p2 ? 135ll : 48ll) * nc, s);
         sigma.zero();
         PatchArgs pa{};
         pa.n_patches = tot.n_patches;
@@ -1831,9 +2259,9 @@ namespace apf
         pa.topo_boundary = d_tbd.get();
         pa.slab_ptr = d_sptr.get();
         pa.slab_cells = d_scell.get();
-        pa.geo = in.y_geo.get();
-        pa.m = in.m_y.size() ? in.m_y.get() : nullptr;
-        pa.ell = in.ell.size() ? in.ell.get() : nullptr;
+        pa.geo = cgeo;
+        pa.m = cm;
+        pa.ell = cell;
         pa.theta = theta.get();
         pa.u = ucell.get();
         pa.sigma = sigma.get();
@@ -1988,32 +2416,58 @@ namespace apf
             throw Error(APF_ERR_NUMERIC, "estimator: singular patch system");
         if (hstat != 0)
             throw Error(APF_ERR_CAPACITY, "estimator: patch system larger than the kernel's buffer");
-        // ---- indicators
-        DeviceBuffer<double> f2(ny, s), d2(ny, s), r2(ny, s), e2(ny, s);
-        IndicatorArgs ia{ny, in.y_geo.get(), pa.m, pa.ell, theta.get(), ucell.get(), ldel.get(), ltil.get(), sigma.get(),
+        // ---- indicators per cell, then (slab cells) summed onto their Y cells
+        DeviceBuffer<double> f2(nc, s), d2(nc, s), r2(nc, s), e2(nc, s);
+        IndicatorArgs ia{nc, cgeo, pa.m, pa.ell, theta.get(), ucell.get(), ldel.get(), ltil.get(), sigma.get(),
                          f2.get(), d2.get(), r2.get(), e2.get()};
         if (p2)
         {
             {
                 APF_KERNEL("est_cell_indicators", s);
-                cell_indicators2<<<nb(ny, 128), 128, 0, s>>>(ia, tables2);
+                cell_indicators2<<<nb(nc, 128), 128, 0, s>>>(ia, tables2);
             }
             // ||lambda_delta - lambda~||^2 in the local A_y energy, eta = flux + that
-            DeviceBuffer<double> dl(nl, s);
-            copy(s, nl, S.solution.get(), dl.get());
-            axpby(s, nl, -1.0, lt.get(), 1.0, dl.get());
-            y_cell_energy(s, in, dl.get(), r2.get());
+            if (sp.identity)
+            {
+                DeviceBuffer<double> dl(nl, s);
+                copy(s, nl, S.solution.get(), dl.get());
+                axpby(s, nl, -1.0, lt.get(), 1.0, dl.get());
+                y_cell_energy(s, in, dl.get(), r2.get());
+            }
+            else
+            {
+                DeviceBuffer<double> dl((long long)nd * nc, s);
+                copy(s, nd * nc, ldel.get(), dl.get());
+                axpby(s, nd * nc, -1.0, ltil.get(), 1.0, dl.get());
+                nodal_energy(s, in.p, nc, cgeo, cm, dl.get(), r2.get());
+            }
             {
                 APF_KERNEL("est_eta", s);
-                add_kernel<<<nb(ny), 256, 0, s>>>(ny, f2.get(), r2.get(), e2.get());
+                add_kernel<<<nb(nc), 256, 0, s>>>(nc, f2.get(), r2.get(), e2.get());
             }
         }
         else
         {
             APF_KERNEL("est_cell_indicators", s);
-            cell_indicators<<<nb(ny, 128), 128, 0, s>>>(ia);
+            cell_indicators<<<nb(nc, 128), 128, 0, s>>>(ia);
         }
         APF_CUDA(cudaGetLastError());
+        if (!sp.identity)
+        {
+            DeviceBuffer<double> tmp(nc, s);
+            for (DeviceBuffer<double>* a : {&f2, &d2, &r2, &e2})
+            {
+                copy(s, nc, a->get(), tmp.get());
+                a->allocate(ny, s);
+                if (ny)
+                {
+                    APF_KERNEL("est_reduce_to_source", s);
+                    reduce_to_source_kernel<<<nb(ny), 256, 0, s>>>(ny, sl.src_ptr.get(), sl.src_list.get(), tmp.get(),
+                                                                   a->get());
+                }
+            }
+            APF_CUDA(cudaGetLastError());
+        }
         tot.flux = device_sum(s, ny, f2.get());
         tot.div = device_sum(s, ny, d2.get());
         tot.recon = device_sum(s, ny, r2.get());

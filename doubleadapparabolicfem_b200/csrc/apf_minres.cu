@@ -441,6 +441,8 @@ namespace apf
             fill(s, n, 0.0, x);
             sum.converged = true;
             sum.true_residual = 0.0;
+            if (opt.parts) // x = 0 solves every part exactly
+                sum.part_residuals.assign(static_cast<std::size_t>(opt.parts->n_parts), 0.0);
             return sum;
         }
         DeviceBuffer<double> seg_tmp(opt.parts ? 2 * std::max(1, opt.parts->n_parts) : 1, s);

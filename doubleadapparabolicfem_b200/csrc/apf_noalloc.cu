@@ -13,7 +13,9 @@
 // blocks, i.e. kMaxRows rows.  Larger matrices are rejected with APF_ERR_CAPACITY.
 // Each call writes every partial slot it later reads, so nothing has to be cleared between
 // calls; calls whose work overlaps on the GPU (different streams, no ordering) race on the
-// shared array and must not be issued.
+// shared array and must not be issued.  The first call on a device looks the array up and
+// loads this file's kernels (which may take device memory for their code); make it before
+// any stream capture, and before the point where nothing may be allocated any more.
 #include <mutex>
 
 #include "apf_internal.hpp"
@@ -29,9 +31,29 @@ namespace
     // [2 kMaxBlocks, 2 kMaxBlocks + 2): absolute and relative residual of the last call
     static __device__ __align__(256) double g_residual_scratch[2 * kMaxBlocks + 2];
 
-    // Device address of g_residual_scratch, looked up once per device.
+    template<int G>
+    __global__ void residual_partials(int rows, const int* __restrict__ rp, const int* __restrict__ ci,
+                                      const double* __restrict__ va, const double* __restrict__ x,
+                                      const double* __restrict__ b, double* scratch);
+    __global__ void residual_finish(int nblocks, double* scratch);
+
+    // Device address of g_residual_scratch, looked up once per device.  The same one-time
+    // set-up also loads the five kernels of this file onto the device: under CUDA's lazy
+    // module loading a kernel's code is otherwise loaded (and device memory taken for it) at
+    // its first launch, so a later call that picks another lanes-per-row variant could still
+    // allocate.  After the first call on a device nothing here allocates.
     std::mutex g_setup_mutex;
     double* g_scratch_addr[64] = {};
+
+    template<class K>
+    void force_load(K kernel)
+    {
+        cudaFuncAttributes attr{};
+        const cudaError_t e = cudaFuncGetAttributes(&attr, kernel);
+        if (e != cudaSuccess)
+            throw apf::Error(APF_ERR_CUDA, std::string("cudaFuncGetAttributes(residual kernel): ") +
+                                               cudaGetErrorString(e));
+    }
 
     double* scratch_address(int device)
     {
@@ -45,6 +67,11 @@ namespace
             if (e != cudaSuccess || p == nullptr)
                 throw apf::Error(APF_ERR_CUDA, std::string("cudaGetSymbolAddress(residual scratch): ") +
                                                    cudaGetErrorString(e));
+            force_load(residual_partials<4>);
+            force_load(residual_partials<8>);
+            force_load(residual_partials<16>);
+            force_load(residual_partials<32>);
+            force_load(residual_finish);
             g_scratch_addr[device] = static_cast<double*>(p);
         }
         return g_scratch_addr[device];
@@ -53,11 +80,9 @@ namespace
     // One block per kRowsPerBlock rows; G lanes per row (same row summation as the
     // library's residual kernel), block-level partial sums written to the scratch.
     template<int G>
-    __global__ void __launch_bounds__(kThreads) residual_partials(int rows, const int* __restrict__ rp,
-                                                                  const int* __restrict__ ci,
-                                                                  const double* __restrict__ va,
-                                                                  const double* __restrict__ x,
-                                                                  const double* __restrict__ b, double* scratch)
+    __global__ void residual_partials(int rows, const int* __restrict__ rp, const int* __restrict__ ci,
+                                      const double* __restrict__ va, const double* __restrict__ x,
+                                      const double* __restrict__ b, double* scratch)
     {
         constexpr int RPW = 32 / G;
         __shared__ double s_rr[kThreads / 32], s_bb[kThreads / 32];

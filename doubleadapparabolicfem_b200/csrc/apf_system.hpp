@@ -75,6 +75,14 @@ namespace apf
     // per Y cell: v_K^T A_y,K v_K, the local A_y energy (int_K grad_x v . M grad_x v) of a
     // Y-space true-DOF vector v (device)
     void y_cell_energy(cudaStream_t s, const SystemInputs& in, const double* v, double* out);
+    // dst[c][k] (n cells, ndof nodal values each) = the local function src[src_index[c]] of
+    // a source prism (geometry src_geo) evaluated at the nodes of prism c (geometry dst_geo),
+    // which lies inside it; src_index NULL = identity.  Exact for nested prisms.
+    void nodal_transfer(cudaStream_t s, int p, int n, const double* dst_geo, const int* src_index, const double* src_geo,
+                        const double* src, double* dst);
+    // out[c] = v_c^T A_c v_c: the local A_y energy (int grad_x v . M grad_x v) of nodal values
+    // v_c on prism c (m: 3 per cell or NULL = identity)
+    void nodal_energy(cudaStream_t s, int p, int n, const double* geo, const double* m, const double* v, double* out);
     // X-marking indicators from lambda_delta (Y true DOFs) and u_delta (X true DOFs), all
     // device arrays: per Y cell lambda energy, per X cell its aggregate, the initial-trace
     // mismatch (0 off the t = 0 layer) and their sum

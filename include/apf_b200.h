@@ -389,8 +389,11 @@ int apf_write_x_indicator_components_binary(apf_ctx* ctx, const char* path, int3
  * pointers, on the context's stream.  Allocates no device memory: its scratch is one
  * fixed 64 KiB device array shared by all calls on a device, so at most 16,777,216 rows
  * (larger K: APF_ERR_CAPACITY).  The first call on a device looks the array's address up
- * (make it before any stream capture); calls whose GPU work overlaps race on the shared
- * array.  Results are written to the host doubles given (either may be NULL). */
+ * and loads the entry point's kernels onto the device (under lazy module loading their code
+ * would otherwise be loaded, taking device memory, at first launch): only that first call
+ * may allocate, so make it at set-up, before any stream capture.  Calls whose GPU work
+ * overlaps race on the shared array.  Results are written to the host doubles given (either
+ * may be NULL). */
 int apf_true_residual_noalloc(apf_ctx* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_idx,
                               const double* values, const double* x, const double* b, double* absolute_residual,
                               double* relative_residual);

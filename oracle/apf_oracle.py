@@ -27,7 +27,14 @@ Restated reference code (paths relative to the reference project root):
 * graph-norm preconditioner block — ``src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:22-65``
   and ``src/linear_algebra/preconditioners/schur_approximations.hpp:79-287``;
 * full saddle matrix of the direct-solver path — ``src/finite_element/assembly/main_system/two_pass_full_saddle_2d.hpp:468``
-  (structural pattern, numeric fill, ``prune(1.0, zero_tol)``).
+  (structural pattern, numeric fill, ``prune(1.0, zero_tol)``);
+* time-slab space and slab reconstruction lambda~ on adaptive meshes —
+  ``src/finite_element/time_slabs/time_slab_builder.hpp:53-215`` (slab times = distinct
+  Y-cell endpoints, every Y cell cut into one slab cell per slab it spans),
+  ``time_slab.hpp:185-242`` (a slab cell is its source cell over the slab interval),
+  ``time_slab_reconstruction_operator.hpp:686-830`` (per slab, A_slab lambda~ = rhs with the
+  main-system forms: the Y-norm stiffness and l - d_t u - M grad u tested against the slab
+  space).
 """
 from __future__ import annotations
 
@@ -398,31 +405,56 @@ def assemble_graph_norm(prob: MainProblem, A_y, C_signed, zero_tol=1e-15, diag_t
 
 
 def _hhat_from_blocks(A_y, C_signed, A_x, B_dt, diag_tol, n_u):
+    """Hhat in the reference's own summation order (schur_approximations.hpp:107-200 and
+    sparse_matrix_ops.hpp:286-316, zero_tol 0): hpar = setFromTriplets of -C (C's stored
+    entries, column-major) followed by (1/A_cc * B_ic) * B_jc for every lambda column c in
+    ascending order (its rows in storage order, i outer, j inner), each stored entry of hpar
+    the sum of its triplets in that order; then Hhat = hpar's nonzero entries plus A_x's.
+    The order matters on adaptive meshes, where Schur terms cancel exactly."""
     d = A_y.diagonal()
     if np.any(~(d > diag_tol)):
         raise RuntimeError("diagonal_schur_approximation: A_y diagonal must be positive.")
+    inv = 1.0 / d
     B_dt = B_dt.tocsc()
     B_dt.sort_indices()
-    # explicit triplets: every (i,j) pair within each B_dt column, scaled by 1/A_y[c,c];
-    # then -C_signed and A_x; summed like setFromTriplets (explicit zeros kept)
-    rows, cols, vals = [], [], []
-    lens = np.diff(B_dt.indptr)
-    for L in np.unique(lens):
-        if L == 0:
-            continue
-        cs = np.nonzero(lens == L)[0]
-        idx = B_dt.indptr[cs][:, None] + np.arange(L)[None, :]
-        r = B_dt.indices[idx]
-        v = B_dt.data[idx] / d[cs][:, None]
-        vv = B_dt.data[idx]
-        rr, cc = np.broadcast_arrays(r[:, :, None], r[:, None, :])
-        val = v[:, :, None] * vv[:, None, :]
-        keep = np.abs(val) > 0.0
-        rows.append(rr[keep]); cols.append(cc[keep]); vals.append(val[keep])
-    Cc = C_signed.tocoo()
+    Cc = C_signed.tocsc()
+    Cc.sort_indices()
+    # triplets in generation order
+    c_cols = np.repeat(np.arange(Cc.shape[1]), np.diff(Cc.indptr))
+    keep = Cc.data != 0.0
+    rows = [Cc.indices[keep]]
+    cols = [c_cols[keep]]
+    vals = [-Cc.data[keep]]
+    bl = np.diff(B_dt.indptr)
+    for c in np.nonzero(bl)[0]:
+        r = B_dt.indices[B_dt.indptr[c]:B_dt.indptr[c + 1]]
+        v = B_dt.data[B_dt.indptr[c]:B_dt.indptr[c + 1]]
+        nz = v != 0.0
+        r, v = r[nz], v[nz]
+        contrib = (inv[c] * v)[:, None] * v[None, :]
+        rr, cc = np.broadcast_arrays(r[:, None], r[None, :])
+        k = np.abs(contrib) > 0.0
+        rows.append(rr[k]); cols.append(cc[k]); vals.append(contrib[k])
+    rows = np.concatenate(rows); cols = np.concatenate(cols); vals = np.concatenate(vals)
+    # per entry, the triplets' sum in generation order (stable sort, sequential sums)
+    order = np.lexsort((cols, rows)) if len(rows) else np.zeros(0, dtype=np.int64)
+    key = rows[order].astype(np.int64) * n_u + cols[order]
+    starts = np.concatenate([[0], np.nonzero(np.diff(key))[0] + 1]) if len(key) else np.zeros(0, dtype=np.int64)
+    sums = np.empty(len(starts))
+    sv = vals[order]
+    bounds = np.append(starts, len(sv))
+    for g in range(len(starts)):
+        acc = 0.0
+        for t in range(bounds[g], bounds[g + 1]):
+            acc += sv[t]
+        sums[g] = acc
+    hk = key[starts] if len(key) else key
+    hpar_keep = sums != 0.0
     Ax = A_x.tocoo()
-    rows += [Cc.row, Ax.row]; cols += [Cc.col, Ax.col]; vals += [-Cc.data, Ax.data]
-    H = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n_u, n_u))
+    ax_keep = Ax.data != 0.0
+    H = sp.csc_matrix((np.concatenate([sums[hpar_keep], Ax.data[ax_keep]]),
+                       (np.concatenate([hk[hpar_keep] // n_u, Ax.row[ax_keep]]),
+                        np.concatenate([hk[hpar_keep] % n_u, Ax.col[ax_keep]]))), shape=(n_u, n_u))
     return dict(Hhat=H, B_dt=B_dt, A_x=A_x)
 
 
@@ -532,3 +564,81 @@ def load_problem(d, p) -> MainProblem:
     return MainProblem(p=p, y_geom=np.load(f"{d}/y_geometry.npy"), x_geom=np.load(f"{d}/x_geometry.npy"),
                        y_to_x=np.load(f"{d}/y_to_x_cell.npy"), y_restr=restr("y_restriction"),
                        x_restr=restr("x_restriction"), n_lambda=n_lambda, n_u=n_u)
+
+
+# ----------------------------------------------------------------------------
+# time-slab space and the slab reconstruction (adaptive meshes)
+# ----------------------------------------------------------------------------
+_NODE_VERTICES = {1: [(0, 0), (1, 1), (2, 2)],
+                  2: [(0, 0), (0, 1), (1, 1), (0, 2), (1, 2), (2, 2)]}
+
+
+def slab_space(p: int, y_geom, y_vertex_ids, y_restr: Restriction):
+    """The reference's time-slab space of a Y space (time_slab_builder.hpp:53-215).
+
+    Slab times: the sorted distinct time endpoints of the Y cells; slab cells: every Y cell
+    once per slab it spans, slabs in time order and each slab's cells in Y order.  The slab
+    space is P_p x P_p per slab, continuous in space inside a slab and broken between slabs;
+    spatial nodes whose Y restriction rows are all empty are Dirichlet nodes.  Returns
+    (source Y cell, slab id, slab geometry, Restriction, number of slab DOFs); the DOF
+    numbering is this function's own (first appearance per slab)."""
+    ns, nt = len(_NODE_VERTICES[p]), p + 1
+    nd = ns * nt
+    ny = y_geom.shape[0]
+    times = np.unique(y_geom[:, 6:8].ravel())
+    kb = np.searchsorted(times, y_geom[:, 6])
+    ke = np.searchsorted(times, y_geom[:, 7])
+    src, slab = [], []
+    for k in range(len(times) - 1):
+        cells = np.nonzero((kb <= k) & (k < ke))[0]
+        src.extend(cells.tolist())
+        slab.extend([k] * len(cells))
+    src = np.asarray(src, dtype=np.int64)
+    slab = np.asarray(slab, dtype=np.int64)
+    off = y_restr.offsets
+    empty = (off[1:] == off[:-1]).reshape(ny, ns, nt).all(axis=2)
+    dof = -np.ones((len(src), nd), dtype=np.int64)
+    base = 0
+    for k in range(len(times) - 1):
+        ids = {}
+        for i in np.nonzero(slab == k)[0]:
+            for s_, (va, vb) in enumerate(_NODE_VERTICES[p]):
+                if empty[src[i], s_]:
+                    continue
+                a, b = int(y_vertex_ids[src[i], va]), int(y_vertex_ids[src[i], vb])
+                key = (min(a, b), max(a, b))
+                j = ids.setdefault(key, len(ids))
+                dof[i, s_ * nt:(s_ + 1) * nt] = base + j * nt + np.arange(nt)
+        base += len(ids) * nt
+    flat = dof.ravel()
+    counts = (flat >= 0).astype(np.int64)
+    offsets = np.concatenate([[0], np.cumsum(counts)])
+    restr = Restriction(offsets, flat[flat >= 0], np.ones(int(counts.sum())), nd)
+    geom = y_geom[src].copy()
+    geom[:, 6] = times[slab]
+    geom[:, 7] = times[slab + 1]
+    return src, slab, geom, restr, base
+
+
+def slab_reconstruction(prob: MainProblem, y_vertex_ids, u, ell=None, zero_tol=1e-15):
+    """lambda~ on the slab space (time_slab_reconstruction_operator.hpp:686-830): the slab
+    forms are the main-system ones with the slab space as test space, so
+    A_slab lambda~ = f_slab - B_slab^T u, solved directly.  Returns (source, slab, slab
+    geometry, slab restriction, lambda~ as slab DOFs)."""
+    import scipy.sparse.linalg as spl
+    src, slab, geom, restr, n = slab_space(prob.p, prob.y_geom, y_vertex_ids, prob.y_restr)
+    sprob = MainProblem(p=prob.p, y_geom=geom, x_geom=prob.x_geom, y_to_x=np.asarray(prob.y_to_x)[src],
+                        y_restr=restr, x_restr=prob.x_restr, n_lambda=n, n_u=prob.n_u,
+                        m_cells=None if prob.m_cells is None else np.asarray(prob.m_cells)[src])
+    blocks = assemble_main_blocks(sprob, ell=ell, zero_tol=zero_tol)
+    lt = spl.spsolve(blocks["A_y"].tocsc(), blocks["f"] - blocks["B"].T @ u)
+    return src, slab, geom, restr, lt
+
+
+def nodal_values(restr: Restriction, v):
+    """[n_cells, ndof] local values of a true-DOF vector through a restriction."""
+    n = (len(restr.offsets) - 1) // restr.ndof
+    rows = np.repeat(np.arange(len(restr.offsets) - 1), np.diff(restr.offsets))
+    out = np.zeros(len(restr.offsets) - 1)
+    np.add.at(out, rows, restr.weights * v[restr.dofs])
+    return out.reshape(n, restr.ndof)

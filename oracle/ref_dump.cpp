@@ -23,7 +23,11 @@
 // usage: apf_ref_dump <dim:1|2> <p:1|2> <uniform_levels> <example> <outdir>
 //        apf_ref_dump bench <p:1|2> <uniform_levels> <example> <reps>
 
+#include <array>
+#include <cmath>
 #include <cstdio>
+#include <memory>
+#include <random>
 #include <cstdlib>
 #include <filesystem>
 #include <limits>
@@ -192,6 +196,43 @@ namespace
         throw std::runtime_error("uniform_isotropic_refine: no spatial shrink after 32 waves");
     }
 
+    // Adaptive-mesh options (environment, all optional):
+    //   APF_REF_X_POINTS="x,y,t;x,y,t"  X refined at these space-time points after the
+    //                                    uniform levels, APF_REF_X_ROUNDS times (default 1),
+    //                                    by the reference's refine_points_n_times
+    //                                    (algorithm/support/space_time_1d.hpp:67): hanging
+    //                                    nodes with weighted CellRestriction rows;
+    //   APF_REF_KAPPA="seed:lo:hi"       M(p) = kappa[K] I with kappa log-uniform in [lo, hi]
+    //                                    per active X cell K (the cell found by
+    //                                    x_space.find_active_cell(p), fespace.hpp:616);
+    //   APF_REF_Y_PASSES=n               n passes of the reference's inner loop before the
+    //                                    dump: estimate, Doerfler marking, then
+    //                                    refine_test_space_from_marked_source_cells
+    //                                    (time_slab_adaptive_loop.hpp:2147-2186), so Y is
+    //                                    finer than X.
+    std::vector<std::array<double, 3>> parse_points(const char* s)
+    {
+        std::vector<std::array<double, 3>> out;
+        std::string str(s);
+        std::size_t pos = 0;
+        while (pos < str.size())
+        {
+            std::size_t end = str.find(';', pos);
+            if (end == std::string::npos) end = str.size();
+            std::array<double, 3> p{};
+            if (std::sscanf(str.substr(pos, end - pos).c_str(), "%lf,%lf,%lf", &p[0], &p[1], &p[2]) == 3)
+                out.push_back(p);
+            pos = end + 1;
+        }
+        return out;
+    }
+
+    int env_int(const char* name, int dflt)
+    {
+        const char* v = std::getenv(name);
+        return v != nullptr ? std::atoi(v) : dflt;
+    }
+
     // Times the reference's own CPU assembly path (main blocks + graph-norm block)
     // on the uniform mesh of outer level `levels`; prints one JSON line.
     template<int P>
@@ -273,7 +314,53 @@ namespace
         adaptive_algorithm::examples::initialize_spaces_from_example(x_space, y_space, example);
         for (int k = 0; k < levels; ++k)
             uniform_isotropic_refine(x_space);
+        if (const char* pts = std::getenv("APF_REF_X_POINTS"))
+        {
+            std::vector<typename XSpace::SpaceTimePoint> points;
+            for (const auto& p : parse_points(pts))
+                points.push_back(typename XSpace::SpaceTimePoint{p[0], p[1], p[2]});
+            adaptive_algorithm::support::refine_points_n_times(x_space, points, env_int("APF_REF_X_ROUNDS", 1));
+        }
         y_space.initialize(x_space.active_cells());
+
+        std::filesystem::create_directories(dir);
+        if (const char* ks = std::getenv("APF_REF_KAPPA"))
+        {
+            unsigned long long seed = 0;
+            double lo = 1.0, hi = 1.0;
+            std::sscanf(ks, "%llu:%lf:%lf", &seed, &lo, &hi);
+            std::mt19937_64 rng(seed);
+            std::uniform_real_distribution<double> uni(std::log(lo), std::log(hi));
+            auto kappa = std::make_shared<std::vector<double>>(static_cast<std::size_t>(mesh.n_cells()), 0.0);
+            std::vector<double> kx;
+            for (const int c : x_space.active_cells())
+            {
+                (*kappa)[static_cast<std::size_t>(c)] = std::exp(uni(rng));
+                kx.push_back((*kappa)[static_cast<std::size_t>(c)]);
+            }
+            apf_oracle::write_npy(dir + "/kappa_x.npy", kx);
+            // the space's point-location index is built lazily on first use; build it here,
+            // before the reference's OpenMP loops call M concurrently
+            (void)x_space.find_active_cell(typename XSpace::SpaceTimePoint{0.5, 0.25, 0.5});
+            const XSpace* xs = &x_space;
+            example.problem.M = [xs, kappa](const adaptive_algorithm::examples::SpaceTime2DPoint& p) {
+                const int c = xs->find_active_cell(p);
+                const double k = (*kappa).at(static_cast<std::size_t>(c));
+                return finite_element::coefficients::DiffusionTensor<2>{{{k, 0.0}, {0.0, k}}};
+            };
+        }
+        for (int pass = 0; pass < env_int("APF_REF_Y_PASSES", 0); ++pass)
+        {
+            typename Backend::Solver solver;
+            la::concepts::SolverOptions opts;
+            finite_element::time_slabs::AdaptiveTestSpaceIterationParameters<Backend, XSpace, YSpace> params;
+            const auto state = finite_element::time_slabs::compute_adaptive_test_space_iteration<QSpace, QTime, Backend>(
+                y_space, x_space, example.problem, solver, opts, params);
+            std::cerr << "y pass " << pass << ": marked " << state.marked_source_cells.size() << " of "
+                      << y_space.active_cells().size() << " Y cells\n";
+            finite_element::time_slabs::refine_test_space_from_marked_source_cells(y_space, x_space,
+                                                                                   state.marked_source_cells);
+        }
 
         const auto& y_cells = y_space.active_cells();
         const auto& x_cells = x_space.active_cells();
@@ -355,6 +442,65 @@ namespace
                 y_space, x_space, example.problem, solver, opts, params);
             dump_vec(dir, "lambda_delta", state.lambda_delta.true_coefficients());
             dump_vec(dir, "u_delta", state.u_delta.true_coefficients());
+            if (state.slab_reconstruction.has_value())
+            {
+                // the reference's time-slab space (time_slab_builder.hpp:53-215) and its
+                // reconstruction lambda~: per slab cell (slabs in time order, cells in each
+                // slab's order) the slab, the source Y cell, the slab cell's geometry and
+                // spatial vertex ids of the slab mesh, its restriction in the slab space (true
+                // DOFs numbered slab after slab) and lambda~ at the 3 vertices x {t0, t1}
+                const auto& ss = state.slab_reconstruction->slab_space_ref();
+                const auto& lt = state.slab_reconstruction->reconstructed_function();
+                std::vector<int> s_slab, s_source, s_vids, r_off{0}, r_dofs, s_dof_base{0};
+                std::vector<double> s_geo, s_lt, r_w;
+                for (int k = 0; k < ss.n_slabs(); ++k)
+                {
+                    const auto& slab = ss.slab(k);
+                    const auto& smesh = slab.mesh_ref();
+                    const int base = s_dof_base.back();
+                    for (const int c : slab.active_cells())
+                    {
+                        s_slab.push_back(k);
+                        s_source.push_back(slab.source_cell_id(c));
+                        const auto& cell = smesh.cell(c);
+                        for (int v = 0; v < 3; ++v)
+                        {
+                            const auto& xy = smesh.spatial_vertices()[cell.spatial_vertex_ids[v]];
+                            s_geo.push_back(xy[0]);
+                            s_geo.push_back(xy[1]);
+                            s_vids.push_back(cell.spatial_vertex_ids[v]);
+                        }
+                        s_geo.push_back(slab.t_begin());
+                        s_geo.push_back(slab.t_end());
+                        for (int v = 0; v < 3; ++v)
+                        {
+                            const auto& xy = smesh.spatial_vertices()[cell.spatial_vertex_ids[v]];
+                            for (const double t : {slab.t_begin(), slab.t_end()})
+                                s_lt.push_back(lt.value_on_cell(k, c, typename XSpace::SpaceTimePoint{xy[0], xy[1], t}));
+                        }
+                        const auto r = finite_element::assembly::build_cell_restriction(slab.fespace_ref(), c);
+                        for (int i = 0; i < r.size(); ++i)
+                        {
+                            for (const auto& e : r[i])
+                            {
+                                r_dofs.push_back(base + e.true_dof);
+                                r_w.push_back(e.weight);
+                            }
+                            r_off.push_back(static_cast<int>(r_dofs.size()));
+                        }
+                    }
+                    s_dof_base.push_back(base + slab.fespace_ref().dof_handler_ref().n_true_dofs());
+                }
+                apf_oracle::write_npy(dir + "/slab_of_cell.npy", s_slab);
+                apf_oracle::write_npy(dir + "/slab_source_cell.npy", s_source);
+                apf_oracle::write_npy(dir + "/slab_vertex_ids.npy", s_vids.data(), {s_slab.size(), 3u});
+                apf_oracle::write_npy(dir + "/slab_geometry.npy", s_geo.data(), {s_slab.size(), 8u});
+                apf_oracle::write_npy(dir + "/slab_lambda_tilde.npy", s_lt.data(), {s_slab.size(), 6u});
+                apf_oracle::write_npy(dir + "/slab_restriction_offsets.npy", r_off);
+                apf_oracle::write_npy(dir + "/slab_restriction_dofs.npy", r_dofs);
+                apf_oracle::write_npy(dir + "/slab_restriction_weights.npy", r_w);
+                apf_oracle::write_npy(dir + "/slab_dof_base.npy", s_dof_base);
+            }
             auto dump_map = [&](const std::string& name, const auto& m) {
                 std::vector<int> ids;
                 std::vector<double> vals;

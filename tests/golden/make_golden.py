@@ -9,7 +9,7 @@ artifacts of the estimate (cellwise_error.bin, cellwise_error_components.bin, as
 6-significant-digit estimator values) of the reference's published paper data
 (algorithm_data_plot/{1d,2d}/*.csv) into paper_uniform_rows.json.
 
-usage: python tests/golden/make_golden.py [REFERENCE_ROOT [CASE ...]]
+usage: python tests/golden/make_golden.py REFERENCE_ROOT [CASE ...]
 """
 from __future__ import annotations
 
@@ -28,7 +28,7 @@ REPO = os.path.abspath(os.path.join(HERE, "..", ".."))
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "apf_ref_dump")
 
 CASES = [
-    # (name, dim, p, outer level, example)
+    # (name, dim, p, outer level, example[, environment of the adaptive mode])
     ("p1_l1_smooth", 2, 1, 1, "smooth_initial"),
     ("p1_l2_smooth", 2, 1, 2, "smooth_initial"),
     ("p2_l1_smooth", 2, 2, 1, "smooth_initial"),
@@ -38,11 +38,25 @@ CASES = [
     ("d1_l2_smooth", 1, 1, 2, "smooth_initial"),
     ("d1_l2_nonmatching", 1, 1, 2, "non_matching_initial"),
     ("d1_l5_smooth", 1, 1, 5, "smooth_initial"),
+    # adaptive meshes: X refined locally at seeded space-time points by the reference's
+    # refine_points_n_times (hanging nodes: weighted restriction rows), Y refined beyond X by
+    # one pass of the reference's inner loop (marking + refine_test_space_from_marked_source_cells),
+    # optionally a diffusivity kappa per X cell log-uniform in [lo, hi]
+    ("p1_adapt_smooth", 2, 1, 2, "smooth_initial",
+     {"APF_REF_X_POINTS": "0.3,0.3,0.3;0.71,0.62,0.8", "APF_REF_X_ROUNDS": "3", "APF_REF_Y_PASSES": "1"}),
+    ("p1_adapt_kappa", 2, 1, 2, "smooth_initial",
+     {"APF_REF_X_POINTS": "0.3,0.3,0.3;0.71,0.62,0.8", "APF_REF_X_ROUNDS": "3", "APF_REF_Y_PASSES": "1",
+      "APF_REF_KAPPA": "7:0.01:100"}),
+    ("p1_adapt_nonmatching", 2, 1, 1, "non_matching_initial",
+     {"APF_REF_X_POINTS": "0.2,0.45,0.1", "APF_REF_X_ROUNDS": "4", "APF_REF_Y_PASSES": "1"}),
+    ("p1_kappa_uniform", 2, 1, 2, "smooth_initial", {"APF_REF_KAPPA": "3:0.1:10"}),
+    ("p2_adapt_smooth", 2, 2, 1, "smooth_initial",
+     {"APF_REF_X_POINTS": "0.3,0.3,0.3", "APF_REF_X_ROUNDS": "2", "APF_REF_Y_PASSES": "1"}),
 ]
 
 
-def dump_case(dim, p, level, example, outdir):
-    env = dict(os.environ, APF_REF_ESTIMATE="1")
+def dump_case(dim, p, level, example, outdir, extra_env=None):
+    env = dict(os.environ, APF_REF_ESTIMATE="1", **(extra_env or {}))
     subprocess.run([REF_BIN, str(dim), str(p), str(level), example, outdir], check=True, env=env)
     arrays = {}
     for f in sorted(glob.glob(os.path.join(outdir, "*.npy"))):
@@ -54,14 +68,19 @@ def dump_case(dim, p, level, example, outdir):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("APF_REFERENCE_ROOT")
+    if not ref_root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [CASE ...] (or set APF_REFERENCE_ROOT)")
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), f"REF={ref_root}"], check=True)
     only = set(sys.argv[2:])
-    for name, dim, p, level, example in CASES:
+    for name, dim, p, level, example, *extra in CASES:
         if only and name not in only:
             continue
+        env = extra[0] if extra else {}
         with tempfile.TemporaryDirectory() as tmp:
-            arrays = dump_case(dim, p, level, example, tmp)
+            arrays = dump_case(dim, p, level, example, tmp, env)
+        for key, value in env.items():
+            arrays["meta_" + key.lower()] = np.array([value])
         arrays["meta_dim"] = np.array([dim])
         arrays["meta_p"] = np.array([p])
         arrays["meta_level"] = np.array([level])

@@ -1,0 +1,147 @@
+"""GPU parity on adaptive meshes and with a diffusivity per cell, against the reference's
+own output on the same meshes.
+
+The fixtures (tests/golden/make_golden.py) come from the reference's templates: X refined
+locally at seeded space-time points by refine_points_n_times (hanging nodes, so restriction
+rows carry several weighted entries), then one pass of the reference's inner loop (its
+marking and refine_test_space_from_marked_source_cells), so Y is finer than X, Y cells span
+several time slabs and the slab reconstruction lambda~ differs from lambda_delta; p1_adapt_kappa
+and p1_kappa_uniform add M = kappa I with kappa log-uniform per X cell.
+
+Bars: block patterns bit-exact and values <= 1e-12 of the largest entry (Hhat: the significant
+pattern; Schur-sum cancellation residues below 1e-13 may differ); per-cell flux^2, div^2,
+recon^2 and eta^2 within 1e-9 of the largest cell's eta^2, totals within 1e-10 (recon^2 1e-8:
+it is a squared difference of two solves), after MINRES to a true relative residual of 1e-13
+(the reference solves directly).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import (ADAPTIVE_CASES, GOLDEN, HHAT_RESIDUE, KAPPA_CASES, assert_same_sparse, load_golden,
+                      to_product_problem)
+
+pytestmark = pytest.mark.gpu
+
+ESTIMATE_CASES = ADAPTIVE_CASES + ["p1_kappa_uniform"]
+
+
+def _assemble(ctx, name):
+    from doubleadapparabolicfem_b200.assembly import assemble_main_system_blocks
+    prob, ref, example = load_golden(name)
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    product = to_product_problem(prob, example)
+    product.y_vertex_ids = z["y_vertex_ids"]
+    blocks = assemble_main_system_blocks(product, ctx=ctx)
+    return blocks, prob, ref, z
+
+
+@pytest.mark.parametrize("name", ESTIMATE_CASES)
+def test_adaptive_blocks_match_reference(gpu_ctx, name):
+    blocks, prob, ref, z = _assemble(gpu_ctx, name)
+    assert_same_sparse(ref["A_y"], blocks.A_y(), 1e-12, "A_y")
+    assert_same_sparse(ref["B"], blocks.lower_left_B(), 1e-12, "B")
+    assert_same_sparse(ref["C_signed"], blocks.C_signed(), 1e-12, "C_signed")
+    assert np.abs(blocks.f() - ref["f"]).max() <= 1e-12 * max(1.0, np.abs(ref["f"]).max())
+    assert np.abs(blocks.g() - ref["g"]).max() <= 1e-12 * np.abs(ref["g"]).max()
+    H = blocks.assemble_parabolic_graph_norm_approximation()
+    residue = HHAT_RESIDUE if name in ADAPTIVE_CASES else 0.0
+    assert_same_sparse(ref["Hhat"], H, 1e-12, "Hhat", residue=residue)
+
+
+@pytest.mark.parametrize("name", ESTIMATE_CASES)
+def test_adaptive_two_pass_full_saddle_matches_reference(gpu_ctx, name):
+    """The direct-solver path's full K on the same meshes (the reference's two-pass output with
+    the example's coefficients)."""
+    from doubleadapparabolicfem_b200.assembly import assemble_main_full_saddle_two_pass
+    prob, ref, example = load_golden(name)
+    two = assemble_main_full_saddle_two_pass(to_product_problem(prob, example), ctx=gpu_ctx)
+    assert_same_sparse(ref["K2p"], two.matrix, 1e-12, "K2p")
+    assert np.abs(two.rhs - ref["K2p_rhs"]).max() <= 1e-12 * np.abs(ref["K2p_rhs"]).max()
+    two.close()
+
+
+@pytest.mark.parametrize("name", ESTIMATE_CASES)
+def test_adaptive_indicators_match_reference(gpu_ctx, name):
+    from doubleadapparabolicfem_b200.estimator import estimate, x_marking_indicator_components
+    from doubleadapparabolicfem_b200.solver import SolverOptions, solve_saddle_system_with_preconditioner
+    blocks, prob, ref, z = _assemble(gpu_ctx, name)
+    blocks.assemble_parabolic_graph_norm_approximation()
+    _, diag = solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=1e-13), copy_out=False)
+    assert diag["converged"] == 1
+    cells, totals = estimate(blocks)
+    eta_ref = z["est_eta"]
+    scale = np.abs(eta_ref).max()
+    for key, ref_key in (("flux", "est_flux"), ("divergence", "est_div"), ("reconstruction", "est_recon"),
+                         ("eta", "est_eta")):
+        err = np.abs(cells[key] - z[ref_key]).max()
+        assert err <= 1e-9 * scale, (key, err / scale)
+    assert abs(totals["flux_squared"] - z["est_flux"].sum()) <= 1e-10 * z["est_flux"].sum()
+    assert abs(totals["eta_squared"] - eta_ref.sum()) <= 1e-10 * eta_ref.sum()
+    recon_ref = z["est_recon"].sum()
+    if name in ADAPTIVE_CASES:
+        # lambda~ genuinely differs from lambda_delta here: the reconstruction term is pinned
+        assert recon_ref > 1e-8 * eta_ref.sum()
+        assert abs(totals["reconstruction_squared"] - recon_ref) <= 1e-8 * recon_ref
+        assert totals["n_slabs"] == int(z["slab_of_cell"].max()) + 1
+    else:
+        assert totals["reconstruction_squared"] <= 1e-12 * eta_ref.sum()
+    # the adaptive driver's X-marking indicators on the same solution
+    xi, _ = x_marking_indicator_components(blocks)
+    xs = np.abs(z["xind_eta_by_x"]).max()
+    for key, ref_key in (("lambda_y_squared_by_y_cell", "xind_lambda_by_y"),
+                         ("lambda_y_squared_by_x_cell", "xind_lambda_by_x"),
+                         ("initial_trace_squared_by_x_cell", "xind_trace_by_x"),
+                         ("eta_squared_by_x_cell", "xind_eta_by_x")):
+        assert np.abs(xi[key] - z[ref_key]).max() <= 1e-9 * xs, key
+
+
+def test_adaptive_fp32_refined_patches_close_to_fp64(gpu_ctx):
+    """The precision form on an adaptive mesh: FP32 patch factorisation + one FP64 refinement
+    step against the FP64 path on the same solution (bound 1e-10 of the largest cell)."""
+    from doubleadapparabolicfem_b200.estimator import estimate
+    from doubleadapparabolicfem_b200.solver import SolverOptions, solve_saddle_system_with_preconditioner
+    blocks, prob, ref, z = _assemble(gpu_ctx, "p1_adapt_kappa")
+    blocks.assemble_parabolic_graph_norm_approximation()
+    solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=1e-12), copy_out=False)
+    c64, _ = estimate(blocks)
+    c32, _ = estimate(blocks, patch_precision="fp32_refined")
+    scale = np.abs(c64["eta"]).max()
+    for key in ("flux", "divergence", "eta"):
+        assert np.abs(c64[key] - c32[key]).max() <= 1e-10 * scale, key
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_per_cell_spd_m_matches_oracle(gpu_ctx, adaptive):
+    """Block assembly and Hhat with a random SPD M per Y cell (anisotropic, constant on each X
+    cell) against the oracle restatement, on a uniform and on an adaptive mesh."""
+    import apf_oracle as O
+    from doubleadapparabolicfem_b200.assembly import assemble_main_system_blocks
+    name = "p1_adapt_smooth" if adaptive else "p1_l2_smooth"
+    prob, ref, example = load_golden(name)
+    rng = np.random.default_rng(11)
+    nx = prob.x_geom.shape[0]
+    a = np.exp(rng.uniform(np.log(0.01), np.log(100.0), nx))
+    b = np.exp(rng.uniform(np.log(0.01), np.log(100.0), nx))
+    th = rng.uniform(0.0, np.pi, nx)
+    c, s = np.cos(th), np.sin(th)
+    mx = np.stack([a * c * c + b * s * s, (a - b) * c * s, a * s * s + b * c * c], axis=1)
+    prob.m_cells = mx[prob.y_to_x]
+    u0 = O.sin_initial if example == "smooth_initial" else O.one_initial
+    want = O.assemble_main_blocks(prob, u0=u0)
+    gn = O.assemble_graph_norm(prob, want["A_y"], want["C_signed"])
+    blocks = assemble_main_system_blocks(to_product_problem(prob, example), ctx=gpu_ctx)
+    assert_same_sparse(want["A_y"], blocks.A_y(), 1e-12, "A_y")
+    assert_same_sparse(want["B"], blocks.lower_left_B(), 1e-12, "B")
+    assert_same_sparse(want["C_signed"], blocks.C_signed(), 1e-12, "C_signed")
+    H = blocks.assemble_parabolic_graph_norm_approximation()
+    assert_same_sparse(gn["Hhat"], H, 1e-12, "Hhat", residue=HHAT_RESIDUE if adaptive else 0.0)
+
+
+@pytest.mark.parametrize("name", KAPPA_CASES)
+def test_kappa_fixture_coefficients_differ_per_cell(name):
+    """Guard for the kappa fixtures: M really varies per X cell (contrast above 100)."""
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    k = z["kappa_x"]
+    assert k.max() / k.min() > 100.0

@@ -6,12 +6,15 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, GOLDEN_CASES, assert_same_sparse, load_golden
+from conftest import ADAPTIVE_CASES, GOLDEN, GOLDEN_CASES, HHAT_RESIDUE, assert_same_sparse, load_golden
 
 import apf_oracle as O
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+ALL_2D = GOLDEN_CASES + ADAPTIVE_CASES + ["p1_kappa_uniform"]
+
+
+@pytest.mark.parametrize("name", ALL_2D)
 def test_oracle_main_blocks_match_reference(name):
     prob, ref, example = load_golden(name)
     u0 = O.sin_initial if example == "smooth_initial" else O.one_initial
@@ -22,29 +25,67 @@ def test_oracle_main_blocks_match_reference(name):
     assert np.abs(out["g"] - ref["g"]).max() <= 1e-12 * np.abs(ref["g"]).max()
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", ALL_2D)
 def test_oracle_graph_norm_matches_reference(name):
     prob, ref, example = load_golden(name)
     gn = O.assemble_graph_norm(prob, ref["A_y"], ref["C_signed"])
-    assert_same_sparse(ref["Hhat"], gn["Hhat"], 1e-12, "Hhat")
+    residue = HHAT_RESIDUE if name in ADAPTIVE_CASES else 0.0
+    assert_same_sparse(ref["Hhat"], gn["Hhat"], 1e-12, "Hhat", residue=residue)
 
 
 M_ANISO = (2.0, 0.5, 1.0)  # (m00, m01, m11) of the fixtures' second two-pass call
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", ALL_2D)
 def test_oracle_two_pass_full_saddle_matches_reference(name):
     prob, ref, example = load_golden(name)
     u0 = O.sin_initial if example == "smooth_initial" else O.one_initial
     assert ref["K2p_pattern_reuse_count"] == 1
+    m_example = prob.m_cells
     for key, m in (("K2p", None), ("K2p_aniso", M_ANISO)):
-        prob.m_cells = None if m is None else np.tile(m, (prob.y_geom.shape[0], 1))
+        prob.m_cells = m_example if m is None else np.tile(m, (prob.y_geom.shape[0], 1))
         K, rhs = O.assemble_main_full_saddle_two_pass(prob, u0=u0)
         assert_same_sparse(ref[key], K, 1e-12, key)
         assert np.abs(rhs - ref[key + "_rhs"]).max() <= 1e-12 * np.abs(ref[key + "_rhs"]).max()
     # the identity coefficient's right-angle couplings cancel to zero and are pruned; the
     # anisotropic one keeps them, so the two patterns differ
     assert ref["K2p"].nnz < ref["K2p_aniso"].nnz
+
+
+def test_adaptive_fixtures_have_hanging_nodes_and_finer_y():
+    """The adaptive fixtures exercise what uniform meshes cannot: restriction rows with several
+    weighted entries (space-time hanging nodes of X, temporal ones of Y), Y cells finer than
+    their X ancestors, and Y cells spanning several time slabs."""
+    for name in ADAPTIVE_CASES:
+        prob, ref, _ = load_golden(name)
+        xo = np.diff(prob.x_restr.offsets)
+        yo = np.diff(prob.y_restr.offsets)
+        assert xo.max() >= 3 and (xo > 1).sum() > 10, name
+        assert (yo > 1).sum() > 0, name
+        assert prob.y_geom.shape[0] > prob.x_geom.shape[0], name
+        z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+        assert len(z["slab_of_cell"]) > prob.y_geom.shape[0], name
+
+
+@pytest.mark.parametrize("name", ADAPTIVE_CASES)
+def test_oracle_slab_reconstruction_matches_reference(name):
+    """lambda~ of the slab reconstruction on the reference's own time-slab space, from the
+    reference's u_delta: the slab DOF count and lambda~ at every slab cell's vertices and
+    slab end times (1e-12 of the largest value)."""
+    prob, ref, example = load_golden(name)
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    src, slab, geom, restr, lt = O.slab_reconstruction(prob, z["y_vertex_ids"], z["u_delta"])
+    assert len(lt) == int(z["slab_dof_base"][-1])
+    nodal = O.nodal_values(restr, lt)
+    p = prob.p
+    vertex_nodes = [0, 1, 2] if p == 1 else [0, 2, 5]
+    time_nodes = [0, 1] if p == 1 else [0, 2]
+    mine = np.stack([nodal[:, s * (p + 1) + a] for s in vertex_nodes for a in time_nodes], axis=1)
+    cell_index = {int(c): i for i, c in enumerate(z["y_cell_ids"])}
+    order = {(int(k), cell_index[int(c)]): i for i, (k, c) in enumerate(zip(z["slab_of_cell"], z["slab_source_cell"]))}
+    perm = [order[(int(k), int(c))] for k, c in zip(slab, src)]
+    theirs = z["slab_lambda_tilde"][perm]
+    assert np.abs(mine - theirs).max() <= 1e-12 * np.abs(theirs).max()
 
 
 def _paper_rows():
