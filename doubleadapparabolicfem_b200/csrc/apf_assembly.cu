@@ -250,7 +250,7 @@ namespace apf
             int* status;         // nonzero on overflow
             const int* list;     // rows to process (null: all)
             int nlist;
-            int kmax;            // restriction entries per local row (at most 4)
+            int kmax;            // restriction entries per local row (at most kMaxRestrictionEntries)
         };
 
         // One warp per row with at most UCAP distinct columns, in one pass over the candidates:
@@ -263,6 +263,9 @@ namespace apf
         // Shared memory per warp: incidences int[2 kIncCap + 2], table keys int[2 UCAP],
         // table sums double[2 UCAP], sorted keys 8 B x UCAP, staged values double[32].
         constexpr int kGatherIncCap = 256;
+        // longest restriction row accepted (hanging-node chains of adaptive meshes: the
+        // reference's 1-irregular refinement gives at most about 9)
+        constexpr int kMaxRestrictionEntries = 16;
 
         template<int UCAP>
         __host__ __device__ constexpr std::size_t gather_u_warp_bytes()
@@ -1142,7 +1145,7 @@ namespace apf
             require(incs[t]->max_len <= 256, APF_ERR_CAPACITY, "a DOF has more than 256 cell incidences");
             cap += incs[t]->max_len * in.ndof * kmax;
         }
-        require(kmax <= 4, APF_ERR_CAPACITY, "restriction rows with more than 4 entries are not supported");
+        require(kmax <= kMaxRestrictionEntries, APF_ERR_CAPACITY, "restriction rows with more than 16 entries are not supported");
         DeviceBuffer<int> status(1, s);
         status.zero();
         a.status = status.get();
@@ -1321,7 +1324,7 @@ namespace apf
                              DeviceCsr& K)
     {
         const int n_lambda = in.n_lambda, n_u = in.n_u, n = n_lambda + n_u;
-        require(in.kmax <= 4, APF_ERR_CAPACITY, "restriction rows with more than 4 entries are not supported");
+        require(in.kmax <= kMaxRestrictionEntries, APF_ERR_CAPACITY, "restriction rows with more than 16 entries are not supported");
         DeviceBuffer<double> vals(static_cast<std::size_t>(std::max(nnz_pattern, 1ll)), s);
         DeviceBuffer<int> status(1, s);
         status.zero();
