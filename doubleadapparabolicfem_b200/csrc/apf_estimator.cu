@@ -1736,27 +1736,68 @@ namespace apf
             }
         }
 
-        // per slab cell: the source Y cell's geometry with the slab's time interval, its M,
-        // load and X ancestor
-        __global__ void slab_cells_kernel(int n, const int* __restrict__ source, const int* __restrict__ slab,
-                                          const double* __restrict__ slab_times, const double* __restrict__ y_geo,
-                                          const double* __restrict__ m_y, const double* __restrict__ ell_y,
-                                          const int* __restrict__ y_to_x, double* __restrict__ geo,
-                                          double* __restrict__ m, double* __restrict__ ell, int* __restrict__ to_x)
+        // per slab cell: the source Y cell's geometry row (gw values, the last two t0 t1) with
+        // the slab's time interval, its M (mw values), load and X ancestor
+        __global__ void slab_cells_kernel(int n, int gw, int mw, const int* __restrict__ source,
+                                          const int* __restrict__ slab, const double* __restrict__ slab_times,
+                                          const double* __restrict__ y_geo, const double* __restrict__ m_y,
+                                          const double* __restrict__ ell_y, const int* __restrict__ y_to_x,
+                                          double* __restrict__ geo, double* __restrict__ m, double* __restrict__ ell,
+                                          int* __restrict__ to_x)
         {
             for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
             {
                 const int y = source[c], k = slab[c];
-                for (int j = 0; j < 6; ++j)
-                    geo[8ll * c + j] = y_geo[8ll * y + j];
-                geo[8ll * c + 6] = slab_times[k];
-                geo[8ll * c + 7] = slab_times[k + 1];
+                for (int j = 0; j < gw - 2; ++j)
+                    geo[(long long)gw * c + j] = y_geo[(long long)gw * y + j];
+                geo[(long long)gw * c + gw - 2] = slab_times[k];
+                geo[(long long)gw * c + gw - 1] = slab_times[k + 1];
                 if (m)
-                    for (int j = 0; j < 3; ++j)
-                        m[3ll * c + j] = m_y[3ll * y + j];
+                    for (int j = 0; j < mw; ++j)
+                        m[(long long)mw * c + j] = m_y[(long long)mw * y + j];
                 if (ell)
                     ell[c] = ell_y[y];
                 to_x[c] = y_to_x[y];
+            }
+        }
+
+        // 1+1D: dst[c] (bilinear nodal values, index x_node * 2 + t_node) = the source quad's
+        // bilinear function at the corners of quad c (inside it)
+        __global__ void nodal_transfer_1d_kernel(int n, const double* __restrict__ dst_geo,
+                                                 const int* __restrict__ src_index, const double* __restrict__ src_geo,
+                                                 const double* __restrict__ src, double* __restrict__ dst)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+            {
+                const int sc = src_index ? src_index[c] : c;
+                const double* gd = dst_geo + 4ll * c;
+                const double* gs = src_geo + 4ll * sc;
+                const double* in = src + 4ll * sc;
+                for (int k = 0; k < 4; ++k)
+                {
+                    const double x = gd[k >> 1], t = gd[2 + (k & 1)];
+                    const double xi = (x - gs[0]) / (gs[1] - gs[0]), tau = (t - gs[2]) / (gs[3] - gs[2]);
+                    const double bx[2] = {1.0 - xi, xi}, bt[2] = {1.0 - tau, tau};
+                    double v = 0.0;
+                    for (int i = 0; i < 2; ++i)
+                        for (int b = 0; b < 2; ++b)
+                            v += in[i * 2 + b] * bx[i] * bt[b];
+                    dst[4ll * c + k] = v;
+                }
+            }
+        }
+
+        // 1+1D: out[c] = int_c m (d_x v)^2 of bilinear nodal values v on quad c
+        __global__ void nodal_energy_1d_kernel(int n, const double* __restrict__ geo, const double* __restrict__ m,
+                                               const double* __restrict__ v, double* __restrict__ out)
+        {
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+            {
+                const double* g = geo + 4ll * c;
+                const double h = g[1] - g[0], ht = g[3] - g[2];
+                const double d0 = v[4ll * c + 2] - v[4ll * c + 0], d1 = v[4ll * c + 3] - v[4ll * c + 1];
+                const double mc = m ? m[c] : 1.0;
+                out[c] = mc * (ht / h) * (d0 * d0 + d0 * d1 + d1 * d1) / 3.0;
             }
         }
 
@@ -1788,12 +1829,13 @@ namespace apf
         std::vector<int> src_ptr, src_list; // Y cell -> its slab cells
     };
 
-    // host integer work: slabs, slab cells, slab DOFs (bnode: Dirichlet flag per Y cell and
-    // spatial node)
-    void build_slab_space(int p, int ny, const std::vector<double>& ytimes, const std::vector<int>& yvids,
-                          const std::vector<unsigned char>& bnode, SlabSpace& sp)
+    // host integer work: slabs, slab cells, slab DOFs.  keys: one 64-bit identity per (Y cell,
+    // spatial node) shared by the nodes that coincide (ns per cell); bnode: Dirichlet flag per
+    // (Y cell, spatial node); yvids (2+1D, may be empty): spatial vertex ids of the Y cells
+    void build_slab_space(int ns, int nt, int ny, const std::vector<double>& ytimes, const std::vector<int>& yvids,
+                          const std::vector<std::uint64_t>& keys, const std::vector<unsigned char>& bnode, SlabSpace& sp)
     {
-        const int ns = p == 1 ? 3 : 6, nt = p + 1, nd = ns * nt;
+        const int nd = ns * nt;
         std::vector<double>& T = sp.slab_times;
         T.assign(ytimes.begin(), ytimes.end());
         std::sort(T.begin(), T.end());
@@ -1829,23 +1871,19 @@ namespace apf
                 }
         }
         sp.times.resize(2ll * nsc);
-        sp.vids.resize(3ll * nsc);
         for (int i = 0; i < nsc; ++i)
         {
             sp.times[2ll * i] = T[sp.slab[i]];
             sp.times[2ll * i + 1] = T[sp.slab[i] + 1];
-            for (int v = 0; v < 3; ++v)
-                sp.vids[3ll * i + v] = yvids[3ll * sp.source[i] + v];
         }
-        // spatial nodes of slab cell i: vertex nodes keyed by their vertex id, P2 edge nodes
-        // by their two vertex ids (node order v0 m01 v1 m02 m12 v2)
-        static const int kNodeVerts[2][6][2] = {{{0, 0}, {1, 1}, {2, 2}, {0, 0}, {0, 0}, {0, 0}},
-                                                {{0, 0}, {0, 1}, {1, 1}, {0, 2}, {1, 2}, {2, 2}}};
-        auto node_key = [&](int i, int s) {
-            const int a = sp.vids[3ll * i + kNodeVerts[p - 1][s][0]], b = sp.vids[3ll * i + kNodeVerts[p - 1][s][1]];
-            const std::uint32_t lo = static_cast<std::uint32_t>(std::min(a, b)), hi = static_cast<std::uint32_t>(std::max(a, b));
-            return (static_cast<std::uint64_t>(lo) << 32) | hi;
-        };
+        if (!yvids.empty())
+        {
+            sp.vids.resize(3ll * nsc);
+            for (int i = 0; i < nsc; ++i)
+                for (int v = 0; v < 3; ++v)
+                    sp.vids[3ll * i + v] = yvids[3ll * sp.source[i] + v];
+        }
+        auto node_key = [&](int i, int s) { return keys[static_cast<std::size_t>(sp.source[i]) * ns + s]; };
         // per slab (host threads): spatial node numbering in first-appearance order
         std::vector<int> local(static_cast<std::size_t>(nsc) * ns, -1), n_spatial(sp.n_slabs, 0);
         const int nthreads = std::max(1, std::min<int>(8, static_cast<int>(std::thread::hardware_concurrency())));
@@ -1914,7 +1952,7 @@ namespace apf
         SystemInputs& in = out.in;
         in.p = yin.p;
         in.ndof = yin.ndof;
-        in.dim = 2;
+        in.dim = yin.dim;
         in.n_y_cells = sp.n_cells;
         in.n_x_cells = yin.n_x_cells;
         in.n_lambda = sp.n_dofs;
@@ -1923,22 +1961,23 @@ namespace apf
         in.zero_tol = yin.zero_tol;
         in.g_scale = yin.g_scale;
         const int n = sp.n_cells, nd = yin.ndof;
+        const int gw = yin.dim == 1 ? 4 : 8, mw = yin.dim == 1 ? 1 : 3;
         DeviceBuffer<int> d_source(0, s), d_slab(0, s);
         DeviceBuffer<double> d_times(0, s);
         d_source.upload(sp.source.data(), sp.source.size());
         d_slab.upload(sp.slab.data(), sp.slab.size());
         d_times.upload(sp.slab_times.data(), sp.slab_times.size());
-        in.y_geo.allocate(8ll * n, s);
+        in.y_geo.allocate(static_cast<std::size_t>(gw) * n, s);
         in.y_to_x.allocate(n, s);
         if (yin.m_y.size())
-            in.m_y.allocate(3ll * n, s);
+            in.m_y.allocate(static_cast<std::size_t>(mw) * n, s);
         if (yin.ell.size())
             in.ell.allocate(n, s);
         if (n > 0)
         {
             APF_KERNEL("est_slab_cells", s);
-            slab_cells_kernel<<<nb(n), 256, 0, s>>>(n, d_source.get(), d_slab.get(), d_times.get(), yin.y_geo.get(),
-                                                     yin.m_y.size() ? yin.m_y.get() : nullptr,
+            slab_cells_kernel<<<nb(n), 256, 0, s>>>(n, gw, mw, d_source.get(), d_slab.get(), d_times.get(),
+                                                     yin.y_geo.get(), yin.m_y.size() ? yin.m_y.get() : nullptr,
                                                      yin.ell.size() ? yin.ell.get() : nullptr, yin.y_to_x.get(),
                                                      in.y_geo.get(), in.m_y.size() ? in.m_y.get() : nullptr,
                                                      in.ell.size() ? in.ell.get() : nullptr, in.y_to_x.get());
@@ -2156,7 +2195,21 @@ namespace apf
                 APF_CUDA(cudaMemcpyAsync(bnode.data(), d_bnode.get(), bnode.size(), cudaMemcpyDeviceToHost, s));
                 sync(s);
             }
-            build_slab_space(in.p, ny, ytimes, vids_host, bnode, sp);
+            // spatial nodes: vertex nodes keyed by their vertex id, P2 edge nodes by their two
+            // vertex ids (node order v0 m01 v1 m02 m12 v2)
+            static const int kNodeVerts[2][6][2] = {{{0, 0}, {1, 1}, {2, 2}, {0, 0}, {0, 0}, {0, 0}},
+                                                    {{0, 0}, {0, 1}, {1, 1}, {0, 2}, {1, 2}, {2, 2}}};
+            std::vector<std::uint64_t> keys(static_cast<std::size_t>(ny) * ns);
+            for (int c = 0; c < ny; ++c)
+                for (int q = 0; q < ns; ++q)
+                {
+                    const int a = vids_host[3ll * c + kNodeVerts[in.p - 1][q][0]];
+                    const int b = vids_host[3ll * c + kNodeVerts[in.p - 1][q][1]];
+                    const std::uint32_t lo = static_cast<std::uint32_t>(std::min(a, b));
+                    const std::uint32_t hi = static_cast<std::uint32_t>(std::max(a, b));
+                    keys[static_cast<std::size_t>(c) * ns + q] = (static_cast<std::uint64_t>(lo) << 32) | hi;
+                }
+            build_slab_space(ns, nt, ny, ytimes, vids_host, keys, bnode, sp);
             upload_slab_system(s, in, sp, sl);
         }
         // the cells the patches and indicators run on: Y cells, or slab cells
@@ -2769,16 +2822,87 @@ namespace apf
         require(S.solution.size() == static_cast<std::size_t>(in.n_lambda + in.n_u), APF_ERR_INVALID,
                 "estimator: solve the main system first");
         require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
-        require(in.n_x_cells == in.n_y_cells, APF_ERR_INVALID, "estimator: Y cells must coincide with X cells");
         EstimatorTotals tot{};
         const int ny = in.n_y_cells, nl = in.n_lambda;
-        // ---- edge patches: host integer work on the cells' intervals
-        std::vector<double> geo(4ll * ny);
+        // ---- Y cell intervals (host) and whether the Y restriction is trivial
+        std::vector<double> ygeo(4ll * ny), ytimes(2ll * ny);
+        int nontrivial = 0;
         if (ny)
-            APF_CUDA(cudaMemcpyAsync(geo.data(), in.y_geo.get(), geo.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-        sync(s);
-        std::vector<int> order(ny);
+        {
+            DeviceBuffer<int> flag(1, s);
+            flag.zero();
+            {
+                APF_KERNEL("est_restriction_check", s);
+                nontrivial_restriction_kernel<<<nb(4ll * ny), 256, 0, s>>>(4ll * ny, in.y_off.get(), in.y_w.get(),
+                                                                          flag.get());
+            }
+            APF_CUDA(cudaMemcpyAsync(ygeo.data(), in.y_geo.get(), ygeo.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+            APF_CUDA(cudaMemcpyAsync(&nontrivial, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+            sync(s);
+        }
         for (int c = 0; c < ny; ++c)
+        {
+            ytimes[2ll * c] = ygeo[4ll * c + 2];
+            ytimes[2ll * c + 1] = ygeo[4ll * c + 3];
+        }
+        // ---- time slabs (as in 2+1D): Y itself, or Y cells cut into slab cells
+        SlabSpace sp;
+        {
+            std::vector<double> T(ytimes);
+            std::sort(T.begin(), T.end());
+            T.erase(std::unique(T.begin(), T.end()), T.end());
+            bool one_slab_each = true;
+            for (int c = 0; c < ny && one_slab_each; ++c)
+            {
+                const auto a = std::upper_bound(T.begin(), T.end(), ytimes[2ll * c]);
+                one_slab_each = a != T.end() && *a == ytimes[2ll * c + 1];
+            }
+            sp.identity = one_slab_each && nontrivial == 0;
+        }
+        SlabSystem sl;
+        std::vector<double> geo; // the cells' geometry on the host (Y cells or slab cells)
+        if (!sp.identity)
+        {
+            APF_HOST_RANGE("est_slab_space");
+            std::vector<unsigned char> bnode(2ll * ny);
+            if (ny)
+            {
+                DeviceBuffer<unsigned char> d_bnode(bnode.size(), s);
+                {
+                    APF_KERNEL("est_dirichlet_nodes", s);
+                    dirichlet_nodes_kernel<<<nb(2ll * ny), 256, 0, s>>>(ny, 2, 2, in.y_off.get(), d_bnode.get());
+                }
+                APF_CUDA(cudaMemcpyAsync(bnode.data(), d_bnode.get(), bnode.size(), cudaMemcpyDeviceToHost, s));
+                sync(s);
+            }
+            // spatial nodes are points of the line: keyed by the bits of their coordinate
+            std::vector<std::uint64_t> keys(2ll * ny);
+            for (int c = 0; c < ny; ++c)
+                for (int q = 0; q < 2; ++q)
+                    std::memcpy(&keys[2ll * c + q], &ygeo[4ll * c + q], sizeof(double));
+            build_slab_space(2, 2, ny, ytimes, {}, keys, bnode, sp);
+            upload_slab_system(s, in, sp, sl);
+            geo.resize(4ll * sp.n_cells);
+            for (int i = 0; i < sp.n_cells; ++i)
+            {
+                geo[4ll * i] = ygeo[4ll * sp.source[i]];
+                geo[4ll * i + 1] = ygeo[4ll * sp.source[i] + 1];
+                geo[4ll * i + 2] = sp.times[2ll * i];
+                geo[4ll * i + 3] = sp.times[2ll * i + 1];
+            }
+        }
+        else
+            geo.swap(ygeo);
+        const int nc = sp.identity ? ny : sp.n_cells;
+        const double* cgeo = sp.identity ? in.y_geo.get() : sl.in.y_geo.get();
+        const double* cm = sp.identity ? (in.m_y.size() ? in.m_y.get() : nullptr)
+                                       : (sl.in.m_y.size() ? sl.in.m_y.get() : nullptr);
+        const double* cell = sp.identity ? (in.ell.size() ? in.ell.get() : nullptr)
+                                         : (sl.in.ell.size() ? sl.in.ell.get() : nullptr);
+        const int* cx = sp.identity ? in.y_to_x.get() : sl.in.y_to_x.get();
+        // ---- edge patches: host integer work on the cells' intervals
+        std::vector<int> order(nc);
+        for (int c = 0; c < nc; ++c)
             order[c] = c;
         // slabs = distinct time intervals (in time order), cells of a slab by x
         std::sort(order.begin(), order.end(), [&](int a, int b) {
@@ -2791,13 +2915,13 @@ namespace apf
             return a < b;
         });
         std::vector<int> left, right;
-        left.reserve(static_cast<std::size_t>(ny) + 64);
-        right.reserve(static_cast<std::size_t>(ny) + 64);
+        left.reserve(static_cast<std::size_t>(nc) + 64);
+        right.reserve(static_cast<std::size_t>(nc) + 64);
         int n_slabs = 0;
-        for (int b = 0; b < ny;)
+        for (int b = 0; b < nc;)
         {
             int e = b + 1;
-            while (e < ny && geo[4ll * order[e] + 2] == geo[4ll * order[b] + 2] &&
+            while (e < nc && geo[4ll * order[e] + 2] == geo[4ll * order[b] + 2] &&
                    geo[4ll * order[e] + 3] == geo[4ll * order[b] + 3])
                 ++e;
             ++n_slabs;
@@ -2817,35 +2941,69 @@ namespace apf
         const int np = static_cast<int>(left.size());
         tot.n_slabs = n_slabs;
         tot.n_patches = np;
-        tot.max_patch_cells = ny > 1 ? 2 : 1;
+        tot.max_patch_cells = nc > 1 ? 2 : 1;
         // ---- lambda~
-        DeviceBuffer<double> lt(nl, s);
-        reconstruct_lambda(s, S, lt, tot);
-        // ---- nodal data per cell
-        DeviceBuffer<double> ltil(4ll * ny, s), ucell(4ll * ny, s);
+        DeviceBuffer<double> lt(sp.identity ? nl : 0, s);
+        if (sp.identity)
+            reconstruct_lambda(s, S, lt, tot);
+        else
+            reconstruct_lambda_slabs(s, S, sl, lt, tot);
+        // ---- nodal data per cell: lambda~ through the slab restriction, lambda_delta and u
+        // as the bilinear functions of the cell's Y cell and X ancestor at its corners
+        DeviceBuffer<double> ltil(4ll * nc, s), ucell(4ll * nc, s), ldel(4ll * nc, s);
         {
+            const SystemInputs& li = sp.identity ? in : sl.in;
             APF_KERNEL("est_gather_nodal", s);
-            gather_nodal<<<nb(4ll * ny), 256, 0, s>>>(ny, 4, in.y_off.get(), in.y_dofs.get(), in.y_w.get(), lt.get(),
+            gather_nodal<<<nb(4ll * nc), 256, 0, s>>>(nc, 4, li.y_off.get(), li.y_dofs.get(), li.y_w.get(), lt.get(),
                                                      nullptr, ltil.get());
         }
         {
-            APF_KERNEL("est_gather_nodal", s);
-            gather_nodal<<<nb(4ll * ny), 256, 0, s>>>(ny, 4, in.x_off.get(), in.x_dofs.get(), in.x_w.get(),
-                                                     S.solution.get() + nl, nullptr, ucell.get());
+            DeviceBuffer<double> ly(4ll * ny, s);
+            {
+                APF_KERNEL("est_gather_nodal", s);
+                gather_nodal<<<nb(4ll * ny), 256, 0, s>>>(ny, 4, in.y_off.get(), in.y_dofs.get(), in.y_w.get(),
+                                                         S.solution.get(), nullptr, ly.get());
+            }
+            if (sp.identity)
+                copy(s, 4 * ny, ly.get(), ldel.get());
+            else if (nc > 0)
+            {
+                DeviceBuffer<int> d_src(0, s);
+                d_src.upload(sp.source.data(), sp.source.size());
+                APF_KERNEL("nodal_transfer", s);
+                nodal_transfer_1d_kernel<<<nb(nc), 256, 0, s>>>(nc, cgeo, d_src.get(), in.y_geo.get(), ly.get(),
+                                                                ldel.get());
+            }
         }
+        {
+            const int nx = in.n_x_cells;
+            DeviceBuffer<double> ux(4ll * nx, s);
+            if (nx > 0)
+            {
+                APF_KERNEL("est_gather_nodal", s);
+                gather_nodal<<<nb(4ll * nx), 256, 0, s>>>(nx, 4, in.x_off.get(), in.x_dofs.get(), in.x_w.get(),
+                                                         S.solution.get() + nl, nullptr, ux.get());
+            }
+            if (nc > 0)
+            {
+                APF_KERNEL("nodal_transfer", s);
+                nodal_transfer_1d_kernel<<<nb(nc), 256, 0, s>>>(nc, cgeo, cx, in.x_geo.get(), ux.get(), ucell.get());
+            }
+        }
+        APF_CUDA(cudaGetLastError());
         DeviceBuffer<int> d_left(0, s), d_right(0, s), status(1, s);
         d_left.upload(left.data(), left.size());
         d_right.upload(right.data(), right.size());
         status.zero();
-        DeviceBuffer<double> sigma(8ll * ny, s);
+        DeviceBuffer<double> sigma(8ll * nc, s);
         sigma.zero();
         EdgeArgs ea{};
         ea.n_patches = np;
         ea.left = d_left.get();
         ea.right = d_right.get();
-        ea.geo = in.y_geo.get();
-        ea.m = in.m_y.size() ? in.m_y.get() : nullptr;
-        ea.ell = in.ell.size() ? in.ell.get() : nullptr;
+        ea.geo = cgeo;
+        ea.m = cm;
+        ea.ell = cell;
         ea.lt = ltil.get();
         ea.u = ucell.get();
         ea.zero_tol = in.zero_tol;
@@ -2861,10 +3019,10 @@ namespace apf
         APF_CUDA(cudaMemcpyAsync(&hstat, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         sync(s);
         require(hstat == 0, APF_ERR_NUMERIC, "1+1D estimator: singular patch system");
-        DeviceBuffer<double> f2(ny, s), d2(ny, s), r2(ny, s), e2(ny, s);
+        DeviceBuffer<double> f2(nc, s), d2(nc, s), r2(nc, s), e2(nc, s);
         EdgeIndArgs ia{};
-        ia.n_cells = ny;
-        ia.geo = in.y_geo.get();
+        ia.n_cells = nc;
+        ia.geo = cgeo;
         ia.m = ea.m;
         ia.ell = ea.ell;
         ia.lt = ltil.get();
@@ -2872,21 +3030,49 @@ namespace apf
         ia.sigma = sigma.get();
         ia.flux = f2.get();
         ia.div = d2.get();
-        if (ny > 0)
+        if (nc > 0)
         {
             APF_KERNEL("est_cell_indicators", s);
-            edge_cell_indicators<<<nb(ny, 128), 128, 0, s>>>(ia);
+            edge_cell_indicators<<<nb(nc, 128), 128, 0, s>>>(ia);
         }
-        DeviceBuffer<double> dl(nl, s);
-        copy(s, nl, S.solution.get(), dl.get());
-        axpby(s, nl, -1.0, lt.get(), 1.0, dl.get());
-        y_cell_energy(s, in, dl.get(), r2.get());
-        if (ny > 0)
+        // ||lambda_delta - lambda~||^2 in the local A_y energy
+        if (sp.identity)
+        {
+            DeviceBuffer<double> dl(nl, s);
+            copy(s, nl, S.solution.get(), dl.get());
+            axpby(s, nl, -1.0, lt.get(), 1.0, dl.get());
+            y_cell_energy(s, in, dl.get(), r2.get());
+        }
+        else if (nc > 0)
+        {
+            DeviceBuffer<double> dl(4ll * nc, s);
+            copy(s, 4 * nc, ldel.get(), dl.get());
+            axpby(s, 4 * nc, -1.0, ltil.get(), 1.0, dl.get());
+            APF_KERNEL("nodal_energy", s);
+            nodal_energy_1d_kernel<<<nb(nc), 256, 0, s>>>(nc, cgeo, cm, dl.get(), r2.get());
+        }
+        if (nc > 0)
         {
             APF_KERNEL("est_eta", s);
-            add_kernel<<<nb(ny), 256, 0, s>>>(ny, f2.get(), r2.get(), e2.get());
+            add_kernel<<<nb(nc), 256, 0, s>>>(nc, f2.get(), r2.get(), e2.get());
         }
         APF_CUDA(cudaGetLastError());
+        if (!sp.identity)
+        {
+            DeviceBuffer<double> tmp(nc, s);
+            for (DeviceBuffer<double>* a : {&f2, &d2, &r2, &e2})
+            {
+                copy(s, nc, a->get(), tmp.get());
+                a->allocate(ny, s);
+                if (ny)
+                {
+                    APF_KERNEL("est_reduce_to_source", s);
+                    reduce_to_source_kernel<<<nb(ny), 256, 0, s>>>(ny, sl.src_ptr.get(), sl.src_list.get(), tmp.get(),
+                                                                   a->get());
+                }
+            }
+            APF_CUDA(cudaGetLastError());
+        }
         tot.flux = device_sum(s, ny, f2.get());
         tot.div = device_sum(s, ny, d2.get());
         tot.recon = device_sum(s, ny, r2.get());

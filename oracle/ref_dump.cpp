@@ -568,7 +568,36 @@ namespace
         adaptive_algorithm::examples::initialize_spaces_from_example(x_space, y_space, example);
         for (int k = 0; k < levels; ++k)
             uniform_isotropic_refine(x_space);
+        if (const char* pts = std::getenv("APF_REF_X_POINTS"))
+        {
+            // 1+1D points "x,t;x,t"
+            std::vector<typename XSpace::SpaceTimePoint> points;
+            std::string str(pts);
+            std::size_t pos = 0;
+            while (pos < str.size())
+            {
+                std::size_t end = str.find(';', pos);
+                if (end == std::string::npos) end = str.size();
+                double a = 0.0, b = 0.0;
+                if (std::sscanf(str.substr(pos, end - pos).c_str(), "%lf,%lf", &a, &b) == 2)
+                    points.push_back(typename XSpace::SpaceTimePoint{a, b});
+                pos = end + 1;
+            }
+            adaptive_algorithm::support::refine_points_n_times(x_space, points, env_int("APF_REF_X_ROUNDS", 1));
+        }
         y_space.initialize(x_space.active_cells());
+        for (int pass = 0; pass < env_int("APF_REF_Y_PASSES", 0); ++pass)
+        {
+            typename Backend::Solver solver;
+            la::concepts::SolverOptions opts;
+            finite_element::time_slabs::AdaptiveTestSpaceIterationParameters<Backend, XSpace, YSpace> params;
+            const auto state = finite_element::time_slabs::compute_adaptive_test_space_iteration<QSpace, QTime, Backend>(
+                y_space, x_space, example.problem, solver, opts, params);
+            std::cerr << "y pass " << pass << ": marked " << state.marked_source_cells.size() << " of "
+                      << y_space.active_cells().size() << " Y cells\n";
+            finite_element::time_slabs::refine_test_space_from_marked_source_cells(y_space, x_space,
+                                                                                   state.marked_source_cells);
+        }
 
         const auto& y_cells = y_space.active_cells();
         const auto& x_cells = x_space.active_cells();

@@ -52,6 +52,11 @@ CASES = [
     ("p1_kappa_uniform", 2, 1, 2, "smooth_initial", {"APF_REF_KAPPA": "3:0.1:10"}),
     ("p2_adapt_smooth", 2, 2, 1, "smooth_initial",
      {"APF_REF_X_POINTS": "0.3,0.3,0.3", "APF_REF_X_ROUNDS": "2", "APF_REF_Y_PASSES": "1"}),
+    # 1+1D (points x,t)
+    ("d1_adapt_smooth", 1, 1, 2, "smooth_initial",
+     {"APF_REF_X_POINTS": "0.3,0.3;0.7,0.8", "APF_REF_X_ROUNDS": "3", "APF_REF_Y_PASSES": "1"}),
+    ("d1_adapt_nonmatching", 1, 1, 2, "non_matching_initial",
+     {"APF_REF_X_POINTS": "0.15,0.05", "APF_REF_X_ROUNDS": "4", "APF_REF_Y_PASSES": "1"}),
 ]
 
 

@@ -16,7 +16,11 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, GOLDEN_CASES_1D, assert_same_sparse, load_golden, to_product_problem
+from conftest import GOLDEN, GOLDEN_CASES_1D, HHAT_RESIDUE, assert_same_sparse, load_golden, to_product_problem
+
+# adaptive 1+1D meshes from the reference: X refined locally (hanging nodes in space and
+# time), Y refined beyond X by one pass of the reference's inner loop
+ADAPTIVE_CASES_1D = ["d1_adapt_smooth", "d1_adapt_nonmatching"]
 
 import apf_oracle as O
 
@@ -39,7 +43,7 @@ def _oracle_u0_ell(example, n_cells):
 # ---------------------------------------------------------------------------------------
 # CPU: oracle and mesh generator
 # ---------------------------------------------------------------------------------------
-@pytest.mark.parametrize("name", GOLDEN_CASES_1D)
+@pytest.mark.parametrize("name", GOLDEN_CASES_1D + ADAPTIVE_CASES_1D)
 def test_oracle_1d_blocks_match_reference(name):
     prob, ref, example = load_golden(name)
     u0, ell = _oracle_u0_ell(example, prob.y_geom.shape[0])
@@ -49,7 +53,17 @@ def test_oracle_1d_blocks_match_reference(name):
     assert np.abs(out["f"] - ref["f"]).max() <= 1e-12 * max(1.0, np.abs(ref["f"]).max())
     assert np.abs(out["g"] - ref["g"]).max() <= 1e-12 * np.abs(ref["g"]).max()
     gn = O.assemble_graph_norm_1d(prob, ref["A_y"], ref["C_signed"])
-    assert_same_sparse(ref["Hhat"], gn["Hhat"], 1e-12, "Hhat")
+    residue = HHAT_RESIDUE if name in ADAPTIVE_CASES_1D else 0.0
+    assert_same_sparse(ref["Hhat"], gn["Hhat"], 1e-12, "Hhat", residue=residue)
+
+
+def test_adaptive_1d_fixtures_have_hanging_nodes():
+    for name in ADAPTIVE_CASES_1D:
+        prob, ref, _ = load_golden(name)
+        assert (np.diff(prob.x_restr.offsets) > 1).sum() > 10, name
+        assert (np.diff(prob.y_restr.offsets) > 1).sum() > 10, name
+        assert prob.y_geom.shape[0] > prob.x_geom.shape[0], name
+        assert np.load(os.path.join(GOLDEN, f"{name}.npz"))["est_recon"].sum() > 0.0
 
 
 def test_uniform_1d_dof_counts_match_paper_data():
@@ -214,3 +228,40 @@ def test_1d_configuration_cycle_and_paper_values(gpu_ctx):
                          ("eta_squared", xt["eta_squared"])):
             want = float(rows[level][key])
             assert abs(val - want) <= 1e-5 * want, (level, key, val, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ADAPTIVE_CASES_1D)
+def test_1d_adaptive_cycle_matches_reference(gpu_ctx, name):
+    """Adaptive 1+1D meshes: blocks (patterns bit-exact, 1e-12; Hhat's significant pattern),
+    MINRES (1e-13), then the slab reconstruction on the time-slab space (Y cells cut at every
+    time endpoint), the edge-patch estimator and the X-marking indicators against the
+    reference's own per-cell values: 1e-9 of the largest cell eta, totals 1e-10 (recon 1e-8)."""
+    from doubleadapparabolicfem_b200.estimator import estimate, x_marking_indicator_components
+    from doubleadapparabolicfem_b200.solver import SolverOptions, solve_saddle_system_with_preconditioner
+    prob, ref, example = load_golden(name)
+    z = _fixture(name)
+    blocks = _assemble(gpu_ctx, to_product_problem(prob, example))
+    assert_same_sparse(ref["A_y"], blocks.A_y(), 1e-12, "A_y")
+    assert_same_sparse(ref["B"], blocks.lower_left_B(), 1e-12, "B")
+    assert_same_sparse(ref["C_signed"], blocks.C_signed(), 1e-12, "C_signed")
+    assert_same_sparse(ref["Hhat"], blocks.assemble_parabolic_graph_norm_approximation(1e-14), 1e-12, "Hhat",
+                       residue=HHAT_RESIDUE)
+    x, diag = solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=1e-13))
+    nl = prob.n_lambda
+    for mine, theirs in ((x[:nl], z["lambda_delta"]), (x[nl:], z["u_delta"])):
+        assert np.abs(mine - theirs).max() <= 1e-9 * np.abs(theirs).max()
+    cells, totals = estimate(blocks)
+    scale = np.abs(z["est_eta"]).max()
+    for key, ref_key in (("flux", "est_flux"), ("divergence", "est_div"), ("reconstruction", "est_recon"),
+                         ("eta", "est_eta")):
+        assert np.abs(cells[key] - z[ref_key]).max() <= 1e-9 * scale, key
+    assert abs(totals["flux_squared"] - z["est_flux"].sum()) <= 1e-10 * z["est_flux"].sum()
+    assert abs(totals["reconstruction_squared"] - z["est_recon"].sum()) <= 1e-8 * z["est_recon"].sum()
+    xc, xt = x_marking_indicator_components(blocks)
+    xs = np.nanmax(np.abs(z["xind_eta_by_x"]))
+    for mine, theirs in (("lambda_y_squared_by_y_cell", "xind_lambda_by_y"),
+                         ("lambda_y_squared_by_x_cell", "xind_lambda_by_x"),
+                         ("initial_trace_squared_by_x_cell", "xind_trace_by_x"),
+                         ("eta_squared_by_x_cell", "xind_eta_by_x")):
+        assert np.abs(xc[mine] - np.nan_to_num(z[theirs], nan=0.0)).max() <= 1e-9 * xs, mine
