@@ -1,11 +1,16 @@
 """Benchmark: one inner iteration of the adaptive cycle of the 2+1D space-time heat problem on B200.
 
-Workload (default): 2+1D heat equation on (0,1)^2 x (0,1), u0 = sin(pi x) sin(pi y),
-f = 0, M = I, uniform space-time prism mesh of outer level 6 (2,097,152 prisms,
-n_lambda = 2,064,512, n_u = 1,048,385: 3,112,897 space-time DOFs), P1, FP64.
-Synthetic input: the mesh and DOF maps are generated on the host
-(doubleadapparabolicfem_b200.mesh.uniform_problem), with the reference's cell
-geometry and DOF counts.
+Workload (default, ``--workload refined``: the learned-preconditioner configuration the
+metric is quoted on): 2+1D heat equation on (0,1)^2 x (0,1), u0 = sin(pi x) sin(pi y),
+f = 0, P1, FP64, on a locally refined space-time mesh of about 4M DOFs
+(doubleadapparabolicfem_b200.refine.locally_refined_problem: the uniform outer-level-6 base,
+6 levels of newest-vertex bisection around a seeded interior point in the time intervals near
+it, 2 halvings of those intervals; 2.84M prisms, 4.21M DOFs, 128k hanging-node rows in X) and
+a diffusivity kappa log-uniform in [0.01, 100], constant on each square of an 8 x 8
+partition (contrast up to 1e4).  The learned preconditioner is timed as the line's value,
+the plain block preconditioner on the same steps beside it.  ``--workload uniform``: the
+uniform outer level ``--level`` mesh (default 6: 2,097,152 prisms, 3,112,897 DOFs) with
+M = I.  Synthetic inputs generated on the host.
 
 A step = the hot path of one inner iteration over one mesh, as
 compute_adaptive_test_space_iteration runs it: main-system assembly (A_y, B, B^T,
@@ -20,8 +25,13 @@ Multi-GPU: the path runs one problem per GPU (replicas; no collective in the dat
 path).  ``value`` = total DOFs processed by all ranks / max-over-ranks time.
 
 ``--impl reference`` times the reference's own CPU implementation of the same inner
-iteration (oracle/_ref/apf_ref_dump: the reference templates compiled here) on the
-host cores, on a bounded sample of the workload.
+iteration (oracle/_ref/apf_ref_dump: the reference templates compiled here) on the host
+cores, on a bounded sample of the workload: the same mesh family two outer levels coarser
+(its own local refinement at the same point, kappa of the same law), every stage of the
+reference's own code (its two-pass saddle assembly, slab reconstruction, patch solves,
+indicators) timed; its main saddle solve, which the reference runs with PARDISO (absent
+here), is not factored (the oracle shim's stand-in direct solver would dominate and is not
+the reference's code), so the reference's DOFs/s excludes the solve while ours includes it.
 """
 from __future__ import annotations
 
@@ -45,6 +55,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="refined", choices=["refined", "uniform"])
+    ap.add_argument("--seed", type=int, default=0, help="seed of the refined workload's point and kappa")
     ap.add_argument("--level", type=int, default=6)
     ap.add_argument("--p", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -138,27 +150,73 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# the refined workload: generator settings (refine.locally_refined_problem)
+REFINED = dict(depth=6, radius0=0.15, time_rounds=2, kappa_range=(0.01, 100.0), kappa_blocks=8)
+
+
+def build_problem(args):
+    if args.workload == "uniform":
+        from doubleadapparabolicfem_b200.mesh import uniform_problem
+        return uniform_problem(args.level, args.p)
+    from doubleadapparabolicfem_b200.refine import locally_refined_problem
+    if args.p != 1:
+        raise SystemExit("the refined workload is P1")
+    return locally_refined_problem(level=args.level, seed=args.seed, **REFINED)
+
+
+def workload_text(args, prob=None):
+    if args.workload == "uniform":
+        return f"2+1D heat, u0=sin(pi x)sin(pi y), M=I, uniform outer level {args.level} P{args.p}"
+    return (f"2+1D heat, u0=sin(pi x)sin(pi y), P1, outer level {args.level} base locally refined "
+            f"({REFINED['depth']} levels of bisection near a seeded point, seed {args.seed}), kappa log-uniform "
+            f"[{REFINED['kappa_range'][0]}, {REFINED['kappa_range'][1]}] on {REFINED['kappa_blocks']}x"
+            f"{REFINED['kappa_blocks']} blocks, learned vs plain preconditioner")
+
+
+def refined_point(args):
+    import numpy as np
+    return np.random.default_rng(args.seed).uniform(0.25, 0.75, 3)
+
+
 def sample_level_for(level: int) -> int:
-    """Outer level of the bounded CPU sample: level 3 (4,096 prisms, 5,625 DOFs, a few
-    seconds per inner iteration on 8 cores) for the large meshes; the reference's direct
-    solves grow superlinearly, so a larger sample would not finish in minutes."""
-    return max(1, min(3, level - 3))
+    """Outer level of the bounded CPU sample: two levels below the workload (the reference's
+    own stages at outer level 4 take a few seconds per inner iteration on 8 cores)."""
+    return max(1, level - 2)
 
 
-def cpu_reference_sample(level: int, p: int, reps: int, threads: int | None = None):
-    """Time the reference's own CPU inner iteration (oracle/_ref) on a bounded sample."""
+def cpu_reference_sample(args, reps: int, threads: int | None = None):
+    """Time the reference's own CPU inner iteration (oracle/_ref) on a bounded sample of the
+    workload: its own mesh at the sample level (refined workload: its refine_points_n_times at
+    the same point, depth rounds, kappa of the same law on the same blocks), every stage of its
+    own code; the main solve (PARDISO in the reference) is not factored."""
     exe = os.path.join(REPO, "oracle", "_ref", "apf_ref_dump")
     if not os.path.exists(exe):
         return None
     env = dict(os.environ)
     env["APF_REF_CYCLE"] = "1"
+    env["APF_SHIM_SKIP_PARDISO"] = "1"
+    if args.workload == "refined":
+        x, y, t = refined_point(args)
+        env["APF_REF_X_POINTS"] = f"{x},{y},{t}"
+        env["APF_REF_X_ROUNDS"] = str(REFINED["depth"])
+        lo, hi = REFINED["kappa_range"]
+        env["APF_REF_KAPPA"] = f"{args.seed}:{lo}:{hi}"
+        env["APF_REF_KAPPA_BLOCKS"] = str(REFINED["kappa_blocks"])
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
-    out = subprocess.run([exe, "bench", str(p), str(level), "smooth_initial", str(reps)], capture_output=True, text=True,
-                         env=env, timeout=900)
+    out = subprocess.run([exe, "bench", str(args.p), str(sample_level_for(args.level)), "smooth_initial", str(reps)],
+                         capture_output=True, text=True, env=env, timeout=1800)
     if out.returncode != 0:
         return None
-    return json.loads(out.stdout.strip().splitlines()[-1])
+    info = json.loads(out.stdout.strip().splitlines()[-1])
+    info["stages_s"] = info["mean_s"] - info.get("main_solve_mean_s", 0.0)
+    return info
+
+
+def sample_text(info, sample_level):
+    return (f"one inner iteration of the reference's own code at outer level {sample_level} of the same mesh family "
+            f"({info['n_cells']} prisms, {info['n_dofs']} DOFs): two-pass saddle assembly, slab reconstruction, "
+            f"patch flux solves, indicators; main solve (PARDISO in the reference) not factored and not timed")
 
 
 def run_reference(args, world, rank):
@@ -172,31 +230,29 @@ def run_reference(args, world, rank):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/apf_ref_dump was not built (needs the reference sources)"}))
         return
     for _ in range(args.warmup):
-        cpu_reference_sample(sample_level, args.p, 1, threads)
+        cpu_reference_sample(args, 1, threads)
     times = []
     info = None
     for _ in range(args.steps):
-        info = cpu_reference_sample(sample_level, args.p, 1, threads)
+        info = cpu_reference_sample(args, 1, threads)
         if info is None:
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/apf_ref_dump bench failed"}))
             return
-        times.append(info["mean_s"])
+        times.append(info["stages_s"])
     t = sum(times)
     value = args.steps * info["n_dofs"] / t
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"2+1D heat, u0=sin(pi x)sin(pi y), uniform outer level {args.level} P{args.p} mesh "
-                               f"(sampled at outer level {sample_level})",
-                   "stages": ["assembly", "graph_norm", "main_solve", "slab_reconstruction", "patch_fluxes",
-                              "indicators"],
-                   "solver": "the reference's main solve through the oracle shim's direct solver",
+        "config": {"workload": workload_text(args),
+                   "stages": ["assembly", "slab_reconstruction", "patch_fluxes", "indicators"],
+                   "excluded": "the main saddle solve (the reference's PARDISO / Eigen solvers are absent; "
+                               "the oracle shim's stand-in is not the reference's code)",
                    "flux_squared": info.get("flux_squared")},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["threads"], "kind": "reference",
-                         "sample": f"one inner iteration of the reference at outer level {sample_level} "
-                                   f"({info['n_cells']} prisms, {info['n_dofs']} DOFs) per step"},
+                         "sample": sample_text(info, sample_level) + " per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -210,7 +266,7 @@ def run_ours(args, world, rank, local):
     from doubleadapparabolicfem_b200 import build as b
     from doubleadapparabolicfem_b200 import _lib
     from doubleadapparabolicfem_b200.assembly import Context, MainSystemBlocks, make_desc, _Keep
-    from doubleadapparabolicfem_b200.mesh import uniform_problem, SpaceTimeProblem, Restriction
+    from doubleadapparabolicfem_b200.mesh import SpaceTimeProblem, Restriction
 
     b.build()
     torch.cuda.set_device(local)
@@ -223,7 +279,7 @@ def run_ours(args, world, rank, local):
     ctx = Context(local, stream=stream.cuda_stream)
     lib = ctx.lib
 
-    host = uniform_problem(args.level, args.p)
+    host = build_problem(args)
     n_dofs = host.n_lambda + host.n_u
     ny = host.n_y_cells
     run_estimator = not args.no_estimator
@@ -243,6 +299,7 @@ def run_ours(args, world, rank, local):
             x_restriction=Restriction(conv(host.x_restriction.offsets, np.int32), conv(host.x_restriction.dofs, np.int32),
                                       conv(host.x_restriction.weights, np.float64), host.ndof),
             n_lambda=host.n_lambda, n_u=host.n_u, u0_kind=host.u0_kind,
+            m_cells=None if host.m_cells is None else conv(host.m_cells, np.float64),
             y_vertex_ids=conv(host.y_vertex_ids, np.int32))
 
     dprob = clone_problem(to_dev)
@@ -250,6 +307,8 @@ def run_ours(args, world, rank, local):
     h2d_tensors = [hprob.y_geometry, hprob.x_geometry, hprob.y_to_x, hprob.y_restriction.offsets,
                    hprob.y_restriction.dofs, hprob.y_restriction.weights, hprob.x_restriction.offsets,
                    hprob.x_restriction.dofs, hprob.x_restriction.weights]
+    if hprob.m_cells is not None:
+        h2d_tensors.append(hprob.m_cells)
     if run_estimator:
         h2d_tensors.append(hprob.y_vertex_ids)
     h2d_bytes = sum(int(t.numel() * t.element_size()) for t in h2d_tensors)
@@ -530,14 +589,10 @@ def run_ours(args, world, rank, local):
     cpu = None
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sample_level = sample_level_for(args.level)
-        info_cpu = cpu_reference_sample(sample_level, args.p, 3, threads)
+        info_cpu = cpu_reference_sample(args, 1, threads)
         if info_cpu:
-            cpu = {"value": info_cpu["n_dofs"] / info_cpu["mean_s"], "unit": UNIT, "cores": info_cpu["threads"],
-                   "kind": "reference",
-                   "sample": f"one inner iteration of the reference (assembly, graph norm, direct main solve, "
-                             f"estimator) at outer level {sample_level} ({info_cpu['n_cells']} prisms, "
-                             f"{info_cpu['n_dofs']} DOFs), mean of 3"}
+            cpu = {"value": info_cpu["n_dofs"] / info_cpu["stages_s"], "unit": UNIT, "cores": info_cpu["threads"],
+                   "kind": "reference", "sample": sample_text(info_cpu, sample_level_for(args.level))}
     total_ms = sum(v[1] for v in kernels.values())
     spmv_roof = {"kernel": "minres_spmv_K", "bound": "hbm", "achieved": spmv_achieved, "peak": peak, "unit": "GB/s",
                  "frac": spmv_achieved / peak, "peak_kind": peak_kind,
@@ -577,8 +632,11 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"2+1D heat, u0=sin(pi x)sin(pi y), uniform outer level {args.level} P{args.p} "
-                               f"({ny} prisms, {n_dofs} DOFs)",
+        "config": {"workload": workload_text(args),
+                   "mesh": {"prisms": ny, "dofs": n_dofs, "n_lambda": host.n_lambda, "n_u": host.n_u,
+                            "hanging_x_rows": int((np.diff(host.x_restriction.offsets) > 1).sum()),
+                            **({k: host.meta[k] for k in ("point", "intervals", "spatial_triangles")}
+                               if args.workload == "refined" else {})},
                    "stages": ["assembly", "graph_norm", "amg_setup", "minres"] +
                              (["slab_reconstruction", "patch_fluxes", "indicators", "x_indicators"]
                               if run_estimator else []),
@@ -607,6 +665,13 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (mesh inputs %.0f MB; K %d nnz, Hhat %d nnz)" % (h2d_bytes / 1e6, nnz_k,
                                                                                                nnz_h)},
+        "learned_vs_plain": None if plain is None else {
+            "learned_ms_per_step": 1e3 * elapsed / args.steps, "plain_ms_per_step": plain["ms_per_step"],
+            "step_speedup": plain["ms_per_step"] / (1e3 * elapsed / args.steps),
+            "minres_iterations_learned": [d["iterations"] for d in timed_diags],
+            "minres_iterations_plain": plain["minres_iterations"],
+            "minres_solve_s_learned": sum(d["solve_seconds"] for d in timed_diags) / len(timed_diags),
+            "minres_solve_s_plain": plain["minres_solve_s_mean"]},
         "e2e": {"value": args.steps * n_dofs * world / e2e_elapsed, "unit": UNIT,
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
         "gpu_launches": launches,

@@ -204,7 +204,9 @@ namespace
     //                                    nodes with weighted CellRestriction rows;
     //   APF_REF_KAPPA="seed:lo:hi"       M(p) = kappa[K] I with kappa log-uniform in [lo, hi]
     //                                    per active X cell K (the cell found by
-    //                                    x_space.find_active_cell(p), fespace.hpp:616);
+    //                                    x_space.find_active_cell(p), fespace.hpp:616), or,
+    //                                    with APF_REF_KAPPA_BLOCKS=n, per square of an n x n
+    //                                    partition of the unit square;
     //   APF_REF_Y_PASSES=n               n passes of the reference's inner loop before the
     //                                    dump: estimate, Doerfler marking, then
     //                                    refine_test_space_from_marked_source_cells
@@ -233,6 +235,61 @@ namespace
         return v != nullptr ? std::atoi(v) : dflt;
     }
 
+    // the adaptive-mesh options on a 2+1D X space after its uniform levels (see above);
+    // returns the kappa of the active X cells (empty: M from the example)
+    template<class XSpace, class Example>
+    std::vector<double> apply_adaptive_options_2d(XSpace& x_space, Example& example)
+    {
+        if (const char* pts = std::getenv("APF_REF_X_POINTS"))
+        {
+            std::vector<typename XSpace::SpaceTimePoint> points;
+            for (const auto& p : parse_points(pts))
+                points.push_back(typename XSpace::SpaceTimePoint{p[0], p[1], p[2]});
+            adaptive_algorithm::support::refine_points_n_times(x_space, points, env_int("APF_REF_X_ROUNDS", 1));
+        }
+        std::vector<double> kx;
+        const char* ks = std::getenv("APF_REF_KAPPA");
+        const int blocks = env_int("APF_REF_KAPPA_BLOCKS", 0);
+        if (ks == nullptr)
+            return kx;
+        unsigned long long seed = 0;
+        double lo = 1.0, hi = 1.0;
+        std::sscanf(ks, "%llu:%lf:%lf", &seed, &lo, &hi);
+        std::mt19937_64 rng(seed);
+        std::uniform_real_distribution<double> uni(std::log(lo), std::log(hi));
+        if (blocks > 0)
+        {
+            // kappa constant on each of blocks x blocks squares of the unit square
+            auto table = std::make_shared<std::vector<double>>(static_cast<std::size_t>(blocks) * blocks);
+            for (auto& v : *table)
+                v = std::exp(uni(rng));
+            example.problem.M = [table, blocks](const adaptive_algorithm::examples::SpaceTime2DPoint& p) {
+                const int i = std::min(blocks - 1, std::max(0, static_cast<int>(p[0] * blocks)));
+                const int j = std::min(blocks - 1, std::max(0, static_cast<int>(p[1] * blocks)));
+                const double k = (*table)[static_cast<std::size_t>(i) * blocks + j];
+                return finite_element::coefficients::DiffusionTensor<2>{{{k, 0.0}, {0.0, k}}};
+            };
+            return *table;
+        }
+        const auto& mesh = x_space.mesh_ref();
+        auto kappa = std::make_shared<std::vector<double>>(static_cast<std::size_t>(mesh.n_cells()), 0.0);
+        for (const int c : x_space.active_cells())
+        {
+            (*kappa)[static_cast<std::size_t>(c)] = std::exp(uni(rng));
+            kx.push_back((*kappa)[static_cast<std::size_t>(c)]);
+        }
+        // the space's point-location index is built lazily on first use; build it here,
+        // before the reference's OpenMP loops call M concurrently
+        (void)x_space.find_active_cell(typename XSpace::SpaceTimePoint{0.5, 0.25, 0.5});
+        const XSpace* xs = &x_space;
+        example.problem.M = [xs, kappa](const adaptive_algorithm::examples::SpaceTime2DPoint& p) {
+            const int c = xs->find_active_cell(p);
+            const double k = (*kappa).at(static_cast<std::size_t>(c));
+            return finite_element::coefficients::DiffusionTensor<2>{{{k, 0.0}, {0.0, k}}};
+        };
+        return kx;
+    }
+
     // Times the reference's own CPU assembly path (main blocks + graph-norm block)
     // on the uniform mesh of outer level `levels`; prints one JSON line.
     template<int P>
@@ -251,6 +308,7 @@ namespace
         adaptive_algorithm::examples::initialize_spaces_from_example(x_space, y_space, example);
         for (int k = 0; k < levels; ++k)
             uniform_isotropic_refine(x_space);
+        (void)apply_adaptive_options_2d(x_space, example);
         y_space.initialize(x_space.active_cells());
         const int n_cells = static_cast<int>(y_space.active_cells().size());
         const int n_dofs = x_space.dof_handler_ref().n_true_dofs() + y_space.dof_handler_ref().n_true_dofs();
@@ -260,23 +318,32 @@ namespace
             // the reference's whole inner iteration (time_slab_adaptive_loop.hpp:727):
             // assembly, graph norm, main solve, slab reconstruction, patch flux solves,
             // indicators
-            double flux = 0.0;
+            // the main solve inside it runs the oracle shim's direct solver (the reference's
+            // own sparse solvers are Eigen / PARDISO, absent here): its time is reported
+            // separately, and the reference's own stages are the rest
+            double flux = 0.0, solve_total = 0.0;
             for (int r = 0; r < reps; ++r)
             {
                 const auto t0 = std::chrono::steady_clock::now();
                 typename Backend::Solver solver;
                 la::concepts::SolverOptions opts;
+                // the production runs' main solver (main_solver: pardiso_ldlt in the example
+                // configurations); the shim factors it unless APF_SHIM_SKIP_PARDISO is set
+                opts.solver = la::concepts::SolverType::PardisoLDLT;
                 finite_element::time_slabs::AdaptiveTestSpaceIterationParameters<Backend, XSpace, YSpace> params;
                 const auto state = finite_element::time_slabs::compute_adaptive_test_space_iteration<QSpace, QTime, Backend>(
                     y_space, x_space, example.problem, solver, opts, params);
                 const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
                 best = std::min(best, dt);
                 total += dt;
+                solve_total += state.main_solve_setup_seconds + state.main_solve_solve_seconds;
                 flux = state.flux_diagnostics.total_flux();
             }
             std::printf("{\"stage\": \"inner_iteration\", \"p\": %d, \"level\": %d, \"n_cells\": %d, \"n_dofs\": %d, "
-                        "\"reps\": %d, \"mean_s\": %.6f, \"best_s\": %.6f, \"threads\": %d, \"flux_squared\": %.12e}\n",
-                        P, levels, n_cells, n_dofs, reps, total / reps, best, omp_get_max_threads(), flux);
+                        "\"reps\": %d, \"mean_s\": %.6f, \"best_s\": %.6f, \"main_solve_mean_s\": %.6f, "
+                        "\"threads\": %d, \"flux_squared\": %.12e}\n",
+                        P, levels, n_cells, n_dofs, reps, total / reps, best, solve_total / reps, omp_get_max_threads(),
+                        flux);
             return 0;
         }
         for (int r = 0; r < reps; ++r)
@@ -314,41 +381,12 @@ namespace
         adaptive_algorithm::examples::initialize_spaces_from_example(x_space, y_space, example);
         for (int k = 0; k < levels; ++k)
             uniform_isotropic_refine(x_space);
-        if (const char* pts = std::getenv("APF_REF_X_POINTS"))
-        {
-            std::vector<typename XSpace::SpaceTimePoint> points;
-            for (const auto& p : parse_points(pts))
-                points.push_back(typename XSpace::SpaceTimePoint{p[0], p[1], p[2]});
-            adaptive_algorithm::support::refine_points_n_times(x_space, points, env_int("APF_REF_X_ROUNDS", 1));
-        }
+        const std::vector<double> kx = apply_adaptive_options_2d(x_space, example);
         y_space.initialize(x_space.active_cells());
 
         std::filesystem::create_directories(dir);
-        if (const char* ks = std::getenv("APF_REF_KAPPA"))
-        {
-            unsigned long long seed = 0;
-            double lo = 1.0, hi = 1.0;
-            std::sscanf(ks, "%llu:%lf:%lf", &seed, &lo, &hi);
-            std::mt19937_64 rng(seed);
-            std::uniform_real_distribution<double> uni(std::log(lo), std::log(hi));
-            auto kappa = std::make_shared<std::vector<double>>(static_cast<std::size_t>(mesh.n_cells()), 0.0);
-            std::vector<double> kx;
-            for (const int c : x_space.active_cells())
-            {
-                (*kappa)[static_cast<std::size_t>(c)] = std::exp(uni(rng));
-                kx.push_back((*kappa)[static_cast<std::size_t>(c)]);
-            }
+        if (!kx.empty())
             apf_oracle::write_npy(dir + "/kappa_x.npy", kx);
-            // the space's point-location index is built lazily on first use; build it here,
-            // before the reference's OpenMP loops call M concurrently
-            (void)x_space.find_active_cell(typename XSpace::SpaceTimePoint{0.5, 0.25, 0.5});
-            const XSpace* xs = &x_space;
-            example.problem.M = [xs, kappa](const adaptive_algorithm::examples::SpaceTime2DPoint& p) {
-                const int c = xs->find_active_cell(p);
-                const double k = (*kappa).at(static_cast<std::size_t>(c));
-                return finite_element::coefficients::DiffusionTensor<2>{{{k, 0.0}, {0.0, k}}};
-            };
-        }
         for (int pass = 0; pass < env_int("APF_REF_Y_PASSES", 0); ++pass)
         {
             typename Backend::Solver solver;

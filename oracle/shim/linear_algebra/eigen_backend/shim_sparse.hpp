@@ -1,4 +1,5 @@
 #pragma once
+#include <cstdlib>
 // ORACLE SHIM (test infrastructure only; never linked into the product library).
 //
 // std-only stand-ins for the sparse part of the reference's Eigen wrapper API
@@ -598,6 +599,19 @@ namespace la::eigen
                 throw std::invalid_argument("Solver::compute refuses to factor a linear system with zero rows or zero columns.");
             if (options.solver == la::concepts::SolverType::MINRES)
                 throw std::invalid_argument("The generic solver wrapper does not construct MINRES.");
+            // Stage timing of the reference's own code (bench.py --impl reference): with
+            // APF_SHIM_SKIP_PARDISO=1 the shim does not factor systems whose options request
+            // PARDISO (the production runs' main saddle solver, absent here, as is Eigen's);
+            // solve() then returns its right-hand side as a placeholder.  The SparseLU
+            // requests of the reference's own stages (slab reconstruction, local solves) are
+            // factored as always.  Off unless set.
+            static const bool skip_pardiso = std::getenv("APF_SHIM_SKIP_PARDISO") != nullptr;
+            skipped_ = skip_pardiso && options.solver != la::concepts::SolverType::SparseLU;
+            if (skipped_)
+            {
+                computed_ = true;
+                return;
+            }
             // PARDISO variants and SparseLU all map to the shim's exact direct solver.
             const auto t0 = std::chrono::steady_clock::now();
             direct_.compute(A);
@@ -613,6 +627,12 @@ namespace la::eigen
             if (!computed_)
                 throw std::runtime_error("Solver::solve called before compute.");
             x.resize(b.size());
+            if (skipped_)
+            {
+                for (int i = 0; i < b.size(); ++i)
+                    x[i] = b[i];
+                return;
+            }
             direct_.solve(b.data(), x.data());
         }
         void solve_with_initial_guess(const VectorType& b, const VectorType& guess, VectorType& x) const
@@ -624,6 +644,7 @@ namespace la::eigen
 
     private:
         bool computed_ = false;
+        bool skipped_ = false;
         shim_detail::SparseDirect direct_{};
         mutable Diagnostics diagnostics_{};
     };
