@@ -14,7 +14,10 @@ Objects:
   sweeps);
 * ``loss(...)``: sum over the two blocks of mean_e (1/k) log(||E^k e||_T^2 / ||e||_T^2),
   E = I - V T;
-* ``fd_gradient(...)``: central finite differences of ``loss``.
+* ``fd_gradient(...)``: central finite differences of ``loss``;
+* ``loss_and_grad_fp64(...)``: the same loss and its exact gradient, in FP64 by reverse mode
+  (torch autograd on the CPU) through the MLP, the weights and every V-cycle, with the
+  Gershgorin rescale factor held constant, as the device's backward pass treats it.
 """
 from __future__ import annotations
 
@@ -160,3 +163,102 @@ def fd_gradient(params, indices, hierarchies, targets, starts_per_block, steps: 
         p[i] = old
         g[k] = (lp - lm) / (2 * h)
     return g
+
+
+# ----------------------------------------------------------------------------------------
+# exact FP64 gradient (reverse mode)
+# ----------------------------------------------------------------------------------------
+def _torch_sparse(A):
+    import torch
+    A = A.tocoo()
+    idx = torch.tensor(np.vstack([A.row, A.col]), dtype=torch.int64)
+    return torch.sparse_coo_tensor(idx, torch.tensor(A.data, dtype=torch.float64), A.shape,
+                                   check_invariants=False).coalesce()
+
+
+def _torch_ops(H):
+    """Sparse operators of a hierarchy as torch tensors (built once per hierarchy)."""
+    if getattr(H, "_torch", None) is None:
+        import torch
+        H._torch = {
+            "A": [_torch_sparse(A) for A in H.A],
+            "absA": [_torch_sparse(abs(A)) for A in H.A],
+            "P": [None if P is None else _torch_sparse(P) for P in H.P],
+            "PT": [None if P is None else _torch_sparse(P.T.tocsr()) for P in H.P],
+            "d": [torch.tensor(A.diagonal(), dtype=torch.float64) for A in H.A],
+            "F": [torch.tensor(F, dtype=torch.float64) for F in H.F],
+            "Cinv": None if H.Cinv is None else torch.tensor(H.Cinv, dtype=torch.float64),
+        }
+    return H._torch
+
+
+def _mv(A, x):
+    import torch
+    return torch.sparse.mm(A, x.unsqueeze(1)).squeeze(1)
+
+
+def loss_and_grad_fp64(params, hierarchies, targets, starts_per_block, steps: int):
+    """(loss, d loss / d params) in FP64, the gradient exact up to rounding."""
+    import torch
+    p = torch.tensor(np.asarray(params, dtype=np.float64), requires_grad=True)
+    w1 = p[W1:B1].reshape(HIDDEN, N_FEATURES)
+    b1 = p[B1:W2]
+    w2 = p[W2:B2].reshape(HIDDEN, HIDDEN)
+    b2 = p[B2:W3]
+    w3 = p[W3:B3].reshape(OUTPUTS, HIDDEN)
+    b3 = p[B3:ALPHA]
+    total = torch.zeros((), dtype=torch.float64)
+    for H, T, S in zip(hierarchies, targets, starts_per_block):
+        ops = _torch_ops(H)
+        L = len(H.A)
+        W, AL = [], []
+        for l in range(L - 1):
+            y = torch.tanh(torch.tanh(ops["F"][l] @ w1.T + b1) @ w2.T + b2) @ w3.T + b3
+            ws = []
+            for o in range(OUTPUTS):
+                w = H.omega[l] / ops["d"][l] * torch.exp(WEIGHT_RANGE * torch.tanh(y[:, o]))
+                with torch.no_grad():
+                    sw = torch.sqrt(w)
+                    g = float((sw * _mv(ops["absA"][l], sw)).max())
+                if g > SMOOTHER_BOUND:
+                    w = w * (SMOOTHER_BOUND / g)     # a constant factor: no gradient through the bound
+                ws.append(w)
+            W.append(ws)
+            th = p[ALPHA + H.block * MAX_LEVELS + min(l, MAX_LEVELS - 1)]
+            AL.append(2.0 / (1.0 + torch.exp(-th)))
+
+        def coarse(b):
+            if H.dense:
+                return ops["Cinv"] @ b
+            w = H.omega[-1] / ops["d"][-1]
+            x = w * b
+            for _ in range(H.sweeps - 1):
+                x = x + w * (b - _mv(ops["A"][-1], x))
+            return x
+
+        def vcycle(b, l=0):
+            if l == L - 1:
+                return coarse(b)
+            A, w, s_ = ops["A"][l], W[l], H.smooth_steps
+            cls = [0] + [1] * (s_ - 1)
+            x = w[0] * b
+            for k in range(1, s_):
+                x = x + w[cls[k]] * (b - _mv(A, x))
+            xc = vcycle(_mv(ops["PT"][l], b - _mv(A, x)), l + 1)
+            x = x + AL[l] * _mv(ops["P"][l], xc)
+            for k in range(s_):
+                x = x + w[cls[s_ - 1 - k]] * (b - _mv(A, x))
+            return x
+
+        Tt = _torch_sparse(T)
+        acc = torch.zeros((), dtype=torch.float64)
+        for e0 in S:
+            e = torch.tensor(e0, dtype=torch.float64)
+            q0 = e @ _mv(Tt, e)
+            for _ in range(steps):
+                e = e - vcycle(_mv(Tt, e))
+            qk = e @ _mv(Tt, e)
+            acc = acc + (torch.log(qk) - torch.log(q0)) / steps
+        total = total + acc / len(S)
+    total.backward()
+    return float(total.detach()), p.grad.detach().numpy().copy()
