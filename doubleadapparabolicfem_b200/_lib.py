@@ -75,6 +75,7 @@ class SolverOptions(C.Structure):
         ("amg_strength", C.c_double),
         ("amg_coarse_size", C.c_int),
         ("amg_aggressive_levels", C.c_int),
+        ("amg_vcycles", C.c_int),
     ]
 
 

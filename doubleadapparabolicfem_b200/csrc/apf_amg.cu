@@ -4,7 +4,9 @@
 // same component (the time-local index of a Y DOF: the broken-in-time test space makes
 // (1,-1) across the two time sides of a node a lower-energy mode than the constant, so the
 // sides are aggregated separately and each keeps its own constant near-nullspace vector);
-// aggregates from a distance-1 maximal independent set (hash priorities, deterministic);
+// aggregates from a distance-1 maximal independent set (hash priorities, deterministic; a
+// level whose strong graph no longer coarsens -- coefficient jumps cut it into small pieces --
+// is aggregated again with every coupling inside a component counted as strong);
 // tentative prolongator T (one 1 per row); P = (I - omega D_F^-1 A_F) T with the filtered
 // operator A_F (weak entries lumped onto the diagonal); A_c = P^T A P.  The coarsest
 // operator is inverted densely on the device once per setup (Gauss-Jordan, one launch per
@@ -437,6 +439,24 @@ namespace apf
         // k = 0..n-1 the array holds A^-1.  An SPD matrix needs no pivoting (every pivot is a
         // diagonal entry of a Schur complement, hence positive); a pivot that is not positive
         // and finite sets *status and the step leaves B = A.
+        // C = (C + C^T) / 2 for a dense n x n row-major matrix: the inverse of a symmetric matrix
+        // computed in finite precision is symmetric only up to cond(A) eps, and the coarse
+        // solve must be exactly symmetric for the V-cycle to stay a symmetric operator
+        __global__ void symmetrize_dense(int n, double* __restrict__ C)
+        {
+            const long long total = static_cast<long long>(n) * n;
+            for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+                 e += (long long)gridDim.x * blockDim.x)
+            {
+                const int i = static_cast<int>(e / n), j = static_cast<int>(e % n);
+                if (j <= i)
+                    continue;
+                const double v = 0.5 * (C[(long long)i * n + j] + C[(long long)j * n + i]);
+                C[(long long)i * n + j] = v;
+                C[(long long)j * n + i] = v;
+            }
+        }
+
         __global__ void gauss_jordan_step(int n, int k, const double* __restrict__ A, double* __restrict__ B,
                                           int* __restrict__ status)
         {
@@ -481,6 +501,9 @@ namespace apf
         }
         w.ensure(s);
         bool force_dense = false, force_jacobi = false;
+        // a level whose strong graph no longer coarsens (coefficient jumps split it into many
+        // small pieces) is aggregated once more with every coupling of its component strong
+        bool weak_retry = false;
         jacobi_coarse_ = false;
         for (int l = 0;; ++l)
         {
@@ -537,6 +560,10 @@ namespace apf
                 }
                 if (cur != coarse_inv_.get())
                     APF_CUDA(cudaMemcpyAsync(coarse_inv_.get(), cur, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                {
+                    APF_KERNEL("amg_coarse_symmetrize", s);
+                    symmetrize_dense<<<gj_blocks, 256, 0, s>>>(n, coarse_inv_.get());
+                }
                 APF_CUDA(cudaGetLastError());
                 int bad = 0;
                 APF_CUDA(cudaMemcpyAsync(&bad, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -552,7 +579,7 @@ namespace apf
                 diag_kernel<<<nblocks(n, 256), 256, 0, s>>>(n, Al.row_ptr.get(), Al.col_idx.get(), Al.values.get(), diag.get());
             }
             L.omega = 4.0 / (3.0 * spectral_radius(s, Al));
-            const Strength st{diag.get(), opt.strength, L.comp.size() ? L.comp.get() : nullptr};
+            const Strength st{diag.get(), weak_retry ? 0.0 : opt.strength, L.comp.size() ? L.comp.get() : nullptr};
             // aggregation
             DeviceBuffer<int> st0(n, s), st1(n, s), cnt(1, s);
             {
@@ -598,6 +625,13 @@ namespace apf
             const int nc = static_cast<int>(exclusive_scan(flag.get(), pos.get(), n, s));
             if (nc == 0 || nc > (4 * static_cast<long long>(n)) / 5)
             {
+                if (!weak_retry && opt.strength > 0.0 && n > kMaxDense)
+                {
+                    weak_retry = true;
+                    --l;
+                    continue;
+                }
+                weak_retry = false;
                 // coarsening stalls: this level becomes the coarsest one
                 if (n <= kMaxDense)
                     force_dense = true;
@@ -606,6 +640,7 @@ namespace apf
                 --l;
                 continue;
             }
+            weak_retry = false; // the next level starts from the configured strength again
             DeviceBuffer<int> comp_c;
             if (st.comp)
                 comp_c.allocate(nc, s);

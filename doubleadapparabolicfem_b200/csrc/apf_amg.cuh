@@ -18,6 +18,9 @@ namespace apf
         // levels (from the finest) whose aggregates come from a distance-2 independent set
         // (roots two strong edges apart: larger aggregates, fewer coarse unknowns)
         int aggressive_levels = 0;
+        // V-cycles per application in the block preconditioner (1, or 2: the scaled two-step
+        // iteration, see BlockPreconditioner::apply)
+        int vcycles = 1;
     };
 
     struct AmgLevel

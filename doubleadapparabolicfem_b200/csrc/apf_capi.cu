@@ -715,6 +715,7 @@ void apf_solver_options_default(apf_solver_options* opt)
     opt->amg_strength = 0.08;
     opt->amg_coarse_size = 256;
     opt->amg_aggressive_levels = 1;
+    opt->amg_vcycles = 1;
 }
 
 namespace
@@ -726,6 +727,7 @@ namespace
         a.strength = o->amg_strength;
         a.coarse_size = std::max(16, o->amg_coarse_size);
         a.aggressive_levels = std::max(0, o->amg_aggressive_levels);
+        a.vcycles = std::min(2, std::max(1, o->amg_vcycles));
         return a;
     }
 
@@ -820,6 +822,7 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
         mo.batch = opt->use_true_residual_batching ? opt->true_residual_check_interval : opt->max_iterations;
         mo.parts = S.partition.n_parts > 0 ? &S.partition : nullptr;
         const auto t0 = std::chrono::steady_clock::now();
+        S.precond->prepare(s, S.ws);
         summary = apf::minres_solve(s, S.blocks[APF_BLOCK_K], *S.precond, S.rhs.get(), S.solution.get(), mo, S.ws);
         used = S.precond_kind;
         if (!summary.converged && S.precond_kind == APF_PRECOND_LEARNED)
@@ -827,6 +830,7 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
             // the plain block preconditioner is the fallback: a fresh run from the learned
             // run's iterate
             install_smoothers(ctx, S, APF_PRECOND_AMG_BLOCK);
+            S.precond->prepare(s, S.ws);
             const apf::MinresSummary first = summary;
             summary = apf::minres_solve(s, S.blocks[APF_BLOCK_K], *S.precond, S.rhs.get(), S.solution.get(), mo, S.ws);
             summary.iterations += first.iterations;
@@ -888,10 +892,9 @@ int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const dou
         apf::DeviceBuffer<double> dr(n, s), dz(n, s);
         APF_CUDA(cudaMemcpyAsync(dr.get(), r, n * sizeof(double),
                                  pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-        if (block == 0)
-            S.precond->amg_a.apply(s, dr.get(), dz.get());
-        else if (block == 1)
-            S.precond->amg_h.apply(s, dr.get(), dz.get());
+        S.precond->prepare(s, S.ws);
+        if (block < 2)
+            S.precond->apply_block(s, block, dr.get(), dz.get());
         else
             S.precond->apply(s, dr.get(), dz.get());
         APF_CUDA(cudaMemcpyAsync(z, dz.get(), n * sizeof(double),

@@ -392,6 +392,89 @@ namespace apf
         }
         build_sell(s, hhat_f);
         amg_h.setup(s, hhat_f, opt, w, x_component);
+        A_y_ = &A_y;
+        H_ = &Hhat;
+        vcycles = opt.vcycles;
+        scale_a = scale_h = 1.0;
+        if (vcycles == 2)
+        {
+            t_a_.allocate(n_lambda, s);
+            w_a_.allocate(n_lambda, s);
+            t_h_.allocate(n_u, s);
+            w_h_.allocate(n_u, s);
+        }
+    }
+
+    namespace
+    {
+        // a fixed start vector with entries in [-1, 1] (integer hash of the index)
+        __global__ void hash_fill_kernel(int n, double* x)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            {
+                unsigned h = static_cast<unsigned>(i) * 2654435761u + 0x9e3779b9u;
+                h ^= h >> 15;
+                h *= 2246822519u;
+                h ^= h >> 13;
+                x[i] = static_cast<double>(h) / 2147483648.0 - 1.0;
+            }
+        }
+    }
+
+    void BlockPreconditioner::prepare(cudaStream_t s, Workspace& w)
+    {
+        if (vcycles != 2)
+            return;
+        // lambda_max(V A) by 15 power steps (V and A SPD: V A is similar to an SPD matrix, its
+        // eigenvalues are positive, the power method converges to the largest from below; the
+        // factor 1.1 and the two-step polynomial's margin (positive up to mu = 2) cover the gap)
+        auto estimate = [&](Amg& amg, const DeviceCsr& A, int n, double* x, double* y) {
+            if (n == 0)
+                return 1.0;
+            {
+                APF_KERNEL("precond_power_start", s);
+                hash_fill_kernel<<<static_cast<int>(std::min<long long>((n + 255) / 256, 148 * 16)), 256, 0, s>>>(n, x);
+            }
+            double nx = std::sqrt(dot_host(s, w, n, x, x));
+            double lam = 1.0;
+            for (int it = 0; it < 15; ++it)
+            {
+                spmv(s, A, x, y);      // y = A x
+                amg.apply(s, y, x);    // x = V A x_old
+                const double nz = std::sqrt(dot_host(s, w, n, x, x));
+                require(std::isfinite(nz) && nz > 0.0, APF_ERR_NUMERIC, "preconditioner power iteration broke down");
+                lam = nz / nx;
+                axpby(s, n, 1.0 / nz, x, 0.0, x);
+                nx = 1.0;
+            }
+            return lam;
+        };
+        scale_a = 1.0 / (1.1 * estimate(amg_a, *A_y_, n_lambda, t_a_.get(), w_a_.get()));
+        scale_h = 1.0 / (1.1 * estimate(amg_h, *H_, n_u, t_h_.get(), w_h_.get()));
+        APF_CUDA(cudaGetLastError());
+    }
+
+    void BlockPreconditioner::apply_block(cudaStream_t s, int block, const double* r, double* z)
+    {
+        Amg& amg = block == 0 ? amg_a : amg_h;
+        if (vcycles != 2)
+        {
+            amg.apply(s, r, z);
+            return;
+        }
+        // z = c V r;  z += c V (r - A z): the two-step iteration from zero, the operator
+        // c V (2 I - c A V), symmetric, with the eigenvalues 2 mu - mu^2 > 0 of its product with
+        // A for mu = c lambda(V A) in (0, 1)
+        const int n = block == 0 ? n_lambda : n_u;
+        const DeviceCsr& A = block == 0 ? *A_y_ : *H_;
+        const double c = block == 0 ? scale_a : scale_h;
+        double* t = block == 0 ? t_a_.get() : t_h_.get();
+        double* v = block == 0 ? w_a_.get() : w_h_.get();
+        amg.apply(s, r, z);
+        axpby(s, n, c, z, 0.0, z);
+        residual(s, A, z, r, t);
+        amg.apply(s, t, v);
+        axpby(s, n, c, v, 1.0, z);
     }
 
     BlockPreconditioner::~BlockPreconditioner()
@@ -412,14 +495,14 @@ namespace apf
             // per-launch event timing: both V-cycles on the caller's stream, one after the
             // other, so that each launch's duration is its own (no overlap with the other
             // block's launches sharing the GPU)
-            amg_h.apply(s, r + n_lambda, z + n_lambda);
-            amg_a.apply(s, r, z);
+            apply_block(s, 1, r + n_lambda, z + n_lambda);
+            apply_block(s, 0, r, z);
             return;
         }
         APF_CUDA(cudaEventRecord(fork_, s));
         APF_CUDA(cudaStreamWaitEvent(side_, fork_, 0));
-        amg_h.apply(side_, r + n_lambda, z + n_lambda);
-        amg_a.apply(s, r, z);
+        apply_block(side_, 1, r + n_lambda, z + n_lambda);
+        apply_block(s, 0, r, z);
         APF_CUDA(cudaEventRecord(join_, side_));
         APF_CUDA(cudaStreamWaitEvent(s, join_, 0));
     }

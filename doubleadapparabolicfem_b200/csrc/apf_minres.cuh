@@ -29,14 +29,25 @@ namespace apf
         void setup(cudaStream_t s, const DeviceCsr& A_y, const DeviceCsr& Hhat, const AmgOptions& opt, Workspace& w,
                    const int* y_component = nullptr, const int* x_component = nullptr);
         void apply(cudaStream_t s, const double* r, double* z) override;
+        // one block's operator alone (block 0: A_y part, 1: Hhat part)
+        void apply_block(cudaStream_t s, int block, const double* r, double* z);
+        // before a solve (outside any stream capture): with two V-cycles per application,
+        // the scale 1 / (1.1 lambda_max(V A)) of each block from a power iteration on the
+        // current smoothers
+        void prepare(cudaStream_t s, Workspace& w);
         int n_lambda = 0, n_u = 0;
         Amg amg_a, amg_h;
         DeviceCsr hhat_f; // filtered SPD operator the Hhat hierarchy is built on
         static constexpr double kHhatDrop = 0.01;
+        int vcycles = 1;
+        double scale_a = 1.0, scale_h = 1.0;
 
     private:
         cudaStream_t side_ = nullptr;
         cudaEvent_t fork_ = nullptr, join_ = nullptr;
+        const DeviceCsr* A_y_ = nullptr;
+        const DeviceCsr* H_ = nullptr;
+        DeviceBuffer<double> t_a_, w_a_, t_h_, w_h_;
     };
 
     // Independent problems stacked block-diagonally in K: segment 2p covers part p's lambda

@@ -249,12 +249,23 @@ def train(ctx: Context, systems, model: LearnedModel, epochs: int = 10, lr: floa
     return history
 
 
+def refined_training_problem(k: int, levels=(3, 4)):
+    """The k-th locally refined training system: outer level from `levels`, 3 to 5 levels of
+    bisection near a seeded point, diffusivity log-uniform in [0.01, 100] on 4x4 or 8x8 blocks
+    (refine.locally_refined_problem; 30k-250k DOFs)."""
+    from .refine import locally_refined_problem
+    level = levels[k % len(levels)]
+    return locally_refined_problem(level=level, seed=20_000 + k, depth=3 + k % 3, radius0=0.2,
+                                   time_rounds=1 + k % 2, kappa_blocks=4 if (k // 2) % 2 else 8)
+
+
 def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, levels=(3, 4), epochs: int = 40,
                         lr: float = 1e-2, seed: int = 0, device: int = 0, log=print, steps: int = 4,
-                        burn_in: int = 8):
+                        burn_in: int = 8, n_refined: int = 0):
     """Train the shipped model on method-generated systems: uniform meshes of the given outer
     levels with seeded random piecewise-constant diffusivity (log-uniform in [0.01, 100] on
-    4x4 or 8x8 blocks), plus the constant-diffusivity mesh of each level."""
+    4x4 or 8x8 blocks), the constant-diffusivity mesh of each level, and n_refined locally
+    refined systems with such a diffusivity (refined_training_problem)."""
     from .assembly import assemble_main_system_blocks
     from .solver import SolverOptions, setup_preconditioner
     ctx = Context(device)
@@ -264,6 +275,7 @@ def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, leve
         prob = random_kappa_problem(level, seed=10_000 + k, blocks_per_side=4 if k % 2 else 8)
         systems.append(prob)
     systems += [uniform_problem(level, 1) for level in levels]
+    systems += [refined_training_problem(k, levels) for k in range(n_refined)]
     blocks = []
     for prob in systems:
         b = assemble_main_system_blocks(prob, ctx=ctx)
@@ -274,7 +286,7 @@ def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, leve
     hist = train(ctx, blocks, model, epochs=epochs, lr=lr, samples=2, steps=steps, seed=seed, log=log,
                  burn_in=burn_in)
     model.save(out_path, history=np.asarray(hist), levels=np.asarray(levels), n_train=n_train, epochs=epochs,
-               steps=steps, burn_in=burn_in)
+               steps=steps, burn_in=burn_in, n_refined=n_refined)
     return model, hist
 
 
@@ -319,6 +331,7 @@ if __name__ == "__main__":
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--burn-in", type=int, default=8)
+    ap.add_argument("--refined", type=int, default=0, help="locally refined high-contrast systems added to the set")
     ap.add_argument("--evaluate", type=int, default=None, metavar="LEVEL",
                     help="instead of training: learned vs plain on seeded random-kappa systems of this level")
     a = ap.parse_args()
@@ -327,4 +340,4 @@ if __name__ == "__main__":
         print(json.dumps(evaluate(a.evaluate)))
         raise SystemExit(0)
     train_default_model(a.out, a.n_train, tuple(int(x) for x in a.levels.split(",")), a.epochs, a.lr, a.seed,
-                        steps=a.steps, burn_in=a.burn_in)
+                        steps=a.steps, burn_in=a.burn_in, n_refined=a.refined)

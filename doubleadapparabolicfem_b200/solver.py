@@ -32,6 +32,7 @@ class SolverOptions:
     amg_strength: float = 0.08
     amg_coarse_size: int = 256
     amg_aggressive_levels: int = 1
+    amg_vcycles: int = 1
 
     def to_c(self) -> _lib.SolverOptions:
         o = _lib.SolverOptions()
@@ -44,6 +45,7 @@ class SolverOptions:
         o.amg_strength = self.amg_strength
         o.amg_coarse_size = self.amg_coarse_size
         o.amg_aggressive_levels = self.amg_aggressive_levels
+        o.amg_vcycles = self.amg_vcycles
         return o
 
 

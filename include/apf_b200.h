@@ -198,6 +198,12 @@ typedef struct apf_solver_options
     int amg_coarse_size;              /* dense coarsest solve at or below this size */
     int amg_aggressive_levels;        /* finest levels aggregated from a distance-2 independent set
                                          (larger aggregates, cheaper V-cycles); default 1, 0 = distance 1 */
+    int amg_vcycles;                  /* V-cycles per block application: 1 (default) = z = V r; 2 = the
+                                         two-step iteration z = s V r, z += s V (r - A z) with
+                                         s = 1 / (1.1 lambda_max(V A)) estimated by power iteration
+                                         before every solve: a fixed SPD operator (eigenvalues of its
+                                         product with A: 2 mu - mu^2, mu in (0, 1)) with about half the
+                                         condition number, for high-contrast coefficients */
 } apf_solver_options;
 
 /* Mirrors SolverDiagnostics.iterative_stats (src/linear_algebra/concepts/solver.hpp:186-197). */
