@@ -8,7 +8,8 @@ f = 0, P1, FP64, on a locally refined space-time mesh of about 4M DOFs
 it, 2 halvings of those intervals; 2.84M prisms, 4.21M DOFs, 128k hanging-node rows in X) and
 a diffusivity kappa log-uniform in [0.01, 100], constant on each square of a 4 x 4
 partition (contrast up to 1e4).  The learned preconditioner is timed as the line's value,
-the plain block preconditioner on the same steps beside it.  ``--workload uniform``: the
+the plain block preconditioner on the same steps beside it; both build their AMG
+hierarchies with strength threshold 0.003 (REFINED_AMG_STRENGTH).  ``--workload uniform``: the
 uniform outer level ``--level`` mesh (default 6: 2,097,152 prisms, 3,112,897 DOFs) with
 M = I.  Synthetic inputs generated on the host.
 
@@ -69,7 +70,7 @@ def parse():
     ap.add_argument("--amg-smooth-steps", type=int, default=None,
                     help="damped-Jacobi sweeps per side of the V-cycle (default: the library's)")
     ap.add_argument("--amg-strength", type=float, default=None,
-                    help="AMG strength-of-connection threshold (default: the library's)")
+                    help="AMG strength-of-connection threshold (default: the library's; the refined workload: 0.003)")
     ap.add_argument("--amg-aggressive-levels", type=int, default=None,
                     help="finest AMG levels aggregated from a distance-2 independent set (default: the library's)")
     ap.add_argument("--precond", default="learned", choices=["learned", "plain"],
@@ -152,6 +153,11 @@ def measured_peaks():
 
 # the refined workload: generator settings (refine.locally_refined_problem)
 REFINED = dict(depth=6, radius0=0.15, time_rounds=2, kappa_range=(0.01, 100.0), kappa_blocks=4)
+# AMG strength-of-connection threshold for the refined workload (both preconditioners): with
+# kappa jumps of 1e4 across block edges and cells graded over six bisection levels, the default
+# 0.08 drops too many couplings; a sweep over {0.08, 0.02, 0.01, 0.005, 0.003, 0.002, 0} gave the
+# fewest MINRES iterations for plain and learned at 0.003
+REFINED_AMG_STRENGTH = 0.003
 # steps of the plain-preconditioner comparison and of the e2e measurement (at most; a step of
 # the refined workload takes seconds, the plain solver's many more)
 PLAIN_STEPS, E2E_STEPS = 2, 3
@@ -331,6 +337,8 @@ def run_ours(args, world, rank, local):
         sopt.amg_smooth_steps = args.amg_smooth_steps
     if args.amg_strength is not None:
         sopt.amg_strength = args.amg_strength
+    elif args.workload == "refined":
+        sopt.amg_strength = REFINED_AMG_STRENGTH
     from doubleadapparabolicfem_b200 import learned as LM
     learned_model = None
     if args.precond == "learned" and os.path.exists(LM.DEFAULT_WEIGHTS):

@@ -787,8 +787,33 @@ int apf_setup_preconditioner(apf_ctx* ctx, apf_system* sys, const apf_solver_opt
     return guarded(ctx, [&] { setup_precond(ctx, sys, opt); });
 }
 
+namespace
+{
+    // MINRES on the system's K; rhs NULL = the assembled [f; g]
+    int solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* rhs,
+                     const double* initial_guess, double* solution, int pointers_on_device,
+                     apf_solver_diagnostics* diag);
+}
+
 int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* initial_guess,
                      double* solution, int pointers_on_device, apf_solver_diagnostics* diag)
+{
+    return solve_minres(ctx, sys, opt, nullptr, initial_guess, solution, pointers_on_device, diag);
+}
+
+int apf_solve_minres_with_rhs(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* rhs,
+                              const double* initial_guess, double* solution, int pointers_on_device,
+                              apf_solver_diagnostics* diag)
+{
+    if (!rhs)
+        return APF_ERR_INVALID;
+    return solve_minres(ctx, sys, opt, rhs, initial_guess, solution, pointers_on_device, diag);
+}
+
+namespace
+{
+int solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* rhs,
+                 const double* initial_guess, double* solution, int pointers_on_device, apf_solver_diagnostics* diag)
 {
     if (!ctx || !sys || !opt)
         return APF_ERR_INVALID;
@@ -806,8 +831,14 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
             install_smoothers(ctx, S, opt->preconditioner);
         const int nl = S.in.n_lambda, nu = S.in.n_u, n = nl + nu;
         S.rhs.allocate(n, s);
-        apf::copy(s, nl, S.f.get(), S.rhs.get());
-        apf::copy(s, nu, S.g.get(), S.rhs.get() + nl);
+        if (rhs)
+            APF_CUDA(cudaMemcpyAsync(S.rhs.get(), rhs, n * sizeof(double),
+                                     pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        else
+        {
+            apf::copy(s, nl, S.f.get(), S.rhs.get());
+            apf::copy(s, nu, S.g.get(), S.rhs.get() + nl);
+        }
         S.solution.allocate(n, s);
         if (initial_guess)
             APF_CUDA(cudaMemcpyAsync(S.solution.get(), initial_guess, n * sizeof(double),
@@ -876,6 +907,7 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
         rc = APF_ERR_NOT_CONVERGED;
     }
     return rc;
+}
 }
 
 int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const double* r, double* z,

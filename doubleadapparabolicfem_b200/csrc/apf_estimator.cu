@@ -241,6 +241,8 @@ namespace apf
             double mmm[3][3][3];                   // int lambda_a lambda_s lambda_r
         };
         constexpr int kPatchTableDoubles = sizeof(PatchTables) / sizeof(double);
+        // local entries of one patch cell (the index t of the patch kernels' entry loop)
+        constexpr int kCellEntries = 113;
 
         PatchTables make_patch_tables(const EstTables& t)
         {
@@ -364,8 +366,8 @@ namespace apf
         // F32 = true: the matrix is assembled and factored in FP32 (half the shared memory per
         // team, so twice the teams per SM), followed by one FP64 iterative-refinement step:
         // the FP64 residual Mt^-1 b - K x is formed matrix-free by a second pass over the
-        // patch cells' local entries (FP64 shared-memory atomics), solved with the FP32
-        // factors and pivots, and added to x in FP64.
+        // patch cells' local entries (row sums in a fixed order, so the result does not depend
+        // on scheduling), solved with the FP32 factors and pivots, and added to x in FP64.
         template<int NMAX, int W, bool F32>
         __global__ void __launch_bounds__(32 * W) patch_solve(PatchArgs A, const PatchTables* __restrict__ tables,
                                                           const int* __restrict__ order, int count)
@@ -374,11 +376,13 @@ namespace apf
             constexpr int LD = NMAX + 3; // odd: NMAX is even
             extern __shared__ double sm[];
             PatchTables& T = *reinterpret_cast<PatchTables*>(sm);
-            // F32: x [2][NMAX], b [2][NMAX], K x [2][NMAX] in FP64 ahead of the matrix
+            // F32: x [2][NMAX], b [2][NMAX], K x [2][NMAX] and one cell's entries [kCellEntries]
+            // in FP64 ahead of the matrix
             double* xd = sm + kPatchTableDoubles + (kPatchTableDoubles & 1);
             double* bd = xd + 2 * NMAX;
             double* kx = bd + 2 * NMAX;
-            V* K = reinterpret_cast<V*>(xd + (F32 ? 6 * NMAX : 0));
+            double* ev = kx + 2 * NMAX;
+            V* K = reinterpret_cast<V*>(xd + (F32 ? 6 * NMAX + kCellEntries : 0));
             int* piv = reinterpret_cast<int*>(K + NMAX * LD);
             const int lane = threadIdx.x;
             constexpr int NT = 32 * W; // threads of the patch team
@@ -404,9 +408,11 @@ namespace apf
                 for (int i = lane; i < n * LD; i += NT)
                     K[i] = 0.0;
                 team_sync<W>();
-                // every local entry (row, col, value) of the patch system; cols n, n + 1 are
-                // the two right-hand sides
-                auto cell_entries = [&](auto&& sink) {
+                // every local entry (row, col, value) of the patch system, cell by cell, with its
+                // entry index t < kCellEntries (the two entries of a symmetric pair share t);
+                // cols n, n + 1 are the two right-hand sides.  after_cell(pd, sbase) runs once
+                // per cell after the cell's entries (behind a team barrier).
+                auto cell_entries = [&](auto&& sink, auto&& after_cell) {
                 double ht = 0.0;
                 for (int ic = 0; ic < nc; ++ic)
                 {
@@ -458,7 +464,7 @@ namespace apf
                     double du[3];
                     for (int s2 = 0; s2 < 3; ++s2)
                         du[s2] = (uu[2 * s2 + 1] - uu[2 * s2]) / k.ht;
-                    for (int t = lane; t < 113; t += NT)
+                    for (int t = lane; t < kCellEntries; t += NT)
                     {
                         if (t < 64)
                         {
@@ -466,7 +472,7 @@ namespace apf
                             if (pd[j] < 0 || pd[l] < 0)
                                 continue;
                             const double r = S00 * T.r00[j][l] + S01 * (T.r01[j][l] + T.r01[l][j]) + S11 * T.r11[j][l];
-                            sink(pd[j], pd[l], e[j] * e[l] * adet * r);
+                            sink(t, pd[j], pd[l], e[j] * e[l] * adet * r);
                         }
                         else if (t < 88)
                         {
@@ -474,8 +480,8 @@ namespace apf
                             if (pd[l] < 0)
                                 continue;
                             const double v = e[l] * adet * T.rd[l][r];
-                            sink(sbase + r, pd[l], v);
-                            sink(pd[l], sbase + r, v);
+                            sink(t, sbase + r, pd[l], v);
+                            sink(t, pd[l], sbase + r, v);
                         }
                         else if (t < 104)
                         {
@@ -484,7 +490,7 @@ namespace apf
                                 continue;
                             const double gJ0 = gth[kk][0] * k.J00 + gth[kk][1] * k.J10;
                             const double gJ1 = gth[kk][0] * k.J01 + gth[kk][1] * k.J11;
-                            sink(pd[j], n + kk, -e[j] * adet * (gJ0 * T.rl[a][j][0] + gJ1 * T.rl[a][j][1]));
+                            sink(t, pd[j], n + kk, -e[j] * adet * (gJ0 * T.rl[a][j][0] + gJ1 * T.rl[a][j][1]));
                         }
                         else if (t < 110)
                         {
@@ -495,22 +501,25 @@ namespace apf
                             const double mg0 = k.m00 * gth[kk][0] + k.m01 * gth[kk][1];
                             const double mg1 = k.m01 * gth[kk][0] + k.m11 * gth[kk][1];
                             const double gpm = k.g[a][0] * mg0 + k.g[a][1] * mg1;
-                            sink(sbase + r, n + kk, (0.5 * k.ht * acc - gpm / 6.0) * adet);
+                            sink(t, sbase + r, n + kk, (0.5 * k.ht * acc - gpm / 6.0) * adet);
                         }
                         else if (interior)
                         {
                             // mean-zero row: int_K lambda_r = |K| / 6 on the reference scale
                             const int r = t - 110;
                             const double v = adet / 6.0;
-                            sink(n - 1, sbase + r, v);
-                            sink(sbase + r, n - 1, v);
+                            sink(t, n - 1, sbase + r, v);
+                            sink(t, sbase + r, n - 1, v);
                         }
                     }
                     team_sync<W>();
+                    after_cell(pd, sbase);
                 }
                 return ht;
                 };
-                const double ht = cell_entries([&](int row, int col, double v) { K[row * LD + col] += static_cast<V>(v); });
+                const double ht = cell_entries(
+                    [&](int, int row, int col, double v) { K[row * LD + col] += static_cast<V>(v); },
+                    [](const int*, int) {});
                 // right-hand sides times Mt^-1 (Mt = ht [[1/3,1/6],[1/6,1/3]], inverse (1/ht) [[4,-2],[-2,4]])
                 for (int i = lane; i < n; i += NT)
                 {
@@ -597,15 +606,60 @@ namespace apf
                         bd[i] = bd[NMAX + i] = kx[i] = kx[NMAX + i] = 0.0;
                     }
                     team_sync<W>();
-                    cell_entries([&](int row, int col, double v) {
-                        if (col >= n)
-                            atomicAdd(bd + (col - n) * NMAX + row, v);
-                        else
-                        {
-                            atomicAdd(kx + row, v * xd[col]);
-                            atomicAdd(kx + NMAX + row, v * xd[NMAX + col]);
-                        }
-                    });
+                    // K x in a fixed order: the cell's matrix entries go to ev[t], then one lane
+                    // per local row of the cell sums that row's entries in entry order (within a
+                    // cell every (row, col) occurs once, and the cell's local rows are distinct
+                    // patch rows); the right-hand-side entries are unique per cell as well
+                    cell_entries(
+                        [&](int t, int row, int col, double v) {
+                            if (col >= n)
+                                bd[(col - n) * NMAX + row] += v;
+                            else
+                                ev[t] = v;
+                        },
+                        [&](const int* pd, int sbase) {
+                            const int q = lane;
+                            double a0 = 0.0, a1 = 0.0;
+                            int row = -1;
+                            auto add = [&](double v, int col) {
+                                a0 += v * xd[col];
+                                a1 += v * xd[NMAX + col];
+                            };
+                            if (q < 8)
+                            {
+                                if (pd[q] >= 0)
+                                {
+                                    row = pd[q];
+                                    for (int l = 0; l < 8; ++l)
+                                        if (pd[l] >= 0)
+                                            add(ev[8 * q + l], pd[l]);
+                                    for (int r = 0; r < 3; ++r)
+                                        add(ev[64 + 8 * r + q], sbase + r);
+                                }
+                            }
+                            else if (q < 11)
+                            {
+                                const int r = q - 8;
+                                row = sbase + r;
+                                for (int l = 0; l < 8; ++l)
+                                    if (pd[l] >= 0)
+                                        add(ev[64 + 8 * r + l], pd[l]);
+                                if (interior)
+                                    add(ev[110 + r], n - 1);
+                            }
+                            else if (q == 11 && interior)
+                            {
+                                row = n - 1;
+                                for (int r = 0; r < 3; ++r)
+                                    add(ev[110 + r], sbase + r);
+                            }
+                            if (row >= 0)
+                            {
+                                kx[row] += a0;
+                                kx[NMAX + row] += a1;
+                            }
+                            team_sync<W>();
+                        });
                     for (int i = lane; i < n; i += NT)
                     {
                         const double b0 = bd[i], b1 = bd[NMAX + i];
@@ -679,7 +733,7 @@ namespace apf
         template<int NMAX, bool F32>
         constexpr std::size_t patch_smem_bytes()
         {
-            return F32 ? sizeof(double) * (kPatchTableDoubles + (kPatchTableDoubles & 1) + 6 * NMAX) +
+            return F32 ? sizeof(double) * (kPatchTableDoubles + (kPatchTableDoubles & 1) + 6 * NMAX + kCellEntries) +
                              sizeof(float) * NMAX * (NMAX + 3) + sizeof(int) * NMAX
                        : sizeof(double) * (kPatchTableDoubles + (kPatchTableDoubles & 1) + NMAX * (NMAX + 3));
         }

@@ -261,11 +261,13 @@ def refined_training_problem(k: int, levels=(3, 4)):
 
 def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, levels=(3, 4), epochs: int = 40,
                         lr: float = 1e-2, seed: int = 0, device: int = 0, log=print, steps: int = 4,
-                        burn_in: int = 8, n_refined: int = 0):
+                        burn_in: int = 8, n_refined: int = 0, refined_strength: float | None = None):
     """Train the shipped model on method-generated systems: uniform meshes of the given outer
     levels with seeded random piecewise-constant diffusivity (log-uniform in [0.01, 100] on
     4x4 or 8x8 blocks), the constant-diffusivity mesh of each level, and n_refined locally
-    refined systems with such a diffusivity (refined_training_problem)."""
+    refined systems with such a diffusivity (refined_training_problem).  The AMG hierarchies
+    the model is trained on are built with the library's default options, those of the
+    refined systems with strength threshold ``refined_strength`` when given."""
     from .assembly import assemble_main_system_blocks
     from .solver import SolverOptions, setup_preconditioner
     ctx = Context(device)
@@ -277,16 +279,21 @@ def train_default_model(out_path: str = DEFAULT_WEIGHTS, n_train: int = 24, leve
     systems += [uniform_problem(level, 1) for level in levels]
     systems += [refined_training_problem(k, levels) for k in range(n_refined)]
     blocks = []
-    for prob in systems:
+    n_plain = len(systems) - n_refined
+    for k, prob in enumerate(systems):
         b = assemble_main_system_blocks(prob, ctx=ctx)
         b.assemble_parabolic_graph_norm_approximation()
-        setup_preconditioner(b, SolverOptions())
+        opts = SolverOptions()
+        if k >= n_plain and refined_strength is not None:
+            opts.amg_strength = refined_strength
+        setup_preconditioner(b, opts)
         blocks.append(b)
     model = LearnedModel.initial(seed)
     hist = train(ctx, blocks, model, epochs=epochs, lr=lr, samples=2, steps=steps, seed=seed, log=log,
                  burn_in=burn_in)
     model.save(out_path, history=np.asarray(hist), levels=np.asarray(levels), n_train=n_train, epochs=epochs,
-               steps=steps, burn_in=burn_in, n_refined=n_refined)
+               steps=steps, burn_in=burn_in, n_refined=n_refined,
+               refined_strength=-1.0 if refined_strength is None else refined_strength)
     return model, hist
 
 
@@ -332,6 +339,8 @@ if __name__ == "__main__":
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--burn-in", type=int, default=8)
     ap.add_argument("--refined", type=int, default=0, help="locally refined high-contrast systems added to the set")
+    ap.add_argument("--refined-strength", type=float, default=None,
+                    help="AMG strength threshold of the refined systems' hierarchies (default: the library's)")
     ap.add_argument("--evaluate", type=int, default=None, metavar="LEVEL",
                     help="instead of training: learned vs plain on seeded random-kappa systems of this level")
     a = ap.parse_args()
@@ -340,4 +349,4 @@ if __name__ == "__main__":
         print(json.dumps(evaluate(a.evaluate)))
         raise SystemExit(0)
     train_default_model(a.out, a.n_train, tuple(int(x) for x in a.levels.split(",")), a.epochs, a.lr, a.seed,
-                        steps=a.steps, burn_in=a.burn_in, n_refined=a.refined)
+                        steps=a.steps, burn_in=a.burn_in, n_refined=a.refined, refined_strength=a.refined_strength)

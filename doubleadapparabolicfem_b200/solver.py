@@ -66,8 +66,12 @@ def setup_preconditioner(blocks: MainSystemBlocks, options: SolverOptions | None
 
 
 def solve_saddle_system_with_preconditioner(blocks: MainSystemBlocks, options: SolverOptions | None = None,
-                                            initial_guess: np.ndarray | None = None, copy_out: bool = True):
-    """Solve K [lambda; u] = [f; g].  Returns (solution or None, diagnostics dict)."""
+                                            initial_guess: np.ndarray | None = None, copy_out: bool = True,
+                                            rhs: np.ndarray | None = None):
+    """Solve K [lambda; u] = [f; g] (or K x = rhs: e.g. the correction equation
+    K d = b - K x0 of an initial guess x0, as the reference's dispatcher solves it with
+    MainSystemInitialGuess::solve_correction_equation).  Returns (solution or None,
+    diagnostics dict)."""
     options = options or SolverOptions()
     ctx = blocks.ctx
     o = options.to_c()
@@ -79,7 +83,14 @@ def solve_saddle_system_with_preconditioner(blocks: MainSystemBlocks, options: S
         if guess.size != n:
             raise ValueError("initial guess size does not match the full saddle system")
     d = _lib.SolverDiagnostics()
-    rc = ctx.lib.apf_solve_minres(ctx.handle, blocks.handle, C.byref(o), _ptr(guess), _ptr(out), 0, C.byref(d))
+    if rhs is None:
+        rc = ctx.lib.apf_solve_minres(ctx.handle, blocks.handle, C.byref(o), _ptr(guess), _ptr(out), 0, C.byref(d))
+    else:
+        b = np.ascontiguousarray(rhs, dtype=np.float64)
+        if b.size != n:
+            raise ValueError("right-hand side size does not match the full saddle system")
+        rc = ctx.lib.apf_solve_minres_with_rhs(ctx.handle, blocks.handle, C.byref(o), _ptr(b), _ptr(guess), _ptr(out),
+                                               0, C.byref(d))
     diag = _diag_dict(d)
     if rc == _lib.APF_ERR_NOT_CONVERGED:
         raise PreconditionedSolveFailure(ctx.lib.apf_ctx_last_error(ctx.handle).decode(), diag)

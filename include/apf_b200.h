@@ -241,6 +241,13 @@ int apf_setup_preconditioner(apf_ctx* ctx, apf_system* sys, const apf_solver_opt
  * PreconditionedSolveFailure, parabolic_graph_norm_minres.hpp:357-366). */
 int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* initial_guess,
                      double* solution, int pointers_on_device, apf_solver_diagnostics* diag);
+/* The same with another right-hand side rhs (n_lambda + n_u values) in place of the
+ * assembled [f; g]: the correction equation K d = b - K x0 of an initial guess x0 that the
+ * reference's dispatcher solves when MainSystemInitialGuess::solve_correction_equation is
+ * set (src/linear_algebra/eigen_backend/preconditioners/solve_saddle_system.hpp:75-86). */
+int apf_solve_minres_with_rhs(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* rhs,
+                              const double* initial_guess, double* solution, int pointers_on_device,
+                              apf_solver_diagnostics* diag);
 /* z = P^{-1} r with the set-up preconditioner: block 0 = A_y part (n_lambda values),
  * 1 = Hhat part (n_u values), 2 = the full block operator (n_lambda + n_u).  For tests
  * and diagnostics (symmetry, PCG quality) of the preconditioner. */
