@@ -408,6 +408,9 @@ def run_ours(args, world, rank, local):
             ctx.check(lib.apf_amg_level_info(ctx.handle, h, block, 0, C.byref(r), C.byref(na), C.byref(npp),
                                              C.byref(om), C.byref(al)))
             sizes.append(f"{name} level 0: {r.value} rows, {na.value} nonzeros")
+        kr, kc, knnz = C.c_int32(), C.c_int32(), C.c_int64()
+        ctx.check(lib.apf_system_block_info(h, _lib.BLOCKS["K"], C.byref(kr), C.byref(kc), C.byref(knnz)))
+        sizes.append(f"K: {kr.value} rows, {knnz.value} nonzeros")
         lib.apf_system_destroy(h)
         print(f"profile run: {solve_diags[-1]['iterations']} MINRES iterations, {ctx.kernel_launches()} launches; "
               + "; ".join(sizes))
@@ -618,8 +621,9 @@ def run_ours(args, world, rank, local):
                  "algorithmic_bytes_per_launch": spmv_bytes, "launches_per_step": spmv_launches,
                  "share": spmv_ms / total_ms if total_ms else None,
                  "traffic": K_SPMV_TRAFFIC_RATIO * spmv_bytes,
-                 "traffic_source": "DRAM bytes per launch of the K SpMV measured by ncu at outer level 5 "
-                                   "(1.016 x its algorithmic bytes) times this launch's algorithmic bytes"}
+                 "traffic_source": "DRAM bytes per launch of the K SpMV measured by ncu on the locally refined workload at "
+                                   "outer level 5 (1.030 x its algorithmic bytes) times this launch's "
+                                   "algorithmic bytes"}
     rooflines = [spmv_roof]
     if sweep_achieved:
         rooflines.insert(0, {
@@ -628,8 +632,9 @@ def run_ours(args, world, rank, local):
             "algorithmic_bytes_per_launch": sweep_bytes, "launches_per_step": sweep_launches,
             "share": sweep_ms / total_ms if total_ms else None,
             "traffic": (SWEEP_L0_TRAFFIC_RATIO * sweep_bytes) if SWEEP_L0_TRAFFIC_RATIO else None,
-            "traffic_source": ("DRAM bytes per launch of the finest-level sweeps measured by ncu at outer level 5 "
-                               "divided by their algorithmic bytes, times this launch's algorithmic bytes")
+            "traffic_source": ("DRAM bytes per launch of the finest-level sweeps measured by ncu on the locally refined "
+                               "workload at outer level 5 (0.987 x their algorithmic bytes), times this "
+                               "launch's algorithmic bytes")
             if SWEEP_L0_TRAFFIC_RATIO else "not captured"})
     # the line's roofline is the dominant kernel's when its byte model is known
     by_name = {r["kernel"]: r for r in rooflines}
@@ -710,14 +715,17 @@ def run_ours(args, world, rank, local):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of the MINRES K SpMV per launch divided by its
-# algorithmic bytes (12 nnz + 4 (n+1) + 16 n), from one ncu capture at outer level 5
-# (123.4 and 124.4 MB for 121.93 MB)
-K_SPMV_TRAFFIC_RATIO = 1.016
-# the same for the finest-level V-cycle sweeps: six launches at outer level 5 (three on
-# A_y's finest operator, 254,016 rows / 2,507,904 nonzeros, 27.34 MB each; three on
-# Hhat_F's, 130,977 rows / 1,900,521 nonzeros, 19.00 MB each) moved 139.02 MB for 142.76 MB
-# of algorithmic bytes (8 nnz + 32 rows); the new iterates stayed in L2 (0 bytes written)
-SWEEP_L0_TRAFFIC_RATIO = 0.974
+# algorithmic bytes (12 nnz + 4 (n+1) + 16 n), from one ncu capture of the locally refined
+# workload at outer level 5 (K: 661,835 rows, 16,645,725 nonzeros, 212.99 MB algorithmic;
+# two launches moved 219.54 and 219.39 MB)
+K_SPMV_TRAFFIC_RATIO = 1.030
+# the same for the finest-level V-cycle sweeps, on the locally refined workload at outer
+# level 5 (kappa on 4 x 4 blocks, strength 0.003): six launches on A_y's finest operator
+# (440,678 rows / 4,523,756 nonzeros, 50.29 MB algorithmic) moved 49.38 MB each, nine on
+# Hhat_F's (221,157 rows / 3,493,345 nonzeros, 35.02 MB) 34.86 MB each: 0.987 of the
+# algorithmic bytes (8 nnz + 32 rows) for one launch of each; the new iterates mostly stay
+# in L2
+SWEEP_L0_TRAFFIC_RATIO = 0.987
 
 
 def main():

@@ -1,0 +1,652 @@
+/*
+ * apf_b200_backend.hpp — the C++20 drop-in of libapf_b200 for the reference's templates
+ * (Rsmeets99/DoubleAdapParabolicFEM).
+ *
+ * It adds one linear-algebra backend, la::b200::Backend, whose host containers are the
+ * reference's Eigen-backend types (so every host-side algorithm of the reference --
+ * marking, refinement, the estimator, the direct solvers, the diagnostics -- runs on them
+ * unchanged) and whose hot path runs on the B200 through the C ABI of apf_b200.h:
+ *
+ *   finite_element::system::assemble_main_system_blocks<QS, QT, la::b200::Backend>
+ *       (src/finite_element/system/assemble_saddle_problem.hpp:131) -> apf_assemble_main_system;
+ *       the blocks come back as the reference's host matrices, and the device system
+ *       stays resident in the calling thread's session;
+ *   la::preconditioners::parabolic_graph_norm_approximation<la::b200::Backend>, the Schur step of
+ *       finite_element::assembly::assemble_parabolic_graph_norm_approximation
+ *       (src/finite_element/assembly/main_system/parabolic_graph_norm.hpp:13-64;
+ *       src/linear_algebra/preconditioners/schur_approximations.hpp:231-287) ->
+ *       apf_assemble_graph_norm on that device system (the caller still assembles its host
+ *       B_dt and A_x, which the device path does not need);
+ *   la::preconditioners::SaddlePreconditionedSolveDispatcher<la::b200::Backend>::solve
+ *       (src/linear_algebra/preconditioners/solve_saddle_system.hpp:43-111, the seam the Eigen
+ *       backend specialises in src/linear_algebra/eigen_backend/preconditioners/
+ *       solve_saddle_system.hpp:32-121) -> apf_solve_minres_with_rhs (block-preconditioned
+ *       MINRES with the reference's true-residual batches) on the device system.
+ *
+ * The assembly function is a constrained overload of the reference's own template, and the
+ * Schur step and the dispatcher are full specialisations; qualified calls bind to the
+ * overloads visible where the calling template is defined, so this header must be included
+ * BEFORE the reference's solver and driver headers
+ * (finite_element/system/solve_main_system.hpp, time_slabs/time_slab_adaptive_loop.hpp,
+ * algorithm/...).  A solve whose blocks were not assembled through this backend in the
+ * same thread throws instead of solving on the host.
+ *
+ * Coefficients: M and ell are evaluated at each Y cell's centroid (the device assembly takes
+ * them constant per cell, exact for the reference's piecewise-constant coefficients); u0
+ * must be one of the examples' initial data sin(pi x) sin(pi y) (sin(pi x) in 1+1D), 1 or 0,
+ * recognised by sampling.  Quadrature orders: the device blocks are the exact integrals,
+ * equal to the reference's at its own orders (QSpace = 4p + 1, QTime = 2p + 1 in 2+1D;
+ * 3 and 3 in 1+1D).
+ *
+ * Link with -lapf_b200.  Not thread-safe across threads sharing a session (each host thread
+ * has its own).
+ */
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <concepts>
+#include <cstdint>
+#include <cstdlib>
+#include <memory>
+#include <optional>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "apf_b200.h"
+
+#include "linear_algebra/eigen_backend/backend.hpp"
+#include "linear_algebra/operations/linalg_ops.hpp"
+#include "linear_algebra/preconditioners/solve_failure.hpp"
+#include "linear_algebra/preconditioners/schur_approximations.hpp"
+#include "linear_algebra/preconditioners/solve_saddle_system.hpp"
+#include "finite_element/assembly/constrained_dofs.hpp"
+#include "finite_element/assembly/detail/active_cell_locator.hpp"
+#include "finite_element/system/assemble_saddle_problem.hpp"
+#include "finite_element/system/main_preconditioner_context.hpp"
+
+namespace la::b200
+{
+    // Host containers of the reference's Eigen backend; a distinct type, so that the
+    // overloads and the dispatcher specialisation below take over the hot path.
+    struct Backend
+    {
+        using scalar_type = double;
+        using index_type = int;
+
+        using SparseBuilder = la::eigen::SparseBuilder;
+        using SparsePatternBuilder = la::eigen::SparsePatternBuilder;
+        using Vector = la::eigen::Vector;
+        using DenseMatrix = la::eigen::DenseMatrix;
+        using DenseSolver = la::eigen::DenseDirectSolver;
+        using SparseMatrix = la::eigen::SparseMatrix;
+        using Solver = la::eigen::Solver;
+    };
+
+    // A failed C-ABI call: the status code and the context's message.
+    class Error : public std::runtime_error
+    {
+    public:
+        Error(int status, const std::string& message)
+            : std::runtime_error(message), status_(status)
+        {}
+
+        [[nodiscard]] int status() const noexcept { return status_; }
+
+    private:
+        int status_;
+    };
+
+    inline void check(apf_ctx* ctx, int rc, const char* what)
+    {
+        if (rc == APF_OK)
+            return;
+        std::string msg = std::string("b200 backend: ") + what + " failed (status " + std::to_string(rc) + ")";
+        if (ctx != nullptr)
+        {
+            const char* e = apf_ctx_last_error(ctx);
+            if (e != nullptr && *e != '\0')
+                msg += ": " + std::string(e);
+        }
+        throw Error(rc, msg);
+    }
+
+    // Per host thread: the device context and the device system of the last assembly, with
+    // a few of its blocks' entries kept to recognise the host copies handed back to the
+    // reference.
+    class Session
+    {
+    public:
+        struct Probe
+        {
+            int block, row, col;
+            double value;
+        };
+
+        Session()
+        {
+            apf_solver_options_default(&options_);
+        }
+        Session(const Session&) = delete;
+        Session& operator=(const Session&) = delete;
+
+        ~Session()
+        {
+            release();
+            if (ctx_ != nullptr)
+                apf_ctx_destroy(ctx_);
+        }
+
+        // CUDA device of the context (before its first use; default: APF_B200_DEVICE or 0)
+        void set_device(int device)
+        {
+            if (ctx_ != nullptr)
+                throw std::logic_error("b200 backend: the session's context already exists");
+            device_ = device;
+        }
+
+        [[nodiscard]] apf_ctx* context()
+        {
+            if (ctx_ == nullptr)
+            {
+                int device = device_;
+                if (device < 0)
+                {
+                    const char* env = std::getenv("APF_B200_DEVICE");
+                    device = env != nullptr ? std::atoi(env) : 0;
+                }
+                check(nullptr, apf_ctx_create(device, nullptr, &ctx_), "apf_ctx_create");
+            }
+            return ctx_;
+        }
+
+        // preconditioner kind and AMG parameters of the solves (tolerance, iteration limit
+        // and batching come from the reference's SolverOptions of each solve)
+        [[nodiscard]] apf_solver_options& solver_options() noexcept { return options_; }
+
+        [[nodiscard]] apf_system* system() const noexcept { return sys_; }
+        [[nodiscard]] double zero_tol() const noexcept { return zero_tol_; }
+        [[nodiscard]] const apf_solver_diagnostics& last_diagnostics() const noexcept { return last_diag_; }
+
+        void adopt(apf_system* sys, double zero_tol)
+        {
+            release();
+            sys_ = sys;
+            zero_tol_ = zero_tol;
+        }
+
+        void release()
+        {
+            if (sys_ != nullptr)
+                apf_system_destroy(sys_);
+            sys_ = nullptr;
+            probes_.clear();
+        }
+
+        void add_probe(const Probe& p) { probes_.push_back(p); }
+
+        // the device system whose blocks the host matrices are (by their recorded entries)
+        template<class SparseMatrix>
+        [[nodiscard]] apf_system* system_for(int block, const SparseMatrix& M) const
+        {
+            if (sys_ == nullptr)
+                return nullptr;
+            int32_t rows = 0, cols = 0;
+            int64_t nnz = 0;
+            if (apf_system_block_info(sys_, block, &rows, &cols, &nnz) != APF_OK || M.rows() != rows ||
+                M.cols() != cols)
+                return nullptr;
+            bool any = false;
+            for (const Probe& p : probes_)
+                if (p.block == block)
+                {
+                    any = true;
+                    if (M.coeff(p.row, p.col) != p.value)
+                        return nullptr;
+                }
+            return any ? sys_ : nullptr;
+        }
+
+        void set_last_diagnostics(const apf_solver_diagnostics& d) noexcept { last_diag_ = d; }
+
+    private:
+        int device_ = -1;
+        apf_ctx* ctx_ = nullptr;
+        apf_system* sys_ = nullptr;
+        double zero_tol_ = 1e-15;
+        apf_solver_options options_{};
+        apf_solver_diagnostics last_diag_{};
+        std::vector<Probe> probes_;
+    };
+
+    [[nodiscard]] inline Session& session()
+    {
+        thread_local Session s;
+        return s;
+    }
+
+    namespace detail
+    {
+        constexpr int kProbesPerBlock = 16;
+
+        // a block of the device system as the reference's host matrix (explicit zeros kept);
+        // records probes of it in the session
+        template<class B>
+        [[nodiscard]] typename B::SparseMatrix download_block(Session& s, int block)
+        {
+            apf_ctx* ctx = s.context();
+            apf_system* sys = s.system();
+            int32_t rows = 0, cols = 0;
+            int64_t nnz = 0;
+            check(ctx, apf_system_block_info(sys, block, &rows, &cols, &nnz), "apf_system_block_info");
+            std::vector<int32_t> rp(static_cast<std::size_t>(rows) + 1), ci(static_cast<std::size_t>(nnz));
+            std::vector<double> va(static_cast<std::size_t>(nnz));
+            check(ctx, apf_system_block_copy(ctx, sys, block, rp.data(), ci.data(), va.data(), 0),
+                  "apf_system_block_copy");
+            typename B::SparseBuilder builder;
+            builder.reserve(static_cast<std::size_t>(nnz));
+            for (int32_t i = 0; i < rows; ++i)
+                for (int32_t k = rp[static_cast<std::size_t>(i)]; k < rp[static_cast<std::size_t>(i) + 1]; ++k)
+                    builder.add(i, ci[static_cast<std::size_t>(k)], va[static_cast<std::size_t>(k)]);
+            typename B::SparseMatrix M(rows, cols);
+            M.set_from_builder(builder);
+            if (nnz > 0)
+            {
+                // entries spread over the rows (binary search of the row of entry k)
+                for (int q = 0; q < kProbesPerBlock; ++q)
+                {
+                    const int64_t k = (nnz - 1) * q / std::max(1, kProbesPerBlock - 1);
+                    const auto it = std::upper_bound(rp.begin(), rp.end(), static_cast<int32_t>(k));
+                    const int row = static_cast<int>(it - rp.begin()) - 1;
+                    s.add_probe({block, row, ci[static_cast<std::size_t>(k)], va[static_cast<std::size_t>(k)]});
+                }
+            }
+            return M;
+        }
+
+        template<class B>
+        [[nodiscard]] typename B::Vector download_vector(Session& s, int which, int n)
+        {
+            std::vector<double> h(static_cast<std::size_t>(n));
+            check(s.context(), apf_system_vector_copy(s.context(), s.system(), which, h.data(), 0),
+                  "apf_system_vector_copy");
+            typename B::Vector v(n);
+            for (int i = 0; i < n; ++i)
+                v[i] = h[static_cast<std::size_t>(i)];
+            return v;
+        }
+
+        // host arrays of an apf_problem_desc built from the reference's spaces and problem data
+        struct ProblemArrays
+        {
+            std::vector<double> y_geo, x_geo, m, ell, y_w, x_w;
+            std::vector<int32_t> y_to_x, y_off, y_dofs, x_off, x_dofs;
+            apf_problem_desc desc{};
+        };
+
+        template<class Space>
+        void append_geometry(const Space& space, int c, std::vector<double>& out)
+        {
+            constexpr int dim = Space::GT::dim_space_v;
+            const auto& mesh = space.mesh_ref();
+            const auto& cell = mesh.cell(c);
+            const auto& sv = mesh.spatial_vertices();
+            const auto& tv = mesh.temporal_vertices();
+            for (int k = 0; k < dim + 1; ++k)
+                for (int d = 0; d < dim; ++d)
+                    out.push_back(sv[cell.spatial_vertex_ids[k]][d]);
+            out.push_back(tv[cell.temporal_vertex_ids[0]][0]);
+            out.push_back(tv[cell.temporal_vertex_ids[1]][0]);
+        }
+
+        template<class Space>
+        void append_restrictions(const Space& space, const std::vector<int>& cells, std::vector<int32_t>& off,
+                                 std::vector<int32_t>& dofs, std::vector<double>& w)
+        {
+            off.assign(1, 0);
+            for (const int c : cells)
+            {
+                const auto r = finite_element::assembly::build_cell_restriction(space, c);
+                for (int i = 0; i < r.size(); ++i)
+                {
+                    for (const auto& e : r[i])
+                    {
+                        dofs.push_back(e.true_dof);
+                        w.push_back(e.weight);
+                    }
+                    off.push_back(static_cast<int32_t>(dofs.size()));
+                }
+            }
+        }
+
+        // which of the examples' initial data u0 is (by values at interior sample points)
+        template<int Dim, class U0>
+        [[nodiscard]] int initial_kind(const U0& u0)
+        {
+            constexpr double pi = 3.14159265358979323846;
+            const double samples[5][2] = {{0.13, 0.71}, {0.37, 0.29}, {0.5, 0.5}, {0.83, 0.17}, {0.61, 0.93}};
+            bool sin_sin = true, one = true, zero = true;
+            for (const auto& q : samples)
+            {
+                std::array<double, Dim> p{};
+                for (int d = 0; d < Dim; ++d)
+                    p[static_cast<std::size_t>(d)] = q[d];
+                const double v = static_cast<double>(u0(p));
+                double s = std::sin(pi * q[0]);
+                if constexpr (Dim == 2)
+                    s *= std::sin(pi * q[1]);
+                sin_sin = sin_sin && std::abs(v - s) <= 1e-12;
+                one = one && std::abs(v - 1.0) <= 1e-12;
+                zero = zero && std::abs(v) <= 1e-14;
+            }
+            if (sin_sin)
+                return APF_U0_SIN_SIN;
+            if (one)
+                return APF_U0_ONE;
+            if (zero)
+                return APF_U0_ZERO;
+            throw std::invalid_argument(
+                "b200 backend: the initial datum is not one of the examples' u0 (sin(pi x) sin(pi y), 1, 0)");
+        }
+
+        // M(p) as the three entries m00, m01, m11 (2+1D) or one scalar (1+1D)
+        template<int Dim, class Value>
+        void append_m(const Value& v, std::vector<double>& out)
+        {
+            if constexpr (std::is_arithmetic_v<Value>)
+            {
+                out.push_back(static_cast<double>(v));
+                if constexpr (Dim == 2)
+                {
+                    out.push_back(0.0);
+                    out.push_back(static_cast<double>(v));
+                }
+            }
+            else if constexpr (Dim == 1)
+                out.push_back(v[0][0]);
+            else
+            {
+                out.push_back(v[0][0]);
+                out.push_back(v[0][1]);
+                out.push_back(v[1][1]);
+            }
+        }
+
+        template<class YSpace, class XSpace, class Problem>
+        [[nodiscard]] ProblemArrays describe(const YSpace& y_space, const XSpace& x_space, const Problem& problem,
+                                             double zero_tol, double g_scale)
+        {
+            constexpr int dim = YSpace::GT::dim_space_v;
+            static_assert(dim == 1 || dim == 2, "b200 backend: 1+1D and 2+1D only");
+            constexpr int p_space = YSpace::FETraitsType::p_space_v;
+            static_assert(p_space == YSpace::FETraitsType::p_time_v, "b200 backend: equal space and time degrees");
+            static_assert(dim == 2 ? (p_space == 1 || p_space == 2) : p_space == 1,
+                          "b200 backend: P1 and P2 prisms (2+1D), P1 quadrilaterals (1+1D)");
+            ProblemArrays a;
+            const std::vector<int> y_cells(y_space.active_cells().begin(), y_space.active_cells().end());
+            const std::vector<int> x_cells(x_space.active_cells().begin(), x_space.active_cells().end());
+            const auto& mesh = x_space.mesh_ref();
+            for (const int c : y_cells)
+                append_geometry(y_space, c, a.y_geo);
+            for (const int c : x_cells)
+                append_geometry(x_space, c, a.x_geo);
+            append_restrictions(y_space, y_cells, a.y_off, a.y_dofs, a.y_w);
+            append_restrictions(x_space, x_cells, a.x_off, a.x_dofs, a.x_w);
+            {
+                finite_element::assembly::detail::ActiveAncestorCache<XSpace> ancestors(x_space);
+                std::vector<int32_t> x_pos(static_cast<std::size_t>(mesh.n_cells()), -1);
+                for (std::size_t k = 0; k < x_cells.size(); ++k)
+                    x_pos[static_cast<std::size_t>(x_cells[k])] = static_cast<int32_t>(k);
+                for (const int c : y_cells)
+                {
+                    const int32_t pos = x_pos[static_cast<std::size_t>(ancestors.find(c))];
+                    if (pos < 0)
+                        throw std::runtime_error("b200 backend: a Y cell has no active X ancestor");
+                    a.y_to_x.push_back(pos);
+                }
+            }
+            // coefficients at each Y cell's centroid
+            const std::size_t row = dim == 2 ? 8u : 4u;
+            for (std::size_t k = 0; k < y_cells.size(); ++k)
+            {
+                const double* g = a.y_geo.data() + k * row;
+                std::array<double, dim + 1> p{};
+                for (int d = 0; d < dim; ++d)
+                {
+                    double s = 0.0;
+                    for (int v = 0; v < dim + 1; ++v)
+                        s += g[v * dim + d];
+                    p[static_cast<std::size_t>(d)] = s / (dim + 1);
+                }
+                p[dim] = 0.5 * (g[row - 2] + g[row - 1]);
+                append_m<dim>(problem.M(p), a.m);
+                a.ell.push_back(static_cast<double>(problem.ell(p)));
+            }
+            apf_problem_desc& d = a.desc;
+            d.p = p_space;
+            d.dim_space = dim;
+            d.n_y_cells = static_cast<int>(y_cells.size());
+            d.n_x_cells = static_cast<int>(x_cells.size());
+            d.n_lambda = y_space.dof_handler_ref().n_true_dofs();
+            d.n_u = x_space.dof_handler_ref().n_true_dofs();
+            d.y_geometry = a.y_geo.data();
+            d.x_geometry = a.x_geo.data();
+            d.y_to_x = a.y_to_x.data();
+            d.y_restr_offsets = a.y_off.data();
+            d.y_restr_dofs = a.y_dofs.data();
+            d.y_restr_weights = a.y_w.data();
+            d.y_restr_nnz = static_cast<int32_t>(a.y_dofs.size());
+            d.x_restr_offsets = a.x_off.data();
+            d.x_restr_dofs = a.x_dofs.data();
+            d.x_restr_weights = a.x_w.data();
+            d.x_restr_nnz = static_cast<int32_t>(a.x_dofs.size());
+            d.m_cells = a.m.data();
+            d.ell_cells = a.ell.data();
+            d.u0_kind = initial_kind<dim>(problem.u0);
+            d.zero_tol = zero_tol;
+            d.g_scale = g_scale;
+            return a;
+        }
+    }
+}
+
+namespace finite_element::system
+{
+    // assemble_main_system_blocks (assemble_saddle_problem.hpp:131) on the B200: the blocks
+    // A_y, B, C_signed, f, g come back as host matrices; the device system stays in the
+    // thread's session for the graph-norm block and the solve.
+    template<int QSpace, int QTime, class Backend, class YSpaceType, class XSpaceType, class ExampleType>
+        requires std::same_as<Backend, la::b200::Backend>
+    [[nodiscard]] MainSystemBlocks<Backend> assemble_main_system_blocks(
+        const YSpaceType& y_space, const XSpaceType& x_space, const ExampleType& example, double zero_tol = 1e-15,
+        double g_scale = -1.0, const finite_element::detail::TimingRecorder& timing = {})
+    {
+        auto timer = timing.scoped("assembly.total_seconds");
+        auto& s = la::b200::session();
+        apf_ctx* ctx = s.context();
+        const auto arrays = la::b200::detail::describe(y_space, x_space, example, zero_tol, g_scale);
+        apf_system* sys = nullptr;
+        la::b200::check(ctx, apf_assemble_main_system(ctx, &arrays.desc, 0, &sys), "apf_assemble_main_system");
+        s.adopt(sys, zero_tol);
+        const int nl = arrays.desc.n_lambda, nu = arrays.desc.n_u;
+        auto A = la::b200::detail::download_block<Backend>(s, APF_BLOCK_A_Y);
+        auto B = la::b200::detail::download_block<Backend>(s, APF_BLOCK_B);
+        auto C = la::b200::detail::download_block<Backend>(s, APF_BLOCK_C);
+        auto f = la::b200::detail::download_vector<Backend>(s, APF_VEC_F, nl);
+        auto g = la::b200::detail::download_vector<Backend>(s, APF_VEC_G, nu);
+        return MainSystemBlocks<Backend>(la::saddle::make_saddle_point_blocks<Backend>(
+            std::move(A), std::move(B), std::move(C), std::move(f), std::move(g)));
+    }
+}
+
+namespace la::preconditioners
+{
+    // parabolic_graph_norm_approximation (src/linear_algebra/preconditioners/
+    // schur_approximations.hpp:231-287), the Schur step of assemble_parabolic_graph_norm_approximation
+    // (parabolic_graph_norm.hpp:13-64), on the B200 for the system of the thread's last b200
+    // assembly: A_y and C_signed must be its blocks; Hhat is built on the device from the
+    // device system (its own B_dt and A_x, with the assembly's zero_tol filter), so the host
+    // B_dt and A_x the reference's caller assembled are only checked for their sizes.  A full
+    // specialisation (the overload set of the caller's template cannot be extended without
+    // an ambiguity, since Backend appears there only in non-deduced contexts).
+    template<>
+    [[nodiscard]] inline ParabolicGraphNormApproximation<la::b200::Backend>
+    parabolic_graph_norm_approximation<la::b200::Backend>(const la::eigen::SparseMatrix& A_y,
+                                                          const la::eigen::SparseMatrix& B_dt,
+                                                          const la::eigen::SparseMatrix& C_signed,
+                                                          const la::eigen::SparseMatrix& A_x,
+                                                          double diagonal_tolerance, double zero_tol)
+    {
+        static_cast<void>(zero_tol);
+        auto& s = la::b200::session();
+        apf_system* sys = s.system_for(APF_BLOCK_A_Y, A_y);
+        if (sys == nullptr || s.system_for(APF_BLOCK_C, C_signed) != sys)
+            throw std::invalid_argument(
+                "b200 backend: A_y and C_signed are not the blocks of this thread's last b200 assembly");
+        if (B_dt.rows() != C_signed.rows() || B_dt.cols() != A_y.rows() || A_x.rows() != C_signed.rows() ||
+            A_x.cols() != C_signed.cols())
+            throw std::runtime_error("parabolic_graph_norm_approximation: block dimensions are inconsistent.");
+        const auto t0 = std::chrono::steady_clock::now();
+        apf_ctx* ctx = s.context();
+        la::b200::check(ctx, apf_assemble_graph_norm(ctx, sys, diagonal_tolerance), "apf_assemble_graph_norm");
+        ParabolicGraphNormApproximation<la::b200::Backend> out;
+        out.hhat = la::b200::detail::download_block<la::b200::Backend>(s, APF_BLOCK_HHAT);
+        auto& d = out.diagnostics;
+        int32_t rows = 0, cols = 0;
+        int64_t nnz = 0;
+        la::b200::check(ctx, apf_system_block_info(sys, APF_BLOCK_HHAT, &rows, &cols, &nnz), "apf_system_block_info");
+        d.hhat_rows = rows;
+        d.hhat_cols = cols;
+        d.hhat_nnz = static_cast<std::size_t>(nnz);
+        la::b200::check(ctx, apf_system_block_info(sys, APF_BLOCK_C, &rows, &cols, &nnz), "apf_system_block_info");
+        d.c_signed_nnz = static_cast<std::size_t>(nnz);
+        la::b200::check(ctx, apf_system_block_info(sys, APF_BLOCK_BDT, &rows, &cols, &nnz), "apf_system_block_info");
+        d.b_or_bdt_nnz_used = static_cast<std::size_t>(nnz);
+        d.setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return out;
+    }
+
+    // The preconditioned saddle solve on the B200 (the seam of solve_saddle_system.hpp:43-111):
+    // MINRES + ParabolicGraphNorm runs on the thread's device system; every other solver
+    // request returns nullopt so that the reference's own direct path takes it, as for the
+    // Eigen backend.
+    template<>
+    struct SaddlePreconditionedSolveDispatcher<la::b200::Backend>
+    {
+        template<class Solver, class Matrix, class Vector, class InitialGuess>
+        [[nodiscard]] static std::optional<SaddlePreconditionedSolveResult<la::b200::Backend>> solve(
+            Solver& solver, const Matrix& K, const Vector& rhs,
+            const la::saddle::SaddlePointBlocks<la::b200::Backend>& blocks,
+            const la::concepts::SolverOptions& options, const InitialGuess& initial_guess,
+            const SaddlePreconditionerContext<la::b200::Backend>& context)
+        {
+            static_cast<void>(solver);
+            const auto validation = la::concepts::validate_solver_preconditioner(options.solver, options.preconditioner);
+            if (!validation.accepted)
+                throw std::invalid_argument(validation.rejection_reason);
+            if (!is_saddle_preconditioned_solve_requested(options))
+                return std::nullopt;
+            blocks.validate();
+            if (K.rows() != K.cols() || K.rows() != rhs.size())
+                throw std::runtime_error(
+                    "solve_saddle_system_with_preconditioner: system dimensions are inconsistent.");
+            if (initial_guess.has_value() && initial_guess.full_vector->size() != rhs.size())
+                throw std::runtime_error("solve_saddle_system_with_preconditioner: initial guess size does not match "
+                                         "the full saddle system.");
+            if (context.graph_norm == nullptr)
+                throw std::runtime_error("solve_saddle_system_with_preconditioner: ParabolicGraphNorm requires "
+                                         "graph-norm block context from assembly.");
+            auto& s = la::b200::session();
+            apf_system* sys = s.system_for(APF_BLOCK_A_Y, blocks.A);
+            if (sys == nullptr || s.system_for(APF_BLOCK_B, blocks.B) != sys ||
+                s.system_for(APF_BLOCK_C, blocks.C) != sys ||
+                s.system_for(APF_BLOCK_HHAT, context.graph_norm->hhat) != sys)
+                throw std::invalid_argument(
+                    "b200 backend: the saddle blocks and the graph-norm block were not assembled by the b200 backend "
+                    "in this thread (include apf_b200_backend.hpp before the reference's solver headers)");
+            apf_ctx* ctx = s.context();
+            const int n = rhs.size();
+
+            // the right-hand side solved for: b, or b - K x0 for the correction equation
+            std::vector<double> b(static_cast<std::size_t>(n)), x0;
+            const bool correction = initial_guess.has_value() && initial_guess.solve_correction_equation;
+            if (correction)
+            {
+                const auto r = la::ops::subtract(rhs, la::ops::matvec(K, *initial_guess.full_vector));
+                for (int i = 0; i < n; ++i)
+                    b[static_cast<std::size_t>(i)] = r[i];
+            }
+            else
+                for (int i = 0; i < n; ++i)
+                    b[static_cast<std::size_t>(i)] = rhs[i];
+            if (initial_guess.has_value() && !correction)
+            {
+                x0.resize(static_cast<std::size_t>(n));
+                for (int i = 0; i < n; ++i)
+                    x0[static_cast<std::size_t>(i)] = (*initial_guess.full_vector)[i];
+            }
+
+            apf_solver_options o = s.solver_options();
+            o.tolerance = options.tolerance;
+            o.max_iterations = options.max_iterations;
+            o.use_true_residual_batching = options.use_true_residual_batching ? 1 : 0;
+            o.true_residual_check_interval = options.true_residual_check_interval;
+            std::vector<double> x(static_cast<std::size_t>(n));
+            apf_solver_diagnostics d{};
+            const int rc = apf_solve_minres_with_rhs(ctx, sys, &o, b.data(), x0.empty() ? nullptr : x0.data(),
+                                                     x.data(), 0, &d);
+            s.set_last_diagnostics(d);
+            if (rc != APF_OK && rc != APF_ERR_NOT_CONVERGED)
+                la::b200::check(ctx, rc, "apf_solve_minres_with_rhs");
+
+            la::concepts::SolverDiagnostics diag;
+            diag.requested_solver = options.solver;
+            diag.effective_solver = la::concepts::SolverType::MINRES;
+            diag.preconditioner = options.preconditioner;
+            diag.rows = K.rows();
+            diag.cols = K.cols();
+            {
+                int32_t kr = 0, kc = 0;
+                int64_t knnz = 0;
+                la::b200::check(ctx, apf_system_block_info(sys, APF_BLOCK_K, &kr, &kc, &knnz), "apf_system_block_info");
+                diag.nnz_matrix = static_cast<std::size_t>(knnz);
+            }
+            diag.direct = false;
+            diag.iterative = true;
+            diag.linear_residual_relative = d.final_true_residual;
+            diag.preconditioner_setup_seconds = d.setup_seconds;
+            diag.preconditioner_stats.setup_seconds = d.setup_seconds;
+            diag.preconditioner_stats.assumes_spd = true;
+            diag.preconditioner_stats.assumes_symmetric = true;
+            diag.preconditioner_stats.is_spd = true;
+            diag.preconditioner_stats.is_symmetric = true;
+            auto& it = diag.iterative_stats;
+            it.iterations = d.iterations;
+            it.final_error = d.backend_reported_error;
+            it.converged = d.converged != 0;
+            it.backend_converged = d.backend_converged != 0;
+            it.backend_reported_error = d.backend_reported_error;
+            it.convergence_accepted_by_true_residual = d.converged != 0;
+            it.residual_check_batches = d.residual_check_batches;
+            it.final_true_residual = d.final_true_residual;
+            it.true_residual_stopping_used = options.use_true_residual_batching;
+            if (rc == APF_ERR_NOT_CONVERGED)
+                throw PreconditionedSolveFailure(apf_ctx_last_error(ctx), diag);
+
+            SaddlePreconditionedSolveResult<la::b200::Backend> result;
+            result.solution = typename la::b200::Backend::Vector(n);
+            for (int i = 0; i < n; ++i)
+                result.solution[i] = x[static_cast<std::size_t>(i)] +
+                                     (correction ? (*initial_guess.full_vector)[i] : 0.0);
+            result.diagnostics = std::move(diag);
+            result.setup_seconds = d.setup_seconds;
+            result.solve_seconds = d.solve_seconds;
+            return result;
+        }
+    };
+}

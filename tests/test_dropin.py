@@ -1,0 +1,116 @@
+"""The compiled C++ drop-in (include/apf_b200_backend.hpp) inside the reference's own callers.
+
+tests/dropin/_build/apf_dropin_test is built by __graft_entry__.build() (tests/dropin/Makefile)
+from the reference's templates where the reference source tree is present, and travels with the
+repository.  It runs, with la::b200::Backend and with the reference's Eigen backend side by side:
+assemble_main_system_blocks + assemble_parabolic_graph_norm_approximation ("blocks"),
+assemble_and_solve_into_functions with MINRES + ParabolicGraphNorm ("solve"), and the reference's
+inner loop compute_adaptive_test_space_iteration + refine_test_space_from_marked_source_cells
+("cycle": device assembly, graph-norm block and MINRES under the reference's host estimator,
+marking and refinement).  Bars: block patterns bit-exact, values 1e-12 (Hhat on adaptive meshes:
+the significant pattern, cancellation residues below 1e-13 may differ); the solve's FP64 true
+residual (on the host, with the Eigen backend's K) within its tolerance and its solution within
+1e-6 of the direct solution; per adaptive pass the same estimator total to 1e-8 and the same
+marked cells as the Eigen backend with its direct solver.
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PROGRAM = os.path.join(HERE, "dropin", "_build", "apf_dropin_test")
+
+# X refined at two space-time points (hanging nodes) and kappa per X cell, as in the
+# adaptive fixtures
+ADAPTIVE_ENV = {"APF_REF_X_POINTS": "0.3,0.6,0.4;0.7,0.25,0.8", "APF_REF_X_ROUNDS": "2",
+                "APF_REF_KAPPA": "7:0.01:100"}
+
+needs_program = pytest.mark.skipif(not os.path.exists(PROGRAM),
+                                   reason="drop-in test program not built (needs the reference source tree)")
+
+
+def _run(args, env=None, timeout=900):
+    e = dict(os.environ)
+    for k in ADAPTIVE_ENV:
+        e.pop(k, None)
+    e.update(env or {})
+    r = subprocess.run([PROGRAM, *map(str, args)], capture_output=True, text=True, env=e, timeout=timeout)
+    return r
+
+
+def _json(r):
+    assert r.returncode == 0, r.stderr[-2000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+@needs_program
+def test_program_fails_loudly_without_a_device():
+    """On a machine without a CUDA device the drop-in reports the context error; nothing falls
+    back to the host."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    r = _run(["blocks", 1, 1, "smooth_initial"])
+    assert r.returncode == 1
+    assert "apf_ctx_create failed" in r.stderr
+
+
+def _assert_blocks(d, hhat_residue):
+    for name in ("A_y", "B", "C_signed"):
+        assert d[name]["pattern_mismatches"] == 0 and d[name]["nnz_ref"] == d[name]["nnz_b200"], (name, d[name])
+        assert d[name]["max_abs_diff_over_max"] <= 1e-12, (name, d[name])
+    hh = d["Hhat_residue_1e-13"] if hhat_residue else d["Hhat"]
+    assert hh["pattern_mismatches"] == 0, hh
+    assert d["Hhat"]["max_abs_diff_over_max"] <= 1e-12, d["Hhat"]
+    assert d["f"] <= 1e-12 and d["g"] <= 1e-12, d
+
+
+@needs_program
+@pytest.mark.gpu
+@pytest.mark.parametrize("p,levels,example", [(1, 2, "smooth_initial"), (2, 1, "smooth_initial"),
+                                              (1, 2, "non_matching_initial")])
+def test_dropin_blocks_match_eigen_backend(p, levels, example):
+    d = _json(_run(["blocks", p, levels, example]))
+    assert d["n_lambda"] > 0 and d["n_u"] > 0
+    _assert_blocks(d, hhat_residue=False)
+
+
+@needs_program
+@pytest.mark.gpu
+def test_dropin_blocks_on_adaptive_mesh_with_kappa():
+    d = _json(_run(["blocks", 1, 2, "smooth_initial"], env=ADAPTIVE_ENV))
+    _assert_blocks(d, hhat_residue=True)
+
+
+@needs_program
+@pytest.mark.gpu
+@pytest.mark.parametrize("env", [None, ADAPTIVE_ENV], ids=["uniform", "adaptive_kappa"])
+def test_dropin_solve_through_reference_caller(env):
+    d = _json(_run(["solve", 1, 3, "smooth_initial", 1e-10], env=env))
+    assert d["effective_solver_minres"] == 1 and d["iterative"] == 1 and d["converged"] == 1
+    assert d["iterations"] > 0 and d["iterations"] == d["device_iterations"]
+    assert d["host_true_residual"] <= 1e-10, d
+    assert abs(d["reported_true_residual"] - d["host_true_residual"]) <= 1e-12 + 1e-6 * d["host_true_residual"], d
+    assert d["max_diff_to_direct_over_max"] <= 1e-6, d
+
+
+@needs_program
+@pytest.mark.gpu
+def test_dropin_adaptive_inner_loop_matches_eigen_backend():
+    """Three passes of the reference's inner loop (estimate, Doerfler marking, Y refinement) on an
+    adaptive X with kappa per cell: the b200 backend's MINRES solution (true residual 1e-12)
+    gives the reference's host estimator the same totals (1e-8) and the same marked cells (up
+    to ties at the threshold, at most 2% of them) as the Eigen backend's direct solve; both
+    test spaces are refined by the direct run's marks, so every pass compares the same mesh."""
+    d = _json(_run(["cycle", 1, 2, "smooth_initial", 3, 1e-12], env=ADAPTIVE_ENV))
+    assert len(d["passes"]) == 3
+    for pas in d["passes"]:
+        assert pas["y_cells"][0] == pas["y_cells"][1], pas
+        assert abs(pas["flux_b200"] - pas["flux_direct"]) <= 1e-8 * pas["flux_direct"], pas
+        # the same marking, up to cells whose indicators tie at the Doerfler threshold
+        assert pas["marked"][1] > 0 and pas["marked_symmetric_difference"] <= max(2, pas["marked"][1] // 50), pas
+        assert pas["minres_iterations"] > 0 and pas["minres_true_residual"] <= 1e-12, pas
+    # the later passes run on the refined (Y finer than X) test space
+    assert d["passes"][2]["y_cells"][0] > d["passes"][1]["y_cells"][0] > d["passes"][0]["y_cells"][0]
