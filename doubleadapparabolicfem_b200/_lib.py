@@ -220,6 +220,15 @@ class XIndicatorTotals(C.Structure):
 SIGNATURES["apf_x_indicators"] = ([_P, _P, C.c_int, _P, _P, _P, _P, C.POINTER(XIndicatorTotals)], C.c_int)
 SIGNATURES["apf_y_estimator_threshold_squared"] = ([C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)], C.c_int)
 
+
+class GEstimatorResult(C.Structure):
+    _fields_ = [("lambda_difference_squared", C.c_double), ("solve_relative_residual", C.c_double),
+                ("solve_iterations", C.c_int), ("n_g", C.c_int)]
+
+
+SIGNATURES["apf_g_estimator"] = ([_P, _P, C.c_int32, _P, _P, _P, C.c_int32, C.c_double,
+                                  C.POINTER(GEstimatorResult)], C.c_int)
+
 SIGNATURES["apf_ctx_reserve_pool"] = ([_P, C.c_int64], C.c_int)
 SIGNATURES["apf_ctx_pool_stats"] = ([_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                      C.POINTER(C.c_int64)], C.c_int)

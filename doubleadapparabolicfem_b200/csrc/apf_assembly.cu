@@ -1880,6 +1880,109 @@ namespace apf
         }
     }
 
+    namespace
+    {
+        // owner[dof]: the smallest local row (cell * nd + k) whose restriction row is the single
+        // entry (dof, 1) -- an unconstrained occurrence of the true DOF
+        __global__ void true_dof_owner_kernel(long long rows, const int* __restrict__ off, const int* __restrict__ dofs,
+                                              const double* __restrict__ w, int* __restrict__ owner)
+        {
+            for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows;
+                 r += (long long)gridDim.x * blockDim.x)
+            {
+                const int a = off[r];
+                if (off[r + 1] - a == 1 && w[a] == 1.0)
+                    atomicMin(owner + dofs[a], static_cast<int>(r));
+            }
+        }
+
+        constexpr int kNoOwner = 0x7f7f7f7f; // the byte pattern 0x7f in every byte of an int
+
+        __global__ void unowned_kernel(int n, const int* __restrict__ owner, int* __restrict__ count)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+                if (owner[i] == kNoOwner)
+                    atomicAdd(count, 1);
+        }
+
+        // out[dof] for every true DOF of the degree-q space (restriction off/dofs, cells with
+        // geometry dst_geo): the degree-p function v (true DOFs through the source restriction
+        // soff/sdofs/sw of the source cells src_index[c], geometry src_geo) at the DOF's node,
+        // evaluated in the owner row's cell only (one deterministic writer per DOF)
+        __global__ void interpolate_kernel(int n, int q, int p, const double* __restrict__ dst_geo,
+                                           const int* __restrict__ src_index, const double* __restrict__ src_geo,
+                                           const int* __restrict__ soff, const int* __restrict__ sdofs,
+                                           const double* __restrict__ sw, const double* __restrict__ v,
+                                           const int* __restrict__ off, const int* __restrict__ dofs,
+                                           const int* __restrict__ owner, double* __restrict__ out)
+        {
+            const RefTables& tq = c_tab[q - 1];
+            const RefTables& tp = c_tab[p - 1];
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+            {
+                const int sc = src_index ? src_index[c] : c;
+                double loc[kMaxNs * kMaxNt];
+                for (int i = 0; i < tp.ndof; ++i)
+                {
+                    const long long row = static_cast<long long>(sc) * tp.ndof + i;
+                    double a = 0.0;
+                    for (int e = soff[row]; e < soff[row + 1]; ++e)
+                        a += sw[e] * v[sdofs[e]];
+                    loc[i] = a;
+                }
+                const CellGeo gd = load_geo(dst_geo, c);
+                const CellGeo gs = load_geo(src_geo, sc);
+                for (int k = 0; k < tq.ndof; ++k)
+                {
+                    const long long row = static_cast<long long>(c) * tq.ndof + k;
+                    const int a = off[row];
+                    if (off[row + 1] - a != 1 || owner[dofs[a]] != static_cast<int>(row))
+                        continue;
+                    double val = 0.0;
+                    for (int i = 0; i < tp.ndof; ++i)
+                        val += loc[i] * transfer_between(tq, tp, gd, gs, i, k);
+                    out[dofs[a]] = val;
+                }
+            }
+        }
+    }
+
+    void interpolate_to_space(cudaStream_t s, int q, int p, int n, const double* dst_geo, const int* src_index,
+                              const double* src_geo, const int* soff, const int* sdofs, const double* sw,
+                              const double* v, const int* off, const int* dofs, const double* w, int n_true,
+                              double* out)
+    {
+        require(q >= 1 && q <= 2 && p >= 1 && p <= q, APF_ERR_INVALID, "interpolate_to_space: degrees");
+        if (n_true <= 0)
+            return;
+        const int ndq = (q + 1) * (q + 2) / 2 * (q + 1);
+        const long long rows = static_cast<long long>(n) * ndq;
+        require(rows < kNoOwner, APF_ERR_CAPACITY, "interpolate_to_space: too many local rows");
+        DeviceBuffer<int> owner(n_true, s), count(1, s);
+        APF_CUDA(cudaMemsetAsync(owner.get(), 0x7f, sizeof(int) * n_true, s)); // kNoOwner, above every row
+        count.zero();
+        {
+            APF_KERNEL("true_dof_owner", s);
+            true_dof_owner_kernel<<<grid_for(rows, 256), 256, 0, s>>>(rows, off, dofs, w, owner.get());
+        }
+        {
+            APF_KERNEL("true_dof_unowned", s);
+            unowned_kernel<<<grid_for(n_true, 256), 256, 0, s>>>(n_true, owner.get(), count.get());
+        }
+        int unowned = 0;
+        APF_CUDA(cudaMemcpyAsync(&unowned, count.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        require(unowned == 0, APF_ERR_INVALID,
+                "interpolate_to_space: a true DOF has no unconstrained occurrence in the restriction");
+        if (n > 0)
+        {
+            APF_KERNEL("interpolate_nodal", s);
+            interpolate_kernel<<<grid_for(n, 128), 128, 0, s>>>(n, q, p, dst_geo, src_index, src_geo, soff, sdofs, sw, v,
+                                                                off, dofs, owner.get(), out);
+        }
+        APF_CUDA(cudaGetLastError());
+    }
+
     void nodal_transfer(cudaStream_t s, int p, int n, const double* dst_geo, const int* src_index, const double* src_geo,
                         const double* src, double* dst)
     {

@@ -14,6 +14,7 @@
 
 #include "apf_internal.hpp"
 #include "apf_estimator.cuh"
+#include "apf_gdelta.cuh"
 #include "apf_learned.cuh"
 #include "apf_system.hpp"
 
@@ -1100,6 +1101,31 @@ int apf_y_estimator_threshold_squared(double rho, double lambda_y_squared, doubl
     const double shifted = rho + 0.5;
     *threshold_squared = rho * rho * (lambda_y_squared + (1.0 + 1.0 / (shifted * shifted)) * initial_trace_squared);
     return APF_OK;
+}
+
+int apf_g_estimator(apf_ctx* ctx, apf_system* sys, int32_t n_g, const int32_t* g_restr_offsets,
+                    const int32_t* g_restr_dofs, const double* g_restr_weights, int32_t g_restr_nnz, double tolerance,
+                    apf_g_estimator_result* result)
+{
+    if (!ctx || !sys || !g_restr_offsets || !result || n_g < 0 || g_restr_nnz < 0 || !(tolerance > 0.0) ||
+        (g_restr_nnz > 0 && (!g_restr_dofs || !g_restr_weights)))
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        APF_HOST_RANGE("call_g_estimator");
+        auto& S = sys->sys;
+        const std::size_t rows = static_cast<std::size_t>(S.in.n_y_cells) * 18;
+        apf::require(S.in.p == 1 && S.in.dim == 2, APF_ERR_INVALID,
+                     "G^delta estimator: 2+1D systems of degree 1 (G of degree 2)");
+        const std::vector<int> off(g_restr_offsets, g_restr_offsets + rows + 1);
+        const std::vector<int> dofs(g_restr_dofs, g_restr_dofs + g_restr_nnz);
+        const std::vector<double> w(g_restr_weights, g_restr_weights + g_restr_nnz);
+        const apf::GDeltaResult r = apf::g_delta(ctx->stream, S, n_g, off, dofs, w, tolerance);
+        *result = apf_g_estimator_result{};
+        result->lambda_difference_squared = r.lambda_difference_squared;
+        result->solve_relative_residual = r.relative_residual;
+        result->solve_iterations = r.iterations;
+        result->n_g = r.n_g;
+    });
 }
 
 int apf_write_cellwise_error_binary(apf_ctx* ctx, const char* path, int32_t n_cells, const int32_t* cell_ids,

@@ -125,4 +125,22 @@ namespace apf
         const int si = i / t.nt, ai = i % t.nt;
         return tri_basis(t.p, si, rx, ry) * seg_basis(t.p, ai, rt);
     }
+
+    // The same between degrees: basis function i of the degree-tb.p prism gx at node k of the
+    // degree-tn.p prism gy (a degree-p function lies in the degree-(p+1) space exactly)
+    __device__ __forceinline__ double transfer_between(const RefTables& tn, const RefTables& tb, const CellGeo& gy,
+                                                       const CellGeo& gx, int i, int k)
+    {
+        const int sk = k / tn.nt, ak = k % tn.nt;
+        const double xi = tn.tri_nodes[sk][0], eta = tn.tri_nodes[sk][1], tau = tn.time_nodes[ak];
+        const double px = gy.x0 + gy.J00 * xi + gy.J01 * eta;
+        const double py = gy.y0 + gy.J10 * xi + gy.J11 * eta;
+        const double pt = gy.t0 + gy.ht * tau;
+        const double dx = px - gx.x0, dy = py - gx.y0;
+        const double rx = gx.iJ00 * dx + gx.iJ01 * dy;
+        const double ry = gx.iJ10 * dx + gx.iJ11 * dy;
+        const double rt = (pt - gx.t0) / gx.ht;
+        const int si = i / tb.nt, ai = i % tb.nt;
+        return tri_basis(tb.p, si, rx, ry) * seg_basis(tb.p, ai, rt);
+    }
 }

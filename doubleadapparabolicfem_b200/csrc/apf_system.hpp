@@ -80,6 +80,15 @@ namespace apf
     // which lies inside it; src_index NULL = identity.  Exact for nested prisms.
     void nodal_transfer(cudaStream_t s, int p, int n, const double* dst_geo, const int* src_index, const double* src_geo,
                         const double* src, double* dst);
+    // true-DOF values of a degree-q space (restriction off/dofs/w on n cells of geometry
+    // dst_geo) interpolating the degree-p function v (true DOFs through the restriction
+    // soff/sdofs/sw of the source cells src_index[c] (NULL = c), geometry src_geo) at its
+    // nodes; each DOF is written from its first unconstrained occurrence (deterministic).
+    // Exact when the source function lies in the degree-q space (nested cells, p <= q).
+    void interpolate_to_space(cudaStream_t s, int q, int p, int n, const double* dst_geo, const int* src_index,
+                              const double* src_geo, const int* soff, const int* sdofs, const double* sw,
+                              const double* v, const int* off, const int* dofs, const double* w, int n_true,
+                              double* out);
     // out[c] = v_c^T A_c v_c: the local A_y energy (int grad_x v . M grad_x v) of nodal values
     // v_c on prism c (m: 3 per cell or NULL = identity)
     void nodal_energy(cudaStream_t s, int p, int n, const double* geo, const double* m, const double* v, double* out);

@@ -76,6 +76,27 @@ def x_marking_indicator_components(blocks: MainSystemBlocks):
     return out, {name: getattr(tot, name) for name, _ in tot._fields_}
 
 
+def g_estimator(blocks: MainSystemBlocks, n_g: int, g_offsets: np.ndarray, g_dofs: np.ndarray,
+                g_weights: np.ndarray, tolerance: float = 1e-14):
+    """The adaptive driver's G^delta estimator on the last solve, mirroring
+    ``AdaptiveDriver::compute_g_estimator_for_accepted_inner_iteration_``
+    (algorithm/adaptive_driver.hpp:2690-2900): the degree-(p+1) space G on the Y cells given
+    by its flattened CellRestriction (offsets [n_y_cells * 18 + 1] for p = 1, the Y cells in
+    input order), A_G lambda_G = f_G - B(X, G)^T u_delta, and ||lambda_G - lambda_delta||^2 in
+    the A_G energy.  Returns a dict (``lambda_difference_squared``, ``solve_relative_residual``,
+    ``solve_iterations``, ``n_g``)."""
+    off = np.ascontiguousarray(g_offsets, dtype=np.int32)
+    dofs = np.ascontiguousarray(g_dofs, dtype=np.int32)
+    w = np.ascontiguousarray(g_weights, dtype=np.float64)
+    if dofs.size != w.size or off.size != blocks.problem.n_y_cells * 18 + 1:
+        raise ValueError("the G restriction does not match the Y cells (p = 1: 18 local rows per cell)")
+    res = _lib.GEstimatorResult()
+    ctx = blocks.ctx
+    ctx.check(ctx.lib.apf_g_estimator(ctx.handle, blocks.handle, int(n_g), _ptr(off), _ptr(dofs), _ptr(w), dofs.size,
+                                      float(tolerance), C.byref(res)))
+    return {name: getattr(res, name) for name, _ in res._fields_}
+
+
 def y_estimator_threshold_squared(rho: float, lambda_y_squared: float, initial_trace_squared: float) -> float:
     """rho^2 (lambda^2 + (1 + 1/(rho + 1/2)^2) trace^2)
     (algorithm/detail/indicator_utilities.hpp:475-491); raises for rho <= 0."""

@@ -362,6 +362,29 @@ int apf_x_indicators(apf_ctx* ctx, apf_system* sys, int pointers_on_device, doub
 int apf_y_estimator_threshold_squared(double rho, double lambda_y_squared, double initial_trace_squared,
                                       double* threshold_squared);
 
+/* ---- G^delta estimator ------------------------------------------------------------ */
+typedef struct apf_g_estimator_result
+{
+    double lambda_difference_squared; /* ||lambda_G - lambda_delta||^2 in the A_G energy */
+    double solve_relative_residual;   /* ||rhs_G - A_G lambda_G|| / ||rhs_G|| of the CG solve */
+    int solve_iterations;
+    int n_g;                          /* true DOFs of G */
+} apf_g_estimator_result;
+
+/* The adaptive driver's G^delta estimator on the solution of the last apf_solve_minres
+ * call, replacing AdaptiveDriver::compute_g_estimator_for_accepted_inner_iteration_
+ * (algorithm/adaptive_driver.hpp:2690-2900): the space G of degree p+1 on the system's Y
+ * cells (broken in time, FESpace<GT, FiniteElementTraits<GT, p+1, p+1>, SpaceOnlyPolicy>),
+ * given by its flattened CellRestriction (host arrays: offsets [n_y_cells * ndof_G + 1] with
+ * ndof_G = (p+2)(p+3)/2 (p+2), the Y cells in the system's order; n_g true DOFs);
+ * A_G lambda_G = f_G - B(X, G)^T u_delta solved by AMG-preconditioned CG to the relative
+ * residual `tolerance` (the reference solves directly), and ||lambda_G - lambda_delta||^2_{A_G}
+ * with lambda_delta prolonged nodally into G (g_lambda_difference_squared).  2+1D systems of
+ * degree 1 (G of degree 2).  APF_ERR_NOT_CONVERGED when CG misses the tolerance. */
+int apf_g_estimator(apf_ctx* ctx, apf_system* sys, int32_t n_g, const int32_t* g_restr_offsets,
+                    const int32_t* g_restr_dofs, const double* g_restr_weights, int32_t g_restr_nnz, double tolerance,
+                    apf_g_estimator_result* result);
+
 /* ---- estimator artifacts ---------------------------------------------------------- */
 /* The reference's binary files of an estimate, written from per-cell arrays (host, or
  * device with pointers_on_device = 1 and a context; ctx may be NULL for host arrays).

@@ -642,3 +642,71 @@ def nodal_values(restr: Restriction, v):
     out = np.zeros(len(restr.offsets) - 1)
     np.add.at(out, rows, restr.weights * v[restr.dofs])
     return out.reshape(n, restr.ndof)
+
+
+# ----------------------------------------------------------------------------
+# the driver's G^delta estimator (algorithm/adaptive_driver.hpp:2690-2900)
+# ----------------------------------------------------------------------------
+def prism_nodes(q: int):
+    """Reference nodes of the degree-q prism in local order i_s*(q+1)+i_t."""
+    tn = triangle_nodes(q)
+    tt = np.arange(q + 1) / q
+    return np.array([(a, b, t) for (a, b) in tn for t in tt])
+
+
+def interpolate_nodal(p: int, src_nodal, src_geom, src_index, dst_geom, q: int):
+    """[n_dst, nodes of degree q]: the degree-p prism function of each source cell (nodal
+    values src_nodal[src_index[c]]) at the degree-q nodes of the destination cell c, which
+    lies inside it (exact for nested cells: prolong_true_coefficients_nodal evaluates the
+    same way)."""
+    ref = prism_nodes(q)
+    n = dst_geom.shape[0]
+    si = np.arange(n) if src_index is None else np.asarray(src_index)
+    out = np.empty((n, ref.shape[0]))
+    for c in range(n):
+        d, s = dst_geom[c], src_geom[si[c]]
+        px = d[0] + (d[2] - d[0]) * ref[:, 0] + (d[4] - d[0]) * ref[:, 1]
+        py = d[1] + (d[3] - d[1]) * ref[:, 0] + (d[5] - d[1]) * ref[:, 1]
+        pt = d[6] + (d[7] - d[6]) * ref[:, 2]
+        J = np.array([[s[2] - s[0], s[4] - s[0]], [s[3] - s[1], s[5] - s[1]]])
+        rs = np.linalg.solve(J, np.stack([px - s[0], py - s[1]]))
+        pts = np.stack([rs[0], rs[1], (pt - s[6]) / (s[7] - s[6])], axis=1)
+        vals, _ = prism_basis(p, pts)
+        out[c] = vals @ src_nodal[si[c]]
+    return out
+
+
+def true_from_nodal(restr: Restriction, local, n: int):
+    """True-DOF vector from per-cell nodal values: each true DOF takes the value at its first
+    unconstrained occurrence (a local row with the single entry (dof, 1))."""
+    out = np.full(n, np.nan)
+    off = restr.offsets
+    flat = local.ravel()
+    for row in range(len(off) - 1):
+        a, b = off[row], off[row + 1]
+        if b - a == 1 and restr.weights[a] == 1.0 and np.isnan(out[restr.dofs[a]]):
+            out[restr.dofs[a]] = flat[row]
+    return out
+
+
+def g_delta(prob: MainProblem, g_restr: Restriction, n_g: int, lam, u, ell=None, zero_tol=1e-15):
+    """||lambda_G - lambda_delta||^2_{A_G} on the Y cells with the degree-(p+1) space G
+    (restriction g_restr): A_G lambda_G = f_G - B(X,G)^T u_delta.  B(X,G)^T u_delta is the
+    mixed form with u_delta interpolated into G (exact: X restricted to a Y cell is a
+    degree-p polynomial, G broken in time), so every block is a same-degree G form."""
+    import scipy.sparse.linalg as spl
+    ny = prob.y_geom.shape[0]
+    q = prob.p + 1
+    gprob = MainProblem(p=q, y_geom=prob.y_geom, x_geom=prob.y_geom, y_to_x=np.arange(ny), y_restr=g_restr,
+                        x_restr=g_restr, n_lambda=n_g, n_u=n_g, m_cells=prob.m_cells)
+    blocks = assemble_main_blocks(gprob, ell=ell, zero_tol=zero_tol)
+    u_g = true_from_nodal(g_restr, interpolate_nodal(prob.p, nodal_values(prob.x_restr, u), prob.x_geom,
+                                                     prob.y_to_x, prob.y_geom, q), n_g)
+    l_g = true_from_nodal(g_restr, interpolate_nodal(prob.p, nodal_values(prob.y_restr, lam), prob.y_geom, None,
+                                                     prob.y_geom, q), n_g)
+    A = blocks["A_y"].tocsc()
+    rhs = blocks["f"] - blocks["B"].T @ u_g
+    lam_g = spl.spsolve(A, rhs)
+    d = lam_g - l_g
+    return float(d @ (A @ d)), {"A_g": A, "f_g": blocks["f"], "rhs_g": rhs, "lambda_g": lam_g,
+                                "lambda_delta_in_g": l_g, "u_in_g": u_g}

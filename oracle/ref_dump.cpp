@@ -18,7 +18,10 @@
 //     cellwise_error.bin, cellwise_error_components.bin and x_indicator_components.bin
 //     (src/finite_element/io/write_cellwise_error_binary.hpp,
 //      src/finite_element/io/write_cellwise_error_components_binary.hpp,
-//      algorithm/output/iteration_snapshot_writer.hpp:173-233).
+//      algorithm/output/iteration_snapshot_writer.hpp:173-233),
+//   * with APF_REF_ESTIMATE and APF_REF_G (2+1D P1): the driver's G^delta estimator, its
+//     space's restriction, A_G, f_G, rhs_G = f_G - B(X,G)^T u_delta, lambda_G and
+//     ||lambda_G - lambda_delta||^2_{A_G} (algorithm/adaptive_driver.hpp:2690-2900).
 //
 // usage: apf_ref_dump <dim:1|2> <p:1|2> <uniform_levels> <example> <outdir>
 //        apf_ref_dump bench <p:1|2> <uniform_levels> <example> <reps>
@@ -58,6 +61,8 @@
 #include "finite_element/io/write_cellwise_error_components_binary.hpp"
 #include "algorithm/output/iteration_snapshot_writer.hpp"
 #include "finite_element/assembly/constrained_dofs.hpp"
+#include "finite_element/fespace/prolongation.hpp"
+#include "linear_algebra/operations/linalg_ops.hpp"
 #include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
 #include "algorithm/detail/indicator_utilities.hpp"
 #include "mesh/mesh_traits.hpp"
@@ -135,6 +140,59 @@ namespace
     using apf_oracle::apply_adaptive_options_2d;
     using apf_oracle::env_int;
     using apf_oracle::uniform_isotropic_refine;
+
+    // The driver's G^delta estimator on the accepted Y mesh, step by step as
+    // AdaptiveDriver::compute_g_estimator_for_accepted_inner_iteration_ runs it
+    // (algorithm/adaptive_driver.hpp:2690-2900): the space G of degree p+1 on the Y cells
+    // (broken in time), A_G, f_G, B(X,G), rhs = f_G - B^T u_delta, lambda_G (direct solve),
+    // lambda_delta prolonged nodally into G, and ||lambda_G - lambda_delta||^2_{A_G}.
+    template<int QSpace, int QTime, class XSpace, class YSpace, class Problem, class YFunction, class XFunction>
+    void dump_g_delta(const std::string& dir, const XSpace& x_space, YSpace& y_space, const std::vector<int>& y_cells,
+                      const Problem& problem, const YFunction& lambda_delta, const XFunction& u_delta)
+    {
+        using GT = typename YSpace::GT;
+        using YFET = typename YSpace::FETraitsType;
+        using GFET = finite_element::FiniteElementTraits<GT, YFET::p_space_v + 1, YFET::p_time_v + 1>;
+        using GSpace = finite_element::FESpace<GT, GFET, finite_element::SpaceOnlyPolicy>;
+        finite_element::FESpaceInitializationOptions options;
+        options.search_index = finite_element::SearchIndexBuildMode::Disabled;
+        options.build_refinement_indices = false;
+        options.build_edge_interval_index = false;
+        GSpace g_space(y_space.unsafe_mesh_ref());
+        g_space.initialize(y_space.active_cells(), options);
+        typename Backend::SparseMatrix A_g, B_xg;
+        typename Backend::Vector f_g;
+        finite_element::assembly::detail::AssemblySpaceCache<GSpace> g_cache(g_space);
+        finite_element::assembly::detail::AssemblySpaceCache<XSpace> x_cache(x_space);
+        finite_element::assembly::detail::ActiveAncestorCache<XSpace> ancestors(x_space);
+        finite_element::assembly::assemble_mat_A<QSpace + 1, QTime + 1, Backend>(A_g, g_space, problem.M, g_cache,
+                                                                                1e-15);
+        finite_element::assembly::assemble_vec_f<QSpace + 1, QTime + 1>(f_g, g_space, problem.ell, g_cache, 1e-15);
+        finite_element::assembly::assemble_mat_B<QSpace + 1, QTime + 1, Backend>(B_xg, x_space, g_space, x_cache,
+                                                                                g_cache, ancestors, problem.M, 1e-15);
+        const auto rhs_g = la::ops::subtract(f_g, la::ops::transpose_matvec(B_xg, u_delta.true_coefficients()));
+        typename Backend::Solver solver;
+        la::concepts::SolverOptions lu;
+        lu.solver = la::concepts::SolverType::SparseLU;
+        solver.compute(A_g, lu);
+        typename Backend::Vector lambda_g;
+        solver.solve(rhs_g, lambda_g);
+        const auto lambda_delta_in_g = finite_element::fespace::prolong_true_coefficients_nodal(lambda_delta, g_space);
+        const auto diff = la::ops::subtract(lambda_g, lambda_delta_in_g);
+        const double energy =
+            la::ops::quadratic_form<typename Backend::SparseMatrix, typename Backend::SparseBuilder>(A_g, diff);
+        dump_restrictions(dir, "g_restriction", g_space, y_cells);
+        dump_csc(dir, "A_g", A_g);
+        dump_vec(dir, "f_g", f_g);
+        dump_vec(dir, "rhs_g", rhs_g);
+        dump_vec(dir, "lambda_g", lambda_g);
+        dump_vec(dir, "lambda_delta_in_g", lambda_delta_in_g);
+        const std::vector<double> e{energy};
+        apf_oracle::write_npy(dir + "/g_lambda_difference_squared.npy", e);
+        const std::vector<int> ng{g_space.dof_handler_ref().n_true_dofs()};
+        apf_oracle::write_npy(dir + "/g_n_dofs.npy", ng);
+        std::fprintf(stderr, "g_delta: n_g=%d ||lambda_G - lambda_delta||^2_A=%.12e\n", ng[0], energy);
+    }
 
     // Times the reference's own CPU assembly path (main blocks + graph-norm block)
     // on the uniform mesh of outer level `levels`; prints one JSON line.
@@ -426,6 +484,10 @@ namespace
             std::fprintf(stderr, "estimate: flux=%.6e div=%.6e recon=%.6e eta=%.6e\n",
                          state.flux_diagnostics.total_flux(), state.flux_diagnostics.total_residual(),
                          state.reconstruction_y_squared.total(), state.estimator.total());
+            if constexpr (P == 1)
+                if (std::getenv("APF_REF_G") != nullptr)
+                    dump_g_delta<QSpace, QTime>(dir, x_space, y_space, y_cells, example.problem, state.lambda_delta,
+                                                state.u_delta);
         }
         return 0;
     }

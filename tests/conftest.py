@@ -20,6 +20,8 @@ GOLDEN_CASES = ["p1_l1_smooth", "p1_l2_smooth", "p2_l1_smooth", "p1_l1_nonmatchi
 # reference's own marking) and a diffusivity per X cell (p1_adapt_kappa, p1_kappa_uniform)
 ADAPTIVE_CASES = ["p1_adapt_smooth", "p1_adapt_kappa", "p1_adapt_nonmatching", "p2_adapt_smooth"]
 KAPPA_CASES = ["p1_adapt_kappa", "p1_kappa_uniform"]
+# fixtures with the driver's G^delta estimator (APF_REF_G): P1 uniform, adaptive, adaptive + kappa
+G_DELTA_CASES = ["p1_l2_smooth", "p1_adapt_smooth", "p1_adapt_kappa"]
 GOLDEN_CASES_1D = ["d1_l2_smooth", "d1_l2_nonmatching", "d1_l5_smooth"]
 
 
@@ -60,6 +62,15 @@ def load_golden(name):
                          dim_space=dim)
     example = str(z["meta_example"][0])
     return prob, out, example
+
+
+def load_g_space(name):
+    """The reference's G space (degree p+1 on the Y cells) of a G^delta fixture: (n_g,
+    Restriction with 18 local rows per Y cell) and the fixture arrays."""
+    import apf_oracle as O
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    restr = O.Restriction(z["g_restriction_offsets"], z["g_restriction_dofs"], z["g_restriction_weights"], 18)
+    return int(z["g_n_dofs"][0]), restr, z
 
 
 def to_product_problem(prob, example):

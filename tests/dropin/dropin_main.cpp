@@ -21,13 +21,19 @@
 //       (device assembly, graph-norm block and MINRES; the reference's host estimator, marking
 //       and refinement) and once with the Eigen backend and its direct solver, each on its own
 //       copy of the spaces; per pass the estimator totals, the marked cells of each run and the
-//       Y meshes (both refined by the direct-solve run's marks).
+//       Y meshes (both refined by the direct-solve run's marks);
+//   adaptive <p> <levels> <example> <outer_cycles> <tol> [compare:1|0]
+//       the reference's whole adaptive algorithm (adaptive_algorithm::run_adaptive_driver,
+//       algorithm/adaptive_driver.hpp:3508) with each backend, each on its own spaces: per outer
+//       cycle the X and Y DOF counts, the number of inner Y iterations and the estimator totals
+//       (compare = 0: the b200 backend only).
 //
 // The adaptive-mesh options of the oracle driver (APF_REF_X_POINTS, APF_REF_X_ROUNDS,
 // APF_REF_KAPPA, APF_REF_KAPPA_BLOCKS) apply to all modes.  Each mode prints one JSON line.
 #include "apf_b200_backend.hpp" // before the reference's solver headers (see its header comment)
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <iterator>
 #include <cstdio>
@@ -35,6 +41,7 @@
 #include <string>
 #include <vector>
 
+#include "algorithm/adaptive_driver.hpp"
 #include "algorithm/example_registry.hpp"
 #include "algorithm/examples/space_time_2d/initial_data_2d_examples.hpp"
 #include "algorithm/examples/space_time_2d/space_time_2d_example.hpp"
@@ -299,6 +306,56 @@ namespace
         return 0;
     }
 
+    // the reference's whole adaptive algorithm (run_adaptive_driver, algorithm/adaptive_driver.hpp:3508)
+    // with each backend: outer cycles of inner Y loops (solve, estimate, Doerfler marking, Y
+    // refinement) and X marking + refinement
+    template<int P>
+    int run_adaptive(int levels, const std::string& name, int outer, double tol, bool compare)
+    {
+        using S = Spaces<P>;
+        S a(name, levels), b(name, levels);
+        adaptive_algorithm::AdaptiveParameters par;
+        par.max_outer_iterations = outer;
+        par.polynomial_degree = P;
+        par.output.print_iteration_tables = !compare; // progress on stderr for long runs
+        par.output.save_mesh_statistics = false;
+        par.output.stream = &std::cerr;
+        const auto t0 = std::chrono::steady_clock::now();
+        typename B200::Solver sa;
+        const auto ra = adaptive_algorithm::run_adaptive_driver<S::QSpace, S::QTime, B200>(
+            a.x_space, a.y_space, a.example.problem, sa, minres_options(tol), par);
+        const auto t1 = std::chrono::steady_clock::now();
+        typename EigenB::Solver sb;
+        la::concepts::SolverOptions lu;
+        lu.solver = la::concepts::SolverType::SparseLU;
+        par.max_outer_iterations = compare ? outer : 0;
+        const auto rb = adaptive_algorithm::run_adaptive_driver<S::QSpace, S::QTime, EigenB>(
+            b.x_space, b.y_space, b.example.problem, sb, lu, par);
+        const auto t2 = std::chrono::steady_clock::now();
+        auto dump = [](const auto& r) {
+            std::string out = "[";
+            for (std::size_t k = 0; k < r.outer_iterations.size(); ++k)
+            {
+                const auto& o = r.outer_iterations[k];
+                char buf[512];
+                std::snprintf(buf, sizeof(buf),
+                              "%s{\"outer\": %d, \"x_dofs\": %d, \"y_dofs\": %d, \"inner\": %zu, "
+                              "\"eta_squared\": %.15e, \"lambda_y_squared\": %.15e, "
+                              "\"initial_trace_squared\": %.15e, \"y_estimator_squared\": %.15e}",
+                              k ? ", " : "", o.outer_iteration, o.n_x_true_dofs_before, o.n_y_true_dofs_after,
+                              o.inner_iterations.size(), o.eta_squared, o.lambda_y_squared,
+                              o.initial_trace_squared, o.y_estimator_squared);
+                out += buf;
+            }
+            return out + "]";
+        };
+        std::printf("{\"mode\": \"adaptive\", \"p\": %d, \"levels\": %d, \"tol\": %.1e, \"b200_s\": %.3f, "
+                    "\"direct_s\": %.3f, \"b200\": %s, \"direct\": %s}\n",
+                    P, levels, tol, std::chrono::duration<double>(t1 - t0).count(),
+                    std::chrono::duration<double>(t2 - t1).count(), dump(ra).c_str(), dump(rb).c_str());
+        return 0;
+    }
+
     template<int P>
     int dispatch(const std::string& mode, int argc, char** argv)
     {
@@ -310,6 +367,9 @@ namespace
             return run_solve<P>(levels, example, std::atof(argv[5]));
         if (mode == "cycle" && argc >= 7)
             return run_cycle<P>(levels, example, std::atoi(argv[5]), std::atof(argv[6]));
+        if (mode == "adaptive" && argc >= 7)
+            return run_adaptive<P>(levels, example, std::atoi(argv[5]), std::atof(argv[6]),
+                                   argc < 8 || std::atoi(argv[7]) != 0);
         return 2;
     }
 }
@@ -318,7 +378,7 @@ int main(int argc, char** argv)
 {
     if (argc < 5)
     {
-        std::fprintf(stderr, "usage: apf_dropin_test blocks|solve|cycle <p:1|2> <levels> <example> [...]\n");
+        std::fprintf(stderr, "usage: apf_dropin_test blocks|solve|cycle|adaptive <p:1|2> <levels> <example> [...]\n");
         return 2;
     }
     const std::string mode = argv[1];

@@ -4,7 +4,9 @@ Runs oracle/_ref/apf_ref_dump (the reference's own templates compiled by
 oracle/Makefile against oracle/shim) on small uniform meshes and packs each case
 into one .npz: mesh and DOF maps, assembled blocks, and the reference's whole inner
 iteration (direct main solve, slab reconstruction, vertex-patch flux solves,
-per-cell indicators), the driver's X-marking indicators and the reference's binary
+per-cell indicators), the driver's X-marking indicators, on the cases marked APF_REF_G the
+driver's G^delta estimator (its space's restriction, A_G, f_G, rhs_G, lambda_G and
+||lambda_G - lambda_delta||^2_{A_G}), and the reference's binary
 artifacts of the estimate (cellwise_error.bin, cellwise_error_components.bin, as bytes).  Also extracts the uniform-refinement rows (exact DOF counts and
 6-significant-digit estimator values) of the reference's published paper data
 (algorithm_data_plot/{1d,2d}/*.csv) into paper_uniform_rows.json.
@@ -30,7 +32,7 @@ REF_BIN = os.path.join(REPO, "oracle", "_ref", "apf_ref_dump")
 CASES = [
     # (name, dim, p, outer level, example[, environment of the adaptive mode])
     ("p1_l1_smooth", 2, 1, 1, "smooth_initial"),
-    ("p1_l2_smooth", 2, 1, 2, "smooth_initial"),
+    ("p1_l2_smooth", 2, 1, 2, "smooth_initial", {"APF_REF_G": "1"}),
     ("p2_l1_smooth", 2, 2, 1, "smooth_initial"),
     ("p1_l1_nonmatching", 2, 1, 1, "non_matching_initial"),
     ("p1_l3_smooth", 2, 1, 3, "smooth_initial"),
@@ -43,10 +45,11 @@ CASES = [
     # one pass of the reference's inner loop (marking + refine_test_space_from_marked_source_cells),
     # optionally a diffusivity kappa per X cell log-uniform in [lo, hi]
     ("p1_adapt_smooth", 2, 1, 2, "smooth_initial",
-     {"APF_REF_X_POINTS": "0.3,0.3,0.3;0.71,0.62,0.8", "APF_REF_X_ROUNDS": "3", "APF_REF_Y_PASSES": "1"}),
+     {"APF_REF_X_POINTS": "0.3,0.3,0.3;0.71,0.62,0.8", "APF_REF_X_ROUNDS": "3", "APF_REF_Y_PASSES": "1",
+      "APF_REF_G": "1"}),
     ("p1_adapt_kappa", 2, 1, 2, "smooth_initial",
      {"APF_REF_X_POINTS": "0.3,0.3,0.3;0.71,0.62,0.8", "APF_REF_X_ROUNDS": "3", "APF_REF_Y_PASSES": "1",
-      "APF_REF_KAPPA": "7:0.01:100"}),
+      "APF_REF_KAPPA": "7:0.01:100", "APF_REF_G": "1"}),
     ("p1_adapt_nonmatching", 2, 1, 1, "non_matching_initial",
      {"APF_REF_X_POINTS": "0.2,0.45,0.1", "APF_REF_X_ROUNDS": "4", "APF_REF_Y_PASSES": "1"}),
     ("p1_kappa_uniform", 2, 1, 2, "smooth_initial", {"APF_REF_KAPPA": "3:0.1:10"}),

@@ -19,8 +19,8 @@ import os
 import numpy as np
 import pytest
 
-from conftest import (ADAPTIVE_CASES, GOLDEN, HHAT_RESIDUE, KAPPA_CASES, assert_same_sparse, load_golden,
-                      to_product_problem)
+from conftest import (ADAPTIVE_CASES, G_DELTA_CASES, GOLDEN, HHAT_RESIDUE, KAPPA_CASES, assert_same_sparse,
+                      load_g_space, load_golden, to_product_problem)
 
 pytestmark = pytest.mark.gpu
 
@@ -147,3 +147,34 @@ def test_kappa_fixture_coefficients_differ_per_cell(name):
     z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     k = z["kappa_x"]
     assert k.max() / k.min() > (1e3 if name == "p1_adapt_kappa" else 50.0)
+
+
+@pytest.mark.parametrize("name", G_DELTA_CASES)
+def test_g_estimator_matches_reference(gpu_ctx, name):
+    """The driver's G^delta estimator on the device (apf_g_estimator: the degree-2 space G on
+    the Y cells from the reference's own restriction, A_G lambda_G = f_G - B(X,G)^T u_delta by
+    AMG-preconditioned CG to 1e-14) after MINRES to a true residual of 1e-13, against the
+    reference's value on its direct solution: ||lambda_G - lambda_delta||^2_{A_G} to 1e-8."""
+    from doubleadapparabolicfem_b200.estimator import g_estimator
+    from doubleadapparabolicfem_b200.solver import SolverOptions, solve_saddle_system_with_preconditioner
+    blocks, prob, ref, z = _assemble(gpu_ctx, name)
+    blocks.assemble_parabolic_graph_norm_approximation()
+    _, diag = solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=1e-13), copy_out=False)
+    assert diag["converged"] == 1
+    n_g, g, _ = load_g_space(name)
+    res = g_estimator(blocks, n_g, g.offsets, g.dofs, g.weights)
+    want = float(z["g_lambda_difference_squared"][0])
+    assert res["n_g"] == n_g and res["solve_iterations"] > 0 and res["solve_relative_residual"] <= 1e-14, res
+    assert abs(res["lambda_difference_squared"] - want) <= 1e-8 * want, (res, want)
+
+
+def test_g_estimator_rejects_a_mismatched_space(gpu_ctx):
+    """A restriction whose row count does not match the Y cells is refused before any launch."""
+    from doubleadapparabolicfem_b200 import _lib
+    from doubleadapparabolicfem_b200.estimator import g_estimator
+    blocks, prob, ref, z = _assemble(gpu_ctx, "p1_l2_smooth")
+    n_g, g, _ = load_g_space("p1_l2_smooth")
+    with pytest.raises(ValueError):
+        g_estimator(blocks, n_g, g.offsets[:-18], g.dofs, g.weights)
+    with pytest.raises(_lib.ApfError):   # no solution yet
+        g_estimator(blocks, n_g, g.offsets, g.dofs, g.weights)

@@ -114,3 +114,21 @@ def test_dropin_adaptive_inner_loop_matches_eigen_backend():
         assert pas["minres_iterations"] > 0 and pas["minres_true_residual"] <= 1e-12, pas
     # the later passes run on the refined (Y finer than X) test space
     assert d["passes"][2]["y_cells"][0] > d["passes"][1]["y_cells"][0] > d["passes"][0]["y_cells"][0]
+
+
+@needs_program
+@pytest.mark.gpu
+def test_dropin_reference_adaptive_driver_matches_eigen_backend():
+    """The reference's whole adaptive algorithm (run_adaptive_driver: inner Y loops, X marking
+    and refinement) for three outer cycles with kappa per X cell (no ties in the marking): the
+    b200 backend (device assembly, graph-norm block, MINRES to 1e-12) follows the same
+    trajectory as the Eigen backend with its direct solver -- the same X and Y DOF counts and
+    inner iteration counts every cycle, and the same estimator totals to 1e-8."""
+    d = _json(_run(["adaptive", 1, 1, "smooth_initial", 3, 1e-12], env={"APF_REF_KAPPA": "11:0.1:10"}))
+    a, b = d["b200"], d["direct"]
+    assert len(a) == len(b) == 3
+    for ra, rb in zip(a, b):
+        assert (ra["x_dofs"], ra["y_dofs"], ra["inner"]) == (rb["x_dofs"], rb["y_dofs"], rb["inner"]), (ra, rb)
+        for key in ("eta_squared", "lambda_y_squared", "y_estimator_squared"):
+            assert abs(ra[key] - rb[key]) <= 1e-8 * abs(rb[key]), (key, ra, rb)
+    assert a[-1]["x_dofs"] > a[0]["x_dofs"]

@@ -6,7 +6,8 @@ import os
 import numpy as np
 import pytest
 
-from conftest import ADAPTIVE_CASES, GOLDEN, GOLDEN_CASES, HHAT_RESIDUE, assert_same_sparse, load_golden
+from conftest import (ADAPTIVE_CASES, G_DELTA_CASES, GOLDEN, GOLDEN_CASES, HHAT_RESIDUE, assert_same_sparse,
+                      load_g_space, load_golden)
 
 import apf_oracle as O
 
@@ -86,6 +87,29 @@ def test_oracle_slab_reconstruction_matches_reference(name):
     perm = [order[(int(k), int(c))] for k, c in zip(slab, src)]
     theirs = z["slab_lambda_tilde"][perm]
     assert np.abs(mine - theirs).max() <= 1e-12 * np.abs(theirs).max()
+
+
+@pytest.mark.parametrize("name", G_DELTA_CASES)
+def test_oracle_g_delta_matches_reference(name):
+    """The driver's G^delta estimator restated with every block a same-degree G form
+    (u_delta and lambda_delta interpolated into G) against the reference's own computation
+    on the same solution: A_G pattern and values to 1e-12 (P2 stiffness entries that cancel
+    exactly leave residues below 1e-13 of the largest entry that the reference keeps where
+    kappa lifts them above its 1e-15 filter: the significant pattern is compared), f_G, rhs_G = f_G -
+    B(X,G)^T u_delta and lambda_G to 1e-12 of their largest entries, and
+    ||lambda_G - lambda_delta||^2_{A_G} to 1e-10."""
+    import scipy.sparse as sp
+    prob, ref, example = load_golden(name)
+    n_g, g, z = load_g_space(name)
+    e, info = O.g_delta(prob, g, n_g, z["lambda_delta"], z["u_delta"])
+    A_ref = sp.csc_matrix((z["A_g_values"], z["A_g_inner"], z["A_g_outer"]),
+                          shape=tuple(int(v) for v in z["A_g_shape"]))
+    assert_same_sparse(A_ref, info["A_g"], 1e-12, "A_G", residue=HHAT_RESIDUE)
+    for key in ("f_g", "rhs_g", "lambda_g", "lambda_delta_in_g"):
+        scale = max(np.abs(z[key]).max(), 1e-300)
+        assert np.abs(info[key] - z[key]).max() <= 1e-12 * scale, key
+    want = float(z["g_lambda_difference_squared"][0])
+    assert want > 0 and abs(e - want) <= 1e-10 * want, (e, want)
 
 
 def _paper_rows():
