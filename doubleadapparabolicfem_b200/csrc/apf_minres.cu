@@ -10,7 +10,8 @@
 //   * batches of `true_residual_check_interval` iterations; after each batch the FP64
 //     true residual ||K x - b|| / ||b|| accepts; if the backend had converged but the
 //     true residual did not, the backend tolerance is multiplied by 0.1 (floor
-//     max(eps, tol sqrt(eps))); the batch restarts from the current iterate.
+//     max(eps, tol sqrt(eps))); the batch restarts from the current iterate (stacked
+//     problems: a restart that needs no iteration tightens the tolerance again).
 // All Lanczos scalars live in device memory; the host only reads the status every
 // `kCheckEvery` iterations, so iterations run back to back on the stream.
 #include <algorithm>
@@ -684,7 +685,14 @@ namespace apf
                 sum.converged = true;
                 return sum;
             }
-            if (!std::isfinite(rel) || !std::isfinite(backend_err) || its <= 0)
+            if (!std::isfinite(rel) || !std::isfinite(backend_err))
+                return sum;
+            // a batch with no iteration: the backend test already held at the restart.  With
+            // one problem that means the true residual met the target (returned above); with
+            // stacked problems (parts) the global residual can be below the backend tolerance
+            // while one problem's own residual is not, so the tolerance is tightened further
+            // until its floor
+            if (its <= 0 && (!opt.parts || backend_tol <= min_backend))
                 return sum;
             if (backend_conv)
                 backend_tol = std::max(min_backend, backend_tol * 0.1);

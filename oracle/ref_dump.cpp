@@ -226,6 +226,7 @@ namespace
             // own sparse solvers are Eigen / PARDISO, absent here): its time is reported
             // separately, and the reference's own stages are the rest
             double flux = 0.0, solve_total = 0.0;
+            std::string stage_list; // per repetition: wall time less the main solve
             for (int r = 0; r < reps; ++r)
             {
                 const auto t0 = std::chrono::steady_clock::now();
@@ -242,12 +243,16 @@ namespace
                 total += dt;
                 solve_total += state.main_solve_setup_seconds + state.main_solve_solve_seconds;
                 flux = state.flux_diagnostics.total_flux();
+                char buf[64];
+                std::snprintf(buf, sizeof(buf), "%s%.6f", r ? ", " : "",
+                              dt - state.main_solve_setup_seconds - state.main_solve_solve_seconds);
+                stage_list += buf;
             }
             std::printf("{\"stage\": \"inner_iteration\", \"p\": %d, \"level\": %d, \"n_cells\": %d, \"n_dofs\": %d, "
                         "\"reps\": %d, \"mean_s\": %.6f, \"best_s\": %.6f, \"main_solve_mean_s\": %.6f, "
-                        "\"threads\": %d, \"flux_squared\": %.12e}\n",
+                        "\"threads\": %d, \"flux_squared\": %.12e, \"stage_s\": [%s]}\n",
                         P, levels, n_cells, n_dofs, reps, total / reps, best, solve_total / reps, omp_get_max_threads(),
-                        flux);
+                        flux, stage_list.c_str());
             return 0;
         }
         for (int r = 0; r < reps; ++r)
