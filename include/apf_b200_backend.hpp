@@ -31,6 +31,10 @@
  * algorithm/...).  A solve whose blocks were not assembled through this backend in the
  * same thread throws instead of solving on the host.
  *
+ * la::b200::estimate(y_space) returns the device estimate of the session's solved system in
+ * the reference's cellwise error types (for its marking), in place of the host stages of
+ * compute_adaptive_test_space_iteration after the main solve.
+ *
  * Coefficients: M and ell are evaluated at each Y cell's centroid (the device assembly takes
  * them constant per cell, exact for the reference's piecewise-constant coefficients); u0
  * must be one of the examples' initial data sin(pi x) sin(pi y) (sin(pi x) in 1+1D), 1 or 0,
@@ -69,6 +73,8 @@
 #include "finite_element/assembly/detail/active_cell_locator.hpp"
 #include "finite_element/system/assemble_saddle_problem.hpp"
 #include "finite_element/system/main_preconditioner_context.hpp"
+#include "finite_element/time_slabs/time_slab_cellwise_errors.hpp"
+#include "finite_element/time_slabs/time_slab_estimator_combination.hpp"
 
 namespace la::b200
 {
@@ -452,6 +458,66 @@ namespace la::b200
             d.g_scale = g_scale;
             return a;
         }
+    }
+}
+
+namespace la::b200
+{
+    // The equilibrated-flux estimate of the session's solved system in the reference's own
+    // types: per source Y cell flux^2 and div^2 (CellwiseEquilibratedFluxError), the Y
+    // reconstruction error (CellwiseSquaredError) and their combination by the reference's
+    // combine_time_slab_estimator_squared_errors_deterministic
+    // (time_slab_estimator_combination.hpp:90), ready for its marking
+    // (estimator.doerfler_marking_deterministic).  Replaces the host stages of
+    // compute_adaptive_test_space_iteration after the main solve (time_slab_adaptive_loop.hpp:
+    // slab reconstruction, vertex-patch flux solves, indicators) with apf_estimate.
+    struct DeviceEstimate
+    {
+        finite_element::time_slabs::CellwiseEquilibratedFluxError<int> flux{};
+        finite_element::time_slabs::CellwiseSquaredError<int> reconstruction_y_squared{};
+        finite_element::time_slabs::CellwiseTimeSlabEstimatorError<int> estimator{};
+        int n_slabs = 0;
+        int n_patches = 0;
+    };
+
+    // y_space: the Y space of the session's last assembly (its active cells in the same order)
+    template<class YSpace>
+    [[nodiscard]] DeviceEstimate estimate(const YSpace& y_space)
+    {
+        Session& s = session();
+        apf_ctx* ctx = s.context();
+        apf_system* sys = s.system();
+        if (sys == nullptr)
+            throw std::logic_error("b200 backend: estimate needs a system assembled and solved in this thread");
+        const std::vector<int> cells(y_space.active_cells().begin(), y_space.active_cells().end());
+        const std::size_t ny = cells.size();
+        std::vector<int32_t> vids;
+        constexpr int dim = YSpace::GT::dim_space_v;
+        if constexpr (dim == 2)
+        {
+            const auto& mesh = y_space.mesh_ref();
+            vids.reserve(3 * ny);
+            for (const int c : cells)
+                for (int k = 0; k < 3; ++k)
+                    vids.push_back(mesh.cell(c).spatial_vertex_ids[k]);
+        }
+        std::vector<double> flux(ny), div(ny), recon(ny), eta(ny);
+        apf_estimator_result res{};
+        check(ctx, apf_estimate(ctx, sys, dim == 2 ? vids.data() : nullptr, 0, flux.data(), div.data(), recon.data(),
+                                eta.data(), &res),
+              "apf_estimate");
+        DeviceEstimate out;
+        for (std::size_t k = 0; k < ny; ++k)
+        {
+            out.flux.by_source_cell_flux[cells[k]] = flux[k];
+            out.flux.by_source_cell_residual[cells[k]] = div[k];
+            out.reconstruction_y_squared.by_source_cell[cells[k]] = recon[k];
+        }
+        out.estimator = finite_element::time_slabs::combine_time_slab_estimator_squared_errors_deterministic(
+            out.flux, out.reconstruction_y_squared);
+        out.n_slabs = res.n_slabs;
+        out.n_patches = res.n_patches;
+        return out;
     }
 }
 

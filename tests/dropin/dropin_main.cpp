@@ -22,6 +22,11 @@
 //       and refinement) and once with the Eigen backend and its direct solver, each on its own
 //       copy of the spaces; per pass the estimator totals, the marked cells of each run and the
 //       Y meshes (both refined by the direct-solve run's marks);
+//   estimate <p> <levels> <example> <tol>
+//       after one pass of the reference's inner loop (Y finer than X): the device estimate in
+//       the reference's types (la::b200::estimate) on the b200 solve against the reference's
+//       host estimate on its direct solve -- per-cell flux^2 / recon^2 / eta^2, totals, slab
+//       count and the Doerfler marking of each;
 //   adaptive <p> <levels> <example> <outer_cycles> <tol> [compare:1|0]
 //       the reference's whole adaptive algorithm (adaptive_algorithm::run_adaptive_driver,
 //       algorithm/adaptive_driver.hpp:3508) with each backend, each on its own spaces: per outer
@@ -306,6 +311,69 @@ namespace
         return 0;
     }
 
+    // the device estimate in the reference's types (la::b200::estimate) against the reference's
+    // host estimate, after one pass of the reference's inner loop (Y finer than X, Y cells
+    // across several slabs): per source Y cell flux^2, recon^2 and eta^2, totals, the slab
+    // count and the Doerfler marking of the two estimates
+    template<int P>
+    int run_estimate(int levels, const std::string& name, double tol)
+    {
+        using S = Spaces<P>;
+        using XSpace = typename S::XSpace;
+        using YSpace = typename S::YSpace;
+        S a(name, levels), b(name, levels);
+        la::concepts::SolverOptions lu;
+        lu.solver = la::concepts::SolverType::SparseLU;
+        finite_element::time_slabs::AdaptiveTestSpaceIterationParameters<EigenB, XSpace, YSpace> pb;
+        {
+            typename EigenB::Solver s0;
+            const auto st0 = finite_element::time_slabs::compute_adaptive_test_space_iteration<S::QSpace, S::QTime,
+                                                                                               EigenB>(
+                b.y_space, b.x_space, b.example.problem, s0, lu, pb);
+            finite_element::time_slabs::refine_test_space_from_marked_source_cells(a.y_space, a.x_space,
+                                                                                   st0.marked_source_cells);
+            finite_element::time_slabs::refine_test_space_from_marked_source_cells(b.y_space, b.x_space,
+                                                                                   st0.marked_source_cells);
+        }
+        typename EigenB::Solver sb;
+        const auto ref = finite_element::time_slabs::compute_adaptive_test_space_iteration<S::QSpace, S::QTime, EigenB>(
+            b.y_space, b.x_space, b.example.problem, sb, lu, pb);
+        finite_element::Function<YSpace, typename B200::Vector> lambda_h(a.y_space);
+        finite_element::Function<XSpace, typename B200::Vector> u_h(a.x_space);
+        typename B200::Solver sa;
+        (void)finite_element::system::assemble_and_solve_into_functions<S::QSpace, S::QTime, B200>(
+            lambda_h, u_h, a.y_space, a.x_space, a.example.problem, sa, minres_options(tol));
+        const auto dev = la::b200::estimate(a.y_space);
+        double scale = 0.0, d_flux = 0.0, d_recon = 0.0, d_eta = 0.0;
+        for (const auto& [c, v] : ref.estimator.estimator_squared.by_source_cell)
+            scale = std::max(scale, std::abs(v));
+        for (const auto& [c, v] : ref.estimator.estimator_squared.by_source_cell)
+        {
+            d_eta = std::max(d_eta, std::abs(v - dev.estimator.estimator_squared.by_source_cell.at(c)));
+            d_flux = std::max(d_flux, std::abs(ref.flux_diagnostics.by_source_cell_flux.at(c) -
+                                               dev.flux.by_source_cell_flux.at(c)));
+            d_recon = std::max(d_recon, std::abs(ref.reconstruction_y_squared.by_source_cell.at(c) -
+                                                 dev.reconstruction_y_squared.by_source_cell.at(c)));
+        }
+        std::vector<int> ma = dev.estimator.doerfler_marking_deterministic(pb.doerfler_theta, pb.doerfler_near_tie_tolerance);
+        std::vector<int> mb(ref.marked_source_cells.begin(), ref.marked_source_cells.end());
+        std::sort(ma.begin(), ma.end());
+        std::sort(mb.begin(), mb.end());
+        std::vector<int> sym;
+        std::set_symmetric_difference(ma.begin(), ma.end(), mb.begin(), mb.end(), std::back_inserter(sym));
+        std::printf("{\"mode\": \"estimate\", \"p\": %d, \"levels\": %d, \"y_cells\": %zu, \"x_cells\": %zu, "
+                    "\"cells_compared\": %zu, \"n_slabs\": [%d, %d], \"eta_total\": [%.15e, %.15e], "
+                    "\"flux_total\": [%.15e, %.15e], \"recon_total\": [%.15e, %.15e], "
+                    "\"max_cell_diff_over_max_eta\": {\"flux\": %.3e, \"recon\": %.3e, \"eta\": %.3e}, "
+                    "\"marked\": [%zu, %zu], \"marked_symmetric_difference\": %zu}\n",
+                    P, levels, a.y_space.active_cells().size(), a.x_space.active_cells().size(),
+                    ref.estimator.estimator_squared.by_source_cell.size(), dev.n_slabs, ref.n_slabs(),
+                    dev.estimator.total(), ref.estimator.total(), dev.flux.total_flux(), ref.flux_diagnostics.total_flux(),
+                    dev.reconstruction_y_squared.total(), ref.reconstruction_y_squared.total(), d_flux / scale,
+                    d_recon / scale, d_eta / scale, ma.size(), mb.size(), sym.size());
+        return 0;
+    }
+
     // the reference's whole adaptive algorithm (run_adaptive_driver, algorithm/adaptive_driver.hpp:3508)
     // with each backend: outer cycles of inner Y loops (solve, estimate, Doerfler marking, Y
     // refinement) and X marking + refinement
@@ -367,6 +435,8 @@ namespace
             return run_solve<P>(levels, example, std::atof(argv[5]));
         if (mode == "cycle" && argc >= 7)
             return run_cycle<P>(levels, example, std::atoi(argv[5]), std::atof(argv[6]));
+        if (mode == "estimate" && argc >= 6)
+            return run_estimate<P>(levels, example, std::atof(argv[5]));
         if (mode == "adaptive" && argc >= 7)
             return run_adaptive<P>(levels, example, std::atoi(argv[5]), std::atof(argv[6]),
                                    argc < 8 || std::atoi(argv[7]) != 0);
@@ -378,7 +448,7 @@ int main(int argc, char** argv)
 {
     if (argc < 5)
     {
-        std::fprintf(stderr, "usage: apf_dropin_test blocks|solve|cycle|adaptive <p:1|2> <levels> <example> [...]\n");
+        std::fprintf(stderr, "usage: apf_dropin_test blocks|solve|cycle|estimate|adaptive <p:1|2> <levels> <example> [...]\n");
         return 2;
     }
     const std::string mode = argv[1];

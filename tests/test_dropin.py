@@ -135,3 +135,28 @@ def test_dropin_reference_adaptive_driver_matches_eigen_backend():
         for key in ("eta_squared", "lambda_y_squared", "y_estimator_squared"):
             assert abs(ra[key] - rb[key]) <= 1e-8 * abs(rb[key]), (key, ra, rb)
     assert a[-1]["x_dofs"] > a[0]["x_dofs"]
+
+
+@needs_program
+@pytest.mark.gpu
+@pytest.mark.parametrize("p,levels,env", [
+    (1, 2, ADAPTIVE_ENV),
+    (2, 1, {"APF_REF_X_POINTS": "0.3,0.6,0.4", "APF_REF_X_ROUNDS": "1", "APF_REF_KAPPA": "5:0.1:10"})],
+    ids=["p1", "p2"])
+def test_dropin_device_estimate_matches_reference_estimator(p, levels, env):
+    """la::b200::estimate (apf_estimate on the drop-in's solve, returned in the reference's
+    cellwise error types and combined by its own combination function) after one pass of the
+    reference's inner loop, so Y is finer than X and Y cells span several slabs, against the
+    reference's host estimator on its direct solve: per-cell flux^2, recon^2, eta^2 within
+    1e-9 of the largest eta^2, totals 1e-10 (recon 1e-8), the same slab count, and the
+    reference's Doerfler marking of the device estimate equal to its marking of its own (up
+    to ties at the threshold)."""
+    d = _json(_run(["estimate", p, levels, "smooth_initial", 1e-12], env=env))
+    assert d["y_cells"] > d["x_cells"] and d["cells_compared"] == d["y_cells"], d
+    assert d["n_slabs"][0] == d["n_slabs"][1], d
+    for key in ("flux", "recon", "eta"):
+        assert d["max_cell_diff_over_max_eta"][key] <= 1e-9, (key, d)
+    (ea, eb), (fa, fb), (ra, rb) = d["eta_total"], d["flux_total"], d["recon_total"]
+    assert abs(ea - eb) <= 1e-10 * eb and abs(fa - fb) <= 1e-10 * fb, d
+    assert rb > 0 and abs(ra - rb) <= 1e-8 * rb, d
+    assert d["marked"][1] > 0 and d["marked_symmetric_difference"] <= max(2, d["marked"][1] // 50), d
