@@ -21,7 +21,12 @@
  *       (src/linear_algebra/preconditioners/solve_saddle_system.hpp:43-111, the seam the Eigen
  *       backend specialises in src/linear_algebra/eigen_backend/preconditioners/
  *       solve_saddle_system.hpp:32-121) -> apf_solve_minres_with_rhs (block-preconditioned
- *       MINRES with the reference's true-residual batches) on the device system.
+ *       MINRES with the reference's true-residual batches) on the device system;
+ *   finite_element::time_slabs::compute_adaptive_test_space_iteration<QS, QT, la::b200::Backend>
+ *       (src/finite_element/time_slabs/time_slab_adaptive_loop.hpp:727) -> the solve above and
+ *       apf_estimate (la::b200::estimate) in place of the reference's host slab
+ *       reconstruction, patch flux solves and indicators, then its own combination and
+ *       marking (the reference's adaptive driver calls this).
  *
  * The assembly function is a constrained overload of the reference's own template, and the
  * Schur step and the dispatcher are full specialisations; qualified calls bind to the
@@ -220,6 +225,10 @@ namespace la::b200
 
         void set_last_diagnostics(const apf_solver_diagnostics& d) noexcept { last_diag_ = d; }
 
+        // estimates run through la::b200::estimate in this thread
+        [[nodiscard]] long long device_estimates() const noexcept { return estimates_; }
+        void count_estimate() noexcept { ++estimates_; }
+
     private:
         int device_ = -1;
         apf_ctx* ctx_ = nullptr;
@@ -227,6 +236,7 @@ namespace la::b200
         double zero_tol_ = 1e-15;
         apf_solver_options options_{};
         apf_solver_diagnostics last_diag_{};
+        long long estimates_ = 0;
         std::vector<Probe> probes_;
     };
 
@@ -517,6 +527,7 @@ namespace la::b200
             out.flux, out.reconstruction_y_squared);
         out.n_slabs = res.n_slabs;
         out.n_patches = res.n_patches;
+        s.count_estimate();
         return out;
     }
 }
@@ -715,4 +726,75 @@ namespace la::preconditioners
             return result;
         }
     };
+}
+
+// ---- the inner iteration with the device estimate --------------------------------------
+// Declared after the seams above, so that the reference's solver headers included here bind
+// to them; the reference's adaptive driver (algorithm/adaptive_driver.hpp), included after
+// this header, binds to the overload below.
+#include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
+
+namespace finite_element::time_slabs
+{
+    // compute_adaptive_test_space_iteration (time_slab_adaptive_loop.hpp:727) on the B200: the
+    // main solve through the b200 seams above, the estimate by apf_estimate in place of the
+    // reference's host slab reconstruction, patch flux solves and indicators
+    // (la::b200::estimate), then the reference's own combination, divergence check and
+    // Doerfler marking.  The state's slab space and vertex-patch set are still built on the
+    // host (their initialize() without any solve) because the driver reads n_slabs(),
+    // n_patches() and copied_slab_cells() from them; lambda_tilde() is not reconstructed on
+    // the host (the device estimate holds it).
+    template<int QSpace, int QTime, class Backend, class XSpaceType, class YSpaceType, class ExampleType>
+        requires std::same_as<Backend, la::b200::Backend>
+    [[nodiscard]] AdaptiveTestSpaceIterationState<Backend, XSpaceType, YSpaceType> compute_adaptive_test_space_iteration(
+        const YSpaceType& y_space, const XSpaceType& x_space, const ExampleType& example,
+        typename Backend::Solver& solver, const la::concepts::SolverOptions& main_solver_options = {},
+        const AdaptiveTestSpaceIterationParameters<Backend, XSpaceType, YSpaceType>& parameters = {},
+        const la::concepts::SolverOptions& local_solver_options = la::concepts::make_sparse_lu_solver_options(),
+        const AdaptiveTestSpaceSolutionSnapshot<Backend, XSpaceType, YSpaceType>* initial_guess_snapshot = nullptr)
+    {
+        static_cast<void>(local_solver_options);
+        AdaptiveTestSpaceIterationState<Backend, XSpaceType, YSpaceType> state(y_space, x_space);
+        {
+            std::optional<typename Backend::Vector> guess_vector;
+            finite_element::system::MainSystemInitialGuess<Backend> guess;
+            if (initial_guess_snapshot != nullptr &&
+                (parameters.use_adaptive_initial_guess || parameters.solve_main_system_correction))
+            {
+                guess_vector = finite_element::system::make_saddle_initial_guess_vector<Backend>(
+                    initial_guess_snapshot->lambda_delta, initial_guess_snapshot->u_delta, y_space, x_space);
+                guess.full_vector = &*guess_vector;
+                guess.solve_correction_equation = parameters.solve_main_system_correction;
+            }
+            const auto main_solve = finite_element::system::assemble_and_solve_into_functions<QSpace, QTime, Backend>(
+                state.lambda_delta, state.u_delta, y_space, x_space, example, solver, main_solver_options,
+                parameters.zero_tol, -1.0, guess,
+                static_cast<const finite_element::system::MainSystemTwoLevelHierarchy<YSpaceType, XSpaceType>*>(nullptr),
+                parameters.timing);
+            state.main_solve_diagnostics = main_solve.solver_diagnostics;
+            state.main_solve_setup_seconds = main_solve.solver_setup_seconds;
+            state.main_solve_solve_seconds = main_solve.solver_solve_seconds;
+        }
+        // host structures the driver reads (no solves)
+        state.slab_reconstruction.emplace(y_space, x_space);
+        state.slab_reconstruction->initialize(0.0, parameters.timing);
+        state.flux_reconstruction.emplace(state.slab_reconstruction->slab_space_ref(), x_space);
+        state.flux_reconstruction->initialize();
+        // the estimate on the device, in the reference's types
+        auto est = la::b200::estimate(y_space);
+        state.flux_diagnostics = std::move(est.flux);
+        state.reconstruction_y_squared = std::move(est.reconstruction_y_squared);
+        state.estimator = std::move(est.estimator);
+        const double div2 = state.estimator.divergence_residual_total();
+        state.divergence_residual_l2 = std::sqrt(div2 > 0.0 ? div2 : 0.0);
+        if (parameters.check_divergence_residual &&
+            state.divergence_residual_l2 > parameters.divergence_residual_l2_tolerance)
+            throw std::runtime_error("compute_adaptive_test_space_iteration: divergence residual L2 norm " +
+                                     std::to_string(state.divergence_residual_l2) + " exceeds tolerance " +
+                                     std::to_string(parameters.divergence_residual_l2_tolerance) + ".");
+        DoerflerMarkingDiagnostics diagnostics;
+        state.marked_source_cells = state.estimator.doerfler_marking_deterministic(
+            parameters.doerfler_theta, parameters.doerfler_near_tie_tolerance, &diagnostics, parameters.timing);
+        return state;
+    }
 }

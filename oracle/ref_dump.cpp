@@ -45,6 +45,7 @@
 
 #include "linear_algebra/eigen_backend/backend.hpp"
 
+#include "algorithm/adaptive_driver.hpp"
 #include "algorithm/example_registry.hpp"
 #include "algorithm/examples/space_time_2d/initial_data_2d_examples.hpp"
 #include "algorithm/examples/space_time_2d/space_time_2d_example.hpp"
@@ -292,10 +293,46 @@ namespace
             uniform_isotropic_refine(x_space);
         const std::vector<double> kx = apply_adaptive_options_2d(x_space, example);
         y_space.initialize(x_space.active_cells());
+        const int driver_outer = env_int("APF_REF_DRIVER_OUTER", 0);
+        if (driver_outer > 0)
+        {
+            // the reference's adaptive driver (algorithm/adaptive_driver.hpp:3508) for
+            // `driver_outer` outer cycles: its own inner Y loops, X marking and refinement
+            typename Backend::Solver solver;
+            la::concepts::SolverOptions opts;
+            adaptive_algorithm::AdaptiveParameters par;
+            par.max_outer_iterations = driver_outer;
+            par.polynomial_degree = P;
+            par.output.print_iteration_tables = false;
+            par.output.save_mesh_statistics = false;
+            par.output.stream = &std::cerr;
+            (void)adaptive_algorithm::run_adaptive_driver<QSpace, QTime, Backend>(x_space, y_space, example.problem,
+                                                                                 solver, opts, par);
+        }
 
         std::filesystem::create_directories(dir);
-        if (!kx.empty())
+        if (!kx.empty() && driver_outer == 0 && env_int("APF_REF_KAPPA_BLOCKS", 0) == 0)
             apf_oracle::write_npy(dir + "/kappa_x.npy", kx);
+        if (std::getenv("APF_REF_KAPPA") != nullptr)
+        {
+            // M = kappa I at each Y cell (the kappa law's value at the cell's centroid)
+            std::vector<double> ky;
+            for (const int c : y_space.active_cells())
+            {
+                const auto& cell = mesh.cell(c);
+                const auto& sv = mesh.spatial_vertices();
+                const auto& tv = mesh.temporal_vertices();
+                adaptive_algorithm::examples::SpaceTime2DPoint q{};
+                for (int k = 0; k < 3; ++k)
+                {
+                    q[0] += sv[cell.spatial_vertex_ids[k]][0] / 3.0;
+                    q[1] += sv[cell.spatial_vertex_ids[k]][1] / 3.0;
+                }
+                q[2] = 0.5 * (tv[cell.temporal_vertex_ids[0]][0] + tv[cell.temporal_vertex_ids[1]][0]);
+                ky.push_back(example.problem.M(q)[0][0]);
+            }
+            apf_oracle::write_npy(dir + "/kappa_y.npy", ky);
+        }
         for (int pass = 0; pass < env_int("APF_REF_Y_PASSES", 0); ++pass)
         {
             typename Backend::Solver solver;

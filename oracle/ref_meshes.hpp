@@ -103,6 +103,8 @@ namespace apf_oracle
     //                                    x_space.find_active_cell(p), fespace.hpp:616), or,
     //                                    with APF_REF_KAPPA_BLOCKS=n, per square of an n x n
     //                                    partition of the unit square;
+    //   APF_REF_DRIVER_OUTER=n           (oracle driver) n outer cycles of the reference's
+    //                                    adaptive driver (run_adaptive_driver) before the dump;
     //   APF_REF_Y_PASSES=n               n passes of the reference's inner loop before the
     //                                    dump: estimate, Doerfler marking, then
     //                                    refine_test_space_from_marked_source_cells

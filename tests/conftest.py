@@ -20,6 +20,9 @@ GOLDEN_CASES = ["p1_l1_smooth", "p1_l2_smooth", "p2_l1_smooth", "p1_l1_nonmatchi
 # reference's own marking) and a diffusivity per X cell (p1_adapt_kappa, p1_kappa_uniform)
 ADAPTIVE_CASES = ["p1_adapt_smooth", "p1_adapt_kappa", "p1_adapt_nonmatching", "p2_adapt_smooth"]
 KAPPA_CASES = ["p1_adapt_kappa", "p1_kappa_uniform"]
+# the mesh of the reference's adaptive driver after three outer cycles (Y cells = X cells,
+# several time slabs, hanging nodes from the driver's own refinement), kappa per block
+DRIVER_CASES = ["p1_driver_kappa"]
 # fixtures with the driver's G^delta estimator (APF_REF_G): P1 uniform, adaptive, adaptive + kappa
 G_DELTA_CASES = ["p1_l2_smooth", "p1_adapt_smooth", "p1_adapt_kappa"]
 GOLDEN_CASES_1D = ["d1_l2_smooth", "d1_l2_nonmatching", "d1_l5_smooth"]
@@ -52,6 +55,10 @@ def load_golden(name):
             out[nm + "_rhs"] = z[nm + "_rhs"]
         out["K2p_pattern_reuse_count"] = int(z["K2p_pattern_reuse_count"][0])
     m_cells = None
+    if "kappa_y" in z and "kappa_x" not in z:
+        # M = kappa I with kappa given per Y cell (a law by position, constant on each cell)
+        kappa = z["kappa_y"]
+        m_cells = np.stack([kappa, np.zeros_like(kappa), kappa], axis=1)
     if "kappa_x" in z:
         # M = kappa I with kappa constant per X cell: every Y cell takes its X ancestor's
         kappa = z["kappa_x"][z["y_to_x_cell"]]

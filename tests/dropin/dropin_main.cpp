@@ -18,8 +18,8 @@
 //       the reference's inner loop, `passes` times: compute_adaptive_test_space_iteration
 //       (src/finite_element/time_slabs/time_slab_adaptive_loop.hpp:727) and
 //       refine_test_space_from_marked_source_cells (:2147-2186), once with la::b200::Backend
-//       (device assembly, graph-norm block and MINRES; the reference's host estimator, marking
-//       and refinement) and once with the Eigen backend and its direct solver, each on its own
+//       (device assembly, graph-norm block, MINRES and estimate; the reference's marking and
+//       refinement) and once with the Eigen backend and its direct solver, each on its own
 //       copy of the spaces; per pass the estimator totals, the marked cells of each run and the
 //       Y meshes (both refined by the direct-solve run's marks);
 //   estimate <p> <levels> <example> <tol>
@@ -34,7 +34,7 @@
 //       (compare = 0: the b200 backend only).
 //
 // The adaptive-mesh options of the oracle driver (APF_REF_X_POINTS, APF_REF_X_ROUNDS,
-// APF_REF_KAPPA, APF_REF_KAPPA_BLOCKS) apply to all modes.  Each mode prints one JSON line.
+// APF_REF_KAPPA, APF_REF_KAPPA_BLOCKS, APF_REF_DRIVER_OUTER) apply to all modes.  Each mode prints one JSON line.
 #include "apf_b200_backend.hpp" // before the reference's solver headers (see its header comment)
 
 #include <algorithm>
@@ -169,6 +169,20 @@ namespace
                 apf_oracle::uniform_isotropic_refine(x_space);
             (void)apf_oracle::apply_adaptive_options_2d(x_space, example);
             y_space.initialize(x_space.active_cells());
+            if (const int outer = apf_oracle::env_int("APF_REF_DRIVER_OUTER", 0); outer > 0)
+            {
+                // the mesh of the reference's adaptive driver after `outer` cycles (Eigen backend)
+                typename la::eigen::Backend::Solver solver;
+                la::concepts::SolverOptions opts;
+                adaptive_algorithm::AdaptiveParameters par;
+                par.max_outer_iterations = outer;
+                par.polynomial_degree = P;
+                par.output.print_iteration_tables = false;
+                par.output.save_mesh_statistics = false;
+                par.output.stream = &std::cerr;
+                (void)adaptive_algorithm::run_adaptive_driver<QSpace, QTime, la::eigen::Backend>(
+                    x_space, y_space, example.problem, solver, opts, par);
+            }
         }
     };
 
@@ -307,7 +321,7 @@ namespace
             finite_element::time_slabs::refine_test_space_from_marked_source_cells(b.y_space, b.x_space,
                                                                                    st_b.marked_source_cells);
         }
-        std::printf("]}\n");
+        std::printf("], \"device_estimates\": %lld}\n", la::b200::session().device_estimates());
         return 0;
     }
 
@@ -418,9 +432,10 @@ namespace
             return out + "]";
         };
         std::printf("{\"mode\": \"adaptive\", \"p\": %d, \"levels\": %d, \"tol\": %.1e, \"b200_s\": %.3f, "
-                    "\"direct_s\": %.3f, \"b200\": %s, \"direct\": %s}\n",
+                    "\"direct_s\": %.3f, \"device_estimates\": %lld, \"b200\": %s, \"direct\": %s}\n",
                     P, levels, tol, std::chrono::duration<double>(t1 - t0).count(),
-                    std::chrono::duration<double>(t2 - t1).count(), dump(ra).c_str(), dump(rb).c_str());
+                    std::chrono::duration<double>(t2 - t1).count(), la::b200::session().device_estimates(),
+                    dump(ra).c_str(), dump(rb).c_str());
         return 0;
     }
 

@@ -53,6 +53,11 @@ CASES = [
     ("p1_adapt_nonmatching", 2, 1, 1, "non_matching_initial",
      {"APF_REF_X_POINTS": "0.2,0.45,0.1", "APF_REF_X_ROUNDS": "4", "APF_REF_Y_PASSES": "1"}),
     ("p1_kappa_uniform", 2, 1, 2, "smooth_initial", {"APF_REF_KAPPA": "3:0.1:10"}),
+    # the mesh of the reference's own adaptive driver after three outer cycles (its X and Y
+    # marking and refinement; Y cells of the refined-in-time X span several slabs), kappa per
+    # square of a 4 x 4 partition
+    ("p1_driver_kappa", 2, 1, 1, "smooth_initial",
+     {"APF_REF_KAPPA": "11:0.1:10", "APF_REF_KAPPA_BLOCKS": "4", "APF_REF_DRIVER_OUTER": "3"}),
     ("p2_adapt_smooth", 2, 2, 1, "smooth_initial",
      {"APF_REF_X_POINTS": "0.3,0.3,0.3", "APF_REF_X_ROUNDS": "2", "APF_REF_Y_PASSES": "1"}),
     # 1+1D (points x,t)

@@ -35,6 +35,10 @@ def _run(args, env=None, timeout=900):
     e = dict(os.environ)
     for k in ADAPTIVE_ENV:
         e.pop(k, None)
+    # the reference's host code single-threaded: its multi-threaded reductions round
+    # differently from run to run, and a Doerfler tie broken the other way refines another
+    # mesh with the same DOF counts (seen in the adaptive-driver comparison)
+    e["OMP_NUM_THREADS"] = "1"
     e.update(env or {})
     r = subprocess.run([PROGRAM, *map(str, args)], capture_output=True, text=True, env=e, timeout=timeout)
     return r
@@ -99,11 +103,13 @@ def test_dropin_solve_through_reference_caller(env):
 @needs_program
 @pytest.mark.gpu
 def test_dropin_adaptive_inner_loop_matches_eigen_backend():
-    """Three passes of the reference's inner loop (estimate, Doerfler marking, Y refinement) on an
-    adaptive X with kappa per cell: the b200 backend's MINRES solution (true residual 1e-12)
-    gives the reference's host estimator the same totals (1e-8) and the same marked cells (up
-    to ties at the threshold, at most 2% of them) as the Eigen backend's direct solve; both
-    test spaces are refined by the direct run's marks, so every pass compares the same mesh."""
+    """Three passes of the reference's inner loop compute_adaptive_test_space_iteration (solve,
+    estimate, Doerfler marking) + Y refinement on an adaptive X with kappa per cell: with
+    la::b200::Backend the call resolves to the drop-in's overload (device assembly, MINRES to
+    1e-12 and device estimate, the reference's own combination and marking), which gives the
+    same totals (1e-8) and the same marked cells (up to ties at the threshold, at most 2% of
+    them) as the reference's host path on the Eigen backend with its direct solve; both test
+    spaces are refined by the direct run's marks, so every pass compares the same mesh."""
     d = _json(_run(["cycle", 1, 2, "smooth_initial", 3, 1e-12], env=ADAPTIVE_ENV))
     assert len(d["passes"]) == 3
     for pas in d["passes"]:
@@ -114,6 +120,8 @@ def test_dropin_adaptive_inner_loop_matches_eigen_backend():
         assert pas["minres_iterations"] > 0 and pas["minres_true_residual"] <= 1e-12, pas
     # the later passes run on the refined (Y finer than X) test space
     assert d["passes"][2]["y_cells"][0] > d["passes"][1]["y_cells"][0] > d["passes"][0]["y_cells"][0]
+    # every b200 pass estimated on the device (the drop-in's inner-iteration overload)
+    assert d["device_estimates"] == 3
 
 
 @needs_program
@@ -135,6 +143,8 @@ def test_dropin_reference_adaptive_driver_matches_eigen_backend():
         for key in ("eta_squared", "lambda_y_squared", "y_estimator_squared"):
             assert abs(ra[key] - rb[key]) <= 1e-8 * abs(rb[key]), (key, ra, rb)
     assert a[-1]["x_dofs"] > a[0]["x_dofs"]
+    # every inner iteration of the b200 run estimated on the device
+    assert d["device_estimates"] >= sum(r["inner"] for r in a)
 
 
 @needs_program

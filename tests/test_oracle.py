@@ -6,13 +6,13 @@ import os
 import numpy as np
 import pytest
 
-from conftest import (ADAPTIVE_CASES, G_DELTA_CASES, GOLDEN, GOLDEN_CASES, HHAT_RESIDUE, assert_same_sparse,
-                      load_g_space, load_golden)
+from conftest import (ADAPTIVE_CASES, DRIVER_CASES, G_DELTA_CASES, GOLDEN, GOLDEN_CASES, HHAT_RESIDUE,
+                      assert_same_sparse, load_g_space, load_golden)
 
 import apf_oracle as O
 
 
-ALL_2D = GOLDEN_CASES + ADAPTIVE_CASES + ["p1_kappa_uniform"]
+ALL_2D = GOLDEN_CASES + ADAPTIVE_CASES + DRIVER_CASES + ["p1_kappa_uniform"]
 
 
 @pytest.mark.parametrize("name", ALL_2D)
@@ -30,7 +30,7 @@ def test_oracle_main_blocks_match_reference(name):
 def test_oracle_graph_norm_matches_reference(name):
     prob, ref, example = load_golden(name)
     gn = O.assemble_graph_norm(prob, ref["A_y"], ref["C_signed"])
-    residue = HHAT_RESIDUE if name in ADAPTIVE_CASES else 0.0
+    residue = HHAT_RESIDUE if name in ADAPTIVE_CASES + DRIVER_CASES else 0.0
     assert_same_sparse(ref["Hhat"], gn["Hhat"], 1e-12, "Hhat", residue=residue)
 
 
@@ -68,7 +68,7 @@ def test_adaptive_fixtures_have_hanging_nodes_and_finer_y():
         assert len(z["slab_of_cell"]) > prob.y_geom.shape[0], name
 
 
-@pytest.mark.parametrize("name", ADAPTIVE_CASES)
+@pytest.mark.parametrize("name", ADAPTIVE_CASES + DRIVER_CASES)
 def test_oracle_slab_reconstruction_matches_reference(name):
     """lambda~ of the slab reconstruction on the reference's own time-slab space, from the
     reference's u_delta: the slab DOF count and lambda~ at every slab cell's vertices and
