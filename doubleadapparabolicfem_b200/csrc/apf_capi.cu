@@ -911,6 +911,20 @@ int solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, c
 }
 }
 
+int apf_system_set_solution(apf_ctx* ctx, apf_system* sys, const double* x, int pointers_on_device)
+{
+    if (!ctx || !sys || !x)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        auto& S = sys->sys;
+        const int n = S.in.n_lambda + S.in.n_u;
+        S.solution.allocate(static_cast<std::size_t>(n), ctx->stream);
+        APF_CUDA(cudaMemcpyAsync(S.solution.get(), x, n * sizeof(double),
+                                 pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+        apf::sync(ctx->stream);
+    });
+}
+
 int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const double* r, double* z,
                              int pointers_on_device)
 {

@@ -248,6 +248,10 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
 int apf_solve_minres_with_rhs(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* rhs,
                               const double* initial_guess, double* solution, int pointers_on_device,
                               apf_solver_diagnostics* diag);
+/* Replace the solution the system holds (n_lambda + n_u values; read by apf_estimate,
+ * apf_x_indicators and apf_g_estimator): e.g. x0 + d after the correction equation's solve
+ * for d, as the reference's dispatcher returns it. */
+int apf_system_set_solution(apf_ctx* ctx, apf_system* sys, const double* x, int pointers_on_device);
 /* z = P^{-1} r with the set-up preconditioner: block 0 = A_y part (n_lambda values),
  * 1 = Hhat part (n_u values), 2 = the full block operator (n_lambda + n_u).  For tests
  * and diagnostics (symmetry, PCG quality) of the preconditioner. */

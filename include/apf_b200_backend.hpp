@@ -717,9 +717,15 @@ namespace la::preconditioners
 
             SaddlePreconditionedSolveResult<la::b200::Backend> result;
             result.solution = typename la::b200::Backend::Vector(n);
+            if (correction)
+            {
+                // the solution is x0 + d; the device system keeps it too (the estimate reads it)
+                for (int i = 0; i < n; ++i)
+                    x[static_cast<std::size_t>(i)] += (*initial_guess.full_vector)[i];
+                la::b200::check(ctx, apf_system_set_solution(ctx, sys, x.data(), 0), "apf_system_set_solution");
+            }
             for (int i = 0; i < n; ++i)
-                result.solution[i] = x[static_cast<std::size_t>(i)] +
-                                     (correction ? (*initial_guess.full_vector)[i] : 0.0);
+                result.solution[i] = x[static_cast<std::size_t>(i)];
             result.diagnostics = std::move(diag);
             result.setup_seconds = d.setup_seconds;
             result.solve_seconds = d.solve_seconds;

@@ -27,11 +27,12 @@
 //       the reference's types (la::b200::estimate) on the b200 solve against the reference's
 //       host estimate on its direct solve -- per-cell flux^2 / recon^2 / eta^2, totals, slab
 //       count and the Doerfler marking of each;
-//   adaptive <p> <levels> <example> <outer_cycles> <tol> [compare:1|0]
+//   adaptive <p> <levels> <example> <outer_cycles> <tol> [compare:1|0] [guess:0|1|2]
 //       the reference's whole adaptive algorithm (adaptive_algorithm::run_adaptive_driver,
 //       algorithm/adaptive_driver.hpp:3508) with each backend, each on its own spaces: per outer
 //       cycle the X and Y DOF counts, the number of inner Y iterations and the estimator totals
-//       (compare = 0: the b200 backend only).
+//       (compare = 0: the b200 backend only; guess = 1: the previous solution as initial guess,
+//       2: the correction equation).
 //
 // The adaptive-mesh options of the oracle driver (APF_REF_X_POINTS, APF_REF_X_ROUNDS,
 // APF_REF_KAPPA, APF_REF_KAPPA_BLOCKS, APF_REF_DRIVER_OUTER) apply to all modes.  Each mode prints one JSON line.
@@ -392,7 +393,7 @@ namespace
     // with each backend: outer cycles of inner Y loops (solve, estimate, Doerfler marking, Y
     // refinement) and X marking + refinement
     template<int P>
-    int run_adaptive(int levels, const std::string& name, int outer, double tol, bool compare)
+    int run_adaptive(int levels, const std::string& name, int outer, double tol, bool compare, int guess)
     {
         using S = Spaces<P>;
         S a(name, levels), b(name, levels);
@@ -402,6 +403,10 @@ namespace
         par.output.print_iteration_tables = !compare; // progress on stderr for long runs
         par.output.save_mesh_statistics = false;
         par.output.stream = &std::cerr;
+        // guess 1: the previous inner iteration's solution as MINRES's initial guess;
+        // 2: the correction equation K d = b - K x0 (MainSystemInitialGuess)
+        par.use_adaptive_initial_guess = guess >= 1;
+        par.solve_main_system_correction = guess == 2;
         const auto t0 = std::chrono::steady_clock::now();
         typename B200::Solver sa;
         const auto ra = adaptive_algorithm::run_adaptive_driver<S::QSpace, S::QTime, B200>(
@@ -454,7 +459,7 @@ namespace
             return run_estimate<P>(levels, example, std::atof(argv[5]));
         if (mode == "adaptive" && argc >= 7)
             return run_adaptive<P>(levels, example, std::atoi(argv[5]), std::atof(argv[6]),
-                                   argc < 8 || std::atoi(argv[7]) != 0);
+                                   argc < 8 || std::atoi(argv[7]) != 0, argc < 9 ? 0 : std::atoi(argv[8]));
         return 2;
     }
 }

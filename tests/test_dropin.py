@@ -126,15 +126,18 @@ def test_dropin_adaptive_inner_loop_matches_eigen_backend():
 
 @needs_program
 @pytest.mark.gpu
-def test_dropin_reference_adaptive_driver_matches_eigen_backend():
+@pytest.mark.parametrize("guess", [0, 1, 2], ids=["cold", "initial_guess", "correction_equation"])
+def test_dropin_reference_adaptive_driver_matches_eigen_backend(guess):
     """The reference's whole adaptive algorithm (run_adaptive_driver: inner Y loops, X marking
     and refinement) for three outer cycles with kappa per block (no ties in the marking): the
     b200 backend (device assembly, graph-norm block, MINRES to 1e-12) follows the same
     trajectory as the Eigen backend with its direct solver -- the same X and Y DOF counts and
-    inner iteration counts every cycle, and the same estimator totals to 1e-8."""
+    inner iteration counts every cycle, and the same estimator totals to 1e-8 -- with a cold
+    start, with the previous solution as MINRES's initial guess, and with the correction
+    equation K d = b - K x0 (the dispatcher's right-hand-side path)."""
     # kappa per square of a 4 x 4 partition (by position: the driver refines X, so a table
     # per initial X cell would not cover the new cells)
-    d = _json(_run(["adaptive", 1, 1, "smooth_initial", 3, 1e-12],
+    d = _json(_run(["adaptive", 1, 1, "smooth_initial", 3, 1e-12, 1, guess],
                    env={"APF_REF_KAPPA": "11:0.1:10", "APF_REF_KAPPA_BLOCKS": "4"}))
     a, b = d["b200"], d["direct"]
     assert len(a) == len(b) == 3
