@@ -349,10 +349,16 @@ namespace la::b200
             bool sin_sin = true, one = true, zero = true;
             for (const auto& q : samples)
             {
-                std::array<double, Dim> p{};
-                for (int d = 0; d < Dim; ++d)
-                    p[static_cast<std::size_t>(d)] = q[d];
-                const double v = static_cast<double>(u0(p));
+                double v = 0.0;
+                if constexpr (Dim == 1 && std::is_invocable_v<const U0&, double>)
+                    v = static_cast<double>(u0(q[0]));
+                else
+                {
+                    std::array<double, Dim> p{};
+                    for (int d = 0; d < Dim; ++d)
+                        p[static_cast<std::size_t>(d)] = q[d];
+                    v = static_cast<double>(u0(p));
+                }
                 double s = std::sin(pi * q[0]);
                 if constexpr (Dim == 2)
                     s *= std::sin(pi * q[1]);

@@ -34,6 +34,8 @@
 //       (compare = 0: the b200 backend only; guess = 1: the previous solution as initial guess,
 //       2: the correction equation).
 //
+// <p> = 1d runs the blocks / solve / cycle / estimate modes on the reference's 1+1D P1
+// configuration (its 1D example on the unit space-time mesh).
 // The adaptive-mesh options of the oracle driver (APF_REF_X_POINTS, APF_REF_X_ROUNDS,
 // APF_REF_KAPPA, APF_REF_KAPPA_BLOCKS, APF_REF_DRIVER_OUTER) apply to all modes.  Each mode prints one JSON line.
 #include "apf_b200_backend.hpp" // before the reference's solver headers (see its header comment)
@@ -153,6 +155,7 @@ namespace
         using YSpace = finite_element::FESpace<GT, FET, finite_element::SpaceOnlyPolicy>;
         static constexpr int QSpace = 4 * P + 1;
         static constexpr int QTime = 2 * P + 1;
+        static constexpr int P_ = P;
 
         decltype(adaptive_algorithm::examples::make_2d_example(std::string{})) example;
         decltype(adaptive_algorithm::examples::make_initial_mesh_from_example(example)) mesh;
@@ -187,6 +190,36 @@ namespace
         }
     };
 
+    // 1+1D P1: the reference's 1D example on its unit space-time mesh, `levels` uniform outer
+    // refinements, Gauss orders QSpace = QTime = 3 (the runner's 1+1D configuration)
+    struct Spaces1D
+    {
+        using GT = mesh::MeshTraits<1>;
+        using FET = finite_element::FiniteElementTraits<GT, 1, 1>;
+        using XSpace = finite_element::FESpace<GT, FET, finite_element::SpaceTimePolicy>;
+        using YSpace = finite_element::FESpace<GT, FET, finite_element::SpaceOnlyPolicy>;
+        static constexpr int QSpace = 3;
+        static constexpr int QTime = 3;
+        static constexpr int P_ = 1;
+
+        decltype(adaptive_algorithm::examples::make_1d_example(std::string{})) example;
+        decltype(adaptive_algorithm::support::make_unit_mesh<GT>()) mesh;
+        XSpace x_space;
+        YSpace y_space;
+
+        Spaces1D(const std::string& name, int levels)
+            : example(adaptive_algorithm::examples::make_1d_example(name)),
+              mesh(adaptive_algorithm::support::make_unit_mesh<GT>()),
+              x_space(mesh),
+              y_space(mesh)
+        {
+            adaptive_algorithm::examples::initialize_spaces_from_example(x_space, y_space, example);
+            for (int k = 0; k < levels; ++k)
+                apf_oracle::uniform_isotropic_refine(x_space);
+            y_space.initialize(x_space.active_cells());
+        }
+    };
+
     la::concepts::SolverOptions minres_options(double tol)
     {
         la::concepts::SolverOptions o;
@@ -197,11 +230,11 @@ namespace
         return o;
     }
 
-    template<int P>
+    template<class S>
     int run_blocks(int levels, const std::string& name)
     {
-        Spaces<P> s(name, levels);
-        using S = Spaces<P>;
+        S s(name, levels);
+        constexpr int P = S::P_;
         const auto ref = finite_element::system::assemble_main_system_blocks<S::QSpace, S::QTime, EigenB>(
             s.y_space, s.x_space, s.example.problem, 1e-15, -1.0);
         const auto mine = finite_element::system::assemble_main_system_blocks<S::QSpace, S::QTime, B200>(
@@ -224,11 +257,11 @@ namespace
         return 0;
     }
 
-    template<int P>
+    template<class S>
     int run_solve(int levels, const std::string& name, double tol)
     {
-        Spaces<P> s(name, levels);
-        using S = Spaces<P>;
+        S s(name, levels);
+        constexpr int P = S::P_;
         using XSpace = typename S::XSpace;
         using YSpace = typename S::YSpace;
         // the Eigen backend's K, rhs and direct solution
@@ -276,10 +309,10 @@ namespace
         return 0;
     }
 
-    template<int P>
+    template<class S>
     int run_cycle(int levels, const std::string& name, int passes, double tol)
     {
-        using S = Spaces<P>;
+        constexpr int P = S::P_;
         using XSpace = typename S::XSpace;
         using YSpace = typename S::YSpace;
         S a(name, levels), b(name, levels); // a: b200 backend, b: Eigen backend with its direct solver
@@ -330,10 +363,10 @@ namespace
     // host estimate, after one pass of the reference's inner loop (Y finer than X, Y cells
     // across several slabs): per source Y cell flux^2, recon^2 and eta^2, totals, the slab
     // count and the Doerfler marking of the two estimates
-    template<int P>
+    template<class S>
     int run_estimate(int levels, const std::string& name, double tol)
     {
-        using S = Spaces<P>;
+        constexpr int P = S::P_;
         using XSpace = typename S::XSpace;
         using YSpace = typename S::YSpace;
         S a(name, levels), b(name, levels);
@@ -444,19 +477,29 @@ namespace
         return 0;
     }
 
+    template<class S>
+    int dispatch_common(const std::string& mode, int argc, char** argv)
+    {
+        const int levels = std::atoi(argv[3]);
+        const std::string example = argv[4];
+        if (mode == "blocks")
+            return run_blocks<S>(levels, example);
+        if (mode == "solve" && argc >= 6)
+            return run_solve<S>(levels, example, std::atof(argv[5]));
+        if (mode == "cycle" && argc >= 7)
+            return run_cycle<S>(levels, example, std::atoi(argv[5]), std::atof(argv[6]));
+        if (mode == "estimate" && argc >= 6)
+            return run_estimate<S>(levels, example, std::atof(argv[5]));
+        return 2;
+    }
+
     template<int P>
     int dispatch(const std::string& mode, int argc, char** argv)
     {
         const int levels = std::atoi(argv[3]);
         const std::string example = argv[4];
-        if (mode == "blocks")
-            return run_blocks<P>(levels, example);
-        if (mode == "solve" && argc >= 6)
-            return run_solve<P>(levels, example, std::atof(argv[5]));
-        if (mode == "cycle" && argc >= 7)
-            return run_cycle<P>(levels, example, std::atoi(argv[5]), std::atof(argv[6]));
-        if (mode == "estimate" && argc >= 6)
-            return run_estimate<P>(levels, example, std::atof(argv[5]));
+        if (mode != "adaptive")
+            return dispatch_common<Spaces<P>>(mode, argc, argv);
         if (mode == "adaptive" && argc >= 7)
             return run_adaptive<P>(levels, example, std::atoi(argv[5]), std::atof(argv[6]),
                                    argc < 8 || std::atoi(argv[7]) != 0, argc < 9 ? 0 : std::atoi(argv[8]));
@@ -468,14 +511,17 @@ int main(int argc, char** argv)
 {
     if (argc < 5)
     {
-        std::fprintf(stderr, "usage: apf_dropin_test blocks|solve|cycle|estimate|adaptive <p:1|2> <levels> <example> [...]\n");
+        std::fprintf(stderr, "usage: apf_dropin_test blocks|solve|cycle|estimate|adaptive <p:1|2|1d> <levels> <example> [...]\n");
         return 2;
     }
     const std::string mode = argv[1];
     try
     {
-        const int p = std::atoi(argv[2]);
-        const int rc = p == 2 ? dispatch<2>(mode, argc, argv) : dispatch<1>(mode, argc, argv);
+        // <p>: 1 or 2 (2+1D prisms), or "1d" (1+1D P1 quadrilaterals)
+        const std::string pa = argv[2];
+        const int rc = pa == "1d" ? dispatch_common<Spaces1D>(mode, argc, argv)
+                       : std::atoi(argv[2]) == 2 ? dispatch<2>(mode, argc, argv)
+                                                 : dispatch<1>(mode, argc, argv);
         if (rc == 2)
             std::fprintf(stderr, "apf_dropin_test: bad arguments\n");
         return rc;

@@ -173,3 +173,33 @@ def test_dropin_device_estimate_matches_reference_estimator(p, levels, env):
     assert abs(ea - eb) <= 1e-10 * eb and abs(fa - fb) <= 1e-10 * fb, d
     assert rb > 0 and abs(ra - rb) <= 1e-8 * rb, d
     assert d["marked"][1] > 0 and d["marked_symmetric_difference"] <= max(2, d["marked"][1] // 50), d
+
+
+@needs_program
+@pytest.mark.gpu
+@pytest.mark.parametrize("example", ["smooth_initial", "non_matching_initial"])
+def test_dropin_1d_blocks_match_eigen_backend(example):
+    """1+1D P1 (the CPU-runnable configuration's element): the reference's 1D example on its
+    unit space-time mesh, two uniform levels; the drop-in's blocks equal the Eigen backend's."""
+    d = _json(_run(["blocks", "1d", 2, example]))
+    _assert_blocks(d, hhat_residue=False)
+
+
+@needs_program
+@pytest.mark.gpu
+def test_dropin_1d_solve_and_inner_loop():
+    """1+1D through the reference's callers: assemble_and_solve_into_functions (true residual
+    1e-10 on the host, 1e-6 of the direct solution) and two passes of its inner loop (device
+    estimate and the reference's marking against its host path, the same marks)."""
+    d = _json(_run(["solve", "1d", 3, "smooth_initial", 1e-10]))
+    assert d["converged"] == 1 and d["host_true_residual"] <= 1e-10 and d["max_diff_to_direct_over_max"] <= 1e-6, d
+    c = _json(_run(["cycle", "1d", 2, "smooth_initial", 2, 1e-12]))
+    for pas in c["passes"]:
+        assert pas["y_cells"][0] == pas["y_cells"][1], pas
+        assert abs(pas["flux_b200"] - pas["flux_direct"]) <= 1e-8 * pas["flux_direct"], pas
+        assert pas["marked_symmetric_difference"] <= max(2, pas["marked"][1] // 50), pas
+    assert c["device_estimates"] == 2
+    e = _json(_run(["estimate", "1d", 3, "smooth_initial", 1e-12]))
+    assert e["y_cells"] > e["x_cells"] and e["n_slabs"][0] == e["n_slabs"][1], e
+    for key in ("flux", "recon", "eta"):
+        assert e["max_cell_diff_over_max_eta"][key] <= 1e-9, (key, e)
