@@ -440,6 +440,7 @@ namespace
         // 2: the correction equation K d = b - K x0 (MainSystemInitialGuess)
         par.use_adaptive_initial_guess = guess >= 1;
         par.solve_main_system_correction = guess == 2;
+        par.timing.enabled = !compare; // the driver's own phase timing for the b200-only run
         const auto t0 = std::chrono::steady_clock::now();
         typename B200::Solver sa;
         const auto ra = adaptive_algorithm::run_adaptive_driver<S::QSpace, S::QTime, B200>(
@@ -469,6 +470,23 @@ namespace
             }
             return out + "]";
         };
+        // the driver's slowest phases (b200-only runs)
+        std::string phases = "[";
+        {
+            std::vector<std::pair<double, std::string>> rec;
+            for (const auto& r : ra.timing_records)
+                if (r.metric_kind == adaptive_algorithm::MetricKind::duration_seconds)
+                    rec.emplace_back(r.total_seconds, r.phase);
+            std::sort(rec.rbegin(), rec.rend());
+            for (std::size_t k = 0; k < rec.size() && k < 25; ++k)
+            {
+                char buf[256];
+                std::snprintf(buf, sizeof(buf), "%s[\"%s\", %.3f]", k ? ", " : "", rec[k].second.c_str(), rec[k].first);
+                phases += buf;
+            }
+        }
+        phases += "]";
+        std::fprintf(stderr, "driver phases (total s): %s\n", phases.c_str());
         std::printf("{\"mode\": \"adaptive\", \"p\": %d, \"levels\": %d, \"tol\": %.1e, \"b200_s\": %.3f, "
                     "\"direct_s\": %.3f, \"device_estimates\": %lld, \"b200\": %s, \"direct\": %s}\n",
                     P, levels, tol, std::chrono::duration<double>(t1 - t0).count(),
