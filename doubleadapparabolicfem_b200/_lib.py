@@ -144,6 +144,10 @@ SIGNATURES = {
                           C.POINTER(SolverDiagnostics)], C.c_int),
     "apf_solve_minres_with_rhs": ([C.c_void_p, C.c_void_p, C.POINTER(SolverOptions), C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_int, C.POINTER(SolverDiagnostics)], C.c_int),
+    "apf_solve_minres_correction": ([C.c_void_p, C.c_void_p, C.POINTER(SolverOptions), C.c_void_p, C.c_void_p,
+                                     C.c_int, C.POINTER(SolverDiagnostics)], C.c_int),
+    "apf_system_residual_norms": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double)], C.c_int),
     "apf_system_set_solution": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "apf_preconditioner_apply": ([C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "apf_system_solution_device_ptr": ([C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),

@@ -2,6 +2,8 @@
 // host-side drivers that sequence the device kernels.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -790,10 +792,11 @@ int apf_setup_preconditioner(apf_ctx* ctx, apf_system* sys, const apf_solver_opt
 
 namespace
 {
-    // MINRES on the system's K; rhs NULL = the assembled [f; g]
+    // MINRES on the system's K; rhs NULL = the assembled [f; g].  correction: initial_guess
+    // is x0, MINRES solves K d = rhs - K x0 from zero and the solution is x0 + d.
     int solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* rhs,
                      const double* initial_guess, double* solution, int pointers_on_device,
-                     apf_solver_diagnostics* diag);
+                     apf_solver_diagnostics* diag, bool correction = false);
 }
 
 int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* initial_guess,
@@ -811,10 +814,19 @@ int apf_solve_minres_with_rhs(apf_ctx* ctx, apf_system* sys, const apf_solver_op
     return solve_minres(ctx, sys, opt, rhs, initial_guess, solution, pointers_on_device, diag);
 }
 
+int apf_solve_minres_correction(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* x0,
+                                double* solution, int pointers_on_device, apf_solver_diagnostics* diag)
+{
+    if (!x0)
+        return APF_ERR_INVALID;
+    return solve_minres(ctx, sys, opt, nullptr, x0, solution, pointers_on_device, diag, true);
+}
+
 namespace
 {
 int solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* rhs,
-                 const double* initial_guess, double* solution, int pointers_on_device, apf_solver_diagnostics* diag)
+                 const double* initial_guess, double* solution, int pointers_on_device, apf_solver_diagnostics* diag,
+                 bool correction)
 {
     if (!ctx || !sys || !opt)
         return APF_ERR_INVALID;
@@ -841,13 +853,23 @@ int solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, c
             apf::copy(s, nu, S.g.get(), S.rhs.get() + nl);
         }
         S.solution.allocate(n, s);
-        if (initial_guess)
+        if (!S.blocks[APF_BLOCK_K].sell)
+            apf::build_sell(s, S.blocks[APF_BLOCK_K]);
+        apf::DeviceBuffer<double> x0;
+        if (correction)
+        {
+            // the correction equation K d = b - K x0 (d from zero), x = x0 + d afterwards
+            x0.allocate(n, s);
+            APF_CUDA(cudaMemcpyAsync(x0.get(), initial_guess, n * sizeof(double),
+                                     pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+            apf::spmv(s, S.blocks[APF_BLOCK_K], x0.get(), S.rhs.get(), -1.0, 1.0);
+            apf::fill(s, n, 0.0, S.solution.get());
+        }
+        else if (initial_guess)
             APF_CUDA(cudaMemcpyAsync(S.solution.get(), initial_guess, n * sizeof(double),
                                      pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
         else
             apf::fill(s, n, 0.0, S.solution.get());
-        if (!S.blocks[APF_BLOCK_K].sell)
-            apf::build_sell(s, S.blocks[APF_BLOCK_K]);
         apf::MinresOptions mo;
         mo.tolerance = opt->tolerance;
         mo.max_iterations = opt->max_iterations;
@@ -871,6 +893,8 @@ int solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, c
             fallback = 1;
         }
         solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (correction)
+            apf::axpby(s, n, 1.0, x0.get(), 1.0, S.solution.get());
         if (solution)
             APF_CUDA(cudaMemcpyAsync(solution, S.solution.get(), n * sizeof(double),
                                      pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
@@ -922,6 +946,36 @@ int apf_system_set_solution(apf_ctx* ctx, apf_system* sys, const double* x, int 
         APF_CUDA(cudaMemcpyAsync(S.solution.get(), x, n * sizeof(double),
                                  pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
         apf::sync(ctx->stream);
+    });
+}
+
+int apf_system_residual_norms(apf_ctx* ctx, apf_system* sys, const double* x, int pointers_on_device,
+                              double* residual_norm, double* rhs_norm)
+{
+    if (!ctx || !sys || !residual_norm || !rhs_norm)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        auto& S = sys->sys;
+        cudaStream_t s = ctx->stream;
+        const int nl = S.in.n_lambda, nu = S.in.n_u, n = nl + nu;
+        apf::require(x != nullptr || S.solution.size() == static_cast<std::size_t>(n), APF_ERR_INVALID,
+                     "apf_system_residual_norms: no solution held (solve first or pass x)");
+        apf::DeviceBuffer<double> b(n, s), r(n, s), xd;
+        apf::copy(s, nl, S.f.get(), b.get());
+        apf::copy(s, nu, S.g.get(), b.get() + nl);
+        const double* xp = S.solution.get();
+        if (x)
+        {
+            xd.allocate(n, s);
+            APF_CUDA(cudaMemcpyAsync(xd.get(), x, n * sizeof(double),
+                                     pointers_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+            xp = xd.get();
+        }
+        apf::residual(s, S.blocks[APF_BLOCK_K], xp, b.get(), r.get());
+        const double rr = apf::dot_host(s, S.ws, n, r.get(), r.get());
+        const double bb = apf::dot_host(s, S.ws, n, b.get(), b.get());
+        *residual_norm = rr >= 0.0 ? std::sqrt(rr) : std::numeric_limits<double>::quiet_NaN();
+        *rhs_norm = bb >= 0.0 ? std::sqrt(bb) : std::numeric_limits<double>::quiet_NaN();
     });
 }
 

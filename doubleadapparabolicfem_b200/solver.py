@@ -67,11 +67,12 @@ def setup_preconditioner(blocks: MainSystemBlocks, options: SolverOptions | None
 
 def solve_saddle_system_with_preconditioner(blocks: MainSystemBlocks, options: SolverOptions | None = None,
                                             initial_guess: np.ndarray | None = None, copy_out: bool = True,
-                                            rhs: np.ndarray | None = None):
-    """Solve K [lambda; u] = [f; g] (or K x = rhs: e.g. the correction equation
-    K d = b - K x0 of an initial guess x0, as the reference's dispatcher solves it with
-    MainSystemInitialGuess::solve_correction_equation).  Returns (solution or None,
-    diagnostics dict)."""
+                                            rhs: np.ndarray | None = None, correction: bool = False):
+    """Solve K [lambda; u] = [f; g] (or K x = rhs).  correction=True with an initial guess
+    x0 solves the correction equation K d = [f; g] - K x0 from zero on the device and
+    returns x0 + d, as the reference's dispatcher does with
+    MainSystemInitialGuess::solve_correction_equation (solve_saddle_system.hpp:75-86).
+    Returns (solution or None, diagnostics dict)."""
     options = options or SolverOptions()
     ctx = blocks.ctx
     o = options.to_c()
@@ -82,8 +83,13 @@ def solve_saddle_system_with_preconditioner(blocks: MainSystemBlocks, options: S
         guess = np.ascontiguousarray(initial_guess, dtype=np.float64)
         if guess.size != n:
             raise ValueError("initial guess size does not match the full saddle system")
+    if correction and (guess is None or rhs is not None):
+        raise ValueError("the correction equation needs an initial guess and the assembled right-hand side")
     d = _lib.SolverDiagnostics()
-    if rhs is None:
+    if correction:
+        rc = ctx.lib.apf_solve_minres_correction(ctx.handle, blocks.handle, C.byref(o), _ptr(guess), _ptr(out), 0,
+                                                 C.byref(d))
+    elif rhs is None:
         rc = ctx.lib.apf_solve_minres(ctx.handle, blocks.handle, C.byref(o), _ptr(guess), _ptr(out), 0, C.byref(d))
     else:
         b = np.ascontiguousarray(rhs, dtype=np.float64)
@@ -96,6 +102,18 @@ def solve_saddle_system_with_preconditioner(blocks: MainSystemBlocks, options: S
         raise PreconditionedSolveFailure(ctx.lib.apf_ctx_last_error(ctx.handle).decode(), diag)
     ctx.check(rc)
     return out, diag
+
+
+def residual_norms(blocks: MainSystemBlocks, x: np.ndarray | None = None) -> tuple[float, float]:
+    """(||[f; g] - K x||, ||[f; g]||) on the device; x None = the solution the system holds
+    (solve_main_system.hpp:540-572: the post-solve and initial-guess residual diagnostics)."""
+    xp = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+    if xp is not None and xp.size != blocks.n_lambda() + blocks.n_u():
+        raise ValueError("x size does not match the full saddle system")
+    r, b = C.c_double(), C.c_double()
+    blocks.ctx.check(blocks.ctx.lib.apf_system_residual_norms(blocks.ctx.handle, blocks.handle, _ptr(xp), 0,
+                                                              C.byref(r), C.byref(b)))
+    return r.value, b.value
 
 
 def split_solution(blocks: MainSystemBlocks, x: np.ndarray):

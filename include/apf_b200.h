@@ -248,6 +248,20 @@ int apf_solve_minres(apf_ctx* ctx, apf_system* sys, const apf_solver_options* op
 int apf_solve_minres_with_rhs(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* rhs,
                               const double* initial_guess, double* solution, int pointers_on_device,
                               apf_solver_diagnostics* diag);
+/* The correction equation on the device: r = [f; g] - K x0, MINRES on K d = r from zero (its
+ * tolerance relative to ||r||), solution = x0 + d, which the system then holds.  The
+ * reference's dispatcher forms r = rhs - K x0 on the host and returns x0 + d
+ * (src/linear_algebra/eigen_backend/preconditioners/solve_saddle_system.hpp:75-86,
+ * src/finite_element/system/solve_main_system.hpp:1547-1560 for the direct path).
+ * x0: n_lambda + n_u values; solution may be NULL (kept on the device only). */
+int apf_solve_minres_correction(apf_ctx* ctx, apf_system* sys, const apf_solver_options* opt, const double* x0,
+                                double* solution, int pointers_on_device, apf_solver_diagnostics* diag);
+/* ||[f; g] - K x|| and ||[f; g]|| on the device, x NULL = the solution the system holds: the
+ * post-solve residual the reference records in Summary diagnostics mode
+ * (src/finite_element/system/solve_main_system.hpp:540-572, 651-700) and, with x = x0, its
+ * initial-guess residual (solve_main_system.hpp:587-604). */
+int apf_system_residual_norms(apf_ctx* ctx, apf_system* sys, const double* x, int pointers_on_device,
+                              double* residual_norm, double* rhs_norm);
 /* Replace the solution the system holds (n_lambda + n_u values; read by apf_estimate,
  * apf_x_indicators and apf_g_estimator): e.g. x0 + d after the correction equation's solve
  * for d, as the reference's dispatcher returns it. */

@@ -59,6 +59,7 @@
 #include <concepts>
 #include <cstdint>
 #include <cstdlib>
+#include <limits>
 #include <memory>
 #include <optional>
 #include <stdexcept>
@@ -567,6 +568,60 @@ namespace finite_element::system
     }
 }
 
+namespace la::b200::detail
+{
+    // the device MINRES options of a solve: the session's preconditioner and AMG parameters
+    // with the tolerance, iteration limit and batching of the reference's SolverOptions
+    [[nodiscard]] inline apf_solver_options minres_options(Session& s, const la::concepts::SolverOptions& options)
+    {
+        apf_solver_options o = s.solver_options();
+        o.tolerance = options.tolerance;
+        o.max_iterations = options.max_iterations;
+        o.use_true_residual_batching = options.use_true_residual_batching ? 1 : 0;
+        o.true_residual_check_interval = options.true_residual_check_interval;
+        return o;
+    }
+
+    // the reference's SolverDiagnostics of a MINRES + ParabolicGraphNorm solve
+    // (parabolic_graph_norm_minres.hpp:267-307, iterative_residual_acceptance.hpp:62-92) from
+    // the device solve's diagnostics
+    [[nodiscard]] inline la::concepts::SolverDiagnostics solver_diagnostics(Session& s,
+                                                                            const la::concepts::SolverOptions& options,
+                                                                            const apf_solver_diagnostics& d)
+    {
+        la::concepts::SolverDiagnostics diag;
+        diag.requested_solver = options.solver;
+        diag.effective_solver = la::concepts::SolverType::MINRES;
+        diag.preconditioner = options.preconditioner;
+        int32_t kr = 0, kc = 0;
+        int64_t knnz = 0;
+        check(s.context(), apf_system_block_info(s.system(), APF_BLOCK_K, &kr, &kc, &knnz), "apf_system_block_info");
+        diag.rows = kr;
+        diag.cols = kc;
+        diag.nnz_matrix = static_cast<std::size_t>(knnz);
+        diag.direct = false;
+        diag.iterative = true;
+        diag.linear_residual_relative = d.final_true_residual;
+        diag.preconditioner_setup_seconds = d.setup_seconds;
+        diag.preconditioner_stats.setup_seconds = d.setup_seconds;
+        diag.preconditioner_stats.assumes_spd = true;
+        diag.preconditioner_stats.assumes_symmetric = true;
+        diag.preconditioner_stats.is_spd = true;
+        diag.preconditioner_stats.is_symmetric = true;
+        auto& it = diag.iterative_stats;
+        it.iterations = d.iterations;
+        it.final_error = d.backend_reported_error;
+        it.converged = d.converged != 0;
+        it.backend_converged = d.backend_converged != 0;
+        it.backend_reported_error = d.backend_reported_error;
+        it.convergence_accepted_by_true_residual = d.converged != 0;
+        it.residual_check_batches = d.residual_check_batches;
+        it.final_true_residual = d.final_true_residual;
+        it.true_residual_stopping_used = options.use_true_residual_batching;
+        return diag;
+    }
+}
+
 namespace la::preconditioners
 {
     // parabolic_graph_norm_approximation (src/linear_algebra/preconditioners/
@@ -674,11 +729,7 @@ namespace la::preconditioners
                     x0[static_cast<std::size_t>(i)] = (*initial_guess.full_vector)[i];
             }
 
-            apf_solver_options o = s.solver_options();
-            o.tolerance = options.tolerance;
-            o.max_iterations = options.max_iterations;
-            o.use_true_residual_batching = options.use_true_residual_batching ? 1 : 0;
-            o.true_residual_check_interval = options.true_residual_check_interval;
+            const apf_solver_options o = la::b200::detail::minres_options(s, options);
             std::vector<double> x(static_cast<std::size_t>(n));
             apf_solver_diagnostics d{};
             const int rc = apf_solve_minres_with_rhs(ctx, sys, &o, b.data(), x0.empty() ? nullptr : x0.data(),
@@ -687,37 +738,7 @@ namespace la::preconditioners
             if (rc != APF_OK && rc != APF_ERR_NOT_CONVERGED)
                 la::b200::check(ctx, rc, "apf_solve_minres_with_rhs");
 
-            la::concepts::SolverDiagnostics diag;
-            diag.requested_solver = options.solver;
-            diag.effective_solver = la::concepts::SolverType::MINRES;
-            diag.preconditioner = options.preconditioner;
-            diag.rows = K.rows();
-            diag.cols = K.cols();
-            {
-                int32_t kr = 0, kc = 0;
-                int64_t knnz = 0;
-                la::b200::check(ctx, apf_system_block_info(sys, APF_BLOCK_K, &kr, &kc, &knnz), "apf_system_block_info");
-                diag.nnz_matrix = static_cast<std::size_t>(knnz);
-            }
-            diag.direct = false;
-            diag.iterative = true;
-            diag.linear_residual_relative = d.final_true_residual;
-            diag.preconditioner_setup_seconds = d.setup_seconds;
-            diag.preconditioner_stats.setup_seconds = d.setup_seconds;
-            diag.preconditioner_stats.assumes_spd = true;
-            diag.preconditioner_stats.assumes_symmetric = true;
-            diag.preconditioner_stats.is_spd = true;
-            diag.preconditioner_stats.is_symmetric = true;
-            auto& it = diag.iterative_stats;
-            it.iterations = d.iterations;
-            it.final_error = d.backend_reported_error;
-            it.converged = d.converged != 0;
-            it.backend_converged = d.backend_converged != 0;
-            it.backend_reported_error = d.backend_reported_error;
-            it.convergence_accepted_by_true_residual = d.converged != 0;
-            it.residual_check_batches = d.residual_check_batches;
-            it.final_true_residual = d.final_true_residual;
-            it.true_residual_stopping_used = options.use_true_residual_batching;
+            auto diag = la::b200::detail::solver_diagnostics(s, options, d);
             if (rc == APF_ERR_NOT_CONVERGED)
                 throw PreconditionedSolveFailure(apf_ctx_last_error(ctx), diag);
 
@@ -745,6 +766,143 @@ namespace la::preconditioners
 // to them; the reference's adaptive driver (algorithm/adaptive_driver.hpp), included after
 // this header, binds to the overload below.
 #include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
+
+namespace la::b200::detail
+{
+    // Whether the main solve of an inner iteration can stay on the device: MINRES with the
+    // parabolic graph-norm preconditioner and no full-matrix symmetry scan (the reference's
+    // Detailed diagnostics mode reads every entry of K on the host).
+    [[nodiscard]] inline bool device_main_solve_applies(const la::concepts::SolverOptions& options)
+    {
+        return la::preconditioners::is_saddle_preconditioned_solve_requested(options) &&
+               finite_element::system::detail::diagnostics_mode_with_required_residual(options) !=
+                   la::concepts::SolverDiagnosticsMode::Detailed;
+    }
+
+    // assemble_and_solve_into_functions (solve_main_system.hpp:1815-2016) for MINRES +
+    // ParabolicGraphNorm with every block kept on the device: assembly, the graph-norm block
+    // Hhat (from the device's own B_dt and A_x, so the host assembly of both that
+    // assemble_parabolic_graph_norm_approximation runs is skipped), the MINRES solve (with
+    // the initial guess or the correction equation), and the Summary diagnostics' residuals;
+    // only the solution comes back, into lambda_h and u_h.  The blocks are not copied to host
+    // matrices and K is not composed on the host.
+    template<class Backend, class YSpaceType, class XSpaceType, class ExampleType>
+    [[nodiscard]] finite_element::system::SaddleProblemSolveResult<Backend, YSpaceType, XSpaceType>
+    device_main_solve(finite_element::Function<YSpaceType, typename Backend::Vector>& lambda_h,
+                      finite_element::Function<XSpaceType, typename Backend::Vector>& u_h,
+                      const YSpaceType& y_space, const XSpaceType& x_space, const ExampleType& example,
+                      const la::concepts::SolverOptions& options, double zero_tol,
+                      const finite_element::system::MainSystemInitialGuess<Backend>& initial_guess,
+                      const finite_element::detail::TimingRecorder& timing)
+    {
+        using Clock = std::chrono::steady_clock;
+        const int nl = y_space.dof_handler_ref().n_true_dofs();
+        const int nu = x_space.dof_handler_ref().n_true_dofs();
+        if (nl == 0 || nu == 0)
+            throw std::runtime_error("solve_main_system_blocks: refusing to solve main system with zero true DoFs. "
+                                     "Y/lambda true DoFs=" + std::to_string(nl) + ", X/u true DoFs=" +
+                                     std::to_string(nu) +
+                                     ". Refine the mesh or use a space with interior true DoFs.");
+        const int n = nl + nu;
+        if (initial_guess.has_value() && initial_guess.full_vector->size() != n)
+            throw std::runtime_error(
+                "solve_main_system_blocks: initial guess size does not match the full saddle system.");
+        Session& s = session();
+        apf_ctx* ctx = s.context();
+        {
+            auto total = timing.scoped("main_system.assembly_total_wall");
+            auto timer = timing.scoped("assembly.total_seconds");
+            const ProblemArrays arrays = [&] {
+                auto t = timing.scoped("b200.describe_spaces_wall");
+                return describe(y_space, x_space, example, zero_tol, -1.0);
+            }();
+            auto t = timing.scoped("b200.upload_and_assembly_wall");
+            apf_system* sys = nullptr;
+            check(ctx, apf_assemble_main_system(ctx, &arrays.desc, 0, &sys), "apf_assemble_main_system");
+            s.adopt(sys, zero_tol);
+        }
+        apf_system* sys = s.system();
+        {
+            // assemble_parabolic_graph_norm_approximation's default diagonal tolerance
+            // (parabolic_graph_norm.hpp:29)
+            auto timer = timing.scoped("main_system.construct_graph_norm_context");
+            check(ctx, apf_assemble_graph_norm(ctx, sys, 1.0e-14), "apf_assemble_graph_norm");
+        }
+        std::vector<double> x0;
+        if (initial_guess.has_value())
+        {
+            const auto& g = *initial_guess.full_vector;
+            x0.resize(static_cast<std::size_t>(n));
+            for (int i = 0; i < n; ++i)
+                x0[static_cast<std::size_t>(i)] = g[i];
+        }
+        const apf_solver_options o = minres_options(s, options);
+        std::vector<double> x(static_cast<std::size_t>(n));
+        apf_solver_diagnostics d{};
+        const auto solve_start = Clock::now();
+        const int rc = initial_guess.has_value() && initial_guess.solve_correction_equation
+                           ? apf_solve_minres_correction(ctx, sys, &o, x0.data(), x.data(), 0, &d)
+                           : apf_solve_minres(ctx, sys, &o, x0.empty() ? nullptr : x0.data(), x.data(), 0, &d);
+        timing.add("main_system.solver_total_wall", std::chrono::duration<double>(Clock::now() - solve_start).count());
+        s.set_last_diagnostics(d);
+        if (rc != APF_OK && rc != APF_ERR_NOT_CONVERGED)
+            check(ctx, rc, "apf_solve_minres");
+        auto diag = solver_diagnostics(s, options, d);
+        if (rc == APF_ERR_NOT_CONVERGED)
+            throw la::preconditioners::PreconditionedSolveFailure(apf_ctx_last_error(ctx), diag);
+
+        const auto postprocess_start = Clock::now();
+        // the residual diagnostics of solve_main_system_blocks (solve_main_system.hpp:1450-1470)
+        auto relative = [](double r, double b) {
+            return std::isfinite(r) ? r / (std::isfinite(b) && b > 0.0 ? b : 1.0)
+                                    : std::numeric_limits<double>::quiet_NaN();
+        };
+        if (initial_guess.has_value())
+        {
+            auto timer = timing.scoped("main_system.correction_or_initial_guess_wall");
+            double r0 = 0.0, b = 0.0, g2 = 0.0;
+            check(ctx, apf_system_residual_norms(ctx, sys, x0.data(), 0, &r0, &b), "apf_system_residual_norms");
+            for (const double v : x0)
+                g2 += v * v;
+            diag.initial_guess_norm = std::sqrt(g2);
+            diag.initial_residual_absolute = r0;
+            diag.initial_residual_relative = relative(r0, b);
+        }
+        if (finite_element::system::detail::diagnostics_mode_with_required_residual(options) !=
+            la::concepts::SolverDiagnosticsMode::Off)
+        {
+            auto timer = timing.scoped("main_system.solver_residual_check_wall");
+            double r = 0.0, b = 0.0;
+            check(ctx, apf_system_residual_norms(ctx, sys, nullptr, 0, &r, &b), "apf_system_residual_norms");
+            diag.linear_residual_absolute = r;
+            diag.linear_residual_relative = relative(r, b);
+        }
+        finite_element::system::SaddleProblemSolveResult<Backend, YSpaceType, XSpaceType> result;
+        result.lambda_true = typename Backend::Vector(nl);
+        result.u_true = typename Backend::Vector(nu);
+        for (int i = 0; i < nl; ++i)
+            result.lambda_true[i] = x[static_cast<std::size_t>(i)];
+        for (int i = 0; i < nu; ++i)
+            result.u_true[i] = x[static_cast<std::size_t>(nl + i)];
+        result.solver_diagnostics = std::move(diag);
+        result.solver_setup_seconds = d.setup_seconds;
+        result.solver_solve_seconds = d.solve_seconds;
+        timing.add("main_system.solver_setup", result.solver_setup_seconds);
+        timing.add("main_system.solver_solve", result.solver_solve_seconds);
+        timing.add("solve.setup_seconds", result.solver_setup_seconds);
+        timing.add("solve.factorization_seconds", result.solver_setup_seconds);
+        timing.add("solve.backsolve_seconds", result.solver_solve_seconds);
+        timing.add("main_system.postprocess_wall",
+                   std::chrono::duration<double>(Clock::now() - postprocess_start).count());
+        {
+            auto timer = timing.scoped("main_system.solution_update_wall");
+            auto function_timer = timing.scoped("main_system.function_update_wall");
+            lambda_h.update_from_true_solution(result.lambda_true);
+            u_h.update_from_true_solution(result.u_true);
+        }
+        return result;
+    }
+}
 
 namespace finite_element::time_slabs
 {
@@ -778,11 +936,17 @@ namespace finite_element::time_slabs
                 guess.full_vector = &*guess_vector;
                 guess.solve_correction_equation = parameters.solve_main_system_correction;
             }
-            const auto main_solve = finite_element::system::assemble_and_solve_into_functions<QSpace, QTime, Backend>(
-                state.lambda_delta, state.u_delta, y_space, x_space, example, solver, main_solver_options,
-                parameters.zero_tol, -1.0, guess,
-                static_cast<const finite_element::system::MainSystemTwoLevelHierarchy<YSpaceType, XSpaceType>*>(nullptr),
-                parameters.timing);
+            const auto main_solve =
+                la::b200::detail::device_main_solve_applies(main_solver_options)
+                    ? la::b200::detail::device_main_solve<Backend>(state.lambda_delta, state.u_delta, y_space,
+                                                                   x_space, example, main_solver_options,
+                                                                   parameters.zero_tol, guess, parameters.timing)
+                    : finite_element::system::assemble_and_solve_into_functions<QSpace, QTime, Backend>(
+                          state.lambda_delta, state.u_delta, y_space, x_space, example, solver,
+                          main_solver_options, parameters.zero_tol, -1.0, guess,
+                          static_cast<const finite_element::system::MainSystemTwoLevelHierarchy<YSpaceType,
+                                                                                                XSpaceType>*>(nullptr),
+                          parameters.timing);
             state.main_solve_diagnostics = main_solve.solver_diagnostics;
             state.main_solve_setup_seconds = main_solve.solver_setup_seconds;
             state.main_solve_solve_seconds = main_solve.solver_solve_seconds;

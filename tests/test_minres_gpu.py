@@ -66,3 +66,38 @@ def test_minres_failure_raises_with_diagnostics(gpu_ctx):
                                                                       true_residual_check_interval=1))
     assert e.value.diagnostics["iterations"] <= 3
     assert e.value.diagnostics["converged"] == 0
+
+
+@pytest.mark.parametrize("level,p", [(3, 1), (2, 2)])
+def test_correction_equation_and_residual_norms(gpu_ctx, level, p):
+    """The device correction equation (K d = b - K x0 from zero, x = x0 + d; the dispatcher's
+    solve_correction_equation, solve_saddle_system.hpp:75-86) against the same equation with
+    the residual formed on the host, and the device residual norms against numpy."""
+    from doubleadapparabolicfem_b200.assembly import assemble_main_system_blocks
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    from doubleadapparabolicfem_b200.solver import (SolverOptions, residual_norms,
+                                                    solve_saddle_system_with_preconditioner)
+    blocks = assemble_main_system_blocks(uniform_problem(level, p), ctx=gpu_ctx)
+    blocks.assemble_parabolic_graph_norm_approximation()
+    K = blocks.K()
+    b = np.concatenate([blocks.f(), blocks.g()])
+    x0 = np.random.default_rng(3).standard_normal(b.size) * 1e-2
+    tol = 1e-10
+    x, diag = solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=tol), initial_guess=x0,
+                                                      correction=True)
+    r0 = b - K @ x0
+    # the tolerance is relative to the correction equation's right-hand side
+    assert np.linalg.norm(K @ x - b) <= 1.0001 * tol * np.linalg.norm(r0), diag
+    assert diag["converged"] == 1
+    d_host, diag_host = solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=tol), rhs=r0)
+    # the two right-hand sides differ by the SpMV's rounding only; on this rough r0 that
+    # moves MINRES's stopping iteration by up to ~15 %, so the solutions are compared
+    assert diag_host["converged"] == 1
+    assert np.linalg.norm(x - (x0 + d_host)) <= 1e-6 * np.linalg.norm(x)
+    # the system holds x0 + d after the correction solve
+    res, bn = residual_norms(blocks)
+    assert abs(bn - np.linalg.norm(b)) <= 1e-13 * np.linalg.norm(b)
+    # (d_host's solve replaced the held solution: compare against it)
+    assert abs(res - np.linalg.norm(K @ d_host - b)) <= 1e-10 * np.linalg.norm(b)
+    res0, _ = residual_norms(blocks, x0)
+    assert abs(res0 - np.linalg.norm(r0)) <= 1e-12 * np.linalg.norm(b)
