@@ -441,6 +441,8 @@ namespace
         par.use_adaptive_initial_guess = guess >= 1;
         par.solve_main_system_correction = guess == 2;
         par.timing.enabled = !compare; // the driver's own phase timing for the b200-only run
+        if (const char* e = std::getenv("APF_DROPIN_AMG_STRENGTH"))
+            la::b200::session().solver_options().amg_strength = std::atof(e);
         const auto t0 = std::chrono::steady_clock::now();
         typename B200::Solver sa;
         const auto ra = adaptive_algorithm::run_adaptive_driver<S::QSpace, S::QTime, B200>(
@@ -462,10 +464,13 @@ namespace
                 std::snprintf(buf, sizeof(buf),
                               "%s{\"outer\": %d, \"x_dofs\": %d, \"y_dofs\": %d, \"inner\": %zu, "
                               "\"eta_squared\": %.15e, \"lambda_y_squared\": %.15e, "
-                              "\"initial_trace_squared\": %.15e, \"y_estimator_squared\": %.15e}",
+                              "\"initial_trace_squared\": %.15e, \"y_estimator_squared\": %.15e, "
+                              "\"last_solve_iterations\": %d, \"last_solve_seconds\": %.4f}",
                               k ? ", " : "", o.outer_iteration, o.n_x_true_dofs_before, o.n_y_true_dofs_after,
                               o.inner_iterations.size(), o.eta_squared, o.lambda_y_squared,
-                              o.initial_trace_squared, o.y_estimator_squared);
+                              o.initial_trace_squared, o.y_estimator_squared,
+                              o.inner_iterations.empty() ? -1 : o.inner_iterations.back().main_solve.iteration_count,
+                              o.inner_iterations.empty() ? 0.0 : o.inner_iterations.back().main_solve.backsolve_seconds);
                 out += buf;
             }
             return out + "]";
@@ -478,11 +483,17 @@ namespace
                 if (r.metric_kind == adaptive_algorithm::MetricKind::duration_seconds)
                     rec.emplace_back(r.total_seconds, r.phase);
             std::sort(rec.rbegin(), rec.rend());
-            for (std::size_t k = 0; k < rec.size() && k < 25; ++k)
+            // the 25 slowest, and every phase of the b200 main solve
+            bool first = true;
+            for (std::size_t k = 0; k < rec.size(); ++k)
             {
+                const std::string& name = rec[k].second;
+                if (k >= 25 && name.rfind("b200.", 0) != 0 && name.rfind("main_system.", 0) != 0)
+                    continue;
                 char buf[256];
-                std::snprintf(buf, sizeof(buf), "%s[\"%s\", %.3f]", k ? ", " : "", rec[k].second.c_str(), rec[k].first);
+                std::snprintf(buf, sizeof(buf), "%s[\"%s\", %.3f]", first ? "" : ", ", name.c_str(), rec[k].first);
                 phases += buf;
+                first = false;
             }
         }
         phases += "]";
