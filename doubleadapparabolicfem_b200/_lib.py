@@ -194,6 +194,11 @@ class EstimatorResult(C.Structure):
 SIGNATURES["apf_estimate"] = ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                C.c_void_p, C.POINTER(EstimatorResult)], C.c_int)
 
+SIGNATURES["apf_system_keep_flux"] = ([C.c_void_p, C.c_void_p, C.c_int], C.c_int)
+SIGNATURES["apf_flux_cells"] = ([C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p], C.c_int)
+SIGNATURES["apf_flux_sample"] = ([C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int],
+                                 C.c_int)
+
 SIGNATURES["apf_true_residual_noalloc"] = ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int)
 

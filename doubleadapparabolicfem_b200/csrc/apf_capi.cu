@@ -979,6 +979,52 @@ int apf_system_residual_norms(apf_ctx* ctx, apf_system* sys, const double* x, in
     });
 }
 
+int apf_system_keep_flux(apf_ctx* ctx, apf_system* sys, int keep)
+{
+    if (!ctx || !sys)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        auto& S = sys->sys;
+        S.keep_flux = keep != 0;
+        if (!S.keep_flux)
+        {
+            S.flux_cells = 0;
+            S.flux_sigma = apf::DeviceBuffer<double>();
+            S.flux_geo = apf::DeviceBuffer<double>();
+            S.flux_slab.clear();
+            S.flux_source.clear();
+        }
+    });
+}
+
+int apf_flux_cells(apf_ctx* ctx, const apf_system* sys, int32_t* n_cells, int32_t* slab, int32_t* source_y_cell)
+{
+    if (!ctx || !sys || !n_cells)
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        const auto& S = sys->sys;
+        *n_cells = S.flux_cells;
+        for (int c = 0; c < S.flux_cells; ++c)
+        {
+            if (slab)
+                slab[c] = S.flux_slab[static_cast<std::size_t>(c)];
+            if (source_y_cell)
+                source_y_cell[c] = S.flux_source[static_cast<std::size_t>(c)];
+        }
+    });
+}
+
+int apf_flux_sample(apf_ctx* ctx, apf_system* sys, int32_t n_points, const int32_t* cell, const double* points,
+                    double* values, int pointers_on_device)
+{
+    if (!ctx || !sys || n_points < 0 || (n_points > 0 && (!cell || !points || !values)))
+        return APF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        APF_HOST_RANGE("call_flux_sample");
+        apf::flux_sample(ctx->stream, sys->sys, n_points, cell, points, values, pointers_on_device != 0);
+    });
+}
+
 int apf_preconditioner_apply(apf_ctx* ctx, apf_system* sys, int block, const double* r, double* z,
                              int pointers_on_device)
 {

@@ -2178,6 +2178,141 @@ namespace apf
         tot.recon_residual = bn > 0.0 ? rn / bn : 0.0;
     }
 
+    namespace
+    {
+        // sigma_x, sigma_y and div sigma of the kept flux at physical points (x, y, t), point i
+        // in estimator cell cell[i]: the cell's three vertex-patch slots summed in a fixed
+        // order (as the indicator kernels do), in the cell's own RT_p basis (Piola map of the
+        // affine cell) times the P_p time basis of its interval.  A cell index out of range
+        // gives NaN values and sets *bad.
+        __global__ void flux_sample_kernel(int n, const int* __restrict__ cell, const double* __restrict__ pts,
+                                           int n_cells, const double* __restrict__ geo,
+                                           const double* __restrict__ sigma, int p,
+                                           const Rt2Tables* __restrict__ t2, double* __restrict__ out,
+                                           int* __restrict__ bad)
+        {
+            for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            {
+                const int c = cell[i];
+                if (c < 0 || c >= n_cells)
+                {
+                    out[3ll * i] = out[3ll * i + 1] = out[3ll * i + 2] = __longlong_as_double(0x7ff8000000000000ll);
+                    *bad = 1;
+                    continue;
+                }
+                const Cell k = load_cell(geo, nullptr, nullptr, c);
+                const double dx = pts[3ll * i] - k.x0, dy = pts[3ll * i + 1] - k.y0;
+                const double x = (k.J11 * dx - k.J01 * dy) / k.det;
+                const double y = (-k.J10 * dx + k.J00 * dy) / k.det;
+                const double tau = (pts[3ll * i + 2] - k.t0) / k.ht;
+                double sx = 0.0, sy = 0.0, sd = 0.0;
+                if (p == 1)
+                {
+                    const double tb[2] = {1.0 - tau, tau};
+                    for (int j = 0; j < 8; ++j)
+                    {
+                        double cj = 0.0;
+                        for (int a = 0; a < 2; ++a)
+                        {
+                            double sj = 0.0;
+                            for (int slot = 0; slot < 3; ++slot)
+                                sj += sigma[((3ll * c + slot) * 2 + a) * 8 + j];
+                            cj += sj * tb[a];
+                        }
+                        double vx, vy, dv;
+                        rt_phys(k, j, x, y, vx, vy, dv);
+                        sx += cj * vx;
+                        sy += cj * vy;
+                        sd += cj * dv;
+                    }
+                }
+                else
+                {
+                    double T[3], dT[3];
+                    p2_time(tau, T, dT);
+                    double mvx[15], mvy[15], mdv[15];
+                    mono15(x, y, mvx, mvy, mdv);
+                    const double sdet = k.det < 0.0 ? -1.0 : 1.0;
+                    for (int j = 0; j < 15; ++j)
+                    {
+                        double vx = 0.0, vy = 0.0, dv = 0.0;
+                        for (int m = 0; m < 15; ++m)
+                        {
+                            vx += t2->c[j][m] * mvx[m];
+                            vy += t2->c[j][m] * mvy[m];
+                            dv += t2->c[j][m] * mdv[m];
+                        }
+                        const double f = (j < 9 ? sdet : 1.0) / k.det;
+                        double cj = 0.0;
+                        for (int a = 0; a < 3; ++a)
+                        {
+                            double sj = 0.0;
+                            for (int slot = 0; slot < 3; ++slot)
+                                sj += sigma[((3ll * c + slot) * 3 + a) * 15 + j];
+                            cj += T[a] * sj;
+                        }
+                        sx += cj * f * (k.J00 * vx + k.J01 * vy);
+                        sy += cj * f * (k.J10 * vx + k.J11 * vy);
+                        sd += cj * f * dv;
+                    }
+                }
+                out[3ll * i] = sx;
+                out[3ll * i + 1] = sy;
+                out[3ll * i + 2] = sd;
+            }
+        }
+    }
+
+    void flux_sample(cudaStream_t s, const System& S, int n, const int* cell, const double* points, double* values,
+                     bool on_device)
+    {
+        require(S.flux_cells > 0 && S.flux_sigma.size() > 0, APF_ERR_INVALID,
+                "flux samples: no kept flux (set keep_flux and run a 2+1D estimate first)");
+        require(n >= 0, APF_ERR_INVALID, "flux samples: negative point count");
+        if (n == 0)
+            return;
+        if (!on_device)
+            for (int i = 0; i < n; ++i)
+                require(cell[i] >= 0 && cell[i] < S.flux_cells, APF_ERR_INVALID, "flux samples: cell index out of range");
+        upload_est_tables_once();
+        DeviceBuffer<double> d_t2(0, s);
+        if (S.flux_p == 2)
+        {
+            const Rt2Tables t2 = make_rt2_tables(make_est_tables());
+            d_t2.upload(reinterpret_cast<const double*>(&t2), kRt2Doubles);
+        }
+        DeviceBuffer<int> d_cell(0, s), bad(1, s);
+        DeviceBuffer<double> d_pts(0, s), d_out(0, s);
+        const int* pc = cell;
+        const double* pp = points;
+        double* po = values;
+        if (!on_device)
+        {
+            d_cell.upload(cell, static_cast<std::size_t>(n));
+            d_pts.upload(points, 3ull * n);
+            d_out.allocate(3ull * n, s);
+            pc = d_cell.get();
+            pp = d_pts.get();
+            po = d_out.get();
+        }
+        bad.zero();
+        {
+            APF_KERNEL("est_flux_sample", s);
+            flux_sample_kernel<<<nb(n, 128), 128, 0, s>>>(n, pc, pp, S.flux_cells, S.flux_geo.get(), S.flux_sigma.get(),
+                                                          S.flux_p,
+                                                          reinterpret_cast<const Rt2Tables*>(d_t2.size() ? d_t2.get()
+                                                                                                         : nullptr),
+                                                          po, bad.get());
+        }
+        APF_CUDA(cudaGetLastError());
+        int hbad = 0;
+        APF_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (!on_device)
+            APF_CUDA(cudaMemcpyAsync(values, d_out.get(), 3ull * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        sync(s);
+        require(hbad == 0, APF_ERR_INVALID, "flux samples: cell index out of range");
+    }
+
     EstimatorTotals estimate(cudaStream_t s, System& S, const std::vector<int>& vids_host, double* flux, double* div,
                                 double* recon, double* eta, bool out_on_device, int patch_precision,
                                 PatchTuner* tuner)
@@ -2190,6 +2325,9 @@ namespace apf
                 "estimator: solve the main system first");
         require(S.precond != nullptr, APF_ERR_INVALID, "estimator: preconditioner missing");
         upload_est_tables_once();
+        S.flux_cells = 0;
+        S.flux_sigma = DeviceBuffer<double>();
+        S.flux_geo = DeviceBuffer<double>();
         EstimatorTotals tot{};
         const int ny = in.n_y_cells, nl = in.n_lambda, nd = in.ndof;
         const int ns = in.p == 1 ? 3 : 6, nt = in.p + 1;
@@ -2559,6 +2697,26 @@ namespace apf
             cell_indicators<<<nb(nc, 128), 128, 0, s>>>(ia);
         }
         APF_CUDA(cudaGetLastError());
+        if (S.keep_flux)
+        {
+            // the flux stays on the device for flux_sample, keyed by (slab, source Y cell)
+            S.flux_p = in.p;
+            S.flux_cells = nc;
+            S.flux_sigma = std::move(sigma);
+            S.flux_geo.allocate(8ll * nc, s);
+            copy(s, 8 * nc, cgeo, S.flux_geo.get());
+            S.flux_slab.assign(static_cast<std::size_t>(nc), -1);
+            for (int sb = 0; sb + 1 < static_cast<int>(ps.slab_ptr.size()); ++sb)
+                for (int q = ps.slab_ptr[sb]; q < ps.slab_ptr[sb + 1]; ++q)
+                    S.flux_slab[static_cast<std::size_t>(ps.slab_cells[q])] = sb;
+            if (sp.identity)
+            {
+                S.flux_source.resize(static_cast<std::size_t>(nc));
+                std::iota(S.flux_source.begin(), S.flux_source.end(), 0);
+            }
+            else
+                S.flux_source = sp.source;
+        }
         if (!sp.identity)
         {
             DeviceBuffer<double> tmp(nc, s);

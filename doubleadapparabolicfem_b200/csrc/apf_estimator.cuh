@@ -58,6 +58,12 @@ namespace apf
                                 double* recon, double* eta, bool out_on_device, int patch_precision = APF_PATCH_FP64,
                                 PatchTuner* tuner = nullptr);
 
+    // sigma_x, sigma_y, div sigma (values: [n][3]) of the flux kept by the last estimate
+    // (System::keep_flux) at physical points (x, y, t) ([n][3]), point i in estimator cell
+    // cell[i] (0 <= cell[i] < S.flux_cells)
+    void flux_sample(cudaStream_t s, const System& S, int n, const int* cell, const double* points, double* values,
+                     bool on_device);
+
     // lambda~ of the slab reconstruction: A_y lambda~ = f - B^T u by PCG with the A_y
     // V-cycle from lambda_delta (relative residual 1e-14, at most 400 iterations)
     void reconstruct_lambda(cudaStream_t s, System& S, DeviceBuffer<double>& lt, EstimatorTotals& tot);

@@ -65,6 +65,13 @@ namespace apf
         unsigned long long precond_model_version = 0; // learned model the weights came from
         Partition partition;                 // stacked independent problems (apf_system_set_partition)
         std::vector<double> part_residuals;  // per-part true relative residuals of the last solve
+        // the equilibrated flux of the last 2+1D estimate, kept when keep_flux is set: per
+        // estimator cell (the Y cells, or the slab cells they are cut into) the flux
+        // coefficients of its three vertex-patch slots, its geometry, time slab and source Y cell
+        bool keep_flux = false;
+        int flux_p = 0, flux_cells = 0;
+        DeviceBuffer<double> flux_sigma, flux_geo;
+        std::vector<int> flux_slab, flux_source;
     };
 
     void upload_tables_once(int device);

@@ -57,6 +57,37 @@ def estimate(blocks: MainSystemBlocks, y_vertex_ids: np.ndarray | None = None, p
     return out, totals
 
 
+def keep_flux(blocks: MainSystemBlocks, keep: bool = True):
+    """Keep the equilibrated flux of the next 2+1D estimates on the device for flux_samples
+    (the reference's flux reconstruction keeps its patch fluxes for
+    sigma_and_div_sigma_on_slab_cell, time_slab_equilibrated_flux_reconstruction.hpp:1317-1341)."""
+    blocks.ctx.check(blocks.ctx.lib.apf_system_keep_flux(blocks.ctx.handle, blocks.handle, 1 if keep else 0))
+
+
+def flux_cells(blocks: MainSystemBlocks) -> tuple[np.ndarray, np.ndarray]:
+    """(slab, source Y cell index) of every cell the kept flux lives on."""
+    ctx = blocks.ctx
+    n = C.c_int32()
+    ctx.check(ctx.lib.apf_flux_cells(ctx.handle, blocks.handle, C.byref(n), None, None))
+    slab = np.empty(n.value, dtype=np.int32)
+    src = np.empty(n.value, dtype=np.int32)
+    ctx.check(ctx.lib.apf_flux_cells(ctx.handle, blocks.handle, C.byref(n), _ptr(slab), _ptr(src)))
+    return slab, src
+
+
+def flux_samples(blocks: MainSystemBlocks, cells: np.ndarray, points: np.ndarray) -> np.ndarray:
+    """[n, 3] = (sigma_x, sigma_y, div sigma) of the kept flux at physical points [n, 3] (x, y, t),
+    point i on kept cell cells[i] (sigma_and_div_sigma_on_slab_cell)."""
+    c = np.ascontiguousarray(cells, dtype=np.int32)
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    if pts.shape[0] != c.size:
+        raise ValueError("one cell per point")
+    out = np.empty((c.size, 3))
+    blocks.ctx.check(blocks.ctx.lib.apf_flux_sample(blocks.ctx.handle, blocks.handle, c.size, _ptr(c), _ptr(pts),
+                                                    _ptr(out), 0))
+    return out
+
+
 def x_marking_indicator_components(blocks: MainSystemBlocks):
     """The adaptive driver's X-marking indicators on the last solve, mirroring
     ``adaptive_algorithm::detail::compute_x_marking_indicator_components``

@@ -353,6 +353,23 @@ const char* apf_ctx_autotune_report(apf_ctx* ctx);
 int apf_estimate(apf_ctx* ctx, apf_system* sys, const int32_t* y_vertex_ids, int pointers_on_device,
                  double* flux_squared, double* divergence_squared, double* reconstruction_squared,
                  double* eta_squared, apf_estimator_result* result);
+/* Keep (keep = 1) the equilibrated flux of the following 2+1D apf_estimate calls on the device
+ * for apf_flux_sample, or drop it (0).  The reference's TimeSlabEquilibratedFluxReconstruction
+ * keeps its patch fluxes for sigma_and_div_sigma_on_slab_cell
+ * (src/finite_element/time_slabs/time_slab_equilibrated_flux_reconstruction.hpp:1317-1341),
+ * which its snapshot writer samples
+ * (src/finite_element/io/write_time_slab_flux_reconstruction_samples_binary.hpp:17-174). */
+int apf_system_keep_flux(apf_ctx* ctx, apf_system* sys, int keep);
+/* The cells the kept flux lives on (the Y cells, or the slab cells they are cut into when Y
+ * cells span several time slabs): their count, and per cell its time slab (slabs in time
+ * order) and source Y cell (index in the system's Y cell order).  slab / source_y_cell may be
+ * NULL (count only). */
+int apf_flux_cells(apf_ctx* ctx, const apf_system* sys, int32_t* n_cells, int32_t* slab, int32_t* source_y_cell);
+/* sigma_x, sigma_y, div sigma (values: n_points x 3) of the kept flux at physical points
+ * (points: n_points x 3 as x, y, t), point i on kept cell cell[i]: the sum of the cell's
+ * vertex-patch fluxes, as sigma_and_div_sigma_on_slab_cell evaluates it. */
+int apf_flux_sample(apf_ctx* ctx, apf_system* sys, int32_t n_points, const int32_t* cell, const double* points,
+                    double* values, int pointers_on_device);
 
 /* ---- X-marking indicators -------------------------------------------------------- */
 /* Totals of XMarkingIndicatorComponents (algorithm/adaptive_result.hpp:294-320). */

@@ -59,12 +59,14 @@
 #include <concepts>
 #include <cstdint>
 #include <cstdlib>
+#include <filesystem>
 #include <limits>
 #include <memory>
 #include <optional>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -230,6 +232,13 @@ namespace la::b200
         [[nodiscard]] long long device_estimates() const noexcept { return estimates_; }
         void count_estimate() noexcept { ++estimates_; }
 
+        // whether la::b200::estimate keeps the flux on the device (default on) for the
+        // snapshot writer (flux_reconstruction_samples.bin); the Y cell ids of that estimate in
+        // the system's order
+        void set_keep_flux(bool keep) noexcept { keep_flux_ = keep; }
+        [[nodiscard]] bool keep_flux() const noexcept { return keep_flux_; }
+        [[nodiscard]] std::vector<int>& flux_y_cells() noexcept { return flux_y_cells_; }
+
     private:
         int device_ = -1;
         apf_ctx* ctx_ = nullptr;
@@ -238,6 +247,8 @@ namespace la::b200
         apf_solver_options options_{};
         apf_solver_diagnostics last_diag_{};
         long long estimates_ = 0;
+        bool keep_flux_ = true;
+        std::vector<int> flux_y_cells_;
         std::vector<Probe> probes_;
     };
 
@@ -520,9 +531,12 @@ namespace la::b200
         }
         std::vector<double> flux(ny), div(ny), recon(ny), eta(ny);
         apf_estimator_result res{};
+        if constexpr (dim == 2)
+            check(ctx, apf_system_keep_flux(ctx, sys, s.keep_flux() ? 1 : 0), "apf_system_keep_flux");
         check(ctx, apf_estimate(ctx, sys, dim == 2 ? vids.data() : nullptr, 0, flux.data(), div.data(), recon.data(),
                                 eta.data(), &res),
               "apf_estimate");
+        s.flux_y_cells() = dim == 2 && s.keep_flux() ? cells : std::vector<int>{};
         DeviceEstimate out;
         for (std::size_t k = 0; k < ny; ++k)
         {
@@ -766,6 +780,9 @@ namespace la::preconditioners
 // to them; the reference's adaptive driver (algorithm/adaptive_driver.hpp), included after
 // this header, binds to the overload below.
 #include "finite_element/time_slabs/time_slab_adaptive_loop.hpp"
+#include "finite_element/geometry/cell_geometry.hpp"
+#include "finite_element/io/write_time_slab_flux_reconstruction_samples_binary.hpp"
+#include "finite_element/io/write_time_slab_vertex_patches_binary.hpp"
 
 namespace la::b200::detail
 {
@@ -901,6 +918,135 @@ namespace la::b200::detail
             u_h.update_from_true_solution(result.u_true);
         }
         return result;
+    }
+}
+
+namespace la::b200
+{
+    // write_time_slab_flux_reconstruction_samples_binary
+    // (src/finite_element/io/write_time_slab_flux_reconstruction_samples_binary.hpp:17-174) from
+    // the device flux of this thread's last estimate: the reference's file layout and sample
+    // lattice, slab cells in the order of the reference's slab space (the host reconstruction's
+    // slab_space_ref(), which the driver builds), sample points mapped by the reference's
+    // CellGeometry, and sigma_x, sigma_y, div sigma evaluated on the device (apf_flux_sample)
+    // on the device cell with the same (slab, source Y cell).
+    template<class FluxReconstructionType>
+    void write_flux_reconstruction_samples_binary(const FluxReconstructionType& reconstruction,
+                                                  const std::filesystem::path& output_dir,
+                                                  const std::string& filename = "flux_reconstruction_samples.bin",
+                                                  int samples_x_per_cell = 4, int samples_t_per_cell = 4)
+    {
+        using SlabSpaceType = typename FluxReconstructionType::SlabSpaceType;
+        using GT = typename SlabSpaceType::GT;
+        using int_t = finite_element::io::detail::binary_int_t;
+        namespace iod = finite_element::io::detail;
+        static_assert(GT::dim_space_v == 2 && GT::dim_time_v == 1, "flux samples: 2+1D reconstructions");
+        if (samples_x_per_cell < 2 || samples_t_per_cell < 2)
+            throw std::runtime_error(
+                "write_time_slab_flux_reconstruction_samples_binary: need at least 2 samples per direction.");
+        Session& s = session();
+        apf_ctx* ctx = s.context();
+        apf_system* sys = s.system();
+        const std::vector<int>& y_cells = s.flux_y_cells();
+        int32_t n_kept = 0;
+        if (sys != nullptr)
+            check(ctx, apf_flux_cells(ctx, sys, &n_kept, nullptr, nullptr), "apf_flux_cells");
+        if (sys == nullptr || n_kept == 0 || y_cells.empty())
+            throw std::runtime_error("b200 backend: no device flux for the flux samples (the session's last estimate "
+                                     "did not keep one: la::b200::session().keep_flux())");
+        std::vector<int32_t> kept_slab(static_cast<std::size_t>(n_kept)), kept_source(static_cast<std::size_t>(n_kept));
+        check(ctx, apf_flux_cells(ctx, sys, &n_kept, kept_slab.data(), kept_source.data()), "apf_flux_cells");
+        auto key = [](long long slab, long long y_cell) { return (slab << 32) | (y_cell & 0xffffffffll); };
+        std::unordered_map<long long, int32_t> device_cell;
+        device_cell.reserve(static_cast<std::size_t>(n_kept));
+        for (int32_t c = 0; c < n_kept; ++c)
+            device_cell.emplace(key(kept_slab[static_cast<std::size_t>(c)],
+                                    y_cells.at(static_cast<std::size_t>(kept_source[static_cast<std::size_t>(c)]))),
+                                c);
+
+        const auto& slab_space = reconstruction.slab_space_ref();
+        const int nx = samples_x_per_cell, nt = samples_t_per_cell;
+        const int n_spatial = nx * (nx + 1) / 2;
+        const auto ref_space = iod::make_triangle_barycentric_lattice_samples(nx);
+        const auto ref_time = iod::make_interval_reference_samples(nt);
+        std::vector<int_t> slab_ids, slab_cell_ids, source_ids;
+        std::vector<int32_t> point_cell;
+        std::vector<double> points;
+        for (int slab_id = 0; slab_id < slab_space.n_slabs(); ++slab_id)
+        {
+            const auto& slab = slab_space.slab(slab_id);
+            const auto& fes = slab.fespace_ref();
+            using Geometry = finite_element::geometry::CellGeometry<std::remove_cvref_t<decltype(fes)>, 2>;
+            for (const int slab_cell : slab.active_cells())
+            {
+                const int source = slab_space.source_cell_id(slab_id, slab_cell);
+                const auto it = device_cell.find(key(slab_id, source));
+                if (it == device_cell.end())
+                    throw std::runtime_error("b200 backend: slab " + std::to_string(slab_id) + " cell of source Y cell " +
+                                             std::to_string(source) + " has no device flux (the estimate's slabs "
+                                             "differ from the reconstruction's)");
+                slab_ids.push_back(static_cast<int_t>(slab_id));
+                slab_cell_ids.push_back(static_cast<int_t>(slab_cell));
+                source_ids.push_back(static_cast<int_t>(source));
+                const auto geom = Geometry::make(fes, slab_cell);
+                for (int jt = 0; jt < nt; ++jt)
+                    for (int is = 0; is < n_spatial; ++is)
+                    {
+                        const auto p = Geometry::map_to_physical(
+                            geom, {ref_space[2 * static_cast<std::size_t>(is)],
+                                   ref_space[2 * static_cast<std::size_t>(is) + 1], ref_time[static_cast<std::size_t>(jt)]});
+                        points.insert(points.end(), {p[0], p[1], p[2]});
+                        point_cell.push_back(it->second);
+                    }
+            }
+        }
+        std::vector<double> values(points.size());
+        check(ctx, apf_flux_sample(ctx, sys, static_cast<int32_t>(point_cell.size()), point_cell.data(), points.data(),
+                                   values.data(), 0),
+              "apf_flux_sample");
+
+        auto file = iod::open_binary_output(output_dir, filename, "write_time_slab_flux_reconstruction_samples_binary");
+        const auto header = iod::make_versioned_header(
+            iod::time_slab_flux_reconstruction_samples_binary_format_version, static_cast<int_t>(slab_space.n_slabs()),
+            static_cast<int_t>(slab_ids.size()), static_cast<int_t>(GT::dim_space_v),
+            static_cast<int_t>(GT::dim_time_v), static_cast<int_t>(nx), static_cast<int_t>(nt),
+            static_cast<int_t>(n_spatial), static_cast<int_t>(n_spatial * nt), static_cast<int_t>(3),
+            iod::function_sample_layout_triangle_barycentric_time);
+        const char* what = "write_time_slab_flux_reconstruction_samples_binary";
+        iod::write_binary_block(file, header, what);
+        iod::write_binary_block(file, slab_ids, what);
+        iod::write_binary_block(file, slab_cell_ids, what);
+        iod::write_binary_block(file, source_ids, what);
+        iod::write_binary_block(file, ref_space, what);
+        iod::write_binary_block(file, ref_time, what);
+        iod::write_binary_block(file, values, what);
+    }
+}
+
+namespace adaptive_algorithm::output::detail
+{
+    // The driver's time-slab estimator snapshot (algorithm/output/iteration_snapshot_writer.hpp:
+    // 143-170) for a b200 iteration state: the vertex patches by the reference's writer (host
+    // topology, which the drop-in's inner iteration builds), the flux samples from the device
+    // flux (its host reconstruction holds no patch solutions).  More specialised than the
+    // reference's template, so the driver's call binds here for la::b200::Backend only.
+    template<class XSpaceType, class YSpaceType>
+    void write_time_slab_estimator_diagnostics_snapshot(
+        const finite_element::time_slabs::AdaptiveTestSpaceIterationState<la::b200::Backend, XSpaceType, YSpaceType>&
+            state,
+        const std::filesystem::path& output_dir)
+    {
+        using GT = typename YSpaceType::GT;
+        if constexpr (GT::dim_space_v == 2 && GT::dim_time_v == 1)
+        {
+            if (!state.flux_reconstruction.has_value())
+                return;
+            std::filesystem::create_directories(output_dir);
+            finite_element::io::write_time_slab_vertex_patches_binary(state.flux_reconstruction->patch_set(), output_dir,
+                                                                     "time_slab_vertex_patches.bin");
+            la::b200::write_flux_reconstruction_samples_binary(*state.flux_reconstruction, output_dir,
+                                                               "flux_reconstruction_samples.bin", 4, 4);
+        }
     }
 }
 

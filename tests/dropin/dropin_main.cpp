@@ -27,6 +27,11 @@
 //       the reference's types (la::b200::estimate) on the b200 solve against the reference's
 //       host estimate on its direct solve -- per-cell flux^2 / recon^2 / eta^2, totals, slab
 //       count and the Doerfler marking of each;
+//   snapshot <p> <levels> <example> <tol> <outdir>
+//       after one pass of the reference's inner loop (Y finer than X): the driver's time-slab
+//       estimator snapshot (algorithm/output/iteration_snapshot_writer.hpp:143-170) of the
+//       Eigen backend's iteration state into <outdir>/eigen and of the b200 state (flux
+//       samples from the device flux) into <outdir>/b200;
 //   adaptive <p> <levels> <example> <outer_cycles> <tol> [compare:1|0] [guess:0|1|2]
 //       the reference's whole adaptive algorithm (adaptive_algorithm::run_adaptive_driver,
 //       algorithm/adaptive_driver.hpp:3508) with each backend, each on its own spaces: per outer
@@ -422,6 +427,45 @@ namespace
         return 0;
     }
 
+    // the driver's time-slab estimator snapshot after one pass of the inner loop (Y finer than
+    // X): the reference's writer on the Eigen backend's state (host patch solves) into
+    // <outdir>/eigen, the b200 overload (device flux) into <outdir>/b200, each on its own copy
+    // of the same spaces
+    template<class S>
+    int run_snapshot(int levels, const std::string& name, double tol, const std::string& outdir)
+    {
+        using XSpace = typename S::XSpace;
+        using YSpace = typename S::YSpace;
+        S a(name, levels), b(name, levels);
+        la::concepts::SolverOptions lu;
+        lu.solver = la::concepts::SolverType::SparseLU;
+        finite_element::time_slabs::AdaptiveTestSpaceIterationParameters<EigenB, XSpace, YSpace> pb;
+        {
+            typename EigenB::Solver s0;
+            const auto st0 = finite_element::time_slabs::compute_adaptive_test_space_iteration<S::QSpace, S::QTime,
+                                                                                               EigenB>(
+                b.y_space, b.x_space, b.example.problem, s0, lu, pb);
+            finite_element::time_slabs::refine_test_space_from_marked_source_cells(a.y_space, a.x_space,
+                                                                                   st0.marked_source_cells);
+            finite_element::time_slabs::refine_test_space_from_marked_source_cells(b.y_space, b.x_space,
+                                                                                   st0.marked_source_cells);
+        }
+        typename EigenB::Solver sb;
+        const auto ref = finite_element::time_slabs::compute_adaptive_test_space_iteration<S::QSpace, S::QTime, EigenB>(
+            b.y_space, b.x_space, b.example.problem, sb, lu, pb);
+        finite_element::time_slabs::AdaptiveTestSpaceIterationParameters<B200, XSpace, YSpace> pa;
+        typename B200::Solver sa;
+        const auto dev = finite_element::time_slabs::compute_adaptive_test_space_iteration<S::QSpace, S::QTime, B200>(
+            a.y_space, a.x_space, a.example.problem, sa, minres_options(tol), pa);
+        adaptive_algorithm::output::detail::write_time_slab_estimator_diagnostics_snapshot(ref, outdir + "/eigen");
+        adaptive_algorithm::output::detail::write_time_slab_estimator_diagnostics_snapshot(dev, outdir + "/b200");
+        std::printf("{\"mode\": \"snapshot\", \"p\": %d, \"levels\": %d, \"y_cells\": %zu, \"x_cells\": %zu, "
+                    "\"n_slabs\": [%d, %d], \"device_estimates\": %lld}\n",
+                    S::P_, levels, a.y_space.active_cells().size(), a.x_space.active_cells().size(), dev.n_slabs(),
+                    ref.n_slabs(), la::b200::session().device_estimates());
+        return 0;
+    }
+
     // the reference's whole adaptive algorithm (run_adaptive_driver, algorithm/adaptive_driver.hpp:3508)
     // with each backend: outer cycles of inner Y loops (solve, estimate, Doerfler marking, Y
     // refinement) and X marking + refinement
@@ -519,6 +563,9 @@ namespace
             return run_cycle<S>(levels, example, std::atoi(argv[5]), std::atof(argv[6]));
         if (mode == "estimate" && argc >= 6)
             return run_estimate<S>(levels, example, std::atof(argv[5]));
+        if constexpr (S::GT::dim_space_v == 2)
+            if (mode == "snapshot" && argc >= 7)
+                return run_snapshot<S>(levels, example, std::atof(argv[5]), argv[6]);
         return 2;
     }
 

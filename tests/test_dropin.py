@@ -17,6 +17,7 @@ import json
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -173,6 +174,56 @@ def test_dropin_device_estimate_matches_reference_estimator(p, levels, env):
     assert abs(ea - eb) <= 1e-10 * eb and abs(fa - fb) <= 1e-10 * fb, d
     assert rb > 0 and abs(ra - rb) <= 1e-8 * rb, d
     assert d["marked"][1] > 0 and d["marked_symmetric_difference"] <= max(2, d["marked"][1] // 50), d
+
+
+def _flux_samples(path):
+    """flux_reconstruction_samples.bin (write_time_slab_flux_reconstruction_samples_binary.hpp:
+    int32 header of 11, int32 slab / slab-cell / source ids, reference lattice, time samples,
+    then [cell][sample][sigma_x, sigma_y, div sigma])."""
+    raw = open(path, "rb").read()
+    h = np.frombuffer(raw[:44], dtype=np.int32)
+    n_cells, nt, nsp, per_cell = int(h[2]), int(h[6]), int(h[7]), int(h[8])
+    off = 44
+    ids = np.frombuffer(raw[off:off + 12 * n_cells], dtype=np.int32).reshape(3, n_cells)
+    off += 12 * n_cells
+    lattice = np.frombuffer(raw[off:off + 16 * nsp], dtype=np.float64)
+    off += 16 * nsp
+    times = np.frombuffer(raw[off:off + 8 * nt], dtype=np.float64)
+    off += 8 * nt
+    values = np.frombuffer(raw[off:], dtype=np.float64)
+    assert values.size == n_cells * per_cell * 3
+    return h, ids, lattice, times, values.reshape(n_cells, per_cell, 3)
+
+
+@needs_program
+@pytest.mark.gpu
+@pytest.mark.parametrize("p,levels,env", [
+    (1, 2, ADAPTIVE_ENV),
+    (2, 1, {"APF_REF_X_POINTS": "0.3,0.6,0.4", "APF_REF_X_ROUNDS": "1", "APF_REF_KAPPA": "5:0.1:10"})],
+    ids=["p1", "p2"])
+def test_dropin_snapshot_flux_samples_match_reference_writer(p, levels, env, tmp_path):
+    """The driver's time-slab estimator snapshot for a b200 iteration state (the overload of
+    write_time_slab_estimator_diagnostics_snapshot: vertex patches by the reference's writer,
+    flux samples from the device flux through apf_flux_sample) against the reference's own
+    writer on the Eigen backend's state (host patch solves on its direct solve), after one
+    pass of the inner loop so that Y cells span several slabs: the same header, slab / slab-cell
+    / source ids and lattice, sigma_x, sigma_y and div sigma within 1e-8 of each component's
+    largest magnitude, and byte-identical vertex-patch files."""
+    d = _json(_run(["snapshot", p, levels, "smooth_initial", 1e-12, str(tmp_path)], env=env))
+    assert d["y_cells"] > d["x_cells"] and d["n_slabs"][0] == d["n_slabs"][1] > 1, d
+    ha, ia, la, ta, va = _flux_samples(tmp_path / "b200" / "flux_reconstruction_samples.bin")
+    hb, ib, lb, tb, vb = _flux_samples(tmp_path / "eigen" / "flux_reconstruction_samples.bin")
+    assert np.array_equal(ha, hb) and np.array_equal(ia, ib), (ha, hb)
+    assert np.array_equal(la, lb) and np.array_equal(ta, tb)
+    assert ha[2] > d["y_cells"]  # slab cells: Y cells cut at the slab times
+    for comp in range(3):
+        scale = np.abs(vb[..., comp]).max()
+        assert scale > 0
+        err = np.abs(va[..., comp] - vb[..., comp]).max() / scale
+        assert err <= 1e-8, (comp, err)
+    pa = (tmp_path / "b200" / "time_slab_vertex_patches.bin").read_bytes()
+    pb = (tmp_path / "eigen" / "time_slab_vertex_patches.bin").read_bytes()
+    assert len(pa) > 0 and pa == pb
 
 
 @needs_program

@@ -194,3 +194,64 @@ def test_cellwise_error_artifacts_from_device_estimate(gpu_ctx, name, tmp_path):
     a, b = np.argsort(my_ids), np.argsort(ref_ids)
     assert np.abs(my_eta[a] - ref_eta[b]).max() <= 1e-9 * np.abs(ref_eta).max()
     assert np.all(np.diff(my_eta) <= 0.0)
+
+
+@pytest.mark.parametrize("level,p", [(3, 1), (2, 2)])
+def test_flux_samples_divergence_and_normal_continuity(gpu_ctx, level, p):
+    """apf_flux_sample on the flux kept by the estimate (a uniform mesh: the estimator cells are
+    the Y cells, one slab per time layer): central differences of the sampled sigma reproduce
+    the sampled div sigma (exact for RT_1's quadratic components, O(h^2) for RT_2), and the
+    normal component of sigma agrees on both sides of every interior edge of a slab (the summed
+    patch fluxes are H(div)-conforming, as the reference's sigma_and_div_sigma_on_slab_cell
+    sums them)."""
+    from doubleadapparabolicfem_b200.estimator import estimate, flux_cells, flux_samples, keep_flux
+    from doubleadapparabolicfem_b200.mesh import uniform_problem
+    from doubleadapparabolicfem_b200.assembly import assemble_main_system_blocks
+    from doubleadapparabolicfem_b200.solver import SolverOptions, solve_saddle_system_with_preconditioner
+    prob = uniform_problem(level, p)
+    blocks = assemble_main_system_blocks(prob, ctx=gpu_ctx)
+    blocks.assemble_parabolic_graph_norm_approximation()
+    solve_saddle_system_with_preconditioner(blocks, SolverOptions(tolerance=1e-10), copy_out=False)
+    keep_flux(blocks)
+    estimate(blocks)
+    slab, src = flux_cells(blocks)
+    geo = prob.y_geometry
+    n = geo.shape[0]
+    assert slab.size == n and np.array_equal(src, np.arange(n))
+    t0 = geo[:, 6]
+    levels = np.unique(t0)
+    assert np.array_equal(slab, np.searchsorted(levels, t0))
+    xy = geo[:, :6].reshape(n, 3, 2)
+    centre = xy.mean(axis=1)
+    tm = 0.5 * (geo[:, 6] + geo[:, 7])
+    h = 1e-4 * np.linalg.norm(xy[:, 1] - xy[:, 0], axis=1)
+    cells = np.arange(n, dtype=np.int32)
+    pts = [np.column_stack([centre[:, 0] + dx * h, centre[:, 1] + dy * h, tm])
+           for dx, dy in ((0, 0), (1, 0), (-1, 0), (0, 1), (0, -1))]
+    v = [flux_samples(blocks, cells, q) for q in pts]
+    div_fd = (v[1][:, 0] - v[2][:, 0]) / (2 * h) + (v[3][:, 1] - v[4][:, 1]) / (2 * h)
+    scale_div = np.abs(v[0][:, 2]).max()
+    assert scale_div > 0
+    assert np.abs(div_fd - v[0][:, 2]).max() <= 1e-6 * scale_div
+    # interior edges of each slab: the two cells sharing (vertex pair, time layer)
+    vids = prob.y_vertex_ids
+    edges = {}
+    for c in range(n):
+        for k in range(3):
+            a, b = int(vids[c, (k + 1) % 3]), int(vids[c, (k + 2) % 3])
+            edges.setdefault((min(a, b), max(a, b), t0[c]), []).append((c, (k + 1) % 3, (k + 2) % 3))
+    pairs = [e for e in edges.values() if len(e) == 2]
+    assert len(pairs) > n // 2
+    ca = np.array([e[0][0] for e in pairs], dtype=np.int32)
+    cb = np.array([e[1][0] for e in pairs], dtype=np.int32)
+    pa = np.array([xy[e[0][0], e[0][1]] for e in pairs])
+    pb = np.array([xy[e[0][0], e[0][2]] for e in pairs])
+    normal = np.column_stack([pb[:, 1] - pa[:, 1], pa[:, 0] - pb[:, 0]])
+    scale_s = np.abs(v[0][:, :2]).max()
+    for frac, tau in ((0.5, 0.5), (0.25, 0.8), (0.9, 0.1)):
+        q = pa + frac * (pb - pa)
+        t = geo[ca, 6] + tau * (geo[ca, 7] - geo[ca, 6])
+        sa = flux_samples(blocks, ca, np.column_stack([q, t]))
+        sb = flux_samples(blocks, cb, np.column_stack([q, t]))
+        jump = np.abs(((sa[:, :2] - sb[:, :2]) * normal).sum(axis=1)) / np.linalg.norm(normal, axis=1)
+        assert jump.max() <= 1e-9 * scale_s, jump.max() / scale_s
