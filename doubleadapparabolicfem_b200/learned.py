@@ -49,6 +49,13 @@ ALPHA = B3 + OUTPUTS
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "learned_precond.npz")
 
 
+def raw_params_path(npz_path: str):
+    """The raw float32 copy of a saved model's parameters."""
+    import pathlib
+    p = pathlib.Path(npz_path)
+    return p.with_name(p.name[:-4] + ".params.f32" if p.name.endswith(".npz") else p.name + ".params.f32")
+
+
 class LearnedModel:
     """Parameters of the learned smoother model (host copy + library handle)."""
 
@@ -82,8 +89,12 @@ class LearnedModel:
         return LearnedModel(p)
 
     def save(self, path: str, **meta):
+        """The model as an npz (parameters and training metadata) and, beside it, the
+        parameters alone as raw little-endian float32 (<path without .npz>.params.f32) for
+        C and C++ callers (la::b200::Session::use_learned_model)."""
         os.makedirs(os.path.dirname(path), exist_ok=True)
         np.savez(path, params=self.params, **{k: np.asarray(v) for k, v in meta.items()})
+        raw_params_path(path).write_bytes(np.asarray(self.params, dtype="<f4").tobytes())
 
     @staticmethod
     def load(path: str = DEFAULT_WEIGHTS) -> "LearnedModel":

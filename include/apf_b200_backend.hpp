@@ -60,6 +60,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <filesystem>
+#include <fstream>
 #include <limits>
 #include <memory>
 #include <optional>
@@ -154,6 +155,8 @@ namespace la::b200
             release();
             if (ctx_ != nullptr)
                 apf_ctx_destroy(ctx_);
+            if (model_ != nullptr)
+                apf_learned_model_destroy(model_);
         }
 
         // CUDA device of the context (before its first use; default: APF_B200_DEVICE or 0)
@@ -182,6 +185,28 @@ namespace la::b200
         // preconditioner kind and AMG parameters of the solves (tolerance, iteration limit
         // and batching come from the reference's SolverOptions of each solve)
         [[nodiscard]] apf_solver_options& solver_options() noexcept { return options_; }
+
+        // the learned preconditioner for the following solves, with the plain block
+        // preconditioner as its fallback (a learned run that misses the tolerance is rerun from
+        // its iterate): the model's APF_LEARNED_NUM_PARAMS float32 parameters, raw
+        // little-endian, as the Python package ships them
+        // (doubleadapparabolicfem_b200/data/learned_precond.params.f32)
+        void use_learned_model(const std::string& params_path)
+        {
+            std::ifstream f(params_path, std::ios::binary);
+            std::vector<float> p(APF_LEARNED_NUM_PARAMS);
+            if (!f.read(reinterpret_cast<char*>(p.data()), static_cast<std::streamsize>(p.size() * sizeof(float))) ||
+                f.peek() != std::ifstream::traits_type::eof())
+                throw std::runtime_error("b200 backend: " + params_path + " is not " +
+                                         std::to_string(APF_LEARNED_NUM_PARAMS) + " float32 parameters");
+            apf_ctx* ctx = context();
+            if (model_ == nullptr)
+                check(ctx, apf_learned_model_create(&model_), "apf_learned_model_create");
+            check(ctx, apf_learned_model_set_params(model_, p.data(), APF_LEARNED_NUM_PARAMS),
+                  "apf_learned_model_set_params");
+            check(ctx, apf_ctx_set_learned_model(ctx, model_), "apf_ctx_set_learned_model");
+            options_.preconditioner = APF_PRECOND_LEARNED;
+        }
 
         [[nodiscard]] apf_system* system() const noexcept { return sys_; }
         [[nodiscard]] double zero_tol() const noexcept { return zero_tol_; }
@@ -226,7 +251,15 @@ namespace la::b200
             return any ? sys_ : nullptr;
         }
 
-        void set_last_diagnostics(const apf_solver_diagnostics& d) noexcept { last_diag_ = d; }
+        void set_last_diagnostics(const apf_solver_diagnostics& d) noexcept
+        {
+            last_diag_ = d;
+            ++solves_;
+            learned_fallbacks_ += d.learned_fallback != 0;
+        }
+        // device MINRES solves in this thread, and those whose learned run fell back to plain
+        [[nodiscard]] long long device_solves() const noexcept { return solves_; }
+        [[nodiscard]] long long learned_fallbacks() const noexcept { return learned_fallbacks_; }
 
         // estimates run through la::b200::estimate in this thread
         [[nodiscard]] long long device_estimates() const noexcept { return estimates_; }
@@ -242,11 +275,12 @@ namespace la::b200
     private:
         int device_ = -1;
         apf_ctx* ctx_ = nullptr;
+        apf_learned_model* model_ = nullptr;
         apf_system* sys_ = nullptr;
         double zero_tol_ = 1e-15;
         apf_solver_options options_{};
         apf_solver_diagnostics last_diag_{};
-        long long estimates_ = 0;
+        long long estimates_ = 0, solves_ = 0, learned_fallbacks_ = 0;
         bool keep_flux_ = true;
         std::vector<int> flux_y_cells_;
         std::vector<Probe> probes_;

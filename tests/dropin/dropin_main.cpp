@@ -487,6 +487,9 @@ namespace
         par.timing.enabled = !compare; // the driver's own phase timing for the b200-only run
         if (const char* e = std::getenv("APF_DROPIN_AMG_STRENGTH"))
             la::b200::session().solver_options().amg_strength = std::atof(e);
+        // the learned preconditioner (plain fallback) from the shipped raw parameters
+        if (const char* e = std::getenv("APF_DROPIN_LEARNED_PARAMS"))
+            la::b200::session().use_learned_model(e);
         const auto t0 = std::chrono::steady_clock::now();
         typename B200::Solver sa;
         const auto ra = adaptive_algorithm::run_adaptive_driver<S::QSpace, S::QTime, B200>(
@@ -543,9 +546,11 @@ namespace
         phases += "]";
         std::fprintf(stderr, "driver phases (total s): %s\n", phases.c_str());
         std::printf("{\"mode\": \"adaptive\", \"p\": %d, \"levels\": %d, \"tol\": %.1e, \"b200_s\": %.3f, "
-                    "\"direct_s\": %.3f, \"device_estimates\": %lld, \"b200\": %s, \"direct\": %s}\n",
+                    "\"direct_s\": %.3f, \"device_estimates\": %lld, \"device_solves\": %lld, "
+                    "\"learned_fallbacks\": %lld, \"b200\": %s, \"direct\": %s}\n",
                     P, levels, tol, std::chrono::duration<double>(t1 - t0).count(),
-                    std::chrono::duration<double>(t2 - t1).count(), la::b200::session().device_estimates(),
+                    std::chrono::duration<double>(t2 - t1).count(), la::b200::session().device_estimates(), la::b200::session().device_solves(),
+                    la::b200::session().learned_fallbacks(),
                     dump(ra).c_str(), dump(rb).c_str());
         return 0;
     }

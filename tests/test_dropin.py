@@ -153,6 +153,26 @@ def test_dropin_reference_adaptive_driver_matches_eigen_backend(guess):
 
 @needs_program
 @pytest.mark.gpu
+def test_dropin_adaptive_driver_with_learned_preconditioner():
+    """The same three-cycle driver comparison with the learned preconditioner loaded from the
+    shipped raw parameters (la::b200::Session::use_learned_model; the plain block
+    preconditioner as its fallback): the same trajectory as the Eigen backend's direct solves,
+    totals to 1e-8, every solve on the device."""
+    params = os.path.join(os.path.dirname(HERE), "doubleadapparabolicfem_b200", "data", "learned_precond.params.f32")
+    d = _json(_run(["adaptive", 1, 1, "smooth_initial", 3, 1e-12, 1, 0],
+                   env={"APF_REF_KAPPA": "11:0.1:10", "APF_REF_KAPPA_BLOCKS": "4",
+                        "APF_DROPIN_LEARNED_PARAMS": params}))
+    a, b = d["b200"], d["direct"]
+    assert len(a) == len(b) == 3
+    for ra, rb in zip(a, b):
+        assert (ra["x_dofs"], ra["y_dofs"], ra["inner"]) == (rb["x_dofs"], rb["y_dofs"], rb["inner"]), (ra, rb)
+        for key in ("eta_squared", "lambda_y_squared", "y_estimator_squared"):
+            assert abs(ra[key] - rb[key]) <= 1e-8 * abs(rb[key]), (key, ra, rb)
+    assert d["device_solves"] >= sum(r["inner"] for r in a)
+
+
+@needs_program
+@pytest.mark.gpu
 @pytest.mark.parametrize("p,levels,env", [
     (1, 2, ADAPTIVE_ENV),
     (2, 1, {"APF_REF_X_POINTS": "0.3,0.6,0.4", "APF_REF_X_ROUNDS": "1", "APF_REF_KAPPA": "5:0.1:10"})],

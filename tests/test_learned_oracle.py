@@ -24,3 +24,13 @@ def test_fp64_gradient_matches_central_differences():
     assert np.abs(grad[idx] - fd).max() <= 1e-7 * np.abs(fd).max()
     # parameters the loss does not see (the second block's coarse scales) get zero
     assert np.all(grad[O.ALPHA + O.MAX_LEVELS:] == 0.0)
+
+
+def test_shipped_raw_parameters_match_the_npz():
+    """The raw float32 copy of the shipped model (read by the C++ drop-in's
+    Session::use_learned_model) holds exactly the npz's parameters."""
+    from doubleadapparabolicfem_b200.learned import DEFAULT_WEIGHTS, raw_params_path
+    with np.load(DEFAULT_WEIGHTS) as z:
+        params = np.asarray(z["params"], dtype="<f4")
+    raw = np.frombuffer(raw_params_path(DEFAULT_WEIGHTS).read_bytes(), dtype="<f4")
+    assert raw.size == 1442 and np.array_equal(raw, params)
