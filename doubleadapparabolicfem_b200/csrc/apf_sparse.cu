@@ -89,7 +89,12 @@ namespace apf
         // latency-bound and warps in flight set its bandwidth; the few spilled values live
         // in L1.  Measured at outer level 6 against 40 registers and six blocks: K SpMV 0.86
         // -> 0.94 of the HBM copy bandwidth, finest-level sweeps 0.59 -> 0.64; a variant
-        // with two accumulators and no spills lost both gains.
+        // with two accumulators and no spills lost both gains.  The f32 operators (the
+        // V-cycle levels) use the paired layout of sell_fill: each load request carries two
+        // entries (8 bytes), as the f64 operator's values do; with the group loop kept
+        // rolled that took the finest-level sweeps from 0.68 to 0.80 of the copy bandwidth
+        // on the locally refined workload (the scalar layout: 68-72 bytes of spills, the
+        // paired one 24-28).
         template<int MODE, class V>
         __global__ void __launch_bounds__(256, 8) sell_kernel(int rows, int slices, const int* __restrict__ sp,
                                                            const int* __restrict__ col, const V* __restrict__ val,
@@ -121,20 +126,50 @@ namespace apf
                 // through once (evict-first loads), x stays cached for the gathers
                 double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
                 int j = 0;
-                for (; j + 3 < width; j += 4)
+                if constexpr (std::is_same_v<V, float>)
                 {
-                    const int c0 = __ldcs(c + 32 * j), c1 = __ldcs(c + 32 * j + 32);
-                    const int c2 = __ldcs(c + 32 * j + 64), c3 = __ldcs(c + 32 * j + 96);
-                    const V v0 = __ldcs(v + 32 * j), v1 = __ldcs(v + 32 * j + 32);
-                    const V v2 = __ldcs(v + 32 * j + 64), v3 = __ldcs(v + 32 * j + 96);
-                    const double x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
-                    s0 += static_cast<double>(v0) * x0;
-                    s1 += static_cast<double>(v1) * x1;
-                    s2 += static_cast<double>(v2) * x2;
-                    s3 += static_cast<double>(v3) * x3;
+                    // paired f32 layout (even width): one 8-byte column load and one 8-byte
+                    // value load per two entries, twice the bytes per outstanding request of
+                    // the scalar layout at the same register count
+                    const int2* cp = reinterpret_cast<const int2*>(col + base) + lane;
+                    const float2* vp = reinterpret_cast<const float2*>(val + base) + lane;
+#pragma unroll 1
+                    for (; j + 3 < width; j += 4)
+                    {
+                        const int2 ca = __ldcs(cp + 16 * j), cb = __ldcs(cp + 16 * j + 32);
+                        const float2 va = __ldcs(vp + 16 * j), vb = __ldcs(vp + 16 * j + 32);
+                        const double x0 = __ldg(x + ca.x), x1 = __ldg(x + ca.y), x2 = __ldg(x + cb.x),
+                                     x3 = __ldg(x + cb.y);
+                        s0 += static_cast<double>(va.x) * x0;
+                        s1 += static_cast<double>(va.y) * x1;
+                        s2 += static_cast<double>(vb.x) * x2;
+                        s3 += static_cast<double>(vb.y) * x3;
+                    }
+                    if (j < width)
+                    {
+                        const int2 ca = __ldcs(cp + 16 * j);
+                        const float2 va = __ldcs(vp + 16 * j);
+                        s0 += static_cast<double>(va.x) * __ldg(x + ca.x);
+                        s0 += static_cast<double>(va.y) * __ldg(x + ca.y);
+                    }
                 }
-                for (; j < width; ++j)
-                    s0 += static_cast<double>(__ldcs(v + 32 * j)) * __ldg(x + __ldcs(c + 32 * j));
+                else
+                {
+                    for (; j + 3 < width; j += 4)
+                    {
+                        const int c0 = __ldcs(c + 32 * j), c1 = __ldcs(c + 32 * j + 32);
+                        const int c2 = __ldcs(c + 32 * j + 64), c3 = __ldcs(c + 32 * j + 96);
+                        const V v0 = __ldcs(v + 32 * j), v1 = __ldcs(v + 32 * j + 32);
+                        const V v2 = __ldcs(v + 32 * j + 64), v3 = __ldcs(v + 32 * j + 96);
+                        const double x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+                        s0 += static_cast<double>(v0) * x0;
+                        s1 += static_cast<double>(v1) * x1;
+                        s2 += static_cast<double>(v2) * x2;
+                        s3 += static_cast<double>(v3) * x3;
+                    }
+                    for (; j < width; ++j)
+                        s0 += static_cast<double>(__ldcs(v + 32 * j)) * __ldg(x + __ldcs(c + 32 * j));
+                }
                 const double sum = (s0 + s1) + (s2 + s3);
                 if (live)
                 {
@@ -200,8 +235,9 @@ namespace apf
                     perm[w0 + k] = w0 + static_cast<int>(key[k] & 0xffffffffu);
         }
 
+        // even = 1: widths rounded up to an even count (the paired f32 layout)
         __global__ void sell_count(int rows, int slices, const int* __restrict__ rp, const int* __restrict__ perm,
-                                   int* __restrict__ cnt)
+                                   int* __restrict__ cnt, int even)
         {
             const int lane = threadIdx.x & 31;
             const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -214,7 +250,7 @@ namespace apf
                 for (int o = 16; o > 0; o >>= 1)
                     len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
                 if (lane == 0)
-                    cnt[sl] = 32 * len;
+                    cnt[sl] = 32 * (even ? (len + 1) & ~1 : len);
             }
         }
 
@@ -236,7 +272,10 @@ namespace apf
                 const int len = rs < rows ? rp[r + 1] - b : 0;
                 for (int j = 0; j < width; ++j)
                 {
-                    const int o = base + 32 * j + lane;
+                    // f64: entry j of the slice's 32 rows contiguous; f32: pairs of entries
+                    // (2q, 2q + 1) of a row adjacent, pair q of the 32 rows contiguous
+                    const int o = std::is_same_v<V, float> ? base + 64 * (j >> 1) + 2 * lane + (j & 1)
+                                                           : base + 32 * j + lane;
                     col[o] = j < len ? ci[b + j] : 0;
                     val[o] = static_cast<V>(j < len ? va[b + j] : 0.0);
                 }
@@ -744,7 +783,7 @@ namespace apf
         }
         {
             APF_KERNEL("sell_count", s);
-            sell_count<<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), S->perm.get(), cnt.get());
+            sell_count<<<grid, 256, 0, s>>>(A.rows, slices, A.row_ptr.get(), S->perm.get(), cnt.get(), 0);
         }
         S->rows = A.rows;
         S->slices = slices;
@@ -797,7 +836,7 @@ namespace apf
         }
         {
             APF_KERNEL("sell_count", s);
-            sell_count<<<grid, 256, 0, s>>>(A.rows, S->slices, A.row_ptr.get(), S->perm.get(), cnt.get());
+            sell_count<<<grid, 256, 0, s>>>(A.rows, S->slices, A.row_ptr.get(), S->perm.get(), cnt.get(), 1);
         }
         const long long total = exclusive_scan(cnt.get(), S->slice_ptr.get(), S->slices, s);
         S->col.allocate(static_cast<std::size_t>(total), s);
