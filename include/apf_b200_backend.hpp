@@ -1034,6 +1034,8 @@ namespace la::b200
                     }
             }
         }
+        if (point_cell.size() > static_cast<std::size_t>(std::numeric_limits<int32_t>::max()))
+            throw std::runtime_error("b200 backend: too many flux sample points for one apf_flux_sample call");
         std::vector<double> values(points.size());
         check(ctx, apf_flux_sample(ctx, sys, static_cast<int32_t>(point_cell.size()), point_cell.data(), points.data(),
                                    values.data(), 0),

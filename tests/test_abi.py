@@ -49,3 +49,17 @@ def test_context_creation_without_gpu_reports_error():
     h = ctypes.c_void_p()
     rc = lib.apf_ctx_create(0, None, ctypes.byref(h))
     assert rc == _lib.APF_ERR_NO_DEVICE
+
+
+def test_flux_samples_validates_arguments_on_the_host():
+    """flux_samples checks its shapes before any library call (no device needed)."""
+    import numpy as np
+    import pytest
+    from doubleadapparabolicfem_b200.estimator import flux_samples
+
+    class _Blocks:  # never reached: the shape check raises first
+        ctx = None
+        handle = None
+
+    with pytest.raises(ValueError):
+        flux_samples(_Blocks(), np.zeros(3, dtype=np.int32), np.zeros((2, 3)))
