@@ -23,10 +23,22 @@
  *       solve_saddle_system.hpp:32-121) -> apf_solve_minres_with_rhs (block-preconditioned
  *       MINRES with the reference's true-residual batches) on the device system;
  *   finite_element::time_slabs::compute_adaptive_test_space_iteration<QS, QT, la::b200::Backend>
- *       (src/finite_element/time_slabs/time_slab_adaptive_loop.hpp:727) -> the solve above and
+ *       (src/finite_element/time_slabs/time_slab_adaptive_loop.hpp:727) -> for MINRES +
+ *       ParabolicGraphNorm a device-resident main solve (apf_assemble_main_system,
+ *       apf_assemble_graph_norm, apf_solve_minres or apf_solve_minres_correction,
+ *       apf_system_residual_norms: no host copies of the blocks, no host K, no host B_dt / A_x;
+ *       only the solution comes back), other solvers through the seams above; then
  *       apf_estimate (la::b200::estimate) in place of the reference's host slab
  *       reconstruction, patch flux solves and indicators, then its own combination and
- *       marking (the reference's adaptive driver calls this).
+ *       marking (the reference's adaptive driver calls this);
+ *   adaptive_algorithm::output::detail::write_time_slab_estimator_diagnostics_snapshot for a
+ *       b200 iteration state (algorithm/output/iteration_snapshot_writer.hpp:143-170) -> the
+ *       vertex patches by the reference's writer and flux_reconstruction_samples.bin from the
+ *       flux the device estimate kept (apf_flux_sample).
+ *
+ * la::b200::session() holds the device context, the last system and the solve options;
+ * use_learned_model(path) switches its solves to the learned preconditioner (plain fallback
+ * armed), set_keep_flux(false) drops the kept flux when no snapshots are written.
  *
  * The assembly function is a constrained overload of the reference's own template, and the
  * Schur step and the dispatcher are full specialisations; qualified calls bind to the
