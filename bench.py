@@ -225,7 +225,8 @@ def cpu_reference_sample(args, reps: int, threads: int | None = None):
 def sample_text(info, sample_level):
     return (f"one inner iteration of the reference's own code at outer level {sample_level} of the same mesh family "
             f"({info['n_cells']} prisms, {info['n_dofs']} DOFs): two-pass saddle assembly, slab reconstruction, "
-            f"patch flux solves, indicators; main solve (PARDISO in the reference) not factored and not timed")
+            f"patch flux solves, indicators; main solve (PARDISO in the reference) not factored and not timed; "
+            f"compiled -O3 -DNDEBUG, as the reference's release presets")
 
 
 def run_reference(args, world, rank):
